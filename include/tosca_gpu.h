@@ -1,0 +1,178 @@
+/*
+ * tosca_gpu.h -- C-ABI of the B200 fractional-step time step for TOSCA.
+ *
+ * One context owns one single-domain DMDA-shaped grid on one GPU. Every array
+ * that crosses this boundary is a caller-owned HOST array laid out exactly like
+ * TOSCA's PETSc DMDA arrays: [k][j][i] with i fastest, vectors as interleaved
+ * Cmpnts {x,y,z} triples (base.h:80-84), scalars as PetscReal (double). The
+ * extent is either the global DMDA extent (mx,my,mz) -- halo = 0 -- or the
+ * single-rank local ghosted extent (mx+2h, my+2h, mz+2h) that DMDAVecGetArray
+ * on a local Vec exposes -- halo = h (TOSCA uses h = 3, mesh.c:42).
+ *
+ * The entry points replace the stage functions that TOSCA's time loop calls
+ * (src/main.c:54-327). Each declaration names the reference function it
+ * stands in for. All calls return a tg_status (0 = success) and never exit,
+ * abort or trap; the text of the last error is available from
+ * tg_last_error(). A context is used by one host thread at a time.
+ *
+ * The same declarations, with the prefix "tor_" instead of "tg_", are exported
+ * by the CPU restatement used as the parity checker (oracle/); both libraries
+ * consume the tg_config structure below.
+ */
+#ifndef TOSCA_GPU_H
+#define TOSCA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+typedef enum tg_status {
+    TG_OK                = 0,
+    TG_ERR_CUDA          = 1,  /* a CUDA runtime call failed                      */
+    TG_ERR_BAD_ARG       = 2,  /* invalid argument or unsupported configuration   */
+    TG_ERR_NOT_CONVERGED = 3,  /* Poisson solve hit its iteration cap             */
+    TG_ERR_NAN           = 4,  /* non-finite value detected in the state          */
+    TG_ERR_ALLOC         = 5,  /* device or host allocation failed                */
+    TG_ERR_STATE         = 6   /* call out of order (e.g. step before mesh)       */
+} tg_status;
+
+/* ---------------------------------------------------- boundary patch types -- */
+/* Velocity patch types (boundary/U). Periodic means TOSCA's periodic type 2
+ * (DM_BOUNDARY_PERIODIC, ghost cells at -2 / m+1: mesh.c:129-136). */
+enum {
+    TG_BC_PERIODIC        = 0,
+    TG_BC_NOSLIP          = 1,  /* "noSlip"                                        */
+    TG_BC_SLIP            = 2,  /* "slip"                                          */
+    TG_BC_WALL_SHUMANN    = 3   /* "velocityWallFunction" type -3 (jLeft only)     */
+};
+/* eddy-viscosity patch types (boundary/nut) */
+enum {
+    TG_NUTBC_PERIODIC     = 0,
+    TG_NUTBC_ZEROGRADIENT = 1,
+    TG_NUTBC_FIXEDVALUE   = 2
+};
+/* -divScheme (ueqn.c:82-110) */
+enum { TG_DIV_CENTRAL = 0, TG_DIV_QUICK = 1 };
+/* -dUdtScheme (ueqn.c:123-323) */
+enum { TG_DDT_FE = 0, TG_DDT_RK4 = 1 };
+/* arithmetic of the step */
+enum {
+    TG_PREC_FP64  = 0,   /* every stage in FP64                                   */
+    TG_PREC_MIXED = 1    /* FP32 stencils/RHS/multigrid inside an FP64 outer loop */
+};
+
+/* patch order used by every 6-entry array below */
+enum { TG_ILEFT = 0, TG_IRIGHT = 1, TG_JLEFT = 2, TG_JRIGHT = 3, TG_KLEFT = 4, TG_KRIGHT = 5 };
+
+/* ------------------------------------------------------------ configuration -- */
+typedef struct tg_config {
+    int32_t mx, my, mz;            /* DMDA extent incl. the one-cell physical ghost layer  */
+    int32_t bc[6];                 /* velocity patch types, TG_ILEFT..TG_KRIGHT order       */
+    int32_t nut_bc[6];             /* eddy-viscosity patch types                            */
+    double  nut_bc_value[6];       /* value for TG_NUTBC_FIXEDVALUE patches                 */
+    int32_t curvilinear;           /* -meshFileType curvilinear (wall-stress branch)        */
+    int32_t les;                   /* -les 1: Smagorinsky eddy viscosity                    */
+    double  cs;                    /* Smagorinsky constant as applied to (vol^(1/3))^2|S|;  */
+                                   /* the reference hard-codes 0.0289 (les.c:10,175)        */
+    double  nu;                    /* -nu                                                   */
+    int32_t div_scheme;            /* TG_DIV_*                                              */
+    int32_t ddt_scheme;            /* TG_DDT_*                                              */
+    double  dt;                    /* -timeStep (fixed)                                     */
+    int32_t buoyancy;              /* -potentialT 1 with a frozen temperature field         */
+    double  t_ref;                 /* -tRef                                                 */
+    int32_t mean_grad_p;           /* -meanGradPForce 1                                     */
+    double  mean_grad_p_value[3];  /* -dpdx_mean, -dpdy_mean, -dpdz_mean                    */
+    double  wall_roughness;        /* velocityWallFunction kRough                           */
+    double  wall_kappa;            /* velocityWallFunction kappa                            */
+    double  poisson_rtol;          /* relative residual tolerance of the pressure solve     */
+    double  poisson_div_tol;       /* >0: also stop once dt*max|r*aj| <= this (div bound)   */
+    int32_t poisson_maxit;         /* iteration cap of the pressure solve                   */
+    int32_t precision;             /* TG_PREC_*                                             */
+    int32_t it_start;              /* clock->itStart                                        */
+    int32_t device;                /* CUDA device ordinal (ignored by the CPU restatement)  */
+} tg_config;
+
+/* per-call statistics */
+typedef struct tg_stats {
+    int64_t steps;                 /* steps completed by this call                          */
+    int32_t poisson_iterations;    /* Krylov iterations of the last pressure solve          */
+    int32_t poisson_total_iterations; /* summed over the steps of this call                 */
+    double  poisson_initial_residual;
+    double  poisson_final_residual;/* relative L2 residual of the last solve                */
+    double  max_divergence;        /* ContinuityErrorsOptimized value after the last step   */
+    double  seconds;               /* device (or CPU) time of this call                     */
+} tg_stats;
+
+typedef struct tg_ctx tg_ctx;
+
+/* metric / field selectors for tg_get_field / tg_set_field */
+enum {
+    TG_F_CENT = 0, TG_F_CSI, TG_F_ETA, TG_F_ZET,
+    TG_F_ICSI, TG_F_IETA, TG_F_IZET, TG_F_JCSI, TG_F_JETA, TG_F_JZET,
+    TG_F_KCSI, TG_F_KETA, TG_F_KZET,                                    /* vectors (3 doubles) */
+    TG_F_AJ, TG_F_IAJ, TG_F_JAJ, TG_F_KAJ,                              /* scalars             */
+    TG_F_UCONT, TG_F_UCAT, TG_F_UCONT_O, TG_F_RHS, TG_F_DP, TG_F_BTHETA,/* vectors             */
+    TG_F_P, TG_F_PHI, TG_F_NUT, TG_F_TMPRT,                             /* scalars             */
+    TG_F_TAUWALL,                                                       /* vector, j=0 plane   */
+    TG_F_COUNT
+};
+
+/* ----------------------------------------------------------------- lifecycle -- */
+/* Replaces simulationInitialize's per-domain allocation (initialization.c:63). */
+tg_status tg_create(const tg_config *cfg, tg_ctx **out);
+tg_status tg_destroy(tg_ctx *ctx);
+const char *tg_last_error(const tg_ctx *ctx);
+const char *tg_status_string(tg_status s);
+
+/* Grid nodes (AoS xyz, global extent, node (k,j,i) at DMDA point (k,j,i) for
+ * k<mz-1, j<my-1, i<mx-1; mesh.c:34-447). Computes all cell and face metrics on
+ * the device: replaces SetMeshMetrics (mesh.c:630-1976) and the metric tensor of
+ * SetCoeffMatrix (peqn.c:703-849). */
+tg_status tg_set_mesh_nodes(tg_ctx *ctx, const double *nodes);
+
+/* Generic field transfer (global extent if halo = 0, local ghosted if halo > 0).
+ * Vectors are AoS triples. Used to hand over TOSCA's own metrics and state
+ * (DMDAVecGetArray pointers) and to read results back. */
+tg_status tg_set_field(tg_ctx *ctx, int32_t which, const double *host, int32_t halo);
+tg_status tg_get_field(tg_ctx *ctx, int32_t which, double *host, int32_t halo);
+
+/* Cartesian cell velocity -> ghost cells -> face fluxes. Replaces the common
+ * tail of SetTaylorGreenFieldU / SetABLInitialFlowU (initialField.c:1100-1204):
+ * Ucat interior, UpdateCartesianBCs, face interpolation, UpdateContravariantBCs. */
+tg_status tg_init_from_cartesian(tg_ctx *ctx, const double *ucat, int32_t halo);
+
+/* ------------------------------------------------------------------ stages -- */
+tg_status tg_contravariant_to_cartesian(tg_ctx *ctx);       /* ueqn.c:528-635          */
+tg_status tg_update_nut(tg_ctx *ctx);                       /* les.c:165-180,2119-2578 */
+tg_status tg_update_wall_models(tg_ctx *ctx);               /* boundary.c:3257-3600    */
+tg_status tg_grad_p(tg_ctx *ctx);                           /* peqn.c:3437-3773        */
+tg_status tg_buoyancy(tg_ctx *ctx);                         /* ueqn_sources.c:2726-2880*/
+/* Rhs (TG_F_RHS) += scale * FormU on the current lUcont/lUcat/nut:
+ * ueqn_solvers.c:6-1083 with formMode 0. Rhs is zeroed first when zero_rhs. */
+tg_status tg_form_u(tg_ctx *ctx, double scale, int32_t zero_rhs);
+tg_status tg_explicit_rhs(tg_ctx *ctx);                     /* ueqn_solvers.c:1276-1407*/
+tg_status tg_solve_u(tg_ctx *ctx);                          /* ueqn.c:397-440 (FE, RK4)*/
+tg_status tg_solve_p(tg_ctx *ctx, tg_stats *stats);         /* peqn.c:3777-3971        */
+tg_status tg_continuity_error(tg_ctx *ctx, double *max_div);/* peqn.c:4114-4181        */
+tg_status tg_update_cartesian_bcs(tg_ctx *ctx);             /* boundary.c:824-2050     */
+tg_status tg_update_contravariant_bcs(tg_ctx *ctx);         /* boundary.c:614-822      */
+tg_status tg_sync_pressure(tg_ctx *ctx);                    /* overset.c:263-315       */
+
+/* nsteps full time steps in the order of main.c:54-327 (fixed dt). */
+tg_status tg_step(tg_ctx *ctx, int32_t nsteps, tg_stats *stats);
+
+/* One drop-in step with host state: Ucont, Ucat, P (and nut when LES is on) are
+ * uploaded from the caller's arrays, one step runs, and the same arrays are
+ * overwritten with the new state. This is the call a host time loop makes when
+ * the state lives in its own (PETSc) vectors. */
+tg_status tg_step_host(tg_ctx *ctx, double *ucont, double *ucat, double *p,
+                       double *nut, int32_t halo, tg_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOSCA_GPU_H */

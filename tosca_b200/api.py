@@ -1,0 +1,300 @@
+"""ctypes mirror of the C-ABI in include/tosca_gpu.h.
+
+`Solver` wraps one context of a library that exports the tg_* entry points
+(the CUDA library, prefix "tg_") or the same entry points under another prefix.
+Arrays are numpy float64 in TOSCA's DMDA layout: shape (mz, my, mx) for scalars
+and (mz, my, mx, 3) for Cmpnts vectors, i fastest (base.h:80-84).
+
+The stage methods carry the names of the reference functions they replace so a
+test reads like the reference's time loop (src/main.c:54-327).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+# ------------------------------------------------------------------ constants
+TG_OK, TG_ERR_CUDA, TG_ERR_BAD_ARG, TG_ERR_NOT_CONVERGED, TG_ERR_NAN, TG_ERR_ALLOC, TG_ERR_STATE = range(7)
+
+BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
+NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
+DIV_CENTRAL, DIV_QUICK = 0, 1
+DDT_FE, DDT_RK4 = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+FIELDS = [
+    "CENT", "CSI", "ETA", "ZET", "ICSI", "IETA", "IZET", "JCSI", "JETA", "JZET",
+    "KCSI", "KETA", "KZET", "AJ", "IAJ", "JAJ", "KAJ",
+    "UCONT", "UCAT", "UCONT_O", "RHS", "DP", "BTHETA",
+    "P", "PHI", "NUT", "TMPRT", "TAUWALL",
+]
+F = {name: i for i, name in enumerate(FIELDS)}
+SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT"}
+
+
+class TgConfig(C.Structure):
+    _fields_ = [
+        ("mx", C.c_int32), ("my", C.c_int32), ("mz", C.c_int32),
+        ("bc", C.c_int32 * 6),
+        ("nut_bc", C.c_int32 * 6),
+        ("nut_bc_value", C.c_double * 6),
+        ("curvilinear", C.c_int32),
+        ("les", C.c_int32),
+        ("cs", C.c_double),
+        ("nu", C.c_double),
+        ("div_scheme", C.c_int32),
+        ("ddt_scheme", C.c_int32),
+        ("dt", C.c_double),
+        ("buoyancy", C.c_int32),
+        ("t_ref", C.c_double),
+        ("mean_grad_p", C.c_int32),
+        ("mean_grad_p_value", C.c_double * 3),
+        ("wall_roughness", C.c_double),
+        ("wall_kappa", C.c_double),
+        ("poisson_rtol", C.c_double),
+        ("poisson_div_tol", C.c_double),
+        ("poisson_maxit", C.c_int32),
+        ("precision", C.c_int32),
+        ("it_start", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
+class TgStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("poisson_iterations", C.c_int32),
+        ("poisson_total_iterations", C.c_int32),
+        ("poisson_initial_residual", C.c_double),
+        ("poisson_final_residual", C.c_double),
+        ("max_divergence", C.c_double),
+        ("seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+@dataclass
+class Config:
+    """Python view of tg_config (include/tosca_gpu.h)."""
+    mx: int
+    my: int
+    mz: int
+    bc: tuple = (BC_PERIODIC,) * 6
+    nut_bc: tuple = (NUTBC_PERIODIC,) * 6
+    nut_bc_value: tuple = (0.0,) * 6
+    curvilinear: int = 0
+    les: int = 0
+    cs: float = 0.0289
+    nu: float = 1.0 / 1600.0
+    div_scheme: int = DIV_CENTRAL
+    ddt_scheme: int = DDT_FE
+    dt: float = 0.005
+    buoyancy: int = 0
+    t_ref: float = 300.0
+    mean_grad_p: int = 0
+    mean_grad_p_value: tuple = (0.0, 0.0, 0.0)
+    wall_roughness: float = 0.1
+    wall_kappa: float = 0.4
+    poisson_rtol: float = 1e-14
+    poisson_div_tol: float = 0.0
+    poisson_maxit: int = 5000
+    precision: int = PREC_FP64
+    it_start: int = 0
+    device: int = 0
+
+    def to_c(self) -> TgConfig:
+        c = TgConfig()
+        for name, _ in TgConfig._fields_:
+            v = getattr(self, name)
+            if isinstance(v, (tuple, list)):
+                arr = getattr(c, name)
+                for q, x in enumerate(v):
+                    arr[q] = x
+            else:
+                setattr(c, name, v)
+        return c
+
+    @property
+    def cells(self) -> int:
+        return (self.mx - 2) * (self.my - 2) * (self.mz - 2)
+
+
+_SIGS = {
+    "create": (C.c_int, [C.POINTER(TgConfig), C.POINTER(C.c_void_p)]),
+    "destroy": (C.c_int, [C.c_void_p]),
+    "last_error": (C.c_char_p, [C.c_void_p]),
+    "status_string": (C.c_char_p, [C.c_int]),
+    "set_mesh_nodes": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "set_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "get_field": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]),
+    "init_from_cartesian": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "contravariant_to_cartesian": (C.c_int, [C.c_void_p]),
+    "update_nut": (C.c_int, [C.c_void_p]),
+    "update_wall_models": (C.c_int, [C.c_void_p]),
+    "grad_p": (C.c_int, [C.c_void_p]),
+    "buoyancy": (C.c_int, [C.c_void_p]),
+    "form_u": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
+    "explicit_rhs": (C.c_int, [C.c_void_p]),
+    "solve_u": (C.c_int, [C.c_void_p]),
+    "solve_p": (C.c_int, [C.c_void_p, C.POINTER(TgStats)]),
+    "continuity_error": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "update_cartesian_bcs": (C.c_int, [C.c_void_p]),
+    "update_contravariant_bcs": (C.c_int, [C.c_void_p]),
+    "sync_pressure": (C.c_int, [C.c_void_p]),
+    "step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
+    "step_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
+}
+
+ENTRY_POINTS = tuple(_SIGS)
+
+
+def bind(lib: C.CDLL, prefix: str) -> dict:
+    """Attach argument/return types to every entry point of `lib` and return
+    them keyed by their unprefixed name. Raises AttributeError if one is missing."""
+    out = {}
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, prefix + name)
+        fn.restype = res
+        fn.argtypes = args
+        out[name] = fn
+    return out
+
+
+class TgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Solver:
+    """One tg_ctx. `fns` comes from bind(); the CUDA library is bound by
+    tosca_b200.load()."""
+
+    def __init__(self, cfg: Config, fns: dict):
+        self.cfg = cfg
+        self.fns = fns
+        self._c = cfg.to_c()
+        h = C.c_void_p()
+        st = fns["create"](C.byref(self._c), C.byref(h))
+        if st != TG_OK:
+            raise TgError(st, "create failed: " + fns["status_string"](st).decode())
+        self.h = h
+        self.last_stats = TgStats()
+
+    # ---------------------------------------------------------------- helpers
+    def _check(self, st: int, what: str):
+        if st != TG_OK:
+            msg = self.fns["last_error"](self.h)
+            raise TgError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.fns["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.cfg.mz, self.cfg.my, self.cfg.mx)
+
+    # ------------------------------------------------------------------ data
+    def set_mesh_nodes(self, nodes: np.ndarray):
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        assert nodes.shape == self.shape + (3,)
+        self._check(self.fns["set_mesh_nodes"](self.h, _ptr(nodes)), "set_mesh_nodes")
+
+    def get(self, name: str, halo: int = 0) -> np.ndarray:
+        mz, my, mx = self.shape
+        if name == "TAUWALL":
+            out = np.zeros((mz, mx, 3))
+        else:
+            shp = (mz + 2 * halo, my + 2 * halo, mx + 2 * halo)
+            out = np.zeros(shp if name in SCALAR_FIELDS else shp + (3,))
+        self._check(self.fns["get_field"](self.h, F[name], _ptr(out), halo), f"get_field {name}")
+        return out
+
+    def set(self, name: str, arr: np.ndarray, halo: int = 0):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        self._check(self.fns["set_field"](self.h, F[name], _ptr(arr), halo), f"set_field {name}")
+
+    def init_from_cartesian(self, ucat: np.ndarray, halo: int = 0):
+        ucat = np.ascontiguousarray(ucat, dtype=np.float64)
+        self._check(self.fns["init_from_cartesian"](self.h, _ptr(ucat), halo), "init_from_cartesian")
+
+    # ---------------------------------------------------------------- stages
+    def contravariantToCartesian(self):
+        self._check(self.fns["contravariant_to_cartesian"](self.h), "contravariantToCartesian")
+
+    def UpdateNut(self):
+        self._check(self.fns["update_nut"](self.h), "UpdateNut")
+
+    def UpdateWallModelsU(self):
+        self._check(self.fns["update_wall_models"](self.h), "UpdateWallModelsU")
+
+    def GradP(self):
+        self._check(self.fns["grad_p"](self.h), "GradP")
+
+    def Buoyancy(self):
+        self._check(self.fns["buoyancy"](self.h), "Buoyancy")
+
+    def FormU(self, scale: float = 1.0, zero_rhs: bool = True):
+        self._check(self.fns["form_u"](self.h, scale, 1 if zero_rhs else 0), "FormU")
+
+    def ExplicitRhsU(self):
+        self._check(self.fns["explicit_rhs"](self.h), "ExplicitRhsU")
+
+    def SolveUEqn(self):
+        self._check(self.fns["solve_u"](self.h), "SolveUEqn")
+
+    def SolvePEqn(self) -> TgStats:
+        st = TgStats()
+        self._check(self.fns["solve_p"](self.h, C.byref(st)), "SolvePEqn")
+        return st
+
+    def ContinuityErrorsOptimized(self) -> float:
+        v = C.c_double()
+        self._check(self.fns["continuity_error"](self.h, C.byref(v)), "ContinuityErrorsOptimized")
+        return v.value
+
+    def UpdateCartesianBCs(self):
+        self._check(self.fns["update_cartesian_bcs"](self.h), "UpdateCartesianBCs")
+
+    def UpdateContravariantBCs(self):
+        self._check(self.fns["update_contravariant_bcs"](self.h), "UpdateContravariantBCs")
+
+    def SyncPressureAcrossDomains(self):
+        self._check(self.fns["sync_pressure"](self.h), "SyncPressureAcrossDomains")
+
+    def step(self, n: int = 1) -> TgStats:
+        st = TgStats()
+        self._check(self.fns["step"](self.h, n, C.byref(st)), "step")
+        self.last_stats = st
+        return st
+
+    def step_host(self, ucont, ucat, p, nut=None, halo: int = 0) -> TgStats:
+        st = TgStats()
+        for a in (ucont, ucat, p) + ((nut,) if nut is not None else ()):
+            assert a.flags.c_contiguous and a.dtype == np.float64
+        self._check(self.fns["step_host"](self.h, _ptr(ucont), _ptr(ucat), _ptr(p),
+                                          _ptr(nut) if nut is not None else None, halo, C.byref(st)),
+                    "step_host")
+        return st
