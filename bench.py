@@ -1,0 +1,375 @@
+"""Benchmark of the B200 TOSCA fractional time step.
+
+Workload (default): the neutral pressure-driven ABL, 256 x 256 x 128 cells
+(DMDA extent 258 x 130 x 258), RK4 momentum, Smagorinsky LES, Schumann wall
+stress, slip top, periodic x/y, pressure solved until the divergence bound
+dt * max|r aj| <= 5e-9 holds (ContinuityErrorsOptimized definition).
+Synthetic seeded inputs (log-law + splitmix64 perturbations); every field is
+larger than the 126 MB L2, so no flush is needed between steps.
+
+One JSON line is printed by rank 0. `--impl reference` times the CPU
+restatement of the reference step (the reference itself cannot be built:
+no MPI/PETSc/HYPRE) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s mixed vs FP64 GPU at div≤1e-8; adjoint/forward time ratio"
+UNIT = "Mcell-steps/s"
+DIV_TOL = 5e-9
+
+# algorithmic bytes per interior cell of one launch (FP64 storage; each array
+# counted once per read and once per write; metrics re-read every launch)
+BYTES_PER_CELL = {
+    "formu_face_fluxes": 46 * 8,   # ucat 3, ucont 3, nut 1, face metrics 30 -> fluxes 9
+    "formu_cell_fp": 12 * 8,       # fluxes 9 -> fp 3
+    "formu_rhs_faces": 21 * 8,     # fp 3, csi/eta/zet 9, face aj 3, rhs 3 -> rhs 3
+    "contra_to_cart": 15 * 8,      # ucont 3, csi/eta/zet 9 -> ucat 3
+    "smagorinsky": 14 * 8,         # ucat 3, csi/eta/zet 9, aj 1 -> nut 1
+    "grad_p": 34 * 8,              # p 1, face metrics 27 + 3 -> dp 3
+    "project": 37 * 8,             # phi 1, face metrics 30, ucont 3 -> ucont 3
+    "pois_apply7": 5 * 8,          # x 1, 3 coefficients -> y 1
+    "pois_apply19": 11 * 8,        # x 1, 9 coefficients -> y 1
+    "mg_smooth_line_L0": 44,       # half the lines: r, aE, aN, aT, diag, x(nb) 6 -> x, tc, td 3 + tc, td re-read 2
+    "mg_smooth_rb_L0": 40,         # half the cells: r, diag, 3+3 coefficients, x(nb) -> x
+    "mg_restrict_L0": 50,          # r, x, 3 coefficients, diag -> coarse r, x (1/8)
+    "mg_prolong_L0": 17,           # x read/write, coarse x (1/8)
+    "pois_cg_update": 48,          # x, r read/write; p, q read
+    "pois_cg_dir": 24,             # z, p read; p write
+    "pois_dot": 16,                # two vectors
+    "rk_stage": 72,                # y = a x + z over 3 components
+    "rk_accumulate": 72,           # y += a x over 3 components
+    "rhs_init": 48,                # dp 3 -> rhs 3
+}
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(name, precision, seed_offset=0, small=False):
+    from tosca_b200 import api, cases
+    if name == "abl":
+        kw = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=250.0) if small else {}
+        cfg, nodes, ucat, p = cases.abl_case(ddt=api.DDT_RK4, seed=20261203 + seed_offset, **kw)
+        T = None
+        desc = "ABL %dx%dx%d cells, RK4, Smagorinsky, Schumann wall, dt=0.25 s" % (
+            cfg.mz - 2, cfg.mx - 2, cfg.my - 2)
+    elif name == "tgv":
+        cfg, nodes, ucat, p = cases.tgv_case(32 if small else 64, ddt=api.DDT_RK4)
+        T = None
+        desc = "Taylor-Green vortex %d^3, RK4, dt=0.005" % (cfg.mx - 2)
+    elif name == "hill":
+        kw = dict(nx=48, ny=24, nz=24) if small else {}
+        cfg, nodes, ucat, p, T = cases.hill_case(ddt=api.DDT_RK4, **kw)
+        desc = "cosine hill %dx%dx%d cells, QUICK, buoyancy, RK4" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    cfg.poisson_rtol = 1e-30
+    cfg.poisson_div_tol = DIV_TOL
+    cfg.poisson_maxit = 400
+    cfg.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
+    return cfg, nodes, ucat, p, T, desc
+
+
+def cpu_baseline(workload, steps, threads=None):
+    """CPU restatement of the reference step on a bounded sample of the
+    workload (same physics, fewer cells), all host threads."""
+    import oracle
+    from tosca_b200 import cases
+    cfg, nodes, ucat, p, T, desc = make_workload(workload, "fp64", small=True)
+    cfg.poisson_rtol = 1e-8          # the reference's default poissonTol (peqn.c:54)
+    cfg.poisson_div_tol = 0.0
+    cfg.poisson_maxit = 20000
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    s.step(1)                        # warm-up
+    t0 = time.perf_counter()
+    st = s.step(steps)
+    dt = time.perf_counter() - t0
+    cells = cfg.cells
+    ncores = oracle.lib().tor_num_threads()
+    s.close()
+    return {
+        "value": cells * steps / dt / 1e6, "unit": UNIT, "cores": int(ncores), "kind": "port",
+        "sample": f"{desc}; {steps} timed steps after 1 warm-up; Jacobi-preconditioned CG to the reference's "
+                  f"poissonTol 1e-8 (oracle, OpenMP)",
+        "seconds": dt, "max_divergence": st.max_divergence,
+    }
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    steps = max(1, args.steps)
+    base = cpu_baseline(args.workload, steps)
+    line = {
+        "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": base["seconds"] / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": base["sample"]},
+        "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "TOSCA needs mpicxx + PETSc 3.15 + HYPRE 2.20 (absent); the reference arm times the CPU restatement",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--profile-json", default=None, help="write per-kernel timings here")
+    args = ap.parse_args()
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import tosca_b200
+    from tosca_b200 import cases
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    cfg, nodes, ucat, p, T, desc = make_workload(args.workload, args.precision, seed_offset=rank)
+    cfg.device = dev
+    solver = tosca_b200.gpu_solver(cfg)
+    cases.setup(solver, nodes, ucat, p, T)
+    lib = solver.fns
+    import ctypes
+    L = ctypes.CDLL(tosca_b200.LIB_PATH)
+    L.tg_prof_enable.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.tg_prof_reset.argtypes = [ctypes.c_void_p]
+    L.tg_prof_count.argtypes = [ctypes.c_void_p]
+    L.tg_prof_count.restype = ctypes.c_int32
+    L.tg_prof_get.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p,
+                              ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    if args.warmup > 0:
+        solver.step(args.warmup)
+
+    # timed region (device events on the library's stream), per-kernel events live
+    L.tg_prof_reset(solver.h)
+    L.tg_prof_enable(solver.h, 1)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        st = solver.step(args.steps)
+        torch.cuda.synchronize()
+    barrier()
+    L.tg_prof_enable(solver.h, 0)
+    t_dev = max_over_ranks(st.seconds)
+    clocks = clk.summary()
+    cells = cfg.cells
+    value = cells * args.steps * world / t_dev / 1e6
+
+    # per-kernel accounting
+    kernels = {}
+    nb = ctypes.create_string_buffer(64)
+    for q in range(L.tg_prof_count(solver.h)):
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        L.tg_prof_get(solver.h, q, nb, ctypes.byref(n), ctypes.byref(ms))
+        kernels[nb.value.decode()] = {"launches": int(n.value), "ms": float(ms.value)}
+    total_k = sum(v["ms"] for v in kernels.values())
+    for v in kernels.values():
+        v["share"] = v["ms"] / total_k if total_k > 0 else 0.0
+    ranked = sorted(kernels.items(), key=lambda kv: -kv[1]["ms"])
+    dom = next((k for k, v in ranked if k in BYTES_PER_CELL), None)
+    peak, peak_src = load_peaks()
+    roofline = None
+    if dom is not None:
+        kv = kernels[dom]
+        per_launch_ms = kv["ms"] / kv["launches"]
+        algo_bytes = BYTES_PER_CELL[dom] * cells
+        achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tj = json.load(f)
+            if dom in tj:
+                traffic = tj[dom] * cells
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                    "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_ms": per_launch_ms,
+                    "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src}
+
+    # end-to-end through the C-ABI with host buffers (drop-in call per step)
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(2, args.steps // 2)
+    mz, my, mx = cfg.mz, cfg.my, cfg.mx
+    h_ucont = torch.empty((mz, my, mx, 3), dtype=torch.float64, pin_memory=True).numpy()
+    h_ucat = torch.empty((mz, my, mx, 3), dtype=torch.float64, pin_memory=True).numpy()
+    h_p = torch.empty((mz, my, mx), dtype=torch.float64, pin_memory=True).numpy()
+    h_nut = torch.empty((mz, my, mx), dtype=torch.float64, pin_memory=True).numpy()
+    h_ucont[...] = solver.get("UCONT")
+    h_ucat[...] = solver.get("UCAT")
+    h_p[...] = solver.get("P")
+    h_nut[...] = solver.get("NUT")
+    nut_arg = h_nut if cfg.les else None
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        se = solver.step_host(h_ucont, h_ucat, h_p, nut_arg)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    bytes_state = h_ucont.nbytes + h_ucat.nbytes + h_p.nbytes + (h_nut.nbytes if cfg.les else 0)
+    e2e = {"value": cells * e2e_steps * world / t_e2e / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": int(bytes_state), "d2h_bytes_per_step": int(bytes_state),
+           "steps": e2e_steps, "max_divergence": se.max_divergence}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.workload, args.cpu_steps)
+        cpu = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": desc, "cells": cells, "dmda_extent": [mx, my, mz],
+                       "precision": args.precision, "divergence_bound": DIV_TOL,
+                       "l2": "every field exceeds the 126 MB L2; no flush",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "poisson_iterations_last": st.poisson_iterations,
+                       "poisson_iterations_per_step": st.poisson_total_iterations / max(1, args.steps),
+                       "max_divergence": st.max_divergence},
+            "clocks": clocks,
+            "e2e": e2e,
+            "gpu_launches": int(sum(v["launches"] for v in kernels.values())),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "kernels_top": {k: {"ms": round(v["ms"], 3), "launches": v["launches"], "share": round(v["share"], 4)}
+                            for k, v in ranked[:12]},
+        }
+        print(json.dumps(line), flush=True)
+        if args.profile_json:
+            with open(args.profile_json, "w") as f:
+                json.dump({"kernels": kernels, "cells": cells, "steps": args.steps}, f, indent=1)
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,56 @@
+"""Shared helpers of the parity tests: build both the CUDA solver and the CPU
+restatement (oracle) on the same case and compare fields."""
+from __future__ import annotations
+
+import numpy as np
+
+import oracle
+import tosca_b200
+from tosca_b200 import cases
+
+
+def interior(a: np.ndarray) -> np.ndarray:
+    return a[1:-1, 1:-1, 1:-1]
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray, region=interior) -> float:
+    a, b = region(a), region(b)
+    den = np.linalg.norm(b.ravel())
+    num = np.linalg.norm((a - b).ravel())
+    return float(num / den) if den > 0 else float(num)
+
+
+def max_abs(a, b) -> float:
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))))
+
+
+def build_case(name: str, **kw):
+    if name == "tgv":
+        cfg, nodes, ucat, p = cases.tgv_case(**kw)
+        return cfg, nodes, ucat, p, None
+    if name == "abl":
+        cfg, nodes, ucat, p = cases.abl_case(**kw)
+        return cfg, nodes, ucat, p, None
+    if name == "hill":
+        return cases.hill_case(**kw)
+    raise ValueError(name)
+
+
+def pair(name: str, cfg_over=None, **kw):
+    """(gpu_solver, oracle_solver) set up identically."""
+    cfg, nodes, ucat, p, T = build_case(name, **kw)
+    if cfg_over:
+        for k, v in cfg_over.items():
+            setattr(cfg, k, v)
+    g = tosca_b200.gpu_solver(cfg)
+    o = oracle.solver(cfg)
+    for s in (g, o):
+        cases.setup(s, nodes, ucat, p, T)
+    return g, o
+
+
+SMALL = {
+    "tgv": dict(n=16),
+    "abl": dict(nx=16, ny=16, nz=12, Lx=160.0, Ly=160.0, H=100.0),
+    "hill": dict(nx=24, ny=12, nz=12),
+}

@@ -1,0 +1,194 @@
+// Internal declarations of the B200 TOSCA time-step library.
+//
+// Device layout: every field lives on the global DMDA extent (mx, my, mz),
+// [k][j][i] with i fastest, as structure-of-arrays (one contiguous plane per
+// vector component) so that a warp reading 32 consecutive i issues one
+// 256-byte coalesced transaction per component. Out-of-range indices of a
+// periodic direction wrap modulo the extent, which is exactly what a
+// single-rank PETSc local vector returns for DM_BOUNDARY_PERIODIC.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tosca_gpu.h"
+
+namespace tg {
+
+// ------------------------------------------------------------------- grid --
+struct Grid {
+    int mx, my, mz;
+    int pi, pj, pk;   // periodic (type 2) per direction
+
+    __host__ __device__ __forceinline__ int wi(int i) const { if (pi) { if (i < 0) i += mx; else if (i >= mx) i -= mx; } return i; }
+    __host__ __device__ __forceinline__ int wj(int j) const { if (pj) { if (j < 0) j += my; else if (j >= my) j -= my; } return j; }
+    __host__ __device__ __forceinline__ int wk(int k) const { if (pk) { if (k < 0) k += mz; else if (k >= mz) k -= mz; } return k; }
+    // wrapped linear index (callers guarantee in-range indices in non-periodic directions)
+    __host__ __device__ __forceinline__ int id(int k, int j, int i) const { return (wk(k) * my + wj(j)) * mx + wi(i); }
+    // unwrapped linear index
+    __host__ __device__ __forceinline__ int lin(int k, int j, int i) const { return (k * my + j) * mx + i; }
+    __host__ __device__ __forceinline__ int64_t size() const { return (int64_t)mx * my * mz; }
+};
+
+// SoA vector field (three planes of the same extent)
+template <class T>
+struct V3f {
+    T *x, *y, *z;
+};
+
+template <class T>
+struct R3 { T x, y, z; };
+
+template <class T>
+__device__ __forceinline__ R3<T> ld3(const V3f<T> &f, int q) { return R3<T>{f.x[q], f.y[q], f.z[q]}; }
+template <class T>
+__device__ __forceinline__ void st3(const V3f<T> &f, int q, R3<T> v) { f.x[q] = v.x; f.y[q] = v.y; f.z[q] = v.z; }
+template <class T>
+__device__ __forceinline__ R3<T> operator+(R3<T> a, R3<T> b) { return R3<T>{a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T>
+__device__ __forceinline__ R3<T> operator-(R3<T> a, R3<T> b) { return R3<T>{a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T>
+__device__ __forceinline__ R3<T> operator*(T s, R3<T> a) { return R3<T>{s * a.x, s * a.y, s * a.z}; }
+template <class T>
+__device__ __forceinline__ T dot3(R3<T> a, R3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// metric fields (mesh.c:630-1976) on the device
+struct Metrics {
+    V3f<double> cent, csi, eta, zet, icsi, ieta, izet, jcsi, jeta, jzet, kcsi, keta, kzet;
+    double *aj, *iaj, *jaj, *kaj;
+    // face metric tensor g_qr * face-aj with boundary remapping (peqn.c:791-849)
+    double *g11, *g12, *g13, *g21, *g22, *g23, *g31, *g32, *g33;
+};
+
+// physical state and work arrays
+struct State {
+    V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, fp, f1, f2, f3, snap;
+    double *p, *phi, *nut, *tmprt, *ssnap;
+    // jLeft wall model (plane mz x mx)
+    double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
+};
+
+struct Params {
+    int bc[6];
+    int nut_bc[6];
+    double nut_bc_value[6];
+    int curvilinear, les, div_scheme, buoyancy, mean_grad_p;
+    double cs, nu, dt, t_ref, mgp[3], z0, kappa;
+};
+
+struct PoissonCtx;   // tg_poisson.cu
+
+// per-kernel event timing (tosca_gpu_prof.h)
+struct ProfPending { int slot; cudaEvent_t a, b; };
+struct ProfAcc { std::string name; int64_t launches = 0; double ms = 0.0; };
+struct Profiler {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t next = 0;
+    std::vector<ProfPending> pending;
+    std::vector<ProfAcc> acc;
+    int slot(const char *name);
+};
+
+}  // namespace tg
+
+struct tg_ctx {
+    tg_config cfg{};
+    tg::Grid g{};
+    tg::Params prm{};
+    tg::Metrics m{};
+    tg::State s{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void *> allocs;          // every device allocation of this context
+    double *d_red = nullptr;             // reduction scratch (partials)
+    double *d_scal = nullptr;            // device scalars
+    double *h_scal = nullptr;            // pinned host mirror of scalars
+    double *stage = nullptr;             // staging buffer for AoS host transfers
+    size_t stage_bytes = 0;
+    int red_blocks = 0;
+    bool has_mesh = false;
+    bool orthogonal = true;              // all cross metric-tensor terms vanish
+    bool ufilt_set = false;
+    int it = 0;
+    std::string err;
+    tg::PoissonCtx *pois = nullptr;
+    tg::Profiler prof;
+};
+
+namespace tg {
+
+// error helpers ----------------------------------------------------------------
+struct CudaError {
+    cudaError_t e;
+    const char *what;
+};
+#define TG_CUDA(call)                                                            \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) throw ::tg::CudaError{_e, #call};                 \
+    } while (0)
+
+void *dalloc(tg_ctx *C, size_t bytes);        // zeroed device allocation owned by C
+inline double *dallocd(tg_ctx *C, size_t n) { return (double *)dalloc(C, n * sizeof(double)); }
+V3f<double> dalloc3(tg_ctx *C, size_t n);
+
+// NaN-propagating maximum (fmax ignores NaN operands)
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
+
+// profiling brackets around one kernel launch on C->stream
+void prof_begin(tg_ctx *C, const char *name, cudaEvent_t *a, cudaEvent_t *b, int *slot);
+void prof_end(tg_ctx *C, cudaEvent_t a, cudaEvent_t b, int slot);
+void prof_flush(tg_ctx *C);
+#define TG_PROF(C, name, ...)                                                       \
+    do {                                                                               \
+        if ((C)->prof.on) {                                                            \
+            cudaEvent_t _a, _b; int _s;                                                \
+            ::tg::prof_begin((C), (name), &_a, &_b, &_s);                              \
+            __VA_ARGS__;                                                               \
+            ::tg::prof_end((C), _a, _b, _s);                                           \
+        } else {                                                                       \
+            __VA_ARGS__;                                                                    \
+        }                                                                              \
+    } while (0)
+
+// launch helpers: 3-D blocks with i fastest
+constexpr int BX = 32, BY = 4, BZ = 2;
+inline dim3 grid3(int ni, int nj, int nk) { return dim3((ni + BX - 1) / BX, (nj + BY - 1) / BY, (nk + BZ - 1) / BZ); }
+inline dim3 block3() { return dim3(BX, BY, BZ); }
+
+// stage entry points (tg_step.cu)
+void metrics_from_nodes(tg_ctx *C, const double *d_nodes);
+void contra_to_cart(tg_ctx *C);
+void reset_cell_periodic(tg_ctx *C, V3f<double> v);
+void reset_cell_periodic_s(tg_ctx *C, double *v);
+void reset_face_periodic(tg_ctx *C, V3f<double> v);
+void reset_no_penetration(tg_ctx *C);
+void update_cartesian_bcs(tg_ctx *C);
+void update_contravariant_bcs(tg_ctx *C);
+void update_scalar_ghosts(tg_ctx *C, double *v);
+void update_nut(tg_ctx *C);
+void update_wall_models(tg_ctx *C);
+void grad_p(tg_ctx *C);
+void buoyancy(tg_ctx *C);
+void form_u(tg_ctx *C, V3f<double> rhs, double scale);
+void explicit_rhs(tg_ctx *C);
+void solve_u(tg_ctx *C);
+int solve_p(tg_ctx *C, tg_stats *st);
+double continuity_error(tg_ctx *C);
+void sync_pressure(tg_ctx *C);
+void init_from_cartesian(tg_ctx *C);
+int step(tg_ctx *C, tg_stats *st);
+
+// device reductions (tg_reduce.cu): result written to d_out[0]
+void reduce_max_abs_div(tg_ctx *C, double *d_out);
+
+// Poisson (tg_poisson.cu)
+void poisson_setup(tg_ctx *C);
+void poisson_destroy(tg_ctx *C);
+int poisson_solve(tg_ctx *C, tg_stats *st);
+
+}  // namespace tg

@@ -1,0 +1,772 @@
+// Pressure Poisson solve for TOSCA's pinned 19-point operator (peqn.c:703-1501)
+// replacing the HYPRE BoomerAMG-GMRES solve (peqn.c:3856-3929).
+//
+// Unknowns live in a compact interior layout c = (kc*ny + jc)*nx + ic
+// (ic = i-1, ...). The operator is applied matrix-free from the nine face
+// metric-tensor arrays g11..g33 at the east/north/top face of each cell; the
+// 19 coefficients of a row are rebuilt in registers with the reference's
+// one-sided rules and its |v| > 1e-10 insertion filter, so the product equals
+// the assembled matrix. On orthogonal grids (all cross terms zero) a 7-point
+// kernel reads three coefficient arrays only.
+//
+// Solved system: L phi = -b with L = -A (positive semidefinite away from the
+// pinned row), row (1,1,1) the identity (peqn.c:883-887). Symmetric operators
+// use preconditioned CG on the reduced system (the pinned unknown stays zero);
+// others use right-preconditioned BiCGStab.
+//
+// Preconditioner: geometric multigrid V-cycle on the 7-point part of the
+// operator with face-sum coarse coefficients, piecewise-constant transfers,
+// red-black point or j-line zebra Gauss-Seidel smoothing and a dense
+// pseudo-inverse on the coarsest grid; applied in the grounded form
+// z = P M P^T r (P shifts so that z at the pinned cell is zero), which is
+// the exact inverse structure of the pinned operator.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tg_internal.cuh"
+
+namespace tg {
+
+struct MGLevel {
+    int nx, ny, nz, pi, pj, pk;
+    int cx, cy, cz;              // coarsening factors towards the next level
+    int64_t n;
+    double *aE, *aN, *aT, *diag; // face coefficients of the east/north/top faces; diagonal
+    double *x, *r;               // unknown and right-hand side
+    double *tc, *td;             // Thomas scratch of the line smoother
+};
+
+struct PoissonCtx {
+    int nx, ny, nz, pi, pj, pk;
+    int64_t n;
+    int pin;                     // compact index of the pinned cell (0)
+    bool ortho;
+    bool line;                   // j-line smoothing (j non-periodic)
+    double *gE1, *gE2, *gE3, *gN1, *gN2, *gN3, *gT1, *gT2, *gT3;  // fine face tensors (compact)
+    double *x, *b, *r, *z, *p, *q, *rhat, *v, *s, *t, *aj;
+    double *part;                // reduction partials (4 per block)
+    int nblocks;
+    MGLevel L[16];               // multigrid levels, finest first (plain data: passed to kernels by value)
+    int nlev;
+    double *Binv;                // dense coarsest inverse (n_c x n_c)
+    int ncoarse;
+    int nu1, nu2;
+};
+
+namespace {
+
+constexpr int RB = 256;   // reduction block size
+
+struct Cg {   // compact grid indexing with periodic wrap
+    int nx, ny, nz, pi, pj, pk;
+    __device__ __forceinline__ int wi(int i) const { if (i < 0) i += nx; else if (i >= nx) i -= nx; return i; }
+    __device__ __forceinline__ int wj(int j) const { if (j < 0) j += ny; else if (j >= ny) j -= ny; return j; }
+    __device__ __forceinline__ int wk(int k) const { if (k < 0) k += nz; else if (k >= nz) k -= nz; return k; }
+    __device__ __forceinline__ int id(int k, int j, int i) const { return (wk(k) * ny + wj(j)) * nx + wi(i); }
+    __device__ __forceinline__ bool in(int k, int j, int i) const {
+        return (pi || (i >= 0 && i < nx)) && (pj || (j >= 0 && j < ny)) && (pk || (k >= 0 && k < nz));
+    }
+};
+
+// ------------------------------------------------------------ setup kernels
+__global__ void k_gather_g(Grid g, Metrics m, PoissonCtx P)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    int c = (kc * P.ny + jc) * P.nx + ic;
+    int d = g.lin(kc + 1, jc + 1, ic + 1);
+    P.gE1[c] = m.g11[d]; P.gE2[c] = m.g12[d]; P.gE3[c] = m.g13[d];
+    P.gN1[c] = m.g21[d]; P.gN2[c] = m.g22[d]; P.gN3[c] = m.g23[d];
+    P.gT1[c] = m.g31[d]; P.gT2[c] = m.g32[d]; P.gT3[c] = m.g33[d];
+    P.aj[c] = m.aj[d];
+}
+
+// 7-point part of the fine operator: masked normal coefficients
+__global__ void k_level0_coeffs(PoissonCtx P, MGLevel L0)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    int c = (kc * P.ny + jc) * P.nx + ic;
+    L0.aE[c] = (ic < P.nx - 1 || P.pi) ? P.gE1[c] : 0.0;
+    L0.aN[c] = (jc < P.ny - 1 || P.pj) ? P.gN2[c] : 0.0;
+    L0.aT[c] = (kc < P.nz - 1 || P.pk) ? P.gT3[c] : 0.0;
+}
+
+__global__ void k_diag(MGLevel L)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= L.nx || jc >= L.ny || kc >= L.nz) return;
+    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
+    int c = (kc * L.ny + jc) * L.nx + ic;
+    double aW = (ic > 0 || L.pi) ? L.aE[q.id(kc, jc, ic - 1)] : 0.0;
+    double aS = (jc > 0 || L.pj) ? L.aN[q.id(kc, jc - 1, ic)] : 0.0;
+    double aB = (kc > 0 || L.pk) ? L.aT[q.id(kc - 1, jc, ic)] : 0.0;
+    L.diag[c] = L.aE[c] + aW + L.aN[c] + aS + L.aT[c] + aB;
+}
+
+// face-sum coarse coefficients: a_coarse = s * sum of the fine faces covering
+// the coarse face, s = 1/2 when the face-normal direction is coarsened
+__global__ void k_coarsen_coeffs(MGLevel F, MGLevel Cc)
+{
+    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
+    int c = (K * Cc.ny + J) * Cc.nx + I;
+    double sE = 0.0, sN = 0.0, sT = 0.0;
+    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) {
+        int fi = F.cx * I + F.cx - 1, fj = F.cy * J + dj, fk = F.cz * K + dk;
+        sE += F.aE[(fk * F.ny + fj) * F.nx + fi];
+    }
+    for (int dk = 0; dk < F.cz; dk++) for (int di = 0; di < F.cx; di++) {
+        int fi = F.cx * I + di, fj = F.cy * J + F.cy - 1, fk = F.cz * K + dk;
+        sN += F.aN[(fk * F.ny + fj) * F.nx + fi];
+    }
+    for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
+        int fi = F.cx * I + di, fj = F.cy * J + dj, fk = F.cz * K + F.cz - 1;
+        sT += F.aT[(fk * F.ny + fj) * F.nx + fi];
+    }
+    Cc.aE[c] = sE * (F.cx == 2 ? 0.5 : 1.0);
+    Cc.aN[c] = sN * (F.cy == 2 ? 0.5 : 1.0);
+    Cc.aT[c] = sT * (F.cz == 2 ? 0.5 : 1.0);
+}
+
+// --------------------------------------------------------- fine operators
+// 7-point: (L x)_c = sum_f a_f (x_c - x_nb); pinned row = identity
+__global__ void k_apply7(PoissonCtx P, const double *__restrict__ x, double *__restrict__ y)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    Cg q{P.nx, P.ny, P.nz, P.pi, P.pj, P.pk};
+    int c = (kc * P.ny + jc) * P.nx + ic;
+    if (c == P.pin) { y[c] = x[c]; return; }
+    double xc = x[c], acc = 0.0;
+    if (ic < P.nx - 1 || P.pi) acc += P.gE1[c] * (xc - x[q.id(kc, jc, ic + 1)]);
+    if (ic > 0 || P.pi)        { int w = q.id(kc, jc, ic - 1); acc += P.gE1[w] * (xc - x[w]); }
+    if (jc < P.ny - 1 || P.pj) acc += P.gN2[c] * (xc - x[q.id(kc, jc + 1, ic)]);
+    if (jc > 0 || P.pj)        { int s = q.id(kc, jc - 1, ic); acc += P.gN2[s] * (xc - x[s]); }
+    if (kc < P.nz - 1 || P.pk) acc += P.gT3[c] * (xc - x[q.id(kc + 1, jc, ic)]);
+    if (kc > 0 || P.pk)        { int b = q.id(kc - 1, jc, ic); acc += P.gT3[b] * (xc - x[b]); }
+    y[c] = acc;
+}
+
+enum { CP, EP, WP, NP, SP, TP, BP, NE, SE, NW, SW, TN, BN, TS, BS, TE, BE, TW, BW, NST };
+
+// 19 coefficients of one row of SetCoeffMatrix (peqn.c:889-1388)
+__device__ void row19(const PoissonCtx &P, const Cg &q, int ic, int jc, int kc, double vol[NST])
+{
+    for (int m = 0; m < NST; m++) vol[m] = 0.0;
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const bool jr = jc == ny - 1, jl = jc == 0, kr = kc == nz - 1, kl = kc == 0, ir = ic == nx - 1, il = ic == 0;
+    int c = (kc * ny + jc) * nx + ic;
+    if (!ir || P.pi) {   // east
+        double a = P.gE1[c], b = P.gE2[c], cc = P.gE3[c];
+        vol[CP] -= a; vol[EP] += a;
+        if (jr)      { vol[CP] += b * 0.5; vol[EP] += b * 0.5; vol[SP] -= b * 0.5; vol[SE] -= b * 0.5; }
+        else if (jl) { vol[NP] += b * 0.5; vol[NE] += b * 0.5; vol[CP] -= b * 0.5; vol[EP] -= b * 0.5; }
+        else         { vol[NP] += b * 0.25; vol[NE] += b * 0.25; vol[SP] -= b * 0.25; vol[SE] -= b * 0.25; }
+        if (kr)      { vol[CP] += cc * 0.5; vol[EP] += cc * 0.5; vol[BP] -= cc * 0.5; vol[BE] -= cc * 0.5; }
+        else if (kl) { vol[TP] += cc * 0.5; vol[TE] += cc * 0.5; vol[CP] -= cc * 0.5; vol[EP] -= cc * 0.5; }
+        else         { vol[TP] += cc * 0.25; vol[TE] += cc * 0.25; vol[BP] -= cc * 0.25; vol[BE] -= cc * 0.25; }
+    }
+    if (!il || P.pi) {   // west
+        int w = q.id(kc, jc, ic - 1);
+        double a = P.gE1[w], b = P.gE2[w], cc = P.gE3[w];
+        vol[CP] -= a; vol[WP] += a;
+        if (jr)      { vol[CP] -= b * 0.5; vol[WP] -= b * 0.5; vol[SP] += b * 0.5; vol[SW] += b * 0.5; }
+        else if (jl) { vol[NP] -= b * 0.5; vol[NW] -= b * 0.5; vol[CP] += b * 0.5; vol[WP] += b * 0.5; }
+        else         { vol[NP] -= b * 0.25; vol[NW] -= b * 0.25; vol[SP] += b * 0.25; vol[SW] += b * 0.25; }
+        if (kr)      { vol[CP] -= cc * 0.5; vol[WP] -= cc * 0.5; vol[BP] += cc * 0.5; vol[BW] += cc * 0.5; }
+        else if (kl) { vol[TP] -= cc * 0.5; vol[TW] -= cc * 0.5; vol[CP] += cc * 0.5; vol[WP] += cc * 0.5; }
+        else         { vol[TP] -= cc * 0.25; vol[TW] -= cc * 0.25; vol[BP] += cc * 0.25; vol[BW] += cc * 0.25; }
+    }
+    if (!jr || P.pj) {   // north
+        double a = P.gN1[c], b = P.gN2[c], cc = P.gN3[c];
+        if (ir)      { vol[CP] += a * 0.5; vol[NP] += a * 0.5; vol[WP] -= a * 0.5; vol[NW] -= a * 0.5; }
+        else if (il) { vol[EP] += a * 0.5; vol[NE] += a * 0.5; vol[CP] -= a * 0.5; vol[NP] -= a * 0.5; }
+        else         { vol[EP] += a * 0.25; vol[NE] += a * 0.25; vol[WP] -= a * 0.25; vol[NW] -= a * 0.25; }
+        vol[CP] -= b; vol[NP] += b;
+        if (kr)      { vol[CP] += cc * 0.5; vol[NP] += cc * 0.5; vol[BP] -= cc * 0.5; vol[BN] -= cc * 0.5; }
+        else if (kl) { vol[TP] += cc * 0.5; vol[TN] += cc * 0.5; vol[CP] -= cc * 0.5; vol[NP] -= cc * 0.5; }
+        else         { vol[TP] += cc * 0.25; vol[TN] += cc * 0.25; vol[BP] -= cc * 0.25; vol[BN] -= cc * 0.25; }
+    }
+    if (!jl || P.pj) {   // south
+        int s = q.id(kc, jc - 1, ic);
+        double a = P.gN1[s], b = P.gN2[s], cc = P.gN3[s];
+        if (ir)      { vol[CP] -= a * 0.5; vol[SP] -= a * 0.5; vol[WP] += a * 0.5; vol[SW] += a * 0.5; }
+        else if (il) { vol[EP] -= a * 0.5; vol[SE] -= a * 0.5; vol[CP] += a * 0.5; vol[SP] += a * 0.5; }
+        else         { vol[EP] -= a * 0.25; vol[SE] -= a * 0.25; vol[WP] += a * 0.25; vol[SW] += a * 0.25; }
+        vol[CP] -= b; vol[SP] += b;
+        if (kr)      { vol[CP] -= cc * 0.5; vol[SP] -= cc * 0.5; vol[BP] += cc * 0.5; vol[BS] += cc * 0.5; }
+        else if (kl) { vol[TP] -= cc * 0.5; vol[TS] -= cc * 0.5; vol[CP] += cc * 0.5; vol[SP] += cc * 0.5; }
+        else         { vol[TP] -= cc * 0.25; vol[TS] -= cc * 0.25; vol[BP] += cc * 0.25; vol[BS] += cc * 0.25; }
+    }
+    if (!kr || P.pk) {   // top
+        double a = P.gT1[c], b = P.gT2[c], cc = P.gT3[c];
+        if (ir)      { vol[CP] += a * 0.5; vol[TP] += a * 0.5; vol[WP] -= a * 0.5; vol[TW] -= a * 0.5; }
+        else if (il) { vol[EP] += a * 0.5; vol[TE] += a * 0.5; vol[CP] -= a * 0.5; vol[TP] -= a * 0.5; }
+        else         { vol[EP] += a * 0.25; vol[TE] += a * 0.25; vol[WP] -= a * 0.25; vol[TW] -= a * 0.25; }
+        if (jr)      { vol[CP] += b * 0.5; vol[TP] += b * 0.5; vol[SP] -= b * 0.5; vol[TS] -= b * 0.5; }
+        else if (jl) { vol[NP] += b * 0.5; vol[TN] += b * 0.5; vol[CP] -= b * 0.5; vol[TP] -= b * 0.5; }
+        else         { vol[NP] += b * 0.25; vol[TN] += b * 0.25; vol[SP] -= b * 0.25; vol[TS] -= b * 0.25; }
+        vol[CP] -= cc; vol[TP] += cc;
+    }
+    if (!kl || P.pk) {   // bottom
+        int bb = q.id(kc - 1, jc, ic);
+        double a = P.gT1[bb], b = P.gT2[bb], cc = P.gT3[bb];
+        if (ir)      { vol[CP] -= a * 0.5; vol[BP] -= a * 0.5; vol[WP] += a * 0.5; vol[BW] += a * 0.5; }
+        else if (il) { vol[EP] -= a * 0.5; vol[BE] -= a * 0.5; vol[CP] += a * 0.5; vol[BP] += a * 0.5; }
+        else         { vol[EP] -= a * 0.25; vol[BE] -= a * 0.25; vol[WP] += a * 0.25; vol[BW] += a * 0.25; }
+        if (jr)      { vol[CP] -= b * 0.5; vol[BP] -= b * 0.5; vol[SP] += b * 0.5; vol[BS] += b * 0.5; }
+        else if (jl) { vol[NP] -= b * 0.5; vol[BN] -= b * 0.5; vol[CP] += b * 0.5; vol[BP] += b * 0.5; }
+        else         { vol[NP] -= b * 0.25; vol[BN] -= b * 0.25; vol[SP] += b * 0.25; vol[BS] += b * 0.25; }
+        vol[CP] -= cc; vol[BP] += cc;
+    }
+}
+
+__constant__ int c_off[NST][3] = {   // (dk, dj, di) of each stencil point
+    {0,0,0},{0,0,1},{0,0,-1},{0,1,0},{0,-1,0},{1,0,0},{-1,0,0},
+    {0,1,1},{0,-1,1},{0,1,-1},{0,-1,-1},
+    {1,1,0},{-1,1,0},{1,-1,0},{-1,-1,0},
+    {1,0,1},{-1,0,1},{1,0,-1},{-1,0,-1}};
+
+// 19-point: y = -(A x) on non-pinned rows (entries |v| <= 1e-10 dropped as
+// at peqn.c:1410-1418), y = x on the pinned row
+__global__ void k_apply19(PoissonCtx P, const double *__restrict__ x, double *__restrict__ y)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    Cg q{P.nx, P.ny, P.nz, P.pi, P.pj, P.pk};
+    int c = (kc * P.ny + jc) * P.nx + ic;
+    if (c == P.pin) { y[c] = x[c]; return; }
+    double vol[NST];
+    row19(P, q, ic, jc, kc, vol);
+    double acc = 0.0;
+    #pragma unroll
+    for (int m = 0; m < NST; m++) {
+        int kk = kc + c_off[m][0], jj = jc + c_off[m][1], ii = ic + c_off[m][2];
+        if (m != CP && (!(fabs(vol[m]) > 1.e-10) || !q.in(kk, jj, ii))) continue;
+        acc += vol[m] * x[q.id(kk, jj, ii)];
+    }
+    y[c] = -acc;
+}
+
+// ---------------------------------------------------------------- smoothers
+// red-black point Gauss-Seidel on L x = r (7-point level operator)
+__global__ void k_smooth_rb(MGLevel L, int color)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= L.nx || jc >= L.ny || kc >= L.nz) return;
+    if (((ic + jc + kc) & 1) != color) return;
+    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
+    int c = (kc * L.ny + jc) * L.nx + ic;
+    double s = L.r[c];
+    if (ic < L.nx - 1 || L.pi) s += L.aE[c] * L.x[q.id(kc, jc, ic + 1)];
+    if (ic > 0 || L.pi)        { int w = q.id(kc, jc, ic - 1); s += L.aE[w] * L.x[w]; }
+    if (jc < L.ny - 1 || L.pj) s += L.aN[c] * L.x[q.id(kc, jc + 1, ic)];
+    if (jc > 0 || L.pj)        { int sI = q.id(kc, jc - 1, ic); s += L.aN[sI] * L.x[sI]; }
+    if (kc < L.nz - 1 || L.pk) s += L.aT[c] * L.x[q.id(kc + 1, jc, ic)];
+    if (kc > 0 || L.pk)        { int b = q.id(kc - 1, jc, ic); s += L.aT[b] * L.x[b]; }
+    L.x[c] = s / L.diag[c];
+}
+
+// zebra j-line Gauss-Seidel (j non-periodic): one thread per (i,k) line of
+// the colour, Thomas algorithm along j
+__global__ void k_smooth_line(MGLevel L, int color)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, kc = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ic >= L.nx || kc >= L.nz) return;
+    if (((ic + kc) & 1) != color) return;
+    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
+    const int sj = L.nx;
+    double cprev = 0.0, dprev = 0.0;
+    for (int jc = 0; jc < L.ny; jc++) {
+        int c = (kc * L.ny + jc) * L.nx + ic;
+        double rhs = L.r[c];
+        if (ic < L.nx - 1 || L.pi) rhs += L.aE[c] * L.x[q.id(kc, jc, ic + 1)];
+        if (ic > 0 || L.pi)        { int w = q.id(kc, jc, ic - 1); rhs += L.aE[w] * L.x[w]; }
+        if (kc < L.nz - 1 || L.pk) rhs += L.aT[c] * L.x[q.id(kc + 1, jc, ic)];
+        if (kc > 0 || L.pk)        { int b = q.id(kc - 1, jc, ic); rhs += L.aT[b] * L.x[b]; }
+        double aS = jc > 0 ? L.aN[c - sj] : 0.0;
+        double aN = jc < L.ny - 1 ? L.aN[c] : 0.0;
+        double mdiag = L.diag[c] - aS * cprev;   // sub-diagonal is -aS
+        double cp = -aN / mdiag;
+        double dp = (rhs + aS * dprev) / mdiag;
+        L.tc[c] = cp; L.td[c] = dp;
+        cprev = cp; dprev = dp;
+    }
+    double xn = 0.0;
+    for (int jc = L.ny - 1; jc >= 0; jc--) {
+        int c = (kc * L.ny + jc) * L.nx + ic;
+        double xv = L.td[c] - L.tc[c] * xn;
+        L.x[c] = xv;
+        xn = xv;
+    }
+}
+
+// coarse rhs = sum over children of the fine residual r - L x
+__global__ void k_restrict_residual(MGLevel F, MGLevel Cc)
+{
+    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
+    Cg q{F.nx, F.ny, F.nz, F.pi, F.pj, F.pk};
+    double sum = 0.0;
+    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
+        int ic = F.cx * I + di, jc = F.cy * J + dj, kc = F.cz * K + dk;
+        int c = (kc * F.ny + jc) * F.nx + ic;
+        double xc = F.x[c], res = F.r[c] - F.diag[c] * xc;
+        if (ic < F.nx - 1 || F.pi) res += F.aE[c] * F.x[q.id(kc, jc, ic + 1)];
+        if (ic > 0 || F.pi)        { int w = q.id(kc, jc, ic - 1); res += F.aE[w] * F.x[w]; }
+        if (jc < F.ny - 1 || F.pj) res += F.aN[c] * F.x[q.id(kc, jc + 1, ic)];
+        if (jc > 0 || F.pj)        { int s = q.id(kc, jc - 1, ic); res += F.aN[s] * F.x[s]; }
+        if (kc < F.nz - 1 || F.pk) res += F.aT[c] * F.x[q.id(kc + 1, jc, ic)];
+        if (kc > 0 || F.pk)        { int b = q.id(kc - 1, jc, ic); res += F.aT[b] * F.x[b]; }
+        sum += res;
+    }
+    int cI = (K * Cc.ny + J) * Cc.nx + I;
+    Cc.r[cI] = sum;
+    Cc.x[cI] = 0.0;
+}
+
+__global__ void k_prolong_add(MGLevel F, MGLevel Cc)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= F.nx || jc >= F.ny || kc >= F.nz) return;
+    int c = (kc * F.ny + jc) * F.nx + ic;
+    F.x[c] += Cc.x[((kc / F.cz) * Cc.ny + (jc / F.cy)) * Cc.nx + (ic / F.cx)];
+}
+
+// coarsest grid: x = B (r - mean r), then x -= mean x (B = (A + 11^T/n)^-1)
+__global__ void k_dense_solve(MGLevel L, const double *B)
+{
+    extern __shared__ double sh[];
+    int n = (int)L.n;
+    double *rr = sh, *red = sh + n;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) { rr[t] = L.r[t]; s += rr[t]; }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
+    double mean = red[0] / n;
+    __syncthreads();
+    double sx = 0.0;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        double acc = 0.0;   // B is symmetric: read column t for coalesced loads
+        for (int u = 0; u < n; u++) acc += B[(size_t)u * n + t] * (rr[u] - mean);
+        L.x[t] = acc;
+        sx += acc;
+    }
+    red[threadIdx.x] = sx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
+    double mx = red[0] / n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) L.x[t] -= mx;
+}
+
+// ------------------------------------------------------ vector kernels
+// partial sums: slot 0 = a.b, slot 1 = sum(a), slot 2 = max |a * w|
+__global__ void k_dot_partial(int64_t n, const double *a, const double *b, const double *w, double *part)
+{
+    __shared__ double s0[RB], s1[RB], s2[RB];
+    double d = 0.0, sa = 0.0, mx = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        double av = a[t];
+        d += av * b[t];
+        sa += av;
+        if (w) mx = fmax(mx, fabs(av * w[t]));
+    }
+    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = s0[0]; part[3 * blockIdx.x + 1] = s1[0]; part[3 * blockIdx.x + 2] = s2[0]; }
+}
+// final: out[0..2] = totals
+__global__ void k_dot_final(const double *part, int nb, double *out)
+{
+    __shared__ double s0[RB], s1[RB], s2[RB];
+    double d = 0.0, sa = 0.0, mx = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) { d += part[3 * b]; sa += part[3 * b + 1]; mx = fmax(mx, part[3 * b + 2]); }
+    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; out[2] = s2[0]; }
+}
+
+// y = b - y (residual from y = L x)
+__global__ void k_resid(int64_t n, const double *b, double *y)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) y[t] = b[t] - y[t];
+}
+__global__ void k_copy(int64_t n, const double *a, double *b)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
+}
+// grounded preconditioner input: level-0 rhs = r with r[pin] = -sum(r)
+__global__ void k_set_pin_rhs(double *r0, int pin, const double *sumr) { r0[pin] = -sumr[0]; }
+// z -= zp (zp is z[pin] captured beforehand), which makes z[pin] exactly zero
+__global__ void k_shift(int64_t n, double *z, const double *zp_ptr)
+{
+    double zp = zp_ptr[0];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) z[t] -= zp;
+}
+__global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
+
+// CG: alpha = rz / pq ; x += alpha p ; r -= alpha q
+__global__ void k_cg_update(int64_t n, const double *rz, const double *pq, double *x, const double *p, double *r, const double *q)
+{
+    double alpha = rz[0] / pq[0];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        x[t] += alpha * p[t];
+        r[t] -= alpha * q[t];
+    }
+}
+// CG: beta = rz_new / rz_old ; p = z + beta p
+__global__ void k_cg_dir(int64_t n, const double *rznew, const double *rzold, const double *z, double *p)
+{
+    double beta = rznew[0] / rzold[0];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) p[t] = z[t] + beta * p[t];
+}
+__global__ void k_scalar_copy(const double *a, double *b, int n) { for (int t = 0; t < n; t++) b[t] = a[t]; }
+
+// BiCGStab pieces (device scalars in sc: rho, alpha, omega, rho_old)
+__global__ void k_bicg_p(int64_t n, const double *sc, double *p, const double *r, const double *v)
+{
+    // beta = (rho/rho_old) * (alpha/omega)
+    double beta = (sc[0] / sc[3]) * (sc[1] / sc[2]);
+    double omega = sc[2];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        p[t] = r[t] + beta * (p[t] - omega * v[t]);
+}
+__global__ void k_bicg_s(int64_t n, const double *rho, const double *rhv, double *alpha_out, double *s, const double *r, const double *v)
+{
+    double alpha = rho[0] / rhv[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) alpha_out[0] = alpha;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) s[t] = r[t] - alpha * v[t];
+}
+__global__ void k_bicg_x(int64_t n, const double *alpha, const double *ts, const double *tt, double *omega_out,
+                         double *x, const double *phat, const double *shat, double *r, const double *s, const double *t_)
+{
+    double om = tt[0] > 0 ? ts[0] / tt[0] : 0.0;
+    double al = alpha[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) omega_out[0] = om;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        x[t] += al * phat[t] + om * shat[t];
+        r[t] = s[t] - om * t_[t];
+    }
+}
+
+inline dim3 cgrid(int nx, int ny, int nz) { return grid3(nx, ny, nz); }
+inline int vblocks(int64_t n) { int64_t b = (n + RB - 1) / RB; return (int)std::min<int64_t>(b, 148 * 8); }
+
+}  // namespace
+
+// ============================================================== host side
+static void apply_op(tg_ctx *C, const double *x, double *y)
+{
+    PoissonCtx &P = *C->pois;
+    if (P.ortho) TG_PROF(C, "pois_apply7", k_apply7<<<cgrid(P.nx, P.ny, P.nz), block3(), 0, C->stream>>>(P, x, y));
+    else TG_PROF(C, "pois_apply19", k_apply19<<<cgrid(P.nx, P.ny, P.nz), block3(), 0, C->stream>>>(P, x, y));
+}
+
+// totals of (a.b, sum a, max|a w|) into out[0..2] (device)
+static void dot3v(tg_ctx *C, const double *a, const double *b, const double *w, double *out)
+{
+    PoissonCtx &P = *C->pois;
+    TG_PROF(C, "pois_dot", k_dot_partial<<<P.nblocks, RB, 0, C->stream>>>(P.n, a, b, w, P.part));
+    k_dot_final<<<1, RB, 0, C->stream>>>(P.part, P.nblocks, out);
+}
+
+static void vcycle(tg_ctx *C, int l)
+{
+    PoissonCtx &P = *C->pois;
+    MGLevel &L = P.L[l];
+    cudaStream_t st = C->stream;
+    if (l == P.nlev - 1) {
+        int nt = 256;
+        size_t shm = sizeof(double) * (L.n + nt);
+        TG_PROF(C, "mg_coarsest", k_dense_solve<<<1, nt, shm, st>>>(L, P.Binv));
+        return;
+    }
+    const bool fine = l == 0;
+    auto smooth = [&](int color) {
+        if (P.line) TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
+                            k_smooth_line<<<dim3((L.nx + 31) / 32, (L.nz + 7) / 8), dim3(32, 8), 0, st>>>(L, color));
+        else TG_PROF(C, fine ? "mg_smooth_rb_L0" : "mg_smooth_rb_coarse",
+                     k_smooth_rb<<<cgrid(L.nx, L.ny, L.nz), block3(), 0, st>>>(L, color));
+    };
+    for (int s = 0; s < P.nu1; s++) { smooth(0); smooth(1); }
+    MGLevel &Cc = P.L[l + 1];
+    TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict_residual<<<cgrid(Cc.nx, Cc.ny, Cc.nz), block3(), 0, st>>>(L, Cc));
+    vcycle(C, l + 1);
+    TG_PROF(C, fine ? "mg_prolong_L0" : "mg_prolong_coarse", k_prolong_add<<<cgrid(L.nx, L.ny, L.nz), block3(), 0, st>>>(L, Cc));
+    for (int s = 0; s < P.nu2; s++) { smooth(1); smooth(0); }
+}
+
+// z = P M P^T r (grounded multigrid); needs sum(r) at d_sum
+static void precondition(tg_ctx *C, const double *r, double *z, const double *d_sum)
+{
+    PoissonCtx &P = *C->pois;
+    MGLevel &L0 = P.L[0];
+    TG_PROF(C, "pois_copy", k_copy<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, r, L0.r));
+    k_set_pin_rhs<<<1, 1, 0, C->stream>>>(L0.r, P.pin, d_sum);
+    TG_CUDA(cudaMemsetAsync(L0.x, 0, sizeof(double) * P.n, C->stream));
+    vcycle(C, 0);
+    TG_PROF(C, "pois_copy", k_copy<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, L0.x, z));
+    k_scalar_copy<<<1, 1, 0, C->stream>>>(z + P.pin, C->d_scal + 60, 1);
+    TG_PROF(C, "pois_shift", k_shift<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, z, C->d_scal + 60));
+}
+
+// SetRHS (peqn.c:1942-2063) into the compact vector, negated (L = -A)
+__global__ void k_set_rhs(Grid g, State s, PoissonCtx P, double dt)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    int c = (kc * P.ny + jc) * P.nx + ic;
+    if (c == P.pin) { P.b[c] = 0.0; return; }
+    int d = g.lin(kc + 1, jc + 1, ic + 1);
+    double val = 0;
+    val += s.ucont.x[d];
+    val -= s.ucont.x[d - 1];
+    val += s.ucont.y[d];
+    val -= s.ucont.y[d - g.mx];
+    val += s.ucont.z[d];
+    val -= s.ucont.z[d - g.mx * g.my];
+    val *= 1.0 / dt;
+    P.b[c] = -val;
+}
+
+// phiToPhi (peqn.c:1579-1636): compact solution into the DMDA interior
+__global__ void k_phi_to_dmda(Grid g, State s, PoissonCtx P)
+{
+    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
+    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
+    s.phi[g.lin(kc + 1, jc + 1, ic + 1)] = P.x[(kc * P.ny + jc) * P.nx + ic];
+}
+
+// dense inverse of (A + 11^T/n) on the host, Gauss-Jordan with partial pivoting
+static bool dense_inverse(std::vector<double> &A, int n, std::vector<double> &inv)
+{
+    inv.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        for (int r = col + 1; r < n; r++) if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col])) piv = r;
+        if (std::fabs(A[(size_t)piv * n + col]) < 1e-300) return false;
+        if (piv != col) for (int k = 0; k < n; k++) { std::swap(A[(size_t)piv * n + k], A[(size_t)col * n + k]); std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]); }
+        double d = 1.0 / A[(size_t)col * n + col];
+        for (int k = 0; k < n; k++) { A[(size_t)col * n + k] *= d; inv[(size_t)col * n + k] *= d; }
+        for (int r = 0; r < n; r++) {
+            if (r == col) continue;
+            double f = A[(size_t)r * n + col];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; k++) { A[(size_t)r * n + k] -= f * A[(size_t)col * n + k]; inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k]; }
+        }
+    }
+    return true;
+}
+
+void poisson_setup(tg_ctx *C)
+{
+    if (C->pois) poisson_destroy(C);
+    PoissonCtx *P = new PoissonCtx();
+    C->pois = P;
+    const Grid g = C->g;
+    P->nx = g.mx - 2; P->ny = g.my - 2; P->nz = g.mz - 2;
+    P->pi = g.pi; P->pj = g.pj; P->pk = g.pk;
+    P->n = (int64_t)P->nx * P->ny * P->nz;
+    P->pin = 0;
+    P->ortho = C->orthogonal;
+    P->line = !g.pj && P->ny >= 2;
+    const int64_t n = P->n;
+    double **fine[] = {&P->gE1, &P->gE2, &P->gE3, &P->gN1, &P->gN2, &P->gN3, &P->gT1, &P->gT2, &P->gT3,
+                       &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj};
+    for (double **f : fine) *f = dallocd(C, n);
+    P->nblocks = vblocks(n);
+    P->part = dallocd(C, 3 * (size_t)P->nblocks);
+    k_gather_g<<<cgrid(P->nx, P->ny, P->nz), block3(), 0, C->stream>>>(g, C->m, *P);
+
+    // multigrid hierarchy: halve every even direction with >= 4 cells until <= 512 cells remain
+    P->nu1 = 2; P->nu2 = 2;
+    P->nlev = 1;
+    MGLevel &L0i = P->L[0];
+    L0i = MGLevel{};
+    L0i.nx = P->nx; L0i.ny = P->ny; L0i.nz = P->nz; L0i.pi = P->pi; L0i.pj = P->pj; L0i.pk = P->pk;
+    for (;;) {
+        MGLevel &F = P->L[P->nlev - 1];
+        F.n = (int64_t)F.nx * F.ny * F.nz;
+        auto can = [](int m) { return m >= 4 && (m % 2) == 0; };
+        F.cx = can(F.nx) ? 2 : 1; F.cy = can(F.ny) ? 2 : 1; F.cz = can(F.nz) ? 2 : 1;
+        bool coarsen = F.n > 512 && (F.cx * F.cy * F.cz) > 1 && P->nlev < 16;
+        if (!coarsen) { F.cx = F.cy = F.cz = 1; break; }
+        MGLevel &Cn = P->L[P->nlev++];
+        Cn = MGLevel{};
+        Cn.nx = F.nx / F.cx; Cn.ny = F.ny / F.cy; Cn.nz = F.nz / F.cz;
+        Cn.pi = F.pi; Cn.pj = F.pj; Cn.pk = F.pk;
+    }
+    for (int l = 0; l < P->nlev; l++) {
+        MGLevel &L = P->L[l];
+        L.n = (int64_t)L.nx * L.ny * L.nz;
+        L.aE = dallocd(C, L.n); L.aN = dallocd(C, L.n); L.aT = dallocd(C, L.n); L.diag = dallocd(C, L.n);
+        L.x = dallocd(C, L.n); L.r = dallocd(C, L.n);
+        if (P->line) { L.tc = dallocd(C, L.n); L.td = dallocd(C, L.n); }
+    }
+    k_level0_coeffs<<<cgrid(P->nx, P->ny, P->nz), block3(), 0, C->stream>>>(*P, P->L[0]);
+    for (int l = 0; l + 1 < P->nlev; l++)
+        k_coarsen_coeffs<<<cgrid(P->L[l + 1].nx, P->L[l + 1].ny, P->L[l + 1].nz), block3(), 0, C->stream>>>(P->L[l], P->L[l + 1]);
+    for (int l = 0; l < P->nlev; l++) k_diag<<<cgrid(P->L[l].nx, P->L[l].ny, P->L[l].nz), block3(), 0, C->stream>>>(P->L[l]);
+
+    // dense coarsest inverse
+    MGLevel &Lc = P->L[P->nlev - 1];
+    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells (use even interior sizes)"};
+    const int nc = (int)Lc.n;
+    std::vector<double> aE(nc), aN(nc), aT(nc);
+    TG_CUDA(cudaMemcpyAsync(aE.data(), Lc.aE, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaMemcpyAsync(aN.data(), Lc.aN, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaMemcpyAsync(aT.data(), Lc.aT, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+    std::vector<double> A((size_t)nc * nc, 1.0 / nc);
+    auto cid = [&](int k, int j, int i) {
+        i = (i + Lc.nx) % Lc.nx; j = (j + Lc.ny) % Lc.ny; k = (k + Lc.nz) % Lc.nz;
+        return (k * Lc.ny + j) * Lc.nx + i;
+    };
+    for (int k = 0; k < Lc.nz; k++) for (int j = 0; j < Lc.ny; j++) for (int i = 0; i < Lc.nx; i++) {
+        int c = cid(k, j, i);
+        auto add = [&](int nb, double a) { A[(size_t)c * nc + c] += a; A[(size_t)c * nc + nb] -= a; };
+        if (i < Lc.nx - 1 || Lc.pi) add(cid(k, j, i + 1), aE[c]);
+        if (i > 0 || Lc.pi)         { int w = cid(k, j, i - 1); add(w, aE[w]); }
+        if (j < Lc.ny - 1 || Lc.pj) add(cid(k, j + 1, i), aN[c]);
+        if (j > 0 || Lc.pj)         { int s = cid(k, j - 1, i); add(s, aN[s]); }
+        if (k < Lc.nz - 1 || Lc.pk) add(cid(k + 1, j, i), aT[c]);
+        if (k > 0 || Lc.pk)         { int b = cid(k - 1, j, i); add(b, aT[b]); }
+    }
+    std::vector<double> inv;
+    if (!dense_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
+    P->Binv = dallocd(C, (size_t)nc * nc);
+    P->ncoarse = nc;
+    TG_CUDA(cudaMemcpyAsync(P->Binv, inv.data(), sizeof(double) * nc * nc, cudaMemcpyHostToDevice, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+    TG_CUDA(cudaGetLastError());
+}
+
+void poisson_destroy(tg_ctx *C)
+{
+    delete C->pois;   // device buffers are owned by the context allocation list
+    C->pois = nullptr;
+}
+
+// host read of device scalars [off, off+cnt)
+static void read_scal(tg_ctx *C, int off, int cnt)
+{
+    TG_CUDA(cudaMemcpyAsync(C->h_scal + off, C->d_scal + off, sizeof(double) * cnt, cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+}
+
+int poisson_solve(tg_ctx *C, tg_stats *st)
+{
+    PoissonCtx &P = *C->pois;
+    const Grid g = C->g;
+    const int64_t n = P.n;
+    cudaStream_t s = C->stream;
+    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
+    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
+    const double divtol = C->cfg.poisson_div_tol;
+    const double dt = C->prm.dt;
+    double *sc = C->d_scal;          // device scalar slots 0..7 used below
+    double *hs = C->h_scal;
+    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
+
+    TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, dt));
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solution
+    dot3v(C, P.b, P.b, nullptr, sc + 0);
+    apply_op(C, P.x, P.r);
+    k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r);   // r = b - L x
+    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+    read_scal(C, 0, 6);
+    const double bn = std::sqrt(hs[0]);
+    double rn = std::sqrt(hs[3]);
+    double rmax = hs[5] * dt;
+    if (st) st->poisson_initial_residual = bn > 0 ? rn / bn : rn;
+    int it = 0;
+    auto converged = [&]() {
+        if (bn == 0.0) return true;
+        if (rn / bn <= rtol) return true;
+        if (divtol > 0 && rmax <= divtol) return true;
+        return false;
+    };
+    if (P.ortho) {
+        // preconditioned CG on the reduced SPD system (r[pin] = 0, x[pin] = 0)
+        precondition(C, P.r, P.z, sc + 4);
+        dot3v(C, P.r, P.z, nullptr, sc + 6);                 // rz at sc[6]
+        TG_PROF(C, "pois_copy", k_copy<<<vblocks(n), RB, 0, s>>>(n, P.z, P.p));
+        while (!converged() && it < maxit) {
+            apply_op(C, P.p, P.q);
+            k_zero_at<<<1, 1, 0, s>>>(P.q, P.pin);
+            dot3v(C, P.p, P.q, nullptr, sc + 9);             // pq at sc[9]
+            TG_PROF(C, "pois_cg_update", k_cg_update<<<vblocks(n), RB, 0, s>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q));
+            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);   // rr, sum r, max|r aj|
+            read_scal(C, 3, 3);
+            rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
+            it++;
+            if (converged()) break;
+            precondition(C, P.r, P.z, sc + 4);
+            k_scalar_copy<<<1, 1, 0, s>>>(sc + 6, sc + 14, 1);   // rz_old
+            dot3v(C, P.r, P.z, nullptr, sc + 6);                 // rz_new
+            TG_PROF(C, "pois_cg_dir", k_cg_dir<<<vblocks(n), RB, 0, s>>>(n, sc + 6, sc + 14, P.z, P.p));
+        }
+    } else {
+        // right-preconditioned BiCGStab on the full pinned system
+        // scalars: sc[20]=rho sc[21]=alpha sc[22]=omega sc[23]=rho_old
+        TG_PROF(C, "pois_copy", k_copy<<<vblocks(n), RB, 0, s>>>(n, P.r, P.rhat));
+        double one[4] = {1.0, 1.0, 1.0, 1.0};
+        TG_CUDA(cudaMemcpyAsync(sc + 20, one, sizeof(one), cudaMemcpyHostToDevice, s));
+        TG_CUDA(cudaMemsetAsync(P.p, 0, sizeof(double) * n, s));
+        TG_CUDA(cudaMemsetAsync(P.v, 0, sizeof(double) * n, s));
+        double *phat = P.z, *shat = P.q;
+        while (!converged() && it < maxit) {
+            dot3v(C, P.rhat, P.r, nullptr, sc + 24);            // rho_new at sc[24]
+            k_scalar_copy<<<1, 1, 0, s>>>(sc + 20, sc + 23, 1); // rho_old
+            k_scalar_copy<<<1, 1, 0, s>>>(sc + 24, sc + 20, 1); // rho
+            TG_PROF(C, "pois_bicg_p", k_bicg_p<<<vblocks(n), RB, 0, s>>>(n, sc + 20, P.p, P.r, P.v));
+            dot3v(C, P.p, P.p, nullptr, sc + 27);               // sum(p) at sc[28]
+            precondition(C, P.p, phat, sc + 28);
+            apply_op(C, phat, P.v);
+            dot3v(C, P.rhat, P.v, nullptr, sc + 30);            // rhat.v at sc[30]
+            TG_PROF(C, "pois_bicg_s", k_bicg_s<<<vblocks(n), RB, 0, s>>>(n, sc + 20, sc + 30, sc + 21, P.s, P.r, P.v));
+            dot3v(C, P.s, P.s, nullptr, sc + 33);               // sum(s) at sc[34]
+            precondition(C, P.s, shat, sc + 34);
+            apply_op(C, shat, P.t);
+            dot3v(C, P.t, P.s, nullptr, sc + 36);               // t.s
+            dot3v(C, P.t, P.t, nullptr, sc + 39);               // t.t
+            TG_PROF(C, "pois_bicg_x", k_bicg_x<<<vblocks(n), RB, 0, s>>>(n, sc + 21, sc + 36, sc + 39, sc + 22, P.x, phat, shat, P.r, P.s, P.t));
+            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+            read_scal(C, 3, 3);
+            rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
+            it++;
+            if (!std::isfinite(rn)) break;
+        }
+        // true residual
+        apply_op(C, P.x, P.r);
+        TG_PROF(C, "pois_resid", k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r));
+        dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+        read_scal(C, 3, 3);
+        rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
+    }
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
+    TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
+    TG_CUDA(cudaGetLastError());
+    if (st) {
+        st->poisson_iterations = it;
+        st->poisson_total_iterations += it;
+        st->poisson_final_residual = bn > 0 ? rn / bn : rn;
+    }
+    if (!std::isfinite(rn)) return 2;
+    return converged() ? 0 : 1;
+}
+
+}  // namespace tg

@@ -1,0 +1,1064 @@
+// Stage kernels of the fractional time step: momentum right-hand side
+// (FormU and its sources), explicit integrators, boundary/ghost updates,
+// projection and divergence. Each kernel restates one loop of the reference
+// (file:line at the kernel). All fields are SoA FP64 on the global DMDA extent.
+#include <cmath>
+
+#include "tg_internal.cuh"
+
+namespace tg {
+namespace {
+
+__device__ __forceinline__ bool is_wall(int t) { return t == TG_BC_NOSLIP || t == TG_BC_SLIP || t == TG_BC_WALL_SHUMANN; }
+
+// 2-D plane launch helper
+inline dim3 g2(int na, int nb) { return dim3((na + 31) / 32, (nb + 7) / 8); }
+const dim3 b2(32, 8);
+
+// ------------------------------------------------------------------------
+// contravariantToCartesian (ueqn.c:528-635): average face fluxes to the
+// centre and solve [csi;eta;zet] u = q by Cramer's rule. Interior cells.
+// ------------------------------------------------------------------------
+__global__ void k_contra_to_cart(Grid g, Metrics m, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    R3<double> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
+    double m00 = sc.x, m01 = sc.y, m02 = sc.z, m10 = e.x, m11 = e.y, m12 = e.z, m20 = z.x, m21 = z.y, m22 = z.z;
+    double q0 = 0.5 * (s.ucont.x[c - 1] + s.ucont.x[c]);
+    double q1 = 0.5 * (s.ucont.y[c - g.mx] + s.ucont.y[c]);
+    double q2 = 0.5 * (s.ucont.z[c - g.mx * g.my] + s.ucont.z[c]);
+    double det  =  m00 * (m11 * m22 - m12 * m21) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+    double det0 =  q0 * (m11 * m22 - m12 * m21) - q1 * (m01 * m22 - m02 * m21) + q2 * (m01 * m12 - m02 * m11);
+    double det1 = -q0 * (m10 * m22 - m12 * m20) + q1 * (m00 * m22 - m02 * m20) - q2 * (m00 * m12 - m02 * m10);
+    double det2 =  q0 * (m10 * m21 - m11 * m20) - q1 * (m00 * m21 - m01 * m20) + q2 * (m00 * m11 - m01 * m10);
+    s.ucat.x[c] = det0 / det; s.ucat.y[c] = det1 / det; s.ucat.z[c] = det2 / det;
+}
+
+// ------------------------------------------------------------------------
+// resetCellPeriodicFluxes (inline.h:5453-5606): periodic ghost cells take the
+// first interior cell of the opposite side. One direction per launch; applied
+// i, then j, then k, which composes to the reference's simultaneous remap.
+// left_only: resetFacePeriodicFluxesVector (inline.h:5357-5451), face 0 <- m-2.
+// ------------------------------------------------------------------------
+template <int NC>
+__global__ void k_periodic_copy(Grid g, double *a0, double *a1, double *a2, int dir, int left_only)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
+    if (a >= na || b >= nb) return;
+    for (int side = 0; side < (left_only ? 1 : 2); side++) {
+        int d, s;
+        if (dir == 0) { d = g.lin(b, a, side ? g.mx - 1 : 0); s = g.lin(b, a, side ? 1 : g.mx - 2); }
+        else if (dir == 1) { d = g.lin(b, side ? g.my - 1 : 0, a); s = g.lin(b, side ? 1 : g.my - 2, a); }
+        else { d = g.lin(side ? g.mz - 1 : 0, b, a); s = g.lin(side ? 1 : g.mz - 2, b, a); }
+        a0[d] = a0[s];
+        if (NC == 3) { a1[d] = a1[s]; a2[d] = a2[s]; }
+    }
+}
+
+template <int NC>
+void periodic_copy(tg_ctx *C, double *a0, double *a1, double *a2, int left_only)
+{
+    const Grid g = C->g;
+    if (g.pi) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 0, left_only));
+    if (g.pj) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 1, left_only));
+    if (g.pk) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, a0, a1, a2, 2, left_only));
+}
+
+// ------------------------------------------------------------------------
+// resetNoPenetrationFluxes (inline.h:5262-5355): zero wall-normal fluxes on
+// wall patches. Plane launch per direction; range [0, m-2] in the others.
+// ------------------------------------------------------------------------
+__global__ void k_no_penetration(Grid g, State s, int dir, int left, int right)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = (dir == 0 ? g.my : g.mx) - 1, nb = (dir == 2 ? g.my : g.mz) - 1;
+    if (a >= na || b >= nb) return;
+    if (dir == 0) {
+        if (left) s.ucont.x[g.lin(b, a, 0)] = 0.0;
+        if (right) s.ucont.x[g.lin(b, a, g.mx - 2)] = 0.0;
+    } else if (dir == 1) {
+        if (left) s.ucont.y[g.lin(b, 0, a)] = 0.0;
+        if (right) s.ucont.y[g.lin(b, g.my - 2, a)] = 0.0;
+    } else {
+        if (left) s.ucont.z[g.lin(0, b, a)] = 0.0;
+        if (right) s.ucont.z[g.lin(g.mz - 2, b, a)] = 0.0;
+    }
+}
+
+// ------------------------------------------------------------------------
+// calculateNormal (inline.h:1210-1268): unit covariant direction of a cell
+// ------------------------------------------------------------------------
+__device__ void calc_normal(R3<double> csi, R3<double> eta, R3<double> zet, int dir, R3<double> &n)
+{
+    const double a11 = csi.x, a12 = csi.y, a13 = csi.z;
+    const double a21 = eta.x, a22 = eta.y, a23 = eta.z;
+    const double a31 = zet.x, a32 = zet.y, a33 = zet.z;
+    double det = a11 * (a33 * a22 - a32 * a23) - a21 * (a33 * a12 - a32 * a13) + a31 * (a23 * a12 - a22 * a13);
+    double x, y, z;
+    if (dir == 0) {        // G[:,0]
+        x = (a33 * a22 - a32 * a23) / det; y = -(a33 * a21 - a31 * a23) / det; z = (a32 * a21 - a31 * a22) / det;
+    } else if (dir == 1) { // G[:,1]
+        x = -(a33 * a12 - a32 * a13) / det; y = (a33 * a11 - a31 * a13) / det; z = -(a32 * a11 - a31 * a12) / det;
+    } else {               // G[:,2]
+        x = (a23 * a12 - a22 * a13) / det; y = -(a23 * a11 - a21 * a13) / det; z = (a22 * a11 - a21 * a12) / det;
+    }
+    double sm = sqrt(x * x + y * y + z * z);
+    n = R3<double>{x / sm, y / sm, z / sm};
+}
+
+// ------------------------------------------------------------------------
+// UpdateCartesianBCs (boundary.c:824-2050): face-adjacent ghost cells.
+// blockIdx.z selects the patch; threads cover the interior of that patch.
+// Reads interior cells only, writes ghost cells only.
+// ------------------------------------------------------------------------
+__global__ void k_cartesian_bcs(Grid g, Metrics m, State s, Params p)
+{
+    int patch = blockIdx.z;
+    int dir = patch >> 1, right = patch & 1;
+    int a = blockIdx.x * blockDim.x + threadIdx.x + 1, b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int na = (dir == 0 ? g.my : g.mx) - 2, nb = (dir == 2 ? g.my : g.mz) - 2;
+    if (a > na || b > nb) return;
+    int type = p.bc[patch];
+    int i, j, k;
+    if (dir == 0) { k = b; j = a; i = right ? g.mx - 2 : 1; }
+    else if (dir == 1) { k = b; i = a; j = right ? g.my - 2 : 1; }
+    else { j = b; i = a; k = right ? g.mz - 2 : 1; }
+    int c = g.lin(k, j, i);
+    int step = dir == 0 ? 1 : (dir == 1 ? g.mx : g.mx * g.my);
+    int ghost = right ? c + step : c - step;
+    R3<double> U = ld3(s.ucat, c);
+    if (type == TG_BC_WALL_SHUMANN) {
+        // slip preserving the wall-normal gradient, boundary.c:1155-1226 (jLeft)
+        R3<double> Uc = ld3(s.ucat, right ? c - step : c + step);
+        R3<double> n; calc_normal(ld3(m.csi, c), ld3(m.eta, c), ld3(m.zet, c), 1, n);
+        R3<double> UbN = dot3(U, n) * n, UcN = dot3(Uc, n) * n;
+        R3<double> UbP = U - UbN, UcP = Uc - UcN;
+        R3<double> Ug{2. * UbP.x - UcP.x, 2. * UbP.y - UcP.y, 2. * UbP.z - UcP.z};
+        st3(s.ucat, ghost, Ug - UbN);
+    } else if (type == TG_BC_SLIP) {
+        // boundary.c:1677-1853
+        R3<double> n; calc_normal(ld3(m.csi, c), ld3(m.eta, c), ld3(m.zet, c), dir, n);
+        R3<double> Un2 = (2.0 * dot3(U, n)) * n;
+        st3(s.ucat, ghost, U - Un2);
+    } else if (type == TG_BC_NOSLIP) {
+        // boundary.c:1855-1895
+        st3(s.ucat, ghost, -1.0 * U);
+    } else {
+        // periodic, boundary.c:1990-2018: ghost <- first interior cell of the opposite side
+        int src;
+        if (dir == 0) src = g.lin(k, j, right ? 1 : g.mx - 2);
+        else if (dir == 1) src = g.lin(k, right ? 1 : g.my - 2, i);
+        else src = g.lin(right ? 1 : g.mz - 2, j, i);
+        st3(s.ucat, ghost, ld3(s.ucat, src));
+    }
+}
+
+// ------------------------------------------------------------------------
+// UpdateContravariantBCs (boundary.c:614-822). Two passes: periodic left
+// faces take the solved right face (from the pre-call values), then the
+// right/left faces of non-wall patches are re-interpolated from Ucat and
+// wall faces zeroed.
+// ------------------------------------------------------------------------
+__global__ void k_contra_bc_periodic(Grid g, State s, int dir)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = (dir == 0 ? g.my : g.mx) - 1, nb = (dir == 2 ? g.my : g.mz) - 1;
+    if (a >= na || b >= nb) return;
+    if (dir == 0) s.ucont.x[g.lin(b, a, 0)] = s.ucont.x[g.lin(b, a, g.mx - 2)];
+    else if (dir == 1) s.ucont.y[g.lin(b, 0, a)] = s.ucont.y[g.lin(b, g.my - 2, a)];
+    else s.ucont.z[g.lin(0, b, a)] = s.ucont.z[g.lin(g.mz - 2, b, a)];
+}
+
+__global__ void k_contra_bc_faces(Grid g, Metrics m, State s, Params p, int dir)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = (dir == 0 ? g.my : g.mx) - 1, nb = (dir == 2 ? g.my : g.mz) - 1;
+    if (a >= na || b >= nb) return;
+    for (int side = 0; side < 2; side++) {
+        int patch = 2 * dir + side;
+        int type = p.bc[patch];
+        bool periodic = type == TG_BC_PERIODIC;
+        if (periodic && side == 0) continue;   // left periodic face handled by the copy pass
+        int f, step;
+        if (dir == 0) { f = g.lin(b, a, side ? g.mx - 2 : 0); step = 1; }
+        else if (dir == 1) { f = g.lin(b, side ? g.my - 2 : 0, a); step = g.mx; }
+        else { f = g.lin(side ? g.mz - 2 : 0, b, a); step = g.mx * g.my; }
+        double *u = dir == 0 ? s.ucont.x : (dir == 1 ? s.ucont.y : s.ucont.z);
+        if (is_wall(type)) { u[f] = 0.0; continue; }
+        R3<double> un = ld3(s.ucat, f + step), uc = ld3(s.ucat, f);
+        R3<double> S = dir == 0 ? ld3(m.icsi, f) : (dir == 1 ? ld3(m.jeta, f) : ld3(m.kzet, f));
+        u[f] = 0.5 * (un.x + uc.x) * S.x + 0.5 * (un.y + uc.y) * S.y + 0.5 * (un.z + uc.z) * S.z;
+    }
+}
+
+// ------------------------------------------------------------------------
+// UpdatePhiBCs (boundary.c:3168-3255) / UpdatePressureBCs (boundary.c:3051-3166):
+// ghost cells copy the first interior cell (zero gradient) or the opposite
+// interior cell (periodic). Sequential per-direction passes compose to the
+// reference's simultaneous remap because every source is interior in the
+// remapped direction.
+// ------------------------------------------------------------------------
+__global__ void k_scalar_ghosts(Grid g, double *v, int dir)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
+    if (a >= na || b >= nb) return;
+    int per = dir == 0 ? g.pi : (dir == 1 ? g.pj : g.pk);
+    int m = dir == 0 ? g.mx : (dir == 1 ? g.my : g.mz);
+    for (int side = 0; side < 2; side++) {
+        int dd = side ? m - 1 : 0;
+        int ss = side ? (per ? 1 : m - 2) : (per ? m - 2 : 1);
+        int d, s;
+        if (dir == 0) { d = g.lin(b, a, dd); s = g.lin(b, a, ss); }
+        else if (dir == 1) { d = g.lin(b, dd, a); s = g.lin(b, ss, a); }
+        else { d = g.lin(dd, b, a); s = g.lin(ss, b, a); }
+        v[d] = v[s];
+    }
+}
+
+// ------------------------------------------------------------------------
+// Smagorinsky eddy viscosity: UpdateCs (les.c:172-178) + UpdateNut
+// (les.c:2119-2514) with Compute_du_center (inline.h:3344-3418) and
+// Compute_du_dxyz (inline.h:3635-3663). Interior cells.
+// ------------------------------------------------------------------------
+__global__ void k_smagorinsky(Grid g, Metrics m, State s, Params p)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
+    double ajc = m.aj[c];
+    R3<double> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
+    R3<double> dc, de, dz;
+    if (!g.pi && i == g.mx - 2) dc = U(k, j, i) - U(k, j, i - 1);
+    else if (!g.pi && i == 1)   dc = U(k, j, i + 1) - U(k, j, i);
+    else                        dc = 0.5 * (U(k, j, i + 1) - U(k, j, i - 1));
+    if (!g.pj && j == g.my - 2) de = U(k, j, i) - U(k, j - 1, i);
+    else if (!g.pj && j == 1)   de = U(k, j + 1, i) - U(k, j, i);
+    else                        de = 0.5 * (U(k, j + 1, i) - U(k, j - 1, i));
+    if (!g.pk && k == g.mz - 2) dz = U(k, j, i) - U(k - 1, j, i);
+    else if (!g.pk && k == 1)   dz = U(k + 1, j, i) - U(k, j, i);
+    else                        dz = 0.5 * (U(k + 1, j, i) - U(k - 1, j, i));
+    double du_dx = (dc.x * sc.x + de.x * e.x + dz.x * z.x) * ajc;
+    double du_dy = (dc.x * sc.y + de.x * e.y + dz.x * z.y) * ajc;
+    double du_dz = (dc.x * sc.z + de.x * e.z + dz.x * z.z) * ajc;
+    double dv_dx = (dc.y * sc.x + de.y * e.x + dz.y * z.x) * ajc;
+    double dv_dy = (dc.y * sc.y + de.y * e.y + dz.y * z.y) * ajc;
+    double dv_dz = (dc.y * sc.z + de.y * e.z + dz.y * z.z) * ajc;
+    double dw_dx = (dc.z * sc.x + de.z * e.x + dz.z * z.x) * ajc;
+    double dw_dy = (dc.z * sc.y + de.z * e.y + dz.z * z.y) * ajc;
+    double dw_dz = (dc.z * sc.z + de.z * e.z + dz.z * z.z) * ajc;
+    double S00 = 0.5 * (du_dx + du_dx), S01 = 0.5 * (du_dy + dv_dx), S02 = 0.5 * (du_dz + dw_dx);
+    double S10 = 0.5 * (dv_dx + du_dy), S11 = 0.5 * (dv_dy + dv_dy), S12 = 0.5 * (dv_dz + dw_dy);
+    double S20 = 0.5 * (dw_dx + du_dz), S21 = 0.5 * (dw_dy + dv_dz), S22 = 0.5 * (dw_dz + dw_dz);
+    double Sabs = sqrt(2.0 * (S00 * S00 + S01 * S01 + S02 * S02 + S10 * S10 + S11 * S11 + S12 * S12 + S20 * S20 + S21 * S21 + S22 * S22));
+    double filter = pow(1. / ajc, 1. / 3.);
+    s.nut[c] = p.cs * pow(filter, 2.0) * Sabs;
+}
+
+// UpdateNutBCs (boundary.c:2630-2930): face-adjacent ghosts of nut
+__global__ void k_nut_bcs(Grid g, State s, Params p)
+{
+    int patch = blockIdx.z;
+    int dir = patch >> 1, right = patch & 1;
+    int a = blockIdx.x * blockDim.x + threadIdx.x + 1, b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int na = (dir == 0 ? g.my : g.mx) - 2, nb = (dir == 2 ? g.my : g.mz) - 2;
+    if (a > na || b > nb) return;
+    int i, j, k;
+    if (dir == 0) { k = b; j = a; i = right ? g.mx - 2 : 1; }
+    else if (dir == 1) { k = b; i = a; j = right ? g.my - 2 : 1; }
+    else { j = b; i = a; k = right ? g.mz - 2 : 1; }
+    int c = g.lin(k, j, i);
+    int step = dir == 0 ? 1 : (dir == 1 ? g.mx : g.mx * g.my);
+    int ghost = right ? c + step : c - step;
+    int t = p.nut_bc[patch];
+    if (t == TG_NUTBC_ZEROGRADIENT) s.nut[ghost] = s.nut[c];
+    else if (t == TG_NUTBC_FIXEDVALUE) s.nut[ghost] = p.nut_bc_value[patch];
+    else {
+        int src;
+        if (dir == 0) src = g.lin(k, j, right ? 1 : g.mx - 2);
+        else if (dir == 1) src = g.lin(k, right ? 1 : g.my - 2, i);
+        else src = g.lin(right ? 1 : g.mz - 2, j, i);
+        s.nut[ghost] = s.nut[src];
+    }
+}
+
+// ------------------------------------------------------------------------
+// UpdateWallModelsU for jLeft wall function -3 (boundary.c:3257-3600):
+// plane averages, neutral friction velocity (wallfunctions.c:12-34), filtered
+// wall-parallel velocity and the contravariant wall stress.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void wall_parallel(Grid g, Metrics m, State s, int k, int i, R3<double> &Up, R3<double> &n)
+{
+    int c = g.lin(k, 1, i);
+    calc_normal(ld3(m.csi, c), ld3(m.eta, c), ld3(m.zet, c), 1, n);
+    R3<double> U = ld3(s.ucat, c);
+    Up = U - dot3(U, n) * n;
+}
+
+// per-block partial sums of |U_par| and wall distance over the j=1 plane
+__global__ void k_wall_plane_sums(Grid g, Metrics m, State s, double *part)
+{
+    __shared__ double sh[2][256];
+    int nI = g.mx - 2, nK = g.mz - 2;
+    double su = 0.0, sd = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
+        int i = t % nI + 1, k = t / nI + 1;
+        int c = g.lin(k, 1, i);
+        double area = sqrt(dot3(ld3(m.eta, c), ld3(m.eta, c)));
+        R3<double> Up, n; wall_parallel(g, m, s, k, i, Up, n);
+        su += sqrt(dot3(Up, Up));
+        sd += 0.5 / m.aj[c] / area;
+    }
+    sh[0][threadIdx.x] = su; sh[1][threadIdx.x] = sd;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) { sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = sh[0][0]; part[2 * blockIdx.x + 1] = sh[1][0]; }
+}
+
+// final sum (deterministic order) and neutral u* = kappa <|U_par|> / ln(<s>/z0)
+__global__ void k_wall_ustar(Grid g, Params p, const double *part, int nb, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double su = 0.0, sd = 0.0;
+    for (int b = 0; b < nb; b++) { su += part[2 * b]; sd += part[2 * b + 1]; }
+    double cnt = (double)(g.mx - 2) * (double)(g.mz - 2);
+    double Umean = su / cnt, dist = sd / cnt;
+    double logLaw = log(dist / p.z0);
+    double us = fmax(0.0, (p.kappa * Umean) / logLaw);
+    out[0] = Umean; out[1] = dist; out[2] = us;
+}
+
+__global__ void k_wall_init_filter(Grid g, Metrics m, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.mx - 2 || k > g.mz - 2) return;
+    R3<double> Up, n; wall_parallel(g, m, s, k, i, Up, n);
+    int w = k * g.mx + i;
+    s.ufx[w] = Up.x; s.ufy[w] = Up.y; s.ufz[w] = Up.z;
+}
+
+__global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double *wsc, double m1, double m2)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.mx - 2 || k > g.mz - 2) return;
+    const double Umean = wsc[0], uStar = wsc[2];
+    int c = g.lin(k, 1, i), w = k * g.mx + i;
+    R3<double> Up, n; wall_parallel(g, m, s, k, i, Up, n);
+    double upm = sqrt(dot3(Up, Up));
+    R3<double> e1{Up.x / (upm + 1.e-12), Up.y / (upm + 1.e-12), Up.z / (upm + 1.e-12)};   // nUnit, inline.h:870-890
+    R3<double> e3 = n;
+    double um = m1 * s.umean[w] + m2 * upm;
+    s.umean[w] = um;
+    R3<double> zz = ld3(m.zet, c), cc = ld3(m.csi, c);
+    double lx = 1.0 / m.aj[c] / sqrt(dot3(zz, zz)), ly = 1.0 / m.aj[c] / sqrt(dot3(cc, cc));
+    double T = fmax(sqrt(lx * lx + ly * ly) / um, p.dt);
+    s.ufx[w] = (1.0 - p.dt / T) * s.ufx[w] + (p.dt / T) * Up.x;
+    s.ufy[w] = (1.0 - p.dt / T) * s.ufy[w] + (p.dt / T) * Up.y;
+    R3<double> je = ld3(m.jeta, g.lin(k, 0, i));
+    if (p.curvilinear) {
+        // rotation to the local (e1, e2 = e3 x e1, e3) frame; only the e1 and e3 columns enter the stress
+        double a11 = e1.x, a13 = e3.x;
+        double a21 = e1.y, a23 = e3.y;
+        double a31 = e1.z, a33 = e3.z;
+        double u2 = uStar * uStar;
+        double t11 = -2.0 * a11 * a13 * u2, t12 = -(a13 * a21 + a11 * a23) * u2, t13 = -(a13 * a31 + a11 * a33) * u2;
+        double t21 = -(a23 * a11 + a21 * a13) * u2, t22 = -2.0 * a23 * a21 * u2, t23 = -(a23 * a31 + a21 * a33) * u2;
+        double t31 = -(a33 * a11 + a31 * a13) * u2, t32 = -(a33 * a21 + a31 * a23) * u2, t33 = -2.0 * a33 * a31 * u2;
+        s.twx[w] = t11 * je.x + t12 * je.y + t13 * je.z;
+        s.twy[w] = t21 * je.x + t22 * je.y + t23 * je.z;
+        s.twz[w] = t31 * je.x + t32 * je.y + t33 * je.z;
+    } else {
+        double TauXZ = -uStar * uStar * (s.ufx[w] / fmax(Umean, 1e-5));
+        double TauYZ = -uStar * uStar * (s.ufy[w] / fmax(Umean, 1e-5));
+        s.twx[w] = je.z * TauXZ;
+        s.twy[w] = je.z * TauYZ;
+        s.twz[w] = je.x * TauXZ + je.y * TauYZ;
+    }
+}
+
+// ------------------------------------------------------------------------
+// GradP (peqn.c:3437-3773): face pressure gradient with the metric tensor,
+// one-sided cross derivatives only at the corner faces. Interior cells.
+// ------------------------------------------------------------------------
+__global__ void k_grad_p(Grid g, Metrics m, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    auto P = [&](int kk, int jj, int ii) { return s.p[g.id(kk, jj, ii)]; };
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    R3<double> ic = ld3(m.icsi, c), ie = ld3(m.ieta, c), iz = ld3(m.izet, c);
+    R3<double> jc = ld3(m.jcsi, c), je = ld3(m.jeta, c), jz = ld3(m.jzet, c);
+    R3<double> kc = ld3(m.kcsi, c), ke = ld3(m.keta, c), kz = ld3(m.kzet, c);
+    double g11 = dot3(ic, ic), g12 = dot3(ie, ic), g13 = dot3(iz, ic);
+    double g21 = dot3(jc, je), g22 = dot3(je, je), g23 = dot3(jz, je);
+    double g31 = dot3(kc, kz), g32 = dot3(ke, kz), g33 = dot3(kz, kz);
+    double dpdc, dpde, dpdz, ox, oy, oz;
+    dpdc = (i == mx - 2 && g.pi) ? P(k, j, mx + 1) - P(k, j, i) : P(k, j, i + 1) - P(k, j, i);
+    if (j == my - 2 && i == mx - 2)  dpde = (P(k, j, i) - P(k, j - 1, i) + P(k, j, i + 1) - P(k, j - 1, i + 1)) * 0.5;
+    else if (j == 1 && i == mx - 2)  dpde = (P(k, j + 1, i) - P(k, j, i) + P(k, j + 1, i + 1) - P(k, j, i + 1)) * 0.5;
+    else                             dpde = (P(k, j + 1, i) - P(k, j - 1, i) + P(k, j + 1, i + 1) - P(k, j - 1, i + 1)) * 0.25;
+    if (k == mz - 2 && i == mx - 2)  dpdz = (P(k, j, i) - P(k - 1, j, i) + P(k, j, i + 1) - P(k - 1, j, i + 1)) * 0.5;
+    else if (k == 1 && i == mx - 2)  dpdz = (P(k + 1, j, i) - P(k, j, i) + P(k + 1, j, i + 1) - P(k, j, i + 1)) * 0.5;
+    else                             dpdz = (P(k + 1, j, i) - P(k - 1, j, i) + P(k + 1, j, i + 1) - P(k - 1, j, i + 1)) * 0.25;
+    ox = (dpdc * g11 + dpde * g12 + dpdz * g13) * m.iaj[c];
+    if (i == mx - 2 && j == my - 2)  dpdc = (P(k, j, i) - P(k, j, i - 1) + P(k, j + 1, i) - P(k, j + 1, i - 1)) * 0.5;
+    else if (i == 1 && j == my - 2)  dpdc = (P(k, j, i + 1) - P(k, j, i) + P(k, j + 1, i + 1) - P(k, j + 1, i)) * 0.5;
+    else                             dpdc = (P(k, j, i + 1) - P(k, j, i - 1) + P(k, j + 1, i + 1) - P(k, j + 1, i - 1)) * 0.25;
+    dpde = (j == my - 2 && g.pj) ? P(k, my + 1, i) - P(k, j, i) : P(k, j + 1, i) - P(k, j, i);
+    if (k == mz - 2 && j == my - 2)  dpdz = (P(k, j, i) - P(k - 1, j, i) + P(k, j + 1, i) - P(k - 1, j + 1, i)) * 0.5;
+    else if (k == 1 && j == my - 2)  dpdz = (P(k + 1, j, i) - P(k, j, i) + P(k + 1, j + 1, i) - P(k, j + 1, i)) * 0.5;
+    else                             dpdz = (P(k + 1, j, i) - P(k - 1, j, i) + P(k + 1, j + 1, i) - P(k - 1, j + 1, i)) * 0.25;
+    oy = (dpdc * g21 + dpde * g22 + dpdz * g23) * m.jaj[c];
+    if (i == mx - 2 && k == mz - 2)  dpdc = (P(k, j, i) - P(k, j, i - 1) + P(k + 1, j, i) - P(k + 1, j, i - 1)) * 0.5;
+    else if (i == 1 && k == mz - 2)  dpdc = (P(k, j, i + 1) - P(k, j, i) + P(k + 1, j, i + 1) - P(k + 1, j, i)) * 0.5;
+    else                             dpdc = (P(k, j, i + 1) - P(k, j, i - 1) + P(k + 1, j, i + 1) - P(k + 1, j, i - 1)) * 0.25;
+    if (j == my - 2 && k == mz - 2)  dpde = (P(k, j, i) - P(k, j - 1, i) + P(k + 1, j, i) - P(k + 1, j - 1, i)) * 0.5;
+    else if (j == 1 && k == mz - 2)  dpde = (P(k, j + 1, i) - P(k, j, i) + P(k + 1, j + 1, i) - P(k + 1, j, i)) * 0.5;
+    else                             dpde = (P(k, j + 1, i) - P(k, j - 1, i) + P(k + 1, j + 1, i) - P(k + 1, j - 1, i)) * 0.25;
+    dpdz = (k == mz - 2 && g.pk) ? P(mz + 1, j, i) - P(k, j, i) : P(k + 1, j, i) - P(k, j, i);
+    oz = (dpdc * g31 + dpde * g32 + dpdz * g33) * m.kaj[c];
+    if (!g.pi && i == mx - 2) ox = 0;
+    if (!g.pj && j == my - 2) oy = 0;
+    if (!g.pk && k == mz - 2) oz = 0;
+    s.dp.x[c] = ox; s.dp.y[c] = oy; s.dp.z[c] = oz;
+}
+
+// ------------------------------------------------------------------------
+// Buoyancy (ueqn_sources.c:2726-2880), frozen temperature: g_cont = g.S_face
+// and bTheta = g_cont (tRef - T_face)/tRef at faces of interior cells.
+// ------------------------------------------------------------------------
+__global__ void k_buoyancy(Grid g, Metrics m, State s, Params p)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.mx || j >= g.my || k >= g.mz) return;
+    int c = g.lin(k, j, i);
+    const double gz = -9.81, tRef = p.t_ref;
+    if (i <= g.mx - 2 && j <= g.my - 2 && k <= g.mz - 2) {
+        if (j > 0 && k > 0) { R3<double> S = ld3(m.icsi, c); s.gcont.x[c] = 0 * S.x + 0 * S.y + gz * S.z; }
+        if (i > 0 && k > 0) { R3<double> S = ld3(m.jeta, c); s.gcont.y[c] = 0 * S.x + 0 * S.y + gz * S.z; }
+        if (i > 0 && j > 0) { R3<double> S = ld3(m.kzet, c); s.gcont.z[c] = 0 * S.x + 0 * S.y + gz * S.z; }
+    }
+    double bx = 0.0, by = 0.0, bz = 0.0;
+    if (i >= 1 && i <= g.mx - 2 && j >= 1 && j <= g.my - 2 && k >= 1 && k <= g.mz - 2) {
+        double T = s.tmprt[c];
+        double tI = 0.5 * (T + s.tmprt[g.id(k, j, i + 1)]);
+        double tJ = 0.5 * (T + s.tmprt[g.id(k, j + 1, i)]);
+        double tK = 0.5 * (T + s.tmprt[g.id(k + 1, j, i)]);
+        bx += 1.0 * (s.gcont.x[c] * (tRef - tI) / tRef);
+        by += 1.0 * (s.gcont.y[c] * (tRef - tJ) / tRef);
+        bz += 1.0 * (s.gcont.z[c] * (tRef - tK) / tRef);
+    }
+    s.btheta.x[c] = bx; s.btheta.y[c] = by; s.btheta.z[c] = bz;
+}
+
+// ------------------------------------------------------------------------
+// FormU (ueqn_solvers.c:6-1083), formMode 0.
+// Pass 1: per face the convective (central or QUICK) plus viscous flux,
+// stored summed per direction in f1 (i faces), f2 (j faces), f3 (k faces).
+// ------------------------------------------------------------------------
+__device__ __forceinline__ R3<double> quick(R3<double> f0, R3<double> f1, R3<double> f2, R3<double> f3, double w)
+{
+    // quadraticUpwindVec, inline.h:5089-5109
+    R3<double> fUU, fU, fD;
+    if (w > 0) { fUU = f0; fU = f1; fD = f2; } else { fUU = f3; fU = f2; fD = f1; }
+    return 0.5 * (fU + fD) + (1. / 8.) * (2.0 * fU - (fD + fUU));
+}
+
+// viscous flux (g . grad u + R . n) * ajc * nuEff, ueqn_solvers.c:180-216, 392-394
+__device__ __forceinline__ R3<double> visc_flux(R3<double> s0, R3<double> s1, R3<double> s2, int dir,
+                                                R3<double> dc, R3<double> de, R3<double> dz, double ajc, double nuEff)
+{
+    double csi0 = s0.x, csi1 = s0.y, csi2 = s0.z, eta0 = s1.x, eta1 = s1.y, eta2 = s1.z, zet0 = s2.x, zet1 = s2.y, zet2 = s2.z;
+    double g11, g21, g31, n0, n1, n2;
+    if (dir == 0) { g11 = csi0 * csi0 + csi1 * csi1 + csi2 * csi2; g21 = eta0 * csi0 + eta1 * csi1 + eta2 * csi2; g31 = zet0 * csi0 + zet1 * csi1 + zet2 * csi2; n0 = csi0; n1 = csi1; n2 = csi2; }
+    else if (dir == 1) { g11 = csi0 * eta0 + csi1 * eta1 + csi2 * eta2; g21 = eta0 * eta0 + eta1 * eta1 + eta2 * eta2; g31 = zet0 * eta0 + zet1 * eta1 + zet2 * eta2; n0 = eta0; n1 = eta1; n2 = eta2; }
+    else { g11 = csi0 * zet0 + csi1 * zet1 + csi2 * zet2; g21 = eta0 * zet0 + eta1 * zet1 + eta2 * zet2; g31 = zet0 * zet0 + zet1 * zet1 + zet2 * zet2; n0 = zet0; n1 = zet1; n2 = zet2; }
+    double r11 = dc.x * csi0 + de.x * eta0 + dz.x * zet0, r21 = dc.y * csi0 + de.y * eta0 + dz.y * zet0, r31 = dc.z * csi0 + de.z * eta0 + dz.z * zet0;
+    double r12 = dc.x * csi1 + de.x * eta1 + dz.x * zet1, r22 = dc.y * csi1 + de.y * eta1 + dz.y * zet1, r32 = dc.z * csi1 + de.z * eta1 + dz.z * zet1;
+    double r13 = dc.x * csi2 + de.x * eta2 + dz.x * zet2, r23 = dc.y * csi2 + de.y * eta2 + dz.y * zet2, r33 = dc.z * csi2 + de.z * eta2 + dz.z * zet2;
+    R3<double> v;
+    v.x = (g11 * dc.x + g21 * de.x + g31 * dz.x + r11 * n0 + r21 * n1 + r31 * n2) * ajc * (nuEff);
+    v.y = (g11 * dc.y + g21 * de.y + g31 * dz.y + r12 * n0 + r22 * n1 + r32 * n2) * ajc * (nuEff);
+    v.z = (g11 * dc.z + g21 * de.z + g31 * dz.z + r13 * n0 + r23 * n1 + r33 * n2) * ajc * (nuEff);
+    return v;
+}
+
+__global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
+    const bool quickDiv = p.div_scheme == TG_DIV_QUICK;
+    const double nu = p.nu;
+    int f = g.lin(k, j, i);
+    auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
+    auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
+    // ---- i faces, ueqn_solvers.c:173-395 with Compute_du_i (inline.h:2748-2807)
+    if (j != 0 && k != 0) {
+        R3<double> dc = U(k, j, i + 1) - U(k, j, i), de, dz;
+        bool edge = (i == 0 || i == mx - 2);
+        if (j == my - 2 && edge && (npj || npi))      de = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
+        else if (j == 1 && edge && (npj || npi))      de = 0.5 * (U(k, j + 1, i + 1) + U(k, j + 1, i) - U(k, j, i + 1) - U(k, j, i));
+        else                                          de = 0.25 * (U(k, j + 1, i + 1) + U(k, j + 1, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
+        if (k == mz - 2 && edge && (npk || npi))      dz = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
+        else if (k == 1 && edge && (npk || npi))      dz = 0.5 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k, j, i + 1) - U(k, j, i));
+        else                                          dz = 0.25 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
+        double uc = s.ucont.x[f];
+        R3<double> dv;
+        if (quickDiv) {
+            int iL, iR;
+            if (i == 0 || i == mx - 2) {
+                if (g.pi && i == mx - 2) { iR = mx + 2; iL = i - 1; }
+                else if (g.pi && i == 0) { iL = -3; iR = i + 2; }
+                else if (i == 0) { iL = i; iR = i + 2; }
+                else { iL = i - 1; iR = i + 1; }
+            } else { iL = i - 1; iR = i + 2; }
+            dv = (-uc) * quick(U(k, j, iL), U(k, j, i), U(k, j, i + 1), U(k, j, iR), uc);
+        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j, i + 1)));
+        double nuEff;
+        if (p.les) {
+            double nt = 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1));
+            if ((p.bc[TG_ILEFT] == TG_BC_SLIP && i == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && i == mx - 2)) nuEff = 0.0;
+            else nuEff = nu + nt;
+        } else nuEff = nu;
+        R3<double> v = visc_flux(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, dc, de, dz, m.iaj[f], nuEff);
+        st3(s.f1, f, dv + v);
+    }
+    // ---- j faces, ueqn_solvers.c:397-602 with Compute_du_j (inline.h:2809-2869)
+    if (i != 0 && k != 0) {
+        R3<double> dc, de = U(k, j + 1, i) - U(k, j, i), dz;
+        bool edge = (j == 0 || j == my - 2);
+        if (i == mx - 2 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k, j + 1, i - 1) - U(k, j, i - 1));
+        else if (i == 1 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i + 1) + U(k, j, i + 1) - U(k, j + 1, i) - U(k, j, i));
+        else                                          dc = 0.25 * (U(k, j + 1, i + 1) + U(k, j, i + 1) - U(k, j + 1, i - 1) - U(k, j, i - 1));
+        if (k == mz - 2 && edge && (npk || npj))      dz = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
+        else if (k == 1 && edge && (npk || npj))      dz = 0.5 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k, j + 1, i) - U(k, j, i));
+        else                                          dz = 0.25 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
+        double uc = s.ucont.y[f];
+        R3<double> dv;
+        if (quickDiv) {
+            int jL, jR;
+            if (j == 0 || j == my - 2) {
+                if (g.pj && j == my - 2) { jR = my + 2; jL = j - 1; }
+                else if (g.pj && j == 0) { jL = -3; jR = j + 2; }
+                else if (j == 0) { jL = j; jR = j + 2; }
+                else { jL = j - 1; jR = j + 1; }
+            } else { jL = j - 1; jR = j + 2; }
+            dv = (-uc) * quick(U(k, jL, i), U(k, j, i), U(k, j + 1, i), U(k, jR, i), uc);
+        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j + 1, i)));
+        double nuEff;
+        R3<double> base{0, 0, 0};
+        if (p.les) {
+            double nt = 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i));
+            // both j patches read the jLeft wall stress, ueqn_solvers.c:548-558
+            if ((p.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN && j == my - 2)) {
+                int w = k * mx + i;
+                base = R3<double>{-s.twx[w], -s.twy[w], -s.twz[w]};
+                nuEff = nu;
+            } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = 0.0;
+            else nuEff = nu + nt;
+        } else nuEff = nu;
+        R3<double> v = visc_flux(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, dc, de, dz, m.jaj[f], nuEff);
+        st3(s.f2, f, dv + (base + v));
+    }
+    // ---- k faces, ueqn_solvers.c:604-778 with Compute_du_k (inline.h:2871-2931)
+    if (i != 0 && j != 0) {
+        R3<double> dc, de, dz = U(k + 1, j, i) - U(k, j, i);
+        bool edge = (k == 0 || k == mz - 2);
+        if (i == mx - 2 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j, i - 1) - U(k, j, i - 1));
+        else if (i == 1 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i + 1) + U(k, j, i + 1) - U(k + 1, j, i) - U(k, j, i));
+        else                                          dc = 0.25 * (U(k + 1, j, i + 1) + U(k, j, i + 1) - U(k + 1, j, i - 1) - U(k, j, i - 1));
+        if (j == my - 2 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
+        else if (j == 1 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j, i) - U(k, j, i));
+        else                                          de = 0.25 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
+        double uc = s.ucont.z[f];
+        R3<double> dv;
+        if (quickDiv) {
+            int kL, kR;
+            if (k == 0 || k == mz - 2) {
+                if (g.pk && k == mz - 2) { kR = mz + 2; kL = k - 1; }
+                else if (g.pk && k == 0) { kL = -3; kR = k + 2; }
+                else if (k == 0) { kL = k; kR = k + 2; }
+                else { kL = k - 1; kR = k + 1; }
+            } else { kL = k - 1; kR = k + 2; }
+            dv = (-uc) * quick(U(kL, j, i), U(k, j, i), U(k + 1, j, i), U(kR, j, i), uc);
+        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k + 1, j, i)));
+        double nuEff;
+        if (p.les) {
+            double nt = 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i));
+            if ((p.bc[TG_KLEFT] == TG_BC_SLIP && k == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && k == mz - 2)) nuEff = 0.0;
+            else nuEff = nu + nt;
+        } else nuEff = nu;
+        R3<double> v = visc_flux(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, dc, de, dz, m.kaj[f], nuEff);
+        st3(s.f3, f, dv + v);
+    }
+}
+
+// Pass 2 (ueqn_solvers.c:825-990): cell divergence of the face fluxes, copied
+// to the ghost cell at non-periodic boundaries.
+__global__ void k_cell_fp(Grid g, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    int iw = c - 1, js = c - g.mx, kb = c - g.mx * g.my;
+    R3<double> F;
+    F.x = s.f1.x[c] - s.f1.x[iw] + s.f2.x[c] - s.f2.x[js] + s.f3.x[c] - s.f3.x[kb];
+    F.y = s.f1.y[c] - s.f1.y[iw] + s.f2.y[c] - s.f2.y[js] + s.f3.y[c] - s.f3.y[kb];
+    F.z = s.f1.z[c] - s.f1.z[iw] + s.f2.z[c] - s.f2.z[js] + s.f3.z[c] - s.f3.z[kb];
+    st3(s.fp, c, F);
+    if (i == 1 && !g.pi)        st3(s.fp, c - 1, F);
+    if (j == 1 && !g.pj)        st3(s.fp, c - g.mx, F);
+    if (k == 1 && !g.pk)        st3(s.fp, c - g.mx * g.my, F);
+    if (i == g.mx - 2 && !g.pi) st3(s.fp, c + 1, F);
+    if (j == g.my - 2 && !g.pj) st3(s.fp, c + g.mx, F);
+    if (k == g.mz - 2 && !g.pk) st3(s.fp, c + g.mx * g.my, F);
+}
+
+// Pass 3 (ueqn_solvers.c:1008-1035): rhs_face += scale * aj_face *
+// central(S . fp) at the faces of interior cells.
+__global__ void k_rhs_faces(Grid g, Metrics m, State s, V3f<double> R, double scale)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    R3<double> fpc = ld3(s.fp, c);
+    double v1, v2;
+    { R3<double> a = ld3(m.csi, c), b = ld3(m.csi, c + 1); R3<double> fb = ld3(s.fp, c + 1);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      R.x[c] += scale * m.iaj[c] * (0.5 * (v1 + v2)); }
+    { int n = c + g.mx; R3<double> a = ld3(m.eta, c), b = ld3(m.eta, n); R3<double> fb = ld3(s.fp, n);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      R.y[c] += scale * m.jaj[c] * (0.5 * (v1 + v2)); }
+    { int n = c + g.mx * g.my; R3<double> a = ld3(m.zet, c), b = ld3(m.zet, n); R3<double> fb = ld3(s.fp, n);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      R.z[c] += scale * m.kaj[c] * (0.5 * (v1 + v2)); }
+}
+
+// meanGradPForcing (ueqn_sources.c:3735-3822)
+__global__ void k_mean_grad_p(Grid g, Metrics m, V3f<double> R, Params p)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    R3<double> a = ld3(m.icsi, c), b = ld3(m.jeta, c), d = ld3(m.kzet, c);
+    R.x[c] += 1.0 * (p.mgp[0] * a.x + p.mgp[1] * a.y + p.mgp[2] * a.z);
+    R.y[c] += 1.0 * (p.mgp[0] * b.x + p.mgp[1] * b.y + p.mgp[2] * b.z);
+    R.z[c] += 1.0 * (p.mgp[0] * d.x + p.mgp[1] * d.y + p.mgp[2] * d.z);
+}
+
+// Rhs = -dP (+ AB2 buoyancy), ueqn_solvers.c:1305-1338 (all points)
+__global__ void k_rhs_init(int64_t n, State s, int buoy, int ab2)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        double x = 0.0 - s.dp.x[q], y = 0.0 - s.dp.y[q], z = 0.0 - s.dp.z[q];
+        if (buoy) {
+            if (ab2) {
+                x = x + (3.0 / 2.0) * s.btheta.x[q]; y = y + (3.0 / 2.0) * s.btheta.y[q]; z = z + (3.0 / 2.0) * s.btheta.z[q];
+                x = x + (-1.0 / 2.0) * s.btheta_o.x[q]; y = y + (-1.0 / 2.0) * s.btheta_o.y[q]; z = z + (-1.0 / 2.0) * s.btheta_o.z[q];
+            } else {
+                x = x + 1.0 * s.btheta.x[q]; y = y + 1.0 * s.btheta.y[q]; z = z + 1.0 * s.btheta.z[q];
+            }
+        }
+        s.rhs.x[q] = x; s.rhs.y[q] = y; s.rhs.z[q] = z;
+    }
+}
+
+// resetNonResolvedCellFaces (inline.h:1674-1835) on the boundary planes of one
+// direction: face 0 kept only for outflow, face m-1 unused, face m-2 of a
+// non-periodic direction kept only for outflow.
+__global__ void k_non_resolved(Grid g, State s, int dir)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
+    if (a >= na || b >= nb) return;
+    int m = dir == 0 ? g.mx : (dir == 1 ? g.my : g.mz);
+    int per = dir == 0 ? g.pi : (dir == 1 ? g.pj : g.pk);
+    double *v = dir == 0 ? s.rhs.x : (dir == 1 ? s.rhs.y : s.rhs.z);
+    const double *uo = dir == 0 ? s.ucont_o.x : (dir == 1 ? s.ucont_o.y : s.ucont_o.z);
+    auto at = [&](int l) { return dir == 0 ? g.lin(b, a, l) : (dir == 1 ? g.lin(b, l, a) : g.lin(l, b, a)); };
+    { int q = at(0); if (!(uo[q] < 0)) v[q] = 0.0; }
+    { int q = at(m - 1); v[q] = 0.0; }
+    if (!per) { int q = at(m - 2); if (!(uo[q] > 0)) v[q] = 0.0; }
+}
+
+// elementwise: y = a*x + z (component-wise over all points)
+__global__ void k_waxpy3(int64_t n, V3f<double> y, double a, V3f<double> x, V3f<double> z)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        y.x[q] = a * x.x[q] + z.x[q]; y.y[q] = a * x.y[q] + z.y[q]; y.z[q] = a * x.z[q] + z.z[q];
+    }
+}
+// FE: y = x*dt + z (VecScale then VecAXPY)
+__global__ void k_fe_update(int64_t n, V3f<double> y, double dt, V3f<double> x, V3f<double> z)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        y.x[q] = x.x[q] * dt + z.x[q]; y.y[q] = x.y[q] * dt + z.y[q]; y.z[q] = x.z[q] * dt + z.z[q];
+    }
+}
+// y += a*x
+__global__ void k_axpy3(int64_t n, V3f<double> y, double a, V3f<double> x)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        y.x[q] = y.x[q] + a * x.x[q]; y.y[q] = y.y[q] + a * x.y[q]; y.z[q] = y.z[q] + a * x.z[q];
+    }
+}
+
+// ------------------------------------------------------------------------
+// ProjectVelocity (peqn.c:2495-2905): V = V* - dt G(phi) with the full
+// metric tensor; faces 0 and m-2 skipped unless periodic.
+// ------------------------------------------------------------------------
+__global__ void k_project(Grid g, Metrics m, State s, double dt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    int f = g.lin(k, j, i);
+    auto F = [&](int kk, int jj, int ii) { return s.phi[g.id(kk, jj, ii)]; };
+    if (j > 0 && k > 0 && ((i > 0 && i < mx - 2) || g.pi)) {
+        double dpdc = F(k, j, i + 1) - F(k, j, i), dpde, dpdz;
+        if (j == my - 2)      dpde = (F(k, j, i) + F(k, j, i + 1) - F(k, j - 1, i) - F(k, j - 1, i + 1)) * 0.5;
+        else if (j == 1)      dpde = (F(k, j + 1, i) + F(k, j + 1, i + 1) - F(k, j, i) - F(k, j, i + 1)) * 0.5;
+        else                  dpde = (F(k, j + 1, i) + F(k, j + 1, i + 1) - F(k, j - 1, i) - F(k, j - 1, i + 1)) * 0.25;
+        if (k == mz - 2)      dpdz = (F(k, j, i) + F(k, j, i + 1) - F(k - 1, j, i) - F(k - 1, j, i + 1)) * 0.5;
+        else if (k == 1)      dpdz = (F(k + 1, j, i) + F(k + 1, j, i + 1) - F(k, j, i) - F(k, j, i + 1)) * 0.5;
+        else                  dpdz = (F(k + 1, j, i) + F(k + 1, j, i + 1) - F(k - 1, j, i) - F(k - 1, j, i + 1)) * 0.25;
+        R3<double> c1 = ld3(m.icsi, f), e1 = ld3(m.ieta, f), z1 = ld3(m.izet, f);
+        double a = m.iaj[f];
+        s.ucont.x[f] -= (dpdc * (c1.x * c1.x + c1.y * c1.y + c1.z * c1.z) * a
+                       + dpde * (e1.x * c1.x + e1.y * c1.y + e1.z * c1.z) * a
+                       + dpdz * (z1.x * c1.x + z1.y * c1.y + z1.z * c1.z) * a) * dt;
+    }
+    if (i > 0 && k > 0 && ((j > 0 && j < my - 2) || g.pj)) {
+        double dpdc, dpde = F(k, j + 1, i) - F(k, j, i), dpdz;
+        if (i == mx - 2)      dpdc = (F(k, j, i) + F(k, j + 1, i) - F(k, j, i - 1) - F(k, j + 1, i - 1)) * 0.5;
+        else if (i == 1)      dpdc = (F(k, j, i + 1) + F(k, j + 1, i + 1) - F(k, j, i) - F(k, j + 1, i)) * 0.5;
+        else                  dpdc = (F(k, j, i + 1) + F(k, j + 1, i + 1) - F(k, j, i - 1) - F(k, j + 1, i - 1)) * 0.25;
+        if (k == mz - 2)      dpdz = (F(k, j, i) + F(k, j + 1, i) - F(k - 1, j, i) - F(k - 1, j + 1, i)) * 0.5;
+        else if (k == 1)      dpdz = (F(k + 1, j, i) + F(k + 1, j + 1, i) - F(k, j, i) - F(k, j + 1, i)) * 0.5;
+        else                  dpdz = (F(k + 1, j, i) + F(k + 1, j + 1, i) - F(k - 1, j, i) - F(k - 1, j + 1, i)) * 0.25;
+        R3<double> c2 = ld3(m.jcsi, f), e2 = ld3(m.jeta, f), z2 = ld3(m.jzet, f);
+        double a = m.jaj[f];
+        s.ucont.y[f] -= (dpdc * (c2.x * e2.x + c2.y * e2.y + c2.z * e2.z) * a
+                       + dpde * (e2.x * e2.x + e2.y * e2.y + e2.z * e2.z) * a
+                       + dpdz * (z2.x * e2.x + z2.y * e2.y + z2.z * e2.z) * a) * dt;
+    }
+    if (i > 0 && j > 0 && ((k > 0 && k < mz - 2) || g.pk)) {
+        double dpdc, dpde, dpdz = F(k + 1, j, i) - F(k, j, i);
+        if (i == mx - 2)      dpdc = (F(k, j, i) + F(k + 1, j, i) - F(k, j, i - 1) - F(k + 1, j, i - 1)) * 0.5;
+        else if (i == 1)      dpdc = (F(k, j, i + 1) + F(k + 1, j, i + 1) - F(k, j, i) - F(k + 1, j, i)) * 0.5;
+        else                  dpdc = (F(k, j, i + 1) + F(k + 1, j, i + 1) - F(k, j, i - 1) - F(k + 1, j, i - 1)) * 0.25;
+        if (j == my - 2)      dpde = (F(k, j, i) + F(k + 1, j, i) - F(k, j - 1, i) - F(k + 1, j - 1, i)) * 0.5;
+        else if (j == 1)      dpde = (F(k, j + 1, i) + F(k + 1, j + 1, i) - F(k, j, i) - F(k + 1, j, i)) * 0.5;
+        else                  dpde = (F(k, j + 1, i) + F(k + 1, j + 1, i) - F(k, j - 1, i) - F(k + 1, j - 1, i)) * 0.25;
+        R3<double> c3 = ld3(m.kcsi, f), e3 = ld3(m.keta, f), z3 = ld3(m.kzet, f);
+        double a = m.kaj[f];
+        s.ucont.z[f] -= (dpdc * (c3.x * z3.x + c3.y * z3.y + c3.z * z3.z) * a
+                       + dpde * (e3.x * z3.x + e3.y * z3.y + e3.z * z3.z) * a
+                       + dpdz * (z3.x * z3.x + z3.y * z3.y + z3.z * z3.z) * a) * dt;
+    }
+}
+
+// UpdatePressure (peqn.c:2909-2962): p += phi at interior cells
+__global__ void k_update_pressure(Grid g, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int c = g.lin(k, j, i);
+    s.p[c] += s.phi[c];
+}
+
+// SyncPressureAcrossDomains (overset.c:263-315): p -= p[1][1][1] everywhere
+__global__ void k_gauge(int64_t n, double *p, const double *ref_cell)
+{
+    double ref = *ref_cell;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) p[q] -= ref;
+}
+__global__ void k_copy1(const double *src, double *dst) { dst[0] = src[0]; }
+
+// ContinuityErrorsOptimized (peqn.c:4114-4181): max |div(V)| * aj, block partials
+__global__ void k_div_partial(Grid g, Metrics m, State s, double *part)
+{
+    __shared__ double sh[256];
+    int nI = g.mx - 2, nJ = g.my - 2, nK = g.mz - 2;
+    int64_t n = (int64_t)nI * nJ * nK;
+    double mm = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(t % nI) + 1; int64_t r = t / nI; int j = (int)(r % nJ) + 1; int k = (int)(r / nJ) + 1;
+        int c = g.lin(k, j, i);
+        double d = fabs((s.ucont.x[c] - s.ucont.x[c - 1] + s.ucont.y[c] - s.ucont.y[c - g.mx]
+                        + s.ucont.z[c] - s.ucont.z[c - g.mx * g.my]) * m.aj[c]);
+        mm = nanmax(mm, d);
+    }
+    sh[threadIdx.x] = mm;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = nanmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_max_final(const double *part, int nb, double *out)
+{
+    __shared__ double sh[256];
+    double mm = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) mm = nanmax(mm, part[b]);
+    sh[threadIdx.x] = mm;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = nanmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+// initial face fluxes from the cell-centre velocity (initialField.c:1140-1190)
+__global__ void k_init_faces(Grid g, Metrics m, State s)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    int f = g.lin(k, j, i);
+    R3<double> a = ld3(s.ucat, f);
+    if (j >= 1 && k >= 1) {
+        R3<double> b = ld3(s.ucat, f + 1), S = ld3(m.icsi, f);
+        R3<double> uf{0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+        s.ucont.x[f] = uf.x * S.x + uf.y * S.y + uf.z * S.z;
+    }
+    if (i >= 1 && k >= 1) {
+        R3<double> b = ld3(s.ucat, f + g.mx), S = ld3(m.jeta, f);
+        R3<double> uf{0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+        s.ucont.y[f] = uf.x * S.x + uf.y * S.y + uf.z * S.z;
+    }
+    if (i >= 1 && j >= 1) {
+        R3<double> b = ld3(s.ucat, f + g.mx * g.my), S = ld3(m.kzet, f);
+        R3<double> uf{0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+        s.ucont.z[f] = uf.x * S.x + uf.y * S.y + uf.z * S.z;
+    }
+}
+
+inline dim3 gi(const Grid &g) { return grid3(g.mx - 2, g.my - 2, g.mz - 2); }
+inline dim3 ga(const Grid &g) { return grid3(g.mx, g.my, g.mz); }
+inline dim3 gf(const Grid &g) { return grid3(g.mx - 1, g.my - 1, g.mz - 1); }
+inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 * 16 ? b : 148 * 16); }
+
+}  // namespace
+
+// ============================================================================ host wrappers
+void contra_to_cart(tg_ctx *C) { k_contra_to_cart<<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s); }
+void reset_cell_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3>(C, v.x, v.y, v.z, 0); }
+void reset_cell_periodic_s(tg_ctx *C, double *v) { periodic_copy<1>(C, v, nullptr, nullptr, 0); }
+void reset_face_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3>(C, v.x, v.y, v.z, 1); }
+
+void reset_no_penetration(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int *bc = C->prm.bc;
+    auto w = [](int t) { return t == TG_BC_NOSLIP || t == TG_BC_SLIP || t == TG_BC_WALL_SHUMANN; };
+    for (int d = 0; d < 3; d++) {
+        int l = w(bc[2 * d]), r = w(bc[2 * d + 1]);
+        if (!l && !r) continue;
+        int na = d == 0 ? g.my : g.mx, nb = d == 2 ? g.my : g.mz;
+        TG_PROF(C, "bc_no_penetration", k_no_penetration<<<g2(na, nb), b2, 0, C->stream>>>(g, C->s, d, l, r));
+    }
+}
+
+void update_cartesian_bcs(tg_ctx *C)
+{
+    const Grid g = C->g;
+    int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
+    dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
+    TG_PROF(C, "bc_cartesian", k_cartesian_bcs<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm));
+}
+
+void update_contravariant_bcs(tg_ctx *C)
+{
+    const Grid g = C->g;
+    for (int d = 0; d < 3; d++) {
+        int na = d == 0 ? g.my : g.mx, nb = d == 2 ? g.my : g.mz;
+        if (C->prm.bc[2 * d] == TG_BC_PERIODIC) k_contra_bc_periodic<<<g2(na, nb), b2, 0, C->stream>>>(g, C->s, d);
+        TG_PROF(C, "bc_contravariant", k_contra_bc_faces<<<g2(na, nb), b2, 0, C->stream>>>(g, C->m, C->s, C->prm, d));
+    }
+}
+
+void update_scalar_ghosts(tg_ctx *C, double *v)
+{
+    const Grid g = C->g;
+    TG_PROF(C, "bc_scalar_ghosts", k_scalar_ghosts<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, v, 0));
+    TG_PROF(C, "bc_scalar_ghosts", k_scalar_ghosts<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, v, 1));
+    TG_PROF(C, "bc_scalar_ghosts", k_scalar_ghosts<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, v, 2));
+}
+
+void update_nut(tg_ctx *C)
+{
+    const Grid g = C->g;
+    TG_CUDA(cudaMemsetAsync(C->s.nut, 0, sizeof(double) * g.size(), C->stream));
+    TG_PROF(C, "smagorinsky", k_smagorinsky<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm));
+    int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
+    dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
+    TG_PROF(C, "bc_nut", k_nut_bcs<<<grid, b2, 0, C->stream>>>(g, C->s, C->prm));
+}
+
+void update_wall_models(tg_ctx *C)
+{
+    if (!C->prm.les || C->prm.bc[TG_JLEFT] != TG_BC_WALL_SHUMANN) return;
+    const Grid g = C->g;
+    const int nb = 148;
+    TG_PROF(C, "wall_plane_sums", k_wall_plane_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->d_red));
+    k_wall_ustar<<<1, 32, 0, C->stream>>>(g, C->prm, C->d_red, nb, C->d_scal + 8);
+    dim3 grid((g.mx - 2 + 31) / 32, (g.mz - 2 + 7) / 8);
+    if (!C->ufilt_set) {
+        k_wall_init_filter<<<grid, b2, 0, C->stream>>>(g, C->m, C->s);
+        C->ufilt_set = true;
+    }
+    double aN = (double)C->it;
+    TG_PROF(C, "wall_stress", k_wall_stress<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_scal + 8, aN / (aN + 1.0), 1.0 / (aN + 1.0)));
+}
+
+void grad_p(tg_ctx *C)
+{
+    TG_CUDA(cudaMemsetAsync(C->s.dp.x, 0, 3 * sizeof(double) * C->g.size(), C->stream));
+    TG_PROF(C, "grad_p", k_grad_p<<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s));
+}
+
+void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
+
+void form_u(tg_ctx *C, V3f<double> rhs, double scale)
+{
+    const Grid g = C->g;
+    const size_t G = (size_t)g.size();
+    // face flux arrays: f1, f2, f3 are contiguous (9 planes); fp follows
+    TG_CUDA(cudaMemsetAsync(C->s.f1.x, 0, 12 * sizeof(double) * G, C->stream));
+    TG_PROF(C, "formu_face_fluxes", k_face_fluxes<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm));
+    reset_face_periodic(C, C->s.f1);
+    reset_face_periodic(C, C->s.f2);
+    reset_face_periodic(C, C->s.f3);
+    TG_PROF(C, "formu_cell_fp", k_cell_fp<<<gi(g), block3(), 0, C->stream>>>(g, C->s));
+    reset_cell_periodic(C, C->s.fp);
+    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, rhs, scale));
+}
+
+void explicit_rhs(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int64_t G = g.size();
+    reset_no_penetration(C);
+    reset_face_periodic(C, C->s.ucont);
+    contra_to_cart(C);
+    reset_cell_periodic(C, C->s.ucat);
+    TG_PROF(C, "rhs_init", k_rhs_init<<<nblk(G), 256, 0, C->stream>>>(G, C->s, C->prm.buoyancy, C->it > C->cfg.it_start ? 1 : 0));
+    form_u(C, C->s.rhs, 1.0);
+    if (C->prm.mean_grad_p) TG_PROF(C, "mean_grad_p", k_mean_grad_p<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s.rhs, C->prm));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, 0));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, 1));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
+}
+
+void solve_u(tg_ctx *C)
+{
+    const int64_t G = C->g.size();
+    const double dt = C->prm.dt;
+    if (C->cfg.ddt_scheme == TG_DDT_FE) {
+        // UeqnFE, ueqn_solvers.c:1411-1442
+        explicit_rhs(C);
+        TG_PROF(C, "fe_update", k_fe_update<<<nblk(G), 256, 0, C->stream>>>(G, C->s.ucont, dt, C->s.rhs, C->s.ucont_o));
+    } else {
+        // UeqnRK4, ueqn_solvers.c:1446-1504
+        const double b[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+        const double a[4] = {0.0, 0.5, 0.5, 1.0};
+        TG_CUDA(cudaMemcpyAsync(C->s.utmp.x, C->s.ucont_o.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+        for (int st = 0; st < 4; st++) {
+            if (st != 0) TG_PROF(C, "rk_stage", k_waxpy3<<<nblk(G), 256, 0, C->stream>>>(G, C->s.ucont, a[st] * dt, C->s.rhs, C->s.ucont_o));
+            explicit_rhs(C);
+            TG_PROF(C, "rk_accumulate", k_axpy3<<<nblk(G), 256, 0, C->stream>>>(G, C->s.utmp, dt * b[st], C->s.rhs));
+        }
+        TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, C->s.utmp.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    }
+    // SolveUEqn tail, ueqn.c:413-437
+    reset_no_penetration(C);
+    reset_face_periodic(C, C->s.ucont);
+    contra_to_cart(C);
+    reset_cell_periodic(C, C->s.ucat);
+}
+
+// SolvePEqn (peqn.c:3777-3971) after the Poisson solve: phi ghosts, pressure
+// update and ghosts, projection
+void pressure_update_and_project(tg_ctx *C)
+{
+    const Grid g = C->g;
+    update_scalar_ghosts(C, C->s.phi);
+    TG_PROF(C, "update_pressure", k_update_pressure<<<gi(g), block3(), 0, C->stream>>>(g, C->s));
+    update_scalar_ghosts(C, C->s.p);
+    TG_PROF(C, "project", k_project<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm.dt));
+}
+
+int solve_p(tg_ctx *C, tg_stats *st)
+{
+    int rc = poisson_solve(C, st);
+    pressure_update_and_project(C);
+    return rc;
+}
+
+void reduce_max_abs_div(tg_ctx *C, double *d_out)
+{
+    const int nb = C->red_blocks;
+    TG_PROF(C, "div_max", k_div_partial<<<nb, 256, 0, C->stream>>>(C->g, C->m, C->s, C->d_red));
+    k_max_final<<<1, 256, 0, C->stream>>>(C->d_red, nb, d_out);
+}
+
+double continuity_error(tg_ctx *C)
+{
+    reduce_max_abs_div(C, C->d_scal + 16);
+    TG_CUDA(cudaMemcpyAsync(C->h_scal + 16, C->d_scal + 16, sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+    return C->h_scal[16];
+}
+
+void sync_pressure(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int64_t G = g.size();
+    k_copy1<<<1, 1, 0, C->stream>>>(C->s.p + g.lin(1, 1, 1), C->d_scal + 17);
+    TG_PROF(C, "gauge", k_gauge<<<nblk(G), 256, 0, C->stream>>>(G, C->s.p, C->d_scal + 17));
+}
+
+void init_from_cartesian(tg_ctx *C)
+{
+    const Grid g = C->g;
+    update_cartesian_bcs(C);
+    k_init_faces<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s);
+    update_contravariant_bcs(C);
+}
+
+// one time step in the order of main.c:54-327
+int step(tg_ctx *C, tg_stats *st)
+{
+    const int64_t G = C->g.size();
+    TG_CUDA(cudaMemcpyAsync(C->s.ucont_o.x, C->s.ucont.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    if (C->prm.les) { update_nut(C); update_wall_models(C); }
+    grad_p(C);
+    if (C->prm.buoyancy) {
+        if (C->it > C->cfg.it_start)
+            TG_CUDA(cudaMemcpyAsync(C->s.btheta_o.x, C->s.btheta.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+        buoyancy(C);
+    }
+    solve_u(C);
+    int rc = solve_p(C, st);
+    contra_to_cart(C);
+    reduce_max_abs_div(C, C->d_scal + 16);
+    update_cartesian_bcs(C);
+    update_contravariant_bcs(C);
+    sync_pressure(C);
+    C->it++;
+    return rc;
+}
+
+}  // namespace tg
