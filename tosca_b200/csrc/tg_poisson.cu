@@ -289,7 +289,9 @@ __global__ void k_smooth_line(MGLevel L, int color)
         if (kc > 0 || L.pk)        { int b = q.id(kc - 1, jc, ic); rhs += L.aT[b] * L.x[b]; }
         double aS = jc > 0 ? L.aN[c - sj] : 0.0;
         double aN = jc < L.ny - 1 ? L.aN[c] : 0.0;
-        double mdiag = L.diag[c] - aS * cprev;   // sub-diagonal is -aS
+        // tridiagonal row: -aS x[j-1] + diag x[j] - aN x[j+1] = rhs; with c' = -aN/m the
+        // eliminated diagonal is m = diag - (-aS) c'[j-1] = diag + aS c'[j-1]
+        double mdiag = L.diag[c] + aS * cprev;
         double cp = -aN / mdiag;
         double dp = (rhs + aS * dprev) / mdiag;
         L.tc[c] = cp; L.td[c] = dp;
@@ -699,6 +701,7 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
         if (divtol > 0 && rmax <= divtol) return true;
         return false;
     };
+    bool ok = converged();
     if (P.ortho) {
         // preconditioned CG on the reduced SPD system (r[pin] = 0, x[pin] = 0)
         precondition(C, P.r, P.z, sc + 4);
@@ -713,7 +716,7 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
             read_scal(C, 3, 3);
             rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
             it++;
-            if (converged()) break;
+            if (converged()) { ok = true; break; }
             precondition(C, P.r, P.z, sc + 4);
             k_scalar_copy<<<1, 1, 0, s>>>(sc + 6, sc + 14, 1);   // rz_old
             dot3v(C, P.r, P.z, nullptr, sc + 6);                 // rz_new
@@ -729,6 +732,15 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
         TG_CUDA(cudaMemsetAsync(P.v, 0, sizeof(double) * n, s));
         double *phat = P.z, *shat = P.q;
         while (!converged() && it < maxit) {
+            if (it > 0 && (it % 50) == 0) {
+                // restart from the true residual (limits recursive drift)
+                apply_op(C, P.x, P.r);
+                TG_PROF(C, "pois_resid", k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r));
+                k_copy<<<vblocks(n), RB, 0, s>>>(n, P.r, P.rhat);
+                TG_CUDA(cudaMemcpyAsync(sc + 20, one, sizeof(one), cudaMemcpyHostToDevice, s));
+                TG_CUDA(cudaMemsetAsync(P.p, 0, sizeof(double) * n, s));
+                TG_CUDA(cudaMemsetAsync(P.v, 0, sizeof(double) * n, s));
+            }
             dot3v(C, P.rhat, P.r, nullptr, sc + 24);            // rho_new at sc[24]
             k_scalar_copy<<<1, 1, 0, s>>>(sc + 20, sc + 23, 1); // rho_old
             k_scalar_copy<<<1, 1, 0, s>>>(sc + 24, sc + 20, 1); // rho
@@ -750,7 +762,8 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
             it++;
             if (!std::isfinite(rn)) break;
         }
-        // true residual
+        ok = converged();
+        // true residual (reported; it may sit slightly above the recursive one at round-off level)
         apply_op(C, P.x, P.r);
         TG_PROF(C, "pois_resid", k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r));
         dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
@@ -766,7 +779,7 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
         st->poisson_final_residual = bn > 0 ? rn / bn : rn;
     }
     if (!std::isfinite(rn)) return 2;
-    return converged() ? 0 : 1;
+    return ok ? 0 : 1;
 }
 
 }  // namespace tg
