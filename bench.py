@@ -127,10 +127,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(name, precision, seed_offset=0, small=False):
+def make_workload(name, precision, seed_offset=0, small=False, cells=None):
     from tosca_b200 import api, cases
     if name == "abl":
         kw = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=250.0) if small else {}
+        if cells:
+            nx, ny, nz = cells
+            kw = dict(nx=nx, ny=ny, nz=nz, Lx=10.0 * nx, Ly=10.0 * ny, H=1000.0 * nz / 128.0)
         cfg, nodes, ucat, p = cases.abl_case(ddt=api.DDT_RK4, seed=20261203 + seed_offset, **kw)
         T = None
         desc = "ABL %dx%dx%d cells, RK4, Smagorinsky, Schumann wall, dt=0.25 s" % (
@@ -209,6 +212,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--profile-json", default=None, help="write per-kernel timings here")
+    ap.add_argument("--cells", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="override the ABL size (profiling captures of a smaller case)")
     args = ap.parse_args()
 
     rank = env_int("RANK", 0)
@@ -232,7 +237,7 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    cfg, nodes, ucat, p, T, desc = make_workload(args.workload, args.precision, seed_offset=rank)
+    cfg, nodes, ucat, p, T, desc = make_workload(args.workload, args.precision, seed_offset=rank, cells=args.cells)
     cfg.device = dev
     solver = tosca_b200.gpu_solver(cfg)
     cases.setup(solver, nodes, ucat, p, T)

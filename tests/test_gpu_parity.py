@@ -120,3 +120,26 @@ def test_tgv_64_ten_steps_fe():
     assert np.linalg.norm(interior(u_g[..., 2] - u_o[..., 2])) < 1e-10 * np.linalg.norm(interior(u_o[..., 0]))
     assert rel_l2(g.get("P"), o.get("P")) < 1e-10
     assert g.last_stats.max_divergence < 1e-10
+
+
+@pytest.mark.parametrize("name", ["tgv", "abl", "hill"])
+def test_mixed_precision_against_fp64_oracle(name):
+    """Mixed mode (FP32 multigrid and stencils inside FP64 outer loops): every
+    field within 1e-6 relative L2 of the FP64 oracle after 5 steps, and the
+    divergence bound met in FP64."""
+    import tosca_b200
+    from tosca_b200 import api
+    g, o = pair(name, dict(TIGHT, precision=api.PREC_MIXED), **SMALL[name])
+    o.close()
+    g2, o = pair(name, TIGHT, **SMALL[name])
+    g2.close()
+    sg = g.step(5)
+    o.step(5)
+    u_g, u_o = g.get("UCAT"), o.get("UCAT")
+    for c in range(3):
+        ref = np.linalg.norm(interior(u_o[..., c]))
+        if ref < 1e-12:
+            continue
+        assert rel_l2(u_g[..., c], u_o[..., c]) < 1e-6, c
+    assert rel_l2(g.get("P"), o.get("P")) < 1e-6
+    assert sg.max_divergence < 1e-8

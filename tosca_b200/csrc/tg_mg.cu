@@ -1,0 +1,596 @@
+// Geometric multigrid V-cycle for the 7-point part of TOSCA's pressure
+// operator, used as the preconditioner of the Krylov pressure solve.
+//
+//  * coarsening: every even direction with >= 4 cells is halved until a level
+//    has <= 512 cells; coarse face coefficients are face sums of the fine
+//    ones, halved when the face-normal direction is coarsened
+//  * transfers: summed residual restriction, piecewise-constant prolongation
+//  * smoothing: zebra j-line Gauss-Seidel when j (the wall-normal direction)
+//    is non-periodic, red-black point Gauss-Seidel otherwise; 2 pre + 2 post
+//    sweeps in reversed colour order, so the cycle is a symmetric operator
+//  * coarsest level: dense (A + 11^T/n)^-1, i.e. the pseudo-inverse on
+//    mean-free vectors
+//
+// Layout: on every level the cells of an (k, j) row are stored with even i
+// first and odd i second. The cells of one zebra colour in a k-row then form
+// one contiguous half-row, so a warp of same-colour lines reads 32 adjacent
+// doubles (or floats): full coalescing, no idle half-warps.
+//
+// The tridiagonal line matrices never change, so their LU factors (c' and
+// 1/m of the Thomas algorithm) are computed once at setup and a line solve is
+// a chain of FMAs. A block solves 32 same-colour lines at once: each of its
+// warps takes one chunk of j, runs the forward and backward recurrences of
+// its chunk as affine maps (coalesced loads, all warps in flight), and the
+// chunk ends are combined in shared memory. Levels with <= 4096 cells run as
+// one single-block kernel (all their sweeps, transfers and the coarsest
+// solve), which removes the launch latency of the smallest levels.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "tg_mg.cuh"
+
+namespace tg {
+
+template <class T>
+struct Lvl {
+    int nx, ny, nz, pi, pj, pk;
+    int h0;                  // number of even i in a row (first half of the row)
+    int cx, cy, cz;          // coarsening factors to the next level
+    int64_t n;
+    T *aE, *aN, *aT, *diag;  // east/north/top face coefficients, diagonal
+    T *cp, *minv;            // Thomas factors of the j-lines
+    T *x, *r, *tmp;          // unknown, right-hand side, line scratch
+};
+
+constexpr int MAXL = 16;
+constexpr int TAIL_CELLS = 4096;
+constexpr int LINE_NW = 8;          // warps per block of the chunked line solver
+
+template <class T>
+struct Tail {
+    Lvl<T> L[MAXL];
+    int nl;
+    int line;
+    int nu;
+};
+
+struct MG {
+    bool fp32;
+    int nlev, tail_start, line, nu;
+    Lvl<double> Ld[MAXL];
+    Lvl<float> Lf[MAXL];
+    double *B;               // dense coarsest inverse (double)
+    int nc;
+};
+
+int mg_levels(const MG *mg) { return mg->nlev; }
+
+namespace {
+
+__device__ __forceinline__ int spos(int i, int h0) { return (i & 1) ? (h0 + (i >> 1)) : (i >> 1); }
+template <class T>
+__device__ __forceinline__ int sidx(const Lvl<T> &L, int k, int j, int i) { return (k * L.ny + j) * L.nx + spos(i, L.h0); }
+
+// sum of a_f x_nb over the i and k neighbours (and j when with_j)
+template <class T>
+__device__ __forceinline__ T nb_sum(const Lvl<T> &L, int k, int j, int i, int c, bool with_j)
+{
+    T s = T(0);
+    if (i + 1 < L.nx)  s += L.aE[c] * L.x[sidx(L, k, j, i + 1)];
+    else if (L.pi)     s += L.aE[c] * L.x[sidx(L, k, j, 0)];
+    if (i > 0)         { int w = sidx(L, k, j, i - 1); s += L.aE[w] * L.x[w]; }
+    else if (L.pi)     { int w = sidx(L, k, j, L.nx - 1); s += L.aE[w] * L.x[w]; }
+    if (k + 1 < L.nz)  s += L.aT[c] * L.x[sidx(L, k + 1, j, i)];
+    else if (L.pk)     s += L.aT[c] * L.x[sidx(L, 0, j, i)];
+    if (k > 0)         { int b = sidx(L, k - 1, j, i); s += L.aT[b] * L.x[b]; }
+    else if (L.pk)     { int b = sidx(L, L.nz - 1, j, i); s += L.aT[b] * L.x[b]; }
+    if (with_j) {
+        if (j + 1 < L.ny)  s += L.aN[c] * L.x[c + L.nx];
+        else if (L.pj)     s += L.aN[c] * L.x[sidx(L, k, 0, i)];
+        if (j > 0)         s += L.aN[c - L.nx] * L.x[c - L.nx];
+        else if (L.pj)     { int q = sidx(L, k, L.ny - 1, i); s += L.aN[q] * L.x[q]; }
+    }
+    return s;
+}
+
+// ------------------------------------------------------------------- setup
+template <class T>
+__global__ void k_l0_coeffs(const double *aE, const double *aN, const double *aT, Lvl<T> L)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+    int q = (k * L.ny + j) * L.nx + i, c = sidx(L, k, j, i);
+    L.aE[c] = (T)((i < L.nx - 1 || L.pi) ? aE[q] : 0.0);
+    L.aN[c] = (T)((j < L.ny - 1 || L.pj) ? aN[q] : 0.0);
+    L.aT[c] = (T)((k < L.nz - 1 || L.pk) ? aT[q] : 0.0);
+}
+
+template <class T>
+__global__ void k_coarsen(Lvl<T> F, Lvl<T> Cc)
+{
+    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
+    double sE = 0.0, sN = 0.0, sT = 0.0;
+    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++)
+        sE += (double)F.aE[sidx(F, F.cz * K + dk, F.cy * J + dj, F.cx * I + F.cx - 1)];
+    for (int dk = 0; dk < F.cz; dk++) for (int di = 0; di < F.cx; di++)
+        sN += (double)F.aN[sidx(F, F.cz * K + dk, F.cy * J + F.cy - 1, F.cx * I + di)];
+    for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++)
+        sT += (double)F.aT[sidx(F, F.cz * K + F.cz - 1, F.cy * J + dj, F.cx * I + di)];
+    int c = sidx(Cc, K, J, I);
+    Cc.aE[c] = (T)(sE * (F.cx == 2 ? 0.5 : 1.0));
+    Cc.aN[c] = (T)(sN * (F.cy == 2 ? 0.5 : 1.0));
+    Cc.aT[c] = (T)(sT * (F.cz == 2 ? 0.5 : 1.0));
+}
+
+template <class T>
+__global__ void k_diag(Lvl<T> L)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+    int c = sidx(L, k, j, i);
+    double aW = i > 0 ? (double)L.aE[sidx(L, k, j, i - 1)] : (L.pi ? (double)L.aE[sidx(L, k, j, L.nx - 1)] : 0.0);
+    double aS = j > 0 ? (double)L.aN[sidx(L, k, j - 1, i)] : (L.pj ? (double)L.aN[sidx(L, k, L.ny - 1, i)] : 0.0);
+    double aB = k > 0 ? (double)L.aT[sidx(L, k - 1, j, i)] : (L.pk ? (double)L.aT[sidx(L, L.nz - 1, j, i)] : 0.0);
+    L.diag[c] = (T)((double)L.aE[c] + aW + (double)L.aN[c] + aS + (double)L.aT[c] + aB);
+}
+
+// Thomas factors of every j-line: m_j = diag_j + aS_j c'_{j-1}, c'_j = -aN_j/m_j
+template <class T>
+__global__ void k_line_factors(Lvl<T> L)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= L.nx || k >= L.nz) return;
+    double cprev = 0.0;
+    for (int j = 0; j < L.ny; j++) {
+        int c = sidx(L, k, j, i);
+        double aS = j > 0 ? (double)L.aN[c - L.nx] : 0.0;
+        double aN = j < L.ny - 1 ? (double)L.aN[c] : 0.0;
+        double m = (double)L.diag[c] + aS * cprev;
+        double cp = -aN / m;
+        L.cp[c] = (T)cp;
+        L.minv[c] = (T)(1.0 / m);
+        cprev = cp;
+    }
+}
+
+// ---------------------------------------------------------------- smoothing
+// one j-line of colour `color` (zebra Gauss-Seidel): forward substitution with
+// the stored factors, then back substitution
+template <class T>
+__device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i)
+{
+    T dprev = T(0);
+    const int nx = L.nx;
+    int c = sidx(L, k, 0, i);
+    for (int j = 0; j < L.ny; j++, c += nx) {
+        T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
+        T aS = j > 0 ? L.aN[c - nx] : T(0);
+        T dp = (rhs + aS * dprev) * L.minv[c];
+        L.tmp[c] = dp;
+        dprev = dp;
+    }
+    T xn = T(0);
+    c -= nx;
+    for (int j = L.ny - 1; j >= 0; j--, c -= nx) {
+        T xv = L.tmp[c] - L.cp[c] * xn;
+        L.x[c] = xv;
+        xn = xv;
+    }
+}
+
+// Chunked zebra line solve (nx even): lane -> one of 32 consecutive
+// same-colour lines (flattened over (k, t)), warp w -> j in [w*cj, (w+1)*cj).
+// dp_j = (rhs_j + aS_j dp_{j-1}) / m_j and x_j = dp_j - c'_j x_{j+1} are first
+// order affine recurrences: each warp composes its chunk into (offset,
+// multiplier) pairs, warp 0 chains the chunk ends, each warp finishes its chunk.
+template <class T>
+__global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int color, int cj)
+{
+    extern __shared__ unsigned char smraw[];
+    T *D = reinterpret_cast<T *>(smraw);            // [ny][32] offsets
+    T *Mu = D + L.ny * 32;                          // [ny][32] multipliers
+    T *SD = Mu + L.ny * 32;                         // [NW][32] chunk offsets
+    T *SM = SD + LINE_NW * 32;                      // [NW][32] chunk multipliers
+    T *ST = SM + LINE_NW * 32;                      // [NW][32] chunk boundary values
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int half = L.nx >> 1;
+    const int lid = blockIdx.x * 32 + lane;
+    const bool active = lid < half * L.nz;
+    const int k = active ? lid / half : 0, t = active ? lid % half : 0;
+    const int i = 2 * t + ((color ^ k) & 1);
+    const int nx = L.nx;
+    const int j0 = w * cj, j1 = min(L.ny, j0 + cj);
+    T dl = T(0), ml = T(1);
+    if (active) {
+        int c = sidx(L, k, j0, i);
+        #pragma unroll 4
+        for (int j = j0; j < j1; j++, c += nx) {
+            T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
+            T aS = j > 0 ? L.aN[c - nx] : T(0);
+            T mi = L.minv[c];
+            T f = aS * mi;
+            dl = rhs * mi + f * dl;
+            ml = f * ml;
+            D[j * 32 + lane] = dl;
+            Mu[j * 32 + lane] = ml;
+        }
+    }
+    SD[w * 32 + lane] = dl;
+    SM[w * 32 + lane] = ml;
+    __syncthreads();
+    if (w == 0) {
+        T s = T(0);
+        for (int q = 0; q < LINE_NW; q++) { ST[q * 32 + lane] = s; s = SD[q * 32 + lane] + SM[q * 32 + lane] * s; }
+    }
+    __syncthreads();
+    const T st = ST[w * 32 + lane];
+    T xl = T(0), nl = T(1);
+    if (active && j1 > j0) {
+        int c = sidx(L, k, j1 - 1, i);
+        #pragma unroll 4
+        for (int j = j1 - 1; j >= j0; j--, c -= nx) {
+            T dp = D[j * 32 + lane] + Mu[j * 32 + lane] * st;
+            T cp = L.cp[c];
+            xl = dp - cp * xl;
+            nl = -cp * nl;
+            D[j * 32 + lane] = xl;
+            Mu[j * 32 + lane] = nl;
+        }
+    }
+    __syncthreads();
+    SD[w * 32 + lane] = xl;
+    SM[w * 32 + lane] = nl;
+    __syncthreads();
+    if (w == 0) {
+        T xn = T(0);
+        for (int q = LINE_NW - 1; q >= 0; q--) { ST[q * 32 + lane] = xn; xn = SD[q * 32 + lane] + SM[q * 32 + lane] * xn; }
+    }
+    __syncthreads();
+    const T xnext = ST[w * 32 + lane];
+    if (active) {
+        int c = sidx(L, k, j0, i);
+        for (int j = j0; j < j1; j++, c += nx) L.x[c] = D[j * 32 + lane] + Mu[j * 32 + lane] * xnext;
+    }
+}
+
+template <class T>
+size_t line_chunk_smem(int ny) { return sizeof(T) * (2 * (size_t)ny * 32 + 3 * LINE_NW * 32); }
+
+// lines of one colour: (i + k) & 1 == color, i.e. i of parity (color ^ k) & 1
+template <class T>
+__global__ void k_smooth_line(Lvl<T> L, int color)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (k >= L.nz) return;
+    int q = (color ^ k) & 1;
+    int cnt = q ? (L.nx >> 1) : ((L.nx + 1) >> 1);
+    if (t >= cnt) return;
+    line_solve(L, k, 2 * t + q);
+}
+
+template <class T>
+__device__ __forceinline__ void point_update(const Lvl<T> &L, int k, int j, int i)
+{
+    int c = sidx(L, k, j, i);
+    L.x[c] = (L.r[c] + nb_sum(L, k, j, i, c, true)) / L.diag[c];
+}
+
+template <class T>
+__global__ void k_smooth_rb(Lvl<T> L, int color)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+    if (((i + j + k) & 1) != color) return;
+    point_update(L, k, j, i);
+}
+
+// ------------------------------------------------------------------ transfers
+template <class T>
+__device__ __forceinline__ void restrict_cell(const Lvl<T> &F, const Lvl<T> &Cc, int I, int J, int K)
+{
+    T sum = T(0);
+    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
+        int i = F.cx * I + di, j = F.cy * J + dj, k = F.cz * K + dk;
+        int c = sidx(F, k, j, i);
+        sum += F.r[c] - F.diag[c] * F.x[c] + nb_sum(F, k, j, i, c, true);
+    }
+    int cc = sidx(Cc, K, J, I);
+    Cc.r[cc] = sum;
+    Cc.x[cc] = T(0);
+}
+
+template <class T>
+__global__ void k_restrict(Lvl<T> F, Lvl<T> Cc)
+{
+    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
+    restrict_cell(F, Cc, I, J, K);
+}
+
+template <class T>
+__global__ void k_prolong(Lvl<T> F, Lvl<T> Cc)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= F.nx || j >= F.ny || k >= F.nz) return;
+    F.x[sidx(F, k, j, i)] += Cc.x[sidx(Cc, k / F.cz, j / F.cy, i / F.cx)];
+}
+
+// -------------------------------------------------------- single-block tail
+template <class T>
+__device__ void blk_smooth(const Lvl<T> &L, int color, bool line)
+{
+    if (line) {
+        int rowcnt = (L.nx + 1) >> 1;
+        for (int t = threadIdx.x; t < rowcnt * L.nz; t += blockDim.x) {
+            int k = t / rowcnt, tt = t % rowcnt;
+            int q = (color ^ k) & 1;
+            int cnt = q ? (L.nx >> 1) : ((L.nx + 1) >> 1);
+            if (tt < cnt) line_solve(L, k, 2 * tt + q);
+        }
+    } else {
+        for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
+            int i = t % L.nx, r2 = t / L.nx, j = r2 % L.ny, k = r2 / L.ny;
+            if (((i + j + k) & 1) == color) point_update(L, k, j, i);
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
+{
+    extern __shared__ double sh[];
+    const int nl = tl.nl;
+    // descend
+    for (int l = 0; l < nl - 1; l++) {
+        const Lvl<T> &L = tl.L[l];
+        for (int s = 0; s < tl.nu; s++) {
+            blk_smooth(L, 0, tl.line != 0); __syncthreads();
+            blk_smooth(L, 1, tl.line != 0); __syncthreads();
+        }
+        const Lvl<T> &Cc = tl.L[l + 1];
+        for (int t = threadIdx.x; t < Cc.n; t += blockDim.x) {
+            int I = t % Cc.nx, r2 = t / Cc.nx, J = r2 % Cc.ny, K = r2 / Cc.ny;
+            restrict_cell(L, Cc, I, J, K);
+        }
+        __syncthreads();
+    }
+    // coarsest: x = B (r - mean r), then remove the mean of x
+    {
+        const Lvl<T> &L = tl.L[nl - 1];
+        const int n = (int)L.n;
+        double *rr = sh, *red = sh + n;
+        double s = 0.0;
+        for (int t = threadIdx.x; t < n; t += blockDim.x) { rr[t] = (double)L.r[t]; s += rr[t]; }
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
+        double mean = red[0] / n;
+        __syncthreads();
+        double sx = 0.0;
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            double acc = 0.0;
+            for (int u = 0; u < n; u++) acc += B[(size_t)u * n + t] * (rr[u] - mean);   // B symmetric: column t
+            rr[n + blockDim.x + t] = acc;
+            sx += acc;
+        }
+        red[threadIdx.x] = sx;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
+        double mx = red[0] / n;
+        for (int t = threadIdx.x; t < n; t += blockDim.x) L.x[t] = (T)(rr[n + blockDim.x + t] - mx);
+        __syncthreads();
+    }
+    // ascend
+    for (int l = nl - 2; l >= 0; l--) {
+        const Lvl<T> &L = tl.L[l];
+        const Lvl<T> &Cc = tl.L[l + 1];
+        for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
+            int i = t % L.nx, r2 = t / L.nx, j = r2 % L.ny, k = r2 / L.ny;
+            L.x[sidx(L, k, j, i)] += Cc.x[sidx(Cc, k / L.cz, j / L.cy, i / L.cx)];
+        }
+        __syncthreads();
+        for (int s = 0; s < tl.nu; s++) {
+            blk_smooth(L, 1, tl.line != 0); __syncthreads();
+            blk_smooth(L, 0, tl.line != 0); __syncthreads();
+        }
+    }
+}
+
+// --------------------------------------------------------- level-0 in/out
+// L0.r <- r (natural order, FP64) with the pinned entry replaced by -sum(r); L0.x <- 0
+template <class T>
+__global__ void k_in(const double *r, const double *d_sum, Lvl<T> L)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+    int q = (k * L.ny + j) * L.nx + i, c = sidx(L, k, j, i);
+    double v = q == 0 ? -d_sum[0] : r[q];
+    L.r[c] = (T)v;
+    L.x[c] = T(0);
+}
+// z <- L0.x - L0.x[pinned] (natural order, FP64)
+template <class T>
+__global__ void k_out(Lvl<T> L, double *z)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= L.nx || j >= L.ny || k >= L.nz) return;
+    int q = (k * L.ny + j) * L.nx + i, c = sidx(L, k, j, i);
+    z[q] = (double)L.x[c] - (double)L.x[0];
+}
+
+inline dim3 g3(int a, int b, int c) { return grid3(a, b, c); }
+
+template <class T>
+void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
+{
+    cudaStream_t st = C->stream;
+    if (l == mg->tail_start) {
+        Tail<T> tl{};
+        tl.nl = mg->nlev - l;
+        for (int q = 0; q < tl.nl; q++) tl.L[q] = L[l + q];
+        tl.line = mg->line; tl.nu = mg->nu;
+        size_t shm = sizeof(double) * (2 * (size_t)mg->nc + 2 * 1024);
+        TG_PROF(C, "mg_tail", k_tail<T><<<1, 1024, shm, st>>>(tl, mg->B));
+        return;
+    }
+    Lvl<T> &F = L[l];
+    const bool fine = l == 0;
+    auto smooth = [&](int color) {
+        if (mg->line && (F.nx % 2) == 0) {
+            int lines = (F.nx >> 1) * F.nz;
+            int cj = (F.ny + LINE_NW - 1) / LINE_NW;
+            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
+                    k_line_chunked<T><<<(lines + 31) / 32, LINE_NW * 32, line_chunk_smem<T>(F.ny), st>>>(F, color, cj));
+        } else if (mg->line) {
+            int half = (F.nx + 1) >> 1;
+            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
+                    k_smooth_line<T><<<dim3((half + 31) / 32, (F.nz + 7) / 8), dim3(32, 8), 0, st>>>(F, color));
+        } else {
+            TG_PROF(C, fine ? "mg_smooth_rb_L0" : "mg_smooth_rb_coarse",
+                    k_smooth_rb<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, color));
+        }
+    };
+    for (int s = 0; s < mg->nu; s++) { smooth(0); smooth(1); }
+    Lvl<T> &Cc = L[l + 1];
+    TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict<T><<<g3(Cc.nx, Cc.ny, Cc.nz), block3(), 0, st>>>(F, Cc));
+    vcycle(C, mg, L, l + 1);
+    TG_PROF(C, fine ? "mg_prolong_L0" : "mg_prolong_coarse", k_prolong<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, Cc));
+    for (int s = 0; s < mg->nu; s++) { smooth(1); smooth(0); }
+}
+
+// split-layout index on the host
+inline int hsidx(int nx, int ny, int h0, int k, int j, int i) { return (k * ny + j) * nx + ((i & 1) ? (h0 + (i >> 1)) : (i >> 1)); }
+
+bool dense_inverse(std::vector<double> &A, int n, std::vector<double> &inv)
+{
+    inv.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        for (int r = col + 1; r < n; r++) if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col])) piv = r;
+        if (std::fabs(A[(size_t)piv * n + col]) < 1e-300) return false;
+        if (piv != col) for (int k = 0; k < n; k++) { std::swap(A[(size_t)piv * n + k], A[(size_t)col * n + k]); std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]); }
+        double d = 1.0 / A[(size_t)col * n + col];
+        for (int k = 0; k < n; k++) { A[(size_t)col * n + k] *= d; inv[(size_t)col * n + k] *= d; }
+        for (int r = 0; r < n; r++) {
+            if (r == col) continue;
+            double f = A[(size_t)r * n + col];
+            if (f == 0.0) continue;
+            for (int k = 0; k < n; k++) { A[(size_t)r * n + k] -= f * A[(size_t)col * n + k]; inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k]; }
+        }
+    }
+    return true;
+}
+
+template <class T>
+void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *aN, const double *aT,
+                  int nx, int ny, int nz, int pi, int pj, int pk)
+{
+    cudaStream_t st = C->stream;
+    mg->nlev = 1;
+    L[0] = Lvl<T>{};
+    L[0].nx = nx; L[0].ny = ny; L[0].nz = nz; L[0].pi = pi; L[0].pj = pj; L[0].pk = pk;
+    for (;;) {
+        Lvl<T> &F = L[mg->nlev - 1];
+        F.n = (int64_t)F.nx * F.ny * F.nz;
+        F.h0 = (F.nx + 1) >> 1;
+        auto can = [](int m) { return m >= 4 && (m % 2) == 0; };
+        F.cx = can(F.nx) ? 2 : 1; F.cy = can(F.ny) ? 2 : 1; F.cz = can(F.nz) ? 2 : 1;
+        bool coarsen = F.n > 512 && (F.cx * F.cy * F.cz) > 1 && mg->nlev < MAXL;
+        if (!coarsen) { F.cx = F.cy = F.cz = 1; break; }
+        Lvl<T> &Cn = L[mg->nlev++];
+        Cn = Lvl<T>{};
+        Cn.nx = F.nx / F.cx; Cn.ny = F.ny / F.cy; Cn.nz = F.nz / F.cz;
+        Cn.pi = F.pi; Cn.pj = F.pj; Cn.pk = F.pk;
+    }
+    for (int l = 0; l < mg->nlev; l++) {
+        Lvl<T> &V = L[l];
+        T **arrs[] = {&V.aE, &V.aN, &V.aT, &V.diag, &V.cp, &V.minv, &V.x, &V.r, &V.tmp};
+        for (T **a : arrs) *a = (T *)dalloc(C, sizeof(T) * (size_t)V.n);
+    }
+    k_l0_coeffs<T><<<g3(nx, ny, nz), block3(), 0, st>>>(aE, aN, aT, L[0]);
+    for (int l = 0; l + 1 < mg->nlev; l++)
+        k_coarsen<T><<<g3(L[l + 1].nx, L[l + 1].ny, L[l + 1].nz), block3(), 0, st>>>(L[l], L[l + 1]);
+    for (int l = 0; l < mg->nlev; l++) {
+        k_diag<T><<<g3(L[l].nx, L[l].ny, L[l].nz), block3(), 0, st>>>(L[l]);
+        if (mg->line) k_line_factors<T><<<dim3((L[l].nx + 31) / 32, (L[l].nz + 7) / 8), dim3(32, 8), 0, st>>>(L[l]);
+    }
+    if (mg->line) {
+        int maxny = 0;
+        for (int l = 0; l < mg->nlev; l++) maxny = std::max(maxny, L[l].ny);
+        size_t shm = line_chunk_smem<T>(maxny);
+        if (shm > 200 * 1024) throw CudaError{cudaErrorInvalidValue, "grid lines too long for the shared-memory line solver"};
+        TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    }
+    mg->tail_start = mg->nlev - 1;
+    while (mg->tail_start > 0 && L[mg->tail_start - 1].n <= TAIL_CELLS) mg->tail_start--;
+
+    // dense coarsest inverse of (A + 11^T/n) in the level's own (split) order
+    Lvl<T> &Lc = L[mg->nlev - 1];
+    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells (use even interior sizes)"};
+    const int nc = (int)Lc.n;
+    std::vector<T> hE(nc), hN(nc), hT(nc);
+    TG_CUDA(cudaMemcpyAsync(hE.data(), Lc.aE, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaMemcpyAsync(hN.data(), Lc.aN, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaMemcpyAsync(hT.data(), Lc.aT, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> A((size_t)nc * nc, 1.0 / nc);
+    auto id = [&](int k, int j, int i) {
+        i = (i + Lc.nx) % Lc.nx; j = (j + Lc.ny) % Lc.ny; k = (k + Lc.nz) % Lc.nz;
+        return hsidx(Lc.nx, Lc.ny, Lc.h0, k, j, i);
+    };
+    for (int k = 0; k < Lc.nz; k++) for (int j = 0; j < Lc.ny; j++) for (int i = 0; i < Lc.nx; i++) {
+        int c = id(k, j, i);
+        auto add = [&](int nb, double a) { A[(size_t)c * nc + c] += a; A[(size_t)c * nc + nb] -= a; };
+        if (i < Lc.nx - 1 || Lc.pi) add(id(k, j, i + 1), hE[c]);
+        if (i > 0 || Lc.pi)         { int w = id(k, j, i - 1); add(w, hE[w]); }
+        if (j < Lc.ny - 1 || Lc.pj) add(id(k, j + 1, i), hN[c]);
+        if (j > 0 || Lc.pj)         { int s = id(k, j - 1, i); add(s, hN[s]); }
+        if (k < Lc.nz - 1 || Lc.pk) add(id(k + 1, j, i), hT[c]);
+        if (k > 0 || Lc.pk)         { int b = id(k - 1, j, i); add(b, hT[b]); }
+    }
+    std::vector<double> inv;
+    if (!dense_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
+    mg->B = (double *)dalloc(C, sizeof(double) * (size_t)nc * nc);
+    mg->nc = nc;
+    size_t shm = sizeof(double) * (2 * (size_t)nc + 2 * 1024);
+    TG_CUDA(cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    TG_CUDA(cudaMemcpyAsync(mg->B, inv.data(), sizeof(double) * (size_t)nc * nc, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaStreamSynchronize(st));
+    TG_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+MG *mg_create(tg_ctx *C, bool fp32, const double *aE, const double *aN, const double *aT,
+              int nx, int ny, int nz, int pi, int pj, int pk)
+{
+    MG *mg = new MG();
+    mg->fp32 = fp32;
+    mg->line = !pj && ny >= 2;
+    mg->nu = 2;
+    if (fp32) setup_levels<float>(C, mg, mg->Lf, aE, aN, aT, nx, ny, nz, pi, pj, pk);
+    else setup_levels<double>(C, mg, mg->Ld, aE, aN, aT, nx, ny, nz, pi, pj, pk);
+    return mg;
+}
+
+void mg_destroy(MG *mg) { delete mg; }
+
+template <class T>
+static void apply_t(tg_ctx *C, MG *mg, Lvl<T> *L, const double *r, const double *d_sum, double *z)
+{
+    cudaStream_t st = C->stream;
+    TG_PROF(C, "mg_in", k_in<T><<<g3(L[0].nx, L[0].ny, L[0].nz), block3(), 0, st>>>(r, d_sum, L[0]));
+    vcycle<T>(C, mg, L, 0);
+    TG_PROF(C, "mg_out", k_out<T><<<g3(L[0].nx, L[0].ny, L[0].nz), block3(), 0, st>>>(L[0], z));
+}
+
+void mg_apply(tg_ctx *C, MG *mg, const double *r, const double *d_sum, double *z)
+{
+    if (mg->fp32) apply_t<float>(C, mg, mg->Lf, r, d_sum, z);
+    else apply_t<double>(C, mg, mg->Ld, r, d_sum, z);
+}
+
+}  // namespace tg

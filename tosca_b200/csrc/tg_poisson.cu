@@ -14,45 +14,31 @@
 // use preconditioned CG on the reduced system (the pinned unknown stays zero);
 // others use right-preconditioned BiCGStab.
 //
-// Preconditioner: geometric multigrid V-cycle on the 7-point part of the
-// operator with face-sum coarse coefficients, piecewise-constant transfers,
-// red-black point or j-line zebra Gauss-Seidel smoothing and a dense
-// pseudo-inverse on the coarsest grid; applied in the grounded form
-// z = P M P^T r (P shifts so that z at the pinned cell is zero), which is
-// the exact inverse structure of the pinned operator.
+// Preconditioner: the geometric multigrid V-cycle of tg_mg.cu on the 7-point
+// part of the operator, applied in the grounded form z = P M P^T r (P shifts
+// so that z at the pinned cell is zero), which is the inverse structure of the
+// pinned operator. In the mixed-precision mode the multigrid stores and
+// computes in FP32; residuals, inner products and the solution stay FP64.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "tg_internal.cuh"
+#include "tg_mg.cuh"
 
 namespace tg {
-
-struct MGLevel {
-    int nx, ny, nz, pi, pj, pk;
-    int cx, cy, cz;              // coarsening factors towards the next level
-    int64_t n;
-    double *aE, *aN, *aT, *diag; // face coefficients of the east/north/top faces; diagonal
-    double *x, *r;               // unknown and right-hand side
-    double *tc, *td;             // Thomas scratch of the line smoother
-};
 
 struct PoissonCtx {
     int nx, ny, nz, pi, pj, pk;
     int64_t n;
     int pin;                     // compact index of the pinned cell (0)
     bool ortho;
-    bool line;                   // j-line smoothing (j non-periodic)
     double *gE1, *gE2, *gE3, *gN1, *gN2, *gN3, *gT1, *gT2, *gT3;  // fine face tensors (compact)
     double *x, *b, *r, *z, *p, *q, *rhat, *v, *s, *t, *aj;
     double *part;                // reduction partials (4 per block)
     int nblocks;
-    MGLevel L[16];               // multigrid levels, finest first (plain data: passed to kernels by value)
-    int nlev;
-    double *Binv;                // dense coarsest inverse (n_c x n_c)
-    int ncoarse;
-    int nu1, nu2;
+    MG *mg;                      // multigrid preconditioner (host object)
 };
 
 namespace {
@@ -81,54 +67,6 @@ __global__ void k_gather_g(Grid g, Metrics m, PoissonCtx P)
     P.gN1[c] = m.g21[d]; P.gN2[c] = m.g22[d]; P.gN3[c] = m.g23[d];
     P.gT1[c] = m.g31[d]; P.gT2[c] = m.g32[d]; P.gT3[c] = m.g33[d];
     P.aj[c] = m.aj[d];
-}
-
-// 7-point part of the fine operator: masked normal coefficients
-__global__ void k_level0_coeffs(PoissonCtx P, MGLevel L0)
-{
-    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
-    if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
-    int c = (kc * P.ny + jc) * P.nx + ic;
-    L0.aE[c] = (ic < P.nx - 1 || P.pi) ? P.gE1[c] : 0.0;
-    L0.aN[c] = (jc < P.ny - 1 || P.pj) ? P.gN2[c] : 0.0;
-    L0.aT[c] = (kc < P.nz - 1 || P.pk) ? P.gT3[c] : 0.0;
-}
-
-__global__ void k_diag(MGLevel L)
-{
-    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
-    if (ic >= L.nx || jc >= L.ny || kc >= L.nz) return;
-    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
-    int c = (kc * L.ny + jc) * L.nx + ic;
-    double aW = (ic > 0 || L.pi) ? L.aE[q.id(kc, jc, ic - 1)] : 0.0;
-    double aS = (jc > 0 || L.pj) ? L.aN[q.id(kc, jc - 1, ic)] : 0.0;
-    double aB = (kc > 0 || L.pk) ? L.aT[q.id(kc - 1, jc, ic)] : 0.0;
-    L.diag[c] = L.aE[c] + aW + L.aN[c] + aS + L.aT[c] + aB;
-}
-
-// face-sum coarse coefficients: a_coarse = s * sum of the fine faces covering
-// the coarse face, s = 1/2 when the face-normal direction is coarsened
-__global__ void k_coarsen_coeffs(MGLevel F, MGLevel Cc)
-{
-    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
-    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
-    int c = (K * Cc.ny + J) * Cc.nx + I;
-    double sE = 0.0, sN = 0.0, sT = 0.0;
-    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) {
-        int fi = F.cx * I + F.cx - 1, fj = F.cy * J + dj, fk = F.cz * K + dk;
-        sE += F.aE[(fk * F.ny + fj) * F.nx + fi];
-    }
-    for (int dk = 0; dk < F.cz; dk++) for (int di = 0; di < F.cx; di++) {
-        int fi = F.cx * I + di, fj = F.cy * J + F.cy - 1, fk = F.cz * K + dk;
-        sN += F.aN[(fk * F.ny + fj) * F.nx + fi];
-    }
-    for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
-        int fi = F.cx * I + di, fj = F.cy * J + dj, fk = F.cz * K + F.cz - 1;
-        sT += F.aT[(fk * F.ny + fj) * F.nx + fi];
-    }
-    Cc.aE[c] = sE * (F.cx == 2 ? 0.5 : 1.0);
-    Cc.aN[c] = sN * (F.cy == 2 ? 0.5 : 1.0);
-    Cc.aT[c] = sT * (F.cz == 2 ? 0.5 : 1.0);
 }
 
 // --------------------------------------------------------- fine operators
@@ -251,120 +189,6 @@ __global__ void k_apply19(PoissonCtx P, const double *__restrict__ x, double *__
     y[c] = -acc;
 }
 
-// ---------------------------------------------------------------- smoothers
-// red-black point Gauss-Seidel on L x = r (7-point level operator)
-__global__ void k_smooth_rb(MGLevel L, int color)
-{
-    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
-    if (ic >= L.nx || jc >= L.ny || kc >= L.nz) return;
-    if (((ic + jc + kc) & 1) != color) return;
-    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
-    int c = (kc * L.ny + jc) * L.nx + ic;
-    double s = L.r[c];
-    if (ic < L.nx - 1 || L.pi) s += L.aE[c] * L.x[q.id(kc, jc, ic + 1)];
-    if (ic > 0 || L.pi)        { int w = q.id(kc, jc, ic - 1); s += L.aE[w] * L.x[w]; }
-    if (jc < L.ny - 1 || L.pj) s += L.aN[c] * L.x[q.id(kc, jc + 1, ic)];
-    if (jc > 0 || L.pj)        { int sI = q.id(kc, jc - 1, ic); s += L.aN[sI] * L.x[sI]; }
-    if (kc < L.nz - 1 || L.pk) s += L.aT[c] * L.x[q.id(kc + 1, jc, ic)];
-    if (kc > 0 || L.pk)        { int b = q.id(kc - 1, jc, ic); s += L.aT[b] * L.x[b]; }
-    L.x[c] = s / L.diag[c];
-}
-
-// zebra j-line Gauss-Seidel (j non-periodic): one thread per (i,k) line of
-// the colour, Thomas algorithm along j
-__global__ void k_smooth_line(MGLevel L, int color)
-{
-    int ic = blockIdx.x * blockDim.x + threadIdx.x, kc = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ic >= L.nx || kc >= L.nz) return;
-    if (((ic + kc) & 1) != color) return;
-    Cg q{L.nx, L.ny, L.nz, L.pi, L.pj, L.pk};
-    const int sj = L.nx;
-    double cprev = 0.0, dprev = 0.0;
-    for (int jc = 0; jc < L.ny; jc++) {
-        int c = (kc * L.ny + jc) * L.nx + ic;
-        double rhs = L.r[c];
-        if (ic < L.nx - 1 || L.pi) rhs += L.aE[c] * L.x[q.id(kc, jc, ic + 1)];
-        if (ic > 0 || L.pi)        { int w = q.id(kc, jc, ic - 1); rhs += L.aE[w] * L.x[w]; }
-        if (kc < L.nz - 1 || L.pk) rhs += L.aT[c] * L.x[q.id(kc + 1, jc, ic)];
-        if (kc > 0 || L.pk)        { int b = q.id(kc - 1, jc, ic); rhs += L.aT[b] * L.x[b]; }
-        double aS = jc > 0 ? L.aN[c - sj] : 0.0;
-        double aN = jc < L.ny - 1 ? L.aN[c] : 0.0;
-        // tridiagonal row: -aS x[j-1] + diag x[j] - aN x[j+1] = rhs; with c' = -aN/m the
-        // eliminated diagonal is m = diag - (-aS) c'[j-1] = diag + aS c'[j-1]
-        double mdiag = L.diag[c] + aS * cprev;
-        double cp = -aN / mdiag;
-        double dp = (rhs + aS * dprev) / mdiag;
-        L.tc[c] = cp; L.td[c] = dp;
-        cprev = cp; dprev = dp;
-    }
-    double xn = 0.0;
-    for (int jc = L.ny - 1; jc >= 0; jc--) {
-        int c = (kc * L.ny + jc) * L.nx + ic;
-        double xv = L.td[c] - L.tc[c] * xn;
-        L.x[c] = xv;
-        xn = xv;
-    }
-}
-
-// coarse rhs = sum over children of the fine residual r - L x
-__global__ void k_restrict_residual(MGLevel F, MGLevel Cc)
-{
-    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
-    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
-    Cg q{F.nx, F.ny, F.nz, F.pi, F.pj, F.pk};
-    double sum = 0.0;
-    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
-        int ic = F.cx * I + di, jc = F.cy * J + dj, kc = F.cz * K + dk;
-        int c = (kc * F.ny + jc) * F.nx + ic;
-        double xc = F.x[c], res = F.r[c] - F.diag[c] * xc;
-        if (ic < F.nx - 1 || F.pi) res += F.aE[c] * F.x[q.id(kc, jc, ic + 1)];
-        if (ic > 0 || F.pi)        { int w = q.id(kc, jc, ic - 1); res += F.aE[w] * F.x[w]; }
-        if (jc < F.ny - 1 || F.pj) res += F.aN[c] * F.x[q.id(kc, jc + 1, ic)];
-        if (jc > 0 || F.pj)        { int s = q.id(kc, jc - 1, ic); res += F.aN[s] * F.x[s]; }
-        if (kc < F.nz - 1 || F.pk) res += F.aT[c] * F.x[q.id(kc + 1, jc, ic)];
-        if (kc > 0 || F.pk)        { int b = q.id(kc - 1, jc, ic); res += F.aT[b] * F.x[b]; }
-        sum += res;
-    }
-    int cI = (K * Cc.ny + J) * Cc.nx + I;
-    Cc.r[cI] = sum;
-    Cc.x[cI] = 0.0;
-}
-
-__global__ void k_prolong_add(MGLevel F, MGLevel Cc)
-{
-    int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
-    if (ic >= F.nx || jc >= F.ny || kc >= F.nz) return;
-    int c = (kc * F.ny + jc) * F.nx + ic;
-    F.x[c] += Cc.x[((kc / F.cz) * Cc.ny + (jc / F.cy)) * Cc.nx + (ic / F.cx)];
-}
-
-// coarsest grid: x = B (r - mean r), then x -= mean x (B = (A + 11^T/n)^-1)
-__global__ void k_dense_solve(MGLevel L, const double *B)
-{
-    extern __shared__ double sh[];
-    int n = (int)L.n;
-    double *rr = sh, *red = sh + n;
-    double s = 0.0;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) { rr[t] = L.r[t]; s += rr[t]; }
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-    double mean = red[0] / n;
-    __syncthreads();
-    double sx = 0.0;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        double acc = 0.0;   // B is symmetric: read column t for coalesced loads
-        for (int u = 0; u < n; u++) acc += B[(size_t)u * n + t] * (rr[u] - mean);
-        L.x[t] = acc;
-        sx += acc;
-    }
-    red[threadIdx.x] = sx;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-    double mx = red[0] / n;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) L.x[t] -= mx;
-}
-
 // ------------------------------------------------------ vector kernels
 // partial sums: slot 0 = a.b, slot 1 = sum(a), slot 2 = max |a * w|
 __global__ void k_dot_partial(int64_t n, const double *a, const double *b, const double *w, double *part)
@@ -408,14 +232,6 @@ __global__ void k_resid(int64_t n, const double *b, double *y)
 __global__ void k_copy(int64_t n, const double *a, double *b)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
-}
-// grounded preconditioner input: level-0 rhs = r with r[pin] = -sum(r)
-__global__ void k_set_pin_rhs(double *r0, int pin, const double *sumr) { r0[pin] = -sumr[0]; }
-// z -= zp (zp is z[pin] captured beforehand), which makes z[pin] exactly zero
-__global__ void k_shift(int64_t n, double *z, const double *zp_ptr)
-{
-    double zp = zp_ptr[0];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) z[t] -= zp;
 }
 __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
 
@@ -484,44 +300,10 @@ static void dot3v(tg_ctx *C, const double *a, const double *b, const double *w, 
     k_dot_final<<<1, RB, 0, C->stream>>>(P.part, P.nblocks, out);
 }
 
-static void vcycle(tg_ctx *C, int l)
-{
-    PoissonCtx &P = *C->pois;
-    MGLevel &L = P.L[l];
-    cudaStream_t st = C->stream;
-    if (l == P.nlev - 1) {
-        int nt = 256;
-        size_t shm = sizeof(double) * (L.n + nt);
-        TG_PROF(C, "mg_coarsest", k_dense_solve<<<1, nt, shm, st>>>(L, P.Binv));
-        return;
-    }
-    const bool fine = l == 0;
-    auto smooth = [&](int color) {
-        if (P.line) TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
-                            k_smooth_line<<<dim3((L.nx + 31) / 32, (L.nz + 7) / 8), dim3(32, 8), 0, st>>>(L, color));
-        else TG_PROF(C, fine ? "mg_smooth_rb_L0" : "mg_smooth_rb_coarse",
-                     k_smooth_rb<<<cgrid(L.nx, L.ny, L.nz), block3(), 0, st>>>(L, color));
-    };
-    for (int s = 0; s < P.nu1; s++) { smooth(0); smooth(1); }
-    MGLevel &Cc = P.L[l + 1];
-    TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict_residual<<<cgrid(Cc.nx, Cc.ny, Cc.nz), block3(), 0, st>>>(L, Cc));
-    vcycle(C, l + 1);
-    TG_PROF(C, fine ? "mg_prolong_L0" : "mg_prolong_coarse", k_prolong_add<<<cgrid(L.nx, L.ny, L.nz), block3(), 0, st>>>(L, Cc));
-    for (int s = 0; s < P.nu2; s++) { smooth(1); smooth(0); }
-}
-
 // z = P M P^T r (grounded multigrid); needs sum(r) at d_sum
 static void precondition(tg_ctx *C, const double *r, double *z, const double *d_sum)
 {
-    PoissonCtx &P = *C->pois;
-    MGLevel &L0 = P.L[0];
-    TG_PROF(C, "pois_copy", k_copy<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, r, L0.r));
-    k_set_pin_rhs<<<1, 1, 0, C->stream>>>(L0.r, P.pin, d_sum);
-    TG_CUDA(cudaMemsetAsync(L0.x, 0, sizeof(double) * P.n, C->stream));
-    vcycle(C, 0);
-    TG_PROF(C, "pois_copy", k_copy<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, L0.x, z));
-    k_scalar_copy<<<1, 1, 0, C->stream>>>(z + P.pin, C->d_scal + 60, 1);
-    TG_PROF(C, "pois_shift", k_shift<<<vblocks(P.n), RB, 0, C->stream>>>(P.n, z, C->d_scal + 60));
+    mg_apply(C, C->pois->mg, r, d_sum, z);
 }
 
 // SetRHS (peqn.c:1942-2063) into the compact vector, negated (L = -A)
@@ -551,28 +333,6 @@ __global__ void k_phi_to_dmda(Grid g, State s, PoissonCtx P)
     s.phi[g.lin(kc + 1, jc + 1, ic + 1)] = P.x[(kc * P.ny + jc) * P.nx + ic];
 }
 
-// dense inverse of (A + 11^T/n) on the host, Gauss-Jordan with partial pivoting
-static bool dense_inverse(std::vector<double> &A, int n, std::vector<double> &inv)
-{
-    inv.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
-    for (int col = 0; col < n; col++) {
-        int piv = col;
-        for (int r = col + 1; r < n; r++) if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col])) piv = r;
-        if (std::fabs(A[(size_t)piv * n + col]) < 1e-300) return false;
-        if (piv != col) for (int k = 0; k < n; k++) { std::swap(A[(size_t)piv * n + k], A[(size_t)col * n + k]); std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]); }
-        double d = 1.0 / A[(size_t)col * n + col];
-        for (int k = 0; k < n; k++) { A[(size_t)col * n + k] *= d; inv[(size_t)col * n + k] *= d; }
-        for (int r = 0; r < n; r++) {
-            if (r == col) continue;
-            double f = A[(size_t)r * n + col];
-            if (f == 0.0) continue;
-            for (int k = 0; k < n; k++) { A[(size_t)r * n + k] -= f * A[(size_t)col * n + k]; inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k]; }
-        }
-    }
-    return true;
-}
-
 void poisson_setup(tg_ctx *C)
 {
     if (C->pois) poisson_destroy(C);
@@ -584,7 +344,6 @@ void poisson_setup(tg_ctx *C)
     P->n = (int64_t)P->nx * P->ny * P->nz;
     P->pin = 0;
     P->ortho = C->orthogonal;
-    P->line = !g.pj && P->ny >= 2;
     const int64_t n = P->n;
     double **fine[] = {&P->gE1, &P->gE2, &P->gE3, &P->gN1, &P->gN2, &P->gN3, &P->gT1, &P->gT2, &P->gT3,
                        &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj};
@@ -593,71 +352,14 @@ void poisson_setup(tg_ctx *C)
     P->part = dallocd(C, 3 * (size_t)P->nblocks);
     k_gather_g<<<cgrid(P->nx, P->ny, P->nz), block3(), 0, C->stream>>>(g, C->m, *P);
 
-    // multigrid hierarchy: halve every even direction with >= 4 cells until <= 512 cells remain
-    P->nu1 = 2; P->nu2 = 2;
-    P->nlev = 1;
-    MGLevel &L0i = P->L[0];
-    L0i = MGLevel{};
-    L0i.nx = P->nx; L0i.ny = P->ny; L0i.nz = P->nz; L0i.pi = P->pi; L0i.pj = P->pj; L0i.pk = P->pk;
-    for (;;) {
-        MGLevel &F = P->L[P->nlev - 1];
-        F.n = (int64_t)F.nx * F.ny * F.nz;
-        auto can = [](int m) { return m >= 4 && (m % 2) == 0; };
-        F.cx = can(F.nx) ? 2 : 1; F.cy = can(F.ny) ? 2 : 1; F.cz = can(F.nz) ? 2 : 1;
-        bool coarsen = F.n > 512 && (F.cx * F.cy * F.cz) > 1 && P->nlev < 16;
-        if (!coarsen) { F.cx = F.cy = F.cz = 1; break; }
-        MGLevel &Cn = P->L[P->nlev++];
-        Cn = MGLevel{};
-        Cn.nx = F.nx / F.cx; Cn.ny = F.ny / F.cy; Cn.nz = F.nz / F.cz;
-        Cn.pi = F.pi; Cn.pj = F.pj; Cn.pk = F.pk;
-    }
-    for (int l = 0; l < P->nlev; l++) {
-        MGLevel &L = P->L[l];
-        L.n = (int64_t)L.nx * L.ny * L.nz;
-        L.aE = dallocd(C, L.n); L.aN = dallocd(C, L.n); L.aT = dallocd(C, L.n); L.diag = dallocd(C, L.n);
-        L.x = dallocd(C, L.n); L.r = dallocd(C, L.n);
-        if (P->line) { L.tc = dallocd(C, L.n); L.td = dallocd(C, L.n); }
-    }
-    k_level0_coeffs<<<cgrid(P->nx, P->ny, P->nz), block3(), 0, C->stream>>>(*P, P->L[0]);
-    for (int l = 0; l + 1 < P->nlev; l++)
-        k_coarsen_coeffs<<<cgrid(P->L[l + 1].nx, P->L[l + 1].ny, P->L[l + 1].nz), block3(), 0, C->stream>>>(P->L[l], P->L[l + 1]);
-    for (int l = 0; l < P->nlev; l++) k_diag<<<cgrid(P->L[l].nx, P->L[l].ny, P->L[l].nz), block3(), 0, C->stream>>>(P->L[l]);
-
-    // dense coarsest inverse
-    MGLevel &Lc = P->L[P->nlev - 1];
-    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells (use even interior sizes)"};
-    const int nc = (int)Lc.n;
-    std::vector<double> aE(nc), aN(nc), aT(nc);
-    TG_CUDA(cudaMemcpyAsync(aE.data(), Lc.aE, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
-    TG_CUDA(cudaMemcpyAsync(aN.data(), Lc.aN, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
-    TG_CUDA(cudaMemcpyAsync(aT.data(), Lc.aT, sizeof(double) * nc, cudaMemcpyDeviceToHost, C->stream));
-    TG_CUDA(cudaStreamSynchronize(C->stream));
-    std::vector<double> A((size_t)nc * nc, 1.0 / nc);
-    auto cid = [&](int k, int j, int i) {
-        i = (i + Lc.nx) % Lc.nx; j = (j + Lc.ny) % Lc.ny; k = (k + Lc.nz) % Lc.nz;
-        return (k * Lc.ny + j) * Lc.nx + i;
-    };
-    for (int k = 0; k < Lc.nz; k++) for (int j = 0; j < Lc.ny; j++) for (int i = 0; i < Lc.nx; i++) {
-        int c = cid(k, j, i);
-        auto add = [&](int nb, double a) { A[(size_t)c * nc + c] += a; A[(size_t)c * nc + nb] -= a; };
-        if (i < Lc.nx - 1 || Lc.pi) add(cid(k, j, i + 1), aE[c]);
-        if (i > 0 || Lc.pi)         { int w = cid(k, j, i - 1); add(w, aE[w]); }
-        if (j < Lc.ny - 1 || Lc.pj) add(cid(k, j + 1, i), aN[c]);
-        if (j > 0 || Lc.pj)         { int s = cid(k, j - 1, i); add(s, aN[s]); }
-        if (k < Lc.nz - 1 || Lc.pk) add(cid(k + 1, j, i), aT[c]);
-        if (k > 0 || Lc.pk)         { int b = cid(k - 1, j, i); add(b, aT[b]); }
-    }
-    std::vector<double> inv;
-    if (!dense_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
-    P->Binv = dallocd(C, (size_t)nc * nc);
-    P->ncoarse = nc;
-    TG_CUDA(cudaMemcpyAsync(P->Binv, inv.data(), sizeof(double) * nc * nc, cudaMemcpyHostToDevice, C->stream));
-    TG_CUDA(cudaStreamSynchronize(C->stream));
+    P->mg = mg_create(C, C->cfg.precision == TG_PREC_MIXED, P->gE1, P->gN2, P->gT3,
+                      P->nx, P->ny, P->nz, P->pi, P->pj, P->pk);
     TG_CUDA(cudaGetLastError());
 }
 
 void poisson_destroy(tg_ctx *C)
 {
+    if (C->pois && C->pois->mg) mg_destroy(C->pois->mg);
     delete C->pois;   // device buffers are owned by the context allocation list
     C->pois = nullptr;
 }

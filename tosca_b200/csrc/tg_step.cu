@@ -625,52 +625,50 @@ __global__ void k_cell_fp(Grid g, State s)
 }
 
 // Pass 3 (ueqn_solvers.c:1008-1035): rhs_face += scale * aj_face *
-// central(S . fp) at the faces of interior cells.
-__global__ void k_rhs_faces(Grid g, Metrics m, State s, V3f<double> R, double scale)
+// central(S . fp) at the faces of interior cells. With `fused` the kernel also
+// forms the rest of ExplicitRhsU at these faces in the reference's order:
+// Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += FormU, +=
+// meanGradPForcing (ueqn_sources.c:3735-3822).
+template <bool fused>
+__global__ void k_rhs_faces(Grid g, Metrics m, State s, V3f<double> R, double scale, Params p, int ab2)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
-    R3<double> fpc = ld3(s.fp, c);
-    double v1, v2;
-    { R3<double> a = ld3(m.csi, c), b = ld3(m.csi, c + 1); R3<double> fb = ld3(s.fp, c + 1);
-      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      R.x[c] += scale * m.iaj[c] * (0.5 * (v1 + v2)); }
-    { int n = c + g.mx; R3<double> a = ld3(m.eta, c), b = ld3(m.eta, n); R3<double> fb = ld3(s.fp, n);
-      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      R.y[c] += scale * m.jaj[c] * (0.5 * (v1 + v2)); }
-    { int n = c + g.mx * g.my; R3<double> a = ld3(m.zet, c), b = ld3(m.zet, n); R3<double> fb = ld3(s.fp, n);
-      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      R.z[c] += scale * m.kaj[c] * (0.5 * (v1 + v2)); }
-}
-
-// meanGradPForcing (ueqn_sources.c:3735-3822)
-__global__ void k_mean_grad_p(Grid g, Metrics m, V3f<double> R, Params p)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
-    int c = g.lin(k, j, i);
-    R3<double> a = ld3(m.icsi, c), b = ld3(m.jeta, c), d = ld3(m.kzet, c);
-    R.x[c] += 1.0 * (p.mgp[0] * a.x + p.mgp[1] * a.y + p.mgp[2] * a.z);
-    R.y[c] += 1.0 * (p.mgp[0] * b.x + p.mgp[1] * b.y + p.mgp[2] * b.z);
-    R.z[c] += 1.0 * (p.mgp[0] * d.x + p.mgp[1] * d.y + p.mgp[2] * d.z);
-}
-
-// Rhs = -dP (+ AB2 buoyancy), ueqn_solvers.c:1305-1338 (all points)
-__global__ void k_rhs_init(int64_t n, State s, int buoy, int ab2)
-{
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        double x = 0.0 - s.dp.x[q], y = 0.0 - s.dp.y[q], z = 0.0 - s.dp.z[q];
-        if (buoy) {
+    R3<double> base;
+    if (fused) {
+        base = R3<double>{0.0 - s.dp.x[c], 0.0 - s.dp.y[c], 0.0 - s.dp.z[c]};
+        if (p.buoyancy) {
+            R3<double> b = ld3(s.btheta, c);
             if (ab2) {
-                x = x + (3.0 / 2.0) * s.btheta.x[q]; y = y + (3.0 / 2.0) * s.btheta.y[q]; z = z + (3.0 / 2.0) * s.btheta.z[q];
-                x = x + (-1.0 / 2.0) * s.btheta_o.x[q]; y = y + (-1.0 / 2.0) * s.btheta_o.y[q]; z = z + (-1.0 / 2.0) * s.btheta_o.z[q];
+                R3<double> bo = ld3(s.btheta_o, c);
+                base = base + (3.0 / 2.0) * b;
+                base = base + (-1.0 / 2.0) * bo;
             } else {
-                x = x + 1.0 * s.btheta.x[q]; y = y + 1.0 * s.btheta.y[q]; z = z + 1.0 * s.btheta.z[q];
+                base = base + 1.0 * b;
             }
         }
-        s.rhs.x[q] = x; s.rhs.y[q] = y; s.rhs.z[q] = z;
+    } else {
+        base = ld3(R, c);
     }
+    R3<double> fpc = ld3(s.fp, c);
+    double v1, v2, ox, oy, oz;
+    { R3<double> a = ld3(m.csi, c), b = ld3(m.csi, c + 1); R3<double> fb = ld3(s.fp, c + 1);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      ox = base.x + scale * m.iaj[c] * (0.5 * (v1 + v2)); }
+    { int n = c + g.mx; R3<double> a = ld3(m.eta, c), b = ld3(m.eta, n); R3<double> fb = ld3(s.fp, n);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      oy = base.y + scale * m.jaj[c] * (0.5 * (v1 + v2)); }
+    { int n = c + g.mx * g.my; R3<double> a = ld3(m.zet, c), b = ld3(m.zet, n); R3<double> fb = ld3(s.fp, n);
+      v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
+      oz = base.z + scale * m.kaj[c] * (0.5 * (v1 + v2)); }
+    if (fused && p.mean_grad_p) {
+        R3<double> a = ld3(m.icsi, c), b = ld3(m.jeta, c), d = ld3(m.kzet, c);
+        ox += 1.0 * (p.mgp[0] * a.x + p.mgp[1] * a.y + p.mgp[2] * a.z);
+        oy += 1.0 * (p.mgp[0] * b.x + p.mgp[1] * b.y + p.mgp[2] * b.z);
+        oz += 1.0 * (p.mgp[0] * d.x + p.mgp[1] * d.y + p.mgp[2] * d.z);
+    }
+    R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
 }
 
 // resetNonResolvedCellFaces (inline.h:1674-1835) on the boundary planes of one
@@ -931,11 +929,11 @@ void grad_p(tg_ctx *C)
 
 void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
 
-void form_u(tg_ctx *C, V3f<double> rhs, double scale)
+// FormU passes 1-2 (face fluxes, cell divergence with ghost handling)
+static void form_u_fp(tg_ctx *C)
 {
     const Grid g = C->g;
     const size_t G = (size_t)g.size();
-    // face flux arrays: f1, f2, f3 are contiguous (9 planes); fp follows
     TG_CUDA(cudaMemsetAsync(C->s.f1.x, 0, 12 * sizeof(double) * G, C->stream));
     TG_PROF(C, "formu_face_fluxes", k_face_fluxes<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm));
     reset_face_periodic(C, C->s.f1);
@@ -943,20 +941,27 @@ void form_u(tg_ctx *C, V3f<double> rhs, double scale)
     reset_face_periodic(C, C->s.f3);
     TG_PROF(C, "formu_cell_fp", k_cell_fp<<<gi(g), block3(), 0, C->stream>>>(g, C->s));
     reset_cell_periodic(C, C->s.fp);
-    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, rhs, scale));
+}
+
+void form_u(tg_ctx *C, V3f<double> rhs, double scale)
+{
+    const Grid g = C->g;
+    form_u_fp(C);
+    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<false><<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, rhs, scale, C->prm, 0));
 }
 
 void explicit_rhs(tg_ctx *C)
 {
     const Grid g = C->g;
-    const int64_t G = g.size();
     reset_no_penetration(C);
     reset_face_periodic(C, C->s.ucont);
     contra_to_cart(C);
     reset_cell_periodic(C, C->s.ucat);
-    TG_PROF(C, "rhs_init", k_rhs_init<<<nblk(G), 256, 0, C->stream>>>(G, C->s, C->prm.buoyancy, C->it > C->cfg.it_start ? 1 : 0));
-    form_u(C, C->s.rhs, 1.0);
-    if (C->prm.mean_grad_p) TG_PROF(C, "mean_grad_p", k_mean_grad_p<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s.rhs, C->prm));
+    form_u_fp(C);
+    // every point outside the interior faces keeps Rhs = -dP + b = 0
+    TG_CUDA(cudaMemsetAsync(C->s.rhs.x, 0, 3 * sizeof(double) * g.size(), C->stream));
+    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<true><<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->s.rhs, 1.0, C->prm,
+                                                                                    C->it > C->cfg.it_start ? 1 : 0));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, 0));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, 1));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
