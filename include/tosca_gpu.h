@@ -121,7 +121,9 @@ enum {
 };
 
 /* ----------------------------------------------------------------- lifecycle -- */
-/* Replaces simulationInitialize's per-domain allocation (initialization.c:63). */
+/* Replaces simulationInitialize's per-domain allocation (initialization.h:39 /
+ * initialization.c:63) and the solver set-up of InitializeUEqn / InitializePEqn
+ * (ueqn.h:92, peqn.h:58). */
 tg_status tg_create(const tg_config *cfg, tg_ctx **out);
 tg_status tg_destroy(tg_ctx *ctx);
 const char *tg_last_error(const tg_ctx *ctx);
@@ -129,8 +131,10 @@ const char *tg_status_string(tg_status s);
 
 /* Grid nodes (AoS xyz, global extent, node (k,j,i) at DMDA point (k,j,i) for
  * k<mz-1, j<my-1, i<mx-1; mesh.c:34-447). Computes all cell and face metrics on
- * the device: replaces SetMeshMetrics (mesh.c:630-1976) and the metric tensor of
- * SetCoeffMatrix (peqn.c:703-849). */
+ * the device: replaces SetMeshMetrics (mesh.h:94 / mesh.c:630-1976) and the
+ * connectivity and matrix of SetPoissonConnectivity / SetCoeffMatrix
+ * (peqn.h:115,118 / peqn.c:107-248, 703-1501), which become a matrix-free
+ * operator and its multigrid hierarchy. */
 tg_status tg_set_mesh_nodes(tg_ctx *ctx, const double *nodes);
 
 /* Generic field transfer (global extent if halo = 0, local ghosted if halo > 0).
@@ -145,21 +149,23 @@ tg_status tg_get_field(tg_ctx *ctx, int32_t which, double *host, int32_t halo);
 tg_status tg_init_from_cartesian(tg_ctx *ctx, const double *ucat, int32_t halo);
 
 /* ------------------------------------------------------------------ stages -- */
-tg_status tg_contravariant_to_cartesian(tg_ctx *ctx);       /* ueqn.c:528-635          */
-tg_status tg_update_nut(tg_ctx *ctx);                       /* les.c:165-180,2119-2578 */
-tg_status tg_update_wall_models(tg_ctx *ctx);               /* boundary.c:3257-3600    */
-tg_status tg_grad_p(tg_ctx *ctx);                           /* peqn.c:3437-3773        */
-tg_status tg_buoyancy(tg_ctx *ctx);                         /* ueqn_sources.c:2726-2880*/
+/* Each replaces one reference function: declaration (header) / definition. */
+tg_status tg_contravariant_to_cartesian(tg_ctx *ctx);  /* ueqn.h:98 / ueqn.c:528-635              */
+tg_status tg_update_nut(tg_ctx *ctx);                  /* les.h:73,76 / les.c:165-180,2119-2578    */
+tg_status tg_update_wall_models(tg_ctx *ctx);          /* boundary.h:188 / boundary.c:3257-3600    */
+tg_status tg_grad_p(tg_ctx *ctx);                      /* peqn.h:109 / peqn.c:3437-3773            */
+tg_status tg_buoyancy(tg_ctx *ctx);                    /* ueqn_sources.h:23 / ueqn_sources.c:2726  */
 /* Rhs (TG_F_RHS) += scale * FormU on the current lUcont/lUcat/nut:
- * ueqn_solvers.c:6-1083 with formMode 0. Rhs is zeroed first when zero_rhs. */
+ * ueqn_solvers.h:15 / ueqn_solvers.c:6-1083 with formMode 0. Rhs is
+ * zeroed first when zero_rhs. */
 tg_status tg_form_u(tg_ctx *ctx, double scale, int32_t zero_rhs);
-tg_status tg_explicit_rhs(tg_ctx *ctx);                     /* ueqn_solvers.c:1276-1407*/
-tg_status tg_solve_u(tg_ctx *ctx);                          /* ueqn.c:397-440 (FE, RK4)*/
-tg_status tg_solve_p(tg_ctx *ctx, tg_stats *stats);         /* peqn.c:3777-3971        */
-tg_status tg_continuity_error(tg_ctx *ctx, double *max_div);/* peqn.c:4114-4181        */
-tg_status tg_update_cartesian_bcs(tg_ctx *ctx);             /* boundary.c:824-2050     */
-tg_status tg_update_contravariant_bcs(tg_ctx *ctx);         /* boundary.c:614-822      */
-tg_status tg_sync_pressure(tg_ctx *ctx);                    /* overset.c:263-315       */
+tg_status tg_explicit_rhs(tg_ctx *ctx);                /* ueqn_solvers.h:24 / ueqn_solvers.c:1276  */
+tg_status tg_solve_u(tg_ctx *ctx);                     /* ueqn.h:107 / ueqn.c:397-440 (FE, RK4)    */
+tg_status tg_solve_p(tg_ctx *ctx, tg_stats *stats);    /* peqn.h:142 / peqn.c:3777-3971            */
+tg_status tg_continuity_error(tg_ctx *ctx, double *max_div); /* peqn.h:148 / peqn.c:4114-4181      */
+tg_status tg_update_cartesian_bcs(tg_ctx *ctx);        /* boundary.h:167 / boundary.c:824-2050     */
+tg_status tg_update_contravariant_bcs(tg_ctx *ctx);    /* boundary.h:164 / boundary.c:614-822      */
+tg_status tg_sync_pressure(tg_ctx *ctx);               /* overset.h:107 / overset.c:263-315        */
 
 /* nsteps full time steps in the order of main.c:54-327 (fixed dt). */
 tg_status tg_step(tg_ctx *ctx, int32_t nsteps, tg_stats *stats);
