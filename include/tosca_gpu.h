@@ -163,6 +163,25 @@ tg_status tg_explicit_rhs(tg_ctx *ctx);                /* ueqn_solvers.h:24 / ue
 tg_status tg_solve_u(tg_ctx *ctx);                     /* ueqn.h:107 / ueqn.c:397-440 (FE, RK4)    */
 tg_status tg_solve_p(tg_ctx *ctx, tg_stats *stats);    /* peqn.h:142 / peqn.c:3777-3971            */
 tg_status tg_continuity_error(tg_ctx *ctx, double *max_div); /* peqn.h:148 / peqn.c:4114-4181      */
+/* Allocation-free form of the divergence check; no counterpart in the
+ * reference. For callers that cannot allocate device memory: code running
+ * while a stream is captured into a CUDA graph (cudaMalloc is not allowed
+ * there), hosts whose device memory belongs to a fixed pool or framework
+ * allocator that must stay the only allocator, and loops that cannot absorb
+ * the device synchronisation of cudaMalloc/cudaFree. Computes the same value
+ * as tg_continuity_error, max over interior cells of |div(Ucont)| * aj, from
+ * caller-owned DEVICE arrays of the global extent (ucont AoS triples, aj
+ * scalars) on the caller's current device, and writes it to the device
+ * scalar *max_div on `stream` (a cudaStream_t; NULL = default stream). No
+ * context is needed and nothing is allocated: the per-plane partial maxima
+ * live in a file-scope device array of 16384 doubles (128 KiB) that every GPU
+ * loading the library holds until exit, so mz - 2 <= 16384 interior planes;
+ * larger grids return TG_ERR_BAD_ARG. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture. All calls share the array: calls that overlap on one GPU
+ * race and must be serialised by the caller. */
+tg_status tg_continuity_error_noalloc(const double *ucont, const double *aj, int32_t mx, int32_t my,
+                                      int32_t mz, double *max_div, void *stream);
 tg_status tg_update_cartesian_bcs(tg_ctx *ctx);        /* boundary.h:167 / boundary.c:824-2050     */
 tg_status tg_update_contravariant_bcs(tg_ctx *ctx);    /* boundary.h:164 / boundary.c:614-822      */
 tg_status tg_sync_pressure(tg_ctx *ctx);               /* overset.h:107 / overset.c:263-315        */

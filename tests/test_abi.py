@@ -18,11 +18,16 @@ def declared_symbols():
     return sorted(set(re.findall(r"^(?:tg_status|const char \*)\s*(tg_[a-z_0-9]+)\(", src, re.M)))
 
 
+# context-free device-pointer entry point: bound directly by its test, and not
+# exported by the CPU restatement
+NO_CONTEXT = {"tg_continuity_error_noalloc"}
+
+
 def test_header_matches_bindings():
     decl = declared_symbols()
     assert decl, "no declarations found"
     bound = {"tg_" + n for n in api.ENTRY_POINTS}
-    assert set(decl) == bound
+    assert set(decl) == bound | NO_CONTEXT
 
 
 def test_library_exports_all_symbols():
@@ -38,6 +43,8 @@ def test_oracle_exports_same_entry_points():
     oracle.load()
     lib = oracle.lib()
     for name in declared_symbols():
+        if name in NO_CONTEXT:
+            continue
         assert hasattr(lib, "tor_" + name[3:]), name
 
 
