@@ -181,17 +181,20 @@ __device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i)
 }
 
 // Chunked zebra line solve (nx even): lane -> one of 32 consecutive
-// same-colour lines (flattened over (k, t)), warp w -> j in [w*cj, (w+1)*cj).
+// same-colour lines (flattened over (k, t)), warp w -> j in [w*CJ, (w+1)*CJ).
 // dp_j = (rhs_j + aS_j dp_{j-1}) / m_j and x_j = dp_j - c'_j x_{j+1} are first
 // order affine recurrences: each warp composes its chunk into (offset,
 // multiplier) pairs, warp 0 chains the chunk ends, each warp finishes its chunk.
-template <class T>
-__global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int color, int cj)
+// The loads of a chunk do not depend on each other, so they are issued in an
+// unrolled pass of compile-time length CJ before the recurrence runs on
+// shared memory.
+template <class T, int CJ>
+__global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int color)
 {
     extern __shared__ unsigned char smraw[];
-    T *D = reinterpret_cast<T *>(smraw);            // [ny][32] offsets
-    T *Mu = D + L.ny * 32;                          // [ny][32] multipliers
-    T *SD = Mu + L.ny * 32;                         // [NW][32] chunk offsets
+    T *D = reinterpret_cast<T *>(smraw);            // [NW*CJ][32] offsets
+    T *Mu = D + LINE_NW * CJ * 32;                  // [NW*CJ][32] multipliers
+    T *SD = Mu + LINE_NW * CJ * 32;                 // [NW][32] chunk offsets
     T *SM = SD + LINE_NW * 32;                      // [NW][32] chunk multipliers
     T *ST = SM + LINE_NW * 32;                      // [NW][32] chunk boundary values
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -200,21 +203,35 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
     const bool active = lid < half * L.nz;
     const int k = active ? lid / half : 0, t = active ? lid % half : 0;
     const int i = 2 * t + ((color ^ k) & 1);
-    const int nx = L.nx;
-    const int j0 = w * cj, j1 = min(L.ny, j0 + cj);
-    T dl = T(0), ml = T(1);
+    const int nx = L.nx, ny = L.ny;
+    const int j0 = w * CJ;
+    // (1a) independent loads: D = rhs * minv, Mu = aS * minv
     if (active) {
-        int c = sidx(L, k, j0, i);
-        #pragma unroll 4
-        for (int j = j0; j < j1; j++, c += nx) {
-            T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
-            T aS = j > 0 ? L.aN[c - nx] : T(0);
-            T mi = L.minv[c];
-            T f = aS * mi;
-            dl = rhs * mi + f * dl;
+        const int c0 = sidx(L, k, j0, i);
+        #pragma unroll
+        for (int u = 0; u < CJ; u++) {
+            const int j = j0 + u;
+            if (j < ny) {
+                const int c = c0 + u * nx;
+                T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
+                T mi = L.minv[c];
+                T aS = j > 0 ? L.aN[c - nx] : T(0);
+                D[(w * CJ + u) * 32 + lane] = rhs * mi;
+                Mu[(w * CJ + u) * 32 + lane] = aS * mi;
+            }
+        }
+    }
+    // (1b) local forward recurrence of the chunk
+    T dl = T(0), ml = T(1);
+    #pragma unroll
+    for (int u = 0; u < CJ; u++) {
+        if (active && j0 + u < ny) {
+            const int q = (w * CJ + u) * 32 + lane;
+            const T f = Mu[q];
+            dl = D[q] + f * dl;
             ml = f * ml;
-            D[j * 32 + lane] = dl;
-            Mu[j * 32 + lane] = ml;
+            D[q] = dl;
+            Mu[q] = ml;
         }
     }
     SD[w * 32 + lane] = dl;
@@ -222,21 +239,28 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
     __syncthreads();
     if (w == 0) {
         T s = T(0);
+        #pragma unroll
         for (int q = 0; q < LINE_NW; q++) { ST[q * 32 + lane] = s; s = SD[q * 32 + lane] + SM[q * 32 + lane] * s; }
     }
     __syncthreads();
     const T st = ST[w * 32 + lane];
+    // (3) backward recurrence of the chunk; c' loaded before the chain
+    T cpv[CJ];
+    if (active) {
+        const int c0 = sidx(L, k, j0, i);
+        #pragma unroll
+        for (int u = 0; u < CJ; u++) cpv[u] = (j0 + u < ny) ? L.cp[c0 + u * nx] : T(0);
+    }
     T xl = T(0), nl = T(1);
-    if (active && j1 > j0) {
-        int c = sidx(L, k, j1 - 1, i);
-        #pragma unroll 4
-        for (int j = j1 - 1; j >= j0; j--, c -= nx) {
-            T dp = D[j * 32 + lane] + Mu[j * 32 + lane] * st;
-            T cp = L.cp[c];
-            xl = dp - cp * xl;
-            nl = -cp * nl;
-            D[j * 32 + lane] = xl;
-            Mu[j * 32 + lane] = nl;
+    #pragma unroll
+    for (int u = CJ - 1; u >= 0; u--) {
+        if (active && j0 + u < ny) {
+            const int q = (w * CJ + u) * 32 + lane;
+            const T dp = D[q] + Mu[q] * st;
+            xl = dp - cpv[u] * xl;
+            nl = -cpv[u] * nl;
+            D[q] = xl;
+            Mu[q] = nl;
         }
     }
     __syncthreads();
@@ -245,18 +269,58 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
     __syncthreads();
     if (w == 0) {
         T xn = T(0);
+        #pragma unroll
         for (int q = LINE_NW - 1; q >= 0; q--) { ST[q * 32 + lane] = xn; xn = SD[q * 32 + lane] + SM[q * 32 + lane] * xn; }
     }
     __syncthreads();
     const T xnext = ST[w * 32 + lane];
     if (active) {
-        int c = sidx(L, k, j0, i);
-        for (int j = j0; j < j1; j++, c += nx) L.x[c] = D[j * 32 + lane] + Mu[j * 32 + lane] * xnext;
+        const int c0 = sidx(L, k, j0, i);
+        #pragma unroll
+        for (int u = 0; u < CJ; u++)
+            if (j0 + u < ny) {
+                const int q = (w * CJ + u) * 32 + lane;
+                L.x[c0 + u * nx] = D[q] + Mu[q] * xnext;
+            }
+    }
+}
+
+// chunk length (power of two >= ceil(ny / NW)) of the line solver; 0 if too long
+inline int line_cj(int ny)
+{
+    int need = (ny + LINE_NW - 1) / LINE_NW;
+    int cj = 1;
+    while (cj < need) cj <<= 1;
+    return cj <= 32 ? cj : 0;
+}
+
+template <class T>
+size_t line_chunk_smem_cj(int cj) { return sizeof(T) * (2 * (size_t)LINE_NW * cj * 32 + 3 * LINE_NW * 32); }
+
+template <class T>
+void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
+{
+    const int lines = (F.nx >> 1) * F.nz;
+    const int nb = (lines + 31) / 32;
+    const int cj = line_cj(F.ny);
+    const size_t shm = line_chunk_smem_cj<T>(cj);
+    switch (cj) {
+    case 1: k_line_chunked<T, 1><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 2: k_line_chunked<T, 2><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 4: k_line_chunked<T, 4><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 8: k_line_chunked<T, 8><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 16: k_line_chunked<T, 16><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    default: k_line_chunked<T, 32><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
     }
 }
 
 template <class T>
-size_t line_chunk_smem(int ny) { return sizeof(T) * (2 * (size_t)ny * 32 + 3 * LINE_NW * 32); }
+void set_line_smem_attrs()
+{
+    TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_chunk_smem_cj<T>(16)));
+    TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_chunk_smem_cj<T>(32)));
+}
+
 
 // lines of one colour: (i + k) & 1 == color, i.e. i of parity (color ^ k) & 1
 template <class T>
@@ -438,11 +502,8 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
     Lvl<T> &F = L[l];
     const bool fine = l == 0;
     auto smooth = [&](int color) {
-        if (mg->line && (F.nx % 2) == 0) {
-            int lines = (F.nx >> 1) * F.nz;
-            int cj = (F.ny + LINE_NW - 1) / LINE_NW;
-            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
-                    k_line_chunked<T><<<(lines + 31) / 32, LINE_NW * 32, line_chunk_smem<T>(F.ny), st>>>(F, color, cj));
+        if (mg->line && (F.nx % 2) == 0 && line_cj(F.ny) > 0) {
+            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse", launch_line_chunked<T>(F, color, st));
         } else if (mg->line) {
             int half = (F.nx + 1) >> 1;
             TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
@@ -517,13 +578,7 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         k_diag<T><<<g3(L[l].nx, L[l].ny, L[l].nz), block3(), 0, st>>>(L[l]);
         if (mg->line) k_line_factors<T><<<dim3((L[l].nx + 31) / 32, (L[l].nz + 7) / 8), dim3(32, 8), 0, st>>>(L[l]);
     }
-    if (mg->line) {
-        int maxny = 0;
-        for (int l = 0; l < mg->nlev; l++) maxny = std::max(maxny, L[l].ny);
-        size_t shm = line_chunk_smem<T>(maxny);
-        if (shm > 200 * 1024) throw CudaError{cudaErrorInvalidValue, "grid lines too long for the shared-memory line solver"};
-        TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-    }
+    if (mg->line) set_line_smem_attrs<T>();
     mg->tail_start = mg->nlev - 1;
     while (mg->tail_start > 0 && L[mg->tail_start - 1].n <= TAIL_CELLS) mg->tail_start--;
 
