@@ -235,12 +235,8 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         State &st = C->s;
         V3f<double> *sv[] = {&st.ucont, &st.ucont_o, &st.ucat, &st.rhs, &st.dp, &st.btheta, &st.btheta_o, &st.gcont, &st.utmp, &st.snap};
         for (auto *v : sv) *v = dalloc3(C, G);
-        // face flux planes f1, f2, f3 and fp contiguous (12 planes) so one memset clears them
-        double *ff = dallocd(C, 12 * G);
-        st.f1 = V3f<double>{ff, ff + G, ff + 2 * G};
-        st.f2 = V3f<double>{ff + 3 * G, ff + 4 * G, ff + 5 * G};
-        st.f3 = V3f<double>{ff + 6 * G, ff + 7 * G, ff + 8 * G};
-        st.fp = V3f<double>{ff + 9 * G, ff + 10 * G, ff + 11 * G};
+        C->mixed = cfg->precision == TG_PREC_MIXED;
+        alloc_precision_work(C);
         double **ss[] = {&st.p, &st.phi, &st.nut, &st.tmprt, &st.ssnap};
         for (auto **v : ss) *v = dallocd(C, G);
         const size_t P = (size_t)g.mx * g.mz;
@@ -291,6 +287,7 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
         k_zero_last_nodes<<<grid3(g.mx, g.my, g.mz), block3(), 0, C->stream>>>(g, dn);
         TG_CUDA(cudaStreamSynchronize(C->stream));
         metrics_from_nodes(C, dn);
+        C->met32_stale = true;
         // orthogonality: every cross term of the face metric tensor vanishes
         std::vector<double> h(G);
         double mx = 0.0;
@@ -310,9 +307,15 @@ tg_status tg_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
     return guarded(C, [&]() -> tg_status {
         if (!host || halo < 0) return fail(C, TG_ERR_BAD_ARG, "bad field argument");
         V3f<double> v;
-        if (vec_field(C, w, v)) { upload(C, host, halo, v.x, v.y, v.z); TG_CUDA(cudaStreamSynchronize(C->stream)); return TG_OK; }
-        if (double *s = scal_field(C, w)) { upload(C, host, halo, s, nullptr, nullptr); TG_CUDA(cudaStreamSynchronize(C->stream)); return TG_OK; }
-        return fail(C, TG_ERR_BAD_ARG, "field not settable");
+        double *sp = nullptr;
+        if (vec_field(C, w, v)) upload(C, host, halo, v.x, v.y, v.z);
+        else if ((sp = scal_field(C, w)) != nullptr) upload(C, host, halo, sp, nullptr, nullptr);
+        else return fail(C, TG_ERR_BAD_ARG, "field not settable");
+        TG_CUDA(cudaStreamSynchronize(C->stream));
+        if (w == TG_F_RHS) C->clear_rhs = true;
+        if (w == TG_F_DP) C->clear_dp = true;
+        if ((w >= TG_F_CSI && w <= TG_F_KZET) || (w >= TG_F_AJ && w <= TG_F_KAJ)) C->met32_stale = true;
+        return TG_OK;
     });
 }
 

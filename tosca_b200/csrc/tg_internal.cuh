@@ -63,9 +63,24 @@ struct Metrics {
     double *g11, *g12, *g13, *g21, *g22, *g23, *g31, *g32, *g33;
 };
 
+// the metric fields read by the momentum stencils at storage precision T:
+// views of Metrics for FP64, converted copies for the mixed-precision mode
+template <class T>
+struct FaceMet {
+    V3f<T> csi, eta, zet, icsi, ieta, izet, jcsi, jeta, jzet, kcsi, keta, kzet;
+    T *aj, *iaj, *jaj, *kaj;
+};
+
+// FormU work planes at storage precision T: face fluxes per direction and
+// their cell divergence
+template <class T>
+struct FluxWork {
+    V3f<T> f1, f2, f3, fp;
+};
+
 // physical state and work arrays
 struct State {
-    V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, fp, f1, f2, f3, snap;
+    V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, snap;
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
@@ -114,6 +129,27 @@ struct tg_ctx {
     bool orthogonal = true;              // all cross metric-tensor terms vanish
     bool ufilt_set = false;
     int it = 0;
+    // mixed precision: FP32 copies of the stencil metrics (and FP32 FormU
+    // planes when the policy stores the face fluxes in FP32)
+    bool mixed = false;
+    // which momentum stages read the FP32 metric copies (and compute in FP32)
+    struct {
+        bool contra_m32 = false;     // contravariantToCartesian: FP32 metrics
+        bool contra_a32 = false;     //   ... and FP32 arithmetic
+        bool visc32 = false;         // FormU viscous fluxes
+        bool flux32 = false;         // FormU face-flux planes stored in FP32
+        bool rhs32 = false;          // FormU face assembly metrics
+        bool smag32 = false;         // Smagorinsky eddy viscosity
+        bool gradp32 = false;        // GradP
+    } pol;
+    bool met32_stale = true;             // metrics changed since the FP32 copies were made
+    tg::FaceMet<double> fm64{};
+    tg::FaceMet<float> fm32{};
+    tg::FluxWork<double> fw64{};
+    tg::FluxWork<float> fw32{};
+    // a caller wrote Rhs / dP through tg_set_field: the next evaluation clears
+    // the points outside the ones it writes
+    bool clear_rhs = false, clear_dp = false;
     std::string err;
     tg::PoissonCtx *pois = nullptr;
     tg::Profiler prof;
@@ -162,6 +198,8 @@ inline dim3 block3() { return dim3(BX, BY, BZ); }
 
 // stage entry points (tg_step.cu)
 void metrics_from_nodes(tg_ctx *C, const double *d_nodes);
+void alloc_precision_work(tg_ctx *C);         // FP64 views, FP32 copies (mixed mode)
+void refresh_met32(tg_ctx *C);                // FP32 metric copies from the FP64 fields
 void contra_to_cart(tg_ctx *C);
 void reset_cell_periodic(tg_ctx *C, V3f<double> v);
 void reset_cell_periodic_s(tg_ctx *C, double *v);

@@ -3,6 +3,7 @@
 // projection and divergence. Each kernel restates one loop of the reference
 // (file:line at the kernel). All fields are SoA FP64 on the global DMDA extent.
 #include <cmath>
+#include <type_traits>
 
 #include "tg_internal.cuh"
 
@@ -15,25 +16,61 @@ __device__ __forceinline__ bool is_wall(int t) { return t == TG_BC_NOSLIP || t =
 inline dim3 g2(int na, int nb) { return dim3((na + 31) / 32, (nb + 7) / 8); }
 const dim3 b2(32, 8);
 
+// element-type conversion of a vector triple
+template <class To, class From>
+__device__ __forceinline__ R3<To> cvta(R3<From> a) { return R3<To>{(To)a.x, (To)a.y, (To)a.z}; }
+
 // ------------------------------------------------------------------------
 // contravariantToCartesian (ueqn.c:528-635): average face fluxes to the
 // centre and solve [csi;eta;zet] u = q by Cramer's rule. Interior cells.
+// MS is the storage type of the metrics (FP32 copies in the mixed-precision
+// mode), A the arithmetic type; Ucont and Ucat stay FP64.
 // ------------------------------------------------------------------------
-__global__ void k_contra_to_cart(Grid g, Metrics m, State s)
+template <class A, class MS>
+__device__ __forceinline__ void contra_cell(const Grid &g, const FaceMet<MS> &m, const State &s, int c)
+{
+    using M = A;
+    R3<M> sc = cvta<M>(ld3(m.csi, c)), e = cvta<M>(ld3(m.eta, c)), z = cvta<M>(ld3(m.zet, c));
+    M m00 = sc.x, m01 = sc.y, m02 = sc.z, m10 = e.x, m11 = e.y, m12 = e.z, m20 = z.x, m21 = z.y, m22 = z.z;
+    M q0 = (M)(0.5 * (s.ucont.x[c - 1] + s.ucont.x[c]));
+    M q1 = (M)(0.5 * (s.ucont.y[c - g.mx] + s.ucont.y[c]));
+    M q2 = (M)(0.5 * (s.ucont.z[c - g.mx * g.my] + s.ucont.z[c]));
+    M det  =  m00 * (m11 * m22 - m12 * m21) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
+    M det0 =  q0 * (m11 * m22 - m12 * m21) - q1 * (m01 * m22 - m02 * m21) + q2 * (m01 * m12 - m02 * m11);
+    M det1 = -q0 * (m10 * m22 - m12 * m20) + q1 * (m00 * m22 - m02 * m20) - q2 * (m00 * m12 - m02 * m10);
+    M det2 =  q0 * (m10 * m21 - m11 * m20) - q1 * (m00 * m21 - m01 * m20) + q2 * (m00 * m11 - m01 * m10);
+    s.ucat.x[c] = (double)(det0 / det); s.ucat.y[c] = (double)(det1 / det); s.ucat.z[c] = (double)(det2 / det);
+}
+
+template <class A, class MS>
+__global__ void k_contra_to_cart(Grid g, FaceMet<MS> m, State s)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
-    int c = g.lin(k, j, i);
-    R3<double> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
-    double m00 = sc.x, m01 = sc.y, m02 = sc.z, m10 = e.x, m11 = e.y, m12 = e.z, m20 = z.x, m21 = z.y, m22 = z.z;
-    double q0 = 0.5 * (s.ucont.x[c - 1] + s.ucont.x[c]);
-    double q1 = 0.5 * (s.ucont.y[c - g.mx] + s.ucont.y[c]);
-    double q2 = 0.5 * (s.ucont.z[c - g.mx * g.my] + s.ucont.z[c]);
-    double det  =  m00 * (m11 * m22 - m12 * m21) - m01 * (m10 * m22 - m12 * m20) + m02 * (m10 * m21 - m11 * m20);
-    double det0 =  q0 * (m11 * m22 - m12 * m21) - q1 * (m01 * m22 - m02 * m21) + q2 * (m01 * m12 - m02 * m11);
-    double det1 = -q0 * (m10 * m22 - m12 * m20) + q1 * (m00 * m22 - m02 * m20) - q2 * (m00 * m12 - m02 * m10);
-    double det2 =  q0 * (m10 * m21 - m11 * m20) - q1 * (m00 * m21 - m01 * m20) + q2 * (m00 * m11 - m01 * m10);
-    s.ucat.x[c] = det0 / det; s.ucat.y[c] = det1 / det; s.ucat.z[c] = det2 / det;
+    contra_cell<A>(g, m, s, g.lin(k, j, i));
+}
+
+// the same on the interior cells next to the boundary only: the cells whose
+// Cartesian velocity reaches the ghost cells through the periodic copies.
+// blockIdx.z selects the boundary plane.
+__global__ void k_contra_to_cart_shell(Grid g, FaceMet<double> m, State s)
+{
+    int patch = blockIdx.z;
+    int dir = patch >> 1, right = patch & 1;
+    int a = blockIdx.x * blockDim.x + threadIdx.x + 1, b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int na = (dir == 0 ? g.my : g.mx) - 2, nb = (dir == 2 ? g.my : g.mz) - 2;
+    if (a > na || b > nb) return;
+    int i, j, k;
+    if (dir == 0) { k = b; j = a; i = right ? g.mx - 2 : 1; }
+    else if (dir == 1) { k = b; i = a; j = right ? g.my - 2 : 1; }
+    else { j = b; i = a; k = right ? g.mz - 2 : 1; }
+    contra_cell<double>(g, m, s, g.lin(k, j, i));
+}
+
+// FP32 copies of the stencil metrics
+__global__ void k_to_f32(int64_t n, const double *a, float *b)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) b[q] = (float)a[q];
 }
 
 // ------------------------------------------------------------------------
@@ -42,8 +79,8 @@ __global__ void k_contra_to_cart(Grid g, Metrics m, State s)
 // i, then j, then k, which composes to the reference's simultaneous remap.
 // left_only: resetFacePeriodicFluxesVector (inline.h:5357-5451), face 0 <- m-2.
 // ------------------------------------------------------------------------
-template <int NC>
-__global__ void k_periodic_copy(Grid g, double *a0, double *a1, double *a2, int dir, int left_only)
+template <int NC, class T>
+__global__ void k_periodic_copy(Grid g, T *a0, T *a1, T *a2, int dir, int left_only)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
     int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
@@ -58,13 +95,13 @@ __global__ void k_periodic_copy(Grid g, double *a0, double *a1, double *a2, int 
     }
 }
 
-template <int NC>
-void periodic_copy(tg_ctx *C, double *a0, double *a1, double *a2, int left_only)
+template <int NC, class T>
+void periodic_copy(tg_ctx *C, T *a0, T *a1, T *a2, int left_only)
 {
     const Grid g = C->g;
-    if (g.pi) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 0, left_only));
-    if (g.pj) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 1, left_only));
-    if (g.pk) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC><<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, a0, a1, a2, 2, left_only));
+    if (g.pi) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC, T><<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 0, left_only));
+    if (g.pj) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC, T><<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, a0, a1, a2, 1, left_only));
+    if (g.pk) TG_PROF(C, "bc_periodic_copy", k_periodic_copy<NC, T><<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, a0, a1, a2, 2, left_only));
 }
 
 // ------------------------------------------------------------------------
@@ -224,14 +261,15 @@ __global__ void k_scalar_ghosts(Grid g, double *v, int dir)
 // (les.c:2119-2514) with Compute_du_center (inline.h:3344-3418) and
 // Compute_du_dxyz (inline.h:3635-3663). Interior cells.
 // ------------------------------------------------------------------------
-__global__ void k_smagorinsky(Grid g, Metrics m, State s, Params p)
+template <class M>
+__global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
     auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
-    double ajc = m.aj[c];
-    R3<double> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
+    M ajc = m.aj[c];
+    R3<M> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
     R3<double> dc, de, dz;
     if (!g.pi && i == g.mx - 2) dc = U(k, j, i) - U(k, j, i - 1);
     else if (!g.pi && i == 1)   dc = U(k, j, i + 1) - U(k, j, i);
@@ -242,21 +280,23 @@ __global__ void k_smagorinsky(Grid g, Metrics m, State s, Params p)
     if (!g.pk && k == g.mz - 2) dz = U(k, j, i) - U(k - 1, j, i);
     else if (!g.pk && k == 1)   dz = U(k + 1, j, i) - U(k, j, i);
     else                        dz = 0.5 * (U(k + 1, j, i) - U(k - 1, j, i));
-    double du_dx = (dc.x * sc.x + de.x * e.x + dz.x * z.x) * ajc;
-    double du_dy = (dc.x * sc.y + de.x * e.y + dz.x * z.y) * ajc;
-    double du_dz = (dc.x * sc.z + de.x * e.z + dz.x * z.z) * ajc;
-    double dv_dx = (dc.y * sc.x + de.y * e.x + dz.y * z.x) * ajc;
-    double dv_dy = (dc.y * sc.y + de.y * e.y + dz.y * z.y) * ajc;
-    double dv_dz = (dc.y * sc.z + de.y * e.z + dz.y * z.z) * ajc;
-    double dw_dx = (dc.z * sc.x + de.z * e.x + dz.z * z.x) * ajc;
-    double dw_dy = (dc.z * sc.y + de.z * e.y + dz.z * z.y) * ajc;
-    double dw_dz = (dc.z * sc.z + de.z * e.z + dz.z * z.z) * ajc;
-    double S00 = 0.5 * (du_dx + du_dx), S01 = 0.5 * (du_dy + dv_dx), S02 = 0.5 * (du_dz + dw_dx);
-    double S10 = 0.5 * (dv_dx + du_dy), S11 = 0.5 * (dv_dy + dv_dy), S12 = 0.5 * (dv_dz + dw_dy);
-    double S20 = 0.5 * (dw_dx + du_dz), S21 = 0.5 * (dw_dy + dv_dz), S22 = 0.5 * (dw_dz + dw_dz);
-    double Sabs = sqrt(2.0 * (S00 * S00 + S01 * S01 + S02 * S02 + S10 * S10 + S11 * S11 + S12 * S12 + S20 * S20 + S21 * S21 + S22 * S22));
-    double filter = pow(1. / ajc, 1. / 3.);
-    s.nut[c] = p.cs * pow(filter, 2.0) * Sabs;
+    const R3<M> a = cvta<M>(dc), b = cvta<M>(de), d = cvta<M>(dz);
+    const M h = M(0.5);
+    M du_dx = (a.x * sc.x + b.x * e.x + d.x * z.x) * ajc;
+    M du_dy = (a.x * sc.y + b.x * e.y + d.x * z.y) * ajc;
+    M du_dz = (a.x * sc.z + b.x * e.z + d.x * z.z) * ajc;
+    M dv_dx = (a.y * sc.x + b.y * e.x + d.y * z.x) * ajc;
+    M dv_dy = (a.y * sc.y + b.y * e.y + d.y * z.y) * ajc;
+    M dv_dz = (a.y * sc.z + b.y * e.z + d.y * z.z) * ajc;
+    M dw_dx = (a.z * sc.x + b.z * e.x + d.z * z.x) * ajc;
+    M dw_dy = (a.z * sc.y + b.z * e.y + d.z * z.y) * ajc;
+    M dw_dz = (a.z * sc.z + b.z * e.z + d.z * z.z) * ajc;
+    M S00 = h * (du_dx + du_dx), S01 = h * (du_dy + dv_dx), S02 = h * (du_dz + dw_dx);
+    M S10 = h * (dv_dx + du_dy), S11 = h * (dv_dy + dv_dy), S12 = h * (dv_dz + dw_dy);
+    M S20 = h * (dw_dx + du_dz), S21 = h * (dw_dy + dv_dz), S22 = h * (dw_dz + dw_dz);
+    M Sabs = sqrt(M(2) * (S00 * S00 + S01 * S01 + S02 * S02 + S10 * S10 + S11 * S11 + S12 * S12 + S20 * S20 + S21 * S21 + S22 * S22));
+    M filter = pow(M(1) / ajc, M(1) / M(3));
+    s.nut[c] = (double)((M)p.cs * pow(filter, M(2)) * Sabs);
 }
 
 // UpdateNutBCs (boundary.c:2630-2930): face-adjacent ghosts of nut
@@ -387,20 +427,22 @@ __global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double
 // GradP (peqn.c:3437-3773): face pressure gradient with the metric tensor,
 // one-sided cross derivatives only at the corner faces. Interior cells.
 // ------------------------------------------------------------------------
-__global__ void k_grad_p(Grid g, Metrics m, State s)
+template <class M>
+__global__ void k_grad_p(Grid g, FaceMet<M> m, State s)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
     auto P = [&](int kk, int jj, int ii) { return s.p[g.id(kk, jj, ii)]; };
     const int mx = g.mx, my = g.my, mz = g.mz;
-    R3<double> ic = ld3(m.icsi, c), ie = ld3(m.ieta, c), iz = ld3(m.izet, c);
-    R3<double> jc = ld3(m.jcsi, c), je = ld3(m.jeta, c), jz = ld3(m.jzet, c);
-    R3<double> kc = ld3(m.kcsi, c), ke = ld3(m.keta, c), kz = ld3(m.kzet, c);
-    double g11 = dot3(ic, ic), g12 = dot3(ie, ic), g13 = dot3(iz, ic);
-    double g21 = dot3(jc, je), g22 = dot3(je, je), g23 = dot3(jz, je);
-    double g31 = dot3(kc, kz), g32 = dot3(ke, kz), g33 = dot3(kz, kz);
-    double dpdc, dpde, dpdz, ox, oy, oz;
+    R3<M> ic = ld3(m.icsi, c), ie = ld3(m.ieta, c), iz = ld3(m.izet, c);
+    R3<M> jc = ld3(m.jcsi, c), je = ld3(m.jeta, c), jz = ld3(m.jzet, c);
+    R3<M> kc = ld3(m.kcsi, c), ke = ld3(m.keta, c), kz = ld3(m.kzet, c);
+    M g11 = dot3(ic, ic), g12 = dot3(ie, ic), g13 = dot3(iz, ic);
+    M g21 = dot3(jc, je), g22 = dot3(je, je), g23 = dot3(jz, je);
+    M g31 = dot3(kc, kz), g32 = dot3(ke, kz), g33 = dot3(kz, kz);
+    double dpdc, dpde, dpdz;
+    M ox, oy, oz;
     dpdc = (i == mx - 2 && g.pi) ? P(k, j, mx + 1) - P(k, j, i) : P(k, j, i + 1) - P(k, j, i);
     if (j == my - 2 && i == mx - 2)  dpde = (P(k, j, i) - P(k, j - 1, i) + P(k, j, i + 1) - P(k, j - 1, i + 1)) * 0.5;
     else if (j == 1 && i == mx - 2)  dpde = (P(k, j + 1, i) - P(k, j, i) + P(k, j + 1, i + 1) - P(k, j, i + 1)) * 0.5;
@@ -408,7 +450,7 @@ __global__ void k_grad_p(Grid g, Metrics m, State s)
     if (k == mz - 2 && i == mx - 2)  dpdz = (P(k, j, i) - P(k - 1, j, i) + P(k, j, i + 1) - P(k - 1, j, i + 1)) * 0.5;
     else if (k == 1 && i == mx - 2)  dpdz = (P(k + 1, j, i) - P(k, j, i) + P(k + 1, j, i + 1) - P(k, j, i + 1)) * 0.5;
     else                             dpdz = (P(k + 1, j, i) - P(k - 1, j, i) + P(k + 1, j, i + 1) - P(k - 1, j, i + 1)) * 0.25;
-    ox = (dpdc * g11 + dpde * g12 + dpdz * g13) * m.iaj[c];
+    ox = ((M)dpdc * g11 + (M)dpde * g12 + (M)dpdz * g13) * m.iaj[c];
     if (i == mx - 2 && j == my - 2)  dpdc = (P(k, j, i) - P(k, j, i - 1) + P(k, j + 1, i) - P(k, j + 1, i - 1)) * 0.5;
     else if (i == 1 && j == my - 2)  dpdc = (P(k, j, i + 1) - P(k, j, i) + P(k, j + 1, i + 1) - P(k, j + 1, i)) * 0.5;
     else                             dpdc = (P(k, j, i + 1) - P(k, j, i - 1) + P(k, j + 1, i + 1) - P(k, j + 1, i - 1)) * 0.25;
@@ -416,7 +458,7 @@ __global__ void k_grad_p(Grid g, Metrics m, State s)
     if (k == mz - 2 && j == my - 2)  dpdz = (P(k, j, i) - P(k - 1, j, i) + P(k, j + 1, i) - P(k - 1, j + 1, i)) * 0.5;
     else if (k == 1 && j == my - 2)  dpdz = (P(k + 1, j, i) - P(k, j, i) + P(k + 1, j + 1, i) - P(k, j + 1, i)) * 0.5;
     else                             dpdz = (P(k + 1, j, i) - P(k - 1, j, i) + P(k + 1, j + 1, i) - P(k - 1, j + 1, i)) * 0.25;
-    oy = (dpdc * g21 + dpde * g22 + dpdz * g23) * m.jaj[c];
+    oy = ((M)dpdc * g21 + (M)dpde * g22 + (M)dpdz * g23) * m.jaj[c];
     if (i == mx - 2 && k == mz - 2)  dpdc = (P(k, j, i) - P(k, j, i - 1) + P(k + 1, j, i) - P(k + 1, j, i - 1)) * 0.5;
     else if (i == 1 && k == mz - 2)  dpdc = (P(k, j, i + 1) - P(k, j, i) + P(k + 1, j, i + 1) - P(k + 1, j, i)) * 0.5;
     else                             dpdc = (P(k, j, i + 1) - P(k, j, i - 1) + P(k + 1, j, i + 1) - P(k + 1, j, i - 1)) * 0.25;
@@ -424,11 +466,11 @@ __global__ void k_grad_p(Grid g, Metrics m, State s)
     else if (j == 1 && k == mz - 2)  dpde = (P(k, j + 1, i) - P(k, j, i) + P(k + 1, j + 1, i) - P(k + 1, j, i)) * 0.5;
     else                             dpde = (P(k, j + 1, i) - P(k, j - 1, i) + P(k + 1, j + 1, i) - P(k + 1, j - 1, i)) * 0.25;
     dpdz = (k == mz - 2 && g.pk) ? P(mz + 1, j, i) - P(k, j, i) : P(k + 1, j, i) - P(k, j, i);
-    oz = (dpdc * g31 + dpde * g32 + dpdz * g33) * m.kaj[c];
+    oz = ((M)dpdc * g31 + (M)dpde * g32 + (M)dpdz * g33) * m.kaj[c];
     if (!g.pi && i == mx - 2) ox = 0;
     if (!g.pj && j == my - 2) oy = 0;
     if (!g.pk && k == mz - 2) oz = 0;
-    s.dp.x[c] = ox; s.dp.y[c] = oy; s.dp.z[c] = oz;
+    s.dp.x[c] = (double)ox; s.dp.y[c] = (double)oy; s.dp.z[c] = (double)oz;
 }
 
 // ------------------------------------------------------------------------
@@ -473,25 +515,29 @@ __device__ __forceinline__ R3<double> quick(R3<double> f0, R3<double> f1, R3<dou
 }
 
 // viscous flux (g . grad u + R . n) * ajc * nuEff, ueqn_solvers.c:180-216, 392-394
-__device__ __forceinline__ R3<double> visc_flux(R3<double> s0, R3<double> s1, R3<double> s2, int dir,
-                                                R3<double> dc, R3<double> de, R3<double> dz, double ajc, double nuEff)
+template <class M>
+__device__ __forceinline__ R3<M> visc_flux(R3<M> s0, R3<M> s1, R3<M> s2, int dir, R3<M> dc, R3<M> de, R3<M> dz, M ajc, M nuEff)
 {
-    double csi0 = s0.x, csi1 = s0.y, csi2 = s0.z, eta0 = s1.x, eta1 = s1.y, eta2 = s1.z, zet0 = s2.x, zet1 = s2.y, zet2 = s2.z;
-    double g11, g21, g31, n0, n1, n2;
+    M csi0 = s0.x, csi1 = s0.y, csi2 = s0.z, eta0 = s1.x, eta1 = s1.y, eta2 = s1.z, zet0 = s2.x, zet1 = s2.y, zet2 = s2.z;
+    M g11, g21, g31, n0, n1, n2;
     if (dir == 0) { g11 = csi0 * csi0 + csi1 * csi1 + csi2 * csi2; g21 = eta0 * csi0 + eta1 * csi1 + eta2 * csi2; g31 = zet0 * csi0 + zet1 * csi1 + zet2 * csi2; n0 = csi0; n1 = csi1; n2 = csi2; }
     else if (dir == 1) { g11 = csi0 * eta0 + csi1 * eta1 + csi2 * eta2; g21 = eta0 * eta0 + eta1 * eta1 + eta2 * eta2; g31 = zet0 * eta0 + zet1 * eta1 + zet2 * eta2; n0 = eta0; n1 = eta1; n2 = eta2; }
     else { g11 = csi0 * zet0 + csi1 * zet1 + csi2 * zet2; g21 = eta0 * zet0 + eta1 * zet1 + eta2 * zet2; g31 = zet0 * zet0 + zet1 * zet1 + zet2 * zet2; n0 = zet0; n1 = zet1; n2 = zet2; }
-    double r11 = dc.x * csi0 + de.x * eta0 + dz.x * zet0, r21 = dc.y * csi0 + de.y * eta0 + dz.y * zet0, r31 = dc.z * csi0 + de.z * eta0 + dz.z * zet0;
-    double r12 = dc.x * csi1 + de.x * eta1 + dz.x * zet1, r22 = dc.y * csi1 + de.y * eta1 + dz.y * zet1, r32 = dc.z * csi1 + de.z * eta1 + dz.z * zet1;
-    double r13 = dc.x * csi2 + de.x * eta2 + dz.x * zet2, r23 = dc.y * csi2 + de.y * eta2 + dz.y * zet2, r33 = dc.z * csi2 + de.z * eta2 + dz.z * zet2;
-    R3<double> v;
+    M r11 = dc.x * csi0 + de.x * eta0 + dz.x * zet0, r21 = dc.y * csi0 + de.y * eta0 + dz.y * zet0, r31 = dc.z * csi0 + de.z * eta0 + dz.z * zet0;
+    M r12 = dc.x * csi1 + de.x * eta1 + dz.x * zet1, r22 = dc.y * csi1 + de.y * eta1 + dz.y * zet1, r32 = dc.z * csi1 + de.z * eta1 + dz.z * zet1;
+    M r13 = dc.x * csi2 + de.x * eta2 + dz.x * zet2, r23 = dc.y * csi2 + de.y * eta2 + dz.y * zet2, r33 = dc.z * csi2 + de.z * eta2 + dz.z * zet2;
+    R3<M> v;
     v.x = (g11 * dc.x + g21 * de.x + g31 * dz.x + r11 * n0 + r21 * n1 + r31 * n2) * ajc * (nuEff);
     v.y = (g11 * dc.y + g21 * de.y + g31 * dz.y + r12 * n0 + r22 * n1 + r32 * n2) * ajc * (nuEff);
     v.z = (g11 * dc.z + g21 * de.z + g31 * dz.z + r13 * n0 + r23 * n1 + r33 * n2) * ajc * (nuEff);
     return v;
 }
 
-__global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
+// M: storage and arithmetic type of the metrics in the viscous flux; F: storage
+// type of the face fluxes. The convective flux is formed in FP64 from the FP64
+// Ucont and Ucat.
+template <class M, class F>
+__global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, State s, FluxWork<F> w, Params p)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -503,7 +549,7 @@ __global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
     auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
     auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
     // ---- i faces, ueqn_solvers.c:173-395 with Compute_du_i (inline.h:2748-2807)
-    if (j != 0 && k != 0) {
+    if (j != 0 && k != 0 && !(g.pi && i == 0)) {
         R3<double> dc = U(k, j, i + 1) - U(k, j, i), de, dz;
         bool edge = (i == 0 || i == mx - 2);
         if (j == my - 2 && edge && (npj || npi))      de = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
@@ -524,17 +570,17 @@ __global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
             } else { iL = i - 1; iR = i + 2; }
             dv = (-uc) * quick(U(k, j, iL), U(k, j, i), U(k, j, i + 1), U(k, j, iR), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j, i + 1)));
-        double nuEff;
+        M nuEff;
         if (p.les) {
             double nt = 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1));
-            if ((p.bc[TG_ILEFT] == TG_BC_SLIP && i == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && i == mx - 2)) nuEff = 0.0;
-            else nuEff = nu + nt;
-        } else nuEff = nu;
-        R3<double> v = visc_flux(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, dc, de, dz, m.iaj[f], nuEff);
-        st3(s.f1, f, dv + v);
+            if ((p.bc[TG_ILEFT] == TG_BC_SLIP && i == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && i == mx - 2)) nuEff = M(0);
+            else nuEff = (M)(nu + nt);
+        } else nuEff = (M)nu;
+        R3<M> v = visc_flux<M>(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff);
+        st3(w.f1, f, cvta<F>(dv + cvta<double>(v)));
     }
     // ---- j faces, ueqn_solvers.c:397-602 with Compute_du_j (inline.h:2809-2869)
-    if (i != 0 && k != 0) {
+    if (i != 0 && k != 0 && !(g.pj && j == 0)) {
         R3<double> dc, de = U(k, j + 1, i) - U(k, j, i), dz;
         bool edge = (j == 0 || j == my - 2);
         if (i == mx - 2 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k, j + 1, i - 1) - U(k, j, i - 1));
@@ -555,7 +601,7 @@ __global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
             } else { jL = j - 1; jR = j + 2; }
             dv = (-uc) * quick(U(k, jL, i), U(k, j, i), U(k, j + 1, i), U(k, jR, i), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j + 1, i)));
-        double nuEff;
+        M nuEff;
         R3<double> base{0, 0, 0};
         if (p.les) {
             double nt = 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i));
@@ -563,15 +609,15 @@ __global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
             if ((p.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN && j == my - 2)) {
                 int w = k * mx + i;
                 base = R3<double>{-s.twx[w], -s.twy[w], -s.twz[w]};
-                nuEff = nu;
-            } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = 0.0;
-            else nuEff = nu + nt;
-        } else nuEff = nu;
-        R3<double> v = visc_flux(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, dc, de, dz, m.jaj[f], nuEff);
-        st3(s.f2, f, dv + (base + v));
+                nuEff = (M)nu;
+            } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = M(0);
+            else nuEff = (M)(nu + nt);
+        } else nuEff = (M)nu;
+        R3<M> v = visc_flux<M>(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff);
+        st3(w.f2, f, cvta<F>(dv + (base + cvta<double>(v))));
     }
     // ---- k faces, ueqn_solvers.c:604-778 with Compute_du_k (inline.h:2871-2931)
-    if (i != 0 && j != 0) {
+    if (i != 0 && j != 0 && !(g.pk && k == 0)) {
         R3<double> dc, de, dz = U(k + 1, j, i) - U(k, j, i);
         bool edge = (k == 0 || k == mz - 2);
         if (i == mx - 2 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j, i - 1) - U(k, j, i - 1));
@@ -592,45 +638,46 @@ __global__ void k_face_fluxes(Grid g, Metrics m, State s, Params p)
             } else { kL = k - 1; kR = k + 2; }
             dv = (-uc) * quick(U(kL, j, i), U(k, j, i), U(k + 1, j, i), U(kR, j, i), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k + 1, j, i)));
-        double nuEff;
+        M nuEff;
         if (p.les) {
             double nt = 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i));
-            if ((p.bc[TG_KLEFT] == TG_BC_SLIP && k == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && k == mz - 2)) nuEff = 0.0;
-            else nuEff = nu + nt;
-        } else nuEff = nu;
-        R3<double> v = visc_flux(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, dc, de, dz, m.kaj[f], nuEff);
-        st3(s.f3, f, dv + v);
+            if ((p.bc[TG_KLEFT] == TG_BC_SLIP && k == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && k == mz - 2)) nuEff = M(0);
+            else nuEff = (M)(nu + nt);
+        } else nuEff = (M)nu;
+        R3<M> v = visc_flux<M>(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff);
+        st3(w.f3, f, cvta<F>(dv + cvta<double>(v)));
     }
 }
 
-// Pass 2 (ueqn_solvers.c:825-990): cell divergence of the face fluxes, copied
-// to the ghost cell at non-periodic boundaries.
-__global__ void k_cell_fp(Grid g, State s)
+// Pass 2 (ueqn_solvers.c:825-947): divergence of the face fluxes of interior
+// cell (k, j, i). A periodic direction reads its face 0 from face m-2
+// (resetFacePeriodicFluxesVector, inline.h:5357-5451, applied to the fluxes).
+template <class M>
+__device__ __forceinline__ R3<M> cell_fp(const Grid &g, const FluxWork<M> &w, int k, int j, int i)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
-    int c = g.lin(k, j, i);
-    int iw = c - 1, js = c - g.mx, kb = c - g.mx * g.my;
-    R3<double> F;
-    F.x = s.f1.x[c] - s.f1.x[iw] + s.f2.x[c] - s.f2.x[js] + s.f3.x[c] - s.f3.x[kb];
-    F.y = s.f1.y[c] - s.f1.y[iw] + s.f2.y[c] - s.f2.y[js] + s.f3.y[c] - s.f3.y[kb];
-    F.z = s.f1.z[c] - s.f1.z[iw] + s.f2.z[c] - s.f2.z[js] + s.f3.z[c] - s.f3.z[kb];
-    st3(s.fp, c, F);
-    if (i == 1 && !g.pi)        st3(s.fp, c - 1, F);
-    if (j == 1 && !g.pj)        st3(s.fp, c - g.mx, F);
-    if (k == 1 && !g.pk)        st3(s.fp, c - g.mx * g.my, F);
-    if (i == g.mx - 2 && !g.pi) st3(s.fp, c + 1, F);
-    if (j == g.my - 2 && !g.pj) st3(s.fp, c + g.mx, F);
-    if (k == g.mz - 2 && !g.pk) st3(s.fp, c + g.mx * g.my, F);
+    const int c = g.lin(k, j, i), pl = g.mx * g.my;
+    const int iw = (i == 1 && g.pi) ? c + g.mx - 3 : c - 1;
+    const int js = (j == 1 && g.pj) ? c + (g.my - 3) * g.mx : c - g.mx;
+    const int kb = (k == 1 && g.pk) ? c + (g.mz - 3) * pl : c - pl;
+    R3<M> F;
+    F.x = w.f1.x[c] - w.f1.x[iw] + w.f2.x[c] - w.f2.x[js] + w.f3.x[c] - w.f3.x[kb];
+    F.y = w.f1.y[c] - w.f1.y[iw] + w.f2.y[c] - w.f2.y[js] + w.f3.y[c] - w.f3.y[kb];
+    F.z = w.f1.z[c] - w.f1.z[iw] + w.f2.z[c] - w.f2.z[js] + w.f3.z[c] - w.f3.z[kb];
+    return F;
 }
 
 // Pass 3 (ueqn_solvers.c:1008-1035): rhs_face += scale * aj_face *
-// central(S . fp) at the faces of interior cells. With `fused` the kernel also
-// forms the rest of ExplicitRhsU at these faces in the reference's order:
+// central(S . fp) at the faces of interior cells, with fp formed here from
+// the face fluxes (pass 2) for the cell and its +i, +j, +k neighbours. The
+// neighbour beyond the last interior cell is the ghost cell, which holds the
+// opposite first interior cell (periodic, resetCellPeriodicFluxes) or a copy
+// of this cell (ueqn_solvers.c:949-990). With `fused` the kernel also forms
+// the rest of ExplicitRhsU at these faces in the reference's order:
 // Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += FormU, +=
-// meanGradPForcing (ueqn_sources.c:3735-3822).
-template <bool fused>
-__global__ void k_rhs_faces(Grid g, Metrics m, State s, V3f<double> R, double scale, Params p, int ab2)
+// meanGradPForcing (ueqn_sources.c:3735-3822). MR: metric storage type; F:
+// face-flux storage type.
+template <class MR, class F, bool fused>
+__global__ void __launch_bounds__(256, 3) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -651,22 +698,32 @@ __global__ void k_rhs_faces(Grid g, Metrics m, State s, V3f<double> R, double sc
     } else {
         base = ld3(R, c);
     }
-    R3<double> fpc = ld3(s.fp, c);
-    double v1, v2, ox, oy, oz;
-    { R3<double> a = ld3(m.csi, c), b = ld3(m.csi, c + 1); R3<double> fb = ld3(s.fp, c + 1);
+    // arithmetic in FP32 only when both the metrics and the fluxes are FP32
+    using M = typename std::conditional<std::is_same<MR, float>::value && std::is_same<F, float>::value, float, double>::type;
+    auto FP = [&](int kk, int jj, int ii) { return cvta<M>(cell_fp(g, w, kk, jj, ii)); };
+    auto MT = [&](const V3f<MR> &v, int q) { return cvta<M>(ld3(v, q)); };
+    const R3<M> fpc = FP(k, j, i);
+    const M sc = (M)scale, h = M(0.5);
+    M v1, v2;
+    double ox, oy, oz;
+    { R3<M> fb = i < g.mx - 2 ? FP(k, j, i + 1) : (g.pi ? FP(k, j, 1) : fpc);
+      R3<M> a = MT(m.csi, c), b = MT(m.csi, c + 1);
       v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      ox = base.x + scale * m.iaj[c] * (0.5 * (v1 + v2)); }
-    { int n = c + g.mx; R3<double> a = ld3(m.eta, c), b = ld3(m.eta, n); R3<double> fb = ld3(s.fp, n);
+      ox = base.x + (double)(sc * (M)m.iaj[c] * (h * (v1 + v2))); }
+    { R3<M> fb = j < g.my - 2 ? FP(k, j + 1, i) : (g.pj ? FP(k, 1, i) : fpc);
+      int n = c + g.mx; R3<M> a = MT(m.eta, c), b = MT(m.eta, n);
       v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      oy = base.y + scale * m.jaj[c] * (0.5 * (v1 + v2)); }
-    { int n = c + g.mx * g.my; R3<double> a = ld3(m.zet, c), b = ld3(m.zet, n); R3<double> fb = ld3(s.fp, n);
+      oy = base.y + (double)(sc * (M)m.jaj[c] * (h * (v1 + v2))); }
+    { R3<M> fb = k < g.mz - 2 ? FP(k + 1, j, i) : (g.pk ? FP(1, j, i) : fpc);
+      int n = c + g.mx * g.my; R3<M> a = MT(m.zet, c), b = MT(m.zet, n);
       v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
-      oz = base.z + scale * m.kaj[c] * (0.5 * (v1 + v2)); }
+      oz = base.z + (double)(sc * (M)m.kaj[c] * (h * (v1 + v2))); }
     if (fused && p.mean_grad_p) {
-        R3<double> a = ld3(m.icsi, c), b = ld3(m.jeta, c), d = ld3(m.kzet, c);
-        ox += 1.0 * (p.mgp[0] * a.x + p.mgp[1] * a.y + p.mgp[2] * a.z);
-        oy += 1.0 * (p.mgp[0] * b.x + p.mgp[1] * b.y + p.mgp[2] * b.z);
-        oz += 1.0 * (p.mgp[0] * d.x + p.mgp[1] * d.y + p.mgp[2] * d.z);
+        R3<M> a = MT(m.icsi, c), b = MT(m.jeta, c), d = MT(m.kzet, c);
+        const M g0 = (M)p.mgp[0], g1 = (M)p.mgp[1], g2 = (M)p.mgp[2];
+        ox += (double)(g0 * a.x + g1 * a.y + g2 * a.z);
+        oy += (double)(g0 * b.x + g1 * b.y + g2 * b.z);
+        oz += (double)(g0 * d.x + g1 * d.y + g2 * d.z);
     }
     R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
 }
@@ -689,25 +746,11 @@ __global__ void k_non_resolved(Grid g, State s, int dir)
     if (!per) { int q = at(m - 2); if (!(uo[q] > 0)) v[q] = 0.0; }
 }
 
-// elementwise: y = a*x + z (component-wise over all points)
-__global__ void k_waxpy3(int64_t n, V3f<double> y, double a, V3f<double> x, V3f<double> z)
-{
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        y.x[q] = a * x.x[q] + z.x[q]; y.y[q] = a * x.y[q] + z.y[q]; y.z[q] = a * x.z[q] + z.z[q];
-    }
-}
 // FE: y = x*dt + z (VecScale then VecAXPY)
 __global__ void k_fe_update(int64_t n, V3f<double> y, double dt, V3f<double> x, V3f<double> z)
 {
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         y.x[q] = x.x[q] * dt + z.x[q]; y.y[q] = x.y[q] * dt + z.y[q]; y.z[q] = x.z[q] * dt + z.z[q];
-    }
-}
-// y += a*x
-__global__ void k_axpy3(int64_t n, V3f<double> y, double a, V3f<double> x)
-{
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        y.x[q] = y.x[q] + a * x.x[q]; y.y[q] = y.y[q] + a * x.y[q]; y.z[q] = y.z[q] + a * x.z[q];
     }
 }
 
@@ -851,10 +894,83 @@ inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 *
 }  // namespace
 
 // ============================================================================ host wrappers
-void contra_to_cart(tg_ctx *C) { k_contra_to_cart<<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s); }
-void reset_cell_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3>(C, v.x, v.y, v.z, 0); }
-void reset_cell_periodic_s(tg_ctx *C, double *v) { periodic_copy<1>(C, v, nullptr, nullptr, 0); }
-void reset_face_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3>(C, v.x, v.y, v.z, 1); }
+void contra_to_cart(tg_ctx *C) { k_contra_to_cart<double, double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s); }
+
+// contravariantToCartesian inside the momentum stages, at the precision the
+// context's policy gives it
+static void contra_to_cart_stage(tg_ctx *C)
+{
+    const dim3 gr = gi(C->g);
+    if (C->pol.contra_a32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<float, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
+    else if (C->pol.contra_m32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
+    else TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, double><<<gr, block3(), 0, C->stream>>>(C->g, C->fm64, C->s));
+}
+
+// Precision of each momentum stage in the mixed mode. Every momentum stencil
+// reads the FP32 metric copies (half the metric bytes, which dominate the
+// stencils' traffic). Two things stay FP64 because the pressure field is set by
+// the divergence of the momentum right-hand side, in which the convective
+// fluxes nearly cancel: the arithmetic of contravariantToCartesian, FormU's
+// convective fluxes and the face assembly, and the storage of the face-flux
+// planes. Measured against the FP64 oracle (ABL 48x48x32, 20 steps) FP32
+// storage of the face fluxes alone raised the relative L2 error of p from
+// 1.3e-7 to 4.9e-6; FP32 Cramer arithmetic raised it to 6e-7 in 5 steps.
+static void set_policy(tg_ctx *C)
+{
+    C->pol.contra_m32 = C->mixed;
+    C->pol.contra_a32 = false;
+    C->pol.visc32 = C->mixed;
+    C->pol.flux32 = false;
+    C->pol.rhs32 = C->mixed;
+    C->pol.smag32 = C->mixed;
+    C->pol.gradp32 = C->mixed;
+}
+
+void alloc_precision_work(tg_ctx *C)
+{
+    const size_t G = (size_t)C->g.size();
+    const Metrics &m = C->m;
+    C->fm64 = FaceMet<double>{m.csi, m.eta, m.zet, m.icsi, m.ieta, m.izet, m.jcsi, m.jeta, m.jzet,
+                              m.kcsi, m.keta, m.kzet, m.aj, m.iaj, m.jaj, m.kaj};
+    set_policy(C);
+    if (!C->pol.flux32) C->fw64 = FluxWork<double>{dalloc3(C, G), dalloc3(C, G), dalloc3(C, G), dalloc3(C, G)};
+    if (!C->mixed) return;
+    auto f3 = [&]() {
+        float *a = (float *)dalloc(C, 3 * G * sizeof(float));
+        return V3f<float>{a, a + G, a + 2 * G};
+    };
+    FaceMet<float> &f = C->fm32;
+    V3f<float> *vv[] = {&f.csi, &f.eta, &f.zet, &f.icsi, &f.ieta, &f.izet, &f.jcsi, &f.jeta, &f.jzet, &f.kcsi, &f.keta, &f.kzet};
+    for (auto *v : vv) *v = f3();
+    float **ss[] = {&f.aj, &f.iaj, &f.jaj, &f.kaj};
+    for (auto **v : ss) *v = (float *)dalloc(C, G * sizeof(float));
+    if (C->pol.flux32) C->fw32 = FluxWork<float>{f3(), f3(), f3(), f3()};
+    C->met32_stale = true;
+}
+
+void refresh_met32(tg_ctx *C)
+{
+    if (!C->mixed || !C->met32_stale) return;
+    const int64_t G = C->g.size();
+    const FaceMet<double> &a = C->fm64;
+    const FaceMet<float> &b = C->fm32;
+    const V3f<double> va[] = {a.csi, a.eta, a.zet, a.icsi, a.ieta, a.izet, a.jcsi, a.jeta, a.jzet, a.kcsi, a.keta, a.kzet};
+    const V3f<float> vb[] = {b.csi, b.eta, b.zet, b.icsi, b.ieta, b.izet, b.jcsi, b.jeta, b.jzet, b.kcsi, b.keta, b.kzet};
+    for (int q = 0; q < 12; q++) {
+        k_to_f32<<<nblk(G), 256, 0, C->stream>>>(G, va[q].x, vb[q].x);
+        k_to_f32<<<nblk(G), 256, 0, C->stream>>>(G, va[q].y, vb[q].y);
+        k_to_f32<<<nblk(G), 256, 0, C->stream>>>(G, va[q].z, vb[q].z);
+    }
+    const double *sa[] = {a.aj, a.iaj, a.jaj, a.kaj};
+    float *sb[] = {b.aj, b.iaj, b.jaj, b.kaj};
+    for (int q = 0; q < 4; q++) k_to_f32<<<nblk(G), 256, 0, C->stream>>>(G, sa[q], sb[q]);
+    TG_CUDA(cudaGetLastError());
+    C->met32_stale = false;
+}
+
+void reset_cell_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3, double>(C, v.x, v.y, v.z, 0); }
+void reset_cell_periodic_s(tg_ctx *C, double *v) { periodic_copy<1, double>(C, v, nullptr, nullptr, 0); }
+void reset_face_periodic(tg_ctx *C, V3f<double> v) { periodic_copy<3, double>(C, v.x, v.y, v.z, 1); }
 
 void reset_no_penetration(tg_ctx *C)
 {
@@ -899,7 +1015,9 @@ void update_nut(tg_ctx *C)
 {
     const Grid g = C->g;
     TG_CUDA(cudaMemsetAsync(C->s.nut, 0, sizeof(double) * g.size(), C->stream));
-    TG_PROF(C, "smagorinsky", k_smagorinsky<<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm));
+    refresh_met32(C);
+    if (C->pol.smag32) TG_PROF(C, "smagorinsky", k_smagorinsky<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fm32, C->s, C->prm));
+    else TG_PROF(C, "smagorinsky", k_smagorinsky<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fm64, C->s, C->prm));
     int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
     dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
     TG_PROF(C, "bc_nut", k_nut_bcs<<<grid, b2, 0, C->stream>>>(g, C->s, C->prm));
@@ -921,33 +1039,52 @@ void update_wall_models(tg_ctx *C)
     TG_PROF(C, "wall_stress", k_wall_stress<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_scal + 8, aN / (aN + 1.0), 1.0 / (aN + 1.0)));
 }
 
+// GradP writes the faces of interior cells; dP is zero elsewhere from its
+// allocation unless a caller wrote it
 void grad_p(tg_ctx *C)
 {
-    TG_CUDA(cudaMemsetAsync(C->s.dp.x, 0, 3 * sizeof(double) * C->g.size(), C->stream));
-    TG_PROF(C, "grad_p", k_grad_p<<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s));
+    if (C->clear_dp) {
+        TG_CUDA(cudaMemsetAsync(C->s.dp.x, 0, 3 * sizeof(double) * C->g.size(), C->stream));
+        C->clear_dp = false;
+    }
+    refresh_met32(C);
+    if (C->pol.gradp32) TG_PROF(C, "grad_p", k_grad_p<float><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
+    else TG_PROF(C, "grad_p", k_grad_p<double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s));
 }
 
 void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
 
-// FormU passes 1-2 (face fluxes, cell divergence with ghost handling)
-static void form_u_fp(tg_ctx *C)
+// FormU pass 1 (face fluxes) at the precision of the context's policy.
+// Passes 2-3 run inside k_rhs_faces; the flux planes are only read at the
+// points this pass writes.
+static void form_u_faces(tg_ctx *C)
 {
     const Grid g = C->g;
-    const size_t G = (size_t)g.size();
-    TG_CUDA(cudaMemsetAsync(C->s.f1.x, 0, 12 * sizeof(double) * G, C->stream));
-    TG_PROF(C, "formu_face_fluxes", k_face_fluxes<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm));
-    reset_face_periodic(C, C->s.f1);
-    reset_face_periodic(C, C->s.f2);
-    reset_face_periodic(C, C->s.f3);
-    TG_PROF(C, "formu_cell_fp", k_cell_fp<<<gi(g), block3(), 0, C->stream>>>(g, C->s));
-    reset_cell_periodic(C, C->s.fp);
+    refresh_met32(C);
+    const dim3 gr = gf(g);
+    const auto &P = C->pol;
+    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<float, float><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm));
+    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<float, double><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm));
+    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, float><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm));
+    else TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, double><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm));
+}
+
+template <bool fused>
+static void rhs_faces(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
+{
+    const Grid g = C->g;
+    const dim3 gr = gi(g);
+    const auto &P = C->pol;
+    if (P.rhs32 && P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, float, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, rhs, scale, C->prm, ab2));
+    else if (P.rhs32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, double, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, rhs, scale, C->prm, ab2));
+    else if (P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, float, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, rhs, scale, C->prm, ab2));
+    else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2));
 }
 
 void form_u(tg_ctx *C, V3f<double> rhs, double scale)
 {
-    const Grid g = C->g;
-    form_u_fp(C);
-    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<false><<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, rhs, scale, C->prm, 0));
+    form_u_faces(C);
+    rhs_faces<false>(C, rhs, scale, 0);
 }
 
 void explicit_rhs(tg_ctx *C)
@@ -955,19 +1092,45 @@ void explicit_rhs(tg_ctx *C)
     const Grid g = C->g;
     reset_no_penetration(C);
     reset_face_periodic(C, C->s.ucont);
-    contra_to_cart(C);
+    contra_to_cart_stage(C);
     reset_cell_periodic(C, C->s.ucat);
-    form_u_fp(C);
-    // every point outside the interior faces keeps Rhs = -dP + b = 0
-    TG_CUDA(cudaMemsetAsync(C->s.rhs.x, 0, 3 * sizeof(double) * g.size(), C->stream));
-    TG_PROF(C, "formu_rhs_faces", k_rhs_faces<true><<<gi(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->s.rhs, 1.0, C->prm,
-                                                                                    C->it > C->cfg.it_start ? 1 : 0));
+    form_u_faces(C);
+    // every point outside the interior faces keeps Rhs = -dP + b = 0: zero from
+    // the allocation, rewritten here only after a caller wrote Rhs
+    if (C->clear_rhs) {
+        TG_CUDA(cudaMemsetAsync(C->s.rhs.x, 0, 3 * sizeof(double) * g.size(), C->stream));
+        C->clear_rhs = false;
+    }
+    rhs_faces<true>(C, C->s.rhs, 1.0, C->it > C->cfg.it_start ? 1 : 0);
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, 0));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, 1));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
 }
 
-void solve_u(tg_ctx *C)
+// UeqnRK4 bookkeeping after stage st (ueqn_solvers.c:1446-1504): the stage
+// sum Utmp += dt b_st Rhs (Utmp starts as Ucont_o) and the next stage's state
+// Ucont = Ucont_o + a_{st+1} dt Rhs, or after the last stage Ucont = Utmp.
+__global__ void k_rk_update(int64_t n, V3f<double> utmp, V3f<double> ucont, V3f<double> ucont_o, V3f<double> rhs,
+                            double cb, double ca, int first, int last)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const double rx = rhs.x[q], ry = rhs.y[q], rz = rhs.z[q];
+        if (last) {
+            ucont.x[q] = cb * rx + utmp.x[q]; ucont.y[q] = cb * ry + utmp.y[q]; ucont.z[q] = cb * rz + utmp.z[q];
+            continue;
+        }
+        const double ox = ucont_o.x[q], oy = ucont_o.y[q], oz = ucont_o.z[q];
+        if (first) { utmp.x[q] = cb * rx + ox; utmp.y[q] = cb * ry + oy; utmp.z[q] = cb * rz + oz; }
+        else { utmp.x[q] = utmp.x[q] + cb * rx; utmp.y[q] = utmp.y[q] + cb * ry; utmp.z[q] = utmp.z[q] + cb * rz; }
+        ucont.x[q] = ca * rx + ox; ucont.y[q] = ca * ry + oy; ucont.z[q] = ca * rz + oz;
+    }
+}
+
+// SolveUEqn (ueqn.c:397-440). cart_tail: finish with contravariantToCartesian
+// on every interior cell as the reference does; the full step converts only
+// the boundary shell, which gives the same Ucat at the end of the step because
+// the projection is followed by its own conversion.
+static void solve_u_impl(tg_ctx *C, bool cart_tail)
 {
     const int64_t G = C->g.size();
     const double dt = C->prm.dt;
@@ -979,20 +1142,30 @@ void solve_u(tg_ctx *C)
         // UeqnRK4, ueqn_solvers.c:1446-1504
         const double b[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
         const double a[4] = {0.0, 0.5, 0.5, 1.0};
-        TG_CUDA(cudaMemcpyAsync(C->s.utmp.x, C->s.ucont_o.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         for (int st = 0; st < 4; st++) {
-            if (st != 0) TG_PROF(C, "rk_stage", k_waxpy3<<<nblk(G), 256, 0, C->stream>>>(G, C->s.ucont, a[st] * dt, C->s.rhs, C->s.ucont_o));
             explicit_rhs(C);
-            TG_PROF(C, "rk_accumulate", k_axpy3<<<nblk(G), 256, 0, C->stream>>>(G, C->s.utmp, dt * b[st], C->s.rhs));
+            TG_PROF(C, "rk_update", k_rk_update<<<nblk(G), 256, 0, C->stream>>>(G, C->s.utmp, C->s.ucont, C->s.ucont_o, C->s.rhs,
+                                                                              dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0, st == 3));
         }
-        TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, C->s.utmp.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
     }
     // SolveUEqn tail, ueqn.c:413-437
     reset_no_penetration(C);
     reset_face_periodic(C, C->s.ucont);
-    contra_to_cart(C);
+    if (cart_tail) {
+        contra_to_cart(C);
+    } else {
+        // the full step converts again after the projection, which rewrites
+        // every interior cell and the face ghosts; only the edge and corner
+        // ghosts keep what the periodic copies below bring from the shell
+        const Grid g = C->g;
+        int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
+        dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
+        TG_PROF(C, "contra_to_cart_shell", k_contra_to_cart_shell<<<grid, b2, 0, C->stream>>>(g, C->fm64, C->s));
+    }
     reset_cell_periodic(C, C->s.ucat);
 }
+
+void solve_u(tg_ctx *C) { solve_u_impl(C, true); }
 
 // SolvePEqn (peqn.c:3777-3971) after the Poisson solve: phi ghosts, pressure
 // update and ghosts, projection
@@ -1055,7 +1228,7 @@ int step(tg_ctx *C, tg_stats *st)
             TG_CUDA(cudaMemcpyAsync(C->s.btheta_o.x, C->s.btheta.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         buoyancy(C);
     }
-    solve_u(C);
+    solve_u_impl(C, false);
     int rc = solve_p(C, st);
     contra_to_cart(C);
     reduce_max_abs_div(C, C->d_scal + 16);
