@@ -285,24 +285,26 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
     }
 }
 
-// chunk length (power of two >= ceil(ny / NW)) of the line solver; 0 if too long
-inline int line_cj(int ny)
+template <class T>
+size_t line_chunk_smem_cj(int cj) { return sizeof(T) * (2 * (size_t)LINE_NW * cj * 32 + 3 * LINE_NW * 32); }
+
+// chunk length (power of two >= ceil(ny / NW)) of the line solver; 0 if the
+// lines are too long for its shared memory
+template <class T>
+int line_cj(int ny)
 {
     int need = (ny + LINE_NW - 1) / LINE_NW;
     int cj = 1;
     while (cj < need) cj <<= 1;
-    return cj <= 32 ? cj : 0;
+    return (cj <= 32 && line_chunk_smem_cj<T>(cj) <= 200 * 1024) ? cj : 0;
 }
-
-template <class T>
-size_t line_chunk_smem_cj(int cj) { return sizeof(T) * (2 * (size_t)LINE_NW * cj * 32 + 3 * LINE_NW * 32); }
 
 template <class T>
 void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
 {
     const int lines = (F.nx >> 1) * F.nz;
     const int nb = (lines + 31) / 32;
-    const int cj = line_cj(F.ny);
+    const int cj = line_cj<T>(F.ny);
     const size_t shm = line_chunk_smem_cj<T>(cj);
     switch (cj) {
     case 1: k_line_chunked<T, 1><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
@@ -317,8 +319,16 @@ void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
 template <class T>
 void set_line_smem_attrs()
 {
-    TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_chunk_smem_cj<T>(16)));
-    TG_CUDA(cudaFuncSetAttribute(k_line_chunked<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)line_chunk_smem_cj<T>(32)));
+    auto set = [](const void *f, int cj) {
+        const size_t b = line_chunk_smem_cj<T>(cj);
+        if (b <= 200 * 1024) TG_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b));
+    };
+    set((const void *)k_line_chunked<T, 1>, 1);
+    set((const void *)k_line_chunked<T, 2>, 2);
+    set((const void *)k_line_chunked<T, 4>, 4);
+    set((const void *)k_line_chunked<T, 8>, 8);
+    set((const void *)k_line_chunked<T, 16>, 16);
+    set((const void *)k_line_chunked<T, 32>, 32);
 }
 
 
@@ -502,7 +512,7 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
     Lvl<T> &F = L[l];
     const bool fine = l == 0;
     auto smooth = [&](int color) {
-        if (mg->line && (F.nx % 2) == 0 && line_cj(F.ny) > 0) {
+        if (mg->line && (F.nx % 2) == 0 && line_cj<T>(F.ny) > 0) {
             TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse", launch_line_chunked<T>(F, color, st));
         } else if (mg->line) {
             int half = (F.nx + 1) >> 1;

@@ -666,18 +666,26 @@ __device__ __forceinline__ R3<M> cell_fp(const Grid &g, const FluxWork<M> &w, in
     return F;
 }
 
+template <class F>
+__global__ void k_cell_fp(Grid g, FluxWork<F> w)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    st3(w.fp, g.lin(k, j, i), cell_fp(g, w, k, j, i));
+}
+
 // Pass 3 (ueqn_solvers.c:1008-1035): rhs_face += scale * aj_face *
-// central(S . fp) at the faces of interior cells, with fp formed here from
-// the face fluxes (pass 2) for the cell and its +i, +j, +k neighbours. The
-// neighbour beyond the last interior cell is the ghost cell, which holds the
-// opposite first interior cell (periodic, resetCellPeriodicFluxes) or a copy
-// of this cell (ueqn_solvers.c:949-990). With `fused` the kernel also forms
+// central(S . fp) at the faces of interior cells, fp of the cell and of its
+// +i, +j, +k neighbours read from pass 2. The neighbour beyond the last
+// interior cell is the ghost cell, which holds the opposite first interior
+// cell (periodic, resetCellPeriodicFluxes) or a copy of this cell
+// (ueqn_solvers.c:949-990). With `fused` the kernel also forms
 // the rest of ExplicitRhsU at these faces in the reference's order:
 // Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += FormU, +=
 // meanGradPForcing (ueqn_sources.c:3735-3822). MR: metric storage type; F:
 // face-flux storage type.
 template <class MR, class F, bool fused>
-__global__ void __launch_bounds__(256, 3) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
+__global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -700,7 +708,7 @@ __global__ void __launch_bounds__(256, 3) k_rhs_faces(Grid g, FaceMet<MR> m, Sta
     }
     // arithmetic in FP32 only when both the metrics and the fluxes are FP32
     using M = typename std::conditional<std::is_same<MR, float>::value && std::is_same<F, float>::value, float, double>::type;
-    auto FP = [&](int kk, int jj, int ii) { return cvta<M>(cell_fp(g, w, kk, jj, ii)); };
+    auto FP = [&](int kk, int jj, int ii) { return cvta<M>(ld3(w.fp, g.lin(kk, jj, ii))); };
     auto MT = [&](const V3f<MR> &v, int q) { return cvta<M>(ld3(v, q)); };
     const R3<M> fpc = FP(k, j, i);
     const M sc = (M)scale, h = M(0.5);
@@ -1055,8 +1063,8 @@ void grad_p(tg_ctx *C)
 void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
 
 // FormU pass 1 (face fluxes) at the precision of the context's policy.
-// Passes 2-3 run inside k_rhs_faces; the flux planes are only read at the
-// points this pass writes.
+// Pass 2 (k_cell_fp) follows; the flux planes are only read at the points
+// pass 1 writes, fp only at interior cells.
 static void form_u_faces(tg_ctx *C)
 {
     const Grid g = C->g;
@@ -1067,6 +1075,8 @@ static void form_u_faces(tg_ctx *C)
     else if (P.visc32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<float, double><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm));
     else if (P.flux32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, float><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm));
     else TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, double><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm));
+    if (P.flux32) TG_PROF(C, "formu_cell_fp", k_cell_fp<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fw32));
+    else TG_PROF(C, "formu_cell_fp", k_cell_fp<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fw64));
 }
 
 template <bool fused>
