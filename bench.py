@@ -32,29 +32,44 @@ METRIC = "Mcell-steps/s mixed vs FP64 GPU at div≤1e-8; adjoint/forward time ra
 UNIT = "Mcell-steps/s"
 DIV_TOL = 5e-9
 
-# algorithmic bytes per interior cell of one launch (FP64 storage; each array
-# counted once per read and once per write; metrics re-read every launch)
-BYTES_PER_CELL = {
-    "formu_face_fluxes": 46 * 8,   # ucat 3, ucont 3, nut 1, face metrics 30 -> fluxes 9
-    "formu_cell_fp": 12 * 8,       # fluxes 9 -> fp 3
-    "formu_rhs_faces": 21 * 8,     # fp 3, csi/eta/zet 9, face aj 3, rhs 3 -> rhs 3
-    "contra_to_cart": 15 * 8,      # ucont 3, csi/eta/zet 9 -> ucat 3
-    "smagorinsky": 14 * 8,         # ucat 3, csi/eta/zet 9, aj 1 -> nut 1
-    "grad_p": 34 * 8,              # p 1, face metrics 27 + 3 -> dp 3
-    "project": 37 * 8,             # phi 1, face metrics 30, ucont 3 -> ucont 3
-    "pois_apply7": 5 * 8,          # x 1, 3 coefficients -> y 1
-    "pois_apply19": 11 * 8,        # x 1, 9 coefficients -> y 1
-    "mg_smooth_line_L0": 44,       # half the lines: r, aE, aN, aT, diag, x(nb) 6 -> x, tc, td 3 + tc, td re-read 2
-    "mg_smooth_rb_L0": 40,         # half the cells: r, diag, 3+3 coefficients, x(nb) -> x
-    "mg_restrict_L0": 50,          # r, x, 3 coefficients, diag -> coarse r, x (1/8)
-    "mg_prolong_L0": 17,           # x read/write, coarse x (1/8)
-    "pois_cg_update": 48,          # x, r read/write; p, q read
-    "pois_cg_dir": 24,             # z, p read; p write
-    "pois_dot": 16,                # two vectors
-    "rk_stage": 72,                # y = a x + z over 3 components
-    "rk_accumulate": 72,           # y += a x over 3 components
-    "rhs_init": 48,                # dp 3 -> rhs 3
-}
+# algorithmic bytes per interior cell of one launch, by storage precision of
+# the arrays the kernel reads (each array counted once per read and once per
+# write; metrics re-read every launch). The mixed mode reads FP32 copies of the
+# metrics (4 B) and keeps the state, fluxes and Krylov vectors in FP64.
+def bytes_per_cell(kernel, precision):
+    m = 4 if precision == "mixed" else 8      # metric storage
+    g = 4 if precision == "mixed" else 8      # multigrid storage
+    table = {
+        # ucat 3, ucont 3, nut 1 (FP64); face metrics 27 + face aj 3; -> fluxes 9 (FP64)
+        "formu_face_fluxes": 7 * 8 + 30 * m + 9 * 8,
+        # fluxes 9 -> fp 3
+        "formu_cell_fp": 12 * 8,
+        # fp 3, dP 3 -> rhs 3 (FP64); csi/eta/zet 9, face aj 3, icsi/jeta/kzet 9 (metrics)
+        "formu_rhs_faces": 9 * 8 + 21 * m,
+        # ucont 3 -> ucat 3 (FP64); csi/eta/zet 9
+        "contra_to_cart": 6 * 8 + 9 * m,
+        # ucat 3 -> nut 1 (FP64); csi/eta/zet 9, aj 1
+        "smagorinsky": 4 * 8 + 10 * m,
+        # p 1 -> dP 3 (FP64); face metrics 27 + 3
+        "grad_p": 4 * 8 + 30 * m,
+        # phi 1, ucont 3 -> ucont 3 (FP64); face metrics 27 + 3
+        "project": 7 * 8 + 30 * m,
+        # one zebra colour (half the cells): r, minv, aN, c', aE, aT, x of the
+        # other colour -> x: 8 values per cell of the colour
+        "mg_smooth_line_L0": 8 * g / 2,
+        # r, x, 3 coefficients -> coarse r (1/8 of the cells)
+        "mg_restrict_L0": 5 * g + g / 8,
+        # x read/write, coarse x (1/8)
+        "mg_prolong_L0": 2 * g + g / 8,
+        "pois_apply7": 5 * 8,          # x 1, 3 coefficients -> y 1
+        "pois_apply19": 11 * 8,        # x 1, 9 coefficients -> y 1
+        "pois_cg_update": 48,          # x, r read/write; p, q read
+        "pois_cg_dir": 24,             # z, p read; p write
+        "pois_dot": 16,                # two vectors
+        # RK4 bookkeeping averaged over the four stages: 12 + 15 + 15 + 9 values
+        "rk_update": 51 * 8 / 4,
+    }
+    return table.get(kernel)
 
 
 def env_int(name, default):
@@ -200,6 +215,46 @@ def run_reference(args, rank, world):
     return 0
 
 
+def kernel_table(L, h):
+    import ctypes
+    kernels = {}
+    nb = ctypes.create_string_buffer(64)
+    for q in range(L.tg_prof_count(h)):
+        n = ctypes.c_int64()
+        ms = ctypes.c_double()
+        L.tg_prof_get(h, q, nb, ctypes.byref(n), ctypes.byref(ms))
+        kernels[nb.value.decode()] = {"launches": int(n.value), "ms": float(ms.value)}
+    total = sum(v["ms"] for v in kernels.values())
+    for v in kernels.values():
+        v["share"] = v["ms"] / total if total > 0 else 0.0
+    return kernels
+
+
+def roofline_of(kernels, precision, cells):
+    """Roofline of the dominant kernel with a known byte count: algorithmic
+    bytes per launch / average launch time (library events on its stream)."""
+    ranked = sorted(kernels.items(), key=lambda kv: -kv[1]["ms"])
+    dom = next((k for k, v in ranked if bytes_per_cell(k, precision) is not None), None)
+    if dom is None:
+        return None
+    peak, peak_src = load_peaks()
+    kv = kernels[dom]
+    per_launch_ms = kv["ms"] / kv["launches"]
+    algo_bytes = bytes_per_cell(dom, precision) * cells
+    achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f).get(precision, {})
+        if dom in tj:
+            traffic = tj[dom] * cells
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_ms": per_launch_ms,
+            "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,11 +262,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: the mixed step is the headline value, the FP64 step is timed beside it")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--profile-steps", type=int, default=2,
+                    help="untimed steps after the timed region with per-kernel events on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--profile-json", default=None, help="write per-kernel timings here")
+    ap.add_argument("--profile-json", default=None, help="write per-kernel timings here (one file per arm)")
     ap.add_argument("--cells", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="override the ABL size (profiling captures of a smaller case)")
     args = ap.parse_args()
@@ -223,6 +281,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
+    import ctypes
     import torch
     import tosca_b200
     from tosca_b200 import cases
@@ -237,12 +296,6 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    cfg, nodes, ucat, p, T, desc = make_workload(args.workload, args.precision, seed_offset=rank, cells=args.cells)
-    cfg.device = dev
-    solver = tosca_b200.gpu_solver(cfg)
-    cases.setup(solver, nodes, ucat, p, T)
-    lib = solver.fns
-    import ctypes
     L = ctypes.CDLL(tosca_b200.LIB_PATH)
     L.tg_prof_enable.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.tg_prof_reset.argtypes = [ctypes.c_void_p]
@@ -262,58 +315,57 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up
-    if args.warmup > 0:
-        solver.step(args.warmup)
-
-    # timed region (device events on the library's stream), per-kernel events live
-    L.tg_prof_reset(solver.h)
-    L.tg_prof_enable(solver.h, 1)
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        st = solver.step(args.steps)
+    def arm(precision):
+        cfg, nodes, ucat, p, T, desc = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells)
+        cfg.device = dev
+        solver = tosca_b200.gpu_solver(cfg)
+        cases.setup(solver, nodes, ucat, p, T)
+        if args.warmup > 0:
+            solver.step(args.warmup)
+        # timed region: device time between events on the library's stream
+        barrier()
         torch.cuda.synchronize()
-    barrier()
-    L.tg_prof_enable(solver.h, 0)
-    t_dev = max_over_ranks(st.seconds)
-    clocks = clk.summary()
-    cells = cfg.cells
-    value = cells * args.steps * world / t_dev / 1e6
+        with ClockSampler(dev) as clk:
+            st = solver.step(args.steps)
+            torch.cuda.synchronize()
+        barrier()
+        t_dev = max_over_ranks(st.seconds)
+        # per-kernel events on a few further steps (outside the timed region)
+        L.tg_prof_reset(solver.h)
+        L.tg_prof_enable(solver.h, 1)
+        solver.step(args.profile_steps)
+        torch.cuda.synchronize()
+        L.tg_prof_enable(solver.h, 0)
+        kernels = kernel_table(L, solver.h)
+        return {"cfg": cfg, "desc": desc, "solver": solver, "st": st, "t_dev": t_dev, "clocks": clk.summary(),
+                "value": cfg.cells * args.steps * world / t_dev / 1e6, "kernels": kernels,
+                "roofline": roofline_of(kernels, precision, cfg.cells)}
 
-    # per-kernel accounting
-    kernels = {}
-    nb = ctypes.create_string_buffer(64)
-    for q in range(L.tg_prof_count(solver.h)):
-        n = ctypes.c_int64()
-        ms = ctypes.c_double()
-        L.tg_prof_get(solver.h, q, nb, ctypes.byref(n), ctypes.byref(ms))
-        kernels[nb.value.decode()] = {"launches": int(n.value), "ms": float(ms.value)}
-    total_k = sum(v["ms"] for v in kernels.values())
-    for v in kernels.values():
-        v["share"] = v["ms"] / total_k if total_k > 0 else 0.0
-    ranked = sorted(kernels.items(), key=lambda kv: -kv[1]["ms"])
-    dom = next((k for k, v in ranked if k in BYTES_PER_CELL), None)
-    peak, peak_src = load_peaks()
-    roofline = None
-    if dom is not None:
-        kv = kernels[dom]
-        per_launch_ms = kv["ms"] / kv["launches"]
-        algo_bytes = BYTES_PER_CELL[dom] * cells
-        achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
-        if os.path.exists(tpath):
-            with open(tpath) as f:
-                tj = json.load(f)
-            if dom in tj:
-                traffic = tj[dom] * cells
-        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
-                    "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                    "algorithmic_bytes_per_launch": algo_bytes, "avg_launch_ms": per_launch_ms,
-                    "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else peak_src}
+    arms = {}
+    order = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    for prec in order:
+        arms[prec] = arm(prec)
+    head_prec = order[-1]
+    head = arms[head_prec]
+    cfg, cells = head["cfg"], head["cfg"].cells
+
+    # mixed against FP64 after the same number of steps from the same state
+    field_err = None
+    if len(arms) == 2:
+        def rel(a, b):
+            a, b = a[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]
+            d = float(np.linalg.norm(b.ravel()))
+            return float(np.linalg.norm((a - b).ravel()) / d) if d > 0 else float(np.linalg.norm(a.ravel()))
+        ua, ub = arms["mixed"]["solver"].get("UCAT"), arms["fp64"]["solver"].get("UCAT")
+        field_err = {"u": rel(ua[..., 0], ub[..., 0]), "v": rel(ua[..., 1], ub[..., 1]),
+                     "w": rel(ua[..., 2], ub[..., 2]),
+                     "p": rel(arms["mixed"]["solver"].get("P"), arms["fp64"]["solver"].get("P")),
+                     "steps": args.warmup + args.steps + args.profile_steps,
+                     "against": "FP64 GPU step (itself within 1e-10 of the FP64 oracle in the parity tests)"}
+        arms["fp64"]["solver"].close()
 
     # end-to-end through the C-ABI with host buffers (drop-in call per step)
+    solver = head["solver"]
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(2, args.steps // 2)
     mz, my, mx = cfg.mz, cfg.my, cfg.mx
     h_ucont = torch.empty((mz, my, mx, 3), dtype=torch.float64, pin_memory=True).numpy()
@@ -336,7 +388,7 @@ def main():
     bytes_state = h_ucont.nbytes + h_ucat.nbytes + h_p.nbytes + (h_nut.nbytes if cfg.les else 0)
     e2e = {"value": cells * e2e_steps * world / t_e2e / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": int(bytes_state), "d2h_bytes_per_step": int(bytes_state),
-           "steps": e2e_steps, "max_divergence": se.max_divergence}
+           "steps": e2e_steps, "precision": head_prec, "max_divergence": se.max_divergence}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,31 +396,47 @@ def main():
         cpu = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:
+        st = head["st"]
+        kernels = head["kernels"]
+        ranked = sorted(kernels.items(), key=lambda kv: -kv[1]["ms"])
+        launches_per_step = sum(v["launches"] for v in kernels.values()) / max(1, args.profile_steps)
         line = {
-            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+            "metric": METRIC, "value": round(head["value"], 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["t_dev"] / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "dtype": "f64" if head_prec == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": desc, "cells": cells, "dmda_extent": [mx, my, mz],
-                       "precision": args.precision, "divergence_bound": DIV_TOL,
+            "config": {"workload": head["desc"], "cells": cells, "dmda_extent": [mx, my, mz],
+                       "precision": head_prec, "divergence_bound": DIV_TOL,
                        "l2": "every field exceeds the 126 MB L2; no flush",
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "poisson_iterations_last": st.poisson_iterations,
                        "poisson_iterations_per_step": st.poisson_total_iterations / max(1, args.steps),
                        "max_divergence": st.max_divergence},
-            "clocks": clocks,
+            "clocks": head["clocks"],
             "e2e": e2e,
-            "gpu_launches": int(sum(v["launches"] for v in kernels.values())),
-            "roofline": roofline,
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "gpu_launches_note": "per-step count of the library's timed launches in the profiled steps x timed steps",
+            "roofline": head["roofline"],
             "cpu_baseline": cpu,
-            "kernels_top": {k: {"ms": round(v["ms"], 3), "launches": v["launches"], "share": round(v["share"], 4)}
-                            for k, v in ranked[:12]},
+            "kernels_top": {k: {"ms_per_step": round(v["ms"] / max(1, args.profile_steps), 3),
+                                "launches_per_step": v["launches"] / max(1, args.profile_steps),
+                                "share": round(v["share"], 4)} for k, v in ranked[:12]},
         }
+        if "fp64" in arms and head_prec != "fp64":
+            a = arms["fp64"]
+            line["fp64"] = {"value": round(a["value"], 3), "ms_per_step": a["t_dev"] / args.steps * 1e3,
+                            "poisson_iterations_per_step": a["st"].poisson_total_iterations / max(1, args.steps),
+                            "max_divergence": a["st"].max_divergence, "clocks": a["clocks"],
+                            "roofline": a["roofline"]}
+            line["mixed_over_fp64"] = round(head["value"] / a["value"], 4)
+            line["mixed_field_error"] = field_err
         print(json.dumps(line), flush=True)
         if args.profile_json:
-            with open(args.profile_json, "w") as f:
-                json.dump({"kernels": kernels, "cells": cells, "steps": args.steps}, f, indent=1)
+            for prec, a in arms.items():
+                path = args.profile_json if len(arms) == 1 else args.profile_json.replace(".json", "_%s.json" % prec)
+                with open(path, "w") as f:
+                    json.dump({"kernels": a["kernels"], "cells": a["cfg"].cells, "steps": args.profile_steps,
+                               "precision": prec}, f, indent=1)
     solver.close()
     if dist is not None:
         dist.barrier()

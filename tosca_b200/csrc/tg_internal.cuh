@@ -141,6 +141,7 @@ struct tg_ctx {
         bool rhs32 = false;          // FormU face assembly metrics
         bool smag32 = false;         // Smagorinsky eddy viscosity
         bool gradp32 = false;        // GradP
+        bool proj32 = false;         // ProjectVelocity (FP64 arithmetic)
     } pol;
     bool met32_stale = true;             // metrics changed since the FP32 copies were made
     tg::FaceMet<double> fm64{};

@@ -45,7 +45,7 @@ struct Lvl {
 
 constexpr int MAXL = 16;
 constexpr int TAIL_CELLS = 4096;
-constexpr int LINE_NW = 8;          // warps per block of the chunked line solver
+constexpr int LINE_NW = 32;         // warps per block of the chunked line solver (one line chunk each)
 
 template <class T>
 struct Tail {
