@@ -93,6 +93,8 @@ typedef struct tg_config {
     int32_t precision;             /* TG_PREC_*                                             */
     int32_t it_start;              /* clock->itStart                                        */
     int32_t device;                /* CUDA device ordinal (ignored by the CPU restatement)  */
+    int32_t source;                /* body force TG_F_SOURCE added by sourceU               */
+                                   /* (ueqn_sources.c:2884-2980, ueqn_solvers.c:1369)       */
 } tg_config;
 
 /* per-call statistics */
@@ -117,6 +119,10 @@ enum {
     TG_F_UCONT, TG_F_UCAT, TG_F_UCONT_O, TG_F_RHS, TG_F_DP, TG_F_BTHETA,/* vectors             */
     TG_F_P, TG_F_PHI, TG_F_NUT, TG_F_TMPRT,                             /* scalars             */
     TG_F_TAUWALL,                                                       /* vector, j=0 plane   */
+    TG_F_SOURCE,                  /* vector: cell-centred Cartesian body force (ueqn->sourceU) */
+    /* adjoint fields of tg_adjoint_*: adjoints of Ucont, Ucat, P and the
+     * gradient of the objective with respect to TG_F_SOURCE */
+    TG_F_UCONT_ADJ, TG_F_UCAT_ADJ, TG_F_P_ADJ, TG_F_SOURCE_ADJ,
     TG_F_COUNT
 };
 

@@ -78,6 +78,10 @@ struct tg_ctx {
 
     // state
     std::vector<V3> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, fp, div1, div2, div3, visc1, visc2, visc3;
+    std::vector<V3> source;                     // ueqn->sourceU (cell-centred Cartesian body force)
+    // adjoints (tosca_oracle_adjoint.inc)
+    std::vector<V3> ucont_adj, ucat_adj, source_adj;
+    std::vector<double> p_adj;
     std::vector<double> p, phi, nut, tmprt;
 
     // jLeft wall model arrays, indexed k*mx + i (tauWall, uMeanMag, uFilt)
@@ -1291,6 +1295,23 @@ void meanGradPForcing(tg_ctx &C, std::vector<V3> &R)
     }
 }
 
+// sourceU, ueqn_sources.c:2884-2980: central face value of the body force
+// dotted with the face area vector, faces of interior cells
+void sourceU(tg_ctx &C, std::vector<V3> &R)
+{
+    const int mx = C.mx, my = C.my, mz = C.mz;
+    const std::vector<V3> &f = C.source;
+    auto lin = [&](int k, int j, int i) { return ((size_t)k * my + j) * mx + i; };   // global Vec: no wrap
+    for (int k = 1; k < mz - 1; k++)
+    for (int j = 1; j < my - 1; j++)
+    for (int i = 1; i < mx - 1; i++) {
+        size_t c = lin(k, j, i), ie = lin(k, j, i + 1), jn = lin(k, j + 1, i), kt = lin(k + 1, j, i);
+        R[c].x += 1.0 * (0.5 * (f[c].x + f[ie].x) * C.icsi[c].x + 0.5 * (f[c].y + f[ie].y) * C.icsi[c].y + 0.5 * (f[c].z + f[ie].z) * C.icsi[c].z);
+        R[c].y += 1.0 * (0.5 * (f[c].x + f[jn].x) * C.jeta[c].x + 0.5 * (f[c].y + f[jn].y) * C.jeta[c].y + 0.5 * (f[c].z + f[jn].z) * C.jeta[c].z);
+        R[c].z += 1.0 * (0.5 * (f[c].x + f[kt].x) * C.kzet[c].x + 0.5 * (f[c].y + f[kt].y) * C.kzet[c].y + 0.5 * (f[c].z + f[kt].z) * C.kzet[c].z);
+    }
+}
+
 // resetNonResolvedCellFaces, inline.h:1674-1835
 void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
 {
@@ -1333,6 +1354,7 @@ void explicitRhsU(tg_ctx &C)
         }
     }
     formU(C, C.rhs, 1.0);
+    if (C.c.source) sourceU(C, C.rhs);                 // ueqn_solvers.c:1365-1370
     if (C.c.mean_grad_p) meanGradPForcing(C, C.rhs);
     resetNonResolvedCellFaces(C, C.rhs);
 }
@@ -1523,9 +1545,9 @@ int step(tg_ctx &C, tg_stats *st)
 void allocState(tg_ctx &C)
 {
     const size_t G = C.G;
-    for (auto *v : {&C.ucont, &C.ucont_o, &C.ucat, &C.rhs, &C.dp, &C.btheta, &C.btheta_o, &C.gcont, &C.utmp, &C.fp,
+    for (auto *v : {&C.ucont, &C.ucont_o, &C.ucat, &C.rhs, &C.dp, &C.btheta, &C.btheta_o, &C.gcont, &C.utmp, &C.fp, &C.source, &C.ucont_adj, &C.ucat_adj, &C.source_adj,
                     &C.div1, &C.div2, &C.div3, &C.visc1, &C.visc2, &C.visc3}) zero(*v, G);
-    for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt}) zero(*v, G);
+    for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt, &C.p_adj}) zero(*v, G);
     const size_t P = (size_t)C.mx * C.mz;
     for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz}) zero(*v, P);
 }
@@ -1539,7 +1561,8 @@ std::vector<V3> *vecField(tg_ctx &C, int w)
     case TG_F_JZET: return &C.jzet;   case TG_F_KCSI: return &C.kcsi; case TG_F_KETA: return &C.keta;
     case TG_F_KZET: return &C.kzet;   case TG_F_UCONT: return &C.ucont; case TG_F_UCAT: return &C.ucat;
     case TG_F_UCONT_O: return &C.ucont_o; case TG_F_RHS: return &C.rhs; case TG_F_DP: return &C.dp;
-    case TG_F_BTHETA: return &C.btheta;
+    case TG_F_BTHETA: return &C.btheta; case TG_F_SOURCE: return &C.source;
+    case TG_F_UCONT_ADJ: return &C.ucont_adj; case TG_F_UCAT_ADJ: return &C.ucat_adj; case TG_F_SOURCE_ADJ: return &C.source_adj;
     default: return nullptr;
     }
 }
@@ -1548,6 +1571,7 @@ std::vector<double> *scalField(tg_ctx &C, int w)
     switch (w) {
     case TG_F_AJ: return &C.aj; case TG_F_IAJ: return &C.iaj; case TG_F_JAJ: return &C.jaj; case TG_F_KAJ: return &C.kaj;
     case TG_F_P: return &C.p; case TG_F_PHI: return &C.phi; case TG_F_NUT: return &C.nut; case TG_F_TMPRT: return &C.tmprt;
+    case TG_F_P_ADJ: return &C.p_adj;
     default: return nullptr;
     }
 }
@@ -1589,6 +1613,8 @@ void copyOut(const tg_ctx &C, double *dst, const double *src, int halo)
 // ============================================================================
 //  C-ABI (prefix tor_), same semantics as the tg_ entry points
 // ============================================================================
+#include "tosca_oracle_adjoint.inc"
+
 extern "C" {
 
 const char *tor_status_string(tg_status s)
@@ -1802,6 +1828,29 @@ int32_t tor_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+// Discrete adjoint of one step (test infrastructure, see tosca_oracle_adjoint.inc).
+// The context holds the state at the start of the step and the adjoint fields
+// the adjoints of the state after it; on return the adjoint fields hold the
+// adjoints of the state before the step, TG_F_SOURCE_ADJ has the step's
+// contribution added, and the state is again the one at the start of the step.
+tg_status tor_adjoint_step(tg_ctx *C)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
+        // state saved around the taped forward step
+        auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
+        auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;
+        int it = C->it;
+        AdjTape T;
+        tg_stats st{};
+        stepTaped(*C, &st, T);
+        C->ucont = ucont; C->ucat = ucat; C->btheta = btheta; C->btheta_o = btheta_o;
+        C->p = p; C->phi = phi; C->phi1d = phi1d; C->nut = nut; C->it = it;
+        adjointStep(*C, T);
+        return TG_OK;
+    });
 }
 
 } // extern "C"

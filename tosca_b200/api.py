@@ -28,10 +28,11 @@ FIELDS = [
     "CENT", "CSI", "ETA", "ZET", "ICSI", "IETA", "IZET", "JCSI", "JETA", "JZET",
     "KCSI", "KETA", "KZET", "AJ", "IAJ", "JAJ", "KAJ",
     "UCONT", "UCAT", "UCONT_O", "RHS", "DP", "BTHETA",
-    "P", "PHI", "NUT", "TMPRT", "TAUWALL",
+    "P", "PHI", "NUT", "TMPRT", "TAUWALL", "SOURCE",
+    "UCONT_ADJ", "UCAT_ADJ", "P_ADJ", "SOURCE_ADJ",
 ]
 F = {name: i for i, name in enumerate(FIELDS)}
-SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT"}
+SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT", "P_ADJ"}
 
 
 class TgConfig(C.Structure):
@@ -59,6 +60,7 @@ class TgConfig(C.Structure):
         ("precision", C.c_int32),
         ("it_start", C.c_int32),
         ("device", C.c_int32),
+        ("source", C.c_int32),
     ]
 
 
@@ -105,6 +107,7 @@ class Config:
     precision: int = PREC_FP64
     it_start: int = 0
     device: int = 0
+    source: int = 0
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

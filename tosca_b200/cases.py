@@ -147,20 +147,21 @@ def tgv_case(n: int = 64, ddt: int = DDT_FE, dt: float = 0.005, nu: float = 1.0 
 def abl_case(nx: int = 256, ny: int = 256, nz: int = 128, Lx: float = 2560.0, Ly: float = 2560.0,
              H: float = 1000.0, dz1: float = 2.0, ustar: float = 0.4, z0: float = 0.1,
              kappa: float = 0.4, cs: float = 0.01, nu: float = 1.5e-5, dt: float = 0.25,
-             ddt: int = DDT_FE, seed: int = 20261203, amp: float = 0.05):
+             ddt: int = DDT_FE, seed: int = 20261203, amp: float = 0.05, wall: int = BC_WALL_SHUMANN):
     """Neutral pressure-driven ABL on a tanh-clustered vertical grid (first
     cell dz1, largest consecutive spacing ratio <= 1.05). Log-law initial profile u = (u*/kappa)
     ln(z/z0) with seeded uniform +-amp perturbations: Ucat = U(z)(1+e_x, e_y,
     e_z), e from splitmix64 over (seed, component, global cell index). Mean
     pressure gradient u*^2/H drives the flow (meanGradPForcing,
-    ueqn_sources.c:3735-3822)."""
+    ueqn_sources.c:3735-3822). `wall` is the bottom patch type: the Schumann
+    wall function, or noSlip for the adjoint configuration."""
     X = np.linspace(0.0, Lx, nx + 1)
     Y = np.linspace(0.0, Ly, ny + 1)
     Z = tanh_stretch(nz, H, dz1)
     nodes = cartesian_nodes(X, Y, Z)
     mx, my, mz = ny + 2, nz + 2, nx + 2
     cfg = Config(mx=mx, my=my, mz=mz,
-                 bc=(BC_PERIODIC, BC_PERIODIC, BC_WALL_SHUMANN, BC_SLIP, BC_PERIODIC, BC_PERIODIC),
+                 bc=(BC_PERIODIC, BC_PERIODIC, wall, BC_SLIP, BC_PERIODIC, BC_PERIODIC),
                  nut_bc=(NUTBC_PERIODIC, NUTBC_PERIODIC, NUTBC_FIXEDVALUE, NUTBC_FIXEDVALUE, NUTBC_PERIODIC, NUTBC_PERIODIC),
                  les=1, cs=cs, nu=nu, div_scheme=DIV_CENTRAL, ddt_scheme=ddt, dt=dt,
                  mean_grad_p=1, mean_grad_p_value=(ustar * ustar / H, 0.0, 0.0),

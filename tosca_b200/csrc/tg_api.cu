@@ -78,6 +78,7 @@ bool vec_field(tg_ctx *C, int w, V3f<double> &out)
     case TG_F_UCAT: out = s.ucat; return true;   case TG_F_UCONT_O: out = s.ucont_o; return true;
     case TG_F_RHS: out = s.rhs; return true;     case TG_F_DP: out = s.dp; return true;
     case TG_F_BTHETA: out = s.btheta; return true;
+    case TG_F_SOURCE: out = s.source; return true;
     default: return false;
     }
 }
@@ -221,7 +222,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         Params &p = C->prm;
         for (int q = 0; q < 6; q++) { p.bc[q] = cfg->bc[q]; p.nut_bc[q] = cfg->nut_bc[q]; p.nut_bc_value[q] = cfg->nut_bc_value[q]; }
         p.curvilinear = cfg->curvilinear; p.les = cfg->les; p.div_scheme = cfg->div_scheme;
-        p.buoyancy = cfg->buoyancy; p.mean_grad_p = cfg->mean_grad_p;
+        p.buoyancy = cfg->buoyancy; p.mean_grad_p = cfg->mean_grad_p; p.source = cfg->source;
         p.cs = cfg->cs; p.nu = cfg->nu; p.dt = cfg->dt; p.t_ref = cfg->t_ref;
         for (int q = 0; q < 3; q++) p.mgp[q] = cfg->mean_grad_p_value[q];
         p.z0 = cfg->wall_roughness; p.kappa = cfg->wall_kappa;
@@ -233,7 +234,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         double **ms[] = {&m.aj, &m.iaj, &m.jaj, &m.kaj, &m.g11, &m.g12, &m.g13, &m.g21, &m.g22, &m.g23, &m.g31, &m.g32, &m.g33};
         for (auto **v : ms) *v = dallocd(C, G);
         State &st = C->s;
-        V3f<double> *sv[] = {&st.ucont, &st.ucont_o, &st.ucat, &st.rhs, &st.dp, &st.btheta, &st.btheta_o, &st.gcont, &st.utmp, &st.snap};
+        V3f<double> *sv[] = {&st.ucont, &st.ucont_o, &st.ucat, &st.rhs, &st.dp, &st.btheta, &st.btheta_o, &st.gcont, &st.utmp, &st.snap, &st.source};
         for (auto *v : sv) *v = dalloc3(C, G);
         C->mixed = cfg->precision == TG_PREC_MIXED;
         alloc_precision_work(C);

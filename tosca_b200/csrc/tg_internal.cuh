@@ -81,6 +81,7 @@ struct FluxWork {
 // physical state and work arrays
 struct State {
     V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, snap;
+    V3f<double> source;          // ueqn->sourceU, cell-centred Cartesian body force
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
@@ -90,7 +91,7 @@ struct Params {
     int bc[6];
     int nut_bc[6];
     double nut_bc_value[6];
-    int curvilinear, les, div_scheme, buoyancy, mean_grad_p;
+    int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source;
     double cs, nu, dt, t_ref, mgp[3], z0, kappa;
 };
 

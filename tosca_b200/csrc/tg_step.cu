@@ -682,8 +682,8 @@ __global__ void k_cell_fp(Grid g, FluxWork<F> w)
 // (ueqn_solvers.c:949-990). With `fused` the kernel also forms
 // the rest of ExplicitRhsU at these faces in the reference's order:
 // Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += FormU, +=
-// meanGradPForcing (ueqn_sources.c:3735-3822). MR: metric storage type; F:
-// face-flux storage type.
+// sourceU (body force), += meanGradPForcing (ueqn_sources.c:3735-3822). MR:
+// metric storage type; F: face-flux storage type.
 template <class MR, class F, bool fused>
 __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
 {
@@ -726,6 +726,15 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
       int n = c + g.mx * g.my; R3<M> a = MT(m.zet, c), b = MT(m.zet, n);
       v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
       oz = base.z + (double)(sc * (M)m.kaj[c] * (h * (v1 + v2))); }
+    if (fused && p.source) {
+        // sourceU (ueqn_solvers.c:1369, ueqn_sources.c:2884-2980): central body force . face area, FP64
+        const V3f<double> &f = s.source;
+        const int ie = c + 1, jn = c + g.mx, kt = c + g.mx * g.my;
+        R3<double> a = cvta<double>(ld3(m.icsi, c)), b = cvta<double>(ld3(m.jeta, c)), d = cvta<double>(ld3(m.kzet, c));
+        ox += 1.0 * (0.5 * (f.x[c] + f.x[ie]) * a.x + 0.5 * (f.y[c] + f.y[ie]) * a.y + 0.5 * (f.z[c] + f.z[ie]) * a.z);
+        oy += 1.0 * (0.5 * (f.x[c] + f.x[jn]) * b.x + 0.5 * (f.y[c] + f.y[jn]) * b.y + 0.5 * (f.z[c] + f.z[jn]) * b.z);
+        oz += 1.0 * (0.5 * (f.x[c] + f.x[kt]) * d.x + 0.5 * (f.y[c] + f.y[kt]) * d.y + 0.5 * (f.z[c] + f.z[kt]) * d.z);
+    }
     if (fused && p.mean_grad_p) {
         R3<M> a = MT(m.icsi, c), b = MT(m.jeta, c), d = MT(m.kzet, c);
         const M g0 = (M)p.mgp[0], g1 = (M)p.mgp[1], g2 = (M)p.mgp[2];
