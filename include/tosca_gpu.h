@@ -195,6 +195,36 @@ tg_status tg_sync_pressure(tg_ctx *ctx);               /* overset.h:107 / overse
 /* nsteps full time steps in the order of main.c:54-327 (fixed dt). */
 tg_status tg_step(tg_ctx *ctx, int32_t nsteps, tg_stats *stats);
 
+/* ----------------------------------------------------------------- adjoint -- */
+/* Discrete adjoint of tg_step. No counterpart in the reference: TOSCA has no
+ * adjoint. Adjoint fields are exchanged with tg_set_field / tg_get_field
+ * (TG_F_UCONT_ADJ, TG_F_UCAT_ADJ, TG_F_P_ADJ: adjoints of Ucont, of the full
+ * Ucat array and of P; TG_F_SOURCE_ADJ: gradient with respect to the body
+ * force TG_F_SOURCE, accumulated). Supported: orthogonal grids, FE and RK4,
+ * central and QUICK convection, constant or Smagorinsky viscosity, noSlip /
+ * slip / periodic patches; anything else returns TG_ERR_BAD_ARG. */
+typedef struct tg_adjoint_stats {
+    int64_t steps;                 /* steps reversed                                        */
+    int64_t forward_steps;         /* forward steps run by the reversal (recomputation)     */
+    int32_t snapshots;             /* device snapshots of the checkpoint schedule           */
+    double  seconds;               /* device time of the call                               */
+} tg_adjoint_stats;
+
+/* Vector-Jacobian product of one step: the context holds the state at the
+ * start of a step and the adjoint fields hold the adjoints of the state after
+ * it; on return they hold the adjoints of the state before it, the body-force
+ * gradient has the step's contribution added, and the state is again the one
+ * at the start of the step (the step is re-run once to record its stages). */
+tg_status tg_adjoint_step(tg_ctx *ctx);
+/* nsteps forward steps from the current state with binomial (revolve)
+ * checkpointing in nsnap device snapshots; leaves the final state in the
+ * context (to seed the adjoint fields from it). */
+tg_status tg_adjoint_forward(tg_ctx *ctx, int32_t nsteps, int32_t nsnap, tg_stats *stats);
+/* Reverse sweep over the steps of the last tg_adjoint_forward, from the adjoint
+ * fields of the final state to those of the initial state; the context returns
+ * to the initial state. */
+tg_status tg_adjoint_reverse(tg_ctx *ctx, tg_adjoint_stats *stats);
+
 /* One drop-in step with host state: Ucont, Ucat, P (and nut when LES is on) are
  * uploaded from the caller's arrays, one step runs, and the same arrays are
  * overwritten with the new state. This is the call a host time loop makes when

@@ -64,6 +64,15 @@ class TgConfig(C.Structure):
     ]
 
 
+class TgAdjointStats(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("forward_steps", C.c_int64),
+        ("snapshots", C.c_int32),
+        ("seconds", C.c_double),
+    ]
+
+
 class TgStats(C.Structure):
     _fields_ = [
         ("steps", C.c_int64),
@@ -152,7 +161,14 @@ _SIGS = {
     "step_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
 }
 
-ENTRY_POINTS = tuple(_SIGS)
+# adjoint entry points (the CPU restatement exports tor_adjoint_step only)
+_ADJ_SIGS = {
+    "adjoint_step": (C.c_int, [C.c_void_p]),
+    "adjoint_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TgStats)]),
+    "adjoint_reverse": (C.c_int, [C.c_void_p, C.POINTER(TgAdjointStats)]),
+}
+
+ENTRY_POINTS = tuple(_SIGS) + tuple(_ADJ_SIGS)
 
 
 def bind(lib: C.CDLL, prefix: str) -> dict:
@@ -164,6 +180,12 @@ def bind(lib: C.CDLL, prefix: str) -> dict:
         fn.restype = res
         fn.argtypes = args
         out[name] = fn
+    for name, (res, args) in _ADJ_SIGS.items():
+        fn = getattr(lib, prefix + name, None)
+        if fn is not None:
+            fn.restype = res
+            fn.argtypes = args
+            out[name] = fn
     return out
 
 
@@ -291,6 +313,21 @@ class Solver:
         st = TgStats()
         self._check(self.fns["step"](self.h, n, C.byref(st)), "step")
         self.last_stats = st
+        return st
+
+    # --------------------------------------------------------------- adjoint
+    def adjoint_step(self):
+        """VJP of one step at the current state (adjoint fields in, adjoint fields out)."""
+        self._check(self.fns["adjoint_step"](self.h), "adjoint_step")
+
+    def adjoint_forward(self, n: int, nsnap: int) -> TgStats:
+        st = TgStats()
+        self._check(self.fns["adjoint_forward"](self.h, n, nsnap, C.byref(st)), "adjoint_forward")
+        return st
+
+    def adjoint_reverse(self) -> TgAdjointStats:
+        st = TgAdjointStats()
+        self._check(self.fns["adjoint_reverse"](self.h, C.byref(st)), "adjoint_reverse")
         return st
 
     def step_host(self, ucont, ucat, p, nut=None, halo: int = 0) -> TgStats:

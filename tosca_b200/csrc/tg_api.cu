@@ -267,6 +267,7 @@ tg_status tg_destroy(tg_ctx *C)
     cudaSetDevice(C->cfg.device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     poisson_destroy(C);
+    adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);
     for (cudaEvent_t e : C->prof.pool) cudaEventDestroy(e);
     if (C->h_scal) cudaFreeHost(C->h_scal);
@@ -309,6 +310,12 @@ tg_status tg_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
         if (!host || halo < 0) return fail(C, TG_ERR_BAD_ARG, "bad field argument");
         V3f<double> v;
         double *sp = nullptr;
+        if (adj_field(C, w, v, sp)) {
+            if (sp) upload(C, host, halo, sp, nullptr, nullptr);
+            else upload(C, host, halo, v.x, v.y, v.z);
+            TG_CUDA(cudaStreamSynchronize(C->stream));
+            return TG_OK;
+        }
         if (vec_field(C, w, v)) upload(C, host, halo, v.x, v.y, v.z);
         else if ((sp = scal_field(C, w)) != nullptr) upload(C, host, halo, sp, nullptr, nullptr);
         else return fail(C, TG_ERR_BAD_ARG, "field not settable");
@@ -334,6 +341,12 @@ tg_status tg_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
             return TG_OK;
         }
         V3f<double> v;
+        double *sp = nullptr;
+        if (adj_field(C, w, v, sp)) {
+            if (sp) download(C, host, halo, sp, nullptr, nullptr);
+            else download(C, host, halo, v.x, v.y, v.z);
+            return TG_OK;
+        }
         if (vec_field(C, w, v)) { download(C, host, halo, v.x, v.y, v.z); return TG_OK; }
         if (double *s = scal_field(C, w)) { download(C, host, halo, s, nullptr, nullptr); return TG_OK; }
         return fail(C, TG_ERR_BAD_ARG, "unknown field");

@@ -96,6 +96,7 @@ struct Params {
 };
 
 struct PoissonCtx;   // tg_poisson.cu
+struct AdjState;     // tg_adjoint.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -154,6 +155,8 @@ struct tg_ctx {
     bool clear_rhs = false, clear_dp = false;
     std::string err;
     tg::PoissonCtx *pois = nullptr;
+    tg::AdjState *adj = nullptr;         // adjoint fields, tape and checkpoints (tg_adjoint.cu)
+    bool taping = false;                 // the running step records its stage states
     tg::Profiler prof;
 };
 
@@ -230,5 +233,15 @@ void reduce_max_abs_div(tg_ctx *C, double *d_out);
 void poisson_setup(tg_ctx *C);
 void poisson_destroy(tg_ctx *C);
 int poisson_solve(tg_ctx *C, tg_stats *st);
+
+// adjoint (tg_adjoint.cu)
+void tape_step_start(tg_ctx *C);
+void tape_nut(tg_ctx *C);
+void tape_stage(tg_ctx *C);
+bool adj_field(tg_ctx *C, int w, V3f<double> &v, double *&s);   // adjoint fields (allocated on first use)
+void adj_destroy(tg_ctx *C);
+int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st);
+double *poisson_x(tg_ctx *C);
+int64_t poisson_n(tg_ctx *C);
 
 }  // namespace tg

@@ -234,6 +234,10 @@ __global__ void k_copy(int64_t n, const double *a, double *b)
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
 }
 __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
+__global__ void k_negcopy(int64_t n, const double *a, double *b)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = -a[t];
+}
 
 // CG: alpha = rz / pq ; x += alpha p ; r -= alpha q
 __global__ void k_cg_update(int64_t n, const double *rz, const double *pq, double *x, const double *p, double *r, const double *q)
@@ -371,22 +375,18 @@ static void read_scal(tg_ctx *C, int off, int cnt)
     TG_CUDA(cudaStreamSynchronize(C->stream));
 }
 
-int poisson_solve(tg_ctx *C, tg_stats *st)
+// Krylov solve of L x = b from the current P.x (P.b set by the caller):
+// preconditioned CG on orthogonal grids, BiCGStab otherwise. Stops at the
+// relative residual rtol or, when divtol > 0, at dt * max|r aj| <= divtol.
+static int krylov_solve(tg_ctx *C, tg_stats *st, double rtol, double divtol, int maxit)
 {
     PoissonCtx &P = *C->pois;
-    const Grid g = C->g;
     const int64_t n = P.n;
     cudaStream_t s = C->stream;
-    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
-    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
-    const double divtol = C->cfg.poisson_div_tol;
     const double dt = C->prm.dt;
     double *sc = C->d_scal;          // device scalar slots 0..7 used below
     double *hs = C->h_scal;
-    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
 
-    TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, dt));
-    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solution
     dot3v(C, P.b, P.b, nullptr, sc + 0);
     apply_op(C, P.x, P.r);
     k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r);   // r = b - L x
@@ -473,7 +473,6 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
         rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
     }
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
-    TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
     TG_CUDA(cudaGetLastError());
     if (st) {
         st->poisson_iterations = it;
@@ -483,5 +482,47 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     if (!std::isfinite(rn)) return 2;
     return ok ? 0 : 1;
 }
+
+int poisson_solve(tg_ctx *C, tg_stats *st)
+{
+    PoissonCtx &P = *C->pois;
+    const Grid g = C->g;
+    cudaStream_t s = C->stream;
+    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
+    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
+    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
+    TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt));
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solution
+    int rc = krylov_solve(C, st, rtol, C->cfg.poisson_div_tol, maxit);
+    TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
+    TG_CUDA(cudaGetLastError());
+    return rc;
+}
+
+// Adjoint pressure solve: lam = A^-T rhs for the pinned operator A of
+// SetCoeffMatrix (rhs and lam compact, pinned entry of rhs ignored,
+// lam[pin] = 0). On orthogonal grids the
+// operator without the pinned row and column is symmetric, so this is the
+// forward Krylov solve with a fresh zero start; the forward warm start P.x is
+// kept. Returns 3 for the non-symmetric curvilinear operator.
+int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st)
+{
+    PoissonCtx &P = *C->pois;
+    if (!P.ortho) return 3;
+    cudaStream_t s = C->stream;
+    const int64_t n = P.n;
+    TG_CUDA(cudaMemcpyAsync(P.v, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_negcopy<<<vblocks(n), RB, 0, s>>>(n, rhs, P.b);       // the solver's operator is L = -A
+    k_zero_at<<<1, 1, 0, s>>>(P.b, P.pin);
+    TG_CUDA(cudaMemsetAsync(P.x, 0, sizeof(double) * n, s));
+    int rc = krylov_solve(C, st, rtol, 0.0, C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500);
+    TG_CUDA(cudaMemcpyAsync(lam, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    TG_CUDA(cudaMemcpyAsync(P.x, P.v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    return rc;
+}
+
+// compact Poisson solution vector (warm start of the next solve): snapshots
+double *poisson_x(tg_ctx *C) { return C->pois->x; }
+int64_t poisson_n(tg_ctx *C) { return C->pois->n; }
 
 }  // namespace tg

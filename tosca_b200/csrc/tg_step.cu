@@ -1125,6 +1125,7 @@ void explicit_rhs(tg_ctx *C)
     reset_face_periodic(C, C->s.ucont);
     contra_to_cart_stage(C);
     reset_cell_periodic(C, C->s.ucat);
+    if (C->taping) tape_stage(C);
     form_u_faces(C);
     // every point outside the interior faces keeps Rhs = -dP + b = 0: zero from
     // the allocation, rewritten here only after a caller wrote Rhs
@@ -1254,7 +1255,9 @@ int step(tg_ctx *C, tg_stats *st)
 {
     const int64_t G = C->g.size();
     TG_CUDA(cudaMemcpyAsync(C->s.ucont_o.x, C->s.ucont.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    if (C->taping) tape_step_start(C);
     if (C->prm.les) { update_nut(C); update_wall_models(C); }
+    if (C->taping) tape_nut(C);
     grad_p(C);
     if (C->prm.buoyancy) {
         if (C->it > C->cfg.it_start)
