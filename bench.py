@@ -215,6 +215,50 @@ def run_reference(args, rank, world):
     return 0
 
 
+def adjoint_ratio(dev, steps=4, warmup=8, cells=(128, 64, 64)):
+    """Adjoint/forward time of the step on the adjoint ABL (128 x 64 x 64 cells,
+    Cartesian, noSlip bottom, Smagorinsky, RK4, body force): device time of
+    tg_step per step against the device time per step of tg_adjoint_reverse
+    (each reversed step re-runs its forward step once to record the stages,
+    then runs the transposed kernels and the transposed pressure solve), with
+    a snapshot per step so that no further recomputation happens."""
+    import tosca_b200
+    from tosca_b200 import api, cases
+    nx, ny, nz = cells
+    cfg, nodes, ucat, p = cases.abl_case(nx=nx, ny=ny, nz=nz, Lx=10.0 * nx, Ly=10.0 * ny, H=1000.0 * nz / 128.0,
+                                         ddt=api.DDT_RK4, wall=api.BC_NOSLIP)
+    cfg.poisson_rtol = 1e-30
+    cfg.poisson_div_tol = DIV_TOL
+    cfg.poisson_maxit = 400
+    cfg.source = 1
+    cfg.device = dev
+    s = tosca_b200.gpu_solver(cfg)
+    cases.setup(s, nodes, ucat, p)
+    rng = np.random.default_rng(4)
+    s.set("SOURCE", rng.standard_normal(ucat.shape) * 1e-3)
+    s.step(warmup)
+    fwd = s.step(steps)
+    inside = np.zeros(p.shape, bool)
+    inside[1:-1, 1:-1, 1:-1] = True
+    seed = rng.standard_normal(ucat.shape) * inside[..., None]
+    out = {"workload": "adjoint ABL %dx%dx%d cells, RK4, Smagorinsky, noSlip bottom, body force, FP64" % (nx, ny, nz),
+           "forward_ms_per_step": fwd.seconds / steps * 1e3, "steps": steps}
+    # (a) every step's tape kept in device memory; (b) half as many snapshots as
+    # steps: binomial checkpointing, each reversed step re-runs its forward step
+    for key, nsnap in (("tapes_kept", steps), ("checkpointed", max(1, steps // 2))):
+        tst = s.adjoint_forward(steps, nsnap)
+        s.set("UCAT_ADJ", seed)
+        s.set("UCONT_ADJ", np.zeros(ucat.shape)); s.set("P_ADJ", np.zeros(p.shape)); s.set("SOURCE_ADJ", np.zeros(ucat.shape))
+        ast = s.adjoint_reverse()
+        a_ms = ast.seconds / steps * 1e3
+        out[key] = {"snapshots": int(ast.snapshots), "forward_steps_in_reversal": int(ast.forward_steps),
+                    "taped_forward_ms_per_step": tst.seconds / steps * 1e3,
+                    "adjoint_ms_per_step": a_ms, "adjoint_over_forward": a_ms / out["forward_ms_per_step"]}
+    s.close()
+    out["adjoint_over_forward"] = out["tapes_kept"]["adjoint_over_forward"]
+    return out
+
+
 def kernel_table(L, h):
     import ctypes
     kernels = {}
@@ -268,6 +312,7 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=2,
                     help="untimed steps after the timed region with per-kernel events on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--profile-json", default=None, help="write per-kernel timings here (one file per arm)")
     ap.add_argument("--cells", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
@@ -390,6 +435,10 @@ def main():
            "h2d_bytes_per_step": int(bytes_state), "d2h_bytes_per_step": int(bytes_state),
            "steps": e2e_steps, "precision": head_prec, "max_divergence": se.max_divergence}
 
+    adj = None
+    if rank == 0 and not args.no_adjoint and args.workload == "abl":
+        adj = adjoint_ratio(dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(args.workload, args.cpu_steps)
@@ -417,6 +466,7 @@ def main():
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "gpu_launches_note": "per-step count of the library's timed launches in the profiled steps x timed steps",
             "roofline": head["roofline"],
+            "adjoint": adj,
             "cpu_baseline": cpu,
             "kernels_top": {k: {"ms_per_step": round(v["ms"] / max(1, args.profile_steps), 3),
                                 "launches_per_step": v["launches"] / max(1, args.profile_steps),

@@ -29,7 +29,11 @@
 // Checkpointing: tg_adjoint_forward runs the forward steps keeping device
 // snapshots of the state at the positions of a binomial (revolve) schedule;
 // tg_adjoint_reverse walks the steps backwards, restoring the nearest
-// snapshot and recomputing forward where the schedule says so.
+// snapshot and recomputing forward where the schedule says so (each reversed
+// step re-runs its own forward step once to record its stages). When there is
+// a snapshot per step and the tapes of all steps fit in 60 % of the free
+// device memory, the forward pass keeps every step's tape instead and the
+// reversal runs no forward step at all.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -46,6 +50,13 @@ struct Snapshot {
     int pos;       // step index of the state held (-1: free)
 };
 
+// forward intermediates of one step
+struct Tape {
+    V3f<double> u_o, ucat_n, ut[4], uc[4];
+    double *nut = nullptr;
+    int nst = 0;
+};
+
 struct AdjState {
     // public adjoint fields
     V3f<double> ua, ca, fa;
@@ -53,10 +64,12 @@ struct AdjState {
     // work
     V3f<double> uoa, usa, uta, cta, ra, dpa, fpa, f1a, f2a, f3a, qa;
     double *pha = nullptr, *na = nullptr, *lam = nullptr, *rhsc = nullptr;
-    // tape of one step
-    V3f<double> t_uo, t_ucatn, t_ut[4], t_uc[4];
-    double *t_nut = nullptr;
-    int nst = 0;
+    // tape of the step being reversed: the work tape, or one of the stored
+    // tapes of a forward run that kept every step's tape
+    Tape work_tape;
+    std::vector<Tape> store;
+    Tape *cur = nullptr;
+    bool stored = false;                 // the last forward run kept every tape
     bool work = false;
     // checkpoints (the last one is the scratch state of an adjoint step)
     std::vector<Snapshot> snaps;
@@ -791,17 +804,27 @@ static AdjState &adj_state(tg_ctx *C)
     return *C->adj;
 }
 
+static Tape make_tape(tg_ctx *C)
+{
+    Tape t;
+    t.u_o = alloc3(C); t.ucat_n = alloc3(C);
+    for (int q = 0; q < 4; q++) { t.ut[q] = alloc3(C); t.uc[q] = alloc3(C); }
+    t.nut = dallocd(C, (size_t)C->g.size());
+    return t;
+}
+static size_t tape_bytes(tg_ctx *C) { return (size_t)C->g.size() * sizeof(double) * (3 * 10 + 1); }
+
 static void adj_work(tg_ctx *C)
 {
     AdjState &A = adj_state(C);
     if (A.work) return;
     const size_t G = (size_t)C->g.size();
-    V3f<double> *v[] = {&A.uoa, &A.usa, &A.uta, &A.cta, &A.ra, &A.dpa, &A.fpa, &A.f1a, &A.f2a, &A.f3a, &A.qa,
-                        &A.t_uo, &A.t_ucatn, &A.t_ut[0], &A.t_ut[1], &A.t_ut[2], &A.t_ut[3],
-                        &A.t_uc[0], &A.t_uc[1], &A.t_uc[2], &A.t_uc[3]};
+    V3f<double> *v[] = {&A.uoa, &A.usa, &A.uta, &A.cta, &A.ra, &A.dpa, &A.fpa, &A.f1a, &A.f2a, &A.f3a, &A.qa};
     for (auto *p : v) *p = alloc3(C);
-    A.pha = dallocd(C, G); A.na = dallocd(C, G); A.t_nut = dallocd(C, G);
+    A.pha = dallocd(C, G); A.na = dallocd(C, G);
     A.lam = dallocd(C, (size_t)poisson_n(C)); A.rhsc = dallocd(C, (size_t)poisson_n(C));
+    A.work_tape = make_tape(C);
+    A.cur = &A.work_tape;
     A.work = true;
 }
 
@@ -834,23 +857,23 @@ static void zero3(tg_ctx *C, V3f<double> v)
 
 void tape_step_start(tg_ctx *C)
 {
-    AdjState &A = *C->adj;
-    copy3(C, A.t_uo, C->s.ucont);
-    copy3(C, A.t_ucatn, C->s.ucat);
-    A.nst = 0;
+    Tape &T = *C->adj->cur;
+    copy3(C, T.u_o, C->s.ucont);
+    copy3(C, T.ucat_n, C->s.ucat);
+    T.nst = 0;
 }
 void tape_nut(tg_ctx *C)
 {
-    AdjState &A = *C->adj;
-    TG_CUDA(cudaMemcpyAsync(A.t_nut, C->s.nut, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
+    Tape &T = *C->adj->cur;
+    TG_CUDA(cudaMemcpyAsync(T.nut, C->s.nut, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
 }
 void tape_stage(tg_ctx *C)
 {
-    AdjState &A = *C->adj;
-    if (A.nst >= 4) return;
-    copy3(C, A.t_ut[A.nst], C->s.ucont);
-    copy3(C, A.t_uc[A.nst], C->s.ucat);
-    A.nst++;
+    Tape &T = *C->adj->cur;
+    if (T.nst >= 4) return;
+    copy3(C, T.ut[T.nst], C->s.ucont);
+    copy3(C, T.uc[T.nst], C->s.ucat);
+    T.nst++;
 }
 
 // reverse per-direction copies
@@ -889,6 +912,7 @@ static bool adjoint_supported(tg_ctx *C, std::string &why)
 static int adjoint_reverse_step(tg_ctx *C)
 {
     AdjState &A = *C->adj;
+    const Tape &T = *A.cur;
     const Grid g = C->g;
     const int64_t G = g.size();
     cudaStream_t st = C->stream;
@@ -916,7 +940,10 @@ static int adjoint_reverse_step(tg_ctx *C)
     adj_scalar_ghosts(C, A.pha);
     k_adj_phi_compact<<<gint(g), block3(), 0, st>>>(g, A.pha, A.rhsc);
     tg_stats ps{};
-    int rc = poisson_solve_adjoint(C, A.rhsc, A.lam, 1e-12, &ps);
+    // started from the previous reversed step's solution, to the context's
+    // relative tolerance when that lies in [1e-14, 1e-10], else to 1e-10
+    const double rt = C->cfg.poisson_rtol;
+    int rc = poisson_solve_adjoint(C, A.rhsc, A.lam, (rt >= 1e-14 && rt < 1e-10) ? rt : 1e-10, &ps);
     if (rc == 3) return 3;
     // SetRHS; u* = utmp after the tail flux resets
     copy3(C, A.usa, A.ua);
@@ -929,18 +956,18 @@ static int adjoint_reverse_step(tg_ctx *C)
     TG_CUDA(cudaMemsetAsync(A.na, 0, sizeof(double) * G, st));
     const double bw[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
     const double aw[4] = {0.0, 0.5, 0.5, 1.0};
-    const bool rk = A.nst == 4;
-    for (int s = A.nst - 1; s >= 0; s--) {
+    const bool rk = T.nst == 4;
+    for (int s = T.nst - 1; s >= 0; s--) {
         double cb = dt * (rk ? bw[s] : 1.0);
         double cn = (rk && s < 3) ? aw[s + 1] * dt : 0.0;
-        TG_PROF(C, "adj_stage_rhs", k_adj_stage_rhs<<<gall(g), block3(), 0, st>>>(g, A.ra, A.usa, A.uta, cb, cn, A.t_uo, A.dpa));
+        TG_PROF(C, "adj_stage_rhs", k_adj_stage_rhs<<<gall(g), block3(), 0, st>>>(g, A.ra, A.usa, A.uta, cb, cn, T.u_o, A.dpa));
         if (C->prm.source) TG_PROF(C, "adj_source", k_adj_source<<<gall(g), block3(), 0, st>>>(g, C->m, A.ra, A.fa));
         // FormU transposed
         TG_PROF(C, "adj_rhs_faces", k_adj_rhs_faces<<<gint(g), block3(), 0, st>>>(g, C->m, A.ra, 1.0, A.fpa));
         TG_PROF(C, "adj_cell_fp", k_adj_cell_fp<<<gfc(g), block3(), 0, st>>>(g, A.fpa, A.f1a, A.f2a, A.f3a));
         zero3(C, A.uta);
         zero3(C, A.cta);
-        TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<<<gfc(g), block3(), 0, st>>>(g, C->m, A.t_ut[s], A.t_uc[s], A.t_nut, C->prm,
+        TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<<<gfc(g), block3(), 0, st>>>(g, C->m, T.ut[s], T.uc[s], T.nut, C->prm,
                                                                                     A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na));
         // stage Ucat: periodic copies, interior from contravariantToCartesian, other ghosts from the state Ucat
         adj_periodic(C, A.cta, 0);
@@ -958,7 +985,7 @@ static int adjoint_reverse_step(tg_ctx *C)
         int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
         dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
         k_adj_nut_bcs<<<grid, b2, 0, st>>>(g, A.na, C->prm);
-        TG_PROF(C, "adj_smagorinsky", k_adj_smagorinsky<<<gint(g), block3(), 0, st>>>(g, C->m, A.t_ucatn, A.na, C->prm, A.ca));
+        TG_PROF(C, "adj_smagorinsky", k_adj_smagorinsky<<<gint(g), block3(), 0, st>>>(g, C->m, T.ucat_n, A.na, C->prm, A.ca));
     }
     copy3(C, A.ua, A.uoa);
     TG_CUDA(cudaGetLastError());
@@ -996,6 +1023,7 @@ static void restore_state(tg_ctx *C, const Snapshot &s)
 // one adjoint step at the current state: taped forward step, restore, reverse
 static int adjoint_step_here(tg_ctx *C, Snapshot &scratch)
 {
+    C->adj->cur = &C->adj->work_tape;
     save_state(C, scratch, -2);
     C->taping = true;
     tg_stats fs{};
@@ -1143,8 +1171,19 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         if (nsteps < 1 || nsnap < 1) { C->err = "nsteps and nsnap must be positive"; return TG_ERR_BAD_ARG; }
         AdjState &A = adj_state(C);
         adj_work(C);
+        // With a snapshot per step and room in device memory, every step's tape
+        // is kept during this pass and the reversal re-runs no forward step.
+        bool store = nsnap >= nsteps;
+        if (store) {
+            size_t freeb = 0, totalb = 0;
+            TG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+            const size_t need = tape_bytes(C) * (size_t)std::max(0, nsteps - (int)A.store.size());
+            store = need <= freeb / 10 * 6;
+        }
+        if (store) while ((int)A.store.size() < nsteps) A.store.push_back(make_tape(C));
+        A.stored = store;
         // nsnap snapshots for the schedule plus one scratch state of the adjoint step
-        const int want = std::min(nsnap, nsteps) + 1;
+        const int want = store ? 2 : std::min(nsnap, nsteps) + 1;
         while ((int)A.snaps.size() < want) A.snaps.push_back(make_snapshot(C));
         while ((int)A.snaps.size() > want) A.snaps.pop_back();     // buffers stay owned by the context
         for (auto &sp : A.snaps) sp.pos = -1;
@@ -1167,8 +1206,11 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         save_state(C, A.snaps[0], 0);
         size_t next = 0;
+        if (store) keep.clear();
         for (int n = 0; n < nsteps; n++) {
+            if (store) { A.cur = &A.store[n]; C->taping = true; }
             int rc = step(C, st);
+            C->taping = false;
             st->steps += 1;
             if (rc == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
             if (next < keep.size() && keep[next] == n + 1) { save_state(C, A.snaps[next + 1], n + 1); next++; }
@@ -1198,7 +1240,16 @@ tg_status tg_adjoint_reverse(tg_ctx *C, tg_adjoint_stats *stats)
         Revolve R;
         R.build(A.nsteps, (int)A.snaps.size() - 2);
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
-        reverse_range(C, R, 0, A.nsteps, 0, st);
+        if (A.stored) {
+            for (int n = A.nsteps - 1; n >= 0; n--) {
+                A.cur = &A.store[n];
+                int rc = adjoint_reverse_step(C);
+                if (rc) { C->err = "adjoint pressure solve failed"; return rc == 3 ? TG_ERR_BAD_ARG : TG_ERR_NOT_CONVERGED; }
+                st->steps += 1;
+            }
+        } else {
+            reverse_range(C, R, 0, A.nsteps, 0, st);
+        }
         restore_state(C, A.snaps[0]);
         TG_CUDA(cudaEventRecord(C->ev1, C->stream));
         TG_CUDA(cudaEventSynchronize(C->ev1));

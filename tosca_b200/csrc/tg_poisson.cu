@@ -501,10 +501,11 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
 
 // Adjoint pressure solve: lam = A^-T rhs for the pinned operator A of
 // SetCoeffMatrix (rhs and lam compact, pinned entry of rhs ignored,
-// lam[pin] = 0). On orthogonal grids the
-// operator without the pinned row and column is symmetric, so this is the
-// forward Krylov solve with a fresh zero start; the forward warm start P.x is
-// kept. Returns 3 for the non-symmetric curvilinear operator.
+// lam[pin] = 0). On orthogonal grids the operator without the pinned row and
+// column is symmetric, so this is the forward Krylov solve started from the
+// value lam holds on entry (the previous reversed step's solution); the
+// forward warm start P.x is kept. Returns 3 for the non-symmetric curvilinear
+// operator.
 int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st)
 {
     PoissonCtx &P = *C->pois;
@@ -514,7 +515,7 @@ int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol
     TG_CUDA(cudaMemcpyAsync(P.v, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     k_negcopy<<<vblocks(n), RB, 0, s>>>(n, rhs, P.b);       // the solver's operator is L = -A
     k_zero_at<<<1, 1, 0, s>>>(P.b, P.pin);
-    TG_CUDA(cudaMemsetAsync(P.x, 0, sizeof(double) * n, s));
+    TG_CUDA(cudaMemcpyAsync(P.x, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     int rc = krylov_solve(C, st, rtol, 0.0, C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500);
     TG_CUDA(cudaMemcpyAsync(lam, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     TG_CUDA(cudaMemcpyAsync(P.x, P.v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
