@@ -242,7 +242,8 @@ def adjoint_ratio(dev, steps=4, warmup=8, cells=(128, 64, 64)):
     inside[1:-1, 1:-1, 1:-1] = True
     seed = rng.standard_normal(ucat.shape) * inside[..., None]
     out = {"workload": "adjoint ABL %dx%dx%d cells, RK4, Smagorinsky, noSlip bottom, body force, FP64" % (nx, ny, nz),
-           "forward_ms_per_step": fwd.seconds / steps * 1e3, "steps": steps}
+           "forward_ms_per_step": fwd.seconds / steps * 1e3, "steps": steps,
+           "forward_poisson_iterations_per_step": fwd.poisson_total_iterations / steps}
     # (a) every step's tape kept in device memory; (b) half as many snapshots as
     # steps: binomial checkpointing, each reversed step re-runs its forward step
     for key, nsnap in (("tapes_kept", steps), ("checkpointed", max(1, steps // 2))):
@@ -252,6 +253,7 @@ def adjoint_ratio(dev, steps=4, warmup=8, cells=(128, 64, 64)):
         ast = s.adjoint_reverse()
         a_ms = ast.seconds / steps * 1e3
         out[key] = {"snapshots": int(ast.snapshots), "forward_steps_in_reversal": int(ast.forward_steps),
+                    "adjoint_poisson_iterations_per_step": ast.poisson_iterations / steps,
                     "taped_forward_ms_per_step": tst.seconds / steps * 1e3,
                     "adjoint_ms_per_step": a_ms, "adjoint_over_forward": a_ms / out["forward_ms_per_step"]}
     s.close()

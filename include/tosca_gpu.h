@@ -207,6 +207,7 @@ typedef struct tg_adjoint_stats {
     int64_t steps;                 /* steps reversed                                        */
     int64_t forward_steps;         /* forward steps run by the reversal (recomputation)     */
     int32_t snapshots;             /* device snapshots of the checkpoint schedule           */
+    int32_t poisson_iterations;    /* Krylov iterations of the transposed pressure solves   */
     double  seconds;               /* device time of the call                               */
 } tg_adjoint_stats;
 

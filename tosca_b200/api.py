@@ -69,6 +69,7 @@ class TgAdjointStats(C.Structure):
         ("steps", C.c_int64),
         ("forward_steps", C.c_int64),
         ("snapshots", C.c_int32),
+        ("poisson_iterations", C.c_int32),
         ("seconds", C.c_double),
     ]
 
