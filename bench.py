@@ -373,9 +373,11 @@ def main():
         barrier()
         torch.cuda.synchronize()
         with ClockSampler(dev) as clk:
+            r0 = solver.graph_info()[0]
             st = solver.step(args.steps)
             torch.cuda.synchronize()
         barrier()
+        replayed = solver.graph_info()[0] - r0
         t_dev = max_over_ranks(st.seconds)
         # per-kernel events on a few further steps (outside the timed region)
         L.tg_prof_reset(solver.h)
@@ -385,6 +387,7 @@ def main():
         L.tg_prof_enable(solver.h, 0)
         kernels = kernel_table(L, solver.h)
         return {"cfg": cfg, "desc": desc, "solver": solver, "st": st, "t_dev": t_dev, "clocks": clk.summary(),
+                "replayed": replayed,
                 "value": cfg.cells * args.steps * world / t_dev / 1e6, "kernels": kernels,
                 "roofline": roofline_of(kernels, precision, cfg.cells)}
 
@@ -462,7 +465,8 @@ def main():
                        "l2": "every field exceeds the 126 MB L2; no flush",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "poisson_iterations_per_step": st.poisson_total_iterations / max(1, args.steps),
-                       "max_divergence": st.max_divergence},
+                       "max_divergence": st.max_divergence,
+                       "steps_replayed_from_cuda_graph": head["replayed"]},
             "clocks": head["clocks"],
             "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),

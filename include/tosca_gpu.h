@@ -195,6 +195,19 @@ tg_status tg_sync_pressure(tg_ctx *ctx);               /* overset.h:107 / overse
 /* nsteps full time steps in the order of main.c:54-327 (fixed dt). */
 tg_status tg_step(tg_ctx *ctx, int32_t nsteps, tg_stats *stats);
 
+/* Step replay (default on; no reference counterpart): from the second step on,
+ * a step on an orthogonal grid is captured once into a CUDA graph whose
+ * pressure-solver loop runs under device-side control, and replayed after
+ * that, with the same arithmetic as the step launched kernel by kernel. With
+ * it on, tg_step runs every requested step (a non-finite residual is reported
+ * at the end of the call rather than stopping it). on = 0 launches every step
+ * kernel by kernel, as profiling and taping do. */
+tg_status tg_set_graphs(tg_ctx *ctx, int32_t on);
+/* Steps replayed from the captured graph since the context was created, and
+ * whether capture failed for this configuration (steps then run kernel by
+ * kernel). */
+tg_status tg_graph_info(tg_ctx *ctx, int64_t *replays, int32_t *capture_failed);
+
 /* ----------------------------------------------------------------- adjoint -- */
 /* Discrete adjoint of tg_step. No counterpart in the reference: TOSCA has no
  * adjoint. Adjoint fields are exchanged with tg_set_field / tg_get_field

@@ -21,9 +21,9 @@ def declared_symbols():
 # context-free device-pointer entry point: bound directly by its test, and not
 # exported by the CPU restatement
 NO_CONTEXT = {"tg_continuity_error_noalloc"}
-# checkpointed adjoint drivers: device snapshots, the CPU restatement has the
-# per-step adjoint only
-GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse"}
+# checkpointed adjoint drivers (device snapshots: the CPU restatement has the
+# per-step adjoint only) and the CUDA-graph replay switch
+GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse", "tg_set_graphs", "tg_graph_info"}
 
 
 def test_header_matches_bindings():

@@ -162,11 +162,14 @@ _SIGS = {
     "step_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
 }
 
-# adjoint entry points (the CPU restatement exports tor_adjoint_step only)
+# adjoint entry points (the CPU restatement exports tor_adjoint_step only) and
+# the step-replay switch of the CUDA library
 _ADJ_SIGS = {
     "adjoint_step": (C.c_int, [C.c_void_p]),
     "adjoint_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TgStats)]),
     "adjoint_reverse": (C.c_int, [C.c_void_p, C.POINTER(TgAdjointStats)]),
+    "set_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
+    "graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
 }
 
 ENTRY_POINTS = tuple(_SIGS) + tuple(_ADJ_SIGS)
@@ -330,6 +333,16 @@ class Solver:
         st = TgAdjointStats()
         self._check(self.fns["adjoint_reverse"](self.h, C.byref(st)), "adjoint_reverse")
         return st
+
+    def set_graphs(self, on: bool):
+        """Replay steps as CUDA graphs (default on) or launch them kernel by kernel."""
+        self._check(self.fns["set_graphs"](self.h, 1 if on else 0), "set_graphs")
+
+    def graph_info(self) -> tuple:
+        """(steps replayed from the captured graph, capture failed)."""
+        n, f = C.c_int64(), C.c_int32()
+        self._check(self.fns["graph_info"](self.h, C.byref(n), C.byref(f)), "graph_info")
+        return n.value, bool(f.value)
 
     def step_host(self, ucont, ucat, p, nut=None, halo: int = 0) -> TgStats:
         st = TgStats()

@@ -1022,6 +1022,7 @@ static void restore_state(tg_ctx *C, const Snapshot &s)
     TG_CUDA(cudaMemcpyAsync(C->s.p, s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_x(C), s.px, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     C->it = s.it;
+    set_device_step(C);
 }
 
 // one adjoint step at the current state: taped forward step, restore, reverse
@@ -1207,20 +1208,23 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         tg_stats local{};
         tg_stats *st = stats ? stats : &local;
         *st = tg_stats{};
+        step_stats_reset(C);
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         save_state(C, A.snaps[0], 0);
         size_t next = 0;
         if (store) keep.clear();
+        bool any = false, last = false;
         for (int n = 0; n < nsteps; n++) {
             if (store) { A.cur = &A.store[n]; C->taping = true; }
-            int rc = step(C, st);
+            int rc = step(C, st, &last);
+            any |= last;
             C->taping = false;
             st->steps += 1;
             if (rc == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
             if (next < keep.size() && keep[next] == n + 1) { save_state(C, A.snaps[next + 1], n + 1); next++; }
         }
         TG_CUDA(cudaEventRecord(C->ev1, C->stream));
-        TG_CUDA(cudaEventSynchronize(C->ev1));
+        if (step_stats_read(C, st, any, last) == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
         float ms = 0.f;
         TG_CUDA(cudaEventElapsedTime(&ms, C->ev0, C->ev1));
         st->seconds = ms * 1e-3;

@@ -246,6 +246,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         C->red_blocks = 148 * 4;
         C->d_red = dallocd(C, 4 * (size_t)C->red_blocks + 64);
         C->d_scal = dallocd(C, 128);
+        set_device_step(C);
         TG_CUDA(cudaMallocHost((void **)&C->h_scal, 128 * sizeof(double)));
         std::memset(C->h_scal, 0, 128 * sizeof(double));
         TG_CUDA(cudaStreamSynchronize(C->stream));
@@ -266,6 +267,8 @@ tg_status tg_destroy(tg_ctx *C)
     if (!C) return TG_OK;
     cudaSetDevice(C->cfg.device);
     if (C->stream) cudaStreamSynchronize(C->stream);
+    graph_destroy(C);
+    if (C->aux[0]) cudaStreamDestroy(C->aux[0]);
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);
@@ -298,6 +301,8 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
             for (double v : h) mx = std::max(mx, std::fabs(v));
         }
         C->orthogonal = (mx == 0.0);
+        graph_destroy(C);          // the captured step refers to the old solver buffers
+        C->graph_failed = false;
         poisson_setup(C);
         C->has_mesh = true;
         return TG_OK;
@@ -431,17 +436,21 @@ tg_status tg_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
         tg_stats local{};
         tg_stats *s = st ? st : &local;
         *s = tg_stats{};
+        step_stats_reset(C);
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         int rc = 0;
+        bool any = false, last = false;
         for (int n = 0; n < nsteps; n++) {
-            int r = step(C, s);
+            int r = step(C, s, &last);
+            any |= last;
             s->steps++;
             if (r == 2) { rc = 2; break; }
             rc |= r;
         }
         TG_CUDA(cudaEventRecord(C->ev1, C->stream));
-        TG_CUDA(cudaMemcpyAsync(C->h_scal + 16, C->d_scal + 16, sizeof(double), cudaMemcpyDeviceToHost, C->stream));
-        TG_CUDA(cudaStreamSynchronize(C->stream));
+        const int gr = step_stats_read(C, s, any, last);
+        if (gr == 2) rc = 2;
+        else if (rc != 2) rc |= gr;
         float ms = 0.f;
         TG_CUDA(cudaEventElapsedTime(&ms, C->ev0, C->ev1));
         s->seconds = ms * 1e-3;
@@ -449,6 +458,26 @@ tg_status tg_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
         check_nan(C);
         if (rc == 2) return fail(C, TG_ERR_NAN, "non-finite residual in the pressure solve");
         return rc ? fail(C, TG_ERR_NOT_CONVERGED, "pressure solve reached its iteration cap") : TG_OK;
+    });
+}
+
+tg_status tg_set_graphs(tg_ctx *C, int32_t on)
+{
+    return guarded(C, [&]() -> tg_status {
+        C->graphs = on != 0;
+        if (!C->graphs) graph_destroy(C);
+        C->graph_failed = false;
+        return TG_OK;
+    });
+}
+
+tg_status tg_graph_info(tg_ctx *C, int64_t *replays, int32_t *capture_failed)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!replays || !capture_failed) return fail(C, TG_ERR_BAD_ARG, "null output");
+        *replays = C->replays;
+        *capture_failed = C->graph_failed ? 1 : 0;
+        return TG_OK;
     });
 }
 
@@ -464,14 +493,16 @@ tg_status tg_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double
         tg_stats local{};
         tg_stats *s = st ? st : &local;
         *s = tg_stats{};
-        int rc = step(C, s);
+        step_stats_reset(C);
+        bool rep = false;
+        int rc = step(C, s, &rep);
         s->steps = 1;
         download(C, ucont, halo, C->s.ucont.x, C->s.ucont.y, C->s.ucont.z);
         download(C, ucat, halo, C->s.ucat.x, C->s.ucat.y, C->s.ucat.z);
         download(C, p, halo, C->s.p, nullptr, nullptr);
         if (nut && C->prm.les) download(C, nut, halo, C->s.nut, nullptr, nullptr);
-        TG_CUDA(cudaMemcpyAsync(C->h_scal + 16, C->d_scal + 16, sizeof(double), cudaMemcpyDeviceToHost, C->stream));
-        TG_CUDA(cudaStreamSynchronize(C->stream));
+        const int gr = step_stats_read(C, s, rep, rep);
+        if (rep) rc = gr;
         s->max_divergence = C->h_scal[16];
         if (rc == 2) return fail(C, TG_ERR_NAN, "non-finite residual in the pressure solve");
         return rc ? fail(C, TG_ERR_NOT_CONVERGED, "pressure solve reached its iteration cap") : TG_OK;

@@ -157,6 +157,13 @@ struct tg_ctx {
     tg::PoissonCtx *pois = nullptr;
     tg::AdjState *adj = nullptr;         // adjoint fields, tape and checkpoints (tg_adjoint.cu)
     bool taping = false;                 // the running step records its stage states
+    // CUDA graph of a whole step (tg_step.cu): built on the first step that can
+    // be captured, replayed afterwards
+    cudaGraphExec_t step_exec = nullptr;
+    bool graphs = true;                  // tg_set_graphs
+    int64_t replays = 0;
+    bool graph_failed = false;
+    cudaStream_t aux[2] = {nullptr, nullptr};   // capture streams of conditional bodies
     tg::Profiler prof;
 };
 
@@ -224,7 +231,12 @@ int solve_p(tg_ctx *C, tg_stats *st);
 double continuity_error(tg_ctx *C);
 void sync_pressure(tg_ctx *C);
 void init_from_cartesian(tg_ctx *C);
-int step(tg_ctx *C, tg_stats *st);
+int step(tg_ctx *C, tg_stats *st, bool *replayed = nullptr);
+void step_stats_reset(tg_ctx *C);            // zero the SC_G* slots before a run of steps
+// after a run of steps: copy d_scal[16..66) to h_scal, merge the statistics of
+// replayed steps into s (last: the final step was replayed); returns 0, 1
+// (iteration cap) or 2 (non-finite residual) for the replayed steps
+int step_stats_read(tg_ctx *C, tg_stats *s, bool any, bool last);
 
 // device reductions (tg_reduce.cu): result written to d_out[0]
 void reduce_max_abs_div(tg_ctx *C, double *d_out);
@@ -233,6 +245,11 @@ void reduce_max_abs_div(tg_ctx *C, double *d_out);
 void poisson_setup(tg_ctx *C);
 void poisson_destroy(tg_ctx *C);
 int poisson_solve(tg_ctx *C, tg_stats *st);
+void poisson_solve_capture(tg_ctx *C);       // the same solve with device-side loop control
+// device scalar slots (C->d_scal) of the captured solve and the step counter
+constexpr int SC_GIT = 60, SC_GRES0 = 61, SC_GRES = 62, SC_GTOT = 63, SC_GNOCONV = 64, SC_GNAN = 65, SC_IT = 66;
+void set_device_step(tg_ctx *C);             // C->d_scal[SC_IT] <- C->it
+void graph_destroy(tg_ctx *C);
 
 // adjoint (tg_adjoint.cu)
 void tape_step_start(tg_ctx *C);

@@ -283,6 +283,49 @@ __global__ void k_bicg_x(int64_t n, const double *alpha, const double *ts, const
     }
 }
 
+// ---- loop control of the captured CG solve (device scalars: sc[50] iteration
+// count, sc[51] first-direction flag, sc[52] converged flag). The tests are
+// those of krylov_solve; a non-finite residual also ends the loop.
+__device__ inline bool cg_converged(const double *sc, double rtol, double divtol, double dt)
+{
+    const double bn = sqrt(sc[0]), rn = sqrt(sc[3]), rmax = sc[5] * dt;
+    return bn == 0.0 || rn / bn <= rtol || (divtol > 0 && rmax <= divtol);
+}
+__global__ void k_cg_start(double *sc, double rtol, double divtol, double dt, int maxit, cudaGraphConditionalHandle h)
+{
+    const double bn = sqrt(sc[0]), rn = sqrt(sc[3]);
+    const bool conv = cg_converged(sc, rtol, divtol, dt);
+    sc[SC_GRES0] = bn > 0 ? rn / bn : rn;
+    sc[50] = 0.0; sc[51] = 1.0; sc[52] = conv ? 1.0 : 0.0;
+    cudaGraphSetConditional(h, (!conv && maxit > 0 && isfinite(rn)) ? 1u : 0u);
+}
+__global__ void k_cg_next(double *sc, double rtol, double divtol, double dt, int maxit, cudaGraphConditionalHandle h)
+{
+    const double rn = sqrt(sc[3]);
+    const int it = (int)sc[50] + 1;
+    const bool conv = cg_converged(sc, rtol, divtol, dt);
+    sc[50] = it; sc[51] = 0.0; sc[52] = conv ? 1.0 : 0.0;
+    cudaGraphSetConditional(h, (!conv && it < maxit && isfinite(rn)) ? 1u : 0u);
+}
+// statistics of the solve, accumulated over the replayed steps
+__global__ void k_cg_finish(double *sc)
+{
+    const double bn = sqrt(sc[0]), rn = sqrt(sc[3]);
+    sc[SC_GIT] = sc[50];
+    sc[SC_GTOT] += sc[50];
+    sc[SC_GRES] = bn > 0 ? rn / bn : rn;
+    if (!isfinite(rn)) sc[SC_GNAN] = 1.0;
+    else if (sc[52] == 0.0) sc[SC_GNOCONV] += 1.0;
+}
+// p = z on the first pass through the loop body, else p = z + (rz_new / rz_old) p
+__global__ void k_cg_dir_loop(int64_t n, const double *sc, const double *z, double *p)
+{
+    const bool first = sc[51] != 0.0;
+    const double beta = first ? 0.0 : sc[6] / sc[14];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        p[t] = first ? z[t] : z[t] + beta * p[t];
+}
+
 inline dim3 cgrid(int nx, int ny, int nz) { return grid3(nx, ny, nz); }
 inline int vblocks(int64_t n) { int64_t b = (n + RB - 1) / RB; return (int)std::min<int64_t>(b, 148 * 8); }
 
@@ -497,6 +540,77 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
     TG_CUDA(cudaGetLastError());
     return rc;
+}
+
+// poisson_solve for a step being captured into a CUDA graph (orthogonal
+// grids): the CG iterations form a conditional WHILE node whose condition a
+// one-thread kernel sets from the device residuals, so the solve needs no
+// host round trip per iteration. The loop body is krylov_solve's iteration
+// rotated to start with the direction update (p = z on the first pass), which
+// performs the same arithmetic in the same order; statistics go to the
+// SC_G* device slots.
+void poisson_solve_capture(tg_ctx *C)
+{
+    PoissonCtx &P = *C->pois;
+    const Grid g = C->g;
+    cudaStream_t s = C->stream;
+    const int64_t n = P.n;
+    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
+    const double divtol = C->cfg.poisson_div_tol;
+    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
+    const double dt = C->prm.dt;
+    double *sc = C->d_scal;
+    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
+    k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, dt);
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
+    dot3v(C, P.b, P.b, nullptr, sc + 0);
+    apply_op(C, P.x, P.r);
+    k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r);
+    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    TG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) throw CudaError{cudaErrorStreamCaptureInvalidated, "poisson_solve_capture: stream not capturing"};
+    cudaGraphConditionalHandle h;
+    TG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
+    TG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &nd));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TG_CUDA(cudaGraphAddNode(&node, graph, deps, nd, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    TG_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+
+    // loop body, captured on the auxiliary stream into the node's body graph
+    cudaStream_t a = C->aux[0];
+    TG_CUDA(cudaStreamBeginCaptureToGraph(a, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    struct Swap { tg_ctx *C; cudaStream_t keep; ~Swap() { C->stream = keep; } } sw{C, s};
+    C->stream = a;
+    precondition(C, P.r, P.z, sc + 4);
+    k_scalar_copy<<<1, 1, 0, a>>>(sc + 6, sc + 14, 1);           // rz_old
+    dot3v(C, P.r, P.z, nullptr, sc + 6);                          // rz
+    k_cg_dir_loop<<<vblocks(n), RB, 0, a>>>(n, sc, P.z, P.p);
+    apply_op(C, P.p, P.q);
+    k_zero_at<<<1, 1, 0, a>>>(P.q, P.pin);
+    dot3v(C, P.p, P.q, nullptr, sc + 9);                          // pq
+    k_cg_update<<<vblocks(n), RB, 0, a>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q);
+    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);      // rr, sum r, max|r aj|
+    k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
+    C->stream = s;
+    cudaGraph_t captured;
+    TG_CUDA(cudaStreamEndCapture(a, &captured));
+
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
+    k_cg_finish<<<1, 1, 0, s>>>(sc);
+    k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P);
+    TG_CUDA(cudaGetLastError());
 }
 
 // Adjoint pressure solve: lam = A^-T rhs for the pinned operator A of

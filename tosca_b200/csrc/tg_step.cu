@@ -384,11 +384,14 @@ __global__ void k_wall_init_filter(Grid g, Metrics m, State s)
     s.ufx[w] = Up.x; s.ufy[w] = Up.y; s.ufz[w] = Up.z;
 }
 
-__global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double *wsc, double m1, double m2)
+// d_it: the step counter (the running mean of |U_parallel| weights the old
+// mean by it / (it + 1))
+__global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double *wsc, const double *d_it)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.mx - 2 || k > g.mz - 2) return;
     const double Umean = wsc[0], uStar = wsc[2];
+    const double aN = d_it[0], m1 = aN / (aN + 1.0), m2 = 1.0 / (aN + 1.0);
     int c = g.lin(k, 1, i), w = k * g.mx + i;
     R3<double> Up, n; wall_parallel(g, m, s, k, i, Up, n);
     double upm = sqrt(dot3(Up, Up));
@@ -1064,8 +1067,7 @@ void update_wall_models(tg_ctx *C)
         k_wall_init_filter<<<grid, b2, 0, C->stream>>>(g, C->m, C->s);
         C->ufilt_set = true;
     }
-    double aN = (double)C->it;
-    TG_PROF(C, "wall_stress", k_wall_stress<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_scal + 8, aN / (aN + 1.0), 1.0 / (aN + 1.0)));
+    TG_PROF(C, "wall_stress", k_wall_stress<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_scal + 8, C->d_scal + SC_IT));
 }
 
 // GradP writes the faces of interior cells; dP is zero elsewhere from its
@@ -1250,8 +1252,15 @@ void init_from_cartesian(tg_ctx *C)
     update_contravariant_bcs(C);
 }
 
-// one time step in the order of main.c:54-327
-int step(tg_ctx *C, tg_stats *st)
+__global__ void k_set_scalar(double *a, double v) { a[0] = v; }
+__global__ void k_incr_scalar(double *a) { a[0] += 1.0; }
+
+void set_device_step(tg_ctx *C) { k_set_scalar<<<1, 1, 0, C->stream>>>(C->d_scal + SC_IT, (double)C->it); }
+
+// one time step in the order of main.c:54-327; capture: the step is being
+// recorded into a CUDA graph (device-side Poisson loop, statistics in the
+// SC_G* device slots)
+static int step_body(tg_ctx *C, tg_stats *st, bool capture)
 {
     const int64_t G = C->g.size();
     TG_CUDA(cudaMemcpyAsync(C->s.ucont_o.x, C->s.ucont.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
@@ -1265,12 +1274,110 @@ int step(tg_ctx *C, tg_stats *st)
         buoyancy(C);
     }
     solve_u_impl(C, false);
-    int rc = solve_p(C, st);
+    int rc = 0;
+    if (capture) poisson_solve_capture(C);
+    else rc = poisson_solve(C, st);
+    pressure_update_and_project(C);
     contra_to_cart(C);
     reduce_max_abs_div(C, C->d_scal + 16);
     update_cartesian_bcs(C);
     update_contravariant_bcs(C);
     sync_pressure(C);
+    k_incr_scalar<<<1, 1, 0, C->stream>>>(C->d_scal + SC_IT);
+    return rc;
+}
+
+// A step replays as one CUDA graph once every choice the host makes in it is
+// fixed: after the first step (Adams-Bashforth flag, btheta_o copy), with the
+// wall filter seeded, no pending clear of a caller-written Rhs or dP, the FP32
+// metric copies current, profiling and taping off, and CG (orthogonal grids)
+// as the Krylov method.
+static bool graph_eligible(const tg_ctx *C)
+{
+    const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
+    return C->graphs && !C->graph_failed && !C->prof.on && !C->taping && C->orthogonal && C->pois &&
+           C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !C->met32_stale;
+}
+
+void graph_destroy(tg_ctx *C)
+{
+    if (C->step_exec) cudaGraphExecDestroy(C->step_exec);
+    C->step_exec = nullptr;
+}
+
+static void graph_build(tg_ctx *C)
+{
+    if (!C->aux[0]) TG_CUDA(cudaStreamCreateWithFlags(&C->aux[0], cudaStreamNonBlocking));
+    cudaStream_t s = C->stream;
+    cudaGraph_t graph = nullptr;
+    TG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        step_body(C, nullptr, true);
+    } catch (...) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t part = nullptr;
+        if (cudaStreamIsCapturing(C->aux[0], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+            cudaStreamEndCapture(C->aux[0], &part);   // the body graph belongs to its conditional node
+        part = nullptr;
+        cudaStreamEndCapture(s, &part);
+        if (part) cudaGraphDestroy(part);
+        C->stream = s;
+        throw;
+    }
+    TG_CUDA(cudaStreamEndCapture(s, &graph));
+    cudaError_t e = cudaGraphInstantiate(&C->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { C->step_exec = nullptr; throw CudaError{e, "cudaGraphInstantiate"}; }
+}
+
+void step_stats_reset(tg_ctx *C)
+{
+    TG_CUDA(cudaMemsetAsync(C->d_scal + SC_GIT, 0, sizeof(double) * (SC_IT - SC_GIT), C->stream));
+}
+
+int step_stats_read(tg_ctx *C, tg_stats *s, bool any, bool last)
+{
+    TG_CUDA(cudaMemcpyAsync(C->h_scal + 16, C->d_scal + 16, sizeof(double) * (SC_IT - 16), cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+    if (!any) return 0;
+    const double *h = C->h_scal;
+    s->poisson_total_iterations += (int32_t)h[SC_GTOT];
+    if (last) {
+        s->poisson_iterations = (int32_t)h[SC_GIT];
+        s->poisson_initial_residual = h[SC_GRES0];
+        s->poisson_final_residual = h[SC_GRES];
+    }
+    if (h[SC_GNAN] != 0.0) return 2;
+    return h[SC_GNOCONV] > 0.0 ? 1 : 0;
+}
+
+// One step: a replay of the captured step graph when the step qualifies,
+// else the eager sequence with a host-side Poisson loop. Returns 0, or for an
+// eager step 1 (iteration cap) / 2 (non-finite residual); a replayed step
+// reports through the SC_G* slots read by the caller.
+int step(tg_ctx *C, tg_stats *st, bool *replayed)
+{
+    if (replayed) *replayed = false;
+    if (graph_eligible(C)) {
+        if (!C->step_exec) {
+            try {
+                graph_build(C);
+            } catch (const CudaError &) {
+                // capture is unsupported for this configuration: stay eager
+                cudaGetLastError();
+                graph_destroy(C);
+                C->graph_failed = true;
+            }
+        }
+        if (C->step_exec) {
+            TG_CUDA(cudaGraphLaunch(C->step_exec, C->stream));
+            C->it++;
+            C->replays++;
+            if (replayed) *replayed = true;
+            return 0;
+        }
+    }
+    int rc = step_body(C, st, false);
     C->it++;
     return rc;
 }
