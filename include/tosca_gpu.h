@@ -196,9 +196,9 @@ tg_status tg_sync_pressure(tg_ctx *ctx);               /* overset.h:107 / overse
 tg_status tg_step(tg_ctx *ctx, int32_t nsteps, tg_stats *stats);
 
 /* Step replay (default on; no reference counterpart): from the second step on,
- * a step on an orthogonal grid is captured once into a CUDA graph whose
- * pressure-solver loop runs under device-side control, and replayed after
- * that, with the same arithmetic as the step launched kernel by kernel. With
+ * a step is captured once into a CUDA graph whose pressure-solver loop runs
+ * under device-side control, and replayed after that, with the same
+ * arithmetic as the step launched kernel by kernel. With
  * it on, tg_step runs every requested step (a non-finite residual is reported
  * at the end of the call rather than stopping it). on = 0 launches every step
  * kernel by kernel, as profiling and taping do. */

@@ -47,9 +47,8 @@ def test_replay_bitwise(name, prec):
     assert se.steps == sr.steps == 6
     replays, failed = r.graph_info()
     assert not failed
-    # the first step runs eagerly (first-step branches); curvilinear grids
-    # (BiCGStab) are not captured
-    assert replays == (0 if name == "hill" else 5)
+    # the first step runs eagerly (first-step branches)
+    assert replays == 5
     assert e.graph_info()[0] == 0
     e.close(); r.close()
 
@@ -106,4 +105,20 @@ def test_graphs_off_then_on():
     r.step(2)
     e.step(4)
     assert_same(e, r)
+    e.close(); r.close()
+
+
+def test_replay_bicgstab_restart():
+    # an unreachable tolerance runs the curvilinear solve to its iteration cap,
+    # through the restart from the true residual at iteration 50
+    e, r = twin("hill", {"poisson_rtol": 1e-17, "poisson_div_tol": 0.0, "poisson_maxit": 60}, **SMALL["hill"])
+    codes = []
+    for s in (e, r):
+        with pytest.raises(api.TgError) as ei:
+            s.step(3)
+        codes.append(ei.value.status)
+    assert codes[0] == codes[1]
+    for f in FIELDS:
+        assert np.array_equal(e.get(f), r.get(f), equal_nan=True), f
+    assert r.graph_info()[0] == 2
     e.close(); r.close()

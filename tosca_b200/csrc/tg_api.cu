@@ -268,7 +268,7 @@ tg_status tg_destroy(tg_ctx *C)
     cudaSetDevice(C->cfg.device);
     if (C->stream) cudaStreamSynchronize(C->stream);
     graph_destroy(C);
-    if (C->aux[0]) cudaStreamDestroy(C->aux[0]);
+    for (cudaStream_t a : C->aux) if (a) cudaStreamDestroy(a);
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);

@@ -542,73 +542,158 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     return rc;
 }
 
-// poisson_solve for a step being captured into a CUDA graph (orthogonal
-// grids): the CG iterations form a conditional WHILE node whose condition a
-// one-thread kernel sets from the device residuals, so the solve needs no
-// host round trip per iteration. The loop body is krylov_solve's iteration
-// rotated to start with the direction update (p = z on the first pass), which
-// performs the same arithmetic in the same order; statistics go to the
-// SC_G* device slots.
-void poisson_solve_capture(tg_ctx *C)
+// ---------------------------------------------------- captured solves
+// Conditional node of `type` appended to the graph being captured on
+// C->stream; body() is captured into the node's body graph on the auxiliary
+// stream `aux` (C->stream points there while body() runs).
+template <class F>
+static void capture_conditional(tg_ctx *C, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                                cudaStream_t aux, F &&body)
 {
-    PoissonCtx &P = *C->pois;
-    const Grid g = C->g;
     cudaStream_t s = C->stream;
-    const int64_t n = P.n;
-    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
-    const double divtol = C->cfg.poisson_div_tol;
-    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
-    const double dt = C->prm.dt;
-    double *sc = C->d_scal;
-    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
-    k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, dt);
-    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
-    dot3v(C, P.b, P.b, nullptr, sc + 0);
-    apply_op(C, P.x, P.r);
-    k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r);
-    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
-
     cudaStreamCaptureStatus cs;
     cudaGraph_t graph;
     const cudaGraphNode_t *deps = nullptr;
     size_t nd = 0;
     TG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &nd));
-    if (cs != cudaStreamCaptureStatusActive) throw CudaError{cudaErrorStreamCaptureInvalidated, "poisson_solve_capture: stream not capturing"};
-    cudaGraphConditionalHandle h;
-    TG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
-    k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
-    TG_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &nd));
     cudaGraphNodeParams cp{};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.type = type;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     TG_CUDA(cudaGraphAddNode(&node, graph, deps, nd, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaGraph_t bg = cp.conditional.phGraph_out[0];
     TG_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    TG_CUDA(cudaStreamBeginCaptureToGraph(aux, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    {
+        struct Swap { tg_ctx *C; cudaStream_t keep; ~Swap() { C->stream = keep; } } sw{C, s};
+        C->stream = aux;
+        body();
+    }
+    cudaGraph_t done;
+    TG_CUDA(cudaStreamEndCapture(aux, &done));
+}
 
-    // loop body, captured on the auxiliary stream into the node's body graph
-    cudaStream_t a = C->aux[0];
-    TG_CUDA(cudaStreamBeginCaptureToGraph(a, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    struct Swap { tg_ctx *C; cudaStream_t keep; ~Swap() { C->stream = keep; } } sw{C, s};
-    C->stream = a;
-    precondition(C, P.r, P.z, sc + 4);
-    k_scalar_copy<<<1, 1, 0, a>>>(sc + 6, sc + 14, 1);           // rz_old
-    dot3v(C, P.r, P.z, nullptr, sc + 6);                          // rz
-    k_cg_dir_loop<<<vblocks(n), RB, 0, a>>>(n, sc, P.z, P.p);
-    apply_op(C, P.p, P.q);
-    k_zero_at<<<1, 1, 0, a>>>(P.q, P.pin);
-    dot3v(C, P.p, P.q, nullptr, sc + 9);                          // pq
-    k_cg_update<<<vblocks(n), RB, 0, a>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q);
-    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);      // rr, sum r, max|r aj|
-    k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
-    C->stream = s;
-    cudaGraph_t captured;
-    TG_CUDA(cudaStreamEndCapture(a, &captured));
+// conditional handle of the graph being captured on C->stream (no default
+// value: a kernel sets it before the node runs)
+static cudaGraphConditionalHandle capture_handle(tg_ctx *C)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph;
+    TG_CUDA(cudaStreamGetCaptureInfo(C->stream, &cs, nullptr, &graph, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive) throw CudaError{cudaErrorStreamCaptureInvalidated, "capture_handle: stream not capturing"};
+    cudaGraphConditionalHandle h;
+    TG_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    return h;
+}
 
+__global__ void k_fill(int64_t n, double *a, double v)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) a[t] = v;
+}
+// BiCGStab restarts from the true residual every 50 iterations
+__global__ void k_bicg_restart_flag(const double *sc, cudaGraphConditionalHandle h)
+{
+    const int it = (int)sc[50];
+    cudaGraphSetConditional(h, (it > 0 && (it % 50) == 0) ? 1u : 0u);
+}
+
+// krylov_solve for a step being captured into a CUDA graph: the iterations
+// form a conditional WHILE node whose condition a one-thread kernel sets from
+// the device residuals, so the solve needs no host round trip per iteration.
+// The CG body is krylov_solve's iteration rotated to start with the direction
+// update (p = z on the first pass), the BiCGStab body is krylov_solve's with
+// its periodic restart as a conditional IF node; both perform the same
+// arithmetic in the same order. Statistics go to the SC_G* device slots.
+static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit)
+{
+    PoissonCtx &P = *C->pois;
+    const int64_t n = P.n;
+    cudaStream_t s = C->stream;
+    const double dt = C->prm.dt;
+    double *sc = C->d_scal;
+    const int vb = vblocks(n);
+    dot3v(C, P.b, P.b, nullptr, sc + 0);
+    apply_op(C, P.x, P.r);
+    k_resid<<<vb, RB, 0, s>>>(n, P.b, P.r);
+    dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+    if (P.ortho) {
+        cudaGraphConditionalHandle h = capture_handle(C);
+        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
+        capture_conditional(C, h, cudaGraphCondTypeWhile, C->aux[0], [&]() {
+            cudaStream_t a = C->stream;
+            precondition(C, P.r, P.z, sc + 4);
+            k_scalar_copy<<<1, 1, 0, a>>>(sc + 6, sc + 14, 1);           // rz_old
+            dot3v(C, P.r, P.z, nullptr, sc + 6);                          // rz
+            k_cg_dir_loop<<<vb, RB, 0, a>>>(n, sc, P.z, P.p);
+            apply_op(C, P.p, P.q);
+            k_zero_at<<<1, 1, 0, a>>>(P.q, P.pin);
+            dot3v(C, P.p, P.q, nullptr, sc + 9);                          // pq
+            k_cg_update<<<vb, RB, 0, a>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q);
+            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);      // rr, sum r, max|r aj|
+            k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
+        });
+    } else {
+        k_copy<<<vb, RB, 0, s>>>(n, P.r, P.rhat);
+        k_fill<<<1, 32, 0, s>>>(4, sc + 20, 1.0);
+        k_fill<<<vb, RB, 0, s>>>(n, P.p, 0.0);
+        k_fill<<<vb, RB, 0, s>>>(n, P.v, 0.0);
+        double *phat = P.z, *shat = P.q;
+        cudaGraphConditionalHandle h = capture_handle(C);
+        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
+        capture_conditional(C, h, cudaGraphCondTypeWhile, C->aux[0], [&]() {
+            cudaStream_t a = C->stream;
+            cudaGraphConditionalHandle hr = capture_handle(C);
+            k_bicg_restart_flag<<<1, 1, 0, a>>>(sc, hr);
+            capture_conditional(C, hr, cudaGraphCondTypeIf, C->aux[1], [&]() {
+                cudaStream_t b = C->stream;
+                apply_op(C, P.x, P.r);
+                k_resid<<<vb, RB, 0, b>>>(n, P.b, P.r);
+                k_copy<<<vb, RB, 0, b>>>(n, P.r, P.rhat);
+                k_fill<<<1, 32, 0, b>>>(4, sc + 20, 1.0);
+                k_fill<<<vb, RB, 0, b>>>(n, P.p, 0.0);
+                k_fill<<<vb, RB, 0, b>>>(n, P.v, 0.0);
+            });
+            dot3v(C, P.rhat, P.r, nullptr, sc + 24);
+            k_scalar_copy<<<1, 1, 0, a>>>(sc + 20, sc + 23, 1);
+            k_scalar_copy<<<1, 1, 0, a>>>(sc + 24, sc + 20, 1);
+            k_bicg_p<<<vb, RB, 0, a>>>(n, sc + 20, P.p, P.r, P.v);
+            dot3v(C, P.p, P.p, nullptr, sc + 27);
+            precondition(C, P.p, phat, sc + 28);
+            apply_op(C, phat, P.v);
+            dot3v(C, P.rhat, P.v, nullptr, sc + 30);
+            k_bicg_s<<<vb, RB, 0, a>>>(n, sc + 20, sc + 30, sc + 21, P.s, P.r, P.v);
+            dot3v(C, P.s, P.s, nullptr, sc + 33);
+            precondition(C, P.s, shat, sc + 34);
+            apply_op(C, shat, P.t);
+            dot3v(C, P.t, P.s, nullptr, sc + 36);
+            dot3v(C, P.t, P.t, nullptr, sc + 39);
+            k_bicg_x<<<vb, RB, 0, a>>>(n, sc + 21, sc + 36, sc + 39, sc + 22, P.x, phat, shat, P.r, P.s, P.t);
+            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+            k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
+        });
+        // true residual (reported)
+        apply_op(C, P.x, P.r);
+        k_resid<<<vb, RB, 0, s>>>(n, P.b, P.r);
+        dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+    }
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
     k_cg_finish<<<1, 1, 0, s>>>(sc);
+}
+
+// poisson_solve for a step being captured into a CUDA graph
+void poisson_solve_capture(tg_ctx *C)
+{
+    PoissonCtx &P = *C->pois;
+    const Grid g = C->g;
+    cudaStream_t s = C->stream;
+    const double rtol = C->cfg.poisson_rtol > 0 ? C->cfg.poisson_rtol : 1e-14;
+    const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
+    const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
+    k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt);
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
+    krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit);
     k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P);
     TG_CUDA(cudaGetLastError());
 }

@@ -1290,13 +1290,13 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
 // A step replays as one CUDA graph once every choice the host makes in it is
 // fixed: after the first step (Adams-Bashforth flag, btheta_o copy), with the
 // wall filter seeded, no pending clear of a caller-written Rhs or dP, the FP32
-// metric copies current, profiling and taping off, and CG (orthogonal grids)
-// as the Krylov method.
+// metric copies current, and profiling and taping off. The Krylov loop of the
+// captured step runs under device control (poisson_solve_capture).
 static bool graph_eligible(const tg_ctx *C)
 {
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
-    return C->graphs && !C->graph_failed && !C->prof.on && !C->taping && C->orthogonal && C->pois &&
-           C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !C->met32_stale;
+    return C->graphs && !C->graph_failed && !C->prof.on && !C->taping && C->pois &&
+           C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 
 void graph_destroy(tg_ctx *C)
@@ -1307,7 +1307,8 @@ void graph_destroy(tg_ctx *C)
 
 static void graph_build(tg_ctx *C)
 {
-    if (!C->aux[0]) TG_CUDA(cudaStreamCreateWithFlags(&C->aux[0], cudaStreamNonBlocking));
+    for (cudaStream_t &a : C->aux)
+        if (!a) TG_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
     cudaStream_t s = C->stream;
     cudaGraph_t graph = nullptr;
     TG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1316,8 +1317,9 @@ static void graph_build(tg_ctx *C)
     } catch (...) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t part = nullptr;
-        if (cudaStreamIsCapturing(C->aux[0], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
-            cudaStreamEndCapture(C->aux[0], &part);   // the body graph belongs to its conditional node
+        for (int q = 1; q >= 0; q--)   // body graphs belong to their conditional nodes
+            if (cudaStreamIsCapturing(C->aux[q], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+                cudaStreamEndCapture(C->aux[q], &part);
         part = nullptr;
         cudaStreamEndCapture(s, &part);
         if (part) cudaGraphDestroy(part);
