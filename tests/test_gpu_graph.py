@@ -107,3 +107,69 @@ def test_graphs_off_then_on():
     assert_same(e, r)
     e.close(); r.close()
 
+
+
+def _adjoint_twin(ddt):
+    from tests.test_gpu_adjoint import _case
+    rng = np.random.default_rng(11)
+    cfg, nodes, ucat, p = _case("abl", ddt)
+    f0 = rng.standard_normal(ucat.shape) * 0.01
+    out = []
+    for graphs in (False, True):
+        s = tosca_b200.gpu_solver(cfg)
+        cases.setup(s, nodes, ucat, p)
+        s.set_graphs(graphs)
+        s.set("SOURCE", f0)
+        s.step(1)
+        out.append(s)
+    inside = np.zeros(p.shape, bool)
+    inside[1:-1, 1:-1, 1:-1] = True
+    seeds = (rng.standard_normal(ucat.shape), rng.standard_normal(ucat.shape) * inside[..., None],
+             rng.standard_normal(p.shape))
+    return out, seeds
+
+
+ADJ = ("UCONT_ADJ", "UCAT_ADJ", "P_ADJ", "SOURCE_ADJ")
+
+
+def _seed(s, seeds):
+    s.set("UCONT_ADJ", seeds[0]); s.set("UCAT_ADJ", seeds[1]); s.set("P_ADJ", seeds[2])
+    s.set("SOURCE_ADJ", np.zeros(seeds[0].shape))
+
+
+def _same_adjoint(e, r):
+    # the forward state is restored bitwise; the transposed face fluxes and
+    # gradients scatter with FP64 atomics, whose summation order varies
+    for f in ("UCONT", "UCAT", "P"):
+        assert np.array_equal(e.get(f), r.get(f)), f
+    for f in ADJ:
+        a, b = e.get(f), r.get(f)
+        assert np.linalg.norm(a - b) <= 1e-11 * np.linalg.norm(b), f
+
+
+@pytest.mark.parametrize("ddt", [api.DDT_FE, api.DDT_RK4])
+def test_adjoint_step_replay(ddt):
+    (e, r), seeds = _adjoint_twin(ddt)
+    for s in (e, r):
+        _seed(s, seeds)
+        for _ in range(3):
+            s.adjoint_step()
+    _same_adjoint(e, r)
+    assert r.graph_info()[0] == 3     # the taped forward steps
+    e.close(); r.close()
+
+
+@pytest.mark.parametrize("nsnap", [5, 2])
+def test_adjoint_reverse_replay(nsnap):
+    # nsnap = steps keeps every tape; fewer snapshots re-run forward steps
+    (e, r), seeds = _adjoint_twin(api.DDT_RK4)
+    stats = []
+    for s in (e, r):
+        s.adjoint_forward(5, nsnap)
+        _seed(s, seeds)
+        stats.append(s.adjoint_reverse())
+    _same_adjoint(e, r)
+    assert abs(stats[0].poisson_iterations - stats[1].poisson_iterations) <= 5
+    assert stats[0].forward_steps == stats[1].forward_steps
+    assert r.graph_info()[0] > 0
+    e.close(); r.close()

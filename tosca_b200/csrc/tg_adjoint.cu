@@ -78,6 +78,9 @@ struct AdjState {
     int base_it = 0, nsteps = 0, fwd_steps = 0;
     int64_t adj_iters = 0;                // Krylov iterations of the transposed solves
     bool recorded = false;
+    // CUDA graph of a reversed step reading the work tape
+    cudaGraphExec_t rev_exec = nullptr;
+    bool rev_failed = false;
     // bounds of the recorded forward run
     int start_pos = 0;
 };
@@ -792,6 +795,8 @@ __global__ void k_adj_smagorinsky(Grid g, Metrics m, V3f<double> ucat, const dou
 }  // namespace
 
 // ===================================================================== host
+struct ApiFail { tg_status s; std::string msg; };
+
 static V3f<double> alloc3(tg_ctx *C) { return dalloc3(C, (size_t)C->g.size()); }
 
 static AdjState &adj_state(tg_ctx *C)
@@ -841,11 +846,22 @@ bool adj_field(tg_ctx *C, int w, V3f<double> &v, double *&s)
     return true;
 }
 
+void adj_graph_destroy(tg_ctx *C)
+{
+    if (!C->adj) return;
+    if (C->adj->rev_exec) cudaGraphExecDestroy(C->adj->rev_exec);
+    C->adj->rev_exec = nullptr;
+    C->adj->rev_failed = false;
+}
+
 void adj_destroy(tg_ctx *C)
 {
+    adj_graph_destroy(C);
     delete C->adj;       // device buffers are owned by the context allocation list
     C->adj = nullptr;
 }
+
+bool tape_in_work(const tg_ctx *C) { return C->adj && C->adj->cur == &C->adj->work_tape; }
 
 static void copy3(tg_ctx *C, V3f<double> dst, V3f<double> src)
 {
@@ -854,6 +870,15 @@ static void copy3(tg_ctx *C, V3f<double> dst, V3f<double> src)
 static void zero3(tg_ctx *C, V3f<double> v)
 {
     TG_CUDA(cudaMemsetAsync(v.x, 0, 3 * sizeof(double) * (size_t)C->g.size(), C->stream));
+}
+
+static void copy_tape(tg_ctx *C, Tape &dst, const Tape &src)
+{
+    copy3(C, dst.u_o, src.u_o);
+    copy3(C, dst.ucat_n, src.ucat_n);
+    for (int q = 0; q < src.nst; q++) { copy3(C, dst.ut[q], src.ut[q]); copy3(C, dst.uc[q], src.uc[q]); }
+    TG_CUDA(cudaMemcpyAsync(dst.nut, src.nut, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
+    dst.nst = src.nst;
 }
 
 void tape_step_start(tg_ctx *C)
@@ -909,8 +934,9 @@ static bool adjoint_supported(tg_ctx *C, std::string &why)
 }
 
 // reverse sweep of one recorded step (tape filled by a taped forward step from
-// the state at its start)
-static int adjoint_reverse_step(tg_ctx *C)
+// the state at its start); capture: the sweep is being recorded into a CUDA
+// graph (device-side transposed-solve loop, statistics in the SC_ADJ slots)
+static int adjoint_reverse_body(tg_ctx *C, bool capture)
 {
     AdjState &A = *C->adj;
     const Tape &T = *A.cur;
@@ -940,15 +966,21 @@ static int adjoint_reverse_step(tg_ctx *C)
     k_adj_update_pressure<<<gint(g), block3(), 0, st>>>(g, A.pa, A.pha, A.rhsc);
     adj_scalar_ghosts(C, A.pha);
     k_adj_phi_compact<<<gint(g), block3(), 0, st>>>(g, A.pha, A.rhsc);
-    tg_stats ps{};
     // started from the previous reversed step's solution, to the context's
     // relative tolerance when that lies in [1e-14, 1e-8], else to 1e-8 (the
     // forward solve then stops on the divergence bound, whose relative
     // residual is of the order of 1e-7)
     const double rt = C->cfg.poisson_rtol;
-    int rc = poisson_solve_adjoint(C, A.rhsc, A.lam, (rt >= 1e-14 && rt <= 1e-8) ? rt : 1e-8, &ps);
-    A.adj_iters += ps.poisson_iterations;
-    if (rc == 3) return 3;
+    const double artol = (rt >= 1e-14 && rt <= 1e-8) ? rt : 1e-8;
+    int rc = 0;
+    if (capture) {
+        poisson_solve_adjoint_capture(C, A.rhsc, A.lam, artol);
+    } else {
+        tg_stats ps{};
+        rc = poisson_solve_adjoint(C, A.rhsc, A.lam, artol, &ps);
+        A.adj_iters += ps.poisson_iterations;
+        if (rc == 3) return 3;
+    }
     // SetRHS; u* = utmp after the tail flux resets
     copy3(C, A.usa, A.ua);
     TG_PROF(C, "adj_set_rhs", k_adj_set_rhs<<<gfc(g), block3(), 0, st>>>(g, A.lam, A.usa, dt));
@@ -994,6 +1026,40 @@ static int adjoint_reverse_step(tg_ctx *C)
     copy3(C, A.ua, A.uoa);
     TG_CUDA(cudaGetLastError());
     return rc;
+}
+
+// One reversed step: a replay of the captured sweep (the tape is first copied
+// into the work tape when it is a stored one), or the sweep launched kernel by
+// kernel when profiling or step replay is off. A replayed sweep returns 0 and
+// reports through the SC_ADJ slots.
+static int adjoint_reverse_step(tg_ctx *C)
+{
+    AdjState &A = *C->adj;
+    if (!C->graphs || C->prof.on || A.rev_failed) return adjoint_reverse_body(C, false);
+    if (A.cur != &A.work_tape) {
+        copy_tape(C, A.work_tape, *A.cur);
+        A.cur = &A.work_tape;
+    }
+    if (!A.rev_exec && !capture_graph(C, &A.rev_exec, [&]() { adjoint_reverse_body(C, true); })) {
+        A.rev_failed = true;
+        return adjoint_reverse_body(C, false);
+    }
+    TG_CUDA(cudaGraphLaunch(A.rev_exec, C->stream));
+    return 0;
+}
+
+// statistics of replayed steps and sweeps since step_stats_reset: throws on a
+// non-finite residual or a transposed solve at its iteration cap
+static void adj_replay_check(tg_ctx *C)
+{
+    TG_CUDA(cudaMemcpyAsync(C->h_scal + SC_G, C->d_scal + SC_G, sizeof(double) * (SC_ADJ + ST_COUNT - SC_G),
+                            cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
+    const double *h = C->h_scal;
+    C->adj->adj_iters += (int64_t)h[SC_ADJ + ST_TOT];
+    if (h[SC_G + ST_NAN] != 0.0) throw ApiFail{TG_ERR_NAN, "non-finite residual in a forward step"};
+    if (h[SC_ADJ + ST_NAN] != 0.0) throw ApiFail{TG_ERR_NAN, "non-finite residual in a transposed pressure solve"};
+    if (h[SC_ADJ + ST_NOCONV] != 0.0) throw ApiFail{TG_ERR_NOT_CONVERGED, "adjoint step failed"};
 }
 
 // ---------------------------------------------------------- snapshots
@@ -1077,7 +1143,6 @@ struct Revolve {
 using namespace tg;
 
 namespace {
-struct ApiFail { tg_status s; std::string msg; };
 
 template <class F>
 tg_status adj_guard(tg_ctx *C, F &&f)
@@ -1160,10 +1225,12 @@ tg_status tg_adjoint_step(tg_ctx *C)
         AdjState &A = adj_state(C);
         adj_work(C);
         if (!A.has_single) { A.single = make_snapshot(C); A.has_single = true; }
+        step_stats_reset(C);
         int rc = adjoint_step_here(C, A.single);
-        TG_CUDA(cudaStreamSynchronize(C->stream));
+        adj_replay_check(C);
         if (rc == 3) { C->err = "adjoint of the non-symmetric pressure operator is not implemented"; return TG_ERR_BAD_ARG; }
         if (rc == 2) { C->err = "non-finite residual in the forward step"; return TG_ERR_NAN; }
+        if (rc == 1) { C->err = "transposed pressure solve reached its iteration cap"; return TG_ERR_NOT_CONVERGED; }
         return TG_OK;
     });
 }
@@ -1215,10 +1282,12 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         if (store) keep.clear();
         bool any = false, last = false;
         for (int n = 0; n < nsteps; n++) {
-            if (store) { A.cur = &A.store[n]; C->taping = true; }
+            // a kept tape is recorded into the work tape and copied out
+            if (store) { A.cur = &A.work_tape; C->taping = true; }
             int rc = step(C, st, &last);
             any |= last;
             C->taping = false;
+            if (store) copy_tape(C, A.store[n], A.work_tape);
             st->steps += 1;
             if (rc == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
             if (next < keep.size() && keep[next] == n + 1) { save_state(C, A.snaps[next + 1], n + 1); next++; }
@@ -1248,6 +1317,7 @@ tg_status tg_adjoint_reverse(tg_ctx *C, tg_adjoint_stats *stats)
         Revolve R;
         R.build(A.nsteps, (int)A.snaps.size() - 2);
         A.adj_iters = 0;
+        step_stats_reset(C);
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         if (A.stored) {
             for (int n = A.nsteps - 1; n >= 0; n--) {
@@ -1261,7 +1331,7 @@ tg_status tg_adjoint_reverse(tg_ctx *C, tg_adjoint_stats *stats)
         }
         restore_state(C, A.snaps[0]);
         TG_CUDA(cudaEventRecord(C->ev1, C->stream));
-        TG_CUDA(cudaEventSynchronize(C->ev1));
+        adj_replay_check(C);
         float ms = 0.f;
         TG_CUDA(cudaEventElapsedTime(&ms, C->ev0, C->ev1));
         st->seconds = ms * 1e-3;

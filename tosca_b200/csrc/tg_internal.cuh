@@ -8,6 +8,7 @@
 // single-rank PETSc local vector returns for DM_BOUNDARY_PERIODIC.
 #pragma once
 
+#include <functional>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -160,6 +161,7 @@ struct tg_ctx {
     // CUDA graph of a whole step (tg_step.cu): built on the first step that can
     // be captured, replayed afterwards
     cudaGraphExec_t step_exec = nullptr;
+    cudaGraphExec_t step_exec_taped = nullptr;   // the same step recording its stages
     bool graphs = true;                  // tg_set_graphs
     int64_t replays = 0;
     bool graph_failed = false;
@@ -232,8 +234,8 @@ double continuity_error(tg_ctx *C);
 void sync_pressure(tg_ctx *C);
 void init_from_cartesian(tg_ctx *C);
 int step(tg_ctx *C, tg_stats *st, bool *replayed = nullptr);
-void step_stats_reset(tg_ctx *C);            // zero the SC_G* slots before a run of steps
-// after a run of steps: copy d_scal[16..66) to h_scal, merge the statistics of
+void step_stats_reset(tg_ctx *C);            // zero the SC_G and SC_ADJ slots before a run of steps
+// after a run of steps: copy d_scal[16..SC_IT) to h_scal, merge the statistics of
 // replayed steps into s (last: the final step was replayed); returns 0, 1
 // (iteration cap) or 2 (non-finite residual) for the replayed steps
 int step_stats_read(tg_ctx *C, tg_stats *s, bool any, bool last);
@@ -246,8 +248,18 @@ void poisson_setup(tg_ctx *C);
 void poisson_destroy(tg_ctx *C);
 int poisson_solve(tg_ctx *C, tg_stats *st);
 void poisson_solve_capture(tg_ctx *C);       // the same solve with device-side loop control
-// device scalar slots (C->d_scal) of the captured solve and the step counter
-constexpr int SC_GIT = 60, SC_GRES0 = 61, SC_GRES = 62, SC_GTOT = 63, SC_GNOCONV = 64, SC_GNAN = 65, SC_IT = 66;
+// device scalar slots (C->d_scal): statistics of captured solves, as offsets
+// from a base (SC_G: forward step, SC_ADJ: transposed solve), and the step counter
+constexpr int ST_IT = 0, ST_RES0 = 1, ST_RES = 2, ST_TOT = 3, ST_NOCONV = 4, ST_NAN = 5, ST_COUNT = 6;
+constexpr int SC_G = 60, SC_ADJ = 70, SC_IT = 80;
+constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
+              SC_GNOCONV = SC_G + ST_NOCONV, SC_GNAN = SC_G + ST_NAN;
+void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol);
+// capture body() (launches on C->stream) into an instantiated graph; false when
+// capture or instantiation fails (nothing is left capturing)
+bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body);
+void adj_graph_destroy(tg_ctx *C);
+bool tape_in_work(const tg_ctx *C);          // the step tapes into the fixed work tape
 void set_device_step(tg_ctx *C);             // C->d_scal[SC_IT] <- C->it
 void graph_destroy(tg_ctx *C);
 

@@ -291,11 +291,11 @@ __device__ inline bool cg_converged(const double *sc, double rtol, double divtol
     const double bn = sqrt(sc[0]), rn = sqrt(sc[3]), rmax = sc[5] * dt;
     return bn == 0.0 || rn / bn <= rtol || (divtol > 0 && rmax <= divtol);
 }
-__global__ void k_cg_start(double *sc, double rtol, double divtol, double dt, int maxit, cudaGraphConditionalHandle h)
+__global__ void k_cg_start(double *sc, double rtol, double divtol, double dt, int maxit, cudaGraphConditionalHandle h, int base)
 {
     const double bn = sqrt(sc[0]), rn = sqrt(sc[3]);
     const bool conv = cg_converged(sc, rtol, divtol, dt);
-    sc[SC_GRES0] = bn > 0 ? rn / bn : rn;
+    sc[base + ST_RES0] = bn > 0 ? rn / bn : rn;
     sc[50] = 0.0; sc[51] = 1.0; sc[52] = conv ? 1.0 : 0.0;
     cudaGraphSetConditional(h, (!conv && maxit > 0 && isfinite(rn)) ? 1u : 0u);
 }
@@ -307,15 +307,16 @@ __global__ void k_cg_next(double *sc, double rtol, double divtol, double dt, int
     sc[50] = it; sc[51] = 0.0; sc[52] = conv ? 1.0 : 0.0;
     cudaGraphSetConditional(h, (!conv && it < maxit && isfinite(rn)) ? 1u : 0u);
 }
-// statistics of the solve, accumulated over the replayed steps
-__global__ void k_cg_finish(double *sc)
+// statistics of the solve, accumulated over the replayed solves in the
+// ST_* slots from base
+__global__ void k_cg_finish(double *sc, int base)
 {
     const double bn = sqrt(sc[0]), rn = sqrt(sc[3]);
-    sc[SC_GIT] = sc[50];
-    sc[SC_GTOT] += sc[50];
-    sc[SC_GRES] = bn > 0 ? rn / bn : rn;
-    if (!isfinite(rn)) sc[SC_GNAN] = 1.0;
-    else if (sc[52] == 0.0) sc[SC_GNOCONV] += 1.0;
+    sc[base + ST_IT] = sc[50];
+    sc[base + ST_TOT] += sc[50];
+    sc[base + ST_RES] = bn > 0 ? rn / bn : rn;
+    if (!isfinite(rn)) sc[base + ST_NAN] = 1.0;
+    else if (sc[52] == 0.0) sc[base + ST_NOCONV] += 1.0;
 }
 // p = z on the first pass through the loop body, else p = z + (rz_new / rz_old) p
 __global__ void k_cg_dir_loop(int64_t n, const double *sc, const double *z, double *p)
@@ -605,8 +606,8 @@ __global__ void k_bicg_restart_flag(const double *sc, cudaGraphConditionalHandle
 // The CG body is krylov_solve's iteration rotated to start with the direction
 // update (p = z on the first pass), the BiCGStab body is krylov_solve's with
 // its periodic restart as a conditional IF node; both perform the same
-// arithmetic in the same order. Statistics go to the SC_G* device slots.
-static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit)
+// arithmetic in the same order. Statistics go to the ST_* slots from base.
+static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit, int base)
 {
     PoissonCtx &P = *C->pois;
     const int64_t n = P.n;
@@ -620,7 +621,7 @@ static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit)
     dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
     if (P.ortho) {
         cudaGraphConditionalHandle h = capture_handle(C);
-        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
+        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h, base);
         capture_conditional(C, h, cudaGraphCondTypeWhile, C->aux[0], [&]() {
             cudaStream_t a = C->stream;
             precondition(C, P.r, P.z, sc + 4);
@@ -641,7 +642,7 @@ static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit)
         k_fill<<<vb, RB, 0, s>>>(n, P.v, 0.0);
         double *phat = P.z, *shat = P.q;
         cudaGraphConditionalHandle h = capture_handle(C);
-        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h);
+        k_cg_start<<<1, 1, 0, s>>>(sc, rtol, divtol, dt, maxit, h, base);
         capture_conditional(C, h, cudaGraphCondTypeWhile, C->aux[0], [&]() {
             cudaStream_t a = C->stream;
             cudaGraphConditionalHandle hr = capture_handle(C);
@@ -679,7 +680,7 @@ static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit)
         dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
     }
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
-    k_cg_finish<<<1, 1, 0, s>>>(sc);
+    k_cg_finish<<<1, 1, 0, s>>>(sc, base);
 }
 
 // poisson_solve for a step being captured into a CUDA graph
@@ -693,8 +694,25 @@ void poisson_solve_capture(tg_ctx *C)
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
-    krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit);
+    krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit, SC_G);
     k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P);
+    TG_CUDA(cudaGetLastError());
+}
+
+// poisson_solve_adjoint for a reversed step being captured into a CUDA graph
+// (statistics in the SC_ADJ slots)
+void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol)
+{
+    PoissonCtx &P = *C->pois;
+    cudaStream_t s = C->stream;
+    const int64_t n = P.n;
+    TG_CUDA(cudaMemcpyAsync(P.v, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    k_negcopy<<<vblocks(n), RB, 0, s>>>(n, rhs, P.b);
+    k_zero_at<<<1, 1, 0, s>>>(P.b, P.pin);
+    TG_CUDA(cudaMemcpyAsync(P.x, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    krylov_capture(C, rtol, 0.0, C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500, SC_ADJ);
+    TG_CUDA(cudaMemcpyAsync(lam, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    TG_CUDA(cudaMemcpyAsync(P.x, P.v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     TG_CUDA(cudaGetLastError());
 }
 

@@ -1295,46 +1295,52 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
 static bool graph_eligible(const tg_ctx *C)
 {
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
-    return C->graphs && !C->graph_failed && !C->prof.on && !C->taping && C->pois &&
+    return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
            C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 
 void graph_destroy(tg_ctx *C)
 {
     if (C->step_exec) cudaGraphExecDestroy(C->step_exec);
-    C->step_exec = nullptr;
+    if (C->step_exec_taped) cudaGraphExecDestroy(C->step_exec_taped);
+    C->step_exec = C->step_exec_taped = nullptr;
+    adj_graph_destroy(C);
 }
 
-static void graph_build(tg_ctx *C)
+bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body)
 {
+    *out = nullptr;
     for (cudaStream_t &a : C->aux)
         if (!a) TG_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
     cudaStream_t s = C->stream;
     cudaGraph_t graph = nullptr;
     TG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
-        step_body(C, nullptr, true);
-    } catch (...) {
+        body();
+    } catch (const CudaError &) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t part = nullptr;
         for (int q = 1; q >= 0; q--)   // body graphs belong to their conditional nodes
             if (cudaStreamIsCapturing(C->aux[q], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
                 cudaStreamEndCapture(C->aux[q], &part);
         part = nullptr;
+        C->stream = s;
         cudaStreamEndCapture(s, &part);
         if (part) cudaGraphDestroy(part);
-        C->stream = s;
-        throw;
+        cudaGetLastError();
+        return false;
     }
-    TG_CUDA(cudaStreamEndCapture(s, &graph));
-    cudaError_t e = cudaGraphInstantiate(&C->step_exec, graph, 0);
+    if (cudaStreamEndCapture(s, &graph) != cudaSuccess) { cudaGetLastError(); return false; }
+    cudaError_t e = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
-    if (e != cudaSuccess) { C->step_exec = nullptr; throw CudaError{e, "cudaGraphInstantiate"}; }
+    if (e != cudaSuccess) { *out = nullptr; cudaGetLastError(); return false; }
+    return true;
 }
 
 void step_stats_reset(tg_ctx *C)
 {
-    TG_CUDA(cudaMemsetAsync(C->d_scal + SC_GIT, 0, sizeof(double) * (SC_IT - SC_GIT), C->stream));
+    TG_CUDA(cudaMemsetAsync(C->d_scal + SC_G, 0, sizeof(double) * ST_COUNT, C->stream));
+    TG_CUDA(cudaMemsetAsync(C->d_scal + SC_ADJ, 0, sizeof(double) * ST_COUNT, C->stream));
 }
 
 int step_stats_read(tg_ctx *C, tg_stats *s, bool any, bool last)
@@ -1361,18 +1367,15 @@ int step(tg_ctx *C, tg_stats *st, bool *replayed)
 {
     if (replayed) *replayed = false;
     if (graph_eligible(C)) {
-        if (!C->step_exec) {
-            try {
-                graph_build(C);
-            } catch (const CudaError &) {
-                // capture is unsupported for this configuration: stay eager
-                cudaGetLastError();
-                graph_destroy(C);
-                C->graph_failed = true;
-            }
+        // the taped step records its stages into the work tape
+        cudaGraphExec_t &ex = C->taping ? C->step_exec_taped : C->step_exec;
+        if (!ex && !capture_graph(C, &ex, [&]() { step_body(C, nullptr, true); })) {
+            // capture is unsupported for this configuration: stay eager
+            graph_destroy(C);
+            C->graph_failed = true;
         }
-        if (C->step_exec) {
-            TG_CUDA(cudaGraphLaunch(C->step_exec, C->stream));
+        if (ex) {
+            TG_CUDA(cudaGraphLaunch(ex, C->stream));
             C->it++;
             C->replays++;
             if (replayed) *replayed = true;
