@@ -139,12 +139,13 @@ def _seed(s, seeds):
 
 def _same_adjoint(e, r):
     # the forward state is restored bitwise; the transposed face fluxes and
-    # gradients scatter with FP64 atomics, whose summation order varies
+    # gradients scatter with FP64 atomics, whose summation order varies (the
+    # adjoint seeds are O(1); P_ADJ itself can be at round-off level)
     for f in ("UCONT", "UCAT", "P"):
         assert np.array_equal(e.get(f), r.get(f)), f
     for f in ADJ:
         a, b = e.get(f), r.get(f)
-        assert np.linalg.norm(a - b) <= 1e-11 * np.linalg.norm(b), f
+        assert np.linalg.norm(a - b) <= 1e-11 * max(np.linalg.norm(b), 1.0), f
 
 
 @pytest.mark.parametrize("ddt", [api.DDT_FE, api.DDT_RK4])
