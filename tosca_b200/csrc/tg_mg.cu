@@ -2,7 +2,7 @@
 // operator, used as the preconditioner of the Krylov pressure solve.
 //
 //  * coarsening: every even direction with >= 4 cells is halved until a level
-//    has <= 512 cells; coarse face coefficients are face sums of the fine
+//    has <= 64 cells; coarse face coefficients are face sums of the fine
 //    ones, halved when the face-normal direction is coarsened
 //  * transfers: summed residual restriction, piecewise-constant prolongation
 //  * smoothing: zebra j-line Gauss-Seidel when j (the wall-normal direction)
@@ -21,9 +21,12 @@
 // a chain of FMAs. A block solves 32 same-colour lines at once: each of its
 // warps takes one chunk of j, runs the forward and backward recurrences of
 // its chunk as affine maps (coalesced loads, all warps in flight), and the
-// chunk ends are combined in shared memory. Levels with <= 4096 cells run as
-// one single-block kernel (all their sweeps, transfers and the coarsest
-// solve), which removes the launch latency of the smallest levels.
+// chunk ends are combined in shared memory. The smallest levels (<= 4096
+// cells each, as many as fit) run as one single-block kernel that stages
+// their coefficients, unknowns and the dense coarsest inverse in shared
+// memory and performs all their sweeps, transfers and the coarsest solve
+// there: no launch latency, and shared-memory instead of L2 latency in the
+// sequential line recurrences.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -45,6 +48,8 @@ struct Lvl {
 
 constexpr int MAXL = 16;
 constexpr int TAIL_CELLS = 4096;
+constexpr int COARSEST_CELLS = 64;
+constexpr int TAIL_SMEM = 220 * 1024;   // dynamic shared memory of the single-block tail
 constexpr int LINE_NW = 32;         // warps per block of the chunked line solver (one line chunk each)
 
 template <class T>
@@ -53,6 +58,7 @@ struct Tail {
     int nl;
     int line;
     int nu;
+    int stage_b;             // the dense coarsest inverse is staged in shared memory
 };
 
 struct MG {
@@ -62,6 +68,8 @@ struct MG {
     Lvl<float> Lf[MAXL];
     double *B;               // dense coarsest inverse (double)
     int nc;
+    size_t tail_shm;         // dynamic shared memory of the tail kernel
+    int stage_b;
 };
 
 int mg_levels(const MG *mg) { return mg->nlev; }
@@ -411,55 +419,110 @@ __device__ void blk_smooth(const Lvl<T> &L, int color, bool line)
     }
 }
 
+// bytes of shared memory a tail level occupies: coefficients, Thomas factors,
+// line scratch, x and r; the coarsest level holds x and r only
+template <class T>
+__host__ __device__ inline size_t tail_level_bytes(int64_t n, bool coarsest) { return sizeof(T) * (size_t)n * (coarsest ? 2 : 9); }
+// dense-solve scratch ahead of the levels: B (when staged), r, partial sums
+// and reduction (max(1024, nc))
+__host__ __device__ inline int tail_part(int nc) { return nc > 1024 ? nc : 1024; }
+inline size_t tail_dense_bytes(int nc, bool stage_b)
+{
+    return sizeof(double) * ((stage_b ? (size_t)nc * nc : 0) + (size_t)nc + (size_t)tail_part(nc));
+}
+
 template <class T>
 __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
 {
-    extern __shared__ double sh[];
+    extern __shared__ __align__(16) double sh[];
+    __shared__ Lvl<T> S[MAXL];
     const int nl = tl.nl;
+    const int nc = (int)tl.L[nl - 1].n;
+    double *Bs = sh;
+    double *dr = sh + (tl.stage_b ? (size_t)nc * nc : 0), *red = dr + nc;
+    T *base = (T *)(red + tail_part(nc));
+    if (threadIdx.x == 0) {
+        T *q = base;
+        for (int l = 0; l < nl; l++) {
+            Lvl<T> v = tl.L[l];
+            const int64_t n = v.n;
+            if (l + 1 < nl) {
+                v.aE = q; q += n; v.aN = q; q += n; v.aT = q; q += n; v.diag = q; q += n;
+                v.cp = q; q += n; v.minv = q; q += n; v.tmp = q; q += n;
+            }
+            v.x = q; q += n; v.r = q; q += n;
+            S[l] = v;
+        }
+    }
+    __syncthreads();
+    // stage the coefficients of the smoothed levels, the inverse, r and x of the first level
+    for (int l = 0; l + 1 < nl; l++) {
+        const Lvl<T> &G = tl.L[l];
+        const Lvl<T> &V = S[l];
+        for (int t = threadIdx.x; t < V.n; t += blockDim.x) {
+            V.aE[t] = G.aE[t]; V.aN[t] = G.aN[t]; V.aT[t] = G.aT[t];
+            V.diag[t] = G.diag[t]; V.cp[t] = G.cp[t]; V.minv[t] = G.minv[t];
+        }
+    }
+    if (tl.stage_b)
+        for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) Bs[t] = B[t];
+    for (int t = threadIdx.x; t < S[0].n; t += blockDim.x) { S[0].r[t] = tl.L[0].r[t]; S[0].x[t] = tl.L[0].x[t]; }
+    __syncthreads();
     // descend
     for (int l = 0; l < nl - 1; l++) {
-        const Lvl<T> &L = tl.L[l];
+        const Lvl<T> &L = S[l];
         for (int s = 0; s < tl.nu; s++) {
             blk_smooth(L, 0, tl.line != 0); __syncthreads();
             blk_smooth(L, 1, tl.line != 0); __syncthreads();
         }
-        const Lvl<T> &Cc = tl.L[l + 1];
+        const Lvl<T> &Cc = S[l + 1];
         for (int t = threadIdx.x; t < Cc.n; t += blockDim.x) {
             int I = t % Cc.nx, r2 = t / Cc.nx, J = r2 % Cc.ny, K = r2 / Cc.ny;
             restrict_cell(L, Cc, I, J, K);
         }
         __syncthreads();
     }
-    // coarsest: x = B (r - mean r), then remove the mean of x
+    // coarsest: x = B (r - mean r), then remove the mean of x; each entry of
+    // B r is split over g = blockDim / nc threads
     {
-        const Lvl<T> &L = tl.L[nl - 1];
-        const int n = (int)L.n;
-        double *rr = sh, *red = sh + n;
+        const Lvl<T> &L = S[nl - 1];
+        const double *Bp = tl.stage_b ? Bs : B;
         double s = 0.0;
-        for (int t = threadIdx.x; t < n; t += blockDim.x) { rr[t] = (double)L.r[t]; s += rr[t]; }
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) { dr[t] = (double)L.r[t]; s += dr[t]; }
         red[threadIdx.x] = s;
         __syncthreads();
         for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-        double mean = red[0] / n;
+        const double mean = red[0] / nc;
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) dr[t] -= mean;
+        __syncthreads();
+        const int g = nc <= (int)blockDim.x ? (int)blockDim.x / nc : 1;
+        for (int q = threadIdx.x; q < nc * g; q += blockDim.x) {
+            const int t = q % nc, h = q / nc;
+            double acc = 0.0;
+            for (int u = h; u < nc; u += g) acc += Bp[(size_t)u * nc + t] * dr[u];   // B symmetric: column t
+            red[q] = acc;                                        // nc * g <= tail_part(nc)
+        }
         __syncthreads();
         double sx = 0.0;
-        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) {
             double acc = 0.0;
-            for (int u = 0; u < n; u++) acc += B[(size_t)u * n + t] * (rr[u] - mean);   // B symmetric: column t
-            rr[n + blockDim.x + t] = acc;
+            for (int h = 0; h < g; h++) acc += red[h * nc + t];
+            dr[t] = acc;
             sx += acc;
         }
+        __syncthreads();
         red[threadIdx.x] = sx;
         __syncthreads();
         for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-        double mx = red[0] / n;
-        for (int t = threadIdx.x; t < n; t += blockDim.x) L.x[t] = (T)(rr[n + blockDim.x + t] - mx);
+        const double mx = red[0] / nc;
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) L.x[t] = (T)(dr[t] - mx);
         __syncthreads();
     }
     // ascend
     for (int l = nl - 2; l >= 0; l--) {
-        const Lvl<T> &L = tl.L[l];
-        const Lvl<T> &Cc = tl.L[l + 1];
+        const Lvl<T> &L = S[l];
+        const Lvl<T> &Cc = S[l + 1];
         for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
             int i = t % L.nx, r2 = t / L.nx, j = r2 % L.ny, k = r2 / L.ny;
             L.x[sidx(L, k, j, i)] += Cc.x[sidx(Cc, k / L.cz, j / L.cy, i / L.cx)];
@@ -470,6 +533,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
             blk_smooth(L, 0, tl.line != 0); __syncthreads();
         }
     }
+    for (int t = threadIdx.x; t < S[0].n; t += blockDim.x) tl.L[0].x[t] = S[0].x[t];
 }
 
 // --------------------------------------------------------- level-0 in/out
@@ -504,9 +568,8 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
         Tail<T> tl{};
         tl.nl = mg->nlev - l;
         for (int q = 0; q < tl.nl; q++) tl.L[q] = L[l + q];
-        tl.line = mg->line; tl.nu = mg->nu;
-        size_t shm = sizeof(double) * (2 * (size_t)mg->nc + 2 * 1024);
-        TG_PROF(C, "mg_tail", k_tail<T><<<1, 1024, shm, st>>>(tl, mg->B));
+        tl.line = mg->line; tl.nu = mg->nu; tl.stage_b = mg->stage_b;
+        TG_PROF(C, "mg_tail", k_tail<T><<<1, 1024, mg->tail_shm, st>>>(tl, mg->B));
         return;
     }
     Lvl<T> &F = L[l];
@@ -569,7 +632,7 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         F.h0 = (F.nx + 1) >> 1;
         auto can = [](int m) { return m >= 4 && (m % 2) == 0; };
         F.cx = can(F.nx) ? 2 : 1; F.cy = can(F.ny) ? 2 : 1; F.cz = can(F.nz) ? 2 : 1;
-        bool coarsen = F.n > 512 && (F.cx * F.cy * F.cz) > 1 && mg->nlev < MAXL;
+        bool coarsen = F.n > COARSEST_CELLS && (F.cx * F.cy * F.cz) > 1 && mg->nlev < MAXL;
         if (!coarsen) { F.cx = F.cy = F.cz = 1; break; }
         Lvl<T> &Cn = L[mg->nlev++];
         Cn = Lvl<T>{};
@@ -589,13 +652,22 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         if (mg->line) k_line_factors<T><<<dim3((L[l].nx + 31) / 32, (L[l].nz + 7) / 8), dim3(32, 8), 0, st>>>(L[l]);
     }
     if (mg->line) set_line_smem_attrs<T>();
-    mg->tail_start = mg->nlev - 1;
-    while (mg->tail_start > 0 && L[mg->tail_start - 1].n <= TAIL_CELLS) mg->tail_start--;
-
     // dense coarsest inverse of (A + 11^T/n) in the level's own (split) order
     Lvl<T> &Lc = L[mg->nlev - 1];
     if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells (use even interior sizes)"};
     const int nc = (int)Lc.n;
+    // the single-block tail: as many of the smallest levels (<= TAIL_CELLS each)
+    // as fit in its shared memory next to the dense-solve scratch
+    mg->stage_b = tail_dense_bytes(nc, true) + tail_level_bytes<T>(nc, true) <= (size_t)TAIL_SMEM / 2;
+    size_t used = tail_dense_bytes(nc, mg->stage_b) + tail_level_bytes<T>(nc, true);
+    if (used > (size_t)TAIL_SMEM) throw CudaError{cudaErrorInvalidValue, "coarsest multigrid level too large"};
+    mg->tail_start = mg->nlev - 1;
+    while (mg->tail_start > 0 && L[mg->tail_start - 1].n <= TAIL_CELLS &&
+           used + tail_level_bytes<T>(L[mg->tail_start - 1].n, false) <= (size_t)TAIL_SMEM) {
+        used += tail_level_bytes<T>(L[mg->tail_start - 1].n, false);
+        mg->tail_start--;
+    }
+    mg->tail_shm = used;
     std::vector<T> hE(nc), hN(nc), hT(nc);
     TG_CUDA(cudaMemcpyAsync(hE.data(), Lc.aE, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaMemcpyAsync(hN.data(), Lc.aN, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
@@ -620,8 +692,7 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
     if (!dense_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
     mg->B = (double *)dalloc(C, sizeof(double) * (size_t)nc * nc);
     mg->nc = nc;
-    size_t shm = sizeof(double) * (2 * (size_t)nc + 2 * 1024);
-    TG_CUDA(cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    TG_CUDA(cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM));
     TG_CUDA(cudaMemcpyAsync(mg->B, inv.data(), sizeof(double) * (size_t)nc * nc, cudaMemcpyHostToDevice, st));
     TG_CUDA(cudaStreamSynchronize(st));
     TG_CUDA(cudaGetLastError());
