@@ -400,22 +400,130 @@ __global__ void k_prolong(Lvl<T> F, Lvl<T> Cc)
 }
 
 // -------------------------------------------------------- single-block tail
+// The tail runs every sweep of a level on one block, so its cost is the
+// instruction latency of the block's active warps. Rows (k, j) are spread over
+// the warps and the cells of a row over the lanes (one index division per
+// row, none per cell); a j-line is solved by a segment of P lanes (P a power
+// of two, P >= min(ny, 32)), each lane a chunk of consecutive cells: the
+// forward and backward Thomas recurrences are first-order affine maps, which
+// the segment composes with a shuffle scan.
+
+// red-black point Gauss-Seidel sweep of one colour
 template <class T>
-__device__ void blk_smooth(const Lvl<T> &L, int color, bool line)
+__device__ void blk_smooth_points(const Lvl<T> &L, int color)
 {
-    if (line) {
-        int rowcnt = (L.nx + 1) >> 1;
-        for (int t = threadIdx.x; t < rowcnt * L.nz; t += blockDim.x) {
-            int k = t / rowcnt, tt = t % rowcnt;
-            int q = (color ^ k) & 1;
-            int cnt = q ? (L.nx >> 1) : ((L.nx + 1) >> 1);
-            if (tt < cnt) line_solve(L, k, 2 * tt + q);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int rows = L.ny * L.nz;
+    for (int r = warp; r < rows; r += nw) {
+        const int k = r / L.ny, j = r - k * L.ny;
+        const int p = (color ^ j ^ k) & 1;                     // parity of i for this colour
+        const int cnt = p ? (L.nx >> 1) : ((L.nx + 1) >> 1);
+        for (int m = lane; m < cnt; m += 32) point_update(L, k, j, 2 * m + p);
+    }
+}
+
+// zebra j-line sweep of one colour (lines at i of parity colour ^ k)
+template <class T>
+__device__ void blk_smooth_lines(const Lvl<T> &L, int color)
+{
+    const int ny = L.ny, nx = L.nx;
+    int P = 1;
+    while (P < ny && P < 32) P <<= 1;
+    const int cj = (ny + P - 1) / P;
+    const int lane = threadIdx.x & 31, sl = lane & (P - 1);
+    const int segs = (int)blockDim.x / P;
+    const int myseg = (int)threadIdx.x / P;
+    const int rowcnt = (nx + 1) >> 1;
+    const int nlines = rowcnt * L.nz;
+    const int j0 = sl * cj, j1 = min(j0 + cj, ny);
+    for (int b0 = 0; b0 < nlines; b0 += segs) {               // uniform over the block
+        const int t = b0 + myseg;
+        bool on = false;
+        int k = 0, i = 0;
+        if (t < nlines) {
+            k = t / rowcnt;
+            const int tt = t - k * rowcnt, q = (color ^ k) & 1;
+            const int cnt = q ? (nx >> 1) : rowcnt;
+            if (tt < cnt) { on = true; i = 2 * tt + q; }
         }
-    } else {
-        for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
-            int i = t % L.nx, r2 = t / L.nx, j = r2 % L.ny, k = r2 / L.ny;
-            if (((i + j + k) & 1) == color) point_update(L, k, j, i);
+        const int c0 = on ? sidx(L, k, 0, i) : 0;
+        // forward: dp_j = minv_j aS_j dp_{j-1} + minv_j rhs_j; b_j kept in tmp
+        T A = T(1), B = T(0);
+        if (on)
+            for (int j = j0; j < j1; j++) {
+                const int c = c0 + j * nx;
+                const T mi = L.minv[c];
+                const T a = j > 0 ? mi * L.aN[c - nx] : T(0);
+                const T b = mi * (L.r[c] + nb_sum(L, k, j, i, c, false));
+                L.tmp[c] = b;
+                B = a * B + b;
+                A = a * A;
+            }
+        for (int d = 1; d < P; d <<= 1) {
+            const T Ap = __shfl_up_sync(0xffffffffu, A, d, P), Bp = __shfl_up_sync(0xffffffffu, B, d, P);
+            if (sl >= d) { B = A * Bp + B; A = A * Ap; }
         }
+        T dp = __shfl_up_sync(0xffffffffu, B, 1, P);
+        if (sl == 0) dp = T(0);
+        if (on)
+            for (int j = j0; j < j1; j++) {
+                const int c = c0 + j * nx;
+                const T a = j > 0 ? L.minv[c] * L.aN[c - nx] : T(0);
+                dp = a * dp + L.tmp[c];
+                L.tmp[c] = dp;
+            }
+        // backward: x_j = -cp_j x_{j+1} + dp_j, composed from the top
+        T Cm = T(1), D = T(0);
+        if (on)
+            for (int j = j1 - 1; j >= j0; j--) {
+                const int c = c0 + j * nx;
+                const T cc = -L.cp[c];
+                D = cc * D + L.tmp[c];
+                Cm = cc * Cm;
+            }
+        for (int d = 1; d < P; d <<= 1) {
+            const T Cn = __shfl_down_sync(0xffffffffu, Cm, d, P), Dn = __shfl_down_sync(0xffffffffu, D, d, P);
+            if (sl + d < P) { D = Cm * Dn + D; Cm = Cm * Cn; }
+        }
+        T xv = __shfl_down_sync(0xffffffffu, D, 1, P);
+        if (sl == P - 1) xv = T(0);
+        if (on)
+            for (int j = j1 - 1; j >= j0; j--) {
+                const int c = c0 + j * nx;
+                xv = L.tmp[c] - L.cp[c] * xv;
+                L.x[c] = xv;
+            }
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void blk_smooth(const Lvl<T> &L, int color, bool line)
+{
+    if (line) blk_smooth_lines(L, color);
+    else blk_smooth_points(L, color);
+}
+
+// restriction to every coarse cell (rows over warps, cells over lanes)
+template <class T>
+__device__ void blk_restrict(const Lvl<T> &F, const Lvl<T> &Cc)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < Cc.ny * Cc.nz; r += nw) {
+        const int K = r / Cc.ny, J = r - K * Cc.ny;
+        for (int I = lane; I < Cc.nx; I += 32) restrict_cell(F, Cc, I, J, K);
+    }
+}
+
+// x_fine += x_coarse (piecewise constant)
+template <class T>
+__device__ void blk_prolong(const Lvl<T> &F, const Lvl<T> &Cc)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < F.ny * F.nz; r += nw) {
+        const int k = r / F.ny, j = r - k * F.ny;
+        const int crow = ((k / F.cz) * Cc.ny + j / F.cy) * Cc.nx;
+        for (int i = lane; i < F.nx; i += 32)
+            F.x[(k * F.ny + j) * F.nx + spos(i, F.h0)] += Cc.x[crow + spos(i / F.cx, Cc.h0)];
     }
 }
 
@@ -475,11 +583,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
             blk_smooth(L, 0, tl.line != 0); __syncthreads();
             blk_smooth(L, 1, tl.line != 0); __syncthreads();
         }
-        const Lvl<T> &Cc = S[l + 1];
-        for (int t = threadIdx.x; t < Cc.n; t += blockDim.x) {
-            int I = t % Cc.nx, r2 = t / Cc.nx, J = r2 % Cc.ny, K = r2 / Cc.ny;
-            restrict_cell(L, Cc, I, J, K);
-        }
+        blk_restrict(L, S[l + 1]);
         __syncthreads();
     }
     // coarsest: x = B (r - mean r), then remove the mean of x; each entry of
@@ -522,11 +626,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
     // ascend
     for (int l = nl - 2; l >= 0; l--) {
         const Lvl<T> &L = S[l];
-        const Lvl<T> &Cc = S[l + 1];
-        for (int t = threadIdx.x; t < L.n; t += blockDim.x) {
-            int i = t % L.nx, r2 = t / L.nx, j = r2 % L.ny, k = r2 / L.ny;
-            L.x[sidx(L, k, j, i)] += Cc.x[sidx(Cc, k / L.cz, j / L.cy, i / L.cx)];
-        }
+        blk_prolong(L, S[l + 1]);
         __syncthreads();
         for (int s = 0; s < tl.nu; s++) {
             blk_smooth(L, 1, tl.line != 0); __syncthreads();
