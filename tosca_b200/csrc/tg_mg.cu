@@ -21,12 +21,12 @@
 // a chain of FMAs. A block solves 32 same-colour lines at once: each of its
 // warps takes one chunk of j, runs the forward and backward recurrences of
 // its chunk as affine maps (coalesced loads, all warps in flight), and the
-// chunk ends are combined in shared memory. The smallest levels (<= 4096
-// cells each, as many as fit) run as one single-block kernel that stages
-// their coefficients, unknowns and the dense coarsest inverse in shared
-// memory and performs all their sweeps, transfers and the coarsest solve
-// there: no launch latency, and shared-memory instead of L2 latency in the
-// sequential line recurrences.
+// chunk ends are combined in shared memory. The smallest levels (<= 512
+// cells each) run as one single-block kernel that stages their coefficients,
+// unknowns and the dense coarsest inverse in shared memory and performs all
+// their sweeps, transfers and the coarsest solve there. One block is issue-
+// and latency-bound, so larger levels run as grid launches (cheap inside the
+// step graph): at 4096 cells the single-block version took 80-130 us.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -47,7 +47,7 @@ struct Lvl {
 };
 
 constexpr int MAXL = 16;
-constexpr int TAIL_CELLS = 4096;
+constexpr int TAIL_CELLS = 512;
 constexpr int COARSEST_CELLS = 64;
 constexpr int TAIL_SMEM = 220 * 1024;   // dynamic shared memory of the single-block tail
 constexpr int LINE_NW = 32;         // warps per block of the chunked line solver (one line chunk each)
@@ -408,17 +408,17 @@ __global__ void k_prolong(Lvl<T> F, Lvl<T> Cc)
 // forward and backward Thomas recurrences are first-order affine maps, which
 // the segment composes with a shuffle scan.
 
-// red-black point Gauss-Seidel sweep of one colour
+// red-black point Gauss-Seidel sweep of one colour: thread -> (row, m), the
+// m-th cell of the colour in the row
 template <class T>
 __device__ void blk_smooth_points(const Lvl<T> &L, int color)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int rows = L.ny * L.nz;
-    for (int r = warp; r < rows; r += nw) {
+    const int half = (L.nx + 1) >> 1, n = half * L.ny * L.nz;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int r = t / half, m = t - r * half;
         const int k = r / L.ny, j = r - k * L.ny;
         const int p = (color ^ j ^ k) & 1;                     // parity of i for this colour
-        const int cnt = p ? (L.nx >> 1) : ((L.nx + 1) >> 1);
-        for (int m = lane; m < cnt; m += 32) point_update(L, k, j, 2 * m + p);
+        if (m < (p ? (L.nx >> 1) : half)) point_update(L, k, j, 2 * m + p);
     }
 }
 
