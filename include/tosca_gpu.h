@@ -123,6 +123,10 @@ enum {
     /* adjoint fields of tg_adjoint_*: adjoints of Ucont, Ucat, P and the
      * gradient of the objective with respect to TG_F_SOURCE */
     TG_F_UCONT_ADJ, TG_F_UCAT_ADJ, TG_F_P_ADJ, TG_F_SOURCE_ADJ,
+    /* turbine body force of the last step (read only, with turbines set):
+     * projected Cartesian force (lsourceFarmCat) and its face values
+     * (sourceFarmCont) */
+    TG_F_FARM_FORCE, TG_F_FARM_CONT,
     TG_F_COUNT
 };
 
@@ -208,6 +212,43 @@ tg_status tg_set_graphs(tg_ctx *ctx, int32_t on);
  * kernel). */
 tg_status tg_graph_info(tg_ctx *ctx, int64_t *replays, int32_t *capture_failed);
 
+/* --------------------------------------------------------------- wind farm -- */
+/* Uniform actuator-disk turbines: TOSCA's "uniformADM" with sampleType
+ * rotorDisk and CtType constant (a disk-based thrust coefficient C_T', axial
+ * induction 0). Per step, after the eddy viscosity (main.c:146,
+ * UpdateWindTurbines turbines.c:39-170): the velocity is sampled at the disk
+ * points by trilinear interpolation (turbines_sampling.c:174-262,
+ * inline.h:6904-7265), the disk-averaged in-plane speed U gives the point
+ * forces 0.5 U^2 dA C_T' along the axis (turbines_force.c:219-383), a
+ * Gaussian projection spreads them to the cells (turbines_force.c:858-910)
+ * and their central face values times the face areas
+ * (bodyForceCartesian2Contravariant, turbines_force.c:1741-1835) are added to
+ * the momentum right-hand side of every stage (ueqn_solvers.c:1340-1344).
+ * Disk points follow turbines_io.c:1925-2000 with zero tilt and precone;
+ * projection cells are the interior cells within r_tip + 2.628 epsilon of the
+ * centre (turbines_parallel.c:40-135). */
+typedef struct tg_turbine {
+    double center[3];        /* rotor centre (x, y, z), mesh coordinates              */
+    double axis[3];          /* rotor axis, pointing upstream (rtrDir)                */
+    double up[3];            /* azimuth-zero direction of the disk points (twrDir)    */
+    double r_tip, r_hub;     /* tip and hub radius (r_hub > 0)                        */
+    double epsilon;          /* width of the Gaussian projection                      */
+    double ct;               /* C_T'                                                  */
+    int32_t n_radial, n_azimuth;
+} tg_turbine;
+
+/* Define the farm (after tg_set_mesh_nodes); n = 0 removes it. rho: air
+ * density of thrust and power (the body force is per unit density). */
+tg_status tg_set_turbines(tg_ctx *ctx, int32_t n, const tg_turbine *turbines, double rho);
+/* Change the C_T' of every turbine (n values) without rebuilding the geometry. */
+tg_status tg_set_turbine_ct(tg_ctx *ctx, const double *ct);
+/* Values of the last step per turbine (n each; any pointer may be NULL): disk
+ * speed U, thrust rho sum(B . axis), power thrust U; power_sum: the farm power
+ * summed over the steps since the last reset (reset != 0 zeroes it after the
+ * read). */
+tg_status tg_turbine_state(tg_ctx *ctx, double *uref, double *thrust, double *power,
+                           double *power_sum, int32_t reset);
+
 /* ----------------------------------------------------------------- adjoint -- */
 /* Discrete adjoint of tg_step. No counterpart in the reference: TOSCA has no
  * adjoint. Adjoint fields are exchanged with tg_set_field / tg_get_field
@@ -223,6 +264,16 @@ typedef struct tg_adjoint_stats {
     int32_t poisson_iterations;    /* Krylov iterations of the transposed pressure solves   */
     double  seconds;               /* device time of the call                               */
 } tg_adjoint_stats;
+
+/* Farm adjoint: the gradient of a functional with respect to the C_T' of the
+ * turbines accumulates in every reversed step (the farm forces enter each
+ * step). With the power objective on, each reversed step also adds the
+ * derivatives of the farm power at the step's start state, so that a
+ * reversal seeded with zero adjoint fields yields the gradient of the farm
+ * power summed over the steps (tg_turbine_state's power_sum). */
+tg_status tg_set_farm_objective(tg_ctx *ctx, int32_t on);
+/* d(functional)/dC_T' per turbine (n values); reset != 0 zeroes it after the read. */
+tg_status tg_ct_gradient(tg_ctx *ctx, double *grad, int32_t reset);
 
 /* Vector-Jacobian product of one step: the context holds the state at the
  * start of a step and the adjoint fields hold the adjoints of the state after

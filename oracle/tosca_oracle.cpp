@@ -60,6 +60,17 @@ struct Csr {
     std::vector<double>  val;
 };
 
+// one uniform actuator disk (tosca_oracle_farm.inc)
+struct Turbine {
+    tg_turbine d{};
+    V3 rtrAxis{}, rotCenter{};
+    std::vector<V3> points;
+    std::vector<double> dA;
+    std::vector<size_t> sphere;                 // controlledCells (interior, k-j-i order)
+    std::vector<int> ci, cj, ck;                 // closestCells
+    double Ct = 0.0, rtrAvgMagU = 0.0, rtrThrust = 0.0, aeroPwr = 0.0;
+};
+
 } // namespace
 
 struct tg_ctx {
@@ -79,6 +90,12 @@ struct tg_ctx {
     // state
     std::vector<V3> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, fp, div1, div2, div3, visc1, visc2, visc3;
     std::vector<V3> source;                     // ueqn->sourceU (cell-centred Cartesian body force)
+    // wind farm: turbines, lsourceFarmCat, sourceFarmCont
+    std::vector<Turbine> farm;
+    double farm_rho = 1.0, farm_power_sum = 0.0;
+    bool farm_objective = false;
+    std::vector<V3> farm_cat, farm_cont;
+    std::vector<double> ct_grad;
     // adjoints (tosca_oracle_adjoint.inc)
     std::vector<V3> ucont_adj, ucat_adj, source_adj;
     std::vector<double> p_adj;
@@ -1334,6 +1351,8 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
     }
 }
 
+#include "tosca_oracle_farm.inc"
+
 // ExplicitRhsU, ueqn_solvers.c:1276-1407
 void explicitRhsU(tg_ctx &C)
 {
@@ -1353,6 +1372,8 @@ void explicitRhsU(tg_ctx &C)
             for (size_t q = 0; q < G; q++) C.rhs[q] = C.rhs[q] + 1.0 * C.btheta[q];
         }
     }
+    if (!C.farm.empty())                                // ueqn_solvers.c:1340-1344
+        for (size_t q = 0; q < G; q++) C.rhs[q] = C.rhs[q] + 1.0 * C.farm_cont[q];
     formU(C, C.rhs, 1.0);
     if (C.c.source) sourceU(C, C.rhs);                 // ueqn_solvers.c:1365-1370
     if (C.c.mean_grad_p) meanGradPForcing(C, C.rhs);
@@ -1525,6 +1546,7 @@ int step(tg_ctx &C, tg_stats *st)
 {
     C.ucont_o = C.ucont;                                 // main.c:81
     if (C.c.les) { updateNut(C); updateWallModels(C); }  // main.c:112-117
+    if (!C.farm.empty()) updateWindTurbines(C);          // main.c:144-147
     gradP(C);                                            // main.c:160-167
     if (C.c.buoyancy) {                                  // main.c:175-192
         if (C.it > C.c.it_start) C.btheta_o = C.btheta;
@@ -1563,6 +1585,8 @@ std::vector<V3> *vecField(tg_ctx &C, int w)
     case TG_F_UCONT_O: return &C.ucont_o; case TG_F_RHS: return &C.rhs; case TG_F_DP: return &C.dp;
     case TG_F_BTHETA: return &C.btheta; case TG_F_SOURCE: return &C.source;
     case TG_F_UCONT_ADJ: return &C.ucont_adj; case TG_F_UCAT_ADJ: return &C.ucat_adj; case TG_F_SOURCE_ADJ: return &C.source_adj;
+    case TG_F_FARM_FORCE: return C.farm.empty() ? nullptr : &C.farm_cat;
+    case TG_F_FARM_CONT: return C.farm.empty() ? nullptr : &C.farm_cont;
     default: return nullptr;
     }
 }
@@ -1828,6 +1852,61 @@ int32_t tor_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+// wind farm (tosca_oracle_farm.inc)
+tg_status tor_set_turbines(tg_ctx *C, int32_t n, const tg_turbine *tb, double rho)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
+        if (n < 0 || (n > 0 && !tb) || !(rho > 0)) return fail(C, TG_ERR_BAD_ARG, "bad turbine arguments");
+        for (int t = 0; t < n; t++)
+            if (tb[t].n_radial < 2 || tb[t].n_azimuth < 1 || !(tb[t].r_tip > tb[t].r_hub) || !(tb[t].r_hub > 0) || !(tb[t].epsilon > 0))
+                return fail(C, TG_ERR_BAD_ARG, "bad turbine description");
+        setTurbines(*C, n, tb, rho);
+        return TG_OK;
+    });
+}
+tg_status tor_set_turbine_ct(tg_ctx *C, const double *ct)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (C->farm.empty()) return fail(C, TG_ERR_STATE, "no turbines");
+        for (size_t t = 0; t < C->farm.size(); t++) C->farm[t].Ct = ct[t];
+        return TG_OK;
+    });
+}
+tg_status tor_turbine_state(tg_ctx *C, double *uref, double *thrust, double *power, double *power_sum, int32_t reset)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (C->farm.empty()) return fail(C, TG_ERR_STATE, "no turbines");
+        for (size_t t = 0; t < C->farm.size(); t++) {
+            if (uref) uref[t] = C->farm[t].rtrAvgMagU;
+            if (thrust) thrust[t] = C->farm[t].rtrThrust;
+            if (power) power[t] = C->farm[t].aeroPwr;
+        }
+        if (power_sum) *power_sum = C->farm_power_sum;
+        if (reset) C->farm_power_sum = 0.0;
+        return TG_OK;
+    });
+}
+tg_status tor_set_farm_objective(tg_ctx *C, int32_t on)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (C->farm.empty()) return fail(C, TG_ERR_STATE, "no turbines");
+        C->farm_objective = on != 0;
+        return TG_OK;
+    });
+}
+tg_status tor_ct_gradient(tg_ctx *C, double *grad, int32_t reset)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (C->farm.empty()) return fail(C, TG_ERR_STATE, "no turbines");
+        for (size_t t = 0; t < C->farm.size(); t++) {
+            if (grad) grad[t] = C->ct_grad[t];
+            if (reset) C->ct_grad[t] = 0.0;
+        }
+        return TG_OK;
+    });
 }
 
 // Discrete adjoint of one step (test infrastructure, see tosca_oracle_adjoint.inc).

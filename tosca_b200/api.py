@@ -30,6 +30,7 @@ FIELDS = [
     "UCONT", "UCAT", "UCONT_O", "RHS", "DP", "BTHETA",
     "P", "PHI", "NUT", "TMPRT", "TAUWALL", "SOURCE",
     "UCONT_ADJ", "UCAT_ADJ", "P_ADJ", "SOURCE_ADJ",
+    "FARM_FORCE", "FARM_CONT",
 ]
 F = {name: i for i, name in enumerate(FIELDS)}
 SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT", "P_ADJ"}
@@ -62,6 +63,32 @@ class TgConfig(C.Structure):
         ("device", C.c_int32),
         ("source", C.c_int32),
     ]
+
+
+class TgTurbine(C.Structure):
+    """tg_turbine: one uniform actuator disk (C_T', sampled on the rotor disk)."""
+    _fields_ = [
+        ("center", C.c_double * 3),
+        ("axis", C.c_double * 3),
+        ("up", C.c_double * 3),
+        ("r_tip", C.c_double),
+        ("r_hub", C.c_double),
+        ("epsilon", C.c_double),
+        ("ct", C.c_double),
+        ("n_radial", C.c_int32),
+        ("n_azimuth", C.c_int32),
+    ]
+
+    @classmethod
+    def make(cls, center, axis=(-1.0, 0.0, 0.0), up=(0.0, 0.0, 1.0), r_tip=63.0, r_hub=1.5, epsilon=20.0,
+             ct=1.33, n_radial=10, n_azimuth=24):
+        t = cls()
+        t.center[:] = center
+        t.axis[:] = axis
+        t.up[:] = up
+        t.r_tip, t.r_hub, t.epsilon, t.ct = r_tip, r_hub, epsilon, ct
+        t.n_radial, t.n_azimuth = n_radial, n_azimuth
+        return t
 
 
 class TgAdjointStats(C.Structure):
@@ -160,6 +187,11 @@ _SIGS = {
     "sync_pressure": (C.c_int, [C.c_void_p]),
     "step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
     "step_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
+    "set_turbines": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TgTurbine), C.c_double]),
+    "set_turbine_ct": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "turbine_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int32]),
+    "set_farm_objective": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ct_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
 }
 
 # adjoint entry points (the CPU restatement exports tor_adjoint_step only) and
@@ -333,6 +365,35 @@ class Solver:
         st = TgAdjointStats()
         self._check(self.fns["adjoint_reverse"](self.h, C.byref(st)), "adjoint_reverse")
         return st
+
+    # -------------------------------------------------------------- turbines
+    def set_turbines(self, turbines, rho: float = 1.225):
+        """Define the actuator-disk farm (a sequence of TgTurbine; empty removes it)."""
+        n = len(turbines)
+        arr = (TgTurbine * max(n, 1))(*turbines)
+        self._check(self.fns["set_turbines"](self.h, n, arr, rho), "set_turbines")
+        self.n_turbines = n
+
+    def set_turbine_ct(self, ct):
+        ct = np.ascontiguousarray(ct, dtype=np.float64)
+        self._check(self.fns["set_turbine_ct"](self.h, _ptr(ct)), "set_turbine_ct")
+
+    def turbine_state(self, reset: bool = False) -> dict:
+        """Last step's disk speed, thrust and power per turbine, and the summed farm power."""
+        n = self.n_turbines
+        u, th, pw = np.zeros(n), np.zeros(n), np.zeros(n)
+        ps = C.c_double()
+        self._check(self.fns["turbine_state"](self.h, _ptr(u), _ptr(th), _ptr(pw), C.byref(ps), 1 if reset else 0),
+                    "turbine_state")
+        return {"uref": u, "thrust": th, "power": pw, "power_sum": ps.value}
+
+    def set_farm_objective(self, on: bool):
+        self._check(self.fns["set_farm_objective"](self.h, 1 if on else 0), "set_farm_objective")
+
+    def ct_gradient(self, reset: bool = False) -> np.ndarray:
+        g = np.zeros(self.n_turbines)
+        self._check(self.fns["ct_gradient"](self.h, _ptr(g), 1 if reset else 0), "ct_gradient")
+        return g
 
     def set_graphs(self, on: bool):
         """Replay steps as CUDA graphs (default on) or launch them kernel by kernel."""

@@ -182,6 +182,28 @@ def abl_case(nx: int = 256, ny: int = 256, nz: int = 128, Lx: float = 2560.0, Ly
     return cfg, nodes, ucat, p
 
 
+def farm_case(nx: int = 384, ny: int = 256, nz: int = 128, Lx: float = 3840.0, Ly: float = 2560.0,
+              H: float = 1000.0, rows: int = 4, cols: int = 4, D: float = 126.0, hub: float = 90.0,
+              sx: float = 7.0, sy: float = 5.0, epsilon: float = None, ct: float = 4.0 / 3.0,
+              r_hub: float = 1.5, n_radial: int = 16, n_azimuth: int = 48, **kw):
+    """ABL (abl_case, flow along +x) with rows x cols uniform actuator disks:
+    diameter D at hub height `hub`, spaced sx D along x and sy D along y and
+    centred in the domain, axes facing the wind (-x), C_T' = ct, Gaussian
+    width epsilon (default twice the x spacing). Returns the abl_case tuple and
+    the list of TgTurbine."""
+    from .api import TgTurbine
+    cfg, nodes, ucat, p = abl_case(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, H=H, **kw)
+    eps = 2.0 * Lx / nx if epsilon is None else epsilon
+    turbines = []
+    for r in range(rows):
+        for c in range(cols):
+            x = 0.5 * Lx + (r - 0.5 * (rows - 1)) * sx * D
+            y = 0.5 * Ly + (c - 0.5 * (cols - 1)) * sy * D
+            turbines.append(TgTurbine.make((x, y, hub), axis=(-1.0, 0.0, 0.0), up=(0.0, 0.0, 1.0), r_tip=0.5 * D,
+                                           r_hub=r_hub, epsilon=eps, ct=ct, n_radial=n_radial, n_azimuth=n_azimuth))
+    return cfg, nodes, ucat, p, turbines
+
+
 def hill_case(nx: int = 192, ny: int = 96, nz: int = 96, dt: float = 0.5, ustar: float = 0.3,
               z0: float = 0.1, kappa: float = 0.4, cs: float = 0.01, nu: float = 1.5e-5,
               theta0: float = 300.0, lapse: float = 0.001, ddt: int = DDT_FE, seed: int = 7, amp: float = 0.02,

@@ -993,11 +993,13 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
     const double bw[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
     const double aw[4] = {0.0, 0.5, 0.5, 1.0};
     const bool rk = T.nst == 4;
+    if (C->prm.farm) farm_adj_begin(C);
     for (int s = T.nst - 1; s >= 0; s--) {
         double cb = dt * (rk ? bw[s] : 1.0);
         double cn = (rk && s < 3) ? aw[s + 1] * dt : 0.0;
         TG_PROF(C, "adj_stage_rhs", k_adj_stage_rhs<<<gall(g), block3(), 0, st>>>(g, A.ra, A.usa, A.uta, cb, cn, T.u_o, A.dpa));
         if (C->prm.source) TG_PROF(C, "adj_source", k_adj_source<<<gall(g), block3(), 0, st>>>(g, C->m, A.ra, A.fa));
+        if (C->prm.farm) farm_adj_stage(C, A.ra);
         // FormU transposed
         TG_PROF(C, "adj_rhs_faces", k_adj_rhs_faces<<<gint(g), block3(), 0, st>>>(g, C->m, A.ra, 1.0, A.fpa));
         TG_PROF(C, "adj_cell_fp", k_adj_cell_fp<<<gfc(g), block3(), 0, st>>>(g, A.fpa, A.f1a, A.f2a, A.f3a));
@@ -1023,6 +1025,8 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
         k_adj_nut_bcs<<<grid, b2, 0, st>>>(g, A.na, C->prm);
         TG_PROF(C, "adj_smagorinsky", k_adj_smagorinsky<<<gint(g), block3(), 0, st>>>(g, C->m, T.ucat_n, A.na, C->prm, A.ca));
     }
+    // turbines: C_T' gradient and the adjoint of the Ucat they sampled
+    if (C->prm.farm) farm_adj_finish(C, T.ucat_n, A.ca);
     copy3(C, A.ua, A.uoa);
     TG_CUDA(cudaGetLastError());
     return rc;

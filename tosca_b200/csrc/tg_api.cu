@@ -79,6 +79,8 @@ bool vec_field(tg_ctx *C, int w, V3f<double> &out)
     case TG_F_RHS: out = s.rhs; return true;     case TG_F_DP: out = s.dp; return true;
     case TG_F_BTHETA: out = s.btheta; return true;
     case TG_F_SOURCE: out = s.source; return true;
+    case TG_F_FARM_FORCE: return farm_field(C, w, out);
+    case TG_F_FARM_CONT: return farm_field(C, w, out);
     default: return false;
     }
 }
@@ -269,6 +271,7 @@ tg_status tg_destroy(tg_ctx *C)
     if (C->stream) cudaStreamSynchronize(C->stream);
     graph_destroy(C);
     for (cudaStream_t a : C->aux) if (a) cudaStreamDestroy(a);
+    try { farm_destroy(C); } catch (...) {}
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);
@@ -303,6 +306,7 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
         C->orthogonal = (mx == 0.0);
         graph_destroy(C);          // the captured step refers to the old solver buffers
         C->graph_failed = false;
+        farm_destroy(C);           // turbine stencils refer to the old cell centres
         poisson_setup(C);
         C->has_mesh = true;
         return TG_OK;

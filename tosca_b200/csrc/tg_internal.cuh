@@ -83,6 +83,7 @@ struct FluxWork {
 struct State {
     V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, snap;
     V3f<double> source;          // ueqn->sourceU, cell-centred Cartesian body force
+    V3f<double> farmcont;        // farm->sourceFarmCont, contravariant turbine body force (tg_farm.cu)
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
@@ -92,12 +93,13 @@ struct Params {
     int bc[6];
     int nut_bc[6];
     double nut_bc_value[6];
-    int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source;
+    int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source, farm;
     double cs, nu, dt, t_ref, mgp[3], z0, kappa;
 };
 
 struct PoissonCtx;   // tg_poisson.cu
 struct AdjState;     // tg_adjoint.cu
+struct Farm;         // tg_farm.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -157,6 +159,7 @@ struct tg_ctx {
     std::string err;
     tg::PoissonCtx *pois = nullptr;
     tg::AdjState *adj = nullptr;         // adjoint fields, tape and checkpoints (tg_adjoint.cu)
+    tg::Farm *farm = nullptr;            // actuator-disk turbines (tg_farm.cu)
     bool taping = false;                 // the running step records its stage states
     // CUDA graph of a whole step (tg_step.cu): built on the first step that can
     // be captured, replayed afterwards
@@ -259,6 +262,17 @@ void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, do
 // capture or instantiation fails (nothing is left capturing)
 bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body);
 void adj_graph_destroy(tg_ctx *C);
+// wind farm (tg_farm.cu)
+void farm_update(tg_ctx *C);                 // sampling, forces, projection, face body force
+void farm_destroy(tg_ctx *C);
+bool farm_field(tg_ctx *C, int w, V3f<double> &out);   // TG_F_FARM_FORCE / TG_F_FARM_CONT
+// reversed step: adjoint of the face body force of one stage accumulates
+// from the stage's Rhs adjoint; farm_adj_finish turns the step's sum into the
+// C_T' gradient and the adjoint of the sampled Ucat (ucat_n: the taped Ucat
+// at the step's start; ca: its adjoint)
+void farm_adj_begin(tg_ctx *C);
+void farm_adj_stage(tg_ctx *C, V3f<double> ra);
+void farm_adj_finish(tg_ctx *C, V3f<double> ucat_n, V3f<double> ca);
 bool tape_in_work(const tg_ctx *C);          // the step tapes into the fixed work tape
 void set_device_step(tg_ctx *C);             // C->d_scal[SC_IT] <- C->it
 void graph_destroy(tg_ctx *C);

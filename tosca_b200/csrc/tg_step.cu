@@ -684,8 +684,9 @@ __global__ void k_cell_fp(Grid g, FluxWork<F> w)
 // cell (periodic, resetCellPeriodicFluxes) or a copy of this cell
 // (ueqn_solvers.c:949-990). With `fused` the kernel also forms
 // the rest of ExplicitRhsU at these faces in the reference's order:
-// Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += FormU, +=
-// sourceU (body force), += meanGradPForcing (ueqn_sources.c:3735-3822). MR:
+// Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += turbine body
+// force (ueqn_solvers.c:1340-1344), += FormU, += sourceU (body force), +=
+// meanGradPForcing (ueqn_sources.c:3735-3822). MR:
 // metric storage type; F: face-flux storage type.
 template <class MR, class F, bool fused>
 __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
@@ -706,6 +707,7 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
                 base = base + 1.0 * b;
             }
         }
+        if (p.farm) base = base + 1.0 * ld3(s.farmcont, c);
     } else {
         base = ld3(R, c);
     }
@@ -1267,6 +1269,7 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     if (C->taping) tape_step_start(C);
     if (C->prm.les) { update_nut(C); update_wall_models(C); }
     if (C->taping) tape_nut(C);
+    if (C->prm.farm) farm_update(C);
     grad_p(C);
     if (C->prm.buoyancy) {
         if (C->it > C->cfg.it_start)
