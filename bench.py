@@ -161,13 +161,24 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None):
         kw = dict(nx=48, ny=24, nz=24) if small else {}
         cfg, nodes, ucat, p, T = cases.hill_case(ddt=api.DDT_RK4, **kw)
         desc = "cosine hill %dx%dx%d cells, QUICK, buoyancy, RK4" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2)
+    elif name == "farm":
+        kw = (dict(nx=96, ny=64, nz=32, Lx=960.0, Ly=640.0, H=250.0, rows=2, cols=2, D=63.0, hub=60.0)
+              if small else {})
+        cfg, nodes, ucat, p, turbines = cases.farm_case(ddt=api.DDT_RK4, seed=20261203 + seed_offset, **kw)
+        T = None
+        desc = ("ABL %dx%dx%d cells with %d uniform actuator disks (C_T' %.3f, D %.0f m, %d points each), RK4, "
+                "Smagorinsky, Schumann wall, dt=0.25 s" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2, len(turbines),
+                                                          turbines[0].ct, 2 * turbines[0].r_tip,
+                                                          turbines[0].n_radial * turbines[0].n_azimuth))
     else:
         raise SystemExit(f"unknown workload {name}")
+    if name != "farm":
+        turbines = None
     cfg.poisson_rtol = 1e-30
     cfg.poisson_div_tol = DIV_TOL
     cfg.poisson_maxit = 400
     cfg.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
-    return cfg, nodes, ucat, p, T, desc
+    return cfg, nodes, ucat, p, T, desc, turbines
 
 
 def cpu_baseline(workload, steps, threads=None):
@@ -175,12 +186,14 @@ def cpu_baseline(workload, steps, threads=None):
     workload (same physics, fewer cells), all host threads."""
     import oracle
     from tosca_b200 import cases
-    cfg, nodes, ucat, p, T, desc = make_workload(workload, "fp64", small=True)
+    cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", small=True)
     cfg.poisson_rtol = 1e-8          # the reference's default poissonTol (peqn.c:54)
     cfg.poisson_div_tol = 0.0
     cfg.poisson_maxit = 20000
     s = oracle.solver(cfg)
     cases.setup(s, nodes, ucat, p, T)
+    if turbines:
+        s.set_turbines(turbines, 1.225)
     s.step(1)                        # warm-up
     t0 = time.perf_counter()
     st = s.step(steps)
@@ -261,6 +274,54 @@ def adjoint_ratio(dev, steps=4, warmup=8, cells=(128, 64, 64)):
     return out
 
 
+def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
+    """Gradient of the farm power summed over `steps` steps with respect to the
+    turbines' C_T' (tg_set_farm_objective) on the farm workload with a noSlip
+    ground (the adjoint has no wall-function transpose), forward in
+    `precision`: tg_adjoint_forward with binomial checkpointing in as many
+    device snapshots as half the free HBM holds, then tg_adjoint_reverse from
+    zero adjoint fields. Device time per reversed step against the device time
+    of a plain step of the same solver."""
+    import torch
+    import tosca_b200
+    from tosca_b200 import api, cases
+    cfg, nodes, ucat, p, turbines = cases.farm_case(ddt=api.DDT_RK4, wall=api.BC_NOSLIP)
+    cfg.poisson_rtol = 1e-30
+    cfg.poisson_div_tol = DIV_TOL
+    cfg.poisson_maxit = 400
+    cfg.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
+    cfg.device = dev
+    solver = tosca_b200.gpu_solver(cfg)
+    cases.setup(solver, nodes, ucat, p)
+    solver.set_turbines(turbines, 1.225)
+    solver.step(warmup)
+    fwd_ms = solver.step(fwd_steps).seconds / fwd_steps * 1e3
+    free, _ = torch.cuda.mem_get_info()
+    G = cfg.mx * cfg.my * cfg.mz
+    snap = 8 * (13 * G + cfg.cells)
+    work = 8 * (49 + 31) * G                       # adjoint work arrays and the work tape
+    nsnap = int(max(2, min(steps, 0.5 * (free - work) // snap)))
+    solver.set_farm_objective(True)
+    solver.ct_gradient(reset=True)
+    solver.turbine_state(reset=True)
+    fw = solver.adjoint_forward(steps, nsnap)
+    J = solver.turbine_state()["power_sum"]
+    shape = (cfg.mz, cfg.my, cfg.mx)
+    for k in ("UCONT_ADJ", "UCAT_ADJ", "SOURCE_ADJ"):
+        solver.set(k, np.zeros(shape + (3,)))
+    solver.set("P_ADJ", np.zeros(shape))
+    rv = solver.adjoint_reverse()
+    g = solver.ct_gradient()
+    solver.close()
+    adj_ms = rv.seconds / steps * 1e3
+    return {"workload": "farm workload with a noSlip ground, %s forward" % precision, "steps": steps, "snapshots": int(rv.snapshots), "forward_steps_in_reversal": int(rv.forward_steps),
+            "recorded_forward_ms_per_step": fw.seconds / steps * 1e3, "adjoint_ms_per_step": adj_ms,
+            "forward_ms_per_step": fwd_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+            "adjoint_poisson_iterations_per_step": rv.poisson_iterations / steps,
+            "objective": "farm power summed over the steps (W)", "J": J,
+            "dJ_dCt": [float(v) for v in g]}
+
+
 def kernel_table(L, h):
     import ctypes
     kernels = {}
@@ -307,7 +368,9 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill"])
+    ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm"])
+    ap.add_argument("--farm-adjoint-steps", type=int, default=200,
+                    help="farm workload: steps of the C_T' gradient of the summed farm power")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: the mixed step is the headline value, the FP64 step is timed beside it")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -363,10 +426,12 @@ def main():
         return float(t.item())
 
     def arm(precision):
-        cfg, nodes, ucat, p, T, desc = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells)
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells)
         cfg.device = dev
         solver = tosca_b200.gpu_solver(cfg)
         cases.setup(solver, nodes, ucat, p, T)
+        if turbines:
+            solver.set_turbines(turbines, 1.225)
         if args.warmup > 0:
             solver.step(args.warmup)
         # timed region: device time between events on the library's stream
@@ -443,6 +508,9 @@ def main():
     adj = None
     if rank == 0 and not args.no_adjoint and args.workload == "abl":
         adj = adjoint_ratio(dev)
+    farm_adj = None
+    if rank == 0 and not args.no_adjoint and args.workload == "farm" and args.farm_adjoint_steps > 0:
+        farm_adj = farm_adjoint(dev, head_prec, args.farm_adjoint_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -473,6 +541,7 @@ def main():
             "gpu_launches_note": "per-step count of the library's timed launches in the profiled steps x timed steps",
             "roofline": head["roofline"],
             "adjoint": adj,
+            "farm_adjoint": farm_adj,
             "cpu_baseline": cpu,
             "kernels_top": {k: {"ms_per_step": round(v["ms"] / max(1, args.profile_steps), 3),
                                 "launches_per_step": v["launches"] / max(1, args.profile_steps),
