@@ -68,6 +68,9 @@ enum {
 enum { TG_ILEFT = 0, TG_IRIGHT = 1, TG_JLEFT = 2, TG_JRIGHT = 3, TG_KLEFT = 4, TG_KRIGHT = 5 };
 
 /* ------------------------------------------------------------ configuration -- */
+/* temperature patch types (boundary/T, UpdateTemperatureBCs boundary.c:2052-2616) */
+enum { TG_TBC_ZERO_GRADIENT = 0, TG_TBC_FIXED_VALUE = 1, TG_TBC_FIXED_GRADIENT = 2, TG_TBC_PERIODIC = 3 };
+
 typedef struct tg_config {
     int32_t mx, my, mz;            /* DMDA extent incl. the one-cell physical ghost layer  */
     int32_t bc[6];                 /* velocity patch types, TG_ILEFT..TG_KRIGHT order       */
@@ -95,6 +98,13 @@ typedef struct tg_config {
     int32_t device;                /* CUDA device ordinal (ignored by the CPU restatement)  */
     int32_t source;                /* body force TG_F_SOURCE added by sourceU               */
                                    /* (ueqn_sources.c:2884-2980, ueqn_solvers.c:1369)       */
+    /* temperature transport (SolveTEqn, teqn.c:259; RK4 only): with teqn = 1
+     * the temperature TG_F_TMPRT is advanced after the projection and the
+     * buoyancy of the next step reads it */
+    int32_t teqn;
+    int32_t t_bc[6];               /* TG_TBC_* per patch (periodic where bc is periodic)    */
+    double  prandtl;               /* -Pr: molecular Prandtl number (no LES)                */
+    double  t_bc_value[6];         /* fixedValue: ghost value; fixedGradient: gradient      */
 } tg_config;
 
 /* per-call statistics */

@@ -100,6 +100,7 @@ struct tg_ctx {
     std::vector<V3> ucont_adj, ucat_adj, source_adj;
     std::vector<double> p_adj;
     std::vector<double> p, phi, nut, tmprt;
+    std::vector<double> tmprt_o;                // teqn->Tmprt_o (tosca_oracle_teqn.inc)
 
     // jLeft wall model arrays, indexed k*mx + i (tauWall, uMeanMag, uFilt)
     std::vector<double> twx, twy, twz, umean, ufx, ufy, ufz;
@@ -1352,6 +1353,7 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
 }
 
 #include "tosca_oracle_farm.inc"
+#include "tosca_oracle_teqn.inc"
 
 // ExplicitRhsU, ueqn_solvers.c:1276-1407
 void explicitRhsU(tg_ctx &C)
@@ -1545,6 +1547,7 @@ void syncPressure(tg_ctx &C)
 int step(tg_ctx &C, tg_stats *st)
 {
     C.ucont_o = C.ucont;                                 // main.c:81
+    if (C.c.teqn) C.tmprt_o = C.tmprt;                   // main.c:83-99
     if (C.c.les) { updateNut(C); updateWallModels(C); }  // main.c:112-117
     if (!C.farm.empty()) updateWindTurbines(C);          // main.c:144-147
     gradP(C);                                            // main.c:160-167
@@ -1555,8 +1558,10 @@ int step(tg_ctx &C, tg_stats *st)
     solveUEqn(C);                                        // main.c:195
     int rc = solvePEqn(C, st);                           // main.c:198
     contravariantToCartesian(C);                         // main.c:201
+    if (C.c.teqn) solveTEqn(C);                          // main.c:194-205
     double md = continuityError(C);                      // main.c:227
     if (st) st->max_divergence = md;
+    if (C.c.teqn) updateTemperatureBCs(C);               // main.c:274-278
     updateCartesianBCs(C);                               // main.c:281
     updateContravariantBCs(C);                           // main.c:284
     syncPressure(C);                                     // main.c:313
@@ -1569,7 +1574,7 @@ void allocState(tg_ctx &C)
     const size_t G = C.G;
     for (auto *v : {&C.ucont, &C.ucont_o, &C.ucat, &C.rhs, &C.dp, &C.btheta, &C.btheta_o, &C.gcont, &C.utmp, &C.fp, &C.source, &C.ucont_adj, &C.ucat_adj, &C.source_adj,
                     &C.div1, &C.div2, &C.div3, &C.visc1, &C.visc2, &C.visc3}) zero(*v, G);
-    for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt, &C.p_adj}) zero(*v, G);
+    for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt, &C.p_adj, &C.tmprt_o}) zero(*v, G);
     const size_t P = (size_t)C.mx * C.mz;
     for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz}) zero(*v, P);
 }
@@ -1665,6 +1670,13 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
         cfg->bc[TG_KRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_KLEFT] == TG_BC_WALL_SHUMANN ||
         cfg->bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN) return TG_ERR_BAD_ARG;
     if (cfg->dt <= 0) return TG_ERR_BAD_ARG;
+    if (cfg->teqn) {
+        if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
+        for (int p = 0; p < 6; p++) {
+            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
+            if ((cfg->t_bc[p] == TG_TBC_PERIODIC) != (cfg->bc[p] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
+        }
+    }
     tg_ctx *C = new (std::nothrow) tg_ctx();
     if (!C) return TG_ERR_ALLOC;
     C->c = *cfg;
@@ -1734,6 +1746,7 @@ tg_status tor_init_from_cartesian(tg_ctx *C, const double *ucat, int32_t halo)
         // SetTaylorGreenFieldU tail, initialField.c:1100-1204
         for (int k = 1; k < mz - 1; k++) for (int j = 1; j < my - 1; j++) for (int i = 1; i < mx - 1; i++)
             C->ucat[C->I(k, j, i)] = in[C->I(k, j, i)];
+        if (C->c.teqn) updateTemperatureBCs(*C);
         updateCartesianBCs(*C);
         auto &U = C->ucat;
         for (int k = 1; k < mz - 1; k++) for (int j = 1; j < my - 1; j++) for (int i = 0; i < mx - 1; i++) {
@@ -1918,6 +1931,7 @@ tg_status tor_adjoint_step(tg_ctx *C)
 {
     return guarded(C, [&]() -> tg_status {
         if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
+        if (C->c.teqn) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the temperature equation is not implemented");
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
         auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;

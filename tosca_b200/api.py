@@ -22,6 +22,7 @@ BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4 = 0, 1
+TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
 FIELDS = [
@@ -62,6 +63,10 @@ class TgConfig(C.Structure):
         ("it_start", C.c_int32),
         ("device", C.c_int32),
         ("source", C.c_int32),
+        ("teqn", C.c_int32),
+        ("t_bc", C.c_int32 * 6),
+        ("prandtl", C.c_double),
+        ("t_bc_value", C.c_double * 6),
     ]
 
 
@@ -145,6 +150,10 @@ class Config:
     it_start: int = 0
     device: int = 0
     source: int = 0
+    teqn: int = 0
+    t_bc: tuple = (TBC_PERIODIC,) * 6
+    prandtl: float = 0.7
+    t_bc_value: tuple = (0.0,) * 6
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

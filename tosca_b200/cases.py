@@ -12,7 +12,8 @@ Workloads (synthetic, seeded; no dataset is involved):
   abl        neutral pressure-driven ABL: periodic x/y, Schumann wall function
              (type -3) at the ground, slip top, Smagorinsky, tanh-stretched z
   hill       terrain-following mesh over a 2-D cosine hill, QUICK, stable
-             Boussinesq stratification with a frozen temperature field
+             Boussinesq stratification, frozen or transported temperature
+  farm       abl with uniform actuator disks
 """
 from __future__ import annotations
 
@@ -21,7 +22,7 @@ import math
 import numpy as np
 
 from .api import (BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, DDT_FE, DDT_RK4, DIV_CENTRAL, DIV_QUICK,
-                  NUTBC_FIXEDVALUE, NUTBC_PERIODIC, Config)
+                  NUTBC_FIXEDVALUE, NUTBC_PERIODIC, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_ZERO_GRADIENT, Config)
 
 
 # --------------------------------------------------------------------- grids
@@ -207,11 +208,13 @@ def farm_case(nx: int = 384, ny: int = 256, nz: int = 128, Lx: float = 3840.0, L
 def hill_case(nx: int = 192, ny: int = 96, nz: int = 96, dt: float = 0.5, ustar: float = 0.3,
               z0: float = 0.1, kappa: float = 0.4, cs: float = 0.01, nu: float = 1.5e-5,
               theta0: float = 300.0, lapse: float = 0.001, ddt: int = DDT_FE, seed: int = 7, amp: float = 0.02,
-              **kw):
+              teqn: bool = False, t_amp: float = 0.0, **kw):
     """Terrain-following cosine-hill case: periodic x/y, Schumann wall stress on
     the terrain (curvilinear branch), slip top, QUICK convection, Smagorinsky,
-    Boussinesq buoyancy from a frozen stable stratification theta = theta0 +
-    lapse * z (tRef = theta0)."""
+    Boussinesq buoyancy from a stable stratification theta = theta0 + lapse * z
+    (tRef = theta0), frozen, or with `teqn` transported (SolveTEqn, RK4:
+    adiabatic terrain, the lapse rate as the fixed gradient at the top, Pr 0.7)
+    with seeded +-t_amp K perturbations of the initial theta."""
     nodes = hill_nodes(nx, ny, nz, **kw)
     mx, my, mz = ny + 2, nz + 2, nx + 2
     H = float(nodes[0, my - 2, 0, 2])
@@ -245,6 +248,14 @@ def hill_case(nx: int = 192, ny: int = 96, nz: int = 96, dt: float = 0.5, ustar:
     T[:, :, -1] = T[:, :, 1]
     T[0] = T[-2]
     T[-1] = T[1]
+    if teqn:
+        cfg.ddt_scheme = DDT_RK4
+        cfg.teqn = 1
+        cfg.t_bc = (TBC_PERIODIC, TBC_PERIODIC, TBC_ZERO_GRADIENT, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_PERIODIC)
+        cfg.t_bc_value = (0.0, 0.0, 0.0, lapse, 0.0, 0.0)
+        cfg.prandtl = 0.7
+        if t_amp:
+            T = T + t_amp * uniform_noise(seed + 11, G, 0).reshape(mz, my, mx) * interior
     p = np.zeros((mz, my, mx))
     return cfg, nodes, ucat, p, T
 

@@ -209,6 +209,13 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
     if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 1) return TG_ERR_BAD_ARG;
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
+    if (cfg->teqn) {
+        if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
+        for (int p = 0; p < 6; p++) {
+            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
+            if ((cfg->t_bc[p] == TG_TBC_PERIODIC) != (cfg->bc[p] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
+        }
+    }
     tg_ctx *C = new (std::nothrow) tg_ctx();
     if (!C) return TG_ERR_ALLOC;
     C->cfg = *cfg;
@@ -228,6 +235,8 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         p.cs = cfg->cs; p.nu = cfg->nu; p.dt = cfg->dt; p.t_ref = cfg->t_ref;
         for (int q = 0; q < 3; q++) p.mgp[q] = cfg->mean_grad_p_value[q];
         p.z0 = cfg->wall_roughness; p.kappa = cfg->wall_kappa;
+        p.teqn = cfg->teqn; p.prandtl = cfg->prandtl;
+        for (int q = 0; q < 6; q++) { p.t_bc[q] = cfg->t_bc[q]; p.t_bc_value[q] = cfg->t_bc_value[q]; }
         C->it = cfg->it_start;
         const size_t G = (size_t)g.size();
         Metrics &m = C->m;
@@ -242,6 +251,10 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         alloc_precision_work(C);
         double **ss[] = {&st.p, &st.phi, &st.nut, &st.tmprt, &st.ssnap};
         for (auto **v : ss) *v = dallocd(C, G);
+        if (cfg->teqn) {
+            st.tdiv = dalloc3(C, G); st.tvisc = dalloc3(C, G);
+            st.trhs = dallocd(C, G); st.tmprt_o = dallocd(C, G); st.ttmp = dallocd(C, G);
+        }
         const size_t P = (size_t)g.mx * g.mz;
         double **ws[] = {&st.twx, &st.twy, &st.twz, &st.umean, &st.ufx, &st.ufy, &st.ufz};
         for (auto **v : ws) *v = dallocd(C, P);

@@ -84,6 +84,9 @@ struct State {
     V3f<double> ucont, ucont_o, ucat, rhs, dp, btheta, btheta_o, gcont, utmp, snap;
     V3f<double> source;          // ueqn->sourceU, cell-centred Cartesian body force
     V3f<double> farmcont;        // farm->sourceFarmCont, contravariant turbine body force (tg_farm.cu)
+    // temperature transport (tg_teqn.cu): lDivT, lViscT face fluxes, Rhs, Tmprt_o, TmprtTmp
+    V3f<double> tdiv, tvisc;
+    double *trhs, *tmprt_o, *ttmp;
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
@@ -95,6 +98,8 @@ struct Params {
     double nut_bc_value[6];
     int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source, farm;
     double cs, nu, dt, t_ref, mgp[3], z0, kappa;
+    int teqn, t_bc[6];
+    double prandtl, t_bc_value[6];
 };
 
 struct PoissonCtx;   // tg_poisson.cu
@@ -262,6 +267,9 @@ void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, do
 // capture or instantiation fails (nothing is left capturing)
 bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body);
 void adj_graph_destroy(tg_ctx *C);
+// temperature transport (tg_teqn.cu)
+void solve_t(tg_ctx *C);
+void update_temperature_bcs(tg_ctx *C);
 // wind farm (tg_farm.cu)
 void farm_update(tg_ctx *C);                 // sampling, forces, projection, face body force
 void farm_destroy(tg_ctx *C);

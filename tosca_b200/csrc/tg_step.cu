@@ -1249,6 +1249,7 @@ void sync_pressure(tg_ctx *C)
 void init_from_cartesian(tg_ctx *C)
 {
     const Grid g = C->g;
+    if (C->prm.teqn) update_temperature_bcs(C);
     update_cartesian_bcs(C);
     k_init_faces<<<gf(g), block3(), 0, C->stream>>>(g, C->m, C->s);
     update_contravariant_bcs(C);
@@ -1267,6 +1268,8 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     const int64_t G = C->g.size();
     TG_CUDA(cudaMemcpyAsync(C->s.ucont_o.x, C->s.ucont.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
     if (C->taping) tape_step_start(C);
+    if (C->prm.teqn)                    // main.c:83-99 (RK4: Tmprt_o = Tmprt)
+        TG_CUDA(cudaMemcpyAsync(C->s.tmprt_o, C->s.tmprt, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
     if (C->prm.les) { update_nut(C); update_wall_models(C); }
     if (C->taping) tape_nut(C);
     if (C->prm.farm) farm_update(C);
@@ -1282,7 +1285,9 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     else rc = poisson_solve(C, st);
     pressure_update_and_project(C);
     contra_to_cart(C);
+    if (C->prm.teqn) solve_t(C);        // main.c:194-205
     reduce_max_abs_div(C, C->d_scal + 16);
+    if (C->prm.teqn) update_temperature_bcs(C);   // main.c:274-278
     update_cartesian_bcs(C);
     update_contravariant_bcs(C);
     sync_pressure(C);

@@ -1,0 +1,229 @@
+// Temperature transport (SolveTEqn, teqn.c:259-276) with the explicit RK4
+// scheme (TeqnRK4, teqn_solvers.c:759-818): FormT (teqn_solvers.c:6-594)
+// evaluates per face the WENO3 convective flux -V^q weno3(T) and the diffusive
+// flux (g^{q1} dT/dcsi + g^{q2} dT/deta + g^{q3} dT/dzeta) ajc kappa_eff, the
+// cell budget times aj forms the right-hand side. kappa_eff = nu/Pr without
+// LES; with Smagorinsky the molecular part is dropped and kappa_eff = nu_t/Pr_t
+// with the stability-corrected Pr_t = 1/(1 + 2 l/delta), delta = (1/ajc)^(1/3),
+// l = min(delta, 7.6 nu_t/delta sqrt(tRef/|g dT/deta|)) in stable
+// stratification (teqn_solvers.c:180-195). Boundary ghosts follow
+// UpdateTemperatureBCs (boundary.c:2052-2616) for zeroGradient, fixedValue,
+// fixedGradient and periodic patches. FP64 in every precision mode.
+#include <cmath>
+
+#include "tg_internal.cuh"
+
+namespace tg {
+
+namespace {
+
+inline dim3 gfaces(const Grid &g) { return grid3(g.mx - 1, g.my - 1, g.mz - 1); }
+inline dim3 gint(const Grid &g) { return grid3(g.mx - 2, g.my - 2, g.mz - 2); }
+inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 * 16 ? b : 148 * 16); }
+
+// weno3, inline.h:5147-5180
+__device__ __forceinline__ double weno3(double f0, double f1, double f2, double f3, double wavespeed)
+{
+    double fL, fC, fR;
+    if (wavespeed > 0) { fL = f0; fC = f1; fR = f2; }
+    else { fL = f3; fC = f2; fR = f1; }
+    const double d0 = 2. / 3., d1 = 1. / 3., eps = 1.e-6;
+    const double beta0 = pow(fC - fR, 2.), beta1 = pow(fL - fC, 2.);
+    const double alpha0 = d0 / pow(eps + beta0, 2.), alpha1 = d1 / pow(eps + beta1, 2.);
+    const double sumalpha = alpha0 + alpha1;
+    const double w0 = alpha0 / sumalpha, w1 = alpha1 / sumalpha;
+    const double u0 = (fC * 0.5 + fR * 0.5), u1 = (-fL * 0.5 + fC * 1.5);
+    return w0 * u0 + w1 * u1;
+}
+
+// kappa_eff at a face (teqn_solvers.c:164-214); dtde: the face's eta derivative
+__device__ __forceinline__ double kappa_eff(const Params &p, double nut, double dtde, double ajc)
+{
+    if (!p.les) return p.nu / p.prandtl;
+    const double nu = 0.0;
+    const double gradTdotG = dtde * (-9.81);
+    const double delta = pow(1. / ajc, 1. / 3.);
+    double l;
+    if (gradTdotG < 0.) l = fmin(delta, 7.6 * nut / delta * sqrt(p.t_ref / fabs(gradTdotG)));
+    else l = delta;
+    const double Prt = 1.0 / (1.0 + (2.0 * l / delta));
+    return (nu / p.prandtl) + (nut / Prt);
+}
+
+// 4-cell stencil ends of a face (getFace2Cell4Stencil*, inline.h:2190-2380)
+__device__ __forceinline__ void stencil4(int i, int m, int per, int &L, int &R)
+{
+    if (i == 0 || i == m - 2) {
+        if (per && i == m - 2) { R = m + 2; L = i - 1; }
+        else if (per && i == 0) { L = -3; R = i + 2; }
+        else if (i == 0) { L = i; R = i + 2; }
+        else { L = i - 1; R = i + 1; }
+    } else { L = i - 1; R = i + 2; }
+}
+
+// pass 1: convective and diffusive fluxes at the faces of cell (k, j, i),
+// i in [0, mx-2] etc.; face 0 of a periodic direction is read from face m-2
+// by the budget and is not formed
+__global__ void k_t_face_fluxes(Grid g, Metrics m, State s, Params p, V3f<double> dv, V3f<double> vs)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
+    const int f = g.lin(k, j, i);
+    auto T = [&](int kk, int jj, int ii) { return s.tmprt[g.id(kk, jj, ii)]; };
+    auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
+    // i faces (Compute_dscalar_i, inline.h:3210-3247)
+    if (j != 0 && k != 0 && !(g.pi && i == 0)) {
+        const double dtdc = T(k, j, i + 1) - T(k, j, i);
+        const bool edge = (i == 0 || i == mx - 2);
+        double dtde, dtdz;
+        if (j == my - 2 && edge && (npj || npi))      dtde = (T(k, j, i + 1) + T(k, j, i) - T(k, j - 1, i + 1) - T(k, j - 1, i)) * 0.5;
+        else if (j == 1 && edge && (npj || npi))      dtde = (T(k, j + 1, i + 1) + T(k, j + 1, i) - T(k, j, i + 1) - T(k, j, i)) * 0.5;
+        else                                          dtde = (T(k, j + 1, i + 1) + T(k, j + 1, i) - T(k, j - 1, i + 1) - T(k, j - 1, i)) * 0.25;
+        if (k == mz - 2 && edge && (npk || npi))      dtdz = (T(k, j, i + 1) + T(k, j, i) - T(k - 1, j, i + 1) - T(k - 1, j, i)) * 0.5;
+        else if (k == 1 && edge && (npk || npi))      dtdz = (T(k + 1, j, i + 1) + T(k + 1, j, i) - T(k, j, i + 1) - T(k, j, i)) * 0.5;
+        else                                          dtdz = (T(k + 1, j, i + 1) + T(k + 1, j, i) - T(k - 1, j, i + 1) - T(k - 1, j, i)) * 0.25;
+        int iL, iR;
+        stencil4(i, mx, g.pi, iL, iR);
+        const double uc = s.ucont.x[f];
+        dv.x[f] = -uc * weno3(T(k, j, iL), T(k, j, i), T(k, j, i + 1), T(k, j, iR), uc);
+        const R3<double> cs = ld3(m.icsi, f), et = ld3(m.ieta, f), ze = ld3(m.izet, f);
+        const double g11 = cs.x * cs.x + cs.y * cs.y + cs.z * cs.z, g21 = et.x * cs.x + et.y * cs.y + et.z * cs.z,
+                     g31 = ze.x * cs.x + ze.y * cs.y + ze.z * cs.z;
+        const double ajc = m.iaj[f];
+        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1)) : 0.0, dtde, ajc);
+        vs.x[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+    }
+    // j faces (Compute_dscalar_j, inline.h:3252-3289)
+    if (i != 0 && k != 0 && !(g.pj && j == 0)) {
+        const bool edge = (j == 0 || j == my - 2);
+        double dtdc, dtdz;
+        if (i == mx - 2 && edge && (npi || npj))      dtdc = (T(k, j + 1, i) + T(k, j, i) - T(k, j + 1, i - 1) - T(k, j, i - 1)) * 0.5;
+        else if (i == 1 && edge && (npi || npj))      dtdc = (T(k, j + 1, i + 1) + T(k, j, i + 1) - T(k, j + 1, i) - T(k, j, i)) * 0.5;
+        else                                          dtdc = (T(k, j + 1, i + 1) + T(k, j, i + 1) - T(k, j + 1, i - 1) - T(k, j, i - 1)) * 0.25;
+        const double dtde = T(k, j + 1, i) - T(k, j, i);
+        if (k == mz - 2 && edge && (npk || npj))      dtdz = (T(k, j + 1, i) + T(k, j, i) - T(k - 1, j + 1, i) - T(k - 1, j, i)) * 0.5;
+        else if (k == 1 && edge && (npk || npj))      dtdz = (T(k + 1, j + 1, i) + T(k + 1, j, i) - T(k, j + 1, i) - T(k, j, i)) * 0.5;
+        else                                          dtdz = (T(k + 1, j + 1, i) + T(k + 1, j, i) - T(k - 1, j + 1, i) - T(k - 1, j, i)) * 0.25;
+        int jL, jR;
+        stencil4(j, my, g.pj, jL, jR);
+        const double uc = s.ucont.y[f];
+        dv.y[f] = -uc * weno3(T(k, jL, i), T(k, j, i), T(k, j + 1, i), T(k, jR, i), uc);
+        const R3<double> cs = ld3(m.jcsi, f), et = ld3(m.jeta, f), ze = ld3(m.jzet, f);
+        const double g11 = cs.x * et.x + cs.y * et.y + cs.z * et.z, g21 = et.x * et.x + et.y * et.y + et.z * et.z,
+                     g31 = ze.x * et.x + ze.y * et.y + ze.z * et.z;
+        const double ajc = m.jaj[f];
+        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)) : 0.0, dtde, ajc);
+        vs.y[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+    }
+    // k faces (Compute_dscalar_k, inline.h:3294-3331)
+    if (i != 0 && j != 0 && !(g.pk && k == 0)) {
+        const bool edge = (k == 0 || k == mz - 2);
+        double dtdc, dtde;
+        if (i == mx - 2 && edge && (npi || npk))      dtdc = (T(k + 1, j, i) + T(k, j, i) - T(k + 1, j, i - 1) - T(k, j, i - 1)) * 0.5;
+        else if (i == 1 && edge && (npi || npk))      dtdc = (T(k + 1, j, i + 1) + T(k, j, i + 1) - T(k + 1, j, i) - T(k, j, i)) * 0.5;
+        else                                          dtdc = (T(k + 1, j, i + 1) + T(k, j, i + 1) - T(k + 1, j, i - 1) - T(k, j, i - 1)) * 0.25;
+        if (j == my - 2 && edge && (npj || npk))      dtde = (T(k + 1, j, i) + T(k, j, i) - T(k + 1, j - 1, i) - T(k, j - 1, i)) * 0.5;
+        else if (j == 1 && edge && (npj || npk))      dtde = (T(k + 1, j + 1, i) + T(k, j + 1, i) - T(k + 1, j, i) - T(k, j, i)) * 0.5;
+        else                                          dtde = (T(k + 1, j + 1, i) + T(k, j + 1, i) - T(k + 1, j - 1, i) - T(k, j - 1, i)) * 0.25;
+        const double dtdz = T(k + 1, j, i) - T(k, j, i);
+        int kL, kR;
+        stencil4(k, mz, g.pk, kL, kR);
+        const double uc = s.ucont.z[f];
+        dv.z[f] = -uc * weno3(T(kL, j, i), T(k, j, i), T(k + 1, j, i), T(kR, j, i), uc);
+        const R3<double> cs = ld3(m.kcsi, f), et = ld3(m.keta, f), ze = ld3(m.kzet, f);
+        const double g11 = cs.x * ze.x + cs.y * ze.y + cs.z * ze.z, g21 = et.x * ze.x + et.y * ze.y + et.z * ze.z,
+                     g31 = ze.x * ze.x + ze.y * ze.y + ze.z * ze.z;
+        const double ajc = m.kaj[f];
+        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i)) : 0.0, dtde, ajc);
+        vs.z[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+    }
+}
+
+// pass 2 (teqn_solvers.c:540-566): rhs = (div budget + visc budget) aj at
+// interior cells, face 0 of a periodic direction read from face m-2
+// (resetFacePeriodicFluxesVector)
+__global__ void k_t_rhs(Grid g, Metrics m, V3f<double> dv, V3f<double> vs, double *rhs)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    const int c = g.lin(k, j, i), pl = g.mx * g.my;
+    const int iw = (i == 1 && g.pi) ? c + g.mx - 3 : c - 1;
+    const int js = (j == 1 && g.pj) ? c + (g.my - 3) * g.mx : c - g.mx;
+    const int kb = (k == 1 && g.pk) ? c + (g.mz - 3) * pl : c - pl;
+    const double divBudget = dv.x[c] - dv.x[iw] + dv.y[c] - dv.y[js] + dv.z[c] - dv.z[kb];
+    const double viscBudget = vs.x[c] - vs.x[iw] + vs.y[c] - vs.y[js] + vs.z[c] - vs.z[kb];
+    rhs[c] = 1.0 * (divBudget + viscBudget) * m.aj[c];
+}
+
+// TeqnRK4 bookkeeping after stage st: Ttmp (+)= dt b Rhs, next stage T = T_o + a dt Rhs, last T = Ttmp
+__global__ void k_t_rk(int64_t n, double *t, const double *to, double *ttmp, const double *rhs, double cb, double ca, int first, int last)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const double tt = (first ? to[q] : ttmp[q]) + cb * rhs[q];
+        if (last) t[q] = tt;
+        else { ttmp[q] = tt; t[q] = ca * rhs[q] + to[q]; }
+    }
+}
+
+// UpdateTemperatureBCs (boundary.c:2052-2616) on the face ghosts of one patch
+// pair (dir: 0 i, 1 j, 2 k), from the interior next to them
+__global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x + 1, b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
+    if (a > na - 2 || b > nb - 2) return;
+    const int mdir = dir == 0 ? g.mx : (dir == 1 ? g.my : g.mz);
+    auto at = [&](int l) { return dir == 0 ? g.lin(b, a, l) : (dir == 1 ? g.lin(b, l, a) : g.lin(l, b, a)); };
+    const V3f<double> &S = dir == 0 ? m.csi : (dir == 1 ? m.eta : m.zet);
+    for (int side = 0; side < 2; side++) {
+        const int patch = 2 * dir + side;
+        const int ci = side == 0 ? 1 : mdir - 2, gh = side == 0 ? 0 : mdir - 1;
+        const int c = at(ci), q = at(gh);
+        const int type = p.t_bc[patch];
+        if (type == TG_TBC_ZERO_GRADIENT) t[q] = t[c];
+        else if (type == TG_TBC_FIXED_VALUE) t[q] = p.t_bc_value[patch];
+        else if (type == TG_TBC_FIXED_GRADIENT) {
+            const double area = sqrt(S.x[c] * S.x[c] + S.y[c] * S.y[c] + S.z[c] * S.z[c]);
+            const double d = (1.0 / m.aj[c]) / area;
+            t[q] = d * p.t_bc_value[patch] + t[c];
+        } else {
+            t[q] = t[at(side == 0 ? mdir - 2 : 1)];   // periodic: the opposite interior cell
+        }
+    }
+}
+
+}  // namespace
+
+// SolveTEqn with TeqnRK4 (teqn.c:259-276, teqn_solvers.c:714-818)
+void solve_t(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int64_t G = g.size();
+    State &s = C->s;
+    const double dt = C->prm.dt;
+    const double b[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+    const double a[4] = {0.0, 0.5, 0.5, 1.0};
+    for (int st = 0; st < 4; st++) {
+        // FormExplicitRhsT: periodic ghosts, FormT (Rhs zero off the interior)
+        reset_cell_periodic_s(C, s.tmprt);
+        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs));
+        TG_PROF(C, "teqn_rk_update", k_t_rk<<<nblk(G), 256, 0, C->stream>>>(G, s.tmprt, s.tmprt_o, s.ttmp, s.trhs,
+                                                                          dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0, st == 3));
+    }
+    reset_cell_periodic_s(C, s.tmprt);
+}
+
+void update_temperature_bcs(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const dim3 b2(32, 8);
+    auto g2 = [](int na, int nb) { return dim3((na - 2 + 31) / 32, (nb - 2 + 7) / 8); };
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 0));
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 1));
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 2));
+}
+
+}  // namespace tg
