@@ -159,8 +159,9 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None):
         desc = "Taylor-Green vortex %d^3, RK4, dt=0.005" % (cfg.mx - 2)
     elif name == "hill":
         kw = dict(nx=48, ny=24, nz=24) if small else {}
-        cfg, nodes, ucat, p, T = cases.hill_case(ddt=api.DDT_RK4, **kw)
-        desc = "cosine hill %dx%dx%d cells, QUICK, buoyancy, RK4" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2)
+        cfg, nodes, ucat, p, T = cases.hill_case(ddt=api.DDT_RK4, teqn=True, **kw)
+        desc = ("cosine hill %dx%dx%d cells, QUICK, Smagorinsky, Schumann wall, Boussinesq buoyancy of the "
+                "transported temperature (RK4, WENO3), RK4" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2))
     elif name == "farm":
         kw = (dict(nx=96, ny=64, nz=32, Lx=960.0, Ly=640.0, H=250.0, rows=2, cols=2, D=63.0, hub=60.0)
               if small else {})
