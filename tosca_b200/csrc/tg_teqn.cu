@@ -21,19 +21,20 @@ inline dim3 gfaces(const Grid &g) { return grid3(g.mx - 1, g.my - 1, g.mz - 1); 
 inline dim3 gint(const Grid &g) { return grid3(g.mx - 2, g.my - 2, g.mz - 2); }
 inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 * 16 ? b : 148 * 16); }
 
-// weno3, inline.h:5147-5180
+// weno3, inline.h:5147-5180, with the weights in one division:
+// w0 = alpha0 / (alpha0 + alpha1) with alpha_q = d_q / (eps + beta_q)^2 is
+// d0 s1^2 / (d0 s1^2 + d1 s0^2), s_q = eps + beta_q (same value up to
+// rounding; a double division or library pow call costs tens of instructions)
 __device__ __forceinline__ double weno3(double f0, double f1, double f2, double f3, double wavespeed)
 {
     double fL, fC, fR;
     if (wavespeed > 0) { fL = f0; fC = f1; fR = f2; }
     else { fL = f3; fC = f2; fR = f1; }
     const double d0 = 2. / 3., d1 = 1. / 3., eps = 1.e-6;
-    const double beta0 = pow(fC - fR, 2.), beta1 = pow(fL - fC, 2.);
-    const double alpha0 = d0 / pow(eps + beta0, 2.), alpha1 = d1 / pow(eps + beta1, 2.);
-    const double sumalpha = alpha0 + alpha1;
-    const double w0 = alpha0 / sumalpha, w1 = alpha1 / sumalpha;
+    const double s0 = eps + (fC - fR) * (fC - fR), s1 = eps + (fL - fC) * (fL - fC);
+    const double A = d0 * (s1 * s1), B = d1 * (s0 * s0);
     const double u0 = (fC * 0.5 + fR * 0.5), u1 = (-fL * 0.5 + fC * 1.5);
-    return w0 * u0 + w1 * u1;
+    return (A * u0 + B * u1) / (A + B);
 }
 
 // kappa_eff at a face (teqn_solvers.c:164-214); dtde: the face's eta derivative
@@ -42,7 +43,7 @@ __device__ __forceinline__ double kappa_eff(const Params &p, double nut, double 
     if (!p.les) return p.nu / p.prandtl;
     const double nu = 0.0;
     const double gradTdotG = dtde * (-9.81);
-    const double delta = pow(1. / ajc, 1. / 3.);
+    const double delta = cbrt(1. / ajc);
     double l;
     if (gradTdotG < 0.) l = fmin(delta, 7.6 * nut / delta * sqrt(p.t_ref / fabs(gradTdotG)));
     else l = delta;
