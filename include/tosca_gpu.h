@@ -162,6 +162,14 @@ tg_status tg_set_mesh_nodes(tg_ctx *ctx, const double *nodes);
  * (DMDAVecGetArray pointers) and to read results back. */
 tg_status tg_set_field(tg_ctx *ctx, int32_t which, const double *host, int32_t halo);
 tg_status tg_get_field(tg_ctx *ctx, int32_t which, double *host, int32_t halo);
+/* A field in TOSCA's field-file format (readFields / writeFields, io.c:247-420,
+ * 2261): PETSc binary VecView of the DMDA vector, big-endian, header of two
+ * 64-bit integers (class id 1211214, entry count) then the entries in natural
+ * order over the whole DMDA extent (components interleaved for vectors). The
+ * reader also accepts the 32-bit-integer header of a PETSc build without
+ * 64-bit indices; a wrong class id or entry count returns TG_ERR_BAD_ARG. */
+tg_status tg_write_field_petsc(tg_ctx *ctx, int32_t which, const char *path);
+tg_status tg_read_field_petsc(tg_ctx *ctx, int32_t which, const char *path);
 
 /* Cartesian cell velocity -> ghost cells -> face fluxes. Replaces the common
  * tail of SetTaylorGreenFieldU / SetABLInitialFlowU (initialField.c:1100-1204):

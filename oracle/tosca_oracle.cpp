@@ -1736,6 +1736,54 @@ tg_status tor_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
     });
 }
 
+// PETSc binary VecView / VecLoad of a DMDA vector (readFields / writeFields,
+// io.c:247-420, 2261): big-endian class id 1211214 and entry count (64-bit,
+// or 32-bit when reading), then big-endian doubles in natural order
+tg_status tor_write_field_petsc(tg_ctx *C, int32_t w, const char *path)
+{
+    return guarded(C, [&]() -> tg_status {
+        size_t dof = vecField(*C, w) ? 3 : (scalField(*C, w) ? 1 : 0);
+        if (!path || !dof || w == TG_F_TAUWALL) return fail(C, TG_ERR_BAD_ARG, "bad field or path");
+        std::vector<double> h(C->G * dof);
+        tg_status s = tor_get_field(C, w, h.data(), 0);
+        if (s != TG_OK) return s;
+        std::vector<unsigned char> out(16 + 8 * h.size());
+        auto put = [&](size_t at, uint64_t v) { for (int b = 0; b < 8; b++) out[at + b] = (unsigned char)(v >> (56 - 8 * b)); };
+        put(0, 1211214);
+        put(8, (uint64_t)h.size());
+        for (size_t q = 0; q < h.size(); q++) { uint64_t u; std::memcpy(&u, &h[q], 8); put(16 + 8 * q, u); }
+        FILE *f = std::fopen(path, "wb");
+        if (!f) return fail(C, TG_ERR_BAD_ARG, "cannot open file");
+        bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+        ok = std::fclose(f) == 0 && ok;
+        return ok ? TG_OK : fail(C, TG_ERR_BAD_ARG, "write failed");
+    });
+}
+tg_status tor_read_field_petsc(tg_ctx *C, int32_t w, const char *path)
+{
+    return guarded(C, [&]() -> tg_status {
+        size_t dof = vecField(*C, w) ? 3 : (scalField(*C, w) ? 1 : 0);
+        if (!path || !dof || w == TG_F_TAUWALL) return fail(C, TG_ERR_BAD_ARG, "bad field or path");
+        FILE *f = std::fopen(path, "rb");
+        if (!f) return fail(C, TG_ERR_BAD_ARG, "cannot open file");
+        std::vector<unsigned char> buf;
+        unsigned char tmp[65536];
+        size_t got;
+        while ((got = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
+        std::fclose(f);
+        auto get = [&](size_t at, int nb) { uint64_t v = 0; for (int b = 0; b < nb; b++) v = (v << 8) | buf[at + b]; return v; };
+        const size_t n = C->G * dof;
+        size_t off;
+        if (buf.size() >= 8 && get(0, 4) == 1211214) off = 8;                   // 32-bit integers
+        else if (buf.size() >= 16 && get(0, 8) == 1211214) off = 16;            // 64-bit integers
+        else return fail(C, TG_ERR_BAD_ARG, "not a PETSc vector file");
+        if ((off == 8 ? get(4, 4) : get(8, 8)) != n || buf.size() != off + 8 * n) return fail(C, TG_ERR_BAD_ARG, "entry count mismatch");
+        std::vector<double> h(n);
+        for (size_t q = 0; q < n; q++) { uint64_t u = get(off + 8 * q, 8); std::memcpy(&h[q], &u, 8); }
+        return tor_set_field(C, w, h.data(), 0);
+    });
+}
+
 tg_status tor_init_from_cartesian(tg_ctx *C, const double *ucat, int32_t halo)
 {
     return guarded(C, [&]() -> tg_status {

@@ -196,6 +196,8 @@ _SIGS = {
     "sync_pressure": (C.c_int, [C.c_void_p]),
     "step": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
     "step_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(TgStats)]),
+    "write_field_petsc": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p]),
+    "read_field_petsc": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p]),
     "set_turbines": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(TgTurbine), C.c_double]),
     "set_turbine_ct": (C.c_int, [C.c_void_p, C.c_void_p]),
     "turbine_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int32]),
@@ -305,6 +307,34 @@ class Solver:
     def set(self, name: str, arr: np.ndarray, halo: int = 0):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
         self._check(self.fns["set_field"](self.h, F[name], _ptr(arr), halo), f"set_field {name}")
+
+    # ----------------------------------------------------- TOSCA field files
+    # file names of readFields / writeFields (io.c:247-420, 2261)
+    FILE_FIELDS = {"V": "UCONT", "U": "UCAT", "p": "P", "nut": "NUT", "T": "TMPRT"}
+
+    def write_field_petsc(self, name: str, path: str):
+        self._check(self.fns["write_field_petsc"](self.h, F[name], path.encode()), f"write_field_petsc {name}")
+
+    def read_field_petsc(self, name: str, path: str):
+        self._check(self.fns["read_field_petsc"](self.h, F[name], path.encode()), f"read_field_petsc {name}")
+
+    def write_fields(self, directory: str):
+        """V, U, p (and nut with LES, T with the temperature equation) as TOSCA writes
+        them into a time directory."""
+        import os
+        os.makedirs(directory, exist_ok=True)
+        for fname, field in self.FILE_FIELDS.items():
+            if (fname == "nut" and not self.cfg.les) or (fname == "T" and not getattr(self.cfg, "teqn", 0)):
+                continue
+            self.write_field_petsc(field, os.path.join(directory, fname))
+
+    def read_fields(self, directory: str):
+        """The fields of a TOSCA time directory that this configuration uses."""
+        import os
+        for fname, field in self.FILE_FIELDS.items():
+            path = os.path.join(directory, fname)
+            if os.path.exists(path):
+                self.read_field_petsc(field, path)
 
     def init_from_cartesian(self, ucat: np.ndarray, halo: int = 0):
         ucat = np.ascontiguousarray(ucat, dtype=np.float64)

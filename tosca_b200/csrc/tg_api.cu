@@ -375,6 +375,87 @@ tg_status tg_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
     });
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr int64_t kPetscVecClassId = 1211214;     // VEC_FILE_CLASSID
+
+// entries per point of a field in the file (0: not a grid field)
+int field_dof(tg_ctx *C, int w)
+{
+    if (w == TG_F_TAUWALL || w < 0 || w >= TG_F_COUNT) return 0;
+    if (w == TG_F_P_ADJ || scal_field(C, w)) return 1;
+    return 3;
+}
+
+template <class T>
+T byteswap(T v)
+{
+    unsigned char b[sizeof(T)];
+    std::memcpy(b, &v, sizeof(T));
+    for (size_t q = 0; q < sizeof(T) / 2; q++) std::swap(b[q], b[sizeof(T) - 1 - q]);
+    std::memcpy(&v, b, sizeof(T));
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+tg_status tg_write_field_petsc(tg_ctx *C, int32_t w, const char *path)
+{
+    return guarded(C, [&]() -> tg_status {
+        const int dof = field_dof(C, w);
+        if (!path || !dof) return fail(C, TG_ERR_BAD_ARG, "bad field or path");
+        const size_t n = (size_t)C->g.size() * dof;
+        std::vector<double> h(n);
+        tg_status s = tg_get_field(C, w, h.data(), 0);
+        if (s != TG_OK) return s;
+        for (double &v : h) v = byteswap(v);
+        FILE *f = std::fopen(path, "wb");
+        if (!f) return fail(C, TG_ERR_BAD_ARG, std::string("cannot open ") + path);
+        const int64_t hdr[2] = {byteswap(kPetscVecClassId), byteswap((int64_t)n)};
+        bool ok = std::fwrite(hdr, sizeof(hdr), 1, f) == 1 && std::fwrite(h.data(), sizeof(double), n, f) == n;
+        ok = (std::fclose(f) == 0) && ok;
+        return ok ? TG_OK : fail(C, TG_ERR_BAD_ARG, std::string("write failed: ") + path);
+    });
+}
+
+tg_status tg_read_field_petsc(tg_ctx *C, int32_t w, const char *path)
+{
+    return guarded(C, [&]() -> tg_status {
+        const int dof = field_dof(C, w);
+        if (!path || !dof) return fail(C, TG_ERR_BAD_ARG, "bad field or path");
+        const size_t n = (size_t)C->g.size() * dof;
+        FILE *f = std::fopen(path, "rb");
+        if (!f) return fail(C, TG_ERR_BAD_ARG, std::string("cannot open ") + path);
+        std::vector<double> h(n);
+        unsigned char hb[16];
+        bool ok = std::fread(hb, 1, 8, f) == 8;
+        int64_t cls = 0, cnt = -1;
+        if (ok) {
+            int32_t c32, n32;
+            std::memcpy(&c32, hb, 4);
+            if (byteswap(c32) == (int32_t)kPetscVecClassId) {          // 32-bit header
+                std::memcpy(&n32, hb + 4, 4);
+                cls = kPetscVecClassId; cnt = byteswap(n32);
+            } else {                                                  // 64-bit header
+                std::memcpy(&cls, hb, 8);
+                cls = byteswap(cls);
+                int64_t n64;
+                ok = std::fread(&n64, 8, 1, f) == 1;
+                cnt = byteswap(n64);
+            }
+        }
+        ok = ok && cls == kPetscVecClassId && cnt == (int64_t)n && std::fread(h.data(), sizeof(double), n, f) == n;
+        std::fclose(f);
+        if (!ok) return fail(C, TG_ERR_BAD_ARG, std::string("not a PETSc vector of ") + std::to_string(n) + " entries: " + path);
+        for (double &v : h) v = byteswap(v);
+        return tg_set_field(C, w, h.data(), 0);
+    });
+}
+
 tg_status tg_init_from_cartesian(tg_ctx *C, const double *ucat, int32_t halo)
 {
     return guarded(C, [&]() -> tg_status {
