@@ -299,7 +299,7 @@ def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     fwd_ms = solver.step(fwd_steps).seconds / fwd_steps * 1e3
     free, _ = torch.cuda.mem_get_info()
     G = cfg.mx * cfg.my * cfg.mz
-    snap = 8 * (13 * G + cfg.cells)
+    snap = 8 * (7 * G + cfg.cells)                   # Ucont, Ucat, P and the Poisson warm start
     work = 8 * (49 + 31) * G                       # adjoint work arrays and the work tape
     nsnap = int(max(2, min(steps, 0.5 * (free - work) // snap)))
     solver.set_farm_objective(True)
@@ -511,6 +511,7 @@ def main():
         adj = adjoint_ratio(dev)
     farm_adj = None
     if rank == 0 and not args.no_adjoint and args.workload == "farm" and args.farm_adjoint_steps > 0:
+        solver.close()                               # its HBM goes to the checkpoints
         farm_adj = farm_adjoint(dev, head_prec, args.farm_adjoint_steps)
 
     cpu = None

@@ -1071,7 +1071,8 @@ static void adj_replay_check(tg_ctx *C)
 static Snapshot make_snapshot(tg_ctx *C)
 {
     Snapshot s{};
-    s.ucont = alloc3(C); s.ucat = alloc3(C); s.btheta = alloc3(C); s.btheta_o = alloc3(C);
+    s.ucont = alloc3(C); s.ucat = alloc3(C);
+    if (C->prm.buoyancy) { s.btheta = alloc3(C); s.btheta_o = alloc3(C); }   // the AB2 history
     s.p = dallocd(C, (size_t)C->g.size());
     s.px = dallocd(C, (size_t)poisson_n(C));
     s.pos = -1;
@@ -1080,7 +1081,7 @@ static Snapshot make_snapshot(tg_ctx *C)
 static void save_state(tg_ctx *C, Snapshot &s, int pos)
 {
     copy3(C, s.ucont, C->s.ucont); copy3(C, s.ucat, C->s.ucat);
-    copy3(C, s.btheta, C->s.btheta); copy3(C, s.btheta_o, C->s.btheta_o);
+    if (s.btheta.x) { copy3(C, s.btheta, C->s.btheta); copy3(C, s.btheta_o, C->s.btheta_o); }
     TG_CUDA(cudaMemcpyAsync(s.p, C->s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(s.px, poisson_x(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     s.it = C->it;
@@ -1089,7 +1090,7 @@ static void save_state(tg_ctx *C, Snapshot &s, int pos)
 static void restore_state(tg_ctx *C, const Snapshot &s)
 {
     copy3(C, C->s.ucont, s.ucont); copy3(C, C->s.ucat, s.ucat);
-    copy3(C, C->s.btheta, s.btheta); copy3(C, C->s.btheta_o, s.btheta_o);
+    if (s.btheta.x) { copy3(C, C->s.btheta, s.btheta); copy3(C, C->s.btheta_o, s.btheta_o); }
     TG_CUDA(cudaMemcpyAsync(C->s.p, s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_x(C), s.px, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     C->it = s.it;
