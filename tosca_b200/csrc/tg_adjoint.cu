@@ -45,7 +45,7 @@ namespace tg {
 
 struct Snapshot {
     V3f<double> ucont, ucat, btheta, btheta_o;
-    double *p, *px;
+    double *p, *px, *pxp;        // P, the last two Poisson solutions (initial guess of the next solve)
     int it;
     int pos;       // step index of the state held (-1: free)
 };
@@ -1075,6 +1075,7 @@ static Snapshot make_snapshot(tg_ctx *C)
     if (C->prm.buoyancy) { s.btheta = alloc3(C); s.btheta_o = alloc3(C); }   // the AB2 history
     s.p = dallocd(C, (size_t)C->g.size());
     s.px = dallocd(C, (size_t)poisson_n(C));
+    s.pxp = dallocd(C, (size_t)poisson_n(C));
     s.pos = -1;
     return s;
 }
@@ -1084,6 +1085,7 @@ static void save_state(tg_ctx *C, Snapshot &s, int pos)
     if (s.btheta.x) { copy3(C, s.btheta, C->s.btheta); copy3(C, s.btheta_o, C->s.btheta_o); }
     TG_CUDA(cudaMemcpyAsync(s.p, C->s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(s.px, poisson_x(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(s.pxp, poisson_xprev(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     s.it = C->it;
     s.pos = pos;
 }
@@ -1093,6 +1095,7 @@ static void restore_state(tg_ctx *C, const Snapshot &s)
     if (s.btheta.x) { copy3(C, C->s.btheta, s.btheta); copy3(C, C->s.btheta_o, s.btheta_o); }
     TG_CUDA(cudaMemcpyAsync(C->s.p, s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_x(C), s.px, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(poisson_xprev(C), s.pxp, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     C->it = s.it;
     set_device_step(C);
 }

@@ -293,6 +293,7 @@ bool adj_field(tg_ctx *C, int w, V3f<double> &v, double *&s);   // adjoint field
 void adj_destroy(tg_ctx *C);
 int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st);
 double *poisson_x(tg_ctx *C);
+double *poisson_xprev(tg_ctx *C);
 int64_t poisson_n(tg_ctx *C);
 
 }  // namespace tg

@@ -36,6 +36,7 @@ struct PoissonCtx {
     bool ortho;
     double *gE1, *gE2, *gE3, *gN1, *gN2, *gN3, *gT1, *gT2, *gT3;  // fine face tensors (compact)
     double *x, *b, *r, *z, *p, *q, *rhat, *v, *s, *t, *aj;
+    double *xprev;               // previous step's solution (extrapolated initial guess)
     double *part;                // reduction partials (4 per block)
     int nblocks;
     MG *mg;                      // multigrid preconditioner (host object)
@@ -234,6 +235,16 @@ __global__ void k_copy(int64_t n, const double *a, double *b)
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
 }
 __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
+// initial guess of the step's solve, 2 x_n - x_{n-1} (linear extrapolation of
+// the last two solutions; the reference starts from x_n), and xprev <- x_n
+__global__ void k_extrapolate(int64_t n, double *x, double *xprev)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const double xn = x[t];
+        x[t] = 2.0 * xn - xprev[t];
+        xprev[t] = xn;
+    }
+}
 __global__ void k_negcopy(int64_t n, const double *a, double *b)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = -a[t];
@@ -394,7 +405,7 @@ void poisson_setup(tg_ctx *C)
     P->ortho = C->orthogonal;
     const int64_t n = P->n;
     double **fine[] = {&P->gE1, &P->gE2, &P->gE3, &P->gN1, &P->gN2, &P->gN3, &P->gT1, &P->gT2, &P->gT3,
-                       &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj};
+                       &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj, &P->xprev};
     for (double **f : fine) *f = dallocd(C, n);
     P->nblocks = vblocks(n);
     P->part = dallocd(C, 3 * (size_t)P->nblocks);
@@ -536,6 +547,7 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt));
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solution
     int rc = krylov_solve(C, st, rtol, C->cfg.poisson_div_tol, maxit);
     TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
@@ -693,6 +705,7 @@ void poisson_solve_capture(tg_ctx *C)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt);
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
     krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit, SC_G);
     k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P);
@@ -739,8 +752,9 @@ int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol
     return rc;
 }
 
-// compact Poisson solution vector (warm start of the next solve): snapshots
+// compact Poisson solution vectors (the next solve starts from 2 x - xprev): snapshots
 double *poisson_x(tg_ctx *C) { return C->pois->x; }
+double *poisson_xprev(tg_ctx *C) { return C->pois->xprev; }
 int64_t poisson_n(tg_ctx *C) { return C->pois->n; }
 
 }  // namespace tg
