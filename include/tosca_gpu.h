@@ -57,7 +57,7 @@ enum {
 /* -divScheme (ueqn.c:82-110) */
 enum { TG_DIV_CENTRAL = 0, TG_DIV_QUICK = 1 };
 /* -dUdtScheme (ueqn.c:123-323) */
-enum { TG_DDT_FE = 0, TG_DDT_RK4 = 1 };
+enum { TG_DDT_FE = 0, TG_DDT_RK4 = 1, TG_DDT_CN = 2 };
 /* arithmetic of the step */
 enum {
     TG_PREC_FP64  = 0,   /* every stage in FP64                                   */
@@ -105,6 +105,11 @@ typedef struct tg_config {
     int32_t t_bc[6];               /* TG_TBC_* per patch (periodic where bc is periodic)    */
     double  prandtl;               /* -Pr: molecular Prandtl number (no LES)                */
     double  t_bc_value[6];         /* fixedValue: ghost value; fixedGradient: gradient      */
+    /* Crank-Nicolson momentum solve (TG_DDT_CN; -absTolU, -relTolU, -snesMaxItersU,
+     * ueqn.c:128-138): stop at |F| <= max(snes_atol, snes_rtol |F_0|) */
+    double  snes_atol;
+    double  snes_rtol;
+    int32_t snes_maxit;
 } tg_config;
 
 /* per-call statistics */

@@ -101,6 +101,7 @@ struct tg_ctx {
     std::vector<double> p_adj;
     std::vector<double> p, phi, nut, tmprt;
     std::vector<double> tmprt_o;                // teqn->Tmprt_o (tosca_oracle_teqn.inc)
+    std::vector<V3> rhs_o;                      // ueqn->Rhs_o (tosca_oracle_cn.inc)
 
     // jLeft wall model arrays, indexed k*mx + i (tauWall, uMeanMag, uFilt)
     std::vector<double> twx, twy, twz, umean, ufx, ufy, ufz;
@@ -1354,6 +1355,7 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
 
 #include "tosca_oracle_farm.inc"
 #include "tosca_oracle_teqn.inc"
+#include "tosca_oracle_cn.inc"
 
 // ExplicitRhsU, ueqn_solvers.c:1276-1407
 void explicitRhsU(tg_ctx &C)
@@ -1383,11 +1385,14 @@ void explicitRhsU(tg_ctx &C)
 }
 
 // SolveUEqn with UeqnFE / UeqnRK4, ueqn.c:397-440, ueqn_solvers.c:1411-1504
-void solveUEqn(tg_ctx &C)
+int solveUEqn(tg_ctx &C)
 {
     const size_t G = C.G;
     const double dt = C.c.dt;
-    if (C.c.ddt_scheme == TG_DDT_FE) {
+    int rc = 0;
+    if (C.c.ddt_scheme == TG_DDT_CN) {
+        rc = ueqnSNES(C);
+    } else if (C.c.ddt_scheme == TG_DDT_FE) {
         explicitRhsU(C);
         // VecScale(Rhs,dt) then VecAXPY(Rhs,1,Ucont_o): dt*rhs + ucont_o
         for (size_t q = 0; q < G; q++) C.ucont[q] = mk(C.rhs[q].x * dt + C.ucont_o[q].x, C.rhs[q].y * dt + C.ucont_o[q].y, C.rhs[q].z * dt + C.ucont_o[q].z);
@@ -1409,6 +1414,7 @@ void solveUEqn(tg_ctx &C)
     resetCellPeriodic(C, C.ucat);
     // adjustFluxesLocal (ueqn.c:748-1135) only acts on non-periodic, non-wall
     // patches; every patch type accepted here is periodic or a wall.
+    return rc;
 }
 
 // SetRHS, peqn.c:1942-2063
@@ -1555,12 +1561,18 @@ int step(tg_ctx &C, tg_stats *st)
         if (C.it > C.c.it_start) C.btheta_o = C.btheta;
         buoyancy(C);
     }
-    solveUEqn(C);                                        // main.c:195
+    const int urc = solveUEqn(C);                        // main.c:195
     int rc = solvePEqn(C, st);                           // main.c:198
+    if (urc == 2) rc = 2;
+    else if (rc != 2) rc |= urc;
     contravariantToCartesian(C);                         // main.c:201
     if (C.c.teqn) solveTEqn(C);                          // main.c:194-205
     double md = continuityError(C);                      // main.c:227
     if (st) st->max_divergence = md;
+    if (C.c.ddt_scheme == TG_DDT_CN) {                   // main.c:214-272: Rhs_o of the next step
+        std::fill(C.rhs_o.begin(), C.rhs_o.end(), V3{0, 0, 0});
+        formU(C, C.rhs_o, 1.0);
+    }
     if (C.c.teqn) updateTemperatureBCs(C);               // main.c:274-278
     updateCartesianBCs(C);                               // main.c:281
     updateContravariantBCs(C);                           // main.c:284
@@ -1575,6 +1587,7 @@ void allocState(tg_ctx &C)
     for (auto *v : {&C.ucont, &C.ucont_o, &C.ucat, &C.rhs, &C.dp, &C.btheta, &C.btheta_o, &C.gcont, &C.utmp, &C.fp, &C.source, &C.ucont_adj, &C.ucat_adj, &C.source_adj,
                     &C.div1, &C.div2, &C.div3, &C.visc1, &C.visc2, &C.visc3}) zero(*v, G);
     for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt, &C.p_adj, &C.tmprt_o}) zero(*v, G);
+    zero(C.rhs_o, G);
     const size_t P = (size_t)C.mx * C.mz;
     for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz}) zero(*v, P);
 }
@@ -1669,7 +1682,7 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->bc[TG_IRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_ILEFT] == TG_BC_WALL_SHUMANN ||
         cfg->bc[TG_KRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_KLEFT] == TG_BC_WALL_SHUMANN ||
         cfg->bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN) return TG_ERR_BAD_ARG;
-    if (cfg->dt <= 0) return TG_ERR_BAD_ARG;
+    if (cfg->dt <= 0 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 2) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
@@ -1980,6 +1993,7 @@ tg_status tor_adjoint_step(tg_ctx *C)
     return guarded(C, [&]() -> tg_status {
         if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
         if (C->c.teqn) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the temperature equation is not implemented");
+        if (C->c.ddt_scheme == TG_DDT_CN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the Crank-Nicolson scheme is not implemented");
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
         auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;

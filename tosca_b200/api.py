@@ -21,7 +21,7 @@ TG_OK, TG_ERR_CUDA, TG_ERR_BAD_ARG, TG_ERR_NOT_CONVERGED, TG_ERR_NAN, TG_ERR_ALL
 BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
-DDT_FE, DDT_RK4 = 0, 1
+DDT_FE, DDT_RK4, DDT_CN = 0, 1, 2
 TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
@@ -67,6 +67,9 @@ class TgConfig(C.Structure):
         ("t_bc", C.c_int32 * 6),
         ("prandtl", C.c_double),
         ("t_bc_value", C.c_double * 6),
+        ("snes_atol", C.c_double),
+        ("snes_rtol", C.c_double),
+        ("snes_maxit", C.c_int32),
     ]
 
 
@@ -154,6 +157,9 @@ class Config:
     t_bc: tuple = (TBC_PERIODIC,) * 6
     prandtl: float = 0.7
     t_bc_value: tuple = (0.0,) * 6
+    snes_atol: float = 1e-5
+    snes_rtol: float = 1e-30
+    snes_maxit: int = 20
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

@@ -207,7 +207,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
-    if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 1) return TG_ERR_BAD_ARG;
+    if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 2) return TG_ERR_BAD_ARG;
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
@@ -251,6 +251,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         alloc_precision_work(C);
         double **ss[] = {&st.p, &st.phi, &st.nut, &st.tmprt, &st.ssnap};
         for (auto **v : ss) *v = dallocd(C, G);
+        if (cfg->ddt_scheme == TG_DDT_CN) st.rhs_o = dalloc3(C, G);
         if (cfg->teqn) {
             st.tdiv = dalloc3(C, G); st.tvisc = dalloc3(C, G);
             st.trhs = dallocd(C, G); st.tmprt_o = dallocd(C, G); st.ttmp = dallocd(C, G);
@@ -285,6 +286,7 @@ tg_status tg_destroy(tg_ctx *C)
     graph_destroy(C);
     for (cudaStream_t a : C->aux) if (a) cudaStreamDestroy(a);
     try { farm_destroy(C); } catch (...) {}
+    cn_destroy(C);
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);

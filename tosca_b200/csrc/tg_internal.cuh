@@ -87,6 +87,7 @@ struct State {
     // temperature transport (tg_teqn.cu): lDivT, lViscT face fluxes, Rhs, Tmprt_o, TmprtTmp
     V3f<double> tdiv, tvisc;
     double *trhs, *tmprt_o, *ttmp;
+    V3f<double> rhs_o;           // ueqn->Rhs_o: FormU of the last step's final state (CN)
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
@@ -105,6 +106,7 @@ struct Params {
 struct PoissonCtx;   // tg_poisson.cu
 struct AdjState;     // tg_adjoint.cu
 struct Farm;         // tg_farm.cu
+struct CnWork;       // tg_cn.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -165,6 +167,8 @@ struct tg_ctx {
     tg::PoissonCtx *pois = nullptr;
     tg::AdjState *adj = nullptr;         // adjoint fields, tape and checkpoints (tg_adjoint.cu)
     tg::Farm *farm = nullptr;            // actuator-disk turbines (tg_farm.cu)
+    tg::CnWork *cn = nullptr;            // Crank-Nicolson Newton-Krylov work (tg_cn.cu)
+    int cn_newton = 0, cn_linear = 0;    // iterations of the last implicit momentum solve
     bool taping = false;                 // the running step records its stage states
     // CUDA graph of a whole step (tg_step.cu): built on the first step that can
     // be captured, replayed afterwards
@@ -268,6 +272,12 @@ void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, do
 bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body);
 void adj_graph_destroy(tg_ctx *C);
 // temperature transport (tg_teqn.cu)
+// Crank-Nicolson momentum step (tg_cn.cu)
+int solve_u_cn(tg_ctx *C, tg_stats *st);
+void cn_destroy(tg_ctx *C);
+void cn_build_bu(tg_ctx *C, V3f<double> bu, bool half_rhs_o);   // tg_step.cu
+void mask_non_resolved(tg_ctx *C, V3f<double> v);               // resetNonResolvedCellFaces on v
+void contra_to_cart_stage(tg_ctx *C);
 void solve_t(tg_ctx *C);
 void update_temperature_bcs(tg_ctx *C);
 // wind farm (tg_farm.cu)

@@ -927,7 +927,7 @@ void contra_to_cart(tg_ctx *C)
 
 // contravariantToCartesian inside the momentum stages, at the precision the
 // context's policy gives it
-static void contra_to_cart_stage(tg_ctx *C)
+void contra_to_cart_stage(tg_ctx *C)
 {
     const dim3 gr = gi(C->g);
     if (C->pol.contra_a32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<float, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
@@ -1143,6 +1143,57 @@ void explicit_rhs(tg_ctx *C)
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
 }
 
+// resetNonResolvedCellFaces (inline.h:1674-1835) on an arbitrary face vector
+void mask_non_resolved(tg_ctx *C, V3f<double> v)
+{
+    const Grid g = C->g;
+    State s = C->s;
+    s.rhs = v;
+    k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, s, 0);
+    k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, s, 1);
+    k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, s, 2);
+}
+
+// constant part of the Crank-Nicolson residual (UeqnSNES, ueqn_solvers.c:1097-1163):
+// bU = -dP (+ AB2 buoyancy) (+ 1/2 Rhs_o) (+ turbine force) + sourceU, and the
+// mean pressure gradient (see tg_cn.cu)
+__global__ void k_cn_bu(Grid g, Metrics m, State s, Params p, V3f<double> bu, int ab2, int half_rhs_o)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.mx || j >= g.my || k >= g.mz) return;
+    const int c = g.lin(k, j, i);
+    R3<double> b = -1.0 * ld3(s.dp, c);
+    if (p.buoyancy) {
+        if (ab2) { b = b + (3.0 / 2.0) * ld3(s.btheta, c); b = b + (-1.0 / 2.0) * ld3(s.btheta_o, c); }
+        else b = b + 1.0 * ld3(s.btheta, c);
+    }
+    if (half_rhs_o) b = b + 0.5 * ld3(s.rhs_o, c);
+    if (p.farm) b = b + 1.0 * ld3(s.farmcont, c);
+    if (i >= 1 && j >= 1 && k >= 1 && i <= g.mx - 2 && j <= g.my - 2 && k <= g.mz - 2) {
+        if (p.source) {
+            const V3f<double> &f = s.source;
+            const int ie = c + 1, jn = c + g.mx, kt = c + g.mx * g.my;
+            const R3<double> a = ld3(m.icsi, c), e = ld3(m.jeta, c), d = ld3(m.kzet, c);
+            b.x += 1.0 * (0.5 * (f.x[c] + f.x[ie]) * a.x + 0.5 * (f.y[c] + f.y[ie]) * a.y + 0.5 * (f.z[c] + f.z[ie]) * a.z);
+            b.y += 1.0 * (0.5 * (f.x[c] + f.x[jn]) * e.x + 0.5 * (f.y[c] + f.y[jn]) * e.y + 0.5 * (f.z[c] + f.z[jn]) * e.z);
+            b.z += 1.0 * (0.5 * (f.x[c] + f.x[kt]) * d.x + 0.5 * (f.y[c] + f.y[kt]) * d.y + 0.5 * (f.z[c] + f.z[kt]) * d.z);
+        }
+        if (p.mean_grad_p) {
+            const R3<double> a = ld3(m.icsi, c), e = ld3(m.jeta, c), d = ld3(m.kzet, c);
+            b.x += p.mgp[0] * a.x + p.mgp[1] * a.y + p.mgp[2] * a.z;
+            b.y += p.mgp[0] * e.x + p.mgp[1] * e.y + p.mgp[2] * e.z;
+            b.z += p.mgp[0] * d.x + p.mgp[1] * d.y + p.mgp[2] * d.z;
+        }
+    }
+    st3(bu, c, b);
+}
+
+void cn_build_bu(tg_ctx *C, V3f<double> bu, bool half_rhs_o)
+{
+    const Grid g = C->g;
+    k_cn_bu<<<ga(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm, bu, C->it > C->cfg.it_start ? 1 : 0, half_rhs_o ? 1 : 0);
+}
+
 // UeqnRK4 bookkeeping after stage st (ueqn_solvers.c:1446-1504): the stage
 // sum Utmp += dt b_st Rhs (Utmp starts as Ucont_o) and the next stage's state
 // Ucont = Ucont_o + a_{st+1} dt Rhs, or after the last stage Ucont = Utmp.
@@ -1166,11 +1217,15 @@ __global__ void k_rk_update(int64_t n, V3f<double> utmp, V3f<double> ucont, V3f<
 // on every interior cell as the reference does; the full step converts only
 // the boundary shell, which gives the same Ucat at the end of the step because
 // the projection is followed by its own conversion.
-static void solve_u_impl(tg_ctx *C, bool cart_tail)
+static int solve_u_impl(tg_ctx *C, bool cart_tail, tg_stats *st = nullptr)
 {
     const int64_t G = C->g.size();
     const double dt = C->prm.dt;
-    if (C->cfg.ddt_scheme == TG_DDT_FE) {
+    int rc = 0;
+    if (C->cfg.ddt_scheme == TG_DDT_CN) {
+        // UeqnSNES, ueqn_solvers.c:1087-1199
+        rc = solve_u_cn(C, st);
+    } else if (C->cfg.ddt_scheme == TG_DDT_FE) {
         // UeqnFE, ueqn_solvers.c:1411-1442
         explicit_rhs(C);
         TG_PROF(C, "fe_update", k_fe_update<<<nblk(G), 256, 0, C->stream>>>(G, C->s.ucont, dt, C->s.rhs, C->s.ucont_o));
@@ -1199,6 +1254,7 @@ static void solve_u_impl(tg_ctx *C, bool cart_tail)
         TG_PROF(C, "contra_to_cart_shell", k_contra_to_cart_shell<<<grid, b2, 0, C->stream>>>(g, C->fm64, C->s));
     }
     reset_cell_periodic(C, C->s.ucat);
+    return rc;
 }
 
 void solve_u(tg_ctx *C) { solve_u_impl(C, true); }
@@ -1279,14 +1335,20 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
             TG_CUDA(cudaMemcpyAsync(C->s.btheta_o.x, C->s.btheta.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         buoyancy(C);
     }
-    solve_u_impl(C, false);
+    const int urc = solve_u_impl(C, false, st);
     int rc = 0;
     if (capture) poisson_solve_capture(C);
     else rc = poisson_solve(C, st);
+    if (urc == 2) rc = 2;
+    else if (rc != 2) rc |= urc;
     pressure_update_and_project(C);
     contra_to_cart(C);
     if (C->prm.teqn) solve_t(C);        // main.c:194-205
     reduce_max_abs_div(C, C->d_scal + 16);
+    if (C->cfg.ddt_scheme == TG_DDT_CN) {   // main.c:214-272: Rhs_o for the next step
+        TG_CUDA(cudaMemsetAsync(C->s.rhs_o.x, 0, 3 * sizeof(double) * G, C->stream));
+        form_u(C, C->s.rhs_o, 1.0);
+    }
     if (C->prm.teqn) update_temperature_bcs(C);   // main.c:274-278
     update_cartesian_bcs(C);
     update_contravariant_bcs(C);
@@ -1304,6 +1366,7 @@ static bool graph_eligible(const tg_ctx *C)
 {
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
     return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
+           C->cfg.ddt_scheme != TG_DDT_CN &&              // host-driven Newton-Krylov loop
            C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 
