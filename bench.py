@@ -142,7 +142,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(name, precision, seed_offset=0, small=False, cells=None):
+def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="rk4"):
     from tosca_b200 import api, cases
     if name == "abl":
         kw = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=250.0) if small else {}
@@ -175,6 +175,10 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None):
         raise SystemExit(f"unknown workload {name}")
     if name != "farm":
         turbines = None
+    if ddt == "cn":                   # ddtScheme CN with the reference's SNES defaults (ueqn.c:128-130)
+        cfg.ddt_scheme = api.DDT_CN
+        cfg.snes_atol, cfg.snes_rtol, cfg.snes_maxit = 1e-5, 1e-30, 20
+        desc = desc.replace("RK4", "Crank-Nicolson (JFNK, absTolU 1e-5)", 1)
     cfg.poisson_rtol = 1e-30
     cfg.poisson_div_tol = DIV_TOL
     cfg.poisson_maxit = 400
@@ -370,6 +374,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm"])
+    ap.add_argument("--ddt", default="rk4", choices=["rk4", "cn"], help="momentum time scheme of the workload")
     ap.add_argument("--farm-adjoint-steps", type=int, default=200,
                     help="farm workload: steps of the C_T' gradient of the summed farm power")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
@@ -427,7 +432,8 @@ def main():
         return float(t.item())
 
     def arm(precision):
-        cfg, nodes, ucat, p, T, desc, turbines = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells)
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells,
+                                                               ddt=args.ddt)
         cfg.device = dev
         solver = tosca_b200.gpu_solver(cfg)
         cases.setup(solver, nodes, ucat, p, T)
