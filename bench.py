@@ -179,11 +179,19 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="
         cfg.ddt_scheme = api.DDT_CN
         cfg.snes_atol, cfg.snes_rtol, cfg.snes_maxit = 1e-5, 1e-30, 20
         desc = desc.replace("RK4", "Crank-Nicolson (JFNK, absTolU 1e-5)", 1)
+    elif ddt in IMEX:                 # IMEX schemes with the reference's KSP defaults (ueqn.c:249-282)
+        cfg.ddt_scheme = getattr(api, IMEX[ddt][0])
+        cfg.snes_atol, cfg.snes_rtol, cfg.gmres_restart = 1e-5, 1e-30, 30
+        desc = desc.replace("RK4", IMEX[ddt][1] + " (GMRES(30), absTolU 1e-5)", 1)
     cfg.poisson_rtol = 1e-30
     cfg.poisson_div_tol = DIV_TOL
     cfg.poisson_maxit = 400
     cfg.precision = api.PREC_MIXED if precision == "mixed" else api.PREC_FP64
     return cfg, nodes, ucat, p, T, desc, turbines
+
+
+IMEX = {"abcn": ("DDT_ABCN", "ABCN IMEX"), "rk3wcn": ("DDT_RK3WCN", "RK3WCN IMEX"),
+        "rk3socn": ("DDT_RK3SOCN", "RK3SOCN IMEX")}
 
 
 def cpu_baseline(workload, steps, threads=None):
@@ -374,7 +382,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm"])
-    ap.add_argument("--ddt", default="rk4", choices=["rk4", "cn"], help="momentum time scheme of the workload")
+    ap.add_argument("--ddt", default="rk4", choices=["rk4", "cn", "abcn", "rk3wcn", "rk3socn"], help="momentum time scheme of the workload")
     ap.add_argument("--farm-adjoint-steps", type=int, default=200,
                     help="farm workload: steps of the C_T' gradient of the summed farm power")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
@@ -450,6 +458,7 @@ def main():
             torch.cuda.synchronize()
         barrier()
         replayed = solver.graph_info()[0] - r0
+        mom = solver.momentum_info()
         t_dev = max_over_ranks(st.seconds)
         # per-kernel events on a few further steps (outside the timed region)
         L.tg_prof_reset(solver.h)
@@ -459,7 +468,7 @@ def main():
         L.tg_prof_enable(solver.h, 0)
         kernels = kernel_table(L, solver.h)
         return {"cfg": cfg, "desc": desc, "solver": solver, "st": st, "t_dev": t_dev, "clocks": clk.summary(),
-                "replayed": replayed,
+                "replayed": replayed, "momentum": mom,
                 "value": cfg.cells * args.steps * world / t_dev / 1e6, "kernels": kernels,
                 "roofline": roofline_of(kernels, precision, cfg.cells)}
 
@@ -555,6 +564,10 @@ def main():
                                 "launches_per_step": v["launches"] / max(1, args.profile_steps),
                                 "share": round(v["share"], 4)} for k, v in ranked[:12]},
         }
+        if args.ddt != "rk4":
+            o, k, r = head["momentum"]
+            line["config"]["momentum_solve_last_step"] = {
+                "newton_steps" if args.ddt == "cn" else "stages": o, "krylov_operator_products": k, "last_residual": r}
         if "fp64" in arms and head_prec != "fp64":
             a = arms["fp64"]
             line["fp64"] = {"value": round(a["value"], 3), "ms_per_step": a["t_dev"] / args.steps * 1e3,

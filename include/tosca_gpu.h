@@ -56,8 +56,12 @@ enum {
 };
 /* -divScheme (ueqn.c:82-110) */
 enum { TG_DIV_CENTRAL = 0, TG_DIV_QUICK = 1 };
-/* -dUdtScheme (ueqn.c:123-323) */
-enum { TG_DDT_FE = 0, TG_DDT_RK4 = 1, TG_DDT_CN = 2 };
+/* -dUdtScheme (ueqn.c:123-323): explicit (FE, RK4), Crank-Nicolson (CN,
+ * UeqnSNES) and the implicit-explicit schemes with a Crank-Nicolson viscous
+ * part solved by GMRES on the shell operator IMEXMatVec
+ * (ueqn_solvers.c:1508-1799): ABCN (Adams-Bashforth 2 convection), RK3WCN
+ * (Wray low-storage RK3) and RK3SOCN (Shu-Osher TVD RK3) */
+enum { TG_DDT_FE = 0, TG_DDT_RK4 = 1, TG_DDT_CN = 2, TG_DDT_ABCN = 3, TG_DDT_RK3WCN = 4, TG_DDT_RK3SOCN = 5 };
 /* arithmetic of the step */
 enum {
     TG_PREC_FP64  = 0,   /* every stage in FP64                                   */
@@ -106,10 +110,13 @@ typedef struct tg_config {
     double  prandtl;               /* -Pr: molecular Prandtl number (no LES)                */
     double  t_bc_value[6];         /* fixedValue: ghost value; fixedGradient: gradient      */
     /* Crank-Nicolson momentum solve (TG_DDT_CN; -absTolU, -relTolU, -snesMaxItersU,
-     * ueqn.c:128-138): stop at |F| <= max(snes_atol, snes_rtol |F_0|) */
+     * ueqn.c:128-138): stop at |F| <= max(snes_atol, snes_rtol |F_0|). The
+     * IMEX schemes stop their GMRES at |r| <= max(snes_atol, snes_rtol |b|)
+     * (KSPSetTolerances(kspIMEX, relTolU, absTolU, 1e30, 1000), ueqn.c:282) */
     double  snes_atol;
     double  snes_rtol;
     int32_t snes_maxit;
+    int32_t gmres_restart;         /* -kspGMRESRestartU (ueqn.c:233), 0 = 30                */
 } tg_config;
 
 /* per-call statistics */
@@ -234,6 +241,12 @@ tg_status tg_set_graphs(tg_ctx *ctx, int32_t on);
  * whether capture failed for this configuration (steps then run kernel by
  * kernel). */
 tg_status tg_graph_info(tg_ctx *ctx, int64_t *replays, int32_t *capture_failed);
+/* Iterations of the last implicit momentum solve (CN, ABCN, RK3WCN, RK3SOCN):
+ * outer = Newton steps (CN) or Runge-Kutta stages solved (IMEX); inner =
+ * operator products of the Krylov solver (the KSPGetIterationNumber values,
+ * summed); residual = the last Krylov residual estimate (KSPGetResidualNorm,
+ * ueqn_solvers.c:1560-1561). Zeros after an explicit step. */
+tg_status tg_momentum_info(tg_ctx *ctx, int32_t *outer, int32_t *inner, double *residual);
 
 /* --------------------------------------------------------------- wind farm -- */
 /* Uniform actuator-disk turbines: TOSCA's "uniformADM" with sampleType

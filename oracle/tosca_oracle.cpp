@@ -102,6 +102,11 @@ struct tg_ctx {
     std::vector<double> p, phi, nut, tmprt;
     std::vector<double> tmprt_o;                // teqn->Tmprt_o (tosca_oracle_teqn.inc)
     std::vector<V3> rhs_o;                      // ueqn->Rhs_o (tosca_oracle_cn.inc)
+    std::vector<V3> conv_o;                     // ueqn->RhsConv_o (ABCN, tosca_oracle_imex.inc)
+    // last implicit momentum solve: Newton steps or IMEX stages, Krylov
+    // operator products, last Krylov residual estimate
+    int mom_outer = 0, mom_inner = 0;
+    double mom_res = 0.0;
 
     // jLeft wall model arrays, indexed k*mx + i (tauWall, uMeanMag, uFilt)
     std::vector<double> twx, twy, twz, umean, ufx, ufy, ufz;
@@ -1091,7 +1096,9 @@ inline V3 quick(const V3 &f0, const V3 &f1, const V3 &f2, const V3 &f3, double w
     return 0.5 * (fU + fD) + (1. / 8.) * (2.0 * fU - (fD + fUU));
 }
 
-void formU(tg_ctx &C, std::vector<V3> &R, double scale)
+// mode: formMode (ueqn_solvers.c:17, 105-106, 877-928): 0 convection +
+// viscosity, 1 convection only, 2 viscosity (with the wall stress) only
+void formU(tg_ctx &C, std::vector<V3> &R, double scale, int mode = 0)
 {
     const int mx = C.mx, my = C.my, mz = C.mz;
     const bool quickDiv = C.c.div_scheme == TG_DIV_QUICK;
@@ -1264,12 +1271,16 @@ void formU(tg_ctx &C, std::vector<V3> &R, double scale)
         size_t c = C.I(k, j, i);
         size_t iw = C.I(k, j, i - 1), js = C.I(k, j - 1, i), kb = C.I(k - 1, j, i);
         V3 &F = C.fp[c];
-        F.x += (C.div1[c].x - C.div1[iw].x + C.div2[c].x - C.div2[js].x + C.div3[c].x - C.div3[kb].x);
-        F.y += (C.div1[c].y - C.div1[iw].y + C.div2[c].y - C.div2[js].y + C.div3[c].y - C.div3[kb].y);
-        F.z += (C.div1[c].z - C.div1[iw].z + C.div2[c].z - C.div2[js].z + C.div3[c].z - C.div3[kb].z);
-        F.x += (C.visc1[c].x - C.visc1[iw].x + C.visc2[c].x - C.visc2[js].x + C.visc3[c].x - C.visc3[kb].x);
-        F.y += (C.visc1[c].y - C.visc1[iw].y + C.visc2[c].y - C.visc2[js].y + C.visc3[c].y - C.visc3[kb].y);
-        F.z += (C.visc1[c].z - C.visc1[iw].z + C.visc2[c].z - C.visc2[js].z + C.visc3[c].z - C.visc3[kb].z);
+        if (mode != 2) {
+            F.x += (C.div1[c].x - C.div1[iw].x + C.div2[c].x - C.div2[js].x + C.div3[c].x - C.div3[kb].x);
+            F.y += (C.div1[c].y - C.div1[iw].y + C.div2[c].y - C.div2[js].y + C.div3[c].y - C.div3[kb].y);
+            F.z += (C.div1[c].z - C.div1[iw].z + C.div2[c].z - C.div2[js].z + C.div3[c].z - C.div3[kb].z);
+        }
+        if (mode != 1) {
+            F.x += (C.visc1[c].x - C.visc1[iw].x + C.visc2[c].x - C.visc2[js].x + C.visc3[c].x - C.visc3[kb].x);
+            F.y += (C.visc1[c].y - C.visc1[iw].y + C.visc2[c].y - C.visc2[js].y + C.visc3[c].y - C.visc3[kb].y);
+            F.z += (C.visc1[c].z - C.visc1[iw].z + C.visc2[c].z - C.visc2[js].z + C.visc3[c].z - C.visc3[kb].z);
+        }
         if (i == 1 && npi)      C.fp[C.I(k, j, i - 1)] = F;
         if (j == 1 && npj)      C.fp[C.I(k, j - 1, i)] = F;
         if (k == 1 && npk)      C.fp[C.I(k - 1, j, i)] = F;
@@ -1357,8 +1368,8 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
 #include "tosca_oracle_teqn.inc"
 #include "tosca_oracle_cn.inc"
 
-// ExplicitRhsU, ueqn_solvers.c:1276-1407
-void explicitRhsU(tg_ctx &C)
+// ExplicitRhsU, ueqn_solvers.c:1276-1407 (mode: formMode of its FormU)
+void explicitRhsU(tg_ctx &C, int mode = 0)
 {
     resetNoPenetration(C);
     resetFacePeriodic(C, C.ucont);
@@ -1378,13 +1389,16 @@ void explicitRhsU(tg_ctx &C)
     }
     if (!C.farm.empty())                                // ueqn_solvers.c:1340-1344
         for (size_t q = 0; q < G; q++) C.rhs[q] = C.rhs[q] + 1.0 * C.farm_cont[q];
-    formU(C, C.rhs, 1.0);
+    formU(C, C.rhs, 1.0, mode);
     if (C.c.source) sourceU(C, C.rhs);                 // ueqn_solvers.c:1365-1370
     if (C.c.mean_grad_p) meanGradPForcing(C, C.rhs);
     resetNonResolvedCellFaces(C, C.rhs);
 }
 
+#include "tosca_oracle_imex.inc"
+
 // SolveUEqn with UeqnFE / UeqnRK4, ueqn.c:397-440, ueqn_solvers.c:1411-1504
+// (UeqnSNES and the IMEX schemes in their own files)
 int solveUEqn(tg_ctx &C)
 {
     const size_t G = C.G;
@@ -1392,6 +1406,8 @@ int solveUEqn(tg_ctx &C)
     int rc = 0;
     if (C.c.ddt_scheme == TG_DDT_CN) {
         rc = ueqnSNES(C);
+    } else if (C.c.ddt_scheme >= TG_DDT_ABCN) {
+        rc = ueqnIMEX(C);
     } else if (C.c.ddt_scheme == TG_DDT_FE) {
         explicitRhsU(C);
         // VecScale(Rhs,dt) then VecAXPY(Rhs,1,Ucont_o): dt*rhs + ucont_o
@@ -1682,7 +1698,8 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->bc[TG_IRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_ILEFT] == TG_BC_WALL_SHUMANN ||
         cfg->bc[TG_KRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_KLEFT] == TG_BC_WALL_SHUMANN ||
         cfg->bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN) return TG_ERR_BAD_ARG;
-    if (cfg->dt <= 0 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 2) return TG_ERR_BAD_ARG;
+    if (cfg->dt <= 0 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
+    if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
@@ -1890,6 +1907,15 @@ tg_status tor_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
     });
 }
 
+tg_status tor_momentum_info(tg_ctx *C, int32_t *outer, int32_t *inner, double *residual)
+{
+    if (!C || !outer || !inner || !residual) return TG_ERR_BAD_ARG;
+    *outer = C->mom_outer;
+    *inner = C->mom_inner;
+    *residual = C->mom_res;
+    return TG_OK;
+}
+
 tg_status tor_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double *nut, int32_t halo, tg_stats *st)
 {
     return guarded(C, [&]() -> tg_status {
@@ -1994,6 +2020,7 @@ tg_status tor_adjoint_step(tg_ctx *C)
         if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
         if (C->c.teqn) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the temperature equation is not implemented");
         if (C->c.ddt_scheme == TG_DDT_CN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the Crank-Nicolson scheme is not implemented");
+        if (C->c.ddt_scheme >= TG_DDT_ABCN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the IMEX schemes is not implemented");
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
         auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;

@@ -21,7 +21,7 @@ TG_OK, TG_ERR_CUDA, TG_ERR_BAD_ARG, TG_ERR_NOT_CONVERGED, TG_ERR_NAN, TG_ERR_ALL
 BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
-DDT_FE, DDT_RK4, DDT_CN = 0, 1, 2
+DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
 TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
@@ -70,6 +70,7 @@ class TgConfig(C.Structure):
         ("snes_atol", C.c_double),
         ("snes_rtol", C.c_double),
         ("snes_maxit", C.c_int32),
+        ("gmres_restart", C.c_int32),
     ]
 
 
@@ -160,6 +161,7 @@ class Config:
     snes_atol: float = 1e-5
     snes_rtol: float = 1e-30
     snes_maxit: int = 20
+    gmres_restart: int = 30
 
     def to_c(self) -> TgConfig:
         c = TgConfig()
@@ -209,6 +211,7 @@ _SIGS = {
     "turbine_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int32]),
     "set_farm_objective": (C.c_int, [C.c_void_p, C.c_int32]),
     "ct_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "momentum_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
 }
 
 # adjoint entry points (the CPU restatement exports tor_adjoint_step only) and
@@ -449,6 +452,13 @@ class Solver:
         n, f = C.c_int64(), C.c_int32()
         self._check(self.fns["graph_info"](self.h, C.byref(n), C.byref(f)), "graph_info")
         return n.value, bool(f.value)
+
+    def momentum_info(self) -> tuple:
+        """(Newton steps or IMEX stages, Krylov operator products, last Krylov
+        residual estimate) of the last implicit momentum solve."""
+        a, b, r = C.c_int32(), C.c_int32(), C.c_double()
+        self._check(self.fns["momentum_info"](self.h, C.byref(a), C.byref(b), C.byref(r)), "momentum_info")
+        return a.value, b.value, r.value
 
     def step_host(self, ucont, ucat, p, nut=None, halo: int = 0) -> TgStats:
         st = TgStats()

@@ -932,6 +932,7 @@ static bool adjoint_supported(tg_ctx *C, std::string &why)
     if (!C->orthogonal) { why = "the adjoint needs the symmetric (orthogonal-grid) pressure operator"; return false; }
     if (C->prm.teqn) { why = "the adjoint of the temperature equation is not implemented"; return false; }
     if (C->cfg.ddt_scheme == TG_DDT_CN) { why = "the adjoint of the Crank-Nicolson scheme is not implemented"; return false; }
+    if (imex_scheme(C->cfg.ddt_scheme)) { why = "the adjoint of the IMEX schemes is not implemented"; return false; }
     return true;
 }
 

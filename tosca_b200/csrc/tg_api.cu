@@ -207,7 +207,8 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
-    if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > 2) return TG_ERR_BAD_ARG;
+    if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
+    if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
@@ -287,6 +288,7 @@ tg_status tg_destroy(tg_ctx *C)
     for (cudaStream_t a : C->aux) if (a) cudaStreamDestroy(a);
     try { farm_destroy(C); } catch (...) {}
     cn_destroy(C);
+    imex_destroy(C);
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);
@@ -577,6 +579,17 @@ tg_status tg_graph_info(tg_ctx *C, int64_t *replays, int32_t *capture_failed)
         if (!replays || !capture_failed) return fail(C, TG_ERR_BAD_ARG, "null output");
         *replays = C->replays;
         *capture_failed = C->graph_failed ? 1 : 0;
+        return TG_OK;
+    });
+}
+
+tg_status tg_momentum_info(tg_ctx *C, int32_t *outer, int32_t *inner, double *residual)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!outer || !inner || !residual) return fail(C, TG_ERR_BAD_ARG, "null output");
+        *outer = C->mom_outer;
+        *inner = C->mom_inner;
+        *residual = C->mom_res;
         return TG_OK;
     });
 }

@@ -22,7 +22,7 @@
 namespace tg {
 
 struct CnWork {
-    int m = 30;                       // GMRES restart
+    int m = 30;                       // GMRES restart (-kspGMRESRestartU)
     V3f<double> bu{}, U{}, F{}, W{}, FW{};
     double *V = nullptr;              // (m + 1) Krylov vectors of 3 G
     double *part = nullptr;           // dot-product partials
@@ -93,6 +93,7 @@ CnWork &work(tg_ctx *C)
     if (!C->cn) {
         CnWork *W = new CnWork();
         const size_t G = (size_t)C->g.size();
+        W->m = C->cfg.gmres_restart > 0 ? C->cfg.gmres_restart : 30;
         W->bu = dalloc3(C, G); W->U = dalloc3(C, G); W->F = dalloc3(C, G); W->W = dalloc3(C, G); W->FW = dalloc3(C, G);
         W->V = dallocd(C, (size_t)(W->m + 1) * 3 * G);
         W->nb = nblk(3 * (int64_t)G);
@@ -236,8 +237,9 @@ int solve_u_cn(tg_ctx *C, tg_stats *st)
     else if (rc == 0 && !(fn <= std::max(atol, rtol * f0))) rc = 1;
     // Ucont <- U (SNESFuncEval left the last evaluated point in the state)
     TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, W.U.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
-    C->cn_newton = newton;
-    C->cn_linear = linear;
+    C->mom_outer = newton;
+    C->mom_inner = linear;
+    C->mom_res = fn;
     (void)st;
     return rc;
 }

@@ -107,6 +107,7 @@ struct PoissonCtx;   // tg_poisson.cu
 struct AdjState;     // tg_adjoint.cu
 struct Farm;         // tg_farm.cu
 struct CnWork;       // tg_cn.cu
+struct ImexWork;     // tg_imex.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -168,7 +169,11 @@ struct tg_ctx {
     tg::AdjState *adj = nullptr;         // adjoint fields, tape and checkpoints (tg_adjoint.cu)
     tg::Farm *farm = nullptr;            // actuator-disk turbines (tg_farm.cu)
     tg::CnWork *cn = nullptr;            // Crank-Nicolson Newton-Krylov work (tg_cn.cu)
-    int cn_newton = 0, cn_linear = 0;    // iterations of the last implicit momentum solve
+    tg::ImexWork *imex = nullptr;        // IMEX GMRES work (tg_imex.cu)
+    // last implicit momentum solve: Newton steps or IMEX stages, Krylov
+    // operator products, last Krylov residual estimate
+    int mom_outer = 0, mom_inner = 0;
+    double mom_res = 0.0;
     bool taping = false;                 // the running step records its stage states
     // CUDA graph of a whole step (tg_step.cu): built on the first step that can
     // be captured, replayed afterwards
@@ -238,8 +243,10 @@ void update_nut(tg_ctx *C);
 void update_wall_models(tg_ctx *C);
 void grad_p(tg_ctx *C);
 void buoyancy(tg_ctx *C);
-void form_u(tg_ctx *C, V3f<double> rhs, double scale);
-void explicit_rhs(tg_ctx *C);
+// formMode (ueqn_solvers.c:17): 0 convection + viscosity, 1 convection, 2 viscosity
+void form_u(tg_ctx *C, V3f<double> rhs, double scale, int mode = 0);
+void form_u_again(tg_ctx *C, V3f<double> rhs, double scale);
+void explicit_rhs(tg_ctx *C, int mode = 0);
 void solve_u(tg_ctx *C);
 int solve_p(tg_ctx *C, tg_stats *st);
 double continuity_error(tg_ctx *C);
@@ -275,6 +282,9 @@ void adj_graph_destroy(tg_ctx *C);
 // Crank-Nicolson momentum step (tg_cn.cu)
 int solve_u_cn(tg_ctx *C, tg_stats *st);
 void cn_destroy(tg_ctx *C);
+bool imex_scheme(int ddt);                                         // tg_imex.cu
+int solve_u_imex(tg_ctx *C);
+void imex_destroy(tg_ctx *C);
 void cn_build_bu(tg_ctx *C, V3f<double> bu, bool half_rhs_o);   // tg_step.cu
 void mask_non_resolved(tg_ctx *C, V3f<double> v);               // resetNonResolvedCellFaces on v
 void contra_to_cart_stage(tg_ctx *C);

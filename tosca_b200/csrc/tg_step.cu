@@ -538,8 +538,10 @@ __device__ __forceinline__ R3<M> visc_flux(R3<M> s0, R3<M> s1, R3<M> s2, int dir
 
 // M: storage and arithmetic type of the metrics in the viscous flux; F: storage
 // type of the face fluxes. The convective flux is formed in FP64 from the FP64
-// Ucont and Ucat.
-template <class M, class F>
+// Ucont and Ucat. mode is FormU's formMode (ueqn_solvers.c:17, 105-106):
+// 0 convection + viscosity, 1 convection only, 2 viscosity (with the wall
+// stress) only; the skipped part of each face flux is zero.
+template <class M, class F, int mode>
 __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, State s, FluxWork<F> w, Params p)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -553,7 +555,9 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
     auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
     // ---- i faces, ueqn_solvers.c:173-395 with Compute_du_i (inline.h:2748-2807)
     if (j != 0 && k != 0 && !(g.pi && i == 0)) {
-        R3<double> dc = U(k, j, i + 1) - U(k, j, i), de, dz;
+      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+      if (mode != 1) {
+        dc = U(k, j, i + 1) - U(k, j, i);
         bool edge = (i == 0 || i == mx - 2);
         if (j == my - 2 && edge && (npj || npi))      de = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
         else if (j == 1 && edge && (npj || npi))      de = 0.5 * (U(k, j + 1, i + 1) + U(k, j + 1, i) - U(k, j, i + 1) - U(k, j, i));
@@ -561,8 +565,9 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
         if (k == mz - 2 && edge && (npk || npi))      dz = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
         else if (k == 1 && edge && (npk || npi))      dz = 0.5 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k, j, i + 1) - U(k, j, i));
         else                                          dz = 0.25 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
+      }
+      if (mode != 2) {
         double uc = s.ucont.x[f];
-        R3<double> dv;
         if (quickDiv) {
             int iL, iR;
             if (i == 0 || i == mx - 2) {
@@ -573,18 +578,23 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
             } else { iL = i - 1; iR = i + 2; }
             dv = (-uc) * quick(U(k, j, iL), U(k, j, i), U(k, j, i + 1), U(k, j, iR), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j, i + 1)));
+      }
+      if (mode != 1) {
         M nuEff;
         if (p.les) {
             double nt = 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1));
             if ((p.bc[TG_ILEFT] == TG_BC_SLIP && i == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && i == mx - 2)) nuEff = M(0);
             else nuEff = (M)(nu + nt);
         } else nuEff = (M)nu;
-        R3<M> v = visc_flux<M>(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff);
-        st3(w.f1, f, cvta<F>(dv + cvta<double>(v)));
+        vv = cvta<double>(visc_flux<M>(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff));
+      }
+      st3(w.f1, f, cvta<F>(dv + vv));
     }
     // ---- j faces, ueqn_solvers.c:397-602 with Compute_du_j (inline.h:2809-2869)
     if (i != 0 && k != 0 && !(g.pj && j == 0)) {
-        R3<double> dc, de = U(k, j + 1, i) - U(k, j, i), dz;
+      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+      if (mode != 1) {
+        de = U(k, j + 1, i) - U(k, j, i);
         bool edge = (j == 0 || j == my - 2);
         if (i == mx - 2 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k, j + 1, i - 1) - U(k, j, i - 1));
         else if (i == 1 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i + 1) + U(k, j, i + 1) - U(k, j + 1, i) - U(k, j, i));
@@ -592,8 +602,9 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
         if (k == mz - 2 && edge && (npk || npj))      dz = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
         else if (k == 1 && edge && (npk || npj))      dz = 0.5 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k, j + 1, i) - U(k, j, i));
         else                                          dz = 0.25 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
+      }
+      if (mode != 2) {
         double uc = s.ucont.y[f];
-        R3<double> dv;
         if (quickDiv) {
             int jL, jR;
             if (j == 0 || j == my - 2) {
@@ -604,6 +615,8 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
             } else { jL = j - 1; jR = j + 2; }
             dv = (-uc) * quick(U(k, jL, i), U(k, j, i), U(k, j + 1, i), U(k, jR, i), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j + 1, i)));
+      }
+      if (mode != 1) {
         M nuEff;
         R3<double> base{0, 0, 0};
         if (p.les) {
@@ -616,12 +629,15 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
             } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = M(0);
             else nuEff = (M)(nu + nt);
         } else nuEff = (M)nu;
-        R3<M> v = visc_flux<M>(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff);
-        st3(w.f2, f, cvta<F>(dv + (base + cvta<double>(v))));
+        vv = base + cvta<double>(visc_flux<M>(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff));
+      }
+      st3(w.f2, f, cvta<F>(dv + vv));
     }
     // ---- k faces, ueqn_solvers.c:604-778 with Compute_du_k (inline.h:2871-2931)
     if (i != 0 && j != 0 && !(g.pk && k == 0)) {
-        R3<double> dc, de, dz = U(k + 1, j, i) - U(k, j, i);
+      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+      if (mode != 1) {
+        dz = U(k + 1, j, i) - U(k, j, i);
         bool edge = (k == 0 || k == mz - 2);
         if (i == mx - 2 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j, i - 1) - U(k, j, i - 1));
         else if (i == 1 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i + 1) + U(k, j, i + 1) - U(k + 1, j, i) - U(k, j, i));
@@ -629,8 +645,9 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
         if (j == my - 2 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
         else if (j == 1 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j, i) - U(k, j, i));
         else                                          de = 0.25 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
+      }
+      if (mode != 2) {
         double uc = s.ucont.z[f];
-        R3<double> dv;
         if (quickDiv) {
             int kL, kR;
             if (k == 0 || k == mz - 2) {
@@ -641,14 +658,17 @@ __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, St
             } else { kL = k - 1; kR = k + 2; }
             dv = (-uc) * quick(U(kL, j, i), U(k, j, i), U(k + 1, j, i), U(kR, j, i), uc);
         } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k + 1, j, i)));
+      }
+      if (mode != 1) {
         M nuEff;
         if (p.les) {
             double nt = 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i));
             if ((p.bc[TG_KLEFT] == TG_BC_SLIP && k == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && k == mz - 2)) nuEff = M(0);
             else nuEff = (M)(nu + nt);
         } else nuEff = (M)nu;
-        R3<M> v = visc_flux<M>(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff);
-        st3(w.f3, f, cvta<F>(dv + cvta<double>(v)));
+        vv = cvta<double>(visc_flux<M>(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff));
+      }
+      st3(w.f3, f, cvta<F>(dv + vv));
     }
 }
 
@@ -1090,16 +1110,26 @@ void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g
 // FormU pass 1 (face fluxes) at the precision of the context's policy.
 // Pass 2 (k_cell_fp) follows; the flux planes are only read at the points
 // pass 1 writes, fp only at interior cells.
-static void form_u_faces(tg_ctx *C)
+template <int mode>
+static void face_fluxes(tg_ctx *C, dim3 gr)
+{
+    const Grid g = C->g;
+    const auto &P = C->pol;
+    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, float, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm)));
+    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, double, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm)));
+    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, float, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm)));
+    else TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, double, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm)));
+}
+
+static void form_u_faces(tg_ctx *C, int mode)
 {
     const Grid g = C->g;
     refresh_met32(C);
     const dim3 gr = gf(g);
     const auto &P = C->pol;
-    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<float, float><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm));
-    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<float, double><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm));
-    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, float><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm));
-    else TG_PROF(C, "formu_face_fluxes", k_face_fluxes<double, double><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm));
+    if (mode == 1) face_fluxes<1>(C, gr);
+    else if (mode == 2) face_fluxes<2>(C, gr);
+    else face_fluxes<0>(C, gr);
     if (P.flux32) TG_PROF(C, "formu_cell_fp", k_cell_fp<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fw32));
     else TG_PROF(C, "formu_cell_fp", k_cell_fp<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fw64));
 }
@@ -1116,13 +1146,20 @@ static void rhs_faces(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
     else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2));
 }
 
-void form_u(tg_ctx *C, V3f<double> rhs, double scale)
+void form_u(tg_ctx *C, V3f<double> rhs, double scale, int mode)
 {
-    form_u_faces(C);
+    form_u_faces(C, mode);
     rhs_faces<false>(C, rhs, scale, 0);
 }
 
-void explicit_rhs(tg_ctx *C)
+// rhs += scale * FormU again from the cell sums the last FormU left (same
+// state and formMode)
+void form_u_again(tg_ctx *C, V3f<double> rhs, double scale)
+{
+    rhs_faces<false>(C, rhs, scale, 0);
+}
+
+void explicit_rhs(tg_ctx *C, int mode)
 {
     const Grid g = C->g;
     reset_no_penetration(C);
@@ -1130,7 +1167,7 @@ void explicit_rhs(tg_ctx *C)
     contra_to_cart_stage(C);
     reset_cell_periodic(C, C->s.ucat);
     if (C->taping) tape_stage(C);
-    form_u_faces(C);
+    form_u_faces(C, mode);
     // every point outside the interior faces keeps Rhs = -dP + b = 0: zero from
     // the allocation, rewritten here only after a caller wrote Rhs
     if (C->clear_rhs) {
@@ -1225,6 +1262,9 @@ static int solve_u_impl(tg_ctx *C, bool cart_tail, tg_stats *st = nullptr)
     if (C->cfg.ddt_scheme == TG_DDT_CN) {
         // UeqnSNES, ueqn_solvers.c:1087-1199
         rc = solve_u_cn(C, st);
+    } else if (imex_scheme(C->cfg.ddt_scheme)) {
+        // UeqnABCN / UeqnRK3CN_W / UeqnRK3CN_SO, ueqn_solvers.c:1508-1735
+        rc = solve_u_imex(C);
     } else if (C->cfg.ddt_scheme == TG_DDT_FE) {
         // UeqnFE, ueqn_solvers.c:1411-1442
         explicit_rhs(C);
@@ -1366,7 +1406,7 @@ static bool graph_eligible(const tg_ctx *C)
 {
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
     return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
-           C->cfg.ddt_scheme != TG_DDT_CN &&              // host-driven Newton-Krylov loop
+           C->cfg.ddt_scheme != TG_DDT_CN && !imex_scheme(C->cfg.ddt_scheme) &&   // host-driven Krylov loops
            C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 
