@@ -321,6 +321,28 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
             for (double v : h) mx = std::max(mx, std::fabs(v));
         }
         C->orthogonal = (mx == 0.0);
+        // axis alignment: in every cell-face (csi, eta, zet) and face (icsi ..
+        // kzet) metric only csi.y, eta.z, zet.x differ from zero by more than
+        // the round-off of the metric evaluation (1e-12 of the array's largest
+        // component; the face averages of a mesh of planes leave ~1e-16)
+        const Metrics &M = C->m;
+        auto amax = [&](const double *a) {
+            TG_CUDA(cudaMemcpy(h.data(), a, G * sizeof(double), cudaMemcpyDeviceToHost));
+            double r = 0.0;
+            for (double v : h) r = std::max(r, std::fabs(v));
+            return r;
+        };
+        bool ax = true;
+        auto along = [&](const V3f<double> &v, int keep) {
+            const double *c[3] = {v.x, v.y, v.z};
+            const double d = amax(c[keep]);
+            for (int q = 0; q < 3 && ax; q++)
+                if (q != keep && !(amax(c[q]) <= 1e-12 * d)) ax = false;
+        };
+        for (const V3f<double> &v : {M.csi, M.icsi, M.jcsi, M.kcsi}) along(v, 1);
+        for (const V3f<double> &v : {M.eta, M.ieta, M.jeta, M.keta}) along(v, 2);
+        for (const V3f<double> &v : {M.zet, M.izet, M.jzet, M.kzet}) along(v, 0);
+        C->axis_aligned = ax;
         graph_destroy(C);          // the captured step refers to the old solver buffers
         C->graph_failed = false;
         farm_destroy(C);           // turbine stencils refer to the old cell centres

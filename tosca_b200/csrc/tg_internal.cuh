@@ -140,6 +140,10 @@ struct tg_ctx {
     int red_blocks = 0;
     bool has_mesh = false;
     bool orthogonal = true;              // all cross metric-tensor terms vanish
+    // csi || y, eta || z, zet || x at every point of every cell and face
+    // metric up to round-off (the reference's i -> y, j -> z, k -> x axes on
+    // a mesh of planes): FormU reads only those components
+    bool axis_aligned = false;
     bool ufilt_set = false;
     int it = 0;
     // mixed precision: FP32 copies of the stencil metrics (and FP32 FormU

@@ -536,140 +536,213 @@ __device__ __forceinline__ R3<M> visc_flux(R3<M> s0, R3<M> s1, R3<M> s2, int dir
     return v;
 }
 
+// Pass 1 runs one thread per interior cell (k, j, i): it forms the i, j and
+// k faces on the cell's + side, and a cell next to a non-periodic 0 boundary
+// also the face on its - side (face 0, which a periodic direction does not
+// form). Ucat and nut are staged in a shared-memory tile covering the block's
+// cells with one cell below and two above in every direction, loaded once
+// with the periodic wrap of the DMDA index (g.id); every stencil read then is
+// a fixed tile offset. Tile points outside a non-periodic extent hold 0 and
+// are never read; the QUICK points of the boundary faces, which may lie
+// outside the tile (the periodic wrap reads i = mx + 2 and i = -3), are read
+// from global memory.
+//
+// visc_flux on an axis-aligned mesh (csi || y, eta || z, zet || x, the
+// reference's i -> y, j -> z, k -> x axes): cs = csi.y, et = eta.z, ze = zet.x
+// of the face. Every other metric component is zero up to the round-off of
+// the metric evaluation (at most 1e-12 of the largest, tg_set_mesh_nodes), so
+// the products left out change the flux by that relative amount at most; the
+// terms kept are the same products.
+template <class M>
+__device__ __forceinline__ R3<M> visc_flux_ax(M cs, M et, M ze, int dir, R3<M> dc, R3<M> de, R3<M> dz, M ajc, M nuEff)
+{
+    R3<M> v;
+    if (dir == 0) {          // n = csi: g11 = cs^2, r21 = dz.y ze, r22 = dc.y cs, r23 = de.y et
+        const M g11 = cs * cs;
+        v.x = (g11 * dc.x + (dz.y * ze) * cs) * ajc * (nuEff);
+        v.y = (g11 * dc.y + (dc.y * cs) * cs) * ajc * (nuEff);
+        v.z = (g11 * dc.z + (de.y * et) * cs) * ajc * (nuEff);
+    } else if (dir == 1) {   // n = eta: g21 = et^2, r31 = dz.z ze, r32 = dc.z cs, r33 = de.z et
+        const M g21 = et * et;
+        v.x = (g21 * de.x + (dz.z * ze) * et) * ajc * (nuEff);
+        v.y = (g21 * de.y + (dc.z * cs) * et) * ajc * (nuEff);
+        v.z = (g21 * de.z + (de.z * et) * et) * ajc * (nuEff);
+    } else {                 // n = zet: g31 = ze^2, r11 = dz.x ze, r12 = dc.x cs, r13 = de.x et
+        const M g31 = ze * ze;
+        v.x = (g31 * dz.x + (dz.x * ze) * ze) * ajc * (nuEff);
+        v.y = (g31 * dz.y + (dc.x * cs) * ze) * ajc * (nuEff);
+        v.z = (g31 * dz.z + (de.x * et) * ze) * ajc * (nuEff);
+    }
+    return v;
+}
+
 // M: storage and arithmetic type of the metrics in the viscous flux; F: storage
 // type of the face fluxes. The convective flux is formed in FP64 from the FP64
 // Ucont and Ucat. mode is FormU's formMode (ueqn_solvers.c:17, 105-106):
 // 0 convection + viscosity, 1 convection only, 2 viscosity (with the wall
-// stress) only; the skipped part of each face flux is zero.
-template <class M, class F, int mode>
+// stress) only; the skipped part of each face flux is zero. AX: the mesh is
+// axis-aligned (visc_flux_ax reads 3 of the 9 face metric components).
+constexpr int FTX = BX + 3, FTY = BY + 3, FTZ = BZ + 3, FTN = FTX * FTY * FTZ;
+
+template <class M, class F, int mode, bool AX>
 __global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, State s, FluxWork<F> w, Params p)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    __shared__ double su[3][FTN];
+    __shared__ double sn[FTN];
     const int mx = g.mx, my = g.my, mz = g.mz;
+    const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY, k0 = 1 + blockIdx.z * BZ;
+    const bool les = p.les;
+    for (int q = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x; q < FTN; q += BX * BY * BZ) {
+        const int tx = q % FTX, ty = (q / FTX) % FTY, tz = q / (FTX * FTY);
+        const int gi = g.wi(i0 - 1 + tx), gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz);
+        double ux = 0.0, uy = 0.0, uz = 0.0, nt = 0.0;
+        if (gi >= 0 && gi < mx && gj >= 0 && gj < my && gk >= 0 && gk < mz) {
+            const int c = (gk * my + gj) * mx + gi;
+            ux = s.ucat.x[c]; uy = s.ucat.y[c]; uz = s.ucat.z[c];
+            if (mode != 1 && les) nt = s.nut[c];
+        }
+        su[0][q] = ux; su[1][q] = uy; su[2][q] = uz; sn[q] = nt;
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0 + threadIdx.z;
+    if (i > mx - 2 || j > my - 2 || k > mz - 2) return;
     const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
     const bool quickDiv = p.div_scheme == TG_DIV_QUICK;
     const double nu = p.nu;
-    int f = g.lin(k, j, i);
+    const int t0 = ((threadIdx.z + 1) * FTY + threadIdx.y + 1) * FTX + threadIdx.x + 1;   // tile index of (k, j, i)
+    auto S = [&](int dk, int dj, int di) { const int q = t0 + (dk * FTY + dj) * FTX + di; return R3<double>{su[0][q], su[1][q], su[2][q]}; };
+    auto SN = [&](int dk, int dj, int di) { return sn[t0 + (dk * FTY + dj) * FTX + di]; };
     auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
-    auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
-    // ---- i faces, ueqn_solvers.c:173-395 with Compute_du_i (inline.h:2748-2807)
-    if (j != 0 && k != 0 && !(g.pi && i == 0)) {
-      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
-      if (mode != 1) {
-        dc = U(k, j, i + 1) - U(k, j, i);
-        bool edge = (i == 0 || i == mx - 2);
-        if (j == my - 2 && edge && (npj || npi))      de = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
-        else if (j == 1 && edge && (npj || npi))      de = 0.5 * (U(k, j + 1, i + 1) + U(k, j + 1, i) - U(k, j, i + 1) - U(k, j, i));
-        else                                          de = 0.25 * (U(k, j + 1, i + 1) + U(k, j + 1, i) - U(k, j - 1, i + 1) - U(k, j - 1, i));
-        if (k == mz - 2 && edge && (npk || npi))      dz = 0.5 * (U(k, j, i + 1) + U(k, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
-        else if (k == 1 && edge && (npk || npi))      dz = 0.5 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k, j, i + 1) - U(k, j, i));
-        else                                          dz = 0.25 * (U(k + 1, j, i + 1) + U(k + 1, j, i) - U(k - 1, j, i + 1) - U(k - 1, j, i));
-      }
-      if (mode != 2) {
-        double uc = s.ucont.x[f];
-        if (quickDiv) {
-            int iL, iR;
-            if (i == 0 || i == mx - 2) {
-                if (g.pi && i == mx - 2) { iR = mx + 2; iL = i - 1; }
-                else if (g.pi && i == 0) { iL = -3; iR = i + 2; }
-                else if (i == 0) { iL = i; iR = i + 2; }
-                else { iL = i - 1; iR = i + 1; }
-            } else { iL = i - 1; iR = i + 2; }
-            dv = (-uc) * quick(U(k, j, iL), U(k, j, i), U(k, j, i + 1), U(k, j, iR), uc);
-        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j, i + 1)));
-      }
-      if (mode != 1) {
-        M nuEff;
-        if (p.les) {
-            double nt = 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1));
-            if ((p.bc[TG_ILEFT] == TG_BC_SLIP && i == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && i == mx - 2)) nuEff = M(0);
-            else nuEff = (M)(nu + nt);
-        } else nuEff = (M)nu;
-        vv = cvta<double>(visc_flux<M>(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff));
-      }
-      st3(w.f1, f, cvta<F>(dv + vv));
-    }
-    // ---- j faces, ueqn_solvers.c:397-602 with Compute_du_j (inline.h:2809-2869)
-    if (i != 0 && k != 0 && !(g.pj && j == 0)) {
-      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
-      if (mode != 1) {
-        de = U(k, j + 1, i) - U(k, j, i);
-        bool edge = (j == 0 || j == my - 2);
-        if (i == mx - 2 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k, j + 1, i - 1) - U(k, j, i - 1));
-        else if (i == 1 && edge && (npi || npj))      dc = 0.5 * (U(k, j + 1, i + 1) + U(k, j, i + 1) - U(k, j + 1, i) - U(k, j, i));
-        else                                          dc = 0.25 * (U(k, j + 1, i + 1) + U(k, j, i + 1) - U(k, j + 1, i - 1) - U(k, j, i - 1));
-        if (k == mz - 2 && edge && (npk || npj))      dz = 0.5 * (U(k, j + 1, i) + U(k, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
-        else if (k == 1 && edge && (npk || npj))      dz = 0.5 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k, j + 1, i) - U(k, j, i));
-        else                                          dz = 0.25 * (U(k + 1, j + 1, i) + U(k + 1, j, i) - U(k - 1, j + 1, i) - U(k - 1, j, i));
-      }
-      if (mode != 2) {
-        double uc = s.ucont.y[f];
-        if (quickDiv) {
-            int jL, jR;
-            if (j == 0 || j == my - 2) {
-                if (g.pj && j == my - 2) { jR = my + 2; jL = j - 1; }
-                else if (g.pj && j == 0) { jL = -3; jR = j + 2; }
-                else if (j == 0) { jL = j; jR = j + 2; }
-                else { jL = j - 1; jR = j + 1; }
-            } else { jL = j - 1; jR = j + 2; }
-            dv = (-uc) * quick(U(k, jL, i), U(k, j, i), U(k, j + 1, i), U(k, jR, i), uc);
-        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k, j + 1, i)));
-      }
-      if (mode != 1) {
-        M nuEff;
-        R3<double> base{0, 0, 0};
-        if (p.les) {
-            double nt = 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i));
-            // both j patches read the jLeft wall stress, ueqn_solvers.c:548-558
-            if ((p.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN && j == my - 2)) {
-                int w = k * mx + i;
-                base = R3<double>{-s.twx[w], -s.twy[w], -s.twz[w]};
-                nuEff = (M)nu;
-            } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = M(0);
-            else nuEff = (M)(nu + nt);
-        } else nuEff = (M)nu;
-        vv = base + cvta<double>(visc_flux<M>(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff));
-      }
-      st3(w.f2, f, cvta<F>(dv + vv));
-    }
-    // ---- k faces, ueqn_solvers.c:604-778 with Compute_du_k (inline.h:2871-2931)
-    if (i != 0 && j != 0 && !(g.pk && k == 0)) {
-      R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
-      if (mode != 1) {
-        dz = U(k + 1, j, i) - U(k, j, i);
-        bool edge = (k == 0 || k == mz - 2);
-        if (i == mx - 2 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j, i - 1) - U(k, j, i - 1));
-        else if (i == 1 && edge && (npi || npk))      dc = 0.5 * (U(k + 1, j, i + 1) + U(k, j, i + 1) - U(k + 1, j, i) - U(k, j, i));
-        else                                          dc = 0.25 * (U(k + 1, j, i + 1) + U(k, j, i + 1) - U(k + 1, j, i - 1) - U(k, j, i - 1));
-        if (j == my - 2 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j, i) + U(k, j, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
-        else if (j == 1 && edge && (npj || npk))      de = 0.5 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j, i) - U(k, j, i));
-        else                                          de = 0.25 * (U(k + 1, j + 1, i) + U(k, j + 1, i) - U(k + 1, j - 1, i) - U(k, j - 1, i));
-      }
-      if (mode != 2) {
-        double uc = s.ucont.z[f];
-        if (quickDiv) {
-            int kL, kR;
-            if (k == 0 || k == mz - 2) {
-                if (g.pk && k == mz - 2) { kR = mz + 2; kL = k - 1; }
-                else if (g.pk && k == 0) { kL = -3; kR = k + 2; }
-                else if (k == 0) { kL = k; kR = k + 2; }
-                else { kL = k - 1; kR = k + 1; }
-            } else { kL = k - 1; kR = k + 2; }
-            dv = (-uc) * quick(U(kL, j, i), U(k, j, i), U(k + 1, j, i), U(kR, j, i), uc);
-        } else dv = (-uc) * (0.5 * (U(k, j, i) + U(k + 1, j, i)));
-      }
-      if (mode != 1) {
-        M nuEff;
-        if (p.les) {
-            double nt = 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i));
-            if ((p.bc[TG_KLEFT] == TG_BC_SLIP && k == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && k == mz - 2)) nuEff = M(0);
-            else nuEff = (M)(nu + nt);
-        } else nuEff = (M)nu;
-        vv = cvta<double>(visc_flux<M>(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff));
-      }
-      st3(w.f3, f, cvta<F>(dv + vv));
-    }
+
+    // ---- i face (k, j, fi), fi = i + e: ueqn_solvers.c:173-395 with Compute_du_i (inline.h:2748-2807)
+    auto iface = [&](int fi, int e) {
+        const int f = g.lin(k, j, fi);
+        const bool edge = (fi == 0 || fi == mx - 2);
+        R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+        if (mode != 1) {
+            dc = S(0, 0, e + 1) - S(0, 0, e);
+            if (j == my - 2 && edge && (npj || npi))      de = 0.5 * (S(0, 0, e + 1) + S(0, 0, e) - S(0, -1, e + 1) - S(0, -1, e));
+            else if (j == 1 && edge && (npj || npi))      de = 0.5 * (S(0, 1, e + 1) + S(0, 1, e) - S(0, 0, e + 1) - S(0, 0, e));
+            else                                          de = 0.25 * (S(0, 1, e + 1) + S(0, 1, e) - S(0, -1, e + 1) - S(0, -1, e));
+            if (k == mz - 2 && edge && (npk || npi))      dz = 0.5 * (S(0, 0, e + 1) + S(0, 0, e) - S(-1, 0, e + 1) - S(-1, 0, e));
+            else if (k == 1 && edge && (npk || npi))      dz = 0.5 * (S(1, 0, e + 1) + S(1, 0, e) - S(0, 0, e + 1) - S(0, 0, e));
+            else                                          dz = 0.25 * (S(1, 0, e + 1) + S(1, 0, e) - S(-1, 0, e + 1) - S(-1, 0, e));
+        }
+        if (mode != 2) {
+            const double uc = s.ucont.x[f];
+            if (quickDiv) {
+                if (edge) {
+                    int iL, iR;
+                    if (g.pi && fi == mx - 2) { iR = mx + 2; iL = fi - 1; }
+                    else if (fi == 0) { iL = fi; iR = fi + 2; }
+                    else { iL = fi - 1; iR = fi + 1; }
+                    dv = (-uc) * quick(U(k, j, iL), U(k, j, fi), U(k, j, fi + 1), U(k, j, iR), uc);
+                } else dv = (-uc) * quick(S(0, 0, e - 1), S(0, 0, e), S(0, 0, e + 1), S(0, 0, e + 2), uc);
+            } else dv = (-uc) * (0.5 * (S(0, 0, e) + S(0, 0, e + 1)));
+        }
+        if (mode != 1) {
+            M nuEff;
+            if (p.les) {
+                const double nt = 0.5 * (SN(0, 0, e) + SN(0, 0, e + 1));
+                if ((p.bc[TG_ILEFT] == TG_BC_SLIP && fi == 0) || (p.bc[TG_IRIGHT] == TG_BC_SLIP && fi == mx - 2)) nuEff = M(0);
+                else nuEff = (M)(nu + nt);
+            } else nuEff = (M)nu;
+            if (AX) vv = cvta<double>(visc_flux_ax<M>(m.icsi.y[f], m.ieta.z[f], m.izet.x[f], 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff));
+            else vv = cvta<double>(visc_flux<M>(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.iaj[f], nuEff));
+        }
+        st3(w.f1, f, cvta<F>(dv + vv));
+    };
+    // ---- j face (k, fj, i), fj = j + e: ueqn_solvers.c:397-602 with Compute_du_j (inline.h:2809-2869)
+    auto jface = [&](int fj, int e) {
+        const int f = g.lin(k, fj, i);
+        const bool edge = (fj == 0 || fj == my - 2);
+        R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+        if (mode != 1) {
+            de = S(0, e + 1, 0) - S(0, e, 0);
+            if (i == mx - 2 && edge && (npi || npj))      dc = 0.5 * (S(0, e + 1, 0) + S(0, e, 0) - S(0, e + 1, -1) - S(0, e, -1));
+            else if (i == 1 && edge && (npi || npj))      dc = 0.5 * (S(0, e + 1, 1) + S(0, e, 1) - S(0, e + 1, 0) - S(0, e, 0));
+            else                                          dc = 0.25 * (S(0, e + 1, 1) + S(0, e, 1) - S(0, e + 1, -1) - S(0, e, -1));
+            if (k == mz - 2 && edge && (npk || npj))      dz = 0.5 * (S(0, e + 1, 0) + S(0, e, 0) - S(-1, e + 1, 0) - S(-1, e, 0));
+            else if (k == 1 && edge && (npk || npj))      dz = 0.5 * (S(1, e + 1, 0) + S(1, e, 0) - S(0, e + 1, 0) - S(0, e, 0));
+            else                                          dz = 0.25 * (S(1, e + 1, 0) + S(1, e, 0) - S(-1, e + 1, 0) - S(-1, e, 0));
+        }
+        if (mode != 2) {
+            const double uc = s.ucont.y[f];
+            if (quickDiv) {
+                if (edge) {
+                    int jL, jR;
+                    if (g.pj && fj == my - 2) { jR = my + 2; jL = fj - 1; }
+                    else if (fj == 0) { jL = fj; jR = fj + 2; }
+                    else { jL = fj - 1; jR = fj + 1; }
+                    dv = (-uc) * quick(U(k, jL, i), U(k, fj, i), U(k, fj + 1, i), U(k, jR, i), uc);
+                } else dv = (-uc) * quick(S(0, e - 1, 0), S(0, e, 0), S(0, e + 1, 0), S(0, e + 2, 0), uc);
+            } else dv = (-uc) * (0.5 * (S(0, e, 0) + S(0, e + 1, 0)));
+        }
+        if (mode != 1) {
+            M nuEff;
+            R3<double> base{0, 0, 0};
+            if (p.les) {
+                const double nt = 0.5 * (SN(0, e, 0) + SN(0, e + 1, 0));
+                // both j patches read the jLeft wall stress, ueqn_solvers.c:548-558
+                if ((p.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && fj == 0) || (p.bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN && fj == my - 2)) {
+                    const int q = k * mx + i;
+                    base = R3<double>{-s.twx[q], -s.twy[q], -s.twz[q]};
+                    nuEff = (M)nu;
+                } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && fj == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && fj == my - 2)) nuEff = M(0);
+                else nuEff = (M)(nu + nt);
+            } else nuEff = (M)nu;
+            if (AX) vv = base + cvta<double>(visc_flux_ax<M>(m.jcsi.y[f], m.jeta.z[f], m.jzet.x[f], 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff));
+            else vv = base + cvta<double>(visc_flux<M>(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.jaj[f], nuEff));
+        }
+        st3(w.f2, f, cvta<F>(dv + vv));
+    };
+    // ---- k face (fk, j, i), fk = k + e: ueqn_solvers.c:604-778 with Compute_du_k (inline.h:2871-2931)
+    auto kface = [&](int fk, int e) {
+        const int f = g.lin(fk, j, i);
+        const bool edge = (fk == 0 || fk == mz - 2);
+        R3<double> dv{0, 0, 0}, vv{0, 0, 0}, dc, de, dz;
+        if (mode != 1) {
+            dz = S(e + 1, 0, 0) - S(e, 0, 0);
+            if (i == mx - 2 && edge && (npi || npk))      dc = 0.5 * (S(e + 1, 0, 0) + S(e, 0, 0) - S(e + 1, 0, -1) - S(e, 0, -1));
+            else if (i == 1 && edge && (npi || npk))      dc = 0.5 * (S(e + 1, 0, 1) + S(e, 0, 1) - S(e + 1, 0, 0) - S(e, 0, 0));
+            else                                          dc = 0.25 * (S(e + 1, 0, 1) + S(e, 0, 1) - S(e + 1, 0, -1) - S(e, 0, -1));
+            if (j == my - 2 && edge && (npj || npk))      de = 0.5 * (S(e + 1, 0, 0) + S(e, 0, 0) - S(e + 1, -1, 0) - S(e, -1, 0));
+            else if (j == 1 && edge && (npj || npk))      de = 0.5 * (S(e + 1, 1, 0) + S(e, 1, 0) - S(e + 1, 0, 0) - S(e, 0, 0));
+            else                                          de = 0.25 * (S(e + 1, 1, 0) + S(e, 1, 0) - S(e + 1, -1, 0) - S(e, -1, 0));
+        }
+        if (mode != 2) {
+            const double uc = s.ucont.z[f];
+            if (quickDiv) {
+                if (edge) {
+                    int kL, kR;
+                    if (g.pk && fk == mz - 2) { kR = mz + 2; kL = fk - 1; }
+                    else if (fk == 0) { kL = fk; kR = fk + 2; }
+                    else { kL = fk - 1; kR = fk + 1; }
+                    dv = (-uc) * quick(U(kL, j, i), U(fk, j, i), U(fk + 1, j, i), U(kR, j, i), uc);
+                } else dv = (-uc) * quick(S(e - 1, 0, 0), S(e, 0, 0), S(e + 1, 0, 0), S(e + 2, 0, 0), uc);
+            } else dv = (-uc) * (0.5 * (S(e, 0, 0) + S(e + 1, 0, 0)));
+        }
+        if (mode != 1) {
+            M nuEff;
+            if (p.les) {
+                const double nt = 0.5 * (SN(e, 0, 0) + SN(e + 1, 0, 0));
+                if ((p.bc[TG_KLEFT] == TG_BC_SLIP && fk == 0) || (p.bc[TG_KRIGHT] == TG_BC_SLIP && fk == mz - 2)) nuEff = M(0);
+                else nuEff = (M)(nu + nt);
+            } else nuEff = (M)nu;
+            if (AX) vv = cvta<double>(visc_flux_ax<M>(m.kcsi.y[f], m.keta.z[f], m.kzet.x[f], 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff));
+            else vv = cvta<double>(visc_flux<M>(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, cvta<M>(dc), cvta<M>(de), cvta<M>(dz), m.kaj[f], nuEff));
+        }
+        st3(w.f3, f, cvta<F>(dv + vv));
+    };
+    // one emitted body per direction: the second pass is the face on the -
+    // side of a cell next to a non-periodic 0 boundary
+    const int ni = (i == 1 && npi) ? 2 : 1, nj = (j == 1 && npj) ? 2 : 1, nk = (k == 1 && npk) ? 2 : 1;
+#pragma unroll 1
+    for (int e = 0; e > -ni; e--) iface(i + e, e);
+#pragma unroll 1
+    for (int e = 0; e > -nj; e--) jface(j + e, e);
+#pragma unroll 1
+    for (int e = 0; e > -nk; e--) kface(k + e, e);
 }
 
 // Pass 2 (ueqn_solvers.c:825-947): divergence of the face fluxes of interior
@@ -708,7 +781,7 @@ __global__ void k_cell_fp(Grid g, FluxWork<F> w)
 // force (ueqn_solvers.c:1340-1344), += FormU, += sourceU (body force), +=
 // meanGradPForcing (ueqn_sources.c:3735-3822). MR:
 // metric storage type; F: face-flux storage type.
-template <class MR, class F, bool fused>
+template <class MR, class F, bool fused, bool AX>
 __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -735,10 +808,36 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
     using M = typename std::conditional<std::is_same<MR, float>::value && std::is_same<F, float>::value, float, double>::type;
     auto FP = [&](int kk, int jj, int ii) { return cvta<M>(ld3(w.fp, g.lin(kk, jj, ii))); };
     auto MT = [&](const V3f<MR> &v, int q) { return cvta<M>(ld3(v, q)); };
-    const R3<M> fpc = FP(k, j, i);
     const M sc = (M)scale, h = M(0.5);
     M v1, v2;
     double ox, oy, oz;
+    if (AX) {
+        // axis-aligned mesh: S . fp is csi.y fp.y, eta.z fp.z, zet.x fp.x
+        const int pl = g.mx * g.my;
+        const int ie = i < g.mx - 2 ? c + 1 : (g.pi ? g.lin(k, j, 1) : c);
+        const int jn = j < g.my - 2 ? c + g.mx : (g.pj ? g.lin(k, 1, i) : c);
+        const int kt = k < g.mz - 2 ? c + pl : (g.pk ? g.lin(1, j, i) : c);
+        v1 = (M)m.csi.y[c] * (M)w.fp.y[c]; v2 = (M)m.csi.y[c + 1] * (M)w.fp.y[ie];
+        ox = base.x + (double)(sc * (M)m.iaj[c] * (h * (v1 + v2)));
+        v1 = (M)m.eta.z[c] * (M)w.fp.z[c]; v2 = (M)m.eta.z[c + g.mx] * (M)w.fp.z[jn];
+        oy = base.y + (double)(sc * (M)m.jaj[c] * (h * (v1 + v2)));
+        v1 = (M)m.zet.x[c] * (M)w.fp.x[c]; v2 = (M)m.zet.x[c + pl] * (M)w.fp.x[kt];
+        oz = base.z + (double)(sc * (M)m.kaj[c] * (h * (v1 + v2)));
+        if (fused && p.source) {
+            const V3f<double> &f = s.source;
+            ox += 1.0 * (0.5 * (f.y[c] + f.y[c + 1]) * (double)m.icsi.y[c]);
+            oy += 1.0 * (0.5 * (f.z[c] + f.z[c + g.mx]) * (double)m.jeta.z[c]);
+            oz += 1.0 * (0.5 * (f.x[c] + f.x[c + pl]) * (double)m.kzet.x[c]);
+        }
+        if (fused && p.mean_grad_p) {
+            ox += (double)((M)p.mgp[1] * (M)m.icsi.y[c]);
+            oy += (double)((M)p.mgp[2] * (M)m.jeta.z[c]);
+            oz += (double)((M)p.mgp[0] * (M)m.kzet.x[c]);
+        }
+        R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
+        return;
+    }
+    const R3<M> fpc = FP(k, j, i);
     { R3<M> fb = i < g.mx - 2 ? FP(k, j, i + 1) : (g.pi ? FP(k, j, 1) : fpc);
       R3<M> a = MT(m.csi, c), b = MT(m.csi, c + 1);
       v1 = a.x * fpc.x + a.y * fpc.y + a.z * fpc.z; v2 = b.x * fb.x + b.y * fb.y + b.z * fb.z;
@@ -1110,40 +1209,48 @@ void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g
 // FormU pass 1 (face fluxes) at the precision of the context's policy.
 // Pass 2 (k_cell_fp) follows; the flux planes are only read at the points
 // pass 1 writes, fp only at interior cells.
-template <int mode>
+template <int mode, bool AX>
 static void face_fluxes(tg_ctx *C, dim3 gr)
 {
     const Grid g = C->g;
     const auto &P = C->pol;
-    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, float, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm)));
-    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, double, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm)));
-    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, float, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm)));
-    else TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, double, mode><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm)));
+    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, float, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm)));
+    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, double, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm)));
+    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, float, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm)));
+    else TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, double, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm)));
 }
 
 static void form_u_faces(tg_ctx *C, int mode)
 {
     const Grid g = C->g;
     refresh_met32(C);
-    const dim3 gr = gf(g);
+    const dim3 gr = gi(g);     // one thread per interior cell (k_face_fluxes)
     const auto &P = C->pol;
-    if (mode == 1) face_fluxes<1>(C, gr);
-    else if (mode == 2) face_fluxes<2>(C, gr);
-    else face_fluxes<0>(C, gr);
+    const bool ax = C->axis_aligned;
+    if (mode == 1) { if (ax) face_fluxes<1, true>(C, gr); else face_fluxes<1, false>(C, gr); }
+    else if (mode == 2) { if (ax) face_fluxes<2, true>(C, gr); else face_fluxes<2, false>(C, gr); }
+    else { if (ax) face_fluxes<0, true>(C, gr); else face_fluxes<0, false>(C, gr); }
     if (P.flux32) TG_PROF(C, "formu_cell_fp", k_cell_fp<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fw32));
     else TG_PROF(C, "formu_cell_fp", k_cell_fp<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fw64));
+}
+
+template <bool fused, bool AX>
+static void rhs_faces_t(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
+{
+    const Grid g = C->g;
+    const dim3 gr = gi(g);
+    const auto &P = C->pol;
+    if (P.rhs32 && P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, rhs, scale, C->prm, ab2));
+    else if (P.rhs32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, rhs, scale, C->prm, ab2));
+    else if (P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, rhs, scale, C->prm, ab2));
+    else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2));
 }
 
 template <bool fused>
 static void rhs_faces(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
 {
-    const Grid g = C->g;
-    const dim3 gr = gi(g);
-    const auto &P = C->pol;
-    if (P.rhs32 && P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, float, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, rhs, scale, C->prm, ab2));
-    else if (P.rhs32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, double, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, rhs, scale, C->prm, ab2));
-    else if (P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, float, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, rhs, scale, C->prm, ab2));
-    else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2));
+    if (C->axis_aligned) rhs_faces_t<fused, true>(C, rhs, scale, ab2);
+    else rhs_faces_t<fused, false>(C, rhs, scale, ab2);
 }
 
 void form_u(tg_ctx *C, V3f<double> rhs, double scale, int mode)
