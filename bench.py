@@ -35,10 +35,30 @@ DIV_TOL = 5e-9
 # algorithmic bytes per interior cell of one launch, by storage precision of
 # the arrays the kernel reads (each array counted once per read and once per
 # write; metrics re-read every launch). The mixed mode reads FP32 copies of the
-# metrics (4 B) and keeps the state, fluxes and Krylov vectors in FP64.
-def bytes_per_cell(kernel, precision):
+# metrics (4 B) and keeps the state, fluxes and Krylov vectors in FP64. On an
+# axis-aligned mesh (tg_mesh_info) the stencil kernels read one component of
+# each metric vector.
+def bytes_per_cell(kernel, precision, axis=False):
     m = 4 if precision == "mixed" else 8      # metric storage
     g = 4 if precision == "mixed" else 8      # multigrid storage
+    if axis:
+        table = {
+            # ucat 3, ucont 3, nut 1; per face the normal metric component of
+            # csi, eta, zet and aj (12) -> fluxes 9
+            "formu_face_fluxes": 7 * 8 + 12 * m + 9 * 8,
+            # fp 3, dP 3 -> rhs 3; csi.y, eta.z, zet.x, face aj 3, icsi.y, jeta.z, kzet.x
+            "formu_rhs_faces": 9 * 8 + 9 * m,
+            # ucont 3 -> ucat 3; csi.y, eta.z, zet.x
+            "contra_to_cart": 6 * 8 + 3 * m,
+            # ucat 3 -> nut 1; csi.y, eta.z, zet.x, aj
+            "smagorinsky": 4 * 8 + 4 * m,
+            # p 1 -> dP 3; icsi.y, jeta.z, kzet.x and the face aj 3
+            "grad_p": 4 * 8 + 6 * m,
+            # phi 1, ucont 3 -> ucont 3; icsi.y, jeta.z, kzet.x and the face aj 3
+            "project": 7 * 8 + 6 * m,
+        }
+        if kernel in table:
+            return table[kernel]
     table = {
         # ucat 3, ucont 3, nut 1 (FP64); face metrics 27 + face aj 3; -> fluxes 9 (FP64)
         "formu_face_fluxes": 7 * 8 + 30 * m + 9 * 8,
@@ -350,23 +370,23 @@ def kernel_table(L, h):
     return kernels
 
 
-def roofline_of(kernels, precision, cells):
+def roofline_of(kernels, precision, cells, axis=False):
     """Roofline of the dominant kernel with a known byte count: algorithmic
     bytes per launch / average launch time (library events on its stream)."""
     ranked = sorted(kernels.items(), key=lambda kv: -kv[1]["ms"])
-    dom = next((k for k, v in ranked if bytes_per_cell(k, precision) is not None), None)
+    dom = next((k for k, v in ranked if bytes_per_cell(k, precision, axis) is not None), None)
     if dom is None:
         return None
     peak, peak_src = load_peaks()
     kv = kernels[dom]
     per_launch_ms = kv["ms"] / kv["launches"]
-    algo_bytes = bytes_per_cell(dom, precision) * cells
+    algo_bytes = bytes_per_cell(dom, precision, axis) * cells
     achieved = algo_bytes / (per_launch_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            tj = json.load(f).get(precision, {})
+            tj = json.load(f).get(precision + ("_axis" if axis else ""), {})
         if dom in tj:
             traffic = tj[dom] * cells
     return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
@@ -445,6 +465,7 @@ def main():
         cfg.device = dev
         solver = tosca_b200.gpu_solver(cfg)
         cases.setup(solver, nodes, ucat, p, T)
+        axis = solver.mesh_info()[1]
         if turbines:
             solver.set_turbines(turbines, 1.225)
         if args.warmup > 0:
@@ -470,7 +491,7 @@ def main():
         return {"cfg": cfg, "desc": desc, "solver": solver, "st": st, "t_dev": t_dev, "clocks": clk.summary(),
                 "replayed": replayed, "momentum": mom,
                 "value": cfg.cells * args.steps * world / t_dev / 1e6, "kernels": kernels,
-                "roofline": roofline_of(kernels, precision, cfg.cells)}
+                "roofline": roofline_of(kernels, precision, cfg.cells, axis), "axis_aligned": axis}
 
     arms = {}
     order = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
@@ -548,6 +569,7 @@ def main():
             "config": {"workload": head["desc"], "cells": cells, "dmda_extent": [mx, my, mz],
                        "precision": head_prec, "divergence_bound": DIV_TOL,
                        "l2": "every field exceeds the 126 MB L2; no flush",
+                       "mesh_axis_aligned": head["axis_aligned"],
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "poisson_iterations_per_step": st.poisson_total_iterations / max(1, args.steps),
                        "max_divergence": st.max_divergence,

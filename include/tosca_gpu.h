@@ -247,6 +247,12 @@ tg_status tg_graph_info(tg_ctx *ctx, int64_t *replays, int32_t *capture_failed);
  * summed); residual = the last Krylov residual estimate (KSPGetResidualNorm,
  * ueqn_solvers.c:1560-1561). Zeros after an explicit step. */
 tg_status tg_momentum_info(tg_ctx *ctx, int32_t *outer, int32_t *inner, double *residual);
+/* How the kernels classified the mesh set by tg_set_mesh_nodes: orthogonal
+ * (every cross term of the face metric tensor is zero: 7-point pressure
+ * operator, conjugate gradients) and axis-aligned (csi || y, eta || z,
+ * zet || x up to round-off: the stencil kernels read one component of each
+ * metric vector). */
+tg_status tg_mesh_info(tg_ctx *ctx, int32_t *orthogonal, int32_t *axis_aligned);
 
 /* --------------------------------------------------------------- wind farm -- */
 /* Uniform actuator-disk turbines: TOSCA's "uniformADM" with sampleType

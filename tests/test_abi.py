@@ -22,8 +22,8 @@ def declared_symbols():
 # exported by the CPU restatement
 NO_CONTEXT = {"tg_continuity_error_noalloc"}
 # checkpointed adjoint drivers (device snapshots: the CPU restatement has the
-# per-step adjoint only) and the CUDA-graph replay switch
-GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse", "tg_set_graphs", "tg_graph_info"}
+# per-step adjoint only), the CUDA-graph replay switch and the mesh classification
+GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse", "tg_set_graphs", "tg_graph_info", "tg_mesh_info"}
 
 
 def test_header_matches_bindings():

@@ -222,6 +222,7 @@ _ADJ_SIGS = {
     "adjoint_reverse": (C.c_int, [C.c_void_p, C.POINTER(TgAdjointStats)]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
     "graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "mesh_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
 }
 
 ENTRY_POINTS = tuple(_SIGS) + tuple(_ADJ_SIGS)
@@ -452,6 +453,12 @@ class Solver:
         n, f = C.c_int64(), C.c_int32()
         self._check(self.fns["graph_info"](self.h, C.byref(n), C.byref(f)), "graph_info")
         return n.value, bool(f.value)
+
+    def mesh_info(self) -> tuple:
+        """(orthogonal, axis_aligned): the CUDA library's classification of the mesh."""
+        a, b = C.c_int32(), C.c_int32()
+        self._check(self.fns["mesh_info"](self.h, C.byref(a), C.byref(b)), "mesh_info")
+        return bool(a.value), bool(b.value)
 
     def momentum_info(self) -> tuple:
         """(Newton steps or IMEX stages, Krylov operator products, last Krylov

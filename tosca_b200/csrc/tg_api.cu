@@ -605,6 +605,17 @@ tg_status tg_graph_info(tg_ctx *C, int64_t *replays, int32_t *capture_failed)
     });
 }
 
+tg_status tg_mesh_info(tg_ctx *C, int32_t *orthogonal, int32_t *axis_aligned)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!orthogonal || !axis_aligned) return fail(C, TG_ERR_BAD_ARG, "null output");
+        if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
+        *orthogonal = C->orthogonal ? 1 : 0;
+        *axis_aligned = C->axis_aligned ? 1 : 0;
+        return TG_OK;
+    });
+}
+
 tg_status tg_momentum_info(tg_ctx *C, int32_t *outer, int32_t *inner, double *residual)
 {
     return guarded(C, [&]() -> tg_status {

@@ -27,9 +27,22 @@ __device__ __forceinline__ R3<To> cvta(R3<From> a) { return R3<To>{(To)a.x, (To)
 // mode), A the arithmetic type; Ucont and Ucat stay FP64.
 // ------------------------------------------------------------------------
 template <class A, class MS>
-__device__ __forceinline__ void contra_cell(const Grid &g, const FaceMet<MS> &m, const State &s, int c)
+__device__ __forceinline__ void contra_cell(const Grid &g, const FaceMet<MS> &m, const State &s, int c, bool ax)
 {
     using M = A;
+    if (ax) {
+        // axis-aligned mesh: [csi; eta; zet] = [0 cs 0; 0 0 et; ze 0 0], the
+        // same Cramer products without the vanishing ones
+        const M cs = (M)m.csi.y[c], et = (M)m.eta.z[c], ze = (M)m.zet.x[c];
+        const M q0 = (M)(0.5 * (s.ucont.x[c - 1] + s.ucont.x[c]));
+        const M q1 = (M)(0.5 * (s.ucont.y[c - g.mx] + s.ucont.y[c]));
+        const M q2 = (M)(0.5 * (s.ucont.z[c - g.mx * g.my] + s.ucont.z[c]));
+        const M det = cs * (et * ze);
+        s.ucat.x[c] = (double)((q2 * (cs * et)) / det);
+        s.ucat.y[c] = (double)((q0 * (et * ze)) / det);
+        s.ucat.z[c] = (double)((q1 * (cs * ze)) / det);
+        return;
+    }
     R3<M> sc = cvta<M>(ld3(m.csi, c)), e = cvta<M>(ld3(m.eta, c)), z = cvta<M>(ld3(m.zet, c));
     M m00 = sc.x, m01 = sc.y, m02 = sc.z, m10 = e.x, m11 = e.y, m12 = e.z, m20 = z.x, m21 = z.y, m22 = z.z;
     M q0 = (M)(0.5 * (s.ucont.x[c - 1] + s.ucont.x[c]));
@@ -43,17 +56,17 @@ __device__ __forceinline__ void contra_cell(const Grid &g, const FaceMet<MS> &m,
 }
 
 template <class A, class MS>
-__global__ void k_contra_to_cart(Grid g, FaceMet<MS> m, State s)
+__global__ void k_contra_to_cart(Grid g, FaceMet<MS> m, State s, bool ax)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
-    contra_cell<A>(g, m, s, g.lin(k, j, i));
+    contra_cell<A>(g, m, s, g.lin(k, j, i), ax);
 }
 
 // the same on the interior cells next to the boundary only: the cells whose
 // Cartesian velocity reaches the ghost cells through the periodic copies.
 // blockIdx.z selects the boundary plane.
-__global__ void k_contra_to_cart_shell(Grid g, FaceMet<double> m, State s)
+__global__ void k_contra_to_cart_shell(Grid g, FaceMet<double> m, State s, bool ax)
 {
     int patch = blockIdx.z;
     int dir = patch >> 1, right = patch & 1;
@@ -64,7 +77,7 @@ __global__ void k_contra_to_cart_shell(Grid g, FaceMet<double> m, State s)
     if (dir == 0) { k = b; j = a; i = right ? g.mx - 2 : 1; }
     else if (dir == 1) { k = b; i = a; j = right ? g.my - 2 : 1; }
     else { j = b; i = a; k = right ? g.mz - 2 : 1; }
-    contra_cell<double>(g, m, s, g.lin(k, j, i));
+    contra_cell<double>(g, m, s, g.lin(k, j, i), ax);
 }
 
 // FP32 copies of the stencil metrics
@@ -262,7 +275,7 @@ __global__ void k_scalar_ghosts(Grid g, double *v, int dir)
 // Compute_du_dxyz (inline.h:3635-3663). Interior cells.
 // ------------------------------------------------------------------------
 template <class M>
-__global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p)
+__global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p, bool ax)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -282,15 +295,23 @@ __global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p)
     else                        dz = 0.5 * (U(k + 1, j, i) - U(k - 1, j, i));
     const R3<M> a = cvta<M>(dc), b = cvta<M>(de), d = cvta<M>(dz);
     const M h = M(0.5);
-    M du_dx = (a.x * sc.x + b.x * e.x + d.x * z.x) * ajc;
-    M du_dy = (a.x * sc.y + b.x * e.y + d.x * z.y) * ajc;
-    M du_dz = (a.x * sc.z + b.x * e.z + d.x * z.z) * ajc;
-    M dv_dx = (a.y * sc.x + b.y * e.x + d.y * z.x) * ajc;
-    M dv_dy = (a.y * sc.y + b.y * e.y + d.y * z.y) * ajc;
-    M dv_dz = (a.y * sc.z + b.y * e.z + d.y * z.z) * ajc;
-    M dw_dx = (a.z * sc.x + b.z * e.x + d.z * z.x) * ajc;
-    M dw_dy = (a.z * sc.y + b.z * e.y + d.z * z.y) * ajc;
-    M dw_dz = (a.z * sc.z + b.z * e.z + d.z * z.z) * ajc;
+    M du_dx, du_dy, du_dz, dv_dx, dv_dy, dv_dz, dw_dx, dw_dy, dw_dz;
+    if (ax) {
+        // axis-aligned mesh: csi = (0, cs, 0), eta = (0, 0, et), zet = (ze, 0, 0)
+        du_dx = (d.x * z.x) * ajc; du_dy = (a.x * sc.y) * ajc; du_dz = (b.x * e.z) * ajc;
+        dv_dx = (d.y * z.x) * ajc; dv_dy = (a.y * sc.y) * ajc; dv_dz = (b.y * e.z) * ajc;
+        dw_dx = (d.z * z.x) * ajc; dw_dy = (a.z * sc.y) * ajc; dw_dz = (b.z * e.z) * ajc;
+    } else {
+        du_dx = (a.x * sc.x + b.x * e.x + d.x * z.x) * ajc;
+        du_dy = (a.x * sc.y + b.x * e.y + d.x * z.y) * ajc;
+        du_dz = (a.x * sc.z + b.x * e.z + d.x * z.z) * ajc;
+        dv_dx = (a.y * sc.x + b.y * e.x + d.y * z.x) * ajc;
+        dv_dy = (a.y * sc.y + b.y * e.y + d.y * z.y) * ajc;
+        dv_dz = (a.y * sc.z + b.y * e.z + d.y * z.z) * ajc;
+        dw_dx = (a.z * sc.x + b.z * e.x + d.z * z.x) * ajc;
+        dw_dy = (a.z * sc.y + b.z * e.y + d.z * z.y) * ajc;
+        dw_dz = (a.z * sc.z + b.z * e.z + d.z * z.z) * ajc;
+    }
     M S00 = h * (du_dx + du_dx), S01 = h * (du_dy + dv_dx), S02 = h * (du_dz + dw_dx);
     M S10 = h * (dv_dx + du_dy), S11 = h * (dv_dy + dv_dy), S12 = h * (dv_dz + dw_dy);
     M S20 = h * (dw_dx + du_dz), S21 = h * (dw_dy + dv_dz), S22 = h * (dw_dz + dw_dz);
@@ -431,13 +452,26 @@ __global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double
 // one-sided cross derivatives only at the corner faces. Interior cells.
 // ------------------------------------------------------------------------
 template <class M>
-__global__ void k_grad_p(Grid g, FaceMet<M> m, State s)
+__global__ void k_grad_p(Grid g, FaceMet<M> m, State s, bool ax)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
     auto P = [&](int kk, int jj, int ii) { return s.p[g.id(kk, jj, ii)]; };
     const int mx = g.mx, my = g.my, mz = g.mz;
+    if (ax) {
+        // axis-aligned mesh: the cross terms g12, g13, g21, g23, g31, g32 vanish
+        const M ic = m.icsi.y[c], je = m.jeta.z[c], kz = m.kzet.x[c];
+        const double dpdc = (i == mx - 2 && g.pi) ? P(k, j, mx + 1) - P(k, j, i) : P(k, j, i + 1) - P(k, j, i);
+        const double dpde = (j == my - 2 && g.pj) ? P(k, my + 1, i) - P(k, j, i) : P(k, j + 1, i) - P(k, j, i);
+        const double dpdz = (k == mz - 2 && g.pk) ? P(mz + 1, j, i) - P(k, j, i) : P(k + 1, j, i) - P(k, j, i);
+        M ox = ((M)dpdc * (ic * ic)) * m.iaj[c], oy = ((M)dpde * (je * je)) * m.jaj[c], oz = ((M)dpdz * (kz * kz)) * m.kaj[c];
+        if (!g.pi && i == mx - 2) ox = 0;
+        if (!g.pj && j == my - 2) oy = 0;
+        if (!g.pk && k == mz - 2) oz = 0;
+        s.dp.x[c] = (double)ox; s.dp.y[c] = (double)oy; s.dp.z[c] = (double)oz;
+        return;
+    }
     R3<M> ic = ld3(m.icsi, c), ie = ld3(m.ieta, c), iz = ld3(m.izet, c);
     R3<M> jc = ld3(m.jcsi, c), je = ld3(m.jeta, c), jz = ld3(m.jzet, c);
     R3<M> kc = ld3(m.kcsi, c), ke = ld3(m.keta, c), kz = ld3(m.kzet, c);
@@ -900,13 +934,29 @@ __global__ void k_fe_update(int64_t n, V3f<double> y, double dt, V3f<double> x, 
 // metric tensor; faces 0 and m-2 skipped unless periodic.
 // ------------------------------------------------------------------------
 template <class M>
-__global__ void k_project(Grid g, FaceMet<M> m, State s, double dt)
+__global__ void k_project(Grid g, FaceMet<M> m, State s, double dt, bool ax)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     const int mx = g.mx, my = g.my, mz = g.mz;
     int f = g.lin(k, j, i);
     auto F = [&](int kk, int jj, int ii) { return s.phi[g.id(kk, jj, ii)]; };
+    if (ax) {
+        // axis-aligned mesh: only the normal derivative of phi has a metric weight
+        if (j > 0 && k > 0 && ((i > 0 && i < mx - 2) || g.pi)) {
+            const double c1 = (double)m.icsi.y[f];
+            s.ucont.x[f] -= ((F(k, j, i + 1) - F(k, j, i)) * (c1 * c1) * (double)m.iaj[f]) * dt;
+        }
+        if (i > 0 && k > 0 && ((j > 0 && j < my - 2) || g.pj)) {
+            const double e2 = (double)m.jeta.z[f];
+            s.ucont.y[f] -= ((F(k, j + 1, i) - F(k, j, i)) * (e2 * e2) * (double)m.jaj[f]) * dt;
+        }
+        if (i > 0 && j > 0 && ((k > 0 && k < mz - 2) || g.pk)) {
+            const double z3 = (double)m.kzet.x[f];
+            s.ucont.z[f] -= ((F(k + 1, j, i) - F(k, j, i)) * (z3 * z3) * (double)m.kaj[f]) * dt;
+        }
+        return;
+    }
     if (j > 0 && k > 0 && ((i > 0 && i < mx - 2) || g.pi)) {
         double dpdc = F(k, j, i + 1) - F(k, j, i), dpde, dpdz;
         if (j == my - 2)      dpde = (F(k, j, i) + F(k, j, i + 1) - F(k, j - 1, i) - F(k, j - 1, i + 1)) * 0.5;
@@ -1041,7 +1091,7 @@ inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 *
 // error of p against the FP64 oracle rose to 3.3e-6 in 5 steps (ABL 16x16x12)
 void contra_to_cart(tg_ctx *C)
 {
-    TG_PROF(C, "contra_to_cart_final", k_contra_to_cart<double, double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s));
+    TG_PROF(C, "contra_to_cart_final", k_contra_to_cart<double, double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s, C->axis_aligned));
 }
 
 // contravariantToCartesian inside the momentum stages, at the precision the
@@ -1049,9 +1099,9 @@ void contra_to_cart(tg_ctx *C)
 void contra_to_cart_stage(tg_ctx *C)
 {
     const dim3 gr = gi(C->g);
-    if (C->pol.contra_a32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<float, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
-    else if (C->pol.contra_m32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
-    else TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, double><<<gr, block3(), 0, C->stream>>>(C->g, C->fm64, C->s));
+    if (C->pol.contra_a32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<float, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s, C->axis_aligned));
+    else if (C->pol.contra_m32) TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, float><<<gr, block3(), 0, C->stream>>>(C->g, C->fm32, C->s, C->axis_aligned));
+    else TG_PROF(C, "contra_to_cart", k_contra_to_cart<double, double><<<gr, block3(), 0, C->stream>>>(C->g, C->fm64, C->s, C->axis_aligned));
 }
 
 // Precision of each momentum stage in the mixed mode. Every momentum stencil
@@ -1169,8 +1219,8 @@ void update_nut(tg_ctx *C)
     const Grid g = C->g;
     TG_CUDA(cudaMemsetAsync(C->s.nut, 0, sizeof(double) * g.size(), C->stream));
     refresh_met32(C);
-    if (C->pol.smag32) TG_PROF(C, "smagorinsky", k_smagorinsky<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fm32, C->s, C->prm));
-    else TG_PROF(C, "smagorinsky", k_smagorinsky<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fm64, C->s, C->prm));
+    if (C->pol.smag32) TG_PROF(C, "smagorinsky", k_smagorinsky<float><<<gi(g), block3(), 0, C->stream>>>(g, C->fm32, C->s, C->prm, C->axis_aligned));
+    else TG_PROF(C, "smagorinsky", k_smagorinsky<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fm64, C->s, C->prm, C->axis_aligned));
     int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
     dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
     TG_PROF(C, "bc_nut", k_nut_bcs<<<grid, b2, 0, C->stream>>>(g, C->s, C->prm));
@@ -1200,8 +1250,8 @@ void grad_p(tg_ctx *C)
         C->clear_dp = false;
     }
     refresh_met32(C);
-    if (C->pol.gradp32) TG_PROF(C, "grad_p", k_grad_p<float><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm32, C->s));
-    else TG_PROF(C, "grad_p", k_grad_p<double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s));
+    if (C->pol.gradp32) TG_PROF(C, "grad_p", k_grad_p<float><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm32, C->s, C->axis_aligned));
+    else TG_PROF(C, "grad_p", k_grad_p<double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s, C->axis_aligned));
 }
 
 void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
@@ -1398,7 +1448,7 @@ static int solve_u_impl(tg_ctx *C, bool cart_tail, tg_stats *st = nullptr)
         const Grid g = C->g;
         int na = std::max(g.mx, g.my) - 2, nb = std::max(g.my, g.mz) - 2;
         dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
-        TG_PROF(C, "contra_to_cart_shell", k_contra_to_cart_shell<<<grid, b2, 0, C->stream>>>(g, C->fm64, C->s));
+        TG_PROF(C, "contra_to_cart_shell", k_contra_to_cart_shell<<<grid, b2, 0, C->stream>>>(g, C->fm64, C->s, C->axis_aligned));
     }
     reset_cell_periodic(C, C->s.ucat);
     return rc;
@@ -1415,8 +1465,8 @@ void pressure_update_and_project(tg_ctx *C)
     TG_PROF(C, "update_pressure", k_update_pressure<<<gi(g), block3(), 0, C->stream>>>(g, C->s));
     update_scalar_ghosts(C, C->s.p);
     refresh_met32(C);
-    if (C->pol.proj32) TG_PROF(C, "project", k_project<float><<<gf(g), block3(), 0, C->stream>>>(g, C->fm32, C->s, C->prm.dt));
-    else TG_PROF(C, "project", k_project<double><<<gf(g), block3(), 0, C->stream>>>(g, C->fm64, C->s, C->prm.dt));
+    if (C->pol.proj32) TG_PROF(C, "project", k_project<float><<<gf(g), block3(), 0, C->stream>>>(g, C->fm32, C->s, C->prm.dt, C->axis_aligned));
+    else TG_PROF(C, "project", k_project<double><<<gf(g), block3(), 0, C->stream>>>(g, C->fm64, C->s, C->prm.dt, C->axis_aligned));
 }
 
 int solve_p(tg_ctx *C, tg_stats *st)
