@@ -46,8 +46,10 @@ def bytes_per_cell(kernel, precision, axis=False):
             # ucat 3, ucont 3, nut 1; per face the normal metric component of
             # csi, eta, zet and aj (12) -> fluxes 9
             "formu_face_fluxes": 7 * 8 + 12 * m + 9 * 8,
-            # fp 3, dP 3 -> rhs 3; csi.y, eta.z, zet.x, face aj 3, icsi.y, jeta.z, kzet.x
-            "formu_rhs_faces": 9 * 8 + 9 * m,
+            # fp 3, dP 3, and the RK4 update applied in place (U_o, Utmp -> Utmp,
+            # U: 9, 12, 12, 6 values over the four stages); csi.y, eta.z, zet.x,
+            # face aj 3, icsi.y, jeta.z, kzet.x
+            "formu_rhs_faces": (6 + 39 / 4) * 8 + 9 * m,
             # ucont 3 -> ucat 3; csi.y, eta.z, zet.x
             "contra_to_cart": 6 * 8 + 3 * m,
             # ucat 3 -> nut 1; csi.y, eta.z, zet.x, aj
@@ -64,8 +66,9 @@ def bytes_per_cell(kernel, precision, axis=False):
         "formu_face_fluxes": 7 * 8 + 30 * m + 9 * 8,
         # fluxes 9 -> fp 3
         "formu_cell_fp": 12 * 8,
-        # fp 3, dP 3 -> rhs 3 (FP64); csi/eta/zet 9, face aj 3, icsi/jeta/kzet 9 (metrics)
-        "formu_rhs_faces": 9 * 8 + 21 * m,
+        # fp 3, dP 3 and the RK4 update in place (9.75 values per stage, FP64);
+        # csi/eta/zet 9, face aj 3, icsi/jeta/kzet 9 (metrics)
+        "formu_rhs_faces": (6 + 39 / 4) * 8 + 21 * m,
         # ucont 3 -> ucat 3 (FP64); csi/eta/zet 9
         "contra_to_cart": 6 * 8 + 9 * m,
         # ucat 3 -> nut 1 (FP64); csi/eta/zet 9, aj 1
@@ -86,8 +89,6 @@ def bytes_per_cell(kernel, precision, axis=False):
         "pois_cg_update": 48,          # x, r read/write; p, q read
         "pois_cg_dir": 24,             # z, p read; p write
         "pois_dot": 16,                # two vectors
-        # RK4 bookkeeping averaged over the four stages: 12 + 15 + 15 + 9 values
-        "rk_update": 51 * 8 / 4,
     }
     return table.get(kernel)
 

@@ -804,6 +804,25 @@ __global__ void k_cell_fp(Grid g, FluxWork<F> w)
     st3(w.fp, g.lin(k, j, i), cell_fp(g, w, k, j, i));
 }
 
+// Explicit time update of one face value u with right-hand side r (UeqnFE,
+// ueqn_solvers.c:1411-1442: U = r dt + U_o; UeqnRK4, ueqn_solvers.c:1446-1504,
+// stage st: Utmp = U_o + b_st dt r (st = 0) or Utmp + b_st dt r, U = U_o +
+// a_{st+1} dt r, after the last stage U = Utmp + b_3 dt r), in the order of
+// the reference's VecScale / VecAXPY / VecWAXPY calls.
+struct RkArgs {
+    double cb, ca;      // b_st dt (FE: dt), a_{st+1} dt
+    int first, last, fe;
+};
+__device__ __forceinline__ void rk_point(double *uc, double *ut, const double *uo, double r, const RkArgs &a)
+{
+    if (a.fe) { *uc = r * a.cb + *uo; return; }
+    if (a.last) { *uc = a.cb * r + *ut; return; }
+    const double o = *uo;
+    if (a.first) *ut = a.cb * r + o;
+    else *ut = *ut + a.cb * r;
+    *uc = a.ca * r + o;
+}
+
 // Pass 3 (ueqn_solvers.c:1008-1035): rhs_face += scale * aj_face *
 // central(S . fp) at the faces of interior cells, fp of the cell and of its
 // +i, +j, +k neighbours read from pass 2. The neighbour beyond the last
@@ -814,13 +833,32 @@ __global__ void k_cell_fp(Grid g, FluxWork<F> w)
 // Rhs = -dP (+ AB2 buoyancy) (ueqn_solvers.c:1305-1338), += turbine body
 // force (ueqn_solvers.c:1340-1344), += FormU, += sourceU (body force), +=
 // meanGradPForcing (ueqn_sources.c:3735-3822). MR:
-// metric storage type; F: face-flux storage type.
-template <class MR, class F, bool fused, bool AX>
-__global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2)
+// metric storage type; F: face-flux storage type. kind: 0 R += scale FormU;
+// 1 the ExplicitRhsU value is stored in R; 2 it is not stored but masked at
+// the non-resolved faces and applied at once by the explicit time update
+// (rk_point, one RK4 stage or the FE step).
+template <class MR, class F, int kind, bool AX>
+__global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State s, FluxWork<F> w, V3f<double> R, double scale, Params p, int ab2, RkArgs rk)
 {
+    constexpr bool fused = kind >= 1;
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
+    // the value of the three faces: stored, or masked and applied (kind 2)
+    auto finish = [&](double ox, double oy, double oz) {
+        if (kind == 2) {
+            // resetNonResolvedCellFaces (inline.h:1674-1835) on the + faces of
+            // the last interior cells of a non-periodic direction
+            if (!g.pi && i == g.mx - 2 && !(s.ucont_o.x[c] > 0)) ox = 0.0;
+            if (!g.pj && j == g.my - 2 && !(s.ucont_o.y[c] > 0)) oy = 0.0;
+            if (!g.pk && k == g.mz - 2 && !(s.ucont_o.z[c] > 0)) oz = 0.0;
+            rk_point(s.ucont.x + c, s.utmp.x + c, s.ucont_o.x + c, ox, rk);
+            rk_point(s.ucont.y + c, s.utmp.y + c, s.ucont_o.y + c, oy, rk);
+            rk_point(s.ucont.z + c, s.utmp.z + c, s.ucont_o.z + c, oz, rk);
+        } else {
+            R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
+        }
+    };
     R3<double> base;
     if (fused) {
         base = R3<double>{0.0 - s.dp.x[c], 0.0 - s.dp.y[c], 0.0 - s.dp.z[c]};
@@ -868,7 +906,7 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
             oy += (double)((M)p.mgp[2] * (M)m.jeta.z[c]);
             oz += (double)((M)p.mgp[0] * (M)m.kzet.x[c]);
         }
-        R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
+        finish(ox, oy, oz);
         return;
     }
     const R3<M> fpc = FP(k, j, i);
@@ -900,7 +938,25 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
         oy += (double)(g0 * b.x + g1 * b.y + g2 * b.z);
         oz += (double)(g0 * d.x + g1 * d.y + g2 * d.z);
     }
-    R.x[c] = ox; R.y[c] = oy; R.z[c] = oz;
+    finish(ox, oy, oz);
+}
+
+// the explicit time update of the points outside the interior cells, whose
+// right-hand side is zero (never formed, or reset at the non-resolved faces):
+// rk_point with r = 0 on the six boundary planes of the DMDA box, each point
+// once
+__global__ void k_rk_shell(Grid g, State s, RkArgs rk)
+{
+    const int patch = blockIdx.z, dir = patch >> 1, right = patch & 1;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
+    int i, j, k;
+    if (dir == 0) { if (a >= g.my || b >= g.mz) return; i = right ? g.mx - 1 : 0; j = a; k = b; }
+    else if (dir == 1) { if (a >= g.mx - 2 || b >= g.mz) return; j = right ? g.my - 1 : 0; i = a + 1; k = b; }
+    else { if (a >= g.mx - 2 || b >= g.my - 2) return; k = right ? g.mz - 1 : 0; i = a + 1; j = b + 1; }
+    const int c = g.lin(k, j, i);
+    rk_point(s.ucont.x + c, s.utmp.x + c, s.ucont_o.x + c, 0.0, rk);
+    rk_point(s.ucont.y + c, s.utmp.y + c, s.ucont_o.y + c, 0.0, rk);
+    rk_point(s.ucont.z + c, s.utmp.z + c, s.ucont_o.z + c, 0.0, rk);
 }
 
 // resetNonResolvedCellFaces (inline.h:1674-1835) on the boundary planes of one
@@ -921,13 +977,6 @@ __global__ void k_non_resolved(Grid g, State s, int dir)
     if (!per) { int q = at(m - 2); if (!(uo[q] > 0)) v[q] = 0.0; }
 }
 
-// FE: y = x*dt + z (VecScale then VecAXPY)
-__global__ void k_fe_update(int64_t n, V3f<double> y, double dt, V3f<double> x, V3f<double> z)
-{
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        y.x[q] = x.x[q] * dt + z.x[q]; y.y[q] = x.y[q] * dt + z.y[q]; y.z[q] = x.z[q] * dt + z.z[q];
-    }
-}
 
 // ------------------------------------------------------------------------
 // ProjectVelocity (peqn.c:2495-2905): V = V* - dt G(phi) with the full
@@ -1284,39 +1333,40 @@ static void form_u_faces(tg_ctx *C, int mode)
     else TG_PROF(C, "formu_cell_fp", k_cell_fp<double><<<gi(g), block3(), 0, C->stream>>>(g, C->fw64));
 }
 
-template <bool fused, bool AX>
-static void rhs_faces_t(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
+template <int fused, bool AX>
+static void rhs_faces_t(tg_ctx *C, V3f<double> rhs, double scale, int ab2, RkArgs rk)
 {
     const Grid g = C->g;
     const dim3 gr = gi(g);
     const auto &P = C->pol;
-    if (P.rhs32 && P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, rhs, scale, C->prm, ab2));
-    else if (P.rhs32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, rhs, scale, C->prm, ab2));
-    else if (P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, rhs, scale, C->prm, ab2));
-    else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2));
+    if (P.rhs32 && P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, rhs, scale, C->prm, ab2, rk));
+    else if (P.rhs32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<float, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, rhs, scale, C->prm, ab2, rk));
+    else if (P.flux32) TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, float, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, rhs, scale, C->prm, ab2, rk));
+    else TG_PROF(C, "formu_rhs_faces", k_rhs_faces<double, double, fused, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, rhs, scale, C->prm, ab2, rk));
 }
 
-template <bool fused>
-static void rhs_faces(tg_ctx *C, V3f<double> rhs, double scale, int ab2)
+template <int fused>
+static void rhs_faces(tg_ctx *C, V3f<double> rhs, double scale, int ab2, RkArgs rk = RkArgs{})
 {
-    if (C->axis_aligned) rhs_faces_t<fused, true>(C, rhs, scale, ab2);
-    else rhs_faces_t<fused, false>(C, rhs, scale, ab2);
+    if (C->axis_aligned) rhs_faces_t<fused, true>(C, rhs, scale, ab2, rk);
+    else rhs_faces_t<fused, false>(C, rhs, scale, ab2, rk);
 }
 
 void form_u(tg_ctx *C, V3f<double> rhs, double scale, int mode)
 {
     form_u_faces(C, mode);
-    rhs_faces<false>(C, rhs, scale, 0);
+    rhs_faces<0>(C, rhs, scale, 0);
 }
 
 // rhs += scale * FormU again from the cell sums the last FormU left (same
 // state and formMode)
 void form_u_again(tg_ctx *C, V3f<double> rhs, double scale)
 {
-    rhs_faces<false>(C, rhs, scale, 0);
+    rhs_faces<0>(C, rhs, scale, 0);
 }
 
-void explicit_rhs(tg_ctx *C, int mode)
+// ExplicitRhsU up to the face fluxes: resets, Cartesian velocity, FormU passes 1-2
+static void explicit_rhs_head(tg_ctx *C, int mode)
 {
     const Grid g = C->g;
     reset_no_penetration(C);
@@ -1331,10 +1381,28 @@ void explicit_rhs(tg_ctx *C, int mode)
         TG_CUDA(cudaMemsetAsync(C->s.rhs.x, 0, 3 * sizeof(double) * g.size(), C->stream));
         C->clear_rhs = false;
     }
-    rhs_faces<true>(C, C->s.rhs, 1.0, C->it > C->cfg.it_start ? 1 : 0);
+}
+
+void explicit_rhs(tg_ctx *C, int mode)
+{
+    const Grid g = C->g;
+    explicit_rhs_head(C, mode);
+    rhs_faces<1>(C, C->s.rhs, 1.0, C->it > C->cfg.it_start ? 1 : 0);
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, 0));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, 1));
     TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
+}
+
+// ExplicitRhsU followed by one explicit update (an RK4 stage or the FE step)
+// without storing Rhs: the face assembly applies the update at the faces of
+// the interior cells, k_rk_shell at every other point (zero right-hand side)
+static void explicit_rhs_update(tg_ctx *C, RkArgs rk)
+{
+    const Grid g = C->g;
+    explicit_rhs_head(C, 0);
+    rhs_faces<2>(C, C->s.rhs, 1.0, C->it > C->cfg.it_start ? 1 : 0, rk);
+    dim3 grid((std::max(g.mx, g.my) + 31) / 32, (std::max(g.my, g.mz) + 7) / 8, 6);
+    TG_PROF(C, "rk_shell", k_rk_shell<<<grid, dim3(32, 8), 0, C->stream>>>(g, C->s, rk));
 }
 
 // resetNonResolvedCellFaces (inline.h:1674-1835) on an arbitrary face vector
@@ -1388,24 +1456,6 @@ void cn_build_bu(tg_ctx *C, V3f<double> bu, bool half_rhs_o)
     k_cn_bu<<<ga(g), block3(), 0, C->stream>>>(g, C->m, C->s, C->prm, bu, C->it > C->cfg.it_start ? 1 : 0, half_rhs_o ? 1 : 0);
 }
 
-// UeqnRK4 bookkeeping after stage st (ueqn_solvers.c:1446-1504): the stage
-// sum Utmp += dt b_st Rhs (Utmp starts as Ucont_o) and the next stage's state
-// Ucont = Ucont_o + a_{st+1} dt Rhs, or after the last stage Ucont = Utmp.
-__global__ void k_rk_update(int64_t n, V3f<double> utmp, V3f<double> ucont, V3f<double> ucont_o, V3f<double> rhs,
-                            double cb, double ca, int first, int last)
-{
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        const double rx = rhs.x[q], ry = rhs.y[q], rz = rhs.z[q];
-        if (last) {
-            ucont.x[q] = cb * rx + utmp.x[q]; ucont.y[q] = cb * ry + utmp.y[q]; ucont.z[q] = cb * rz + utmp.z[q];
-            continue;
-        }
-        const double ox = ucont_o.x[q], oy = ucont_o.y[q], oz = ucont_o.z[q];
-        if (first) { utmp.x[q] = cb * rx + ox; utmp.y[q] = cb * ry + oy; utmp.z[q] = cb * rz + oz; }
-        else { utmp.x[q] = utmp.x[q] + cb * rx; utmp.y[q] = utmp.y[q] + cb * ry; utmp.z[q] = utmp.z[q] + cb * rz; }
-        ucont.x[q] = ca * rx + ox; ucont.y[q] = ca * ry + oy; ucont.z[q] = ca * rz + oz;
-    }
-}
 
 // SolveUEqn (ueqn.c:397-440). cart_tail: finish with contravariantToCartesian
 // on every interior cell as the reference does; the full step converts only
@@ -1424,17 +1474,13 @@ static int solve_u_impl(tg_ctx *C, bool cart_tail, tg_stats *st = nullptr)
         rc = solve_u_imex(C);
     } else if (C->cfg.ddt_scheme == TG_DDT_FE) {
         // UeqnFE, ueqn_solvers.c:1411-1442
-        explicit_rhs(C);
-        TG_PROF(C, "fe_update", k_fe_update<<<nblk(G), 256, 0, C->stream>>>(G, C->s.ucont, dt, C->s.rhs, C->s.ucont_o));
+        explicit_rhs_update(C, RkArgs{dt, 0.0, 0, 0, 1});
     } else {
         // UeqnRK4, ueqn_solvers.c:1446-1504
         const double b[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
         const double a[4] = {0.0, 0.5, 0.5, 1.0};
-        for (int st = 0; st < 4; st++) {
-            explicit_rhs(C);
-            TG_PROF(C, "rk_update", k_rk_update<<<nblk(G), 256, 0, C->stream>>>(G, C->s.utmp, C->s.ucont, C->s.ucont_o, C->s.rhs,
-                                                                              dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0, st == 3));
-        }
+        for (int st = 0; st < 4; st++)
+            explicit_rhs_update(C, RkArgs{dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0 ? 1 : 0, st == 3 ? 1 : 0, 0});
     }
     // SolveUEqn tail, ueqn.c:413-437
     reset_no_penetration(C);
