@@ -312,6 +312,7 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
         k_zero_last_nodes<<<grid3(g.mx, g.my, g.mz), block3(), 0, C->stream>>>(g, dn);
         TG_CUDA(cudaStreamSynchronize(C->stream));
         metrics_from_nodes(C, dn);
+        refresh_filter(C);
         C->met32_stale = true;
         // orthogonality: every cross term of the face metric tensor vanishes
         std::vector<double> h(G);

@@ -70,6 +70,7 @@ template <class T>
 struct FaceMet {
     V3f<T> csi, eta, zet, icsi, ieta, izet, jcsi, jeta, jzet, kcsi, keta, kzet;
     T *aj, *iaj, *jaj, *kaj;
+    T *flt2;      // Smagorinsky filter width squared, ((1/aj)^(1/3))^2 (les.c:2204-2514)
 };
 
 // FormU work planes at storage precision T: face fluxes per direction and
@@ -234,7 +235,8 @@ inline dim3 block3() { return dim3(BX, BY, BZ); }
 // stage entry points (tg_step.cu)
 void metrics_from_nodes(tg_ctx *C, const double *d_nodes);
 void alloc_precision_work(tg_ctx *C);         // FP64 views, FP32 copies (mixed mode)
-void refresh_met32(tg_ctx *C);                // FP32 metric copies from the FP64 fields
+void refresh_met32(tg_ctx *C);
+void refresh_filter(tg_ctx *C);          // FP64 Smagorinsky filter widths after a mesh change                // FP32 metric copies from the FP64 fields
 void contra_to_cart(tg_ctx *C);
 void reset_cell_periodic(tg_ctx *C, V3f<double> v);
 void reset_cell_periodic_s(tg_ctx *C, double *v);

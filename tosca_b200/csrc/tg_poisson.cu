@@ -76,16 +76,20 @@ __global__ void k_apply7(PoissonCtx P, const double *__restrict__ x, double *__r
 {
     int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y, kc = blockIdx.z * blockDim.z + threadIdx.z;
     if (ic >= P.nx || jc >= P.ny || kc >= P.nz) return;
-    Cg q{P.nx, P.ny, P.nz, P.pi, P.pj, P.pk};
-    int c = (kc * P.ny + jc) * P.nx + ic;
+    const int nx = P.nx, pl = P.nx * P.ny;
+    int c = (kc * P.ny + jc) * nx + ic;
     if (c == P.pin) { y[c] = x[c]; return; }
+    // neighbours by offset; a periodic seam wraps to the opposite end
+    const int e = ic < nx - 1 ? c + 1 : c + 1 - nx, w = ic > 0 ? c - 1 : c - 1 + nx;
+    const int n = jc < P.ny - 1 ? c + nx : c + nx - pl, s = jc > 0 ? c - nx : c - nx + pl;
+    const int t = kc < P.nz - 1 ? c + pl : c + pl - pl * P.nz, b = kc > 0 ? c - pl : c - pl + pl * P.nz;
     double xc = x[c], acc = 0.0;
-    if (ic < P.nx - 1 || P.pi) acc += P.gE1[c] * (xc - x[q.id(kc, jc, ic + 1)]);
-    if (ic > 0 || P.pi)        { int w = q.id(kc, jc, ic - 1); acc += P.gE1[w] * (xc - x[w]); }
-    if (jc < P.ny - 1 || P.pj) acc += P.gN2[c] * (xc - x[q.id(kc, jc + 1, ic)]);
-    if (jc > 0 || P.pj)        { int s = q.id(kc, jc - 1, ic); acc += P.gN2[s] * (xc - x[s]); }
-    if (kc < P.nz - 1 || P.pk) acc += P.gT3[c] * (xc - x[q.id(kc + 1, jc, ic)]);
-    if (kc > 0 || P.pk)        { int b = q.id(kc - 1, jc, ic); acc += P.gT3[b] * (xc - x[b]); }
+    if (ic < nx - 1 || P.pi)   acc += P.gE1[c] * (xc - x[e]);
+    if (ic > 0 || P.pi)        acc += P.gE1[w] * (xc - x[w]);
+    if (jc < P.ny - 1 || P.pj) acc += P.gN2[c] * (xc - x[n]);
+    if (jc > 0 || P.pj)        acc += P.gN2[s] * (xc - x[s]);
+    if (kc < P.nz - 1 || P.pk) acc += P.gT3[c] * (xc - x[t]);
+    if (kc > 0 || P.pk)        acc += P.gT3[b] * (xc - x[b]);
     y[c] = acc;
 }
 

@@ -280,7 +280,8 @@ __global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p, bool ax)
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
-    auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.id(kk, jj, ii)); };
+    // the +-1 neighbours of an interior cell lie inside the DMDA: no wrap
+    auto U = [&](int kk, int jj, int ii) { return ld3(s.ucat, g.lin(kk, jj, ii)); };
     M ajc = m.aj[c];
     R3<M> sc = ld3(m.csi, c), e = ld3(m.eta, c), z = ld3(m.zet, c);
     R3<double> dc, de, dz;
@@ -316,8 +317,8 @@ __global__ void k_smagorinsky(Grid g, FaceMet<M> m, State s, Params p, bool ax)
     M S10 = h * (dv_dx + du_dy), S11 = h * (dv_dy + dv_dy), S12 = h * (dv_dz + dw_dy);
     M S20 = h * (dw_dx + du_dz), S21 = h * (dw_dy + dv_dz), S22 = h * (dw_dz + dw_dz);
     M Sabs = sqrt(M(2) * (S00 * S00 + S01 * S01 + S02 * S02 + S10 * S10 + S11 * S11 + S12 * S12 + S20 * S20 + S21 * S21 + S22 * S22));
-    M filter = pow(M(1) / ajc, M(1) / M(3));
-    s.nut[c] = (double)((M)p.cs * pow(filter, M(2)) * Sabs);
+    // filter width squared pow(pow(1/aj, 1/3), 2), evaluated once per mesh (k_filter2)
+    s.nut[c] = (double)((M)p.cs * m.flt2[c] * Sabs);
 }
 
 // UpdateNutBCs (boundary.c:2630-2930): face-adjacent ghosts of nut
@@ -461,10 +462,13 @@ __global__ void k_grad_p(Grid g, FaceMet<M> m, State s, bool ax)
     const int mx = g.mx, my = g.my, mz = g.mz;
     if (ax) {
         // axis-aligned mesh: the cross terms g12, g13, g21, g23, g31, g32 vanish
+        // the + neighbours lie inside the DMDA except across a periodic seam,
+        // where index m + 1 wraps to 1
         const M ic = m.icsi.y[c], je = m.jeta.z[c], kz = m.kzet.x[c];
-        const double dpdc = (i == mx - 2 && g.pi) ? P(k, j, mx + 1) - P(k, j, i) : P(k, j, i + 1) - P(k, j, i);
-        const double dpde = (j == my - 2 && g.pj) ? P(k, my + 1, i) - P(k, j, i) : P(k, j + 1, i) - P(k, j, i);
-        const double dpdz = (k == mz - 2 && g.pk) ? P(mz + 1, j, i) - P(k, j, i) : P(k + 1, j, i) - P(k, j, i);
+        const double pc = s.p[c];
+        const double dpdc = ((i == mx - 2 && g.pi) ? s.p[g.lin(k, j, 1)] : s.p[c + 1]) - pc;
+        const double dpde = ((j == my - 2 && g.pj) ? s.p[g.lin(k, 1, i)] : s.p[c + mx]) - pc;
+        const double dpdz = ((k == mz - 2 && g.pk) ? s.p[g.lin(1, j, i)] : s.p[c + mx * my]) - pc;
         M ox = ((M)dpdc * (ic * ic)) * m.iaj[c], oy = ((M)dpde * (je * je)) * m.jaj[c], oz = ((M)dpdz * (kz * kz)) * m.kaj[c];
         if (!g.pi && i == mx - 2) ox = 0;
         if (!g.pj && j == my - 2) oy = 0;
@@ -1178,12 +1182,29 @@ static void set_policy(tg_ctx *C)
     C->pol.proj32 = false;
 }
 
+// Smagorinsky filter width squared of every cell from its Jacobian, in the
+// arithmetic of the eddy-viscosity kernel (les.c:2204-2514)
+template <class T>
+__global__ void k_filter2(int64_t n, const T *aj, T *out)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const T filter = pow(T(1) / aj[q], T(1) / T(3));
+        out[q] = pow(filter, T(2));
+    }
+}
+
+void refresh_filter(tg_ctx *C)
+{
+    const int64_t G = C->g.size();
+    k_filter2<double><<<nblk(G), 256, 0, C->stream>>>(G, C->fm64.aj, C->fm64.flt2);
+}
+
 void alloc_precision_work(tg_ctx *C)
 {
     const size_t G = (size_t)C->g.size();
     const Metrics &m = C->m;
     C->fm64 = FaceMet<double>{m.csi, m.eta, m.zet, m.icsi, m.ieta, m.izet, m.jcsi, m.jeta, m.jzet,
-                              m.kcsi, m.keta, m.kzet, m.aj, m.iaj, m.jaj, m.kaj};
+                              m.kcsi, m.keta, m.kzet, m.aj, m.iaj, m.jaj, m.kaj, dallocd(C, G)};
     set_policy(C);
     if (!C->pol.flux32) C->fw64 = FluxWork<double>{dalloc3(C, G), dalloc3(C, G), dalloc3(C, G), dalloc3(C, G)};
     if (!C->mixed) return;
@@ -1194,7 +1215,7 @@ void alloc_precision_work(tg_ctx *C)
     FaceMet<float> &f = C->fm32;
     V3f<float> *vv[] = {&f.csi, &f.eta, &f.zet, &f.icsi, &f.ieta, &f.izet, &f.jcsi, &f.jeta, &f.jzet, &f.kcsi, &f.keta, &f.kzet};
     for (auto *v : vv) *v = f3();
-    float **ss[] = {&f.aj, &f.iaj, &f.jaj, &f.kaj};
+    float **ss[] = {&f.aj, &f.iaj, &f.jaj, &f.kaj, &f.flt2};
     for (auto **v : ss) *v = (float *)dalloc(C, G * sizeof(float));
     if (C->pol.flux32) C->fw32 = FluxWork<float>{f3(), f3(), f3(), f3()};
     C->met32_stale = true;
@@ -1216,6 +1237,7 @@ void refresh_met32(tg_ctx *C)
     const double *sa[] = {a.aj, a.iaj, a.jaj, a.kaj};
     float *sb[] = {b.aj, b.iaj, b.jaj, b.kaj};
     for (int q = 0; q < 4; q++) k_to_f32<<<nblk(G), 256, 0, C->stream>>>(G, sa[q], sb[q]);
+    k_filter2<float><<<nblk(G), 256, 0, C->stream>>>(G, b.aj, b.flt2);
     TG_CUDA(cudaGetLastError());
     C->met32_stale = false;
 }
