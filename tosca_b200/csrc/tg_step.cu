@@ -620,17 +620,18 @@ __device__ __forceinline__ R3<M> visc_flux_ax(M cs, M et, M ze, int dir, R3<M> d
 // 0 convection + viscosity, 1 convection only, 2 viscosity (with the wall
 // stress) only; the skipped part of each face flux is zero. AX: the mesh is
 // axis-aligned (visc_flux_ax reads 3 of the 9 face metric components).
-constexpr int FTX = BX + 3, FTY = BY + 3, FTZ = BZ + 3, FTN = FTX * FTY * FTZ;
+constexpr int FBX = 32, FBY = 4, FBZ = 2, FBN = FBX * FBY * FBZ, FMINB = 4;   // block of k_face_fluxes
+constexpr int FTX = FBX + 3, FTY = FBY + 3, FTZ = FBZ + 3, FTN = FTX * FTY * FTZ;
 
 template <class M, class F, int mode, bool AX>
-__global__ void __launch_bounds__(256, 4) k_face_fluxes(Grid g, FaceMet<M> m, State s, FluxWork<F> w, Params p)
+__global__ void __launch_bounds__(FBN, FMINB) k_face_fluxes(Grid g, FaceMet<M> m, State s, FluxWork<F> w, Params p)
 {
     __shared__ double su[3][FTN];
     __shared__ double sn[FTN];
     const int mx = g.mx, my = g.my, mz = g.mz;
-    const int i0 = 1 + blockIdx.x * BX, j0 = 1 + blockIdx.y * BY, k0 = 1 + blockIdx.z * BZ;
+    const int i0 = 1 + blockIdx.x * FBX, j0 = 1 + blockIdx.y * FBY, k0 = 1 + blockIdx.z * FBZ;
     const bool les = p.les;
-    for (int q = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x; q < FTN; q += BX * BY * BZ) {
+    for (int q = (threadIdx.z * FBY + threadIdx.y) * FBX + threadIdx.x; q < FTN; q += FBN) {
         const int tx = q % FTX, ty = (q / FTX) % FTY, tz = q / (FTX * FTY);
         const int gi = g.wi(i0 - 1 + tx), gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz);
         double ux = 0.0, uy = 0.0, uz = 0.0, nt = 0.0;
@@ -1335,17 +1336,18 @@ static void face_fluxes(tg_ctx *C, dim3 gr)
 {
     const Grid g = C->g;
     const auto &P = C->pol;
-    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, float, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm)));
-    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, double, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm)));
-    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, float, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm)));
-    else TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, double, mode, AX><<<gr, block3(), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm)));
+    if (P.visc32 && P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, float, mode, AX><<<gr, dim3(FBX, FBY, FBZ), 0, C->stream>>>(g, C->fm32, C->s, C->fw32, C->prm)));
+    else if (P.visc32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<float, double, mode, AX><<<gr, dim3(FBX, FBY, FBZ), 0, C->stream>>>(g, C->fm32, C->s, C->fw64, C->prm)));
+    else if (P.flux32) TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, float, mode, AX><<<gr, dim3(FBX, FBY, FBZ), 0, C->stream>>>(g, C->fm64, C->s, C->fw32, C->prm)));
+    else TG_PROF(C, "formu_face_fluxes", (k_face_fluxes<double, double, mode, AX><<<gr, dim3(FBX, FBY, FBZ), 0, C->stream>>>(g, C->fm64, C->s, C->fw64, C->prm)));
 }
 
 static void form_u_faces(tg_ctx *C, int mode)
 {
     const Grid g = C->g;
     refresh_met32(C);
-    const dim3 gr = gi(g);     // one thread per interior cell (k_face_fluxes)
+    // one thread per interior cell (k_face_fluxes)
+    const dim3 gr((g.mx - 2 + FBX - 1) / FBX, (g.my - 2 + FBY - 1) / FBY, (g.mz - 2 + FBZ - 1) / FBZ);
     const auto &P = C->pol;
     const bool ax = C->axis_aligned;
     if (mode == 1) { if (ax) face_fluxes<1, true>(C, gr); else face_fluxes<1, false>(C, gr); }
