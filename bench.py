@@ -538,9 +538,10 @@ def main():
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     barrier()
-    bytes_state = h_ucont.nbytes + h_ucat.nbytes + h_p.nbytes + (h_nut.nbytes if cfg.les else 0)
+    bytes_in = h_ucont.nbytes + h_ucat.nbytes + h_p.nbytes          # nut is output only
+    bytes_out = bytes_in + (h_nut.nbytes if cfg.les else 0)
     e2e = {"value": cells * e2e_steps * world / t_e2e / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": int(bytes_state), "d2h_bytes_per_step": int(bytes_state),
+           "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(bytes_out),
            "steps": e2e_steps, "precision": head_prec, "max_divergence": se.max_divergence}
 
     adj = None

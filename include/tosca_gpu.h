@@ -332,10 +332,12 @@ tg_status tg_adjoint_forward(tg_ctx *ctx, int32_t nsteps, int32_t nsnap, tg_stat
  * to the initial state. */
 tg_status tg_adjoint_reverse(tg_ctx *ctx, tg_adjoint_stats *stats);
 
-/* One drop-in step with host state: Ucont, Ucat, P (and nut when LES is on) are
- * uploaded from the caller's arrays, one step runs, and the same arrays are
- * overwritten with the new state. This is the call a host time loop makes when
- * the state lives in its own (PETSc) vectors. */
+/* One drop-in step with host state: Ucont, Ucat and P are uploaded from the
+ * caller's arrays, one step runs, and the same arrays are overwritten with the
+ * new state; nut (LES on) is only written, since the step recomputes it from
+ * Ucat before any use (UpdateNut at the start of the step, main.c:54-99). This
+ * is the call a host time loop makes when the state lives in its own (PETSc)
+ * vectors. */
 tg_status tg_step_host(tg_ctx *ctx, double *ucont, double *ucat, double *p,
                        double *nut, int32_t halo, tg_stats *stats);
 

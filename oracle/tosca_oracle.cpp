@@ -1923,7 +1923,7 @@ tg_status tor_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, doubl
         copyIn<3>(*C, (double *)C->ucont.data(), ucont, halo);
         copyIn<3>(*C, (double *)C->ucat.data(), ucat, halo);
         copyIn<1>(*C, C->p.data(), p, halo);
-        if (nut && C->c.les) copyIn<1>(*C, C->nut.data(), nut, halo);
+        // nut is recomputed from Ucat before any read (updateNut): output only
         tg_status s = tor_step(C, 1, st);
         copyOut<3>(*C, ucont, (const double *)C->ucont.data(), halo);
         copyOut<3>(*C, ucat, (const double *)C->ucat.data(), halo);

@@ -636,7 +636,7 @@ tg_status tg_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double
         upload(C, ucont, halo, C->s.ucont.x, C->s.ucont.y, C->s.ucont.z);
         upload(C, ucat, halo, C->s.ucat.x, C->s.ucat.y, C->s.ucat.z);
         upload(C, p, halo, C->s.p, nullptr, nullptr);
-        if (nut && C->prm.les) upload(C, nut, halo, C->s.nut, nullptr, nullptr);
+        // nut is recomputed from Ucat before any read: output only
         tg_stats local{};
         tg_stats *s = st ? st : &local;
         *s = tg_stats{};
