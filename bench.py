@@ -332,7 +332,7 @@ def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     fwd_ms = solver.step(fwd_steps).seconds / fwd_steps * 1e3
     free, _ = torch.cuda.mem_get_info()
     G = cfg.mx * cfg.my * cfg.mz
-    snap = 8 * (7 * G + 2 * cfg.cells)               # Ucont, Ucat, P and the last two Poisson solutions
+    snap = 8 * (7 * G + 3 * cfg.cells)               # Ucont, Ucat, P and the last three Poisson solutions
     work = 8 * (49 + 31) * G                       # adjoint work arrays and the work tape
     nsnap = int(max(2, min(steps, 0.5 * (free - work) // snap)))
     solver.set_farm_objective(True)

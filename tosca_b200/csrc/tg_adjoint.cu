@@ -45,7 +45,8 @@ namespace tg {
 
 struct Snapshot {
     V3f<double> ucont, ucat, btheta, btheta_o;
-    double *p, *px, *pxp;        // P, the last two Poisson solutions (initial guess of the next solve)
+    double *p, *px, *pxp, *pxp2; // P, the last three Poisson solutions (initial guess of the next solve)
+    double phist = 0.0;          // solutions in that history (device slot SC_PHIST)
     int it;
     int pos;       // step index of the state held (-1: free)
 };
@@ -1078,9 +1079,12 @@ static Snapshot make_snapshot(tg_ctx *C)
     s.p = dallocd(C, (size_t)C->g.size());
     s.px = dallocd(C, (size_t)poisson_n(C));
     s.pxp = dallocd(C, (size_t)poisson_n(C));
+    s.pxp2 = dallocd(C, (size_t)poisson_n(C));
     s.pos = -1;
     return s;
 }
+__global__ void k_set_phist(double *a, double v) { a[0] = v; }
+
 static void save_state(tg_ctx *C, Snapshot &s, int pos)
 {
     copy3(C, s.ucont, C->s.ucont); copy3(C, s.ucat, C->s.ucat);
@@ -1088,6 +1092,9 @@ static void save_state(tg_ctx *C, Snapshot &s, int pos)
     TG_CUDA(cudaMemcpyAsync(s.p, C->s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(s.px, poisson_x(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(s.pxp, poisson_xprev(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(s.pxp2, poisson_xprev2(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(&s.phist, C->d_scal + SC_PHIST, sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    TG_CUDA(cudaStreamSynchronize(C->stream));
     s.it = C->it;
     s.pos = pos;
 }
@@ -1098,6 +1105,8 @@ static void restore_state(tg_ctx *C, const Snapshot &s)
     TG_CUDA(cudaMemcpyAsync(C->s.p, s.p, sizeof(double) * (size_t)C->g.size(), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_x(C), s.px, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_xprev(C), s.pxp, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(poisson_xprev2(C), s.pxp2, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
+    k_set_phist<<<1, 1, 0, C->stream>>>(C->d_scal + SC_PHIST, s.phist);
     C->it = s.it;
     set_device_step(C);
 }

@@ -277,6 +277,8 @@ void poisson_solve_capture(tg_ctx *C);       // the same solve with device-side 
 // from a base (SC_G: forward step, SC_ADJ: transposed solve), and the step counter
 constexpr int ST_IT = 0, ST_RES0 = 1, ST_RES = 2, ST_TOT = 3, ST_NOCONV = 4, ST_NAN = 5, ST_COUNT = 6;
 constexpr int SC_G = 60, SC_ADJ = 70, SC_IT = 80;
+// solutions in the Poisson guess history (0, 1, 2 or more: order of the extrapolation)
+constexpr int SC_PHIST = 96;
 constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
               SC_GNOCONV = SC_G + ST_NOCONV, SC_GNAN = SC_G + ST_NAN;
 void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol);
@@ -320,6 +322,7 @@ void adj_destroy(tg_ctx *C);
 int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st);
 double *poisson_x(tg_ctx *C);
 double *poisson_xprev(tg_ctx *C);
+double *poisson_xprev2(tg_ctx *C);
 int64_t poisson_n(tg_ctx *C);
 
 }  // namespace tg

@@ -36,7 +36,7 @@ struct PoissonCtx {
     bool ortho;
     double *gE1, *gE2, *gE3, *gN1, *gN2, *gN3, *gT1, *gT2, *gT3;  // fine face tensors (compact)
     double *x, *b, *r, *z, *p, *q, *rhat, *v, *s, *t, *aj;
-    double *xprev;               // previous step's solution (extrapolated initial guess)
+    double *xprev, *xprev2;      // the two previous steps' solutions (extrapolated initial guess)
     double *part;                // reduction partials (4 per block)
     int nblocks;
     MG *mg;                      // multigrid preconditioner (host object)
@@ -239,16 +239,23 @@ __global__ void k_copy(int64_t n, const double *a, double *b)
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
 }
 __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
-// initial guess of the step's solve, 2 x_n - x_{n-1} (linear extrapolation of
-// the last two solutions; the reference starts from x_n), and xprev <- x_n
-__global__ void k_extrapolate(int64_t n, double *x, double *xprev)
+// initial guess of the step's solve from the last three solutions (the
+// reference starts from x_n): 3 x_n - 3 x_{n-1} + x_{n-2} (quadratic
+// extrapolation), 2 x_n - x_{n-1} while only two are known, x_n with one;
+// the history shifts (xprev2 <- xprev <- x_n). hist: device count of the
+// solutions in the history, read here and advanced by k_hist_next
+__global__ void k_extrapolate(int64_t n, double *x, double *xprev, double *xprev2, const double *hist)
 {
+    const double h = hist[0];
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const double xn = x[t];
-        x[t] = 2.0 * xn - xprev[t];
+        const double xn = x[t], xp = xprev[t];
+        if (h >= 2.0) x[t] = 3.0 * xn - 3.0 * xp + xprev2[t];
+        else if (h >= 1.0) x[t] = 2.0 * xn - xp;
+        xprev2[t] = xp;
         xprev[t] = xn;
     }
 }
+__global__ void k_hist_next(double *hist) { hist[0] = hist[0] + 1.0; }
 __global__ void k_negcopy(int64_t n, const double *a, double *b)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = -a[t];
@@ -409,8 +416,9 @@ void poisson_setup(tg_ctx *C)
     P->ortho = C->orthogonal;
     const int64_t n = P->n;
     double **fine[] = {&P->gE1, &P->gE2, &P->gE3, &P->gN1, &P->gN2, &P->gN3, &P->gT1, &P->gT2, &P->gT3,
-                       &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj, &P->xprev};
+                       &P->x, &P->b, &P->r, &P->z, &P->p, &P->q, &P->rhat, &P->v, &P->s, &P->t, &P->aj, &P->xprev, &P->xprev2};
     for (double **f : fine) *f = dallocd(C, n);
+    TG_CUDA(cudaMemsetAsync(C->d_scal + SC_PHIST, 0, sizeof(double), C->stream));   // empty guess history
     P->nblocks = vblocks(n);
     P->part = dallocd(C, 3 * (size_t)P->nblocks);
     k_gather_g<<<cgrid(P->nx, P->ny, P->nz), block3(), 0, C->stream>>>(g, C->m, *P);
@@ -551,8 +559,9 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt));
-    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev);
-    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solution
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST);
+    k_hist_next<<<1, 1, 0, s>>>(C->d_scal + SC_PHIST);
+    k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solutions
     int rc = krylov_solve(C, st, rtol, C->cfg.poisson_div_tol, maxit);
     TG_PROF(C, "pois_phi_to_dmda", k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P));
     TG_CUDA(cudaGetLastError());
@@ -709,7 +718,8 @@ void poisson_solve_capture(tg_ctx *C)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt);
-    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev);
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST);
+    k_hist_next<<<1, 1, 0, s>>>(C->d_scal + SC_PHIST);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
     krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit, SC_G);
     k_phi_to_dmda<<<cg3, block3(), 0, s>>>(g, C->s, P);
@@ -756,9 +766,10 @@ int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol
     return rc;
 }
 
-// compact Poisson solution vectors (the next solve starts from 2 x - xprev): snapshots
+// compact Poisson solution vectors (the next solve extrapolates x, xprev, xprev2): snapshots
 double *poisson_x(tg_ctx *C) { return C->pois->x; }
 double *poisson_xprev(tg_ctx *C) { return C->pois->xprev; }
+double *poisson_xprev2(tg_ctx *C) { return C->pois->xprev2; }
 int64_t poisson_n(tg_ctx *C) { return C->pois->n; }
 
 }  // namespace tg
