@@ -261,14 +261,30 @@ __global__ void k_negcopy(int64_t n, const double *a, double *b)
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = -a[t];
 }
 
-// CG: alpha = rz / pq ; x += alpha p ; r -= alpha q
-__global__ void k_cg_update(int64_t n, const double *rz, const double *pq, double *x, const double *p, double *r, const double *q)
+// CG: alpha = rz / pq ; x += alpha p ; r -= alpha q, with the partials of
+// k_dot_partial(r, r, w) formed in the same grid-stride order (same grid), so
+// the totals equal those of a separate update and dot product
+__global__ void k_cg_update_rr(int64_t n, const double *rz, const double *pq, double *x, const double *p, double *r,
+                               const double *q, const double *w, double *part)
 {
-    double alpha = rz[0] / pq[0];
+    __shared__ double s0[RB], s1[RB], s2[RB];
+    const double alpha = rz[0] / pq[0];
+    double d = 0.0, sa = 0.0, mx = 0.0;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         x[t] += alpha * p[t];
         r[t] -= alpha * q[t];
+        const double av = r[t];
+        d += av * av;
+        sa += av;
+        if (w) mx = fmax(mx, fabs(av * w[t]));
     }
+    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = s0[0]; part[3 * blockIdx.x + 1] = s1[0]; part[3 * blockIdx.x + 2] = s2[0]; }
 }
 // CG: beta = rz_new / rz_old ; p = z + beta p
 __global__ void k_cg_dir(int64_t n, const double *rznew, const double *rzold, const double *z, double *p)
@@ -480,8 +496,9 @@ static int krylov_solve(tg_ctx *C, tg_stats *st, double rtol, double divtol, int
             apply_op(C, P.p, P.q);
             k_zero_at<<<1, 1, 0, s>>>(P.q, P.pin);
             dot3v(C, P.p, P.q, nullptr, sc + 9);             // pq at sc[9]
-            TG_PROF(C, "pois_cg_update", k_cg_update<<<vblocks(n), RB, 0, s>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q));
-            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);   // rr, sum r, max|r aj|
+            // x += alpha p, r -= alpha q; rr, sum r, max|r aj|
+            TG_PROF(C, "pois_cg_update", k_cg_update_rr<<<P.nblocks, RB, 0, s>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q, divtol > 0 ? P.aj : nullptr, P.part));
+            k_dot_final<<<1, RB, 0, s>>>(P.part, P.nblocks, sc + 3);
             read_scal(C, 3, 3);
             rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
             it++;
@@ -656,8 +673,8 @@ static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit, int
             apply_op(C, P.p, P.q);
             k_zero_at<<<1, 1, 0, a>>>(P.q, P.pin);
             dot3v(C, P.p, P.q, nullptr, sc + 9);                          // pq
-            k_cg_update<<<vb, RB, 0, a>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q);
-            dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);      // rr, sum r, max|r aj|
+            k_cg_update_rr<<<P.nblocks, RB, 0, a>>>(n, sc + 6, sc + 9, P.x, P.p, P.r, P.q, divtol > 0 ? P.aj : nullptr, P.part);
+            k_dot_final<<<1, RB, 0, a>>>(P.part, P.nblocks, sc + 3);      // rr, sum r, max|r aj|
             k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
         });
     } else {
