@@ -543,7 +543,7 @@ __global__ void k_buoyancy(Grid g, Metrics m, State s, Params p)
 }
 
 // ------------------------------------------------------------------------
-// FormU (ueqn_solvers.c:6-1083), formMode 0.
+// FormU (ueqn_solvers.c:6-1083), every formMode (pass 1 selects the terms).
 // Pass 1: per face the convective (central or QUICK) plus viscous flux,
 // stored summed per direction in f1 (i faces), f2 (j faces), f3 (k faces).
 // ------------------------------------------------------------------------
