@@ -243,6 +243,25 @@ def cpu_baseline(workload, steps, threads=None):
     }
 
 
+def max_over_ranks_of(dist, x):
+    """The largest of the ranks' values of x (device time of the timed steps):
+    all_reduce(MAX) on the process group (a CUDA tensor under NCCL, a CPU one
+    under gloo); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(cells, steps, world, seconds):
+    """Whole-job Mcell-steps/s of `world` replicas that each advanced `cells`
+    cells by `steps` steps, timed by the slowest rank."""
+    return cells * steps * world / seconds / 1e6
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -454,11 +473,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(dist, x)
 
     def arm(precision):
         cfg, nodes, ucat, p, T, desc, turbines = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells,
@@ -491,7 +506,7 @@ def main():
         kernels = kernel_table(L, solver.h)
         return {"cfg": cfg, "desc": desc, "solver": solver, "st": st, "t_dev": t_dev, "clocks": clk.summary(),
                 "replayed": replayed, "momentum": mom,
-                "value": cfg.cells * args.steps * world / t_dev / 1e6, "kernels": kernels,
+                "value": replica_throughput(cfg.cells, args.steps, world, t_dev), "kernels": kernels,
                 "roofline": roofline_of(kernels, precision, cfg.cells, axis), "axis_aligned": axis}
 
     arms = {}
