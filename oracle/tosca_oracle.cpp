@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -103,6 +104,7 @@ struct tg_ctx {
     std::vector<double> tmprt_o;                // teqn->Tmprt_o (tosca_oracle_teqn.inc)
     std::vector<V3> rhs_o;                      // ueqn->Rhs_o (tosca_oracle_cn.inc)
     std::vector<V3> conv_o;                     // ueqn->RhsConv_o (ABCN, tosca_oracle_imex.inc)
+    std::vector<double> tconv_o;                // teqn->RhsConv_o (ABBE, tosca_oracle_teqn.inc)
     // last implicit momentum solve: Newton steps or IMEX stages, Krylov
     // operator products, last Krylov residual estimate
     int mom_outer = 0, mom_inner = 0;
@@ -1582,7 +1584,11 @@ int step(tg_ctx &C, tg_stats *st)
     if (urc == 2) rc = 2;
     else if (rc != 2) rc |= urc;
     contravariantToCartesian(C);                         // main.c:201
-    if (C.c.teqn) solveTEqn(C);                          // main.c:194-205
+    if (C.c.teqn) {                                      // main.c:194-205
+        const int trc = solveTEqn(C);
+        if (trc == 2) rc = 2;
+        else if (rc != 2) rc |= trc;
+    }
     double md = continuityError(C);                      // main.c:227
     if (st) st->max_divergence = md;
     if (C.c.ddt_scheme == TG_DDT_CN) {                   // main.c:214-272: Rhs_o of the next step
@@ -1702,6 +1708,8 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
+        if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_ABBE) return TG_ERR_BAD_ARG;
+        if (cfg->t_gmres_restart < 0 || cfg->t_gmres_restart > 60) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
             if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
             if ((cfg->t_bc[p] == TG_TBC_PERIODIC) != (cfg->bc[p] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;

@@ -48,3 +48,26 @@ def test_teqn_replay_and_mixed():
     assert rel_l2(tm, te) < 1e-6 and rel_l2(um, ue) < 1e-6
     for s, _, _ in res:
         s.close()
+
+
+@pytest.mark.parametrize("les", [1, 0])
+def test_abbe_temperature_matches_oracle(les):
+    # ABBE: AB2 convection and backward-Euler diffusion by GMRES (TeqnABBE),
+    # converged to 1e-13 of |b| on both sides
+    cfg, nodes, ucat, p, T = cases.hill_case(teqn=True, t_amp=0.5, nx=24, ny=12, nz=12)
+    cfg.poisson_rtol = 1e-13
+    cfg.les = les
+    cfg.t_ddt_scheme = api.TDDT_ABBE
+    cfg.t_atol, cfg.t_rtol = 0.0, 1e-13
+    out = []
+    for make in (tosca_b200.gpu_solver, oracle.solver):
+        s = make(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        s.step(5)
+        out.append(s)
+    g, o = out
+    for f in ("TMPRT", "UCAT", "UCONT"):
+        assert rel_l2(g.get(f), o.get(f)) < 1e-10, f
+    assert rel_l2(g.get("P"), o.get("P")) < 1e-9
+    assert g.graph_info()[0] == 0          # the GMRES loop runs on the host
+    g.close(); o.close()

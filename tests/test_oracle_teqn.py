@@ -6,6 +6,7 @@ import numpy as np
 
 import oracle
 from tosca_b200 import api, cases
+from tests.common import rel_l2
 
 SMALL = dict(nx=24, ny=12, nz=12)
 
@@ -43,3 +44,35 @@ def test_perturbation_is_transported():
     # zero gradient at the terrain
     assert np.array_equal(t1[1:-1, 0, 1:-1], t1[1:-1, 1, 1:-1])
     s.close()
+
+
+def _abbe_run(dt, steps, scheme, rtol=1e-13, restart=30, les=1):
+    cfg, nodes, ucat, p, T = cases.hill_case(teqn=True, t_amp=0.5, nx=16, ny=8, nz=8, dt=dt)
+    cfg.les = les
+    cfg.poisson_rtol = 1e-13
+    cfg.t_ddt_scheme = scheme
+    cfg.t_atol, cfg.t_rtol, cfg.t_gmres_restart = 0.0, rtol, restart
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    s.step(steps)
+    t = s.get("TMPRT")
+    s.close()
+    return t
+
+
+def test_abbe_temperature_converges_to_rk4():
+    # ABBE (AB2 convection, backward-Euler diffusion, forward Euler on the
+    # first step) against the explicit RK4 temperature: first order in dt
+    errs = []
+    for dt, steps in ((0.5, 4), (0.25, 8)):
+        a = _abbe_run(dt, steps, api.TDDT_ABBE)
+        r = _abbe_run(dt, steps, api.TDDT_RK4)
+        assert np.isfinite(a).all()
+        errs.append(rel_l2(a, r))
+    assert errs[0] < 1e-4 and 1.6 < errs[0] / errs[1] < 4.5, errs
+
+
+def test_abbe_gmres_restart_independent():
+    a = _abbe_run(0.5, 2, api.TDDT_ABBE, restart=30, les=0)
+    b = _abbe_run(0.5, 2, api.TDDT_ABBE, restart=1, les=0)
+    assert rel_l2(b, a) < 1e-11

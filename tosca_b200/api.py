@@ -22,6 +22,7 @@ BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
+TDDT_RK4, TDDT_ABBE = 0, 1
 TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
@@ -71,6 +72,10 @@ class TgConfig(C.Structure):
         ("snes_rtol", C.c_double),
         ("snes_maxit", C.c_int32),
         ("gmres_restart", C.c_int32),
+        ("t_ddt_scheme", C.c_int32),
+        ("t_gmres_restart", C.c_int32),
+        ("t_atol", C.c_double),
+        ("t_rtol", C.c_double),
     ]
 
 
@@ -162,6 +167,10 @@ class Config:
     snes_rtol: float = 1e-30
     snes_maxit: int = 20
     gmres_restart: int = 30
+    t_ddt_scheme: int = 0
+    t_gmres_restart: int = 30
+    t_atol: float = 1e-5
+    t_rtol: float = 1e-30
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

@@ -26,15 +26,20 @@
 
 namespace tg {
 
-struct ImexWork {
-    int m = 30;                       // GMRES restart
-    int64_t n = 0;                    // unknowns: 3 G
-    V3f<double> bu{}, visc{}, conv{}, conv_o{}, x{}, rhs_o{};
+// restarted GMRES on n unknowns (gmres_solve)
+struct GmresWork {
+    int m = 30;                       // restart
+    int64_t n = 0;                    // unknowns
     double *V = nullptr;              // (m + 1) Krylov vectors of n
     double *part = nullptr;           // block partials: (m + 1) x nb
     double *d_out = nullptr;          // reduced dot products (m + 2)
     double *h_out = nullptr;          // pinned host copy
     int nb = 0;                       // blocks of the chunked kernels
+};
+
+struct ImexWork {
+    GmresWork k;                      // n = 3 G
+    V3f<double> bu{}, visc{}, conv{}, conv_o{}, x{}, rhs_o{};
 };
 
 namespace {
@@ -201,28 +206,33 @@ __global__ void k_rk3so_bu(int64_t n, double *bu, double *x, const double *uo, c
 
 inline int nblk(int64_t n) { int64_t b = (n + TB - 1) / TB; return (int)(b < 148 * 8 ? b : 148 * 8); }
 
+void gmres_init(tg_ctx *C, GmresWork &W, int64_t n, int m)
+{
+    W.m = m;
+    W.n = n;
+    W.V = dallocd(C, (size_t)(W.m + 1) * W.n);
+    W.nb = (int)((W.n + CH - 1) / CH);
+    W.part = dallocd(C, (size_t)(W.m + 1) * W.nb);
+    W.d_out = dallocd(C, MAXV + 2);
+    TG_CUDA(cudaMallocHost((void **)&W.h_out, (MAXV + 2) * sizeof(double)));
+}
+
 ImexWork &work(tg_ctx *C)
 {
     if (!C->imex) {
         ImexWork *W = new ImexWork();
         const size_t G = (size_t)C->g.size();
-        W->m = C->cfg.gmres_restart > 0 ? C->cfg.gmres_restart : 30;
-        W->n = 3 * (int64_t)G;
         W->bu = dalloc3(C, G); W->visc = dalloc3(C, G); W->x = dalloc3(C, G);
         if (C->cfg.ddt_scheme == TG_DDT_ABCN) { W->conv = dalloc3(C, G); W->conv_o = dalloc3(C, G); }
         if (C->cfg.ddt_scheme == TG_DDT_RK3WCN) W->rhs_o = dalloc3(C, G);
-        W->V = dallocd(C, (size_t)(W->m + 1) * W->n);
-        W->nb = (int)((W->n + CH - 1) / CH);
-        W->part = dallocd(C, (size_t)(W->m + 1) * W->nb);
-        W->d_out = dallocd(C, MAXV + 2);
-        TG_CUDA(cudaMallocHost((void **)&W->h_out, (MAXV + 2) * sizeof(double)));
         C->imex = W;
+        gmres_init(C, W->k, 3 * (int64_t)G, C->cfg.gmres_restart > 0 ? C->cfg.gmres_restart : 30);
     }
     return *C->imex;
 }
 
 // |a| (VecNorm NORM_2)
-double norm(tg_ctx *C, ImexWork &W, const double *a)
+double norm(tg_ctx *C, GmresWork &W, const double *a)
 {
     k_norm2<<<W.nb, TB, 0, C->stream>>>(W.n, a, W.part);
     k_rows_sum<<<1, TB, 0, C->stream>>>(W.part, W.nb, W.d_out);
@@ -233,9 +243,9 @@ double norm(tg_ctx *C, ImexWork &W, const double *a)
 
 // Av = A v = v - dtp s Visc(v) (IMEXMatVec): leaves Ucont = v and its Ucat in
 // the state, as the reference does
-void apply(tg_ctx *C, ImexWork &W, const double *v, double *Av, double dtp, double s)
+void apply(tg_ctx *C, const double *v, double *Av, double dtp, double s)
 {
-    const int64_t n = W.n, G = C->g.size();
+    const int64_t G = C->g.size(), n = 3 * G;
     TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
     reset_no_penetration(C);
     reset_face_periodic(C, C->s.ucont);
@@ -248,13 +258,16 @@ void apply(tg_ctx *C, ImexWork &W, const double *v, double *Av, double dtp, doub
     k_add<<<nblk(n), TB, 0, C->stream>>>(n, Av, v);
 }
 
-// KSPSolve(kspIMEX, b, x) with KSPGMRES: 0 converged, 1 iteration limit,
-// 2 not a number or breakdown
-int gmres(tg_ctx *C, ImexWork &W, const double *b, double *x, double dtp, double s, int &its, double &res)
+}  // namespace
+
+// KSPSolve with KSPGMRES on the operator A (A(v, Av) writes A v): 0
+// converged, 1 iteration limit, 2 not a number or breakdown
+int gmres_solve(tg_ctx *C, GmresWork &W, const std::function<void(const double *, double *)> &A, const double *b, double *x,
+                double rtol, double atol, int &its, double &res)
 {
     const int64_t n = W.n;
     const int m = W.m, maxit = 1000;
-    const double rtol = C->cfg.snes_rtol, atol = C->cfg.snes_atol, haptol = 1e-30;
+    const double haptol = 1e-30;
     auto Vk = [&](int k) { return W.V + (int64_t)k * n; };
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     auto Hq = [&](int r, int c) -> double & { return H[(size_t)r * m + c]; };
@@ -265,7 +278,7 @@ int gmres(tg_ctx *C, ImexWork &W, const double *b, double *x, double dtp, double
     int reason = 0;   // 1 converged, -1 iteration limit, -2 nan / breakdown
     while (!reason) {
         // KSPInitialResidual: V0 = b - A x
-        apply(C, W, x, Vk(0), dtp, s);
+        A(x, Vk(0));
         k_axpby<<<nblk(n), TB, 0, C->stream>>>(n, 1.0, b, -1.0, Vk(0));
         const double beta = norm(C, W, Vk(0));
         if (first) {
@@ -284,7 +297,7 @@ int gmres(tg_ctx *C, ImexWork &W, const double *b, double *x, double dtp, double
         int k = 0;
         while (!reason && k < m && its < maxit) {
             double *w = Vk(k + 1);
-            apply(C, W, Vk(k), w, dtp, s);
+            A(Vk(k), w);
             // classical Gram-Schmidt: h = V^T w, w -= V h, |w|
             k_mdot<<<W.nb, TB, 0, C->stream>>>(n, w, W.V, k + 1, W.part);
             k_rows_sum<<<k + 1, TB, 0, C->stream>>>(W.part, W.nb, W.d_out);
@@ -342,11 +355,22 @@ int gmres(tg_ctx *C, ImexWork &W, const double *b, double *x, double dtp, double
     return reason == 1 ? 0 : reason == -1 ? 1 : 2;
 }
 
-}  // namespace
+GmresWork *gmres_alloc(tg_ctx *C, int64_t n, int m)
+{
+    GmresWork *W = new GmresWork();
+    gmres_init(C, *W, n, m);
+    return W;
+}
+
+void gmres_free(GmresWork *W)
+{
+    if (W && W->h_out) cudaFreeHost(W->h_out);
+    delete W;            // device buffers are owned by the context allocation list
+}
 
 void imex_destroy(tg_ctx *C)
 {
-    if (C->imex && C->imex->h_out) cudaFreeHost(C->imex->h_out);
+    if (C->imex && C->imex->k.h_out) cudaFreeHost(C->imex->k.h_out);
     delete C->imex;      // device buffers are owned by the context allocation list
     C->imex = nullptr;
 }
@@ -357,7 +381,7 @@ bool imex_scheme(int ddt) { return ddt == TG_DDT_ABCN || ddt == TG_DDT_RK3WCN ||
 int solve_u_imex(tg_ctx *C)
 {
     ImexWork &W = work(C);
-    const int64_t n = W.n;
+    const int64_t n = W.k.n;
     const double dt = C->prm.dt;
     const size_t bytes = sizeof(double) * n;
     int rc = 0, stages = 0, inner = 0;
@@ -370,7 +394,8 @@ int solve_u_imex(tg_ctx *C)
     };
     auto solve = [&](double dtp, double s) {
         int its = 0;
-        const int r = gmres(C, W, W.bu.x, W.x.x, dtp, s, its, res);
+        const int r = gmres_solve(C, W.k, [&](const double *v, double *Av) { apply(C, v, Av, dtp, s); }, W.bu.x, W.x.x,
+                                  C->cfg.snes_rtol, C->cfg.snes_atol, its, res);
         inner += its;
         stages++;
         if (r == 2) rc = 2;

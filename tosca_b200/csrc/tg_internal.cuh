@@ -109,6 +109,7 @@ struct AdjState;     // tg_adjoint.cu
 struct Farm;         // tg_farm.cu
 struct CnWork;       // tg_cn.cu
 struct ImexWork;     // tg_imex.cu
+struct GmresWork;    // tg_imex.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -175,6 +176,9 @@ struct tg_ctx {
     tg::Farm *farm = nullptr;            // actuator-disk turbines (tg_farm.cu)
     tg::CnWork *cn = nullptr;            // Crank-Nicolson Newton-Krylov work (tg_cn.cu)
     tg::ImexWork *imex = nullptr;        // IMEX GMRES work (tg_imex.cu)
+    tg::GmresWork *tgm = nullptr;        // GMRES work of the ABBE temperature solve (tg_teqn.cu)
+    double *tconv = nullptr, *tconv_o = nullptr;   // teqn->RhsConv, RhsConv_o (ABBE)
+    int t_its = 0;                       // GMRES iterations of the last ABBE temperature solve
     // last implicit momentum solve: Newton steps or IMEX stages, Krylov
     // operator products, last Krylov residual estimate
     int mom_outer = 0, mom_inner = 0;
@@ -291,12 +295,17 @@ void adj_graph_destroy(tg_ctx *C);
 int solve_u_cn(tg_ctx *C, tg_stats *st);
 void cn_destroy(tg_ctx *C);
 bool imex_scheme(int ddt);                                         // tg_imex.cu
+// restarted GMRES as PETSc's KSPGMRES (tg_imex.cu): A(v, Av) writes A v
+GmresWork *gmres_alloc(tg_ctx *C, int64_t n, int m);
+void gmres_free(GmresWork *W);
+int gmres_solve(tg_ctx *C, GmresWork &W, const std::function<void(const double *, double *)> &A, const double *b, double *x,
+                double rtol, double atol, int &its, double &res);
 int solve_u_imex(tg_ctx *C);
 void imex_destroy(tg_ctx *C);
 void cn_build_bu(tg_ctx *C, V3f<double> bu, bool half_rhs_o);   // tg_step.cu
 void mask_non_resolved(tg_ctx *C, V3f<double> v);               // resetNonResolvedCellFaces on v
 void contra_to_cart_stage(tg_ctx *C);
-void solve_t(tg_ctx *C);
+int solve_t(tg_ctx *C);      // 0, or the ABBE GMRES status (1 iteration cap, 2 breakdown)
 void update_temperature_bcs(tg_ctx *C);
 // wind farm (tg_farm.cu)
 void farm_update(tg_ctx *C);                 // sampling, forces, projection, face body force

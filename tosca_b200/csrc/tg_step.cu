@@ -1610,7 +1610,11 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     else if (rc != 2) rc |= urc;
     pressure_update_and_project(C);
     contra_to_cart(C);
-    if (C->prm.teqn) solve_t(C);        // main.c:194-205
+    if (C->prm.teqn) {                  // main.c:194-205
+        const int trc = solve_t(C);
+        if (trc == 2) rc = 2;
+        else if (rc != 2) rc |= trc;
+    }
     reduce_max_abs_div(C, C->d_scal + 16);
     if (C->cfg.ddt_scheme == TG_DDT_CN) {   // main.c:214-272: Rhs_o for the next step
         TG_CUDA(cudaMemsetAsync(C->s.rhs_o.x, 0, 3 * sizeof(double) * G, C->stream));
@@ -1634,6 +1638,7 @@ static bool graph_eligible(const tg_ctx *C)
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
     return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
            C->cfg.ddt_scheme != TG_DDT_CN && !imex_scheme(C->cfg.ddt_scheme) &&   // host-driven Krylov loops
+           !(C->prm.teqn && C->cfg.t_ddt_scheme == TG_TDDT_ABBE) &&
            C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 

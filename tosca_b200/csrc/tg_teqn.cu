@@ -142,10 +142,11 @@ __global__ void k_t_face_fluxes(Grid g, Metrics m, State s, Params p, V3f<double
     }
 }
 
-// pass 2 (teqn_solvers.c:540-566): rhs = (div budget + visc budget) aj at
+// pass 2 (teqn_solvers.c:520-566): rhs = (div budget + visc budget) aj at
 // interior cells, face 0 of a periodic direction read from face m-2
-// (resetFacePeriodicFluxesVector)
-__global__ void k_t_rhs(Grid g, Metrics m, V3f<double> dv, V3f<double> vs, double *rhs)
+// (resetFacePeriodicFluxesVector); formMode 1 keeps the convective budget
+// only, 2 the diffusive one
+__global__ void k_t_rhs(Grid g, Metrics m, V3f<double> dv, V3f<double> vs, double *rhs, int mode)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -155,7 +156,30 @@ __global__ void k_t_rhs(Grid g, Metrics m, V3f<double> dv, V3f<double> vs, doubl
     const int kb = (k == 1 && g.pk) ? c + (g.mz - 3) * pl : c - pl;
     const double divBudget = dv.x[c] - dv.x[iw] + dv.y[c] - dv.y[js] + dv.z[c] - dv.z[kb];
     const double viscBudget = vs.x[c] - vs.x[iw] + vs.y[c] - vs.y[js] + vs.z[c] - vs.z[kb];
-    rhs[c] = 1.0 * (divBudget + viscBudget) * m.aj[c];
+    rhs[c] = 1.0 * ((mode != 2 ? divBudget : 0.0) + (mode != 1 ? viscBudget : 0.0)) * m.aj[c];
+}
+
+// TeqnABBE steps 3-5 (teqn_solvers.c:835-880): bT = 3/2 Conv - 1/2 Conv_o
+// (Conv on the first step), b = dt bT (zero off the interior) + T_o, and the
+// guess x = b
+__global__ void k_t_abbe_b(int64_t n, double *b, double *x, const double *conv, const double *conv_o, const double *to,
+                           double dt, int ab2)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        double bt = 0.0;
+        if (ab2) { bt = bt + 1.5 * conv[q]; bt = bt + -0.5 * conv_o[q]; }
+        else bt = bt + 1.0 * conv[q];
+        const double v = bt * dt + 1.0 * to[q];
+        b[q] = v;
+        x[q] = v;
+    }
+}
+
+// ABBEMatVec tail (teqn_solvers.c:930-943): Av = v - dt D(v), D(v) zero off the interior
+__global__ void k_t_abbe_av(int64_t n, double *Av, const double *v, const double *d, double dt)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        Av[q] = v[q] + -1.0 * (d[q] * dt);
 }
 
 // TeqnRK4 bookkeeping after stage st: Ttmp (+)= dt b Rhs, next stage T = T_o + a dt Rhs, last T = Ttmp
@@ -197,24 +221,72 @@ __global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
 
 }  // namespace
 
-// SolveTEqn with TeqnRK4 (teqn.c:259-276, teqn_solvers.c:714-818)
-void solve_t(tg_ctx *C)
+// SolveTEqn with TeqnABBE (teqn_solvers.c:821-945): AB2 convection,
+// backward-Euler diffusion A T = b, A v = v - dt D(v) (ABBEMatVec: D is FormT
+// with formMode 2 of v, periodic ghosts reset, zero off the interior; the
+// boundary ghosts of v stay those of the Krylov vector, and kappa_eff follows
+// v's vertical gradient, so A is not linear in v for LES, as in the reference)
+// by GMRES (kspIMEX: PCNONE, restart -kspGMRESRestartT, relTolT / absTolT,
+// 1000 iterations, the b as initial guess). Returns the GMRES status.
+static int solve_t_abbe(tg_ctx *C)
 {
     const Grid g = C->g;
     const int64_t G = g.size();
     State &s = C->s;
     const double dt = C->prm.dt;
+    if (!C->tgm) C->tgm = gmres_alloc(C, G, C->cfg.t_gmres_restart > 0 ? C->cfg.t_gmres_restart : 30);
+    // Steps 1-2: periodic ghosts, convective right-hand side at T^n
+    reset_cell_periodic_s(C, s.tmprt);
+    TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+    TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, C->tconv, 1));
+    // Steps 3-4: b (in Ttmp) and the guess; as in the reference the solution
+    // goes into RhsConv_o, whose AB2 history this kernel consumes first
+    double *b = s.ttmp, *x = C->tconv_o;
+    TG_PROF(C, "teqn_abbe_b", k_t_abbe_b<<<nblk(G), 256, 0, C->stream>>>(G, b, x, C->tconv, C->tconv_o, s.tmprt_o, dt,
+                                                                         C->it > C->cfg.it_start ? 1 : 0));
+    // Step 5: GMRES on ABBEMatVec
+    auto A = [&](const double *v, double *Av) {
+        TG_CUDA(cudaMemcpyAsync(s.tmprt, v, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+        reset_cell_periodic_s(C, s.tmprt);
+        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 2));
+        TG_PROF(C, "teqn_abbe_av", k_t_abbe_av<<<nblk(G), 256, 0, C->stream>>>(G, Av, v, s.trhs, dt));
+    };
+    int its = 0;
+    double res = 0.0;
+    const int rc = gmres_solve(C, *C->tgm, A, b, x, C->cfg.t_rtol, C->cfg.t_atol, its, res);
+    // Steps 6-7: T = solution, RhsConv_o = RhsConv
+    TG_CUDA(cudaMemcpyAsync(s.tmprt, x, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(C->tconv_o, C->tconv, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    C->t_its = its;
+    return rc;
+}
+
+// SolveTEqn (teqn.c:259-276) with TeqnRK4 (teqn_solvers.c:714-818) or
+// TeqnABBE; returns the implicit solve's status (0 for RK4)
+int solve_t(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int64_t G = g.size();
+    State &s = C->s;
+    const double dt = C->prm.dt;
+    if (C->cfg.t_ddt_scheme == TG_TDDT_ABBE) {
+        const int rc = solve_t_abbe(C);
+        reset_cell_periodic_s(C, s.tmprt);
+        return rc;
+    }
     const double b[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
     const double a[4] = {0.0, 0.5, 0.5, 1.0};
     for (int st = 0; st < 4; st++) {
         // FormExplicitRhsT: periodic ghosts, FormT (Rhs zero off the interior)
         reset_cell_periodic_s(C, s.tmprt);
         TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
-        TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs));
+        TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 0));
         TG_PROF(C, "teqn_rk_update", k_t_rk<<<nblk(G), 256, 0, C->stream>>>(G, s.tmprt, s.tmprt_o, s.ttmp, s.trhs,
                                                                           dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0, st == 3));
     }
     reset_cell_periodic_s(C, s.tmprt);
+    return 0;
 }
 
 void update_temperature_bcs(tg_ctx *C)
