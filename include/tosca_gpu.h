@@ -74,10 +74,11 @@ enum { TG_ILEFT = 0, TG_IRIGHT = 1, TG_JLEFT = 2, TG_JRIGHT = 3, TG_KLEFT = 4, T
 /* ------------------------------------------------------------ configuration -- */
 /* temperature patch types (boundary/T, UpdateTemperatureBCs boundary.c:2052-2616) */
 enum { TG_TBC_ZERO_GRADIENT = 0, TG_TBC_FIXED_VALUE = 1, TG_TBC_FIXED_GRADIENT = 2, TG_TBC_PERIODIC = 3 };
-/* -dTdtScheme (teqn.c:66-230): explicit RK4, or ABBE (Adams-Bashforth 2
+/* -dTdtScheme (teqn.c:66-230): explicit RK4; ABBE (Adams-Bashforth 2
  * convection, backward-Euler diffusion solved by GMRES on ABBEMatVec,
- * teqn_solvers.c:821-945) */
-enum { TG_TDDT_RK4 = 0, TG_TDDT_ABBE = 1 };
+ * teqn_solvers.c:821-945); BE and BDF2 (implicit, Newton-Krylov on
+ * SNESFuncEvalT, teqn_solvers.c:596-712) */
+enum { TG_TDDT_RK4 = 0, TG_TDDT_ABBE = 1, TG_TDDT_BE = 2, TG_TDDT_BDF2 = 3 };
 
 typedef struct tg_config {
     int32_t mx, my, mz;            /* DMDA extent incl. the one-cell physical ghost layer  */
@@ -123,7 +124,8 @@ typedef struct tg_config {
     int32_t gmres_restart;         /* -kspGMRESRestartU (ueqn.c:233), 0 = 30                */
     /* temperature scheme (teqn = 1): TG_TDDT_*; ABBE's GMRES stops at
      * |r| <= max(t_rtol |b|, t_atol) (-relTolT, -absTolT, defaults 1e-30, 1e-5)
-     * or 1000 iterations, restart -kspGMRESRestartT (0 = 30) */
+     * or 1000 iterations, restart -kspGMRESRestartT (0 = 30); BE/BDF2 stop
+     * their Newton iteration at |F| <= max(t_atol, t_rtol |F_0|) or 20 steps */
     int32_t t_ddt_scheme;
     int32_t t_gmres_restart;
     double  t_atol;

@@ -105,6 +105,7 @@ struct tg_ctx {
     std::vector<V3> rhs_o;                      // ueqn->Rhs_o (tosca_oracle_cn.inc)
     std::vector<V3> conv_o;                     // ueqn->RhsConv_o (ABCN, tosca_oracle_imex.inc)
     std::vector<double> tconv_o;                // teqn->RhsConv_o (ABBE, tosca_oracle_teqn.inc)
+    std::vector<double> tmprt_oo;               // teqn->Tmprt_oo (BDF2)
     // last implicit momentum solve: Newton steps or IMEX stages, Krylov
     // operator products, last Krylov residual estimate
     int mom_outer = 0, mom_inner = 0;
@@ -1367,8 +1368,8 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
 }
 
 #include "tosca_oracle_farm.inc"
-#include "tosca_oracle_teqn.inc"
 #include "tosca_oracle_cn.inc"
+#include "tosca_oracle_teqn.inc"
 
 // ExplicitRhsU, ueqn_solvers.c:1276-1407 (mode: formMode of its FormU)
 void explicitRhsU(tg_ctx &C, int mode = 0)
@@ -1571,7 +1572,10 @@ void syncPressure(tg_ctx &C)
 int step(tg_ctx &C, tg_stats *st)
 {
     C.ucont_o = C.ucont;                                 // main.c:81
-    if (C.c.teqn) C.tmprt_o = C.tmprt;                   // main.c:83-99
+    if (C.c.teqn) {                                      // main.c:83-99
+        if (C.c.t_ddt_scheme == TG_TDDT_BDF2) C.tmprt_oo = C.tmprt_o.empty() ? std::vector<double>(C.G, 0.0) : C.tmprt_o;
+        C.tmprt_o = C.tmprt;
+    }
     if (C.c.les) { updateNut(C); updateWallModels(C); }  // main.c:112-117
     if (!C.farm.empty()) updateWindTurbines(C);          // main.c:144-147
     gradP(C);                                            // main.c:160-167
@@ -1708,7 +1712,7 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
-        if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_ABBE) return TG_ERR_BAD_ARG;
+        if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;
         if (cfg->t_gmres_restart < 0 || cfg->t_gmres_restart > 60) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
             if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;

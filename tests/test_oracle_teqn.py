@@ -3,6 +3,7 @@ uniform temperature is preserved by the WENO3 convection and the diffusion
 (up to the projected divergence), and the temperature changes where the
 flow advects a perturbation."""
 import numpy as np
+import pytest
 
 import oracle
 from tosca_b200 import api, cases
@@ -76,3 +77,22 @@ def test_abbe_gmres_restart_independent():
     a = _abbe_run(0.5, 2, api.TDDT_ABBE, restart=30, les=0)
     b = _abbe_run(0.5, 2, api.TDDT_ABBE, restart=1, les=0)
     assert rel_l2(b, a) < 1e-11
+
+
+@pytest.mark.parametrize("scheme,lo,hi", [(api.TDDT_BE, 1.8, 2.2), (api.TDDT_BDF2, 3.0, 5.0)])
+def test_implicit_temperature_order(scheme, lo, hi):
+    # TeqnSNES: backward Euler is first order, BDF2 (BE on the first step)
+    # second order against the explicit RK4 temperature
+    errs = []
+    for dt, steps in ((0.5, 4), (0.25, 8)):
+        a = _abbe_run(dt, steps, scheme, rtol=1e-10)
+        r = _abbe_run(dt, steps, api.TDDT_RK4)
+        errs.append(rel_l2(a, r))
+    assert errs[0] < 1e-5 and lo < errs[0] / errs[1] < hi, errs
+
+
+def test_temperature_scheme_checked():
+    cfg, nodes, ucat, p, T = cases.hill_case(teqn=True, t_amp=0.5, nx=16, ny=8, nz=8)
+    cfg.t_ddt_scheme = 4
+    with pytest.raises(api.TgError):
+        oracle.solver(cfg)

@@ -22,7 +22,7 @@ BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
-TDDT_RK4, TDDT_ABBE = 0, 1
+TDDT_RK4, TDDT_ABBE, TDDT_BE, TDDT_BDF2 = 0, 1, 2, 3
 TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 

@@ -212,7 +212,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (cfg->ddt_scheme != TG_DDT_RK4 || !(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
-        if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_ABBE) return TG_ERR_BAD_ARG;
+        if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;
         if (cfg->t_gmres_restart < 0 || cfg->t_gmres_restart > 60) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
             if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
@@ -259,6 +259,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
             st.tdiv = dalloc3(C, G); st.tvisc = dalloc3(C, G);
             st.trhs = dallocd(C, G); st.tmprt_o = dallocd(C, G); st.ttmp = dallocd(C, G);
             if (cfg->t_ddt_scheme == TG_TDDT_ABBE) { C->tconv = dallocd(C, G); C->tconv_o = dallocd(C, G); }
+            if (cfg->t_ddt_scheme == TG_TDDT_BDF2) C->tmprt_oo = dallocd(C, G);
         }
         const size_t P = (size_t)g.mx * g.mz;
         double **ws[] = {&st.twx, &st.twy, &st.twz, &st.umean, &st.ufx, &st.ufy, &st.ufz};
@@ -294,6 +295,8 @@ tg_status tg_destroy(tg_ctx *C)
     imex_destroy(C);
     gmres_free(C->tgm);
     C->tgm = nullptr;
+    jfnk_free(C->tsn);
+    C->tsn = nullptr;
     poisson_destroy(C);
     adj_destroy(C);
     for (void *p : C->allocs) cudaFree(p);

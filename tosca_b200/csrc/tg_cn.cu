@@ -21,12 +21,19 @@
 
 namespace tg {
 
-struct CnWork {
-    int m = 30;                       // GMRES restart (-kspGMRESRestartU)
-    V3f<double> bu{}, U{}, F{}, W{}, FW{};
-    double *V = nullptr;              // (m + 1) Krylov vectors of 3 G
+// Jacobian-free Newton-Krylov work on n unknowns (jfnk_solve)
+struct JfnkWork {
+    int m = 30;                       // GMRES restart
+    int64_t n = 0;
+    double *U = nullptr, *F = nullptr, *W = nullptr, *FW = nullptr;   // iterate, F(U), correction, F(probe)
+    double *V = nullptr;              // (m + 1) Krylov vectors of n
     double *part = nullptr;           // dot-product partials
     int nb = 0;
+};
+
+struct CnWork {
+    JfnkWork j;                       // n = 3 G
+    V3f<double> bu{};
 };
 
 namespace {
@@ -79,7 +86,7 @@ __global__ void k_cn_time(int64_t n, double *F, const double *U, const double *U
 
 inline int nblk(int64_t n) { int64_t b = (n + DB - 1) / DB; return (int)(b < 148 * 8 ? b : 148 * 8); }
 
-double dot(tg_ctx *C, CnWork &W, const double *a, const double *b, int64_t n)
+double dot(tg_ctx *C, JfnkWork &W, const double *a, const double *b, int64_t n)
 {
     k_dot_part<<<W.nb, DB, 0, C->stream>>>(n, a, b, W.part);
     k_dot_sum<<<1, DB, 0, C->stream>>>(W.part, W.nb, C->d_scal + 90);
@@ -88,17 +95,24 @@ double dot(tg_ctx *C, CnWork &W, const double *a, const double *b, int64_t n)
     return C->h_scal[90];
 }
 
+void jfnk_init(tg_ctx *C, JfnkWork &W, int64_t n, int m)
+{
+    W.m = m;
+    W.n = n;
+    W.U = dallocd(C, n); W.F = dallocd(C, n); W.W = dallocd(C, n); W.FW = dallocd(C, n);
+    W.V = dallocd(C, (size_t)(m + 1) * n);
+    W.nb = nblk(n);
+    W.part = dallocd(C, W.nb);
+}
+
 CnWork &work(tg_ctx *C)
 {
     if (!C->cn) {
         CnWork *W = new CnWork();
         const size_t G = (size_t)C->g.size();
-        W->m = C->cfg.gmres_restart > 0 ? C->cfg.gmres_restart : 30;
-        W->bu = dalloc3(C, G); W->U = dalloc3(C, G); W->F = dalloc3(C, G); W->W = dalloc3(C, G); W->FW = dalloc3(C, G);
-        W->V = dallocd(C, (size_t)(W->m + 1) * 3 * G);
-        W->nb = nblk(3 * (int64_t)G);
-        W->part = dallocd(C, W->nb);
+        W->bu = dalloc3(C, G);
         C->cn = W;
+        jfnk_init(C, W->j, 3 * (int64_t)G, C->cfg.gmres_restart > 0 ? C->cfg.gmres_restart : 30);
     }
     return *C->cn;
 }
@@ -113,10 +127,11 @@ void cn_destroy(tg_ctx *C)
 
 // SNESFuncEval (ueqn_solvers.c:1203-1272): F(U) into Fout; leaves Ucont = U
 // and the Ucat of U in the state, as the reference does
-static void cn_eval(tg_ctx *C, CnWork &W, V3f<double> U, V3f<double> Fout, double scale)
+static void cn_eval(tg_ctx *C, CnWork &W, const double *U, double *F, double scale)
 {
-    const int64_t n = 3 * C->g.size();
-    TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, U.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+    const int64_t G = C->g.size(), n = 3 * G;
+    V3f<double> Fout{F, F + G, F + 2 * G};
+    TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
     reset_no_penetration(C);
     reset_face_periodic(C, C->s.ucont);
     contra_to_cart_stage(C);
@@ -125,32 +140,34 @@ static void cn_eval(tg_ctx *C, CnWork &W, V3f<double> U, V3f<double> Fout, doubl
     form_u(C, Fout, scale);
     k_scale<<<nblk(n), DB, 0, C->stream>>>(n, C->prm.dt, Fout.x);
     mask_non_resolved(C, Fout);
-    k_cn_time<<<nblk(n), DB, 0, C->stream>>>(n, Fout.x, U.x, C->s.ucont_o.x);
+    k_cn_time<<<nblk(n), DB, 0, C->stream>>>(n, Fout.x, U, C->s.ucont_o.x);
 }
 
-// UeqnSNES (ueqn_solvers.c:1087-1199): Ucont <- the root of F from Ucont_o
-int solve_u_cn(tg_ctx *C, tg_stats *st)
+// Jacobian-free Newton-Krylov root of F (Feval(U, F) writes F(U)) from the
+// guess in W.U, left in W.U: restarted GMRES on J d = -F to 1e-3 relative
+// residual per Newton step, J v = (F(U + h v) - F(U)) / h with PETSc's
+// MATMFFD_WP h = sqrt(eps) sqrt(1 + |U|) / |v|, Newton steps halved while |F|
+// does not fall; stop at |F| <= max(atol, rtol |F_0|) or maxit Newton steps.
+// Returns 0 converged, 1 not converged, 2 not finite.
+int jfnk_solve(tg_ctx *C, JfnkWork &W, const std::function<void(const double *, double *)> &Feval, double atol, double rtol,
+               int maxit, int &newton, int &linear, double &fn_out)
 {
-    CnWork &W = work(C);
-    const int64_t n = 3 * C->g.size();
-    const double scale = C->it > C->cfg.it_start ? 0.5 : 1.0;
-    cn_build_bu(C, W.bu, C->it > C->cfg.it_start);
-    TG_CUDA(cudaMemcpyAsync(W.U.x, C->s.ucont_o.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
-    cn_eval(C, W, W.U, W.F, scale);
-    double fn = std::sqrt(dot(C, W, W.F.x, W.F.x, n));
+    const int64_t n = W.n;
+    Feval(W.U, W.F);
+    double fn = std::sqrt(dot(C, W, W.F, W.F, n));
     const double f0 = fn;
-    const double atol = C->cfg.snes_atol, rtol = C->cfg.snes_rtol;
-    const int maxit = C->cfg.snes_maxit > 0 ? C->cfg.snes_maxit : 20;
     const double erel = std::sqrt(2.220446049250313e-16);
     const int m = W.m;
     auto Vk = [&](int k) { return W.V + (size_t)k * n; };
-    int newton = 0, linear = 0, rc = 0;
+    newton = 0;
+    linear = 0;
+    int rc = 0;
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     while (!(fn <= std::max(atol, rtol * f0)) && newton < maxit) {
         if (!std::isfinite(fn)) { rc = 2; break; }
         // GMRES(m) on J d = -F from d = 0, to 1e-3 relative residual (inexact Newton)
-        const double unorm = std::sqrt(dot(C, W, W.U.x, W.U.x, n));
-        double *d = W.W.x;                                  // accumulated correction (reuse of W)
+        const double unorm = std::sqrt(dot(C, W, W.U, W.U, n));
+        double *d = W.W;                                    // accumulated correction
         TG_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, C->stream));
         const double beta0 = fn, tol = 1e-3 * fn;
         double res = beta0;
@@ -158,18 +175,18 @@ int solve_u_cn(tg_ctx *C, tg_stats *st)
             // r = -F - J d (J d = 0 on the first cycle)
             double *v0 = Vk(0);
             if (cycle == 0) {
-                k_axpby<<<nblk(n), DB, 0, C->stream>>>(n, -1.0, W.F.x, 0.0, v0);
+                k_axpby<<<nblk(n), DB, 0, C->stream>>>(n, -1.0, W.F, 0.0, v0);
             } else {
                 // J d by differencing
                 const double dn = std::sqrt(dot(C, W, d, d, n));
                 const double h = erel * std::sqrt(1.0 + unorm) / dn;
-                V3f<double> UP{Vk(m), Vk(m) + n / 3, Vk(m) + 2 * (n / 3)};
-                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, UP.x, W.U.x, h, d);
-                cn_eval(C, W, UP, W.FW, scale);
+                double *UP = Vk(m);
+                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, UP, W.U, h, d);
+                Feval(UP, W.FW);
                 linear++;
                 // v0 = -F - (FW - F) / h
-                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, v0, W.FW.x, -1.0, W.F.x);
-                k_axpby<<<nblk(n), DB, 0, C->stream>>>(n, -1.0, W.F.x, -1.0 / h, v0);
+                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, v0, W.FW, -1.0, W.F);
+                k_axpby<<<nblk(n), DB, 0, C->stream>>>(n, -1.0, W.F, -1.0 / h, v0);
             }
             double beta = std::sqrt(dot(C, W, v0, v0, n));
             if (!(beta > 0)) break;
@@ -181,11 +198,10 @@ int solve_u_cn(tg_ctx *C, tg_stats *st)
                 // w = J v_k
                 double *w = Vk(kk + 1);
                 const double h = erel * std::sqrt(1.0 + unorm);        // |v_k| = 1
-                V3f<double> UP{w, w + n / 3, w + 2 * (n / 3)};
-                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, w, W.U.x, h, Vk(kk));
-                cn_eval(C, W, UP, W.FW, scale);
+                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, w, W.U, h, Vk(kk));
+                Feval(w, W.FW);
                 linear++;
-                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, w, W.FW.x, -1.0, W.F.x);
+                k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, w, W.FW, -1.0, W.F);
                 k_axpby<<<nblk(n), DB, 0, C->stream>>>(n, 0.0, w, 1.0 / h, w);
                 // modified Gram-Schmidt
                 for (int q = 0; q <= kk; q++) {
@@ -220,23 +236,51 @@ int solve_u_cn(tg_ctx *C, tg_stats *st)
         }
         // Newton step, halved while |F| does not decrease
         double lam = 1.0, fnew = 0.0;
-        V3f<double> UT{Vk(m), Vk(m) + n / 3, Vk(m) + 2 * (n / 3)};
+        double *UT = Vk(m);
         for (int ls = 0; ls < 8; ls++) {
-            k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, UT.x, W.U.x, lam, d);
-            cn_eval(C, W, UT, W.FW, scale);
-            fnew = std::sqrt(dot(C, W, W.FW.x, W.FW.x, n));
+            k_waxpy<<<nblk(n), DB, 0, C->stream>>>(n, UT, W.U, lam, d);
+            Feval(UT, W.FW);
+            fnew = std::sqrt(dot(C, W, W.FW, W.FW, n));
             if (fnew < fn || !std::isfinite(fnew)) break;
             lam *= 0.5;
         }
-        TG_CUDA(cudaMemcpyAsync(W.U.x, UT.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
-        TG_CUDA(cudaMemcpyAsync(W.F.x, W.FW.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+        TG_CUDA(cudaMemcpyAsync(W.U, UT, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+        TG_CUDA(cudaMemcpyAsync(W.F, W.FW, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
         fn = fnew;
         newton++;
     }
     if (!std::isfinite(fn)) rc = 2;
     else if (rc == 0 && !(fn <= std::max(atol, rtol * f0))) rc = 1;
+    fn_out = fn;
+    return rc;
+}
+
+JfnkWork *jfnk_alloc(tg_ctx *C, int64_t n, int m)
+{
+    JfnkWork *W = new JfnkWork();
+    jfnk_init(C, *W, n, m);
+    return W;
+}
+
+void jfnk_free(JfnkWork *W) { delete W; }   // device buffers are owned by the context allocation list
+
+double *jfnk_u(JfnkWork *W) { return W->U; }
+
+// UeqnSNES (ueqn_solvers.c:1087-1199): Ucont <- the root of F from Ucont_o
+int solve_u_cn(tg_ctx *C, tg_stats *st)
+{
+    CnWork &W = work(C);
+    const int64_t n = 3 * C->g.size();
+    const double scale = C->it > C->cfg.it_start ? 0.5 : 1.0;
+    cn_build_bu(C, W.bu, C->it > C->cfg.it_start);
+    TG_CUDA(cudaMemcpyAsync(W.j.U, C->s.ucont_o.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+    const int maxit = C->cfg.snes_maxit > 0 ? C->cfg.snes_maxit : 20;
+    int newton = 0, linear = 0;
+    double fn = 0.0;
+    const int rc = jfnk_solve(C, W.j, [&](const double *U, double *F) { cn_eval(C, W, U, F, scale); }, C->cfg.snes_atol,
+                              C->cfg.snes_rtol, maxit, newton, linear, fn);
     // Ucont <- U (SNESFuncEval left the last evaluated point in the state)
-    TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, W.U.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+    TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, W.j.U, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
     C->mom_outer = newton;
     C->mom_inner = linear;
     C->mom_res = fn;

@@ -110,6 +110,7 @@ struct Farm;         // tg_farm.cu
 struct CnWork;       // tg_cn.cu
 struct ImexWork;     // tg_imex.cu
 struct GmresWork;    // tg_imex.cu
+struct JfnkWork;     // tg_cn.cu
 
 // per-kernel event timing (tosca_gpu_prof.h)
 struct ProfPending { int slot; cudaEvent_t a, b; };
@@ -179,6 +180,8 @@ struct tg_ctx {
     tg::GmresWork *tgm = nullptr;        // GMRES work of the ABBE temperature solve (tg_teqn.cu)
     double *tconv = nullptr, *tconv_o = nullptr;   // teqn->RhsConv, RhsConv_o (ABBE)
     int t_its = 0;                       // GMRES iterations of the last ABBE temperature solve
+    tg::JfnkWork *tsn = nullptr;         // Newton-Krylov work of the BE/BDF2 temperature solve (tg_teqn.cu)
+    double *tmprt_oo = nullptr;          // teqn->Tmprt_oo (BDF2)
     // last implicit momentum solve: Newton steps or IMEX stages, Krylov
     // operator products, last Krylov residual estimate
     int mom_outer = 0, mom_inner = 0;
@@ -293,6 +296,13 @@ void adj_graph_destroy(tg_ctx *C);
 // temperature transport (tg_teqn.cu)
 // Crank-Nicolson momentum step (tg_cn.cu)
 int solve_u_cn(tg_ctx *C, tg_stats *st);
+// Jacobian-free Newton-Krylov root of F, Feval(U, F) (tg_cn.cu): the guess and
+// the root in the work's U
+JfnkWork *jfnk_alloc(tg_ctx *C, int64_t n, int m);
+void jfnk_free(JfnkWork *W);
+double *jfnk_u(JfnkWork *W);
+int jfnk_solve(tg_ctx *C, JfnkWork &W, const std::function<void(const double *, double *)> &Feval, double atol, double rtol,
+               int maxit, int &newton, int &linear, double &fn_out);
 void cn_destroy(tg_ctx *C);
 bool imex_scheme(int ddt);                                         // tg_imex.cu
 // restarted GMRES as PETSc's KSPGMRES (tg_imex.cu): A(v, Av) writes A v

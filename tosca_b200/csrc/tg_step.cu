@@ -1591,8 +1591,11 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     const int64_t G = C->g.size();
     TG_CUDA(cudaMemcpyAsync(C->s.ucont_o.x, C->s.ucont.x, 3 * sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
     if (C->taping) tape_step_start(C);
-    if (C->prm.teqn)                    // main.c:83-99 (RK4: Tmprt_o = Tmprt)
+    if (C->prm.teqn) {                  // main.c:83-99: (BDF2: Tmprt_oo = Tmprt_o,) Tmprt_o = Tmprt
+        if (C->cfg.t_ddt_scheme == TG_TDDT_BDF2)
+            TG_CUDA(cudaMemcpyAsync(C->tmprt_oo, C->s.tmprt_o, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         TG_CUDA(cudaMemcpyAsync(C->s.tmprt_o, C->s.tmprt, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    }
     if (C->prm.les) { update_nut(C); update_wall_models(C); }
     if (C->taping) tape_nut(C);
     if (C->prm.farm) farm_update(C);
@@ -1638,7 +1641,7 @@ static bool graph_eligible(const tg_ctx *C)
     const bool wall = C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN;
     return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
            C->cfg.ddt_scheme != TG_DDT_CN && !imex_scheme(C->cfg.ddt_scheme) &&   // host-driven Krylov loops
-           !(C->prm.teqn && C->cfg.t_ddt_scheme == TG_TDDT_ABBE) &&
+           !(C->prm.teqn && C->cfg.t_ddt_scheme != TG_TDDT_RK4) &&
            C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 

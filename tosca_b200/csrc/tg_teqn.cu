@@ -175,6 +175,19 @@ __global__ void k_t_abbe_b(int64_t n, double *b, double *x, const double *conv, 
     }
 }
 
+// SNESFuncEvalT tail (teqn_solvers.c:688-711): F = dt FormT(T) (zero off the
+// interior) - T + T_o, or with BDF2 - 3/2 T + 2 T_o - 1/2 T_oo
+__global__ void k_t_snes_f(int64_t n, double *F, const double *rhs, const double *t, const double *to, const double *too,
+                           double dt, int bdf2)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        double r = rhs[q] * dt;
+        if (bdf2) { r = r + (-3.0 / 2.0) * t[q]; r = r + 2.0 * to[q]; r = r + (-1.0 / 2.0) * too[q]; }
+        else { r = r + -1.0 * t[q]; r = r + 1.0 * to[q]; }
+        F[q] = r;
+    }
+}
+
 // ABBEMatVec tail (teqn_solvers.c:930-943): Av = v - dt D(v), D(v) zero off the interior
 __global__ void k_t_abbe_av(int64_t n, double *Av, const double *v, const double *d, double dt)
 {
@@ -262,14 +275,50 @@ static int solve_t_abbe(tg_ctx *C)
     return rc;
 }
 
-// SolveTEqn (teqn.c:259-276) with TeqnRK4 (teqn_solvers.c:714-818) or
-// TeqnABBE; returns the implicit solve's status (0 for RK4)
+// SolveTEqn with TeqnSNES (teqn_solvers.c:596-712; bT = 0 without
+// hyperviscosity or controller): the root of SNESFuncEvalT from T_o by the
+// Newton-Krylov solver of the Crank-Nicolson momentum step (jfnk_solve; the
+// reference uses SNESNEWTONTR with MATMFFD products: converged tightly, the
+// root does not depend on the path), -absTolT / -relTolT, 20 Newton steps
+static int solve_t_snes(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const int64_t G = g.size();
+    State &s = C->s;
+    const double dt = C->prm.dt;
+    const int bdf2 = (C->cfg.t_ddt_scheme == TG_TDDT_BDF2 && C->it > C->cfg.it_start) ? 1 : 0;
+    if (!C->tsn) C->tsn = jfnk_alloc(C, G, C->cfg.t_gmres_restart > 0 ? C->cfg.t_gmres_restart : 30);
+    double *T = jfnk_u(C->tsn);
+    TG_CUDA(cudaMemcpyAsync(T, s.tmprt_o, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    auto Feval = [&](const double *t, double *F) {
+        TG_CUDA(cudaMemcpyAsync(s.tmprt, t, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+        reset_cell_periodic_s(C, s.tmprt);
+        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 0));
+        TG_PROF(C, "teqn_snes_f", k_t_snes_f<<<nblk(G), 256, 0, C->stream>>>(G, F, s.trhs, t, s.tmprt_o,
+                                                                           bdf2 ? C->tmprt_oo : s.tmprt_o, dt, bdf2));
+    };
+    int newton = 0, linear = 0;
+    double fn = 0.0;
+    const int rc = jfnk_solve(C, *C->tsn, Feval, C->cfg.t_atol, C->cfg.t_rtol, 20, newton, linear, fn);
+    TG_CUDA(cudaMemcpyAsync(s.tmprt, T, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
+    C->t_its = linear;
+    return rc;
+}
+
+// SolveTEqn (teqn.c:259-276) with TeqnRK4 (teqn_solvers.c:714-818),
+// TeqnABBE or TeqnSNES; returns the implicit solve's status (0 for RK4)
 int solve_t(tg_ctx *C)
 {
     const Grid g = C->g;
     const int64_t G = g.size();
     State &s = C->s;
     const double dt = C->prm.dt;
+    if (C->cfg.t_ddt_scheme == TG_TDDT_BE || C->cfg.t_ddt_scheme == TG_TDDT_BDF2) {
+        const int rc = solve_t_snes(C);
+        reset_cell_periodic_s(C, s.tmprt);
+        return rc;
+    }
     if (C->cfg.t_ddt_scheme == TG_TDDT_ABBE) {
         const int rc = solve_t_abbe(C);
         reset_cell_periodic_s(C, s.tmprt);
