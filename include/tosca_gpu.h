@@ -107,9 +107,9 @@ typedef struct tg_config {
     int32_t device;                /* CUDA device ordinal (ignored by the CPU restatement)  */
     int32_t source;                /* body force TG_F_SOURCE added by sourceU               */
                                    /* (ueqn_sources.c:2884-2980, ueqn_solvers.c:1369)       */
-    /* temperature transport (SolveTEqn, teqn.c:259; RK4 only): with teqn = 1
-     * the temperature TG_F_TMPRT is advanced after the projection and the
-     * buoyancy of the next step reads it */
+    /* temperature transport (SolveTEqn, teqn.c:259; scheme t_ddt_scheme,
+     * independent of ddt_scheme): with teqn = 1 the temperature TG_F_TMPRT is
+     * advanced after the projection and the buoyancy of the next step reads it */
     int32_t teqn;
     int32_t t_bc[6];               /* TG_TBC_* per patch (periodic where bc is periodic)    */
     double  prandtl;               /* -Pr: molecular Prandtl number (no LES)                */

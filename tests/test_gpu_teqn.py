@@ -73,3 +73,25 @@ def test_implicit_temperature_matches_oracle(les, scheme, rtol):
     assert rel_l2(g.get("P"), o.get("P")) < 1e-9
     assert g.graph_info()[0] == 0          # the Krylov loops run on the host
     g.close(); o.close()
+
+
+@pytest.mark.parametrize("ddt,tddt", [(api.DDT_CN, api.TDDT_BDF2), (api.DDT_ABCN, api.TDDT_ABBE)])
+def test_temperature_with_implicit_momentum(ddt, tddt):
+    # the temperature and momentum schemes are independent (-dTdtScheme,
+    # -dUdtScheme): implicit pairs against the oracle after 3 steps
+    cfg, nodes, ucat, p, T = cases.hill_case(teqn=True, t_amp=0.5, nx=24, ny=12, nz=12)
+    cfg.poisson_rtol = 1e-13
+    cfg.ddt_scheme, cfg.t_ddt_scheme = ddt, tddt
+    cfg.snes_atol, cfg.snes_rtol, cfg.snes_maxit = 0.0, 1e-13, 30
+    cfg.t_atol, cfg.t_rtol = 0.0, 1e-10 if tddt == api.TDDT_BDF2 else 1e-13
+    out = []
+    for make in (tosca_b200.gpu_solver, oracle.solver):
+        s = make(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        s.step(3)
+        out.append(s)
+    g, o = out
+    for f in ("TMPRT", "UCAT", "UCONT"):
+        assert rel_l2(g.get(f), o.get(f)) < 1e-10, f
+    assert rel_l2(g.get("P"), o.get("P")) < 1e-9
+    g.close(); o.close()
