@@ -130,6 +130,10 @@ typedef struct tg_config {
     int32_t t_gmres_restart;
     double  t_atol;
     double  t_rtol;
+    /* -pTildeBuoyancy 1 (teqn.c:38-57): the buoyancy term is ghGradRhoK,
+     * g z grad((tRef - T)/tRef) at the faces (teqn.c:278-652), in place of
+     * Buoyancy; needs buoyancy = 1 */
+    int32_t p_tilde;
 } tg_config;
 
 /* per-call statistics */

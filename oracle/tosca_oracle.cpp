@@ -1007,11 +1007,13 @@ void updateWallModels(tg_ctx &C)
 // ---------------------------------------------------------------------------
 // GradP, peqn.c:3437-3773
 // ---------------------------------------------------------------------------
-void gradP(tg_ctx &C)
+// the GradP stencil applied to the scalar val(q) into outv
+template <class Val>
+void gradField(tg_ctx &C, Val val, std::vector<V3> &outv)
 {
     const int mx = C.mx, my = C.my, mz = C.mz;
-    std::fill(C.dp.begin(), C.dp.end(), V3{0, 0, 0});
-    auto P = [&](int k, int j, int i) { return C.p[C.I(k, j, i)]; };
+    std::fill(outv.begin(), outv.end(), V3{0, 0, 0});
+    auto P = [&](int k, int j, int i) { return val(C.I(k, j, i)); };
     #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 1; k < mz - 1; k++)
     for (int j = 1; j < my - 1; j++)
@@ -1056,7 +1058,30 @@ void gradP(tg_ctx &C)
         if (!C.pi && i == mx - 2) out.x = 0;
         if (!C.pj && j == my - 2) out.y = 0;
         if (!C.pk && k == mz - 2) out.z = 0;
-        C.dp[c] = out;
+        outv[c] = out;
+    }
+}
+
+void gradP(tg_ctx &C)
+{
+    gradField(C, [&](size_t q) { return C.p[q]; }, C.dp);
+}
+
+// ghGradRhoK, teqn.c:278-652 (-pTildeBuoyancy 1): the GradP stencil on
+// rho_k = (tRef - T) / tRef scaled by g z of the cell's node, stored negated in
+// bTheta so that the AB2 buoyancy sum of ExplicitRhsU (+3/2 b - 1/2 b_o) reads
+// -3/2 ghGradRhok + 1/2 ghGradRhok_o (ueqn_solvers.c:1314-1324)
+void ghGradRhoK(tg_ctx &C)
+{
+    const double tRef = C.c.t_ref;
+    std::vector<V3> db(C.G);
+    gradField(C, [&](size_t q) { return (tRef - C.tmprt[q]) / tRef; }, db);
+    for (int k = 1; k < C.mz - 1; k++)
+    for (int j = 1; j < C.my - 1; j++)
+    for (int i = 1; i < C.mx - 1; i++) {
+        const size_t c = C.I(k, j, i);
+        const double gz = -9.81 * C.coor[c].z;
+        C.btheta[c] = mk(-(gz * db[c].x), -(gz * db[c].y), -(gz * db[c].z));
     }
 }
 
@@ -1581,7 +1606,7 @@ int step(tg_ctx &C, tg_stats *st)
     gradP(C);                                            // main.c:160-167
     if (C.c.buoyancy) {                                  // main.c:175-192
         if (C.it > C.c.it_start) C.btheta_o = C.btheta;
-        buoyancy(C);
+        if (C.c.p_tilde) ghGradRhoK(C); else buoyancy(C);   // main.c:176-181
     }
     const int urc = solveUEqn(C);                        // main.c:195
     int rc = solvePEqn(C, st);                           // main.c:198
@@ -1710,6 +1735,7 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
         cfg->bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN) return TG_ERR_BAD_ARG;
     if (cfg->dt <= 0 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
+    if (cfg->p_tilde && !cfg->buoyancy) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (!(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
         if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;
@@ -1866,7 +1892,7 @@ TOR_STAGE(tor_contravariant_to_cartesian, contravariantToCartesian(*C); resetCel
 TOR_STAGE(tor_update_nut, updateNut(*C))
 TOR_STAGE(tor_update_wall_models, updateWallModels(*C))
 TOR_STAGE(tor_grad_p, gradP(*C))
-TOR_STAGE(tor_buoyancy, buoyancy(*C))
+TOR_STAGE(tor_buoyancy, (C->c.p_tilde ? ghGradRhoK(*C) : buoyancy(*C)))
 TOR_STAGE(tor_explicit_rhs, explicitRhsU(*C))
 TOR_STAGE(tor_solve_u, solveUEqn(*C))
 TOR_STAGE(tor_update_cartesian_bcs, updateCartesianBCs(*C))

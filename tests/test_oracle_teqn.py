@@ -96,3 +96,24 @@ def test_temperature_scheme_checked():
     cfg.t_ddt_scheme = 4
     with pytest.raises(api.TgError):
         oracle.solver(cfg)
+
+
+def test_p_tilde_buoyancy():
+    # ghGradRhoK vanishes for T = tRef, is finite and non-zero for the
+    # stratified hill, and needs the buoyancy switch
+    cfg, nodes, ucat, p, T = cases.hill_case(teqn=True, t_amp=0.5, nx=16, ny=8, nz=8)
+    cfg.p_tilde = 1
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, np.full_like(T, cfg.t_ref))
+    s.Buoyancy()
+    # the top patch has a fixed lapse-rate gradient: its ghosts differ from tRef
+    assert np.abs(s.get("BTHETA")[:, 1:-3]).max() == 0.0
+    s.set("TMPRT", T)
+    s.Buoyancy()
+    b = s.get("BTHETA")
+    assert np.isfinite(b).all() and np.abs(b).max() > 0
+    s.step(2)
+    s.close()
+    cfg.buoyancy = 0
+    with pytest.raises(api.TgError):
+        oracle.solver(cfg)

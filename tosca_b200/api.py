@@ -76,6 +76,7 @@ class TgConfig(C.Structure):
         ("t_gmres_restart", C.c_int32),
         ("t_atol", C.c_double),
         ("t_rtol", C.c_double),
+        ("p_tilde", C.c_int32),
     ]
 
 
@@ -171,6 +172,7 @@ class Config:
     t_gmres_restart: int = 30
     t_atol: float = 1e-5
     t_rtol: float = 1e-30
+    p_tilde: int = 0
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

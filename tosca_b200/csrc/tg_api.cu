@@ -209,6 +209,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
     if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
+    if (cfg->p_tilde && !cfg->buoyancy) return TG_ERR_BAD_ARG;
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (!(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
@@ -321,6 +322,11 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
         TG_CUDA(cudaStreamSynchronize(C->stream));
         metrics_from_nodes(C, dn);
         refresh_filter(C);
+        if (C->cfg.p_tilde) {
+            if (!C->node_z) C->node_z = dallocd(C, G);
+            TG_CUDA(cudaMemcpy2DAsync(C->node_z, sizeof(double), dn + 2, 3 * sizeof(double), sizeof(double), G,
+                                      cudaMemcpyDeviceToDevice, C->stream));
+        }
         C->met32_stale = true;
         // orthogonality: every cross term of the face metric tensor vanishes
         std::vector<double> h(G);

@@ -182,6 +182,7 @@ struct tg_ctx {
     int t_its = 0;                       // GMRES iterations of the last ABBE temperature solve
     tg::JfnkWork *tsn = nullptr;         // Newton-Krylov work of the BE/BDF2 temperature solve (tg_teqn.cu)
     double *tmprt_oo = nullptr;          // teqn->Tmprt_oo (BDF2)
+    double *node_z = nullptr;            // z of node (k, j, i) (ghGradRhoK, p_tilde)
     // last implicit momentum solve: Newton steps or IMEX stages, Krylov
     // operator products, last Krylov residual estimate
     int mom_outer = 0, mom_inner = 0;

@@ -452,15 +452,24 @@ __global__ void k_wall_stress(Grid g, Metrics m, State s, Params p, const double
 // GradP (peqn.c:3437-3773): face pressure gradient with the metric tensor,
 // one-sided cross derivatives only at the corner faces. Interior cells.
 // ------------------------------------------------------------------------
-template <class M>
-__global__ void k_grad_p(Grid g, FaceMet<M> m, State s, bool ax)
+// GH = true: ghGradRhoK (teqn.c:278-652, -pTildeBuoyancy 1), the same
+// stencil applied to rho_k = (tRef - T) / tRef and scaled by g z of the cell's
+// node (g = -9.81), stored negated in bTheta so that ExplicitRhsU's AB2
+// buoyancy sum +3/2 b - 1/2 b_o reads -3/2 ghGradRhok + 1/2 ghGradRhok_o
+// (ueqn_solvers.c:1314-1324); the products are associated as (g z) (grad .
+// S) aj, the reference's g z (grad . S) aj up to rounding
+template <class M, bool GH = false>
+__global__ void k_grad_p(Grid g, FaceMet<M> m, State s, bool ax, const double *node_z = nullptr, double t_ref = 0.0)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y * blockDim.y + threadIdx.y + 1, k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
     int c = g.lin(k, j, i);
-    auto P = [&](int kk, int jj, int ii) { return s.p[g.id(kk, jj, ii)]; };
+    auto P = [&](int kk, int jj, int ii) {
+        const double v = GH ? s.tmprt[g.id(kk, jj, ii)] : s.p[g.id(kk, jj, ii)];
+        return GH ? (t_ref - v) / t_ref : v;
+    };
     const int mx = g.mx, my = g.my, mz = g.mz;
-    if (ax) {
+    if (ax && !GH) {
         // axis-aligned mesh: the cross terms g12, g13, g21, g23, g31, g32 vanish
         // the + neighbours lie inside the DMDA except across a periodic seam,
         // where index m + 1 wraps to 1
@@ -511,6 +520,11 @@ __global__ void k_grad_p(Grid g, FaceMet<M> m, State s, bool ax)
     if (!g.pi && i == mx - 2) ox = 0;
     if (!g.pj && j == my - 2) oy = 0;
     if (!g.pk && k == mz - 2) oz = 0;
+    if (GH) {
+        const double gz = -9.81 * node_z[c];
+        s.btheta.x[c] = -(gz * (double)ox); s.btheta.y[c] = -(gz * (double)oy); s.btheta.z[c] = -(gz * (double)oz);
+        return;
+    }
     s.dp.x[c] = (double)ox; s.dp.y[c] = (double)oy; s.dp.z[c] = (double)oz;
 }
 
@@ -1326,7 +1340,13 @@ void grad_p(tg_ctx *C)
     else TG_PROF(C, "grad_p", k_grad_p<double><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s, C->axis_aligned));
 }
 
-void buoyancy(tg_ctx *C) { k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm); }
+void buoyancy(tg_ctx *C)
+{
+    if (C->cfg.p_tilde)   // ghGradRhoK (teqn.c:278), FP64
+        TG_PROF(C, "gh_grad_rhok", (k_grad_p<double, true><<<gi(C->g), block3(), 0, C->stream>>>(C->g, C->fm64, C->s, false, C->node_z, C->prm.t_ref)));
+    else
+        k_buoyancy<<<ga(C->g), block3(), 0, C->stream>>>(C->g, C->m, C->s, C->prm);
+}
 
 // FormU pass 1 (face fluxes) at the precision of the context's policy.
 // Pass 2 (k_cell_fp) follows; the flux planes are only read at the points
