@@ -119,6 +119,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.path = None
+        self.skip = 0          # samples written before the region began
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -129,6 +130,18 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait (at most 5 s) for its first
+        # sample so that the sampling covers the region from its start; that
+        # sample, taken before the region, is used only if no later one exists
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            with open(self.path) as f:
+                n = sum(1 for _ in f)
+            if n > 0:
+                self.skip = n
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
@@ -144,7 +157,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = open(self.path).read().splitlines()
+        if len(lines) > self.skip:
+            lines = lines[self.skip:]
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
