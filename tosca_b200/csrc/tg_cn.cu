@@ -14,6 +14,9 @@
 // argument in SNESFuncEval (ueqn_solvers.c:1258), which leaves the term out of
 // F and corrupts the residual stored for the matrix-free products; here the
 // term is part of bU, as in the explicit schemes.
+//
+// The Newton-Krylov iteration (jfnk_solve) takes F as a callback and also
+// solves the BE/BDF2 temperature step (SNESFuncEvalT, tg_teqn.cu).
 #include <cmath>
 #include <vector>
 

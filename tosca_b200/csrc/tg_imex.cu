@@ -18,7 +18,8 @@
 // b - A x, stops on the rotated residual estimate and adds V y to x.
 // The dot products return to the host (one synchronisation per Arnoldi step
 // for the Hessenberg column, one for its norm); every vector operation runs
-// on the device over the 3 G unknowns of the face-velocity field.
+// on the device. gmres_solve takes the operator as a callback and serves the
+// ABBE temperature solve too (tg_teqn.cu, n = G instead of 3 G).
 #include <cmath>
 #include <vector>
 
