@@ -41,3 +41,22 @@ def test_cn_reports_iteration_cap():
         s.step(1)
     assert e.value.status == api.TG_ERR_NOT_CONVERGED
     s.close()
+
+
+def test_cn_mixed_close_to_fp64():
+    # the Newton residual is evaluated in FP64 in the mixed mode too (the
+    # differenced Jacobian needs it); the rest of the step runs mixed
+    cfg, nodes, ucat, p, T = build_case("abl", **SMALL["abl"])
+    cfg.ddt_scheme = api.DDT_CN
+    cfg.snes_atol, cfg.snes_rtol, cfg.snes_maxit = 0.0, 1e-12, 30
+    res = []
+    for prec in (api.PREC_FP64, api.PREC_MIXED):
+        cfg.precision = prec
+        s = tosca_b200.gpu_solver(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        st = s.step(3)
+        res.append((s.get("UCAT"), st.max_divergence, s.momentum_info()))
+        s.close()
+    assert rel_l2(res[1][0], res[0][0]) < 1e-6
+    assert res[1][1] < 1e-8
+    assert res[1][2][0] <= res[0][2][0] + 1          # Newton steps as in FP64

@@ -280,8 +280,14 @@ int solve_u_cn(tg_ctx *C, tg_stats *st)
     const int maxit = C->cfg.snes_maxit > 0 ? C->cfg.snes_maxit : 20;
     int newton = 0, linear = 0;
     double fn = 0.0;
+    // F is evaluated in FP64 in every precision mode: the differenced
+    // Jacobian-vector products divide F's change over h ~ 1e-8 |U|, below
+    // the rounding of an FP32 residual
+    const auto pol = C->pol;
+    C->pol = decltype(C->pol){};
     const int rc = jfnk_solve(C, W.j, [&](const double *U, double *F) { cn_eval(C, W, U, F, scale); }, C->cfg.snes_atol,
                               C->cfg.snes_rtol, maxit, newton, linear, fn);
+    C->pol = pol;
     // Ucont <- U (SNESFuncEval left the last evaluated point in the state)
     TG_CUDA(cudaMemcpyAsync(C->s.ucont.x, W.j.U, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
     C->mom_outer = newton;
