@@ -134,6 +134,10 @@ typedef struct tg_config {
      * g z grad((tRef - T)/tRef) at the faces (teqn.c:278-652), in place of
      * Buoyancy; needs buoyancy = 1 */
     int32_t p_tilde;
+    /* initial guess of each pressure solve: 0 the previous solution (the
+     * reference's, peqn.c:3885), 1 its linear, 2 (default) its quadratic
+     * extrapolation from the previous two or three solutions; -1 = 2 */
+    int32_t poisson_guess;
 } tg_config;
 
 /* per-call statistics */

@@ -143,3 +143,20 @@ def test_mixed_precision_against_fp64_oracle(name):
         assert rel_l2(u_g[..., c], u_o[..., c]) < 1e-6, c
     assert rel_l2(g.get("P"), o.get("P")) < 1e-6
     assert sg.max_divergence < 1e-8
+
+
+def test_poisson_guess_orders():
+    # the initial guess of each pressure solve (the previous solution as the
+    # reference, or its linear / quadratic extrapolation) changes the Krylov
+    # path, not the converged step
+    out = {}
+    for order in (0, 1, 2):
+        g, o = pair("abl", dict(TIGHT, ddt_scheme=1, poisson_guess=order), **SMALL["abl"])
+        st = g.step(6)
+        out[order] = (g.get("UCAT"), g.get("P"), st.poisson_total_iterations)
+        g.close(); o.close()
+    for order in (1, 2):
+        assert rel_l2(out[order][0], out[0][0]) < 1e-10
+        assert rel_l2(out[order][1], out[0][1]) < 1e-9
+    # (at this tight tolerance the extrapolations save no iterations; on the
+    # benchmark's divergence-bound stop the quadratic one does)

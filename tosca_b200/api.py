@@ -77,6 +77,7 @@ class TgConfig(C.Structure):
         ("t_atol", C.c_double),
         ("t_rtol", C.c_double),
         ("p_tilde", C.c_int32),
+        ("poisson_guess", C.c_int32),
     ]
 
 
@@ -173,6 +174,7 @@ class Config:
     t_atol: float = 1e-5
     t_rtol: float = 1e-30
     p_tilde: int = 0
+    poisson_guess: int = 2
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

@@ -244,9 +244,9 @@ __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
 // extrapolation), 2 x_n - x_{n-1} while only two are known, x_n with one;
 // the history shifts (xprev2 <- xprev <- x_n). hist: device count of the
 // solutions in the history, read here and advanced by k_hist_next
-__global__ void k_extrapolate(int64_t n, double *x, double *xprev, double *xprev2, const double *hist)
+__global__ void k_extrapolate(int64_t n, double *x, double *xprev, double *xprev2, const double *hist, int order)
 {
-    const double h = hist[0];
+    const double h = fmin(hist[0], (double)order);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const double xn = x[t], xp = xprev[t];
         if (h >= 2.0) x[t] = 3.0 * xn - 3.0 * xp + xprev2[t];
@@ -256,6 +256,7 @@ __global__ void k_extrapolate(int64_t n, double *x, double *xprev, double *xprev
     }
 }
 __global__ void k_hist_next(double *hist) { hist[0] = hist[0] + 1.0; }
+inline int guess_order(const tg_ctx *C) { return C->cfg.poisson_guess < 0 ? 2 : C->cfg.poisson_guess; }
 __global__ void k_negcopy(int64_t n, const double *a, double *b)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = -a[t];
@@ -576,7 +577,7 @@ int poisson_solve(tg_ctx *C, tg_stats *st)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     TG_PROF(C, "pois_set_rhs", k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt));
-    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST);
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST, guess_order(C));
     k_hist_next<<<1, 1, 0, s>>>(C->d_scal + SC_PHIST);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);            // warm start from the previous solutions
     int rc = krylov_solve(C, st, rtol, C->cfg.poisson_div_tol, maxit);
@@ -735,7 +736,7 @@ void poisson_solve_capture(tg_ctx *C)
     const int maxit = C->cfg.poisson_maxit > 0 ? C->cfg.poisson_maxit : 500;
     const dim3 cg3 = cgrid(P.nx, P.ny, P.nz);
     k_set_rhs<<<cg3, block3(), 0, s>>>(g, C->s, P, C->prm.dt);
-    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST);
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, P.x, P.xprev, P.xprev2, C->d_scal + SC_PHIST, guess_order(C));
     k_hist_next<<<1, 1, 0, s>>>(C->d_scal + SC_PHIST);
     k_zero_at<<<1, 1, 0, s>>>(P.x, P.pin);
     krylov_capture(C, rtol, C->cfg.poisson_div_tol, maxit, SC_G);
