@@ -1736,7 +1736,7 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->dt <= 0 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->p_tilde && !cfg->buoyancy) return TG_ERR_BAD_ARG;
-    if (cfg->poisson_guess > 2) return TG_ERR_BAD_ARG;   // the CUDA solver's initial guess; the oracle starts from 0
+    if (cfg->poisson_guess > 2 || cfg->poisson_guess < -1) return TG_ERR_BAD_ARG;   // the CUDA solver's initial guess; the oracle starts from 0
     if (cfg->teqn) {
         if (!(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
         if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;

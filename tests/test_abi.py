@@ -51,11 +51,33 @@ def test_oracle_exports_same_entry_points():
         assert hasattr(lib, "tor_" + name[3:]), name
 
 
-def test_config_struct_layout():
-    # offsets of the C struct as laid out by the C compiler rules (x86-64)
-    c = api.TgConfig
-    assert c.bc.offset == 12 and c.nut_bc.offset == 36 and c.nut_bc_value.offset == 64
-    assert ctypes.sizeof(api.TgStats) == 48
+STRUCTS = {"tg_config": api.TgConfig, "tg_stats": api.TgStats, "tg_turbine": api.TgTurbine,
+           "tg_adjoint_stats": api.TgAdjointStats}
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """Every field offset and the size of each struct in the ctypes mirror
+    equal what gcc lays out from include/tosca_gpu.h."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "tosca_gpu.h"', "int main(void) {"]
+    for cname, py in STRUCTS.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in STRUCTS.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
 
 
 def test_bad_config_rejected_by_oracle():
@@ -66,3 +88,9 @@ def test_bad_config_rejected_by_oracle():
     cfg = api.Config(mx=8, my=8, mz=8, bc=(api.BC_PERIODIC, api.BC_SLIP) + (api.BC_PERIODIC,) * 4)
     with pytest.raises(api.TgError):
         oracle.solver(cfg)
+    # order of the extrapolated pressure guess: -1 (default), 0, 1 or 2
+    for bad in (3, -2, -7):
+        with pytest.raises(api.TgError):
+            oracle.solver(api.Config(mx=8, my=8, mz=8, poisson_guess=bad))
+    for good in (-1, 0, 1, 2):
+        oracle.solver(api.Config(mx=8, my=8, mz=8, poisson_guess=good)).close()

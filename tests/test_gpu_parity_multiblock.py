@@ -1,0 +1,129 @@
+"""Oracle parity at sizes that span several blocks of every kernel in every
+direction, several multigrid levels and several line-solver chunks.
+
+ABL 64 x 64 x 32 cells (DMDA 66 x 34 x 66): the face-flux tile is 32 cells
+wide in i, so i holds two full blocks plus the periodic seam; LES, the
+Schumann wall stress and the mean pressure gradient are on (FormU,
+ueqn_solvers.c:173-993; wall stress :548-558). Hill 96 x 48 x 48: curvilinear
+metrics, QUICK, Boussinesq buoyancy and the transported temperature.
+
+Bars: u, v, w and p within 1e-10 relative L2 after 10 steps; the GPU's
+max|div| (ContinuityErrorsOptimized, peqn.c:4114-4181) at or below the
+oracle's plus a 1e-14 floor; the mixed-precision step within 1e-6 of the FP64
+oracle; and the drop-in call tg_step_host on TOSCA's local ghosted arrays
+(halo = 3, mesh.c:42) against the oracle's step."""
+import numpy as np
+import pytest
+
+import oracle
+import tosca_b200
+from tosca_b200 import api, cases
+from tests.common import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ABL_MB = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=300.0)
+HILL_MB = dict(nx=96, ny=48, nz=48)
+DIV_FLOOR = 1e-14
+
+
+def _make(name, rtol=1e-13, **over):
+    if name == "abl":
+        cfg, nodes, ucat, p = cases.abl_case(ddt=api.DDT_RK4, **ABL_MB)
+        T = None
+    else:
+        cfg, nodes, ucat, p, T = cases.hill_case(ddt=api.DDT_RK4, teqn=True, t_amp=0.5, **HILL_MB)
+    cfg.poisson_rtol = rtol
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    return cfg, nodes, ucat, p, T
+
+
+def _pair(name, gpu_over=None, **over):
+    cfg, nodes, ucat, p, T = _make(name, **over)
+    o = oracle.solver(cfg)
+    cases.setup(o, nodes, ucat, p, T)
+    if gpu_over:
+        for k, v in gpu_over.items():
+            setattr(cfg, k, v)
+    g = tosca_b200.gpu_solver(cfg)
+    cases.setup(g, nodes, ucat, p, T)
+    return g, o
+
+
+def _check_fields(g, o, tol, with_t=False):
+    u_g, u_o = g.get("UCAT"), o.get("UCAT")
+    for c in range(3):
+        assert rel_l2(u_g[..., c], u_o[..., c]) < tol, ("UCAT", c)
+    assert rel_l2(g.get("P"), o.get("P")) < tol, "P"
+    if with_t:
+        assert rel_l2(g.get("TMPRT"), o.get("TMPRT")) < tol, "TMPRT"
+
+
+@pytest.mark.parametrize("name", ["abl", "hill"])
+def test_ten_steps_multiblock(name):
+    g, o = _pair(name)
+    if name == "abl":
+        assert g.mesh_info() == (True, True)          # axis-aligned kernel variants
+    else:
+        assert g.mesh_info() == (False, False)        # general curvilinear variants
+    div_g, div_o = [], []
+    for _ in range(10):
+        div_g.append(g.step(1).max_divergence)
+        div_o.append(o.step(1).max_divergence)
+    _check_fields(g, o, 1e-10, with_t=(name == "hill"))
+    assert rel_l2(g.get("UCONT"), o.get("UCONT")) < 1e-10
+    for s, (a, b) in enumerate(zip(div_g, div_o)):
+        assert a <= b + DIV_FLOOR, (s, a, b)
+    g.close(); o.close()
+
+
+def test_abl_multiblock_mixed_precision():
+    """FP32 multigrid and stencil metrics inside the FP64 outer loop: every
+    field within 1e-6 of the FP64 oracle after 10 steps, divergence <= 1e-8."""
+    g, o = _pair("abl", gpu_over=dict(precision=api.PREC_MIXED))
+    sg = g.step(10)
+    o.step(10)
+    _check_fields(g, o, 1e-6)
+    assert sg.max_divergence <= 1e-8
+    g.close(); o.close()
+
+
+def test_step_host_halo3_against_oracle():
+    """tg_step_host on host arrays in the layout of TOSCA's local ghosted Vecs
+    (extent + 3 on every side): three drop-in steps equal three oracle steps,
+    and the caller's ghost entries outside the global extent are left as they
+    were."""
+    g, o = _pair("abl")
+    h = 3
+    sentinel = 12345.0
+
+    def ghosted(a):
+        pad = ((h, h), (h, h), (h, h)) + (((0, 0),) if a.ndim == 4 else ())
+        return np.ascontiguousarray(np.pad(a, pad, constant_values=sentinel))
+
+    ucont, ucat, p = ghosted(o.get("UCONT")), ghosted(o.get("UCAT")), ghosted(o.get("P"))
+    nut = ghosted(np.zeros(g.shape))
+    for _ in range(3):
+        g.step_host(ucont, ucat, p, nut, halo=h)
+        o.step(1)
+    core = (slice(h, -h),) * 3
+    for name, arr in (("UCONT", ucont), ("UCAT", ucat)):
+        ref = o.get(name)
+        for c in range(3):
+            assert rel_l2(arr[core][..., c], ref[..., c]) < 1e-10, (name, c)
+    assert rel_l2(p[core], o.get("P")) < 1e-10
+    assert rel_l2(nut[core], o.get("NUT")) < 1e-10
+    for arr in (ucont, ucat, p, nut):
+        m = np.ones(arr.shape[:3], bool)
+        m[core] = False
+        assert np.all(arr[m] == sentinel)
+    g.close(); o.close()
+
+
+def test_create_rejects_bad_guess_order():
+    cfg, *_ = _make("abl")
+    for bad in (3, -2):
+        cfg.poisson_guess = bad
+        with pytest.raises(api.TgError):
+            tosca_b200.gpu_solver(cfg)

@@ -26,10 +26,23 @@ def _bind():
     return fn
 
 
-def test_noalloc_divergence_matches_context_entry_point():
+CASES = {
+    # axis-aligned ABL, square-ish planes
+    "abl": lambda: build_case("abl", **SMALL["abl"]),
+    # ragged, non-square planes (mx != my): exercises the i/j split of a plane
+    "abl_ragged": lambda: build_case("abl", nx=14, ny=18, nz=10, Lx=140.0, Ly=180.0, H=100.0),
+    # curvilinear metrics
+    "hill": lambda: build_case("hill", **SMALL["hill"]),
+    # shallow in k with large planes: each plane is split over several blocks
+    "abl_shallow": lambda: build_case("abl", nx=8, ny=64, nz=48, Lx=80.0, Ly=640.0, H=300.0),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_noalloc_divergence_matches_context_entry_point(name):
     import torch
     fn = _bind()
-    cfg, nodes, ucat, p, T = build_case("abl", **SMALL["abl"])
+    cfg, nodes, ucat, p, T = CASES[name]()
     s = tosca_b200.gpu_solver(cfg)
     cases.setup(s, nodes, ucat, p, T)
     dev = torch.device("cuda", cfg.device)

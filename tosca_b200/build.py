@@ -6,6 +6,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -33,14 +34,21 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
+    cmds = []
     for src in sources():
         obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+        cmds.append(([NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj], obj))
+
+    def compile_one(item):
+        cmd, _ = item
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    # one nvcc per translation unit, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(compile_one, cmds))
+    objs = [obj for _, obj in cmds]
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-ccbin", "/usr/bin/g++"]
     subprocess.run(cmd, check=True)
     return LIB

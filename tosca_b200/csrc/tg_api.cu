@@ -210,7 +210,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     if (cfg->dt <= 0 || cfg->div_scheme < 0 || cfg->div_scheme > 1 || cfg->ddt_scheme < 0 || cfg->ddt_scheme > TG_DDT_RK3SOCN) return TG_ERR_BAD_ARG;
     if (cfg->gmres_restart < 0 || cfg->gmres_restart > 60) return TG_ERR_BAD_ARG;
     if (cfg->p_tilde && !cfg->buoyancy) return TG_ERR_BAD_ARG;
-    if (cfg->poisson_guess > 2) return TG_ERR_BAD_ARG;
+    if (cfg->poisson_guess > 2 || cfg->poisson_guess < -1) return TG_ERR_BAD_ARG;
     if (cfg->precision != TG_PREC_FP64 && cfg->precision != TG_PREC_MIXED) return TG_ERR_BAD_ARG;
     if (cfg->teqn) {
         if (!(cfg->prandtl > 0) || (cfg->les && !(cfg->t_ref > 0))) return TG_ERR_BAD_ARG;
