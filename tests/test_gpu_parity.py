@@ -5,7 +5,7 @@ full steps to the north-star bound of 1e-10 relative L2 on u, v, w and p."""
 import numpy as np
 import pytest
 
-from tests.common import SMALL, interior, max_abs, pair, rel_l2
+from tests.common import SMALL, div_roundoff_floor, interior, max_abs, pair, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -99,14 +99,16 @@ def test_one_step(case):
 @pytest.mark.parametrize("name,ddt", [("tgv", 0), ("tgv", 1), ("abl", 0), ("hill", 0)])
 def test_ten_steps(name, ddt):
     g, o = pair(name, dict(TIGHT, ddt_scheme=ddt), **SMALL[name])
-    g.step(10)
-    o.step(10)
+    div_g = [g.step(1).max_divergence for _ in range(10)]
+    div_o = [o.step(1).max_divergence for _ in range(10)]
     u_g, u_o = g.get("UCAT"), o.get("UCAT")
     for c in range(3):
         assert rel_l2(u_g[..., c], u_o[..., c]) < 1e-10, c
     assert rel_l2(g.get("P"), o.get("P")) < 1e-10
-    # the divergence check at or below the oracle's, with a 1e-14 floor
-    assert g.last_stats.max_divergence <= o.last_stats.max_divergence + 1e-14
+    # the largest divergence of the ten steps at or below the oracle's, up to
+    # the round-off floor of the divergence sum
+    floor = div_roundoff_floor(o.get("UCONT"), o.get("AJ"))
+    assert max(div_g) <= max(div_o) + floor, (div_g, div_o, floor)
 
 
 def test_tgv_64_ten_steps_fe():

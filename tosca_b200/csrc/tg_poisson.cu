@@ -323,7 +323,8 @@ __global__ void k_bicg_x(int64_t n, const double *alpha, const double *ts, const
 }
 
 // ---- loop control of the captured CG solve (device scalars: sc[50] iteration
-// count, sc[51] first-direction flag, sc[52] converged flag). The tests are
+// count, sc[51] first-direction flag, sc[52] converged flag, sc[53] BiCGStab
+// restart after a failed true-residual check). The tests are
 // those of krylov_solve; a non-finite residual also ends the loop.
 __device__ inline bool cg_converged(const double *sc, double rtol, double divtol, double dt)
 {
@@ -335,7 +336,7 @@ __global__ void k_cg_start(double *sc, double rtol, double divtol, double dt, in
     const double bn = sqrt(sc[0]), rn = sqrt(sc[3]);
     const bool conv = cg_converged(sc, rtol, divtol, dt);
     sc[base + ST_RES0] = bn > 0 ? rn / bn : rn;
-    sc[50] = 0.0; sc[51] = 1.0; sc[52] = conv ? 1.0 : 0.0;
+    sc[50] = 0.0; sc[51] = 1.0; sc[52] = conv ? 1.0 : 0.0; sc[53] = 0.0;
     cudaGraphSetConditional(h, (!conv && maxit > 0 && isfinite(rn)) ? 1u : 0u);
 }
 __global__ void k_cg_next(double *sc, double rtol, double divtol, double dt, int maxit, cudaGraphConditionalHandle h)
@@ -518,9 +519,11 @@ static int krylov_solve(tg_ctx *C, tg_stats *st, double rtol, double divtol, int
         TG_CUDA(cudaMemsetAsync(P.p, 0, sizeof(double) * n, s));
         TG_CUDA(cudaMemsetAsync(P.v, 0, sizeof(double) * n, s));
         double *phat = P.z, *shat = P.q;
+        bool restart_pending = false;
         while (!converged() && it < maxit) {
-            if (it > 0 && (it % 50) == 0) {
+            if ((it > 0 && (it % 50) == 0) || restart_pending) {
                 // restart from the true residual (limits recursive drift)
+                restart_pending = false;
                 apply_op(C, P.x, P.r);
                 TG_PROF(C, "pois_resid", k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r));
                 k_copy<<<vblocks(n), RB, 0, s>>>(n, P.r, P.rhat);
@@ -548,6 +551,16 @@ static int krylov_solve(tg_ctx *C, tg_stats *st, double rtol, double divtol, int
             rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
             it++;
             if (!std::isfinite(rn)) break;
+            if (converged()) {
+                // the recursive residual drifts from b - L x: stop only when
+                // the true residual meets the test, else restart from it
+                apply_op(C, P.x, P.r);
+                TG_PROF(C, "pois_resid", k_resid<<<vblocks(n), RB, 0, s>>>(n, P.b, P.r));
+                dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+                read_scal(C, 3, 3);
+                rn = std::sqrt(hs[3]); rmax = hs[5] * dt;
+                if (!converged()) restart_pending = true;
+            }
         }
         ok = converged();
         // true residual (reported; it may sit slightly above the recursive one at round-off level)
@@ -636,11 +649,24 @@ __global__ void k_fill(int64_t n, double *a, double v)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) a[t] = v;
 }
-// BiCGStab restarts from the true residual every 50 iterations
-__global__ void k_bicg_restart_flag(const double *sc, cudaGraphConditionalHandle h)
+// BiCGStab restarts from the true residual every 50 iterations, and after a
+// true residual that missed the stopping test (sc[53] set); clears sc[53]
+__global__ void k_bicg_restart_flag(double *sc, cudaGraphConditionalHandle h)
 {
     const int it = (int)sc[50];
-    cudaGraphSetConditional(h, (it > 0 && (it % 50) == 0) ? 1u : 0u);
+    const bool pending = sc[53] != 0.0;
+    sc[53] = 0.0;
+    cudaGraphSetConditional(h, ((it > 0 && (it % 50) == 0) || pending) ? 1u : 0u);
+}
+// the recursive residual met the stopping test: verify it on b - L x
+__global__ void k_bicg_verify_flag(const double *sc, double rtol, double divtol, double dt, cudaGraphConditionalHandle h)
+{
+    cudaGraphSetConditional(h, cg_converged(sc, rtol, divtol, dt) ? 1u : 0u);
+}
+// after the verification: restart on the next pass if the true residual missed
+__global__ void k_bicg_mark_restart(double *sc, double rtol, double divtol, double dt)
+{
+    sc[53] = cg_converged(sc, rtol, divtol, dt) ? 0.0 : 1.0;
 }
 
 // krylov_solve for a step being captured into a CUDA graph: the iterations
@@ -648,7 +674,7 @@ __global__ void k_bicg_restart_flag(const double *sc, cudaGraphConditionalHandle
 // the device residuals, so the solve needs no host round trip per iteration.
 // The CG body is krylov_solve's iteration rotated to start with the direction
 // update (p = z on the first pass), the BiCGStab body is krylov_solve's with
-// its periodic restart as a conditional IF node; both perform the same
+// its restarts and its true-residual check as conditional IF nodes; both perform the same
 // arithmetic in the same order. Statistics go to the ST_* slots from base.
 static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit, int base)
 {
@@ -715,6 +741,15 @@ static void krylov_capture(tg_ctx *C, double rtol, double divtol, int maxit, int
             dot3v(C, P.t, P.t, nullptr, sc + 39);
             k_bicg_x<<<vb, RB, 0, a>>>(n, sc + 21, sc + 36, sc + 39, sc + 22, P.x, phat, shat, P.r, P.s, P.t);
             dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+            cudaGraphConditionalHandle hv = capture_handle(C);
+            k_bicg_verify_flag<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, hv);
+            capture_conditional(C, hv, cudaGraphCondTypeIf, C->aux[1], [&]() {
+                cudaStream_t b = C->stream;
+                apply_op(C, P.x, P.r);
+                k_resid<<<vb, RB, 0, b>>>(n, P.b, P.r);
+                dot3v(C, P.r, P.r, divtol > 0 ? P.aj : nullptr, sc + 3);
+                k_bicg_mark_restart<<<1, 1, 0, b>>>(sc, rtol, divtol, dt);
+            });
             k_cg_next<<<1, 1, 0, a>>>(sc, rtol, divtol, dt, maxit, h);
         });
         // true residual (reported)
