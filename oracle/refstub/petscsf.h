@@ -1,0 +1,2 @@
+/* single-rank stand-in: see petsc_stub.h */
+#include "petsc_stub.h"

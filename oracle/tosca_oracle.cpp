@@ -6,18 +6,23 @@
 //  (tosca_b200/csrc) and the timed CPU baseline. Only tests/, the smoke check
 //  and the CPU-baseline leg of bench.py load it.
 //
-//  TOSCA cannot be built in this environment (mpicxx, PETSc 3.15.5, HYPRE
-//  2.20.0 and HDF5 are absent), so every routine below is a restatement of the
-//  cited reference source, written from reading it. Where the reference uses
+//  TOSCA as a whole cannot be built in this environment (mpicxx, PETSc 3.15.5,
+//  HYPRE 2.20.0 and HDF5 are absent), so every routine below is a restatement
+//  of the cited reference source, written from reading it. Where the reference uses
 //  HYPRE (BoomerAMG-preconditioned GMRES, peqn.c:357-429), this file assembles
 //  the same 19-point matrix (peqn.c:703-1501) and solves it with its own
 //  Krylov method to a tight tolerance: the pinned system has a unique solution,
 //  so the solver choice does not change the answer beyond the tolerance.
 //
-//  PARITY UNPINNED: the reference ships no golden outputs for this path and
-//  cannot be run here, so this restatement is checked only against derived
-//  known-answer properties (tests/test_oracle_kat.py), not against outputs of
-//  TOSCA itself.
+//  PINNED to TOSCA's own code: oracle/refstub compiles the reference's stage
+//  functions unmodified from their source files against single-rank
+//  stand-ins of PETSc, HYPRE and MPI (oracle/_ref), and tests/test_ref_pin.py
+//  compares this restatement with them stage by stage (metrics, the assembled
+//  matrix, contravariantToCartesian, GradP, UpdateNut, the wall model, FormU,
+//  ExplicitRhsU) and over whole FE / RK4 steps. The temperature equation,
+//  buoyancy, Crank-Nicolson / IMEX, the turbines and the adjoint are checked
+//  against derived known answers and finite differences only
+//  (tests/test_oracle_*.py).
 //
 //  Single-rank PETSc semantics: a local (ghosted) vector equals the global one,
 //  with out-of-range indices of a DM_BOUNDARY_PERIODIC direction wrapping

@@ -4,7 +4,7 @@
 values at a few natural indices. test_petsc_io.py reads the same file with
 the oracle's and the CUDA library's readers and compares with this summary.
 
-    python tests/golden/make_petsc_fixture.py /root/reference
+    python tests/golden/make_petsc_fixture.py <reference checkout>
 """
 import json
 import os
@@ -30,4 +30,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_petsc_fixture.py <reference checkout>")
+    main(sys.argv[1])

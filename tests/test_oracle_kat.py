@@ -1,9 +1,9 @@
 """Known-answer checks that pin the CPU restatement (oracle) of TOSCA's step.
 
-The reference ships no golden outputs (its tests are input decks only), so
-the restatement is pinned by properties the discretisation must satisfy:
-Cartesian metric identities with TOSCA's axis mapping, the committed golden
-fixtures (tests/golden/, generated by tests/golden/make_golden.py), exact
+The reference ships no golden outputs (its tests are input decks only). Its
+own code pins the restatement stage by stage in tests/test_ref_pin.py; the
+checks here hold independently of it: properties the discretisation must
+satisfy, i.e. Cartesian metric identities with TOSCA's axis mapping, exact
 projection to a divergence-free field, symmetry of the pressure operator on
 orthogonal grids, free-stream preservation on the curvilinear hill, and the
 analytic decay rate of the 2-D Taylor-Green vortex."""
