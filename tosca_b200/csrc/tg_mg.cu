@@ -1,9 +1,11 @@
 // Geometric multigrid V-cycle for the 7-point part of TOSCA's pressure
 // operator, used as the preconditioner of the Krylov pressure solve.
 //
-//  * coarsening: every even direction with >= 4 cells is halved until a level
-//    has <= 64 cells; coarse face coefficients are face sums of the fine
-//    ones, halved when the face-normal direction is coarsened
+//  * coarsening: every direction with >= 3 cells is halved (n -> ceil(n/2):
+//    fine cells 2I and 2I+1 form coarse cell I; the last coarse cell of an
+//    odd direction holds one fine cell) until a level has <= 64 cells, so
+//    every grid size coarsens; coarse face coefficients are face sums of the
+//    fine ones, halved when the face-normal direction is coarsened
 //  * transfers: summed residual restriction, piecewise-constant prolongation
 //  * smoothing: zebra j-line Gauss-Seidel when j (the wall-normal direction)
 //    is non-periodic, red-black point Gauss-Seidel otherwise; 2 pre + 2 post
@@ -119,13 +121,13 @@ __global__ void k_coarsen(Lvl<T> F, Lvl<T> Cc)
 {
     int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
     if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
+    // fine cells of the aggregate (the last one of an odd direction has one)
+    const int i0 = F.cx * I, i1 = min(i0 + F.cx, F.nx), j0 = F.cy * J, j1 = min(j0 + F.cy, F.ny);
+    const int k0 = F.cz * K, k1 = min(k0 + F.cz, F.nz);
     double sE = 0.0, sN = 0.0, sT = 0.0;
-    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++)
-        sE += (double)F.aE[sidx(F, F.cz * K + dk, F.cy * J + dj, F.cx * I + F.cx - 1)];
-    for (int dk = 0; dk < F.cz; dk++) for (int di = 0; di < F.cx; di++)
-        sN += (double)F.aN[sidx(F, F.cz * K + dk, F.cy * J + F.cy - 1, F.cx * I + di)];
-    for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++)
-        sT += (double)F.aT[sidx(F, F.cz * K + F.cz - 1, F.cy * J + dj, F.cx * I + di)];
+    for (int k = k0; k < k1; k++) for (int j = j0; j < j1; j++) sE += (double)F.aE[sidx(F, k, j, i1 - 1)];
+    for (int k = k0; k < k1; k++) for (int i = i0; i < i1; i++) sN += (double)F.aN[sidx(F, k, j1 - 1, i)];
+    for (int j = j0; j < j1; j++) for (int i = i0; i < i1; i++) sT += (double)F.aT[sidx(F, k1 - 1, j, i)];
     int c = sidx(Cc, K, J, I);
     Cc.aE[c] = (T)(sE * (F.cx == 2 ? 0.5 : 1.0));
     Cc.aN[c] = (T)(sN * (F.cy == 2 ? 0.5 : 1.0));
@@ -373,8 +375,8 @@ template <class T>
 __device__ __forceinline__ void restrict_cell(const Lvl<T> &F, const Lvl<T> &Cc, int I, int J, int K)
 {
     T sum = T(0);
-    for (int dk = 0; dk < F.cz; dk++) for (int dj = 0; dj < F.cy; dj++) for (int di = 0; di < F.cx; di++) {
-        int i = F.cx * I + di, j = F.cy * J + dj, k = F.cz * K + dk;
+    const int i1 = min(F.cx * I + F.cx, F.nx), j1 = min(F.cy * J + F.cy, F.ny), k1 = min(F.cz * K + F.cz, F.nz);
+    for (int k = F.cz * K; k < k1; k++) for (int j = F.cy * J; j < j1; j++) for (int i = F.cx * I; i < i1; i++) {
         int c = sidx(F, k, j, i);
         sum += F.r[c] - F.diag[c] * F.x[c] + nb_sum(F, k, j, i, c, true);
     }
@@ -730,13 +732,13 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         Lvl<T> &F = L[mg->nlev - 1];
         F.n = (int64_t)F.nx * F.ny * F.nz;
         F.h0 = (F.nx + 1) >> 1;
-        auto can = [](int m) { return m >= 4 && (m % 2) == 0; };
+        auto can = [](int m) { return m >= 3; };
         F.cx = can(F.nx) ? 2 : 1; F.cy = can(F.ny) ? 2 : 1; F.cz = can(F.nz) ? 2 : 1;
         bool coarsen = F.n > COARSEST_CELLS && (F.cx * F.cy * F.cz) > 1 && mg->nlev < MAXL;
         if (!coarsen) { F.cx = F.cy = F.cz = 1; break; }
         Lvl<T> &Cn = L[mg->nlev++];
         Cn = Lvl<T>{};
-        Cn.nx = F.nx / F.cx; Cn.ny = F.ny / F.cy; Cn.nz = F.nz / F.cz;
+        Cn.nx = (F.nx + F.cx - 1) / F.cx; Cn.ny = (F.ny + F.cy - 1) / F.cy; Cn.nz = (F.nz + F.cz - 1) / F.cz;
         Cn.pi = F.pi; Cn.pj = F.pj; Cn.pk = F.pk;
     }
     for (int l = 0; l < mg->nlev; l++) {
@@ -754,7 +756,7 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
     if (mg->line) set_line_smem_attrs<T>();
     // dense coarsest inverse of (A + 11^T/n) in the level's own (split) order
     Lvl<T> &Lc = L[mg->nlev - 1];
-    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells (use even interior sizes)"};
+    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells"};
     const int nc = (int)Lc.n;
     // the single-block tail: as many of the smallest levels (<= TAIL_CELLS each)
     // as fit in its shared memory next to the dense-solve scratch
