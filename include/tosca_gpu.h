@@ -170,6 +170,11 @@ enum {
      * projected Cartesian force (lsourceFarmCat) and its face values
      * (sourceFarmCont) */
     TG_F_FARM_FORCE, TG_F_FARM_CONT,
+    /* adjoint of the state of the Schumann wall model (the time-filtered
+     * wall-parallel velocity and the running mean of its magnitude,
+     * boundary.c:3490-3520), a plane of (mz x mx) triples (filtered x, filtered
+     * y, running mean); carried from one reversed step to the one before */
+    TG_F_WALL_ADJ,
     TG_F_COUNT
 };
 

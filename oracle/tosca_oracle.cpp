@@ -119,6 +119,9 @@ struct tg_ctx {
     // jLeft wall model arrays, indexed k*mx + i (tauWall, uMeanMag, uFilt)
     std::vector<double> twx, twy, twz, umean, ufx, ufy, ufz;
     bool ufilt_set = false;
+    // adjoints of the wall-model state (ufx, ufy, umean) and, within one
+    // reversed step, of the wall stress (tosca_oracle_adjoint.inc)
+    std::vector<double> wadj_x, wadj_y, wadj_m, twa_x, twa_y, twa_z;
 
     // pressure system
     Csr A;
@@ -1645,7 +1648,8 @@ void allocState(tg_ctx &C)
     for (auto *v : {&C.p, &C.phi, &C.nut, &C.tmprt, &C.p_adj, &C.tmprt_o}) zero(*v, G);
     zero(C.rhs_o, G);
     const size_t P = (size_t)C.mx * C.mz;
-    for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz}) zero(*v, P);
+    for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz, &C.wadj_x, &C.wadj_y, &C.wadj_m,
+                    &C.twa_x, &C.twa_y, &C.twa_z}) zero(*v, P);
 }
 
 std::vector<V3> *vecField(tg_ctx &C, int w)
@@ -1789,6 +1793,10 @@ tg_status tor_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
 {
     return guarded(C, [&]() -> tg_status {
         if (!host || halo < 0) return fail(C, TG_ERR_BAD_ARG, "bad field argument");
+        if (w == TG_F_WALL_ADJ) {
+            for (size_t q = 0; q < (size_t)C->mx * C->mz; q++) { C->wadj_x[q] = host[3 * q]; C->wadj_y[q] = host[3 * q + 1]; C->wadj_m[q] = host[3 * q + 2]; }
+            return TG_OK;
+        }
         if (auto *v = vecField(*C, w)) { copyIn<3>(*C, (double *)v->data(), host, halo); return TG_OK; }
         if (auto *s = scalField(*C, w)) { copyIn<1>(*C, s->data(), host, halo); return TG_OK; }
         return fail(C, TG_ERR_BAD_ARG, "field not settable");
@@ -1802,6 +1810,10 @@ tg_status tor_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
         if (w == TG_F_TAUWALL) {
             // plane (mz x mx) of the j-left wall stress
             for (size_t q = 0; q < (size_t)C->mx * C->mz; q++) { host[3 * q] = C->twx[q]; host[3 * q + 1] = C->twy[q]; host[3 * q + 2] = C->twz[q]; }
+            return TG_OK;
+        }
+        if (w == TG_F_WALL_ADJ) {
+            for (size_t q = 0; q < (size_t)C->mx * C->mz; q++) { host[3 * q] = C->wadj_x[q]; host[3 * q + 1] = C->wadj_y[q]; host[3 * q + 2] = C->wadj_m[q]; }
             return TG_OK;
         }
         if (auto *v = vecField(*C, w)) { copyOut<3>(*C, host, (const double *)v->data(), halo); return TG_OK; }
@@ -2068,12 +2080,16 @@ tg_status tor_adjoint_step(tg_ctx *C)
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
         auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;
+        auto umean = C->umean, ufx = C->ufx, ufy = C->ufy, ufz = C->ufz, twx = C->twx, twy = C->twy, twz = C->twz;
+        const bool ufilt_set = C->ufilt_set;
         int it = C->it;
         AdjTape T;
         tg_stats st{};
         stepTaped(*C, &st, T);
         C->ucont = ucont; C->ucat = ucat; C->btheta = btheta; C->btheta_o = btheta_o;
         C->p = p; C->phi = phi; C->phi1d = phi1d; C->nut = nut; C->it = it;
+        C->umean = umean; C->ufx = ufx; C->ufy = ufy; C->ufz = ufz; C->twx = twx; C->twy = twy; C->twz = twz;
+        C->ufilt_set = ufilt_set;
         adjointStep(*C, T);
         return TG_OK;
     });

@@ -30,8 +30,10 @@ def _case(name, ddt, div=api.DIV_CENTRAL, les=None):
     if name == "tgv":
         cfg, nodes, ucat, p = cases.tgv_case(12, ddt=ddt)
     else:
+        # "abl_wall": the Schumann wall function on the ground (its filter
+        # state is part of the state, adjoint field WALL_ADJ)
         cfg, nodes, ucat, p = cases.abl_case(nx=12, ny=10, nz=8, Lx=120.0, Ly=100.0, H=80.0, dz1=4.0, ddt=ddt,
-                                             wall=api.BC_NOSLIP)
+                                             wall=api.BC_WALL_SHUMANN if name == "abl_wall" else api.BC_NOSLIP)
     cfg.div_scheme = div
     if les is not None:
         cfg.les = les
@@ -68,6 +70,8 @@ def _seeds(rng, shape3, shape1):
     ("abl", api.DDT_FE, api.DIV_CENTRAL),
     ("abl", api.DDT_RK4, api.DIV_CENTRAL),
     ("abl", api.DDT_RK4, api.DIV_QUICK),
+    ("abl_wall", api.DDT_FE, api.DIV_CENTRAL),
+    ("abl_wall", api.DDT_RK4, api.DIV_QUICK),
 ])
 def test_adjoint_step_matches_oracle(name, ddt, div):
     rng = np.random.default_rng(7)
@@ -76,12 +80,18 @@ def test_adjoint_step_matches_oracle(name, ddt, div):
     g = _start(tosca_b200.gpu_solver, cfg, nodes, ucat, p, f0)
     o = _start(oracle.solver, cfg, nodes, ucat, p, f0)
     wu, wc, wp = _seeds(rng, ucat.shape, p.shape)
+    keys = ADJ
     for s in (g, o):
         s.set("UCONT_ADJ", wu); s.set("UCAT_ADJ", wc); s.set("P_ADJ", wp); s.set("SOURCE_ADJ", np.zeros_like(f0))
+    if name == "abl_wall":
+        ww = rng.standard_normal((cfg.mz, cfg.mx, 3))
+        for s in (g, o):
+            s.set("WALL_ADJ", ww)
+        keys = ADJ + ("WALL_ADJ",)
     g.adjoint_step()
     L = _olib()
     assert L.tor_adjoint_step(o.h) == 0, L.tor_last_error(o.h)
-    for k in ADJ:
+    for k in keys:
         a, b = g.get(k), o.get(k)
         nb = np.linalg.norm(b)
         if nb < 1e-12:
@@ -94,11 +104,14 @@ def test_adjoint_step_matches_oracle(name, ddt, div):
     g.close(); o.close(); o2.close()
 
 
-def test_dot_product_with_central_difference_tangent():
+@pytest.mark.parametrize("name", ["abl", "abl_wall"])
+def test_dot_product_with_central_difference_tangent(name):
     """<w, (F(x + eps v) - F(x - eps v)) / 2 eps> = <J^T w, v> for the one-step
-    map F on Ucont (ABL, RK4, Smagorinsky)."""
+    map F on Ucont (ABL, RK4, Smagorinsky; with the wall function, F also
+    carries the wall filter state, so every evaluation starts from a context
+    with the same history)."""
     rng = np.random.default_rng(11)
-    cfg, nodes, ucat, p = _case("abl", api.DDT_RK4)
+    cfg, nodes, ucat, p = _case(name, api.DDT_RK4)
     f0 = rng.standard_normal(ucat.shape) * 0.01
     g = _start(tosca_b200.gpu_solver, cfg, nodes, ucat, p, f0)
     x0 = {k: g.get(k) for k in ("UCONT", "UCAT", "P")}
@@ -106,13 +119,14 @@ def test_dot_product_with_central_difference_tangent():
     v = rng.standard_normal(ucat.shape) * np.abs(x0["UCONT"]).max() * 1e-3
 
     def F(du):
-        g.set("UCONT", x0["UCONT"] + du); g.set("UCAT", x0["UCAT"]); g.set("P", x0["P"])
-        g.step(1)
-        out = (wu * g.get("UCONT")).sum() + (wc * g.get("UCAT")).sum() + (wp * g.get("P")).sum()
+        t = _start(tosca_b200.gpu_solver, cfg, nodes, ucat, p, f0)
+        t.set("UCONT", x0["UCONT"] + du); t.set("UCAT", x0["UCAT"]); t.set("P", x0["P"])
+        t.step(1)
+        out = (wu * t.get("UCONT")).sum() + (wc * t.get("UCAT")).sum() + (wp * t.get("P")).sum()
+        t.close()
         return out
 
     lhs = (F(EPS * v) - F(-EPS * v)) / (2 * EPS)
-    g.set("UCONT", x0["UCONT"]); g.set("UCAT", x0["UCAT"]); g.set("P", x0["P"])
     g.set("UCONT_ADJ", wu); g.set("UCAT_ADJ", wc); g.set("P_ADJ", wp); g.set("SOURCE_ADJ", np.zeros_like(f0))
     g.adjoint_step()
     rhs = (g.get("UCONT_ADJ") * v).sum()
@@ -120,13 +134,13 @@ def test_dot_product_with_central_difference_tangent():
     g.close()
 
 
-@pytest.mark.parametrize("nsteps,nsnap", [(4, 2), (5, 5)])
-def test_gradient_with_checkpointing_matches_central_differences(nsteps, nsnap):
+@pytest.mark.parametrize("name,nsteps,nsnap", [("abl", 4, 2), ("abl", 5, 5), ("abl_wall", 4, 2), ("abl_wall", 5, 5)])
+def test_gradient_with_checkpointing_matches_central_differences(name, nsteps, nsnap):
     """dJ/df . v over N steps, reversed with a binomial checkpoint schedule,
     against central differences of the CUDA step and of the oracle's CPU step
     (the reference gradient)."""
     rng = np.random.default_rng(5)
-    cfg, nodes, ucat, p = _case("abl", api.DDT_RK4)
+    cfg, nodes, ucat, p = _case(name, api.DDT_RK4)
     f0 = rng.standard_normal(ucat.shape) * 0.01
     g = _start(tosca_b200.gpu_solver, cfg, nodes, ucat, p, f0)
     x0 = {k: g.get(k) for k in ("UCONT", "UCAT", "P")}
@@ -161,9 +175,10 @@ def test_gradient_with_checkpointing_matches_central_differences(nsteps, nsnap):
 
 
 def test_unsupported_configurations_are_rejected():
-    cfg, nodes, ucat, p = cases.abl_case(nx=12, ny=10, nz=8, Lx=120.0, Ly=100.0, H=80.0, dz1=4.0)
+    # the curvilinear hill: non-symmetric pressure operator
+    cfg, nodes, ucat, p, T = cases.hill_case(nx=12, ny=8, nz=8)
     g = tosca_b200.gpu_solver(cfg)
-    cases.setup(g, nodes, ucat, p)
+    cases.setup(g, nodes, ucat, p, T)
     with pytest.raises(api.TgError) as e:
         g.adjoint_step()
     assert e.value.status == api.TG_ERR_BAD_ARG

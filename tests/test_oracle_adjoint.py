@@ -24,8 +24,9 @@ def _case(name, ddt, div):
     if name == "tgv":
         cfg, nodes, ucat, p = cases.tgv_case(8, ddt=ddt)
     else:
+        # "abl_wall": the Schumann wall function (-3) on the ground
         cfg, nodes, ucat, p = cases.abl_case(nx=8, ny=6, nz=6, Lx=80.0, Ly=60.0, H=60.0, dz1=4.0, ddt=ddt,
-                                             wall=api.BC_NOSLIP)
+                                             wall=api.BC_WALL_SHUMANN if name == "abl_wall" else api.BC_NOSLIP)
     cfg.div_scheme = div
     cfg.poisson_rtol = 1e-14
     cfg.source = 1
@@ -66,6 +67,8 @@ def adjoint_vs_fd(name, ddt, div=api.DIV_CENTRAL, nsteps=1, seed=3):
 
     L = _lib()
     adj = {"UCONT_ADJ": wu, "UCAT_ADJ": wc, "P_ADJ": wp, "SOURCE_ADJ": np.zeros_like(f0)}
+    if cfg.bc[2] == api.BC_WALL_SHUMANN:
+        adj["WALL_ADJ"] = np.zeros((cfg.mz, cfg.mx, 3))   # the filter state after the last step feeds no functional
     for n in reversed(range(nsteps)):
         r = _start(cfg, nodes, ucat, p, f0, extra_steps=n)
         for k, v in adj.items():
@@ -108,3 +111,11 @@ def test_one_step_gradient_matches_finite_differences(name, ddt, div):
 
 def test_three_steps_gradient_matches_finite_differences():
     _check(adjoint_vs_fd("abl", api.DDT_RK4, nsteps=3))
+
+
+@pytest.mark.parametrize("ddt,nsteps", [(api.DDT_FE, 1), (api.DDT_RK4, 1), (api.DDT_RK4, 3)])
+def test_wall_function_gradient_matches_finite_differences(ddt, nsteps):
+    """The Schumann wall stress (UpdateWallModelsU, boundary.c:3257-3600) and
+    its time-filtered wall velocity differentiated: the filter state passes
+    between reversed steps through TG_F_WALL_ADJ."""
+    _check(adjoint_vs_fd("abl_wall", ddt, nsteps=nsteps))

@@ -32,7 +32,7 @@ FIELDS = [
     "UCONT", "UCAT", "UCONT_O", "RHS", "DP", "BTHETA",
     "P", "PHI", "NUT", "TMPRT", "TAUWALL", "SOURCE",
     "UCONT_ADJ", "UCAT_ADJ", "P_ADJ", "SOURCE_ADJ",
-    "FARM_FORCE", "FARM_CONT",
+    "FARM_FORCE", "FARM_CONT", "WALL_ADJ",
 ]
 F = {name: i for i, name in enumerate(FIELDS)}
 SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT", "P_ADJ"}
@@ -319,7 +319,7 @@ class Solver:
 
     def get(self, name: str, halo: int = 0) -> np.ndarray:
         mz, my, mx = self.shape
-        if name == "TAUWALL":
+        if name in ("TAUWALL", "WALL_ADJ"):
             out = np.zeros((mz, mx, 3))
         else:
             shp = (mz + 2 * halo, my + 2 * halo, mx + 2 * halo)

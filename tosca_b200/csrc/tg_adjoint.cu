@@ -21,10 +21,12 @@
 //
 // Scope: orthogonal grids (symmetric pressure operator), FE and RK4, central
 // and QUICK convection, constant or Smagorinsky viscosity, noSlip, slip and
-// periodic patches; the body force, frozen-temperature buoyancy and the mean
-// pressure gradient enter as forcings. The wall function and the curvilinear
-// (non-symmetric) pressure operator are rejected with TG_ERR_BAD_ARG. The
-// adjoint arithmetic is FP64 in every precision mode.
+// periodic patches, the Schumann wall function on jLeft (neutral, plane-
+// averaged u*, Cartesian branch: its time-filter state is part of the state,
+// adjoint TG_F_WALL_ADJ); the body force, frozen-temperature buoyancy and the
+// mean pressure gradient enter as forcings. The curvilinear (non-symmetric)
+// pressure operator and the curvilinear wall-stress branch are rejected with
+// TG_ERR_BAD_ARG. The adjoint arithmetic is FP64 in every precision mode.
 //
 // Checkpointing: tg_adjoint_forward runs the forward steps keeping device
 // snapshots of the state at the positions of a binomial (revolve) schedule;
@@ -47,6 +49,8 @@ struct Snapshot {
     V3f<double> ucont, ucat, btheta, btheta_o;
     double *p, *px, *pxp, *pxp2; // P, the last three Poisson solutions (initial guess of the next solve)
     double phist = 0.0;          // solutions in that history (device slot SC_PHIST)
+    double *wum = nullptr, *wfx = nullptr, *wfy = nullptr;   // wall-model state (planes), with the wall function
+    bool ufilt_set = false;
     int it;
     int pos;       // step index of the state held (-1: free)
 };
@@ -55,6 +59,9 @@ struct Snapshot {
 struct Tape {
     V3f<double> u_o, ucat_n, ut[4], uc[4];
     double *nut = nullptr;
+    // wall-model state at the step start (planes mz x mx) and, on the device,
+    // [0] the step counter of the step, [1] 1 when the step seeded the filter
+    double *wum = nullptr, *wfx = nullptr, *wfy = nullptr, *meta = nullptr;
     int nst = 0;
 };
 
@@ -62,6 +69,10 @@ struct AdjState {
     // public adjoint fields
     V3f<double> ua, ca, fa;
     double *pa = nullptr;
+    double *wxa = nullptr, *wya = nullptr, *wma = nullptr;   // TG_F_WALL_ADJ (planes)
+    // wall reverse work: tauWall adjoint, Up and |Up| adjoints, block partials, scalars
+    double *twa[3] = {nullptr, nullptr, nullptr}, *upa[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *wpart = nullptr, *wsc = nullptr;
     // work
     V3f<double> uoa, usa, uta, cta, ra, dpa, fpa, f1a, f2a, f3a, qa;
     double *pha = nullptr, *na = nullptr, *lam = nullptr, *rhsc = nullptr;
@@ -276,6 +287,12 @@ __global__ void k_adj_cartesian_bcs(Grid g, Metrics m, V3f<double> ca, Params p)
         aadd3(ca, c, 1.0, ga - (2.0 * dot3(ga, n)) * n);
     } else if (type == TG_BC_NOSLIP) {
         aadd3(ca, c, -1.0, ga);
+    } else if (type == TG_BC_WALL_SHUMANN && dir == 1 && !right) {
+        // ghost = 2 Ub - 3 (Ub.n) n - Uc + (Uc.n) n, Ub = (k, 1, i), Uc = (k, 2, i)
+        R3<double> n; calc_normal_adj(ld3(m.csi, c), ld3(m.eta, c), ld3(m.zet, c), 1, n);
+        const double gn = dot3(ga, n);
+        aadd3(ca, c, 1.0, 2.0 * ga - (3.0 * gn) * n);
+        aadd3(ca, c + g.mx, 1.0, gn * n - ga);
     } else if (type == TG_BC_PERIODIC) {
         int src;
         if (dir == 0) src = g.lin(k, j, right ? 1 : g.mx - 2);
@@ -516,7 +533,7 @@ __device__ __forceinline__ void visc_adj(R3<double> s0, R3<double> s1, R3<double
 // pass 1 transpose: per face, scatter to Ucat (atomics), Ucont (own face) and nut
 __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double> uc, const double *nut, Params p,
                                   V3f<double> f1a, V3f<double> f2a, V3f<double> f3a,
-                                  V3f<double> uta, V3f<double> cta, double *na)
+                                  V3f<double> uta, V3f<double> cta, double *na, V3f<double> twa)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
@@ -610,7 +627,11 @@ __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double>
         uta.y[f] += -dot3(gv, uface);
         double nuEff; bool vnut = false;
         if (p.les) {
-            if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = 0.0;
+            if ((p.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_WALL_SHUMANN && j == my - 2)) {
+                // the face flux holds -tauWall (ueqn_solvers.c:548-558)
+                aadd3(twa, k * mx + i, -1.0, gv);
+                nuEff = nu;
+            } else if ((p.bc[TG_JLEFT] == TG_BC_SLIP && j == 0) || (p.bc[TG_JRIGHT] == TG_BC_SLIP && j == my - 2)) nuEff = 0.0;
             else { nuEff = nu + 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)); vnut = true; }
         } else nuEff = nu;
         R3<double> dd[3];
@@ -796,9 +817,135 @@ __global__ void k_adj_smagorinsky(Grid g, Metrics m, V3f<double> ucat, const dou
 }  // namespace
 
 // ===================================================================== host
+// ------------------------------------------------- UpdateWallModelsU reverse
+// Forward (k_wall_stress, Cartesian branch): per plane cell w at j = 1,
+// Up = U - (U.n) n, Umean = mean |Up|, u* = max(0, kappa Umean / ln(d/z0)),
+// S = u*^2, D = max(Umean, 1e-5); umean' = m1 umean + m2 |Up|;
+// r = dt / max(L/umean', dt); uf' = (1-r) uf + r Up (x, y; uf = Up on the
+// seeding step); tau = -S uf' / D; tw = (je.z tau_x, je.z tau_y, je.x tau_x +
+// je.y tau_y). The reverse maps the tauWall adjoint (from FormU) and the
+// adjoint of the state after the step (wxa, wya, wma) to the adjoint of the
+// step-start Ucat at j = 1 and of the step-start wall state. Plane sums are
+// per-block trees summed in a fixed order (bitwise reproducible).
+constexpr int WNB = 148;     // blocks of the plane reductions
+
+__device__ __forceinline__ void wall_par(const Grid &g, const Metrics &m, const V3f<double> &ucat, int k, int i,
+                                         R3<double> &Up, R3<double> &n)
+{
+    const int c = g.lin(k, 1, i);
+    calc_normal_adj(ld3(m.csi, c), ld3(m.eta, c), ld3(m.zet, c), 1, n);
+    const R3<double> U = ld3(ucat, c);
+    Up = U - dot3(U, n) * n;
+}
+
+// block sums of (a, b) into part[2 blockIdx], part[2 blockIdx + 1]
+__device__ __forceinline__ void block_sum2(double a, double b, double *part)
+{
+    __shared__ double sh[2][256];
+    sh[0][threadIdx.x] = a; sh[1][threadIdx.x] = b;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) { sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = sh[0][0]; part[2 * blockIdx.x + 1] = sh[1][0]; }
+}
+
+// forward plane sums of |Up| and the wall distance (the step-start Ucat)
+__global__ void __launch_bounds__(256) k_adj_wall_fwd(Grid g, Metrics m, V3f<double> ucat, double *part)
+{
+    const int nI = g.mx - 2, nK = g.mz - 2;
+    double su = 0.0, sd = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
+        const int i = t % nI + 1, k = t / nI + 1, c = g.lin(k, 1, i);
+        const double area = sqrt(dot3(ld3(m.eta, c), ld3(m.eta, c)));
+        R3<double> Up, n; wall_par(g, m, ucat, k, i, Up, n);
+        su += sqrt(dot3(Up, Up));
+        sd += 0.5 / m.aj[c] / area;
+    }
+    block_sum2(su, sd, part);
+}
+// wsc <- Umean, dist, u*, S, D, logLaw
+__global__ void k_adj_wall_fwd_final(Grid g, Params p, const double *part, double *wsc)
+{
+    double su = 0.0, sd = 0.0;
+    for (int b = 0; b < WNB; b++) { su += part[2 * b]; sd += part[2 * b + 1]; }
+    const double cnt = (double)(g.mx - 2) * (double)(g.mz - 2);
+    const double Umean = su / cnt, dist = sd / cnt, logLaw = log(dist / p.z0);
+    const double us = fmax(0.0, (p.kappa * Umean) / logLaw);
+    wsc[0] = Umean; wsc[1] = dist; wsc[2] = us; wsc[3] = us * us; wsc[4] = fmax(Umean, 1e-5); wsc[5] = logLaw;
+}
+// per cell: filter and running-mean reverse; block sums of the S and D adjoints
+__global__ void __launch_bounds__(256) k_adj_wall_local(Grid g, Metrics m, Params p, V3f<double> ucat, const double *wum0,
+                                                        const double *wfx0, const double *wfy0, const double *meta,
+                                                        V3f<double> twa, double *wxa, double *wya, double *wma,
+                                                        V3f<double> upa, double *upma, const double *wsc, double *part)
+{
+    const int nI = g.mx - 2, nK = g.mz - 2;
+    const double aN = meta[0], m1 = aN / (aN + 1.0), m2 = 1.0 / (aN + 1.0);
+    const bool seed = meta[1] != 0.0;
+    const double S = wsc[3], D = wsc[4], dt = p.dt;
+    double sa = 0.0, da = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
+        const int i = t % nI + 1, k = t / nI + 1, c = g.lin(k, 1, i), w = k * g.mx + i;
+        R3<double> Up, n; wall_par(g, m, ucat, k, i, Up, n);
+        const double upm = sqrt(dot3(Up, Up));
+        const double um = m1 * wum0[w] + m2 * upm;
+        const R3<double> zz = ld3(m.zet, c), cc = ld3(m.csi, c);
+        const double lx = 1.0 / m.aj[c] / sqrt(dot3(zz, zz)), ly = 1.0 / m.aj[c] / sqrt(dot3(cc, cc));
+        const double L = sqrt(lx * lx + ly * ly);
+        const bool filt = L / um > dt;
+        const double r = dt / (filt ? L / um : dt);
+        const double fx0 = seed ? Up.x : wfx0[w], fy0 = seed ? Up.y : wfy0[w];
+        const double fx = (1.0 - r) * fx0 + r * Up.x, fy = (1.0 - r) * fy0 + r * Up.y;
+        const R3<double> je = ld3(m.jeta, g.lin(k, 0, i));
+        const double txa = je.z * twa.x[w] + je.x * twa.z[w];
+        const double tya = je.z * twa.y[w] + je.y * twa.z[w];
+        const double fxa = wxa[w] + txa * (-S / D), fya = wya[w] + tya * (-S / D);
+        sa += txa * (-fx / D) + tya * (-fy / D);
+        da += txa * (S * fx / (D * D)) + tya * (S * fy / (D * D));
+        double fx0a = (1.0 - r) * fxa, fy0a = (1.0 - r) * fya;
+        R3<double> pa{r * fxa, r * fya, 0.0};
+        const double ra = (Up.x - fx0) * fxa + (Up.y - fy0) * fya;
+        const double uma = wma[w] + (filt ? ra * dt / L : 0.0);
+        if (seed) { pa.x += fx0a; pa.y += fy0a; fx0a = 0.0; fy0a = 0.0; }
+        wxa[w] = fx0a; wya[w] = fy0a; wma[w] = m1 * uma;
+        upma[w] = m2 * uma;
+        st3(upa, w, pa);
+    }
+    block_sum2(sa, da, part);
+}
+// wsc[6] <- adjoint of Umean
+__global__ void k_adj_wall_mean(Grid g, Params p, const double *part, double *wsc)
+{
+    double sa = 0.0, da = 0.0;
+    for (int b = 0; b < WNB; b++) { sa += part[2 * b]; da += part[2 * b + 1]; }
+    const double Umean = wsc[0], us = wsc[2], logLaw = wsc[5];
+    wsc[6] = (us > 0.0 ? sa * 2.0 * us * p.kappa / logLaw : 0.0) + (Umean > 1e-5 ? da : 0.0);
+}
+// Up and |Up| adjoints (with the plane mean's share) into the Ucat adjoint at j = 1
+__global__ void k_adj_wall_scatter(Grid g, Metrics m, V3f<double> ucat, V3f<double> upa, const double *upma,
+                                   const double *wsc, V3f<double> ca)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.mx - 2 || k > g.mz - 2) return;
+    const int c = g.lin(k, 1, i), w = k * g.mx + i;
+    const double cnt = (double)(g.mx - 2) * (double)(g.mz - 2);
+    R3<double> Up, n; wall_par(g, m, ucat, k, i, Up, n);
+    const double upm = sqrt(dot3(Up, Up));
+    const double ma = upma[w] + wsc[6] / cnt;
+    R3<double> pa = ld3(upa, w);
+    if (upm > 0.0) pa = pa + (ma / upm) * Up;
+    aadd3(ca, c, 1.0, pa - dot3(pa, n) * n);
+}
+__global__ void k_tape_wall_meta(double *meta, const double *d_it, double seed) { meta[0] = d_it[0]; meta[1] = seed; }
+
 struct ApiFail { tg_status s; std::string msg; };
 
 static V3f<double> alloc3(tg_ctx *C) { return dalloc3(C, (size_t)C->g.size()); }
+
+static size_t wall_plane(const tg_ctx *C) { return (size_t)C->g.mx * C->g.mz; }
+static bool wall_on(const tg_ctx *C) { return C->prm.les && C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN; }
 
 static AdjState &adj_state(tg_ctx *C)
 {
@@ -807,6 +954,7 @@ static AdjState &adj_state(tg_ctx *C)
         C->adj = A;
         A->ua = alloc3(C); A->ca = alloc3(C); A->fa = alloc3(C);
         A->pa = dallocd(C, (size_t)C->g.size());
+        A->wxa = dallocd(C, wall_plane(C)); A->wya = dallocd(C, wall_plane(C)); A->wma = dallocd(C, wall_plane(C));
     }
     return *C->adj;
 }
@@ -817,6 +965,8 @@ static Tape make_tape(tg_ctx *C)
     t.u_o = alloc3(C); t.ucat_n = alloc3(C);
     for (int q = 0; q < 4; q++) { t.ut[q] = alloc3(C); t.uc[q] = alloc3(C); }
     t.nut = dallocd(C, (size_t)C->g.size());
+    t.wum = dallocd(C, wall_plane(C)); t.wfx = dallocd(C, wall_plane(C)); t.wfy = dallocd(C, wall_plane(C));
+    t.meta = dallocd(C, 2);
     return t;
 }
 static size_t tape_bytes(tg_ctx *C) { return (size_t)C->g.size() * sizeof(double) * (3 * 10 + 1); }
@@ -832,7 +982,18 @@ static void adj_work(tg_ctx *C)
     A.lam = dallocd(C, (size_t)poisson_n(C)); A.rhsc = dallocd(C, (size_t)poisson_n(C));
     A.work_tape = make_tape(C);
     A.cur = &A.work_tape;
+    for (int q = 0; q < 3; q++) A.twa[q] = dallocd(C, wall_plane(C));
+    for (int q = 0; q < 4; q++) A.upa[q] = dallocd(C, wall_plane(C));
+    A.wpart = dallocd(C, 2 * WNB);
+    A.wsc = dallocd(C, 8);
     A.work = true;
+}
+
+bool adj_wall_field(tg_ctx *C, double *&x, double *&y, double *&m)
+{
+    AdjState &A = adj_state(C);
+    x = A.wxa; y = A.wya; m = A.wma;
+    return true;
 }
 
 bool adj_field(tg_ctx *C, int w, V3f<double> &v, double *&s)
@@ -873,8 +1034,17 @@ static void zero3(tg_ctx *C, V3f<double> v)
     TG_CUDA(cudaMemsetAsync(v.x, 0, 3 * sizeof(double) * (size_t)C->g.size(), C->stream));
 }
 
+static void copy_plane(tg_ctx *C, double *dst, const double *src, size_t n)
+{
+    TG_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, C->stream));
+}
+
 static void copy_tape(tg_ctx *C, Tape &dst, const Tape &src)
 {
+    copy_plane(C, dst.wum, src.wum, wall_plane(C));
+    copy_plane(C, dst.wfx, src.wfx, wall_plane(C));
+    copy_plane(C, dst.wfy, src.wfy, wall_plane(C));
+    copy_plane(C, dst.meta, src.meta, 2);
     copy3(C, dst.u_o, src.u_o);
     copy3(C, dst.ucat_n, src.ucat_n);
     for (int q = 0; q < src.nst; q++) { copy3(C, dst.ut[q], src.ut[q]); copy3(C, dst.uc[q], src.uc[q]); }
@@ -887,6 +1057,12 @@ void tape_step_start(tg_ctx *C)
     Tape &T = *C->adj->cur;
     copy3(C, T.u_o, C->s.ucont);
     copy3(C, T.ucat_n, C->s.ucat);
+    if (wall_on(C)) {
+        copy_plane(C, T.wum, C->s.umean, wall_plane(C));
+        copy_plane(C, T.wfx, C->s.ufx, wall_plane(C));
+        copy_plane(C, T.wfy, C->s.ufy, wall_plane(C));
+        k_tape_wall_meta<<<1, 1, 0, C->stream>>>(T.meta, C->d_scal + SC_IT, C->ufilt_set ? 0.0 : 1.0);
+    }
     T.nst = 0;
 }
 void tape_nut(tg_ctx *C)
@@ -928,8 +1104,9 @@ static void adj_contra(tg_ctx *C, V3f<double> ca, V3f<double> ua)
 
 static bool adjoint_supported(tg_ctx *C, std::string &why)
 {
-    for (int p = 0; p < 6; p++)
-        if (C->prm.bc[p] == TG_BC_WALL_SHUMANN) { why = "the adjoint of the wall function is not implemented"; return false; }
+    if (C->prm.bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && C->prm.curvilinear) {
+        why = "the adjoint of the curvilinear wall-stress branch is not implemented"; return false;
+    }
     if (!C->orthogonal) { why = "the adjoint needs the symmetric (orthogonal-grid) pressure operator"; return false; }
     if (C->prm.teqn) { why = "the adjoint of the temperature equation is not implemented"; return false; }
     if (C->cfg.ddt_scheme == TG_DDT_CN) { why = "the adjoint of the Crank-Nicolson scheme is not implemented"; return false; }
@@ -993,6 +1170,9 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
     // stages
     copy3(C, A.uoa, A.usa);
     zero3(C, A.dpa);
+    const bool wall = wall_on(C);
+    if (wall) for (int q = 0; q < 3; q++) TG_CUDA(cudaMemsetAsync(A.twa[q], 0, sizeof(double) * wall_plane(C), st));
+    const V3f<double> twa{A.twa[0], A.twa[1], A.twa[2]};
     TG_CUDA(cudaMemsetAsync(A.na, 0, sizeof(double) * G, st));
     const double bw[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
     const double aw[4] = {0.0, 0.5, 0.5, 1.0};
@@ -1010,7 +1190,7 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
         zero3(C, A.uta);
         zero3(C, A.cta);
         TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<<<gfc(g), block3(), 0, st>>>(g, C->m, T.ut[s], T.uc[s], T.nut, C->prm,
-                                                                                    A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na));
+                                                                                    A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na, twa));
         // stage Ucat: periodic copies, interior from contravariantToCartesian, other ghosts from the state Ucat
         adj_periodic(C, A.cta, 0);
         adj_contra(C, A.cta, A.uta);
@@ -1028,6 +1208,17 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
         dim3 grid((na + 31) / 32, (nb + 7) / 8, 6);
         k_adj_nut_bcs<<<grid, b2, 0, st>>>(g, A.na, C->prm);
         TG_PROF(C, "adj_smagorinsky", k_adj_smagorinsky<<<gint(g), block3(), 0, st>>>(g, C->m, T.ucat_n, A.na, C->prm, A.ca));
+    }
+    // the wall model (its stress feeds every stage; it reads the step-start Ucat)
+    if (wall) {
+        const V3f<double> upa{A.upa[0], A.upa[1], A.upa[2]};
+        dim3 grid((g.mx - 2 + 31) / 32, (g.mz - 2 + 7) / 8);
+        TG_PROF(C, "adj_wall", k_adj_wall_fwd<<<WNB, 256, 0, st>>>(g, C->m, T.ucat_n, A.wpart));
+        k_adj_wall_fwd_final<<<1, 1, 0, st>>>(g, C->prm, A.wpart, A.wsc);
+        TG_PROF(C, "adj_wall", k_adj_wall_local<<<WNB, 256, 0, st>>>(g, C->m, C->prm, T.ucat_n, T.wum, T.wfx, T.wfy, T.meta,
+                                                                      twa, A.wxa, A.wya, A.wma, upa, A.upa[3], A.wsc, A.wpart));
+        k_adj_wall_mean<<<1, 1, 0, st>>>(g, C->prm, A.wpart, A.wsc);
+        TG_PROF(C, "adj_wall", k_adj_wall_scatter<<<grid, b2, 0, st>>>(g, C->m, T.ucat_n, upa, A.upa[3], A.wsc, A.ca));
     }
     // turbines: C_T' gradient and the adjoint of the Ucat they sampled
     if (C->prm.farm) farm_adj_finish(C, T.ucat_n, A.ca);
@@ -1080,6 +1271,7 @@ static Snapshot make_snapshot(tg_ctx *C)
     s.px = dallocd(C, (size_t)poisson_n(C));
     s.pxp = dallocd(C, (size_t)poisson_n(C));
     s.pxp2 = dallocd(C, (size_t)poisson_n(C));
+    if (wall_on(C)) { s.wum = dallocd(C, wall_plane(C)); s.wfx = dallocd(C, wall_plane(C)); s.wfy = dallocd(C, wall_plane(C)); }
     s.pos = -1;
     return s;
 }
@@ -1094,7 +1286,13 @@ static void save_state(tg_ctx *C, Snapshot &s, int pos)
     TG_CUDA(cudaMemcpyAsync(s.pxp, poisson_xprev(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(s.pxp2, poisson_xprev2(C), sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(&s.phist, C->d_scal + SC_PHIST, sizeof(double), cudaMemcpyDeviceToHost, C->stream));
+    if (s.wum) {
+        copy_plane(C, s.wum, C->s.umean, wall_plane(C));
+        copy_plane(C, s.wfx, C->s.ufx, wall_plane(C));
+        copy_plane(C, s.wfy, C->s.ufy, wall_plane(C));
+    }
     TG_CUDA(cudaStreamSynchronize(C->stream));
+    s.ufilt_set = C->ufilt_set;
     s.it = C->it;
     s.pos = pos;
 }
@@ -1107,6 +1305,12 @@ static void restore_state(tg_ctx *C, const Snapshot &s)
     TG_CUDA(cudaMemcpyAsync(poisson_xprev(C), s.pxp, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     TG_CUDA(cudaMemcpyAsync(poisson_xprev2(C), s.pxp2, sizeof(double) * (size_t)poisson_n(C), cudaMemcpyDeviceToDevice, C->stream));
     k_set_phist<<<1, 1, 0, C->stream>>>(C->d_scal + SC_PHIST, s.phist);
+    if (s.wum) {
+        copy_plane(C, C->s.umean, s.wum, wall_plane(C));
+        copy_plane(C, C->s.ufx, s.wfx, wall_plane(C));
+        copy_plane(C, C->s.ufy, s.wfy, wall_plane(C));
+        C->ufilt_set = s.ufilt_set;
+    }
     C->it = s.it;
     set_device_step(C);
 }

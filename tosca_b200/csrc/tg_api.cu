@@ -372,6 +372,17 @@ tg_status tg_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
 {
     return guarded(C, [&]() -> tg_status {
         if (!host || halo < 0) return fail(C, TG_ERR_BAD_ARG, "bad field argument");
+        if (w == TG_F_WALL_ADJ) {
+            double *x, *y, *m;
+            adj_wall_field(C, x, y, m);
+            const size_t P = (size_t)C->g.mx * C->g.mz;
+            std::vector<double> a(P), b(P), c(P);
+            for (size_t q = 0; q < P; q++) { a[q] = host[3 * q]; b[q] = host[3 * q + 1]; c[q] = host[3 * q + 2]; }
+            TG_CUDA(cudaMemcpy(x, a.data(), P * sizeof(double), cudaMemcpyHostToDevice));
+            TG_CUDA(cudaMemcpy(y, b.data(), P * sizeof(double), cudaMemcpyHostToDevice));
+            TG_CUDA(cudaMemcpy(m, c.data(), P * sizeof(double), cudaMemcpyHostToDevice));
+            return TG_OK;
+        }
         V3f<double> v;
         double *sp = nullptr;
         if (adj_field(C, w, v, sp)) {
@@ -404,6 +415,18 @@ tg_status tg_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
             for (size_t q = 0; q < P; q++) { host[3 * q] = a[q]; host[3 * q + 1] = b[q]; host[3 * q + 2] = c[q]; }
             return TG_OK;
         }
+        if (w == TG_F_WALL_ADJ) {
+            double *x, *y, *m;
+            adj_wall_field(C, x, y, m);
+            TG_CUDA(cudaStreamSynchronize(C->stream));
+            const size_t P = (size_t)C->g.mx * C->g.mz;
+            std::vector<double> a(P), b(P), c(P);
+            TG_CUDA(cudaMemcpy(a.data(), x, P * sizeof(double), cudaMemcpyDeviceToHost));
+            TG_CUDA(cudaMemcpy(b.data(), y, P * sizeof(double), cudaMemcpyDeviceToHost));
+            TG_CUDA(cudaMemcpy(c.data(), m, P * sizeof(double), cudaMemcpyDeviceToHost));
+            for (size_t q = 0; q < P; q++) { host[3 * q] = a[q]; host[3 * q + 1] = b[q]; host[3 * q + 2] = c[q]; }
+            return TG_OK;
+        }
         V3f<double> v;
         double *sp = nullptr;
         if (adj_field(C, w, v, sp)) {
@@ -426,7 +449,7 @@ constexpr int64_t kPetscVecClassId = 1211214;     // VEC_FILE_CLASSID
 // entries per point of a field in the file (0: not a grid field)
 int field_dof(tg_ctx *C, int w)
 {
-    if (w == TG_F_TAUWALL || w < 0 || w >= TG_F_COUNT) return 0;
+    if (w == TG_F_TAUWALL || w == TG_F_WALL_ADJ || w < 0 || w >= TG_F_COUNT) return 0;
     if (w == TG_F_P_ADJ || scal_field(C, w)) return 1;
     return 3;
 }

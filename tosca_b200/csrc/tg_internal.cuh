@@ -338,6 +338,7 @@ void tape_step_start(tg_ctx *C);
 void tape_nut(tg_ctx *C);
 void tape_stage(tg_ctx *C);
 bool adj_field(tg_ctx *C, int w, V3f<double> &v, double *&s);   // adjoint fields (allocated on first use)
+bool adj_wall_field(tg_ctx *C, double *&x, double *&y, double *&m);   // TG_F_WALL_ADJ planes
 void adj_destroy(tg_ctx *C);
 int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st);
 double *poisson_x(tg_ctx *C);
