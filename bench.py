@@ -297,56 +297,80 @@ def run_reference(args, rank, world):
     return 0
 
 
-def adjoint_ratio(dev, steps=4, warmup=8, cells=(128, 64, 64)):
-    """Adjoint/forward time of the step on the adjoint ABL (128 x 64 x 64 cells,
-    Cartesian, noSlip bottom, Smagorinsky, RK4, body force): device time of
-    tg_step per step against the device time per step of tg_adjoint_reverse
-    (each reversed step re-runs its forward step once to record the stages,
-    then runs the transposed kernels and the transposed pressure solve), with
-    a snapshot per step so that no further recomputation happens."""
+def adjoint_ratio(dev, steps=20, warmup=8, cells=(128, 64, 64)):
+    """Adjoint/forward time on the adjoint configuration: ABL 128 x 64 x 64
+    cells, Cartesian, Schumann wall function, Smagorinsky, RK4, 3-D body force;
+    objective J = sum (u - u_obs)^2 over the 64 x 64 hub-height probe plane
+    after `steps` steps (u_obs from a run with a seeded body-force
+    perturbation, seed 4). Device time of tg_step per step against the device
+    time per step of tg_adjoint_reverse seeded with dJ/dUcat: (a) every step's
+    tape kept (no forward step in the reversal), (b) binomial checkpointing
+    with half as many snapshots as steps (each reversed step re-runs its
+    forward step to record the stages, plus the schedule's recomputation)."""
     import tosca_b200
     from tosca_b200 import api, cases
     nx, ny, nz = cells
     cfg, nodes, ucat, p = cases.abl_case(nx=nx, ny=ny, nz=nz, Lx=10.0 * nx, Ly=10.0 * ny, H=1000.0 * nz / 128.0,
-                                         ddt=api.DDT_RK4, wall=api.BC_NOSLIP)
+                                         ddt=api.DDT_RK4)
     cfg.poisson_rtol = 1e-30
     cfg.poisson_div_tol = DIV_TOL
     cfg.poisson_maxit = 400
     cfg.source = 1
     cfg.device = dev
-    s = tosca_b200.gpu_solver(cfg)
-    cases.setup(s, nodes, ucat, p)
+    # probe plane: the j-plane of cell centres nearest 90 m, every second x cell, every y cell
+    zc = 0.5 * (nodes[0, :-2, 0, 2] + nodes[0, 1:-1, 0, 2])
+    jh, ks, is_ = 1 + int(np.argmin(np.abs(zc - 90.0))), np.arange(1, cfg.mz - 1, 2), np.arange(1, cfg.mx - 1)
+
+    def start(f):
+        s = tosca_b200.gpu_solver(cfg)
+        cases.setup(s, nodes, ucat, p)
+        s.set("SOURCE", f)
+        s.step(warmup)
+        return s
+
     rng = np.random.default_rng(4)
-    s.set("SOURCE", rng.standard_normal(ucat.shape) * 1e-3)
-    s.step(warmup)
+    f_obs = rng.standard_normal(ucat.shape) * 1e-3
+    f0 = np.random.default_rng(21).standard_normal(ucat.shape) * 1e-3
+    s = start(f_obs)
+    s.step(steps)
+    u_obs = s.get("UCAT")[ks][:, jh][:, is_, 0]
+    s.close()
+    s = start(f0)
+    x0 = {k: s.get(k) for k in ("UCONT", "UCAT", "P")}
     fwd = s.step(steps)
-    inside = np.zeros(p.shape, bool)
-    inside[1:-1, 1:-1, 1:-1] = True
-    seed = rng.standard_normal(ucat.shape) * inside[..., None]
-    out = {"workload": "adjoint ABL %dx%dx%d cells, RK4, Smagorinsky, noSlip bottom, body force, FP64" % (nx, ny, nz),
+    for k, v in x0.items():
+        s.set(k, v)
+    out = {"workload": "adjoint ABL %dx%dx%d cells, RK4, Smagorinsky, Schumann wall function, body force, FP64; "
+                       "J = hub-height 64x64 probe misfit after %d steps" % (nx, ny, nz, steps),
            "forward_ms_per_step": fwd.seconds / steps * 1e3, "steps": steps,
            "forward_poisson_iterations_per_step": fwd.poisson_total_iterations / steps}
-    # (a) every step's tape kept in device memory; (b) half as many snapshots as
-    # steps: binomial checkpointing, each reversed step re-runs its forward step
     for key, nsnap in (("tapes_kept", steps), ("checkpointed", max(1, steps // 2))):
         tst = s.adjoint_forward(steps, nsnap)
+        u = s.get("UCAT")
+        seed = np.zeros(ucat.shape)
+        seed[np.ix_(ks, [jh], is_, [0])] = 2.0 * (u[np.ix_(ks, [jh], is_, [0])] - u_obs[:, None, :, None])
+        J = float(((u[ks][:, jh][:, is_, 0] - u_obs) ** 2).sum())
         s.set("UCAT_ADJ", seed)
         s.set("UCONT_ADJ", np.zeros(ucat.shape)); s.set("P_ADJ", np.zeros(p.shape)); s.set("SOURCE_ADJ", np.zeros(ucat.shape))
+        s.set("WALL_ADJ", np.zeros((cfg.mz, cfg.mx, 3)))
         ast = s.adjoint_reverse()
         a_ms = ast.seconds / steps * 1e3
+        g = s.get("SOURCE_ADJ")
         out[key] = {"snapshots": int(ast.snapshots), "forward_steps_in_reversal": int(ast.forward_steps),
                     "adjoint_poisson_iterations_per_step": ast.poisson_iterations / steps,
                     "taped_forward_ms_per_step": tst.seconds / steps * 1e3,
-                    "adjoint_ms_per_step": a_ms, "adjoint_over_forward": a_ms / out["forward_ms_per_step"]}
+                    "adjoint_ms_per_step": a_ms, "adjoint_over_forward": a_ms / out["forward_ms_per_step"],
+                    "J": J, "grad_norm": float(np.linalg.norm(g))}
     s.close()
     out["adjoint_over_forward"] = out["tapes_kept"]["adjoint_over_forward"]
+    out["adjoint_over_forward_checkpointed"] = out["checkpointed"]["adjoint_over_forward"]
     return out
 
 
 def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     """Gradient of the farm power summed over `steps` steps with respect to the
-    turbines' C_T' (tg_set_farm_objective) on the farm workload with a noSlip
-    ground (the adjoint has no wall-function transpose), forward in
+    turbines' C_T' (tg_set_farm_objective) on the farm workload (Schumann wall
+    function on the ground), forward in
     `precision`: tg_adjoint_forward with binomial checkpointing in as many
     device snapshots as half the free HBM holds, then tg_adjoint_reverse from
     zero adjoint fields. Device time per reversed step against the device time
@@ -354,7 +378,7 @@ def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     import torch
     import tosca_b200
     from tosca_b200 import api, cases
-    cfg, nodes, ucat, p, turbines = cases.farm_case(ddt=api.DDT_RK4, wall=api.BC_NOSLIP)
+    cfg, nodes, ucat, p, turbines = cases.farm_case(ddt=api.DDT_RK4)
     cfg.poisson_rtol = 1e-30
     cfg.poisson_div_tol = DIV_TOL
     cfg.poisson_maxit = 400
@@ -379,11 +403,12 @@ def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     for k in ("UCONT_ADJ", "UCAT_ADJ", "SOURCE_ADJ"):
         solver.set(k, np.zeros(shape + (3,)))
     solver.set("P_ADJ", np.zeros(shape))
+    solver.set("WALL_ADJ", np.zeros((cfg.mz, cfg.mx, 3)))
     rv = solver.adjoint_reverse()
     g = solver.ct_gradient()
     solver.close()
     adj_ms = rv.seconds / steps * 1e3
-    return {"workload": "farm workload with a noSlip ground, %s forward" % precision, "steps": steps, "snapshots": int(rv.snapshots), "forward_steps_in_reversal": int(rv.forward_steps),
+    return {"workload": "farm workload (Schumann wall function), %s forward" % precision, "steps": steps, "snapshots": int(rv.snapshots), "forward_steps_in_reversal": int(rv.forward_steps),
             "recorded_forward_ms_per_step": fw.seconds / steps * 1e3, "adjoint_ms_per_step": adj_ms,
             "forward_ms_per_step": fwd_ms, "adjoint_over_forward": adj_ms / fwd_ms,
             "adjoint_poisson_iterations_per_step": rv.poisson_iterations / steps,
