@@ -304,9 +304,11 @@ def adjoint_ratio(dev, steps=20, warmup=8, cells=(128, 64, 64)):
     after `steps` steps (u_obs from a run with a seeded body-force
     perturbation, seed 4). Device time of tg_step per step against the device
     time per step of tg_adjoint_reverse seeded with dJ/dUcat: (a) every step's
-    tape kept (no forward step in the reversal), (b) binomial checkpointing
-    with half as many snapshots as steps (each reversed step re-runs its
-    forward step to record the stages, plus the schedule's recomputation)."""
+    tape kept (no forward step in the reversal), (b) the segment schedule
+    (a snapshot every 10 steps, each segment re-run taped once in the
+    reversal), (c) binomial checkpointing with half as many snapshots as steps
+    and no tapes (each reversed step re-runs its forward step to record the
+    stages, plus the schedule's recomputation)."""
     import tosca_b200
     from tosca_b200 import api, cases
     nx, ny, nz = cells
@@ -344,7 +346,13 @@ def adjoint_ratio(dev, steps=20, warmup=8, cells=(128, 64, 64)):
                        "J = hub-height 64x64 probe misfit after %d steps" % (nx, ny, nz, steps),
            "forward_ms_per_step": fwd.seconds / steps * 1e3, "steps": steps,
            "forward_poisson_iterations_per_step": fwd.poisson_total_iterations / steps}
-    for key, nsnap in (("tapes_kept", steps), ("checkpointed", max(1, steps // 2))):
+    # (a) every tape kept; (b) snapshots every 10 steps, the tapes of one
+    # segment re-recorded in the reversal (each step re-run once); (c) the
+    # binomial schedule over half as many snapshots as steps, no tapes. A first
+    # untimed pass captures the reversal's CUDA graphs.
+    for key, nsnap, tapes in (("warmup", steps, -1), ("tapes_kept", steps, -1), ("segments", max(1, steps // 10), 10),
+                              ("checkpointed", max(1, steps // 2), 0)):
+        s.adjoint_set_tapes(tapes)
         tst = s.adjoint_forward(steps, nsnap)
         u = s.get("UCAT")
         seed = np.zeros(ucat.shape)
@@ -356,6 +364,8 @@ def adjoint_ratio(dev, steps=20, warmup=8, cells=(128, 64, 64)):
         ast = s.adjoint_reverse()
         a_ms = ast.seconds / steps * 1e3
         g = s.get("SOURCE_ADJ")
+        if key == "warmup":
+            continue
         out[key] = {"snapshots": int(ast.snapshots), "forward_steps_in_reversal": int(ast.forward_steps),
                     "adjoint_poisson_iterations_per_step": ast.poisson_iterations / steps,
                     "taped_forward_ms_per_step": tst.seconds / steps * 1e3,
@@ -363,6 +373,7 @@ def adjoint_ratio(dev, steps=20, warmup=8, cells=(128, 64, 64)):
                     "J": J, "grad_norm": float(np.linalg.norm(g))}
     s.close()
     out["adjoint_over_forward"] = out["tapes_kept"]["adjoint_over_forward"]
+    out["adjoint_over_forward_segments"] = out["segments"]["adjoint_over_forward"]
     out["adjoint_over_forward_checkpointed"] = out["checkpointed"]["adjoint_over_forward"]
     return out
 

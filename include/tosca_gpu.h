@@ -349,10 +349,21 @@ tg_status tg_ct_gradient(tg_ctx *ctx, double *grad, int32_t reset);
  * gradient has the step's contribution added, and the state is again the one
  * at the start of the step (the step is re-run once to record its stages). */
 tg_status tg_adjoint_step(tg_ctx *ctx);
-/* nsteps forward steps from the current state with binomial (revolve)
- * checkpointing in nsnap device snapshots; leaves the final state in the
- * context (to seed the adjoint fields from it). */
+/* nsteps forward steps from the current state with checkpointing in at most
+ * nsnap device snapshots; leaves the final state in the context (to seed the
+ * adjoint fields from it). The reversal re-runs forward steps from the
+ * snapshots to record their stages (tapes). With nsnap >= nsteps and room in
+ * device memory every step's tape is kept and nothing is re-run. Otherwise,
+ * when tapes of k >= 2 steps fit (see tg_adjoint_set_tapes) and ceil(nsteps/k)
+ * snapshots suffice, snapshots are kept every k steps and the reversal re-runs
+ * each segment once, taped, before reversing it (every step runs forward once
+ * in the reversal); else a binomial (revolve) schedule over the snapshots. */
 tg_status tg_adjoint_forward(tg_ctx *ctx, int32_t nsteps, int32_t nsnap, tg_stats *stats);
+/* Cap on the step tapes the segment schedule of tg_adjoint_forward may hold:
+ * -1 (default) as many as 60 % of the free device memory holds, 0 none (the
+ * binomial schedule over the snapshots only), n > 0 at most n. No counterpart
+ * in the reference (it has no adjoint). */
+tg_status tg_adjoint_set_tapes(tg_ctx *ctx, int32_t max_tapes);
 /* Reverse sweep over the steps of the last tg_adjoint_forward, from the adjoint
  * fields of the final state to those of the initial state; the context returns
  * to the initial state. */

@@ -23,7 +23,8 @@ def declared_symbols():
 NO_CONTEXT = {"tg_continuity_error_noalloc"}
 # checkpointed adjoint drivers (device snapshots: the CPU restatement has the
 # per-step adjoint only), the CUDA-graph replay switch and the mesh classification
-GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse", "tg_set_graphs", "tg_graph_info", "tg_mesh_info"}
+GPU_ONLY = {"tg_adjoint_forward", "tg_adjoint_reverse", "tg_adjoint_set_tapes", "tg_set_graphs", "tg_graph_info",
+            "tg_mesh_info"}
 
 
 def test_header_matches_bindings():

@@ -134,11 +134,14 @@ def test_dot_product_with_central_difference_tangent(name):
     g.close()
 
 
-@pytest.mark.parametrize("name,nsteps,nsnap", [("abl", 4, 2), ("abl", 5, 5), ("abl_wall", 4, 2), ("abl_wall", 5, 5)])
-def test_gradient_with_checkpointing_matches_central_differences(name, nsteps, nsnap):
-    """dJ/df . v over N steps, reversed with a binomial checkpoint schedule,
-    against central differences of the CUDA step and of the oracle's CPU step
-    (the reference gradient)."""
+@pytest.mark.parametrize("name,nsteps,nsnap,tapes", [("abl", 4, 2, 0), ("abl", 5, 5, -1), ("abl_wall", 4, 2, 0),
+                                                     ("abl_wall", 5, 5, -1), ("abl_wall", 5, 3, 2), ("abl", 6, 3, -1)])
+def test_gradient_with_checkpointing_matches_central_differences(name, nsteps, nsnap, tapes):
+    """dJ/df . v over N steps, reversed with a binomial checkpoint schedule
+    (tapes = 0), every tape kept (nsnap = N) or the segment schedule (tapes of
+    k steps: each step re-run once in the reversal), against central
+    differences of the CUDA step and of the oracle's CPU step (the reference
+    gradient)."""
     rng = np.random.default_rng(5)
     cfg, nodes, ucat, p = _case(name, api.DDT_RK4)
     f0 = rng.standard_normal(ucat.shape) * 0.01
@@ -154,14 +157,19 @@ def test_gradient_with_checkpointing_matches_central_differences(name, nsteps, n
         s.close()
         return out
 
+    g.adjoint_set_tapes(tapes)
     st = g.adjoint_forward(nsteps, nsnap)
     assert st.steps == nsteps
     g.set("UCONT_ADJ", wu); g.set("UCAT_ADJ", wc); g.set("P_ADJ", np.zeros_like(p))
     g.set("SOURCE_ADJ", np.zeros_like(f0))
+    if cfg.bc[2] == api.BC_WALL_SHUMANN:
+        g.set("WALL_ADJ", np.zeros((cfg.mz, cfg.mx, 3)))
     ast = g.adjoint_reverse()
     assert ast.steps == nsteps
-    if nsnap < nsteps:
-        assert ast.forward_steps > nsteps           # recomputation happened
+    if nsnap < nsteps and tapes == 0:
+        assert ast.forward_steps > nsteps           # binomial schedule: recomputation happened
+    elif nsnap < nsteps:
+        assert ast.forward_steps == nsteps          # segment schedule: each step re-run once
     grad = g.get("SOURCE_ADJ")
     # the context is back at the initial state
     assert rel_l2(g.get("UCONT"), x0["UCONT"]) < 1e-14

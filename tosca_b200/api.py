@@ -233,6 +233,7 @@ _ADJ_SIGS = {
     "adjoint_step": (C.c_int, [C.c_void_p]),
     "adjoint_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(TgStats)]),
     "adjoint_reverse": (C.c_int, [C.c_void_p, C.POINTER(TgAdjointStats)]),
+    "adjoint_set_tapes": (C.c_int, [C.c_void_p, C.c_int32]),
     "set_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
     "graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
     "mesh_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
@@ -422,6 +423,10 @@ class Solver:
         st = TgStats()
         self._check(self.fns["adjoint_forward"](self.h, n, nsnap, C.byref(st)), "adjoint_forward")
         return st
+
+    def adjoint_set_tapes(self, max_tapes: int):
+        """Cap the step tapes of the segment checkpoint schedule (-1: memory decides, 0: none)."""
+        self._check(self.fns["adjoint_set_tapes"](self.h, max_tapes), "adjoint_set_tapes")
 
     def adjoint_reverse(self) -> TgAdjointStats:
         st = TgAdjointStats()

@@ -88,10 +88,14 @@ struct AdjState {
     Snapshot single{};                  // scratch state of tg_adjoint_step
     bool has_single = false;
     int base_it = 0, nsteps = 0, fwd_steps = 0;
+    int max_tapes = -1;                 // cap of the segment schedule's tapes (-1: memory decides)
+    int seg = 0;                        // segment length of the last forward run (0: other schedule)
     int64_t adj_iters = 0;                // Krylov iterations of the transposed solves
     bool recorded = false;
-    // CUDA graph of a reversed step reading the work tape
+    // CUDA graphs of a reversed step: reading the work tape, and reading each
+    // of the first stored tapes (no copy into the work tape)
     cudaGraphExec_t rev_exec = nullptr;
+    std::vector<cudaGraphExec_t> rev_store;
     bool rev_failed = false;
     // bounds of the recorded forward run
     int start_pos = 0;
@@ -1012,6 +1016,8 @@ void adj_graph_destroy(tg_ctx *C)
 {
     if (!C->adj) return;
     if (C->adj->rev_exec) cudaGraphExecDestroy(C->adj->rev_exec);
+    for (cudaGraphExec_t e : C->adj->rev_store) if (e) cudaGraphExecDestroy(e);
+    C->adj->rev_store.clear();
     C->adj->rev_exec = nullptr;
     C->adj->rev_failed = false;
 }
@@ -1148,11 +1154,11 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
     adj_scalar_ghosts(C, A.pha);
     k_adj_phi_compact<<<gint(g), block3(), 0, st>>>(g, A.pha, A.rhsc);
     // started from the previous reversed step's solution, to the context's
-    // relative tolerance when that lies in [1e-14, 1e-8], else to 1e-8 (the
-    // forward solve then stops on the divergence bound, whose relative
-    // residual is of the order of 1e-7)
+    // relative tolerance when that lies in [1e-14, 1e-8]; when the forward
+    // solve stops on the divergence bound instead, to 1e-7, the relative
+    // residual that bound leaves in the forward solve; else to 1e-8
     const double rt = C->cfg.poisson_rtol;
-    const double artol = (rt >= 1e-14 && rt <= 1e-8) ? rt : 1e-8;
+    const double artol = (rt >= 1e-14 && rt <= 1e-8) ? rt : (C->cfg.poisson_div_tol > 0.0 ? 1e-7 : 1e-8);
     int rc = 0;
     if (capture) {
         poisson_solve_adjoint_capture(C, A.rhsc, A.lam, artol);
@@ -1231,19 +1237,28 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
 // into the work tape when it is a stored one), or the sweep launched kernel by
 // kernel when profiling or step replay is off. A replayed sweep returns 0 and
 // reports through the SC_ADJ slots.
+constexpr int REV_STORE_GRAPHS = 64;   // stored tapes with their own reverse graph
+
 static int adjoint_reverse_step(tg_ctx *C)
 {
     AdjState &A = *C->adj;
     if (!C->graphs || C->prof.on || A.rev_failed) return adjoint_reverse_body(C, false);
+    cudaGraphExec_t *ex = &A.rev_exec;
     if (A.cur != &A.work_tape) {
-        copy_tape(C, A.work_tape, *A.cur);
-        A.cur = &A.work_tape;
+        const long q = A.cur - A.store.data();
+        if (q >= 0 && q < (long)A.store.size() && q < REV_STORE_GRAPHS) {
+            if ((long)A.rev_store.size() <= q) A.rev_store.resize(q + 1, nullptr);
+            ex = &A.rev_store[q];
+        } else {
+            copy_tape(C, A.work_tape, *A.cur);
+            A.cur = &A.work_tape;
+        }
     }
-    if (!A.rev_exec && !capture_graph(C, &A.rev_exec, [&]() { adjoint_reverse_body(C, true); })) {
+    if (!*ex && !capture_graph(C, ex, [&]() { adjoint_reverse_body(C, true); })) {
         A.rev_failed = true;
         return adjoint_reverse_body(C, false);
     }
-    TG_CUDA(cudaGraphLaunch(A.rev_exec, C->stream));
+    TG_CUDA(cudaGraphLaunch(*ex, C->stream));
     return 0;
 }
 
@@ -1478,8 +1493,21 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         }
         if (store) while ((int)A.store.size() < nsteps) A.store.push_back(make_tape(C));
         A.stored = store;
-        // nsnap snapshots for the schedule plus one scratch state of the adjoint step
-        const int want = store ? 2 : std::min(nsnap, nsteps) + 1;
+        // segment schedule: snapshots every seg steps, the tapes of one segment
+        int seg = 0;
+        if (!store && A.max_tapes != 0 && nsteps >= 2) {
+            size_t freeb = 0, totalb = 0;
+            TG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+            const int64_t budget = (int64_t)(freeb / 10 * 6);
+            int fit = (int)A.store.size() + (int)std::max<int64_t>(0, budget / (int64_t)tape_bytes(C));
+            if (A.max_tapes > 0) fit = std::min(fit, A.max_tapes);
+            fit = std::min(fit, nsteps);
+            if (fit >= 2 && (nsteps + fit - 1) / fit <= nsnap) seg = fit;
+        }
+        if (seg) while ((int)A.store.size() < seg) A.store.push_back(make_tape(C));
+        A.seg = seg;
+        // snapshots of the schedule plus one scratch state of the adjoint step
+        const int want = store ? 2 : (seg ? (nsteps + seg - 1) / seg + 1 : std::min(nsnap, nsteps) + 1);
         while ((int)A.snaps.size() < want) A.snaps.push_back(make_snapshot(C));
         while ((int)A.snaps.size() > want) A.snaps.pop_back();     // buffers stay owned by the context
         for (auto &sp : A.snaps) sp.pos = -1;
@@ -1503,7 +1531,7 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         save_state(C, A.snaps[0], 0);
         size_t next = 0;
-        if (store) keep.clear();
+        if (store || seg) keep.clear();
         bool any = false, last = false;
         for (int n = 0; n < nsteps; n++) {
             // a kept tape is recorded into the work tape and copied out
@@ -1515,6 +1543,7 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
             st->steps += 1;
             if (rc == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
             if (next < keep.size() && keep[next] == n + 1) { save_state(C, A.snaps[next + 1], n + 1); next++; }
+            if (seg && (n + 1) % seg == 0 && n + 1 < nsteps) save_state(C, A.snaps[(n + 1) / seg], n + 1);
         }
         TG_CUDA(cudaEventRecord(C->ev1, C->stream));
         if (step_stats_read(C, st, any, last) == 2) { C->err = "non-finite residual in the pressure solve"; return TG_ERR_NAN; }
@@ -1523,6 +1552,15 @@ tg_status tg_adjoint_forward(tg_ctx *C, int32_t nsteps, int32_t nsnap, tg_stats 
         st->seconds = ms * 1e-3;
         A.nsteps = nsteps;
         A.recorded = true;
+        return TG_OK;
+    });
+}
+
+tg_status tg_adjoint_set_tapes(tg_ctx *C, int32_t max_tapes)
+{
+    return adj_guard(C, [&]() -> tg_status {
+        if (max_tapes < -1) { C->err = "max_tapes must be -1, 0 or positive"; return TG_ERR_BAD_ARG; }
+        adj_state(C).max_tapes = max_tapes;
         return TG_OK;
     });
 }
@@ -1549,6 +1587,30 @@ tg_status tg_adjoint_reverse(tg_ctx *C, tg_adjoint_stats *stats)
                 int rc = adjoint_reverse_step(C);
                 if (rc) { C->err = "adjoint pressure solve failed"; return rc == 3 ? TG_ERR_BAD_ARG : TG_ERR_NOT_CONVERGED; }
                 st->steps += 1;
+            }
+        } else if (A.seg) {
+            // per segment, last first: re-run its steps taped from its snapshot, then reverse them
+            const int nseg = (A.nsteps + A.seg - 1) / A.seg;
+            for (int b = nseg - 1; b >= 0; b--) {
+                const int len = std::min(A.seg, A.nsteps - b * A.seg);
+                restore_state(C, A.snaps[b]);
+                for (int q = 0; q < len; q++) {
+                    // recorded into the work tape (a replayed taped step) and copied out
+                    A.cur = &A.work_tape;
+                    C->taping = true;
+                    tg_stats fs{};
+                    const int frc = step(C, &fs);
+                    C->taping = false;
+                    copy_tape(C, A.store[q], A.work_tape);
+                    st->forward_steps += 1;
+                    if (frc == 2) { C->err = "non-finite residual in a re-run forward step"; return TG_ERR_NAN; }
+                }
+                for (int q = len - 1; q >= 0; q--) {
+                    A.cur = &A.store[q];
+                    int rc = adjoint_reverse_step(C);
+                    if (rc) { C->err = "adjoint pressure solve failed"; return rc == 3 ? TG_ERR_BAD_ARG : TG_ERR_NOT_CONVERGED; }
+                    st->steps += 1;
+                }
             }
         } else {
             reverse_range(C, R, 0, A.nsteps, 0, st);
