@@ -72,8 +72,12 @@ enum {
 enum { TG_ILEFT = 0, TG_IRIGHT = 1, TG_JLEFT = 2, TG_JRIGHT = 3, TG_KLEFT = 4, TG_KRIGHT = 5 };
 
 /* ------------------------------------------------------------ configuration -- */
-/* temperature patch types (boundary/T, UpdateTemperatureBCs boundary.c:2052-2616) */
-enum { TG_TBC_ZERO_GRADIENT = 0, TG_TBC_FIXED_VALUE = 1, TG_TBC_FIXED_GRADIENT = 2, TG_TBC_PERIODIC = 3 };
+/* temperature patch types (boundary/T, UpdateTemperatureBCs boundary.c:2052-2616);
+ * TG_TBC_WALL_FUNCTION is thetaWallFunction, jLeft only (see t_wall_type) */
+enum { TG_TBC_ZERO_GRADIENT = 0, TG_TBC_FIXED_VALUE = 1, TG_TBC_FIXED_GRADIENT = 2, TG_TBC_PERIODIC = 3,
+       TG_TBC_WALL_FUNCTION = 4 };
+/* thetaWallFunction types (boundary/T "type", boundary.c:5110-5180) */
+enum { TG_TWALL_FIXED_FLUX = -2, TG_TWALL_SHUMANN = -3 };
 /* -dTdtScheme (teqn.c:66-230): explicit RK4; ABBE (Adams-Bashforth 2
  * convection, backward-Euler diffusion solved by GMRES on ABBEMatVec,
  * teqn_solvers.c:821-945); BE and BDF2 (implicit, Newton-Krylov on
@@ -138,6 +142,34 @@ typedef struct tg_config {
      * reference's, peqn.c:3885), 1 its linear, 2 (default) its quadratic
      * extrapolation from the previous two or three solutions; -1 = 2 */
     int32_t poisson_guess;
+    /* thetaWallFunction on the jLeft temperature patch (t_bc[TG_JLEFT] =
+     * TG_TBC_WALL_FUNCTION; needs teqn = 1 and les = 1). UpdateWallModelsT
+     * (boundary.c:3858-4178) sets the wall heat flux qWall of the j = 0
+     * faces, which FormT applies in place of the diffusive flux
+     * (teqn_solvers.c:337-352); the ghost temperature is zero-gradient.
+     * t_wall_type TG_TWALL_SHUMANN (-3): Schumann-Grotzbach with Monin-Obukhov
+     * stability (qWallShumann, wallfunctions.c:133-290) from the difference
+     * between the first-cell temperature and a surface temperature that starts
+     * at the wall value and rises by t_wall_heating_rate * dt every step;
+     * t_wall_localized 0 ("averaged") evaluates it once from plane means,
+     * 1 ("localized") per wall cell. TG_TWALL_FIXED_FLUX (-2): qWall =
+     * t_wall_qwall everywhere. */
+    int32_t t_wall_type;
+    int32_t t_wall_localized;
+    double  t_wall_qwall;          /* -2: heat flux (K m/s)                                  */
+    double  t_wall_heating_rate;   /* -3: heatingRate (K/s)                                  */
+    double  t_wall_kappa;          /* -3: kappa                                              */
+    double  t_wall_theta_ref;      /* -3: thetaRef (K)                                       */
+    double  t_wall_roughness;      /* -3: kRough (m)                                         */
+    double  t_wall_gamma_m;        /* -3: gammaM                                             */
+    double  t_wall_gamma_h;        /* -3: gammaH                                             */
+    double  t_wall_alpha_h;        /* -3: alphaH                                             */
+    /* stability correction of the velocity wall function -3 (uStarShumann,
+     * wallfunctions.c:12-130, boundary.c:3336-3420): with a thetaWallFunction
+     * on the temperature jLeft patch, the plane mean of its qWall enters the
+     * friction velocity; gammaM and thetaRef of velocityWallFunction */
+    double  wall_gamma_m;
+    double  wall_theta_ref;
 } tg_config;
 
 /* per-call statistics */
@@ -175,6 +207,10 @@ enum {
      * boundary.c:3490-3520), a plane of (mz x mx) triples (filtered x, filtered
      * y, running mean); carried from one reversed step to the one before */
     TG_F_WALL_ADJ,
+    /* thetaWallFunction state, planes of (mz x mx) scalars: the wall heat
+     * flux qWall of the last UpdateWallModelsT and the surface temperature of
+     * the -3 model (set by the first step from the wall value unless written) */
+    TG_F_QWALL, TG_F_SURF_THETA,
     TG_F_COUNT
 };
 
@@ -221,6 +257,10 @@ tg_status tg_update_nut(tg_ctx *ctx);                  /* les.h:73,76 / les.c:16
 tg_status tg_update_wall_models(tg_ctx *ctx);          /* boundary.h:188 / boundary.c:3257-3600    */
 tg_status tg_grad_p(tg_ctx *ctx);                      /* peqn.h:109 / peqn.c:3437-3773            */
 tg_status tg_buoyancy(tg_ctx *ctx);                    /* ueqn_sources.h:23 / ueqn_sources.c:2726  */
+/* with teqn = 1 (TG_ERR_STATE otherwise): the jLeft thetaWallFunction's
+ * qWall (TG_F_QWALL, TG_F_SURF_THETA) and the temperature ghost cells */
+tg_status tg_update_wall_models_t(tg_ctx *ctx);        /* boundary.h:191 / boundary.c:3858-4520    */
+tg_status tg_update_temperature_bcs(tg_ctx *ctx);      /* boundary.h:170 / boundary.c:2052-2616    */
 /* Rhs (TG_F_RHS) += scale * FormU on the current lUcont/lUcat/nut:
  * ueqn_solvers.h:15 / ueqn_solvers.c:6-1083 with formMode 0. Rhs is
  * zeroed first when zero_rhs. */

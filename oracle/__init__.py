@@ -36,6 +36,10 @@ def load():
         _LIB.tor_poisson_symmetric.restype = ctypes.c_int32
         _LIB.tor_poisson_symmetric.argtypes = [ctypes.c_void_p]
         _LIB.tor_num_threads.restype = ctypes.c_int32
+        _LIB.tor_mo_ustar.restype = ctypes.c_double
+        _LIB.tor_mo_ustar.argtypes = [ctypes.c_double] * 7
+        _LIB.tor_mo_qwall.restype = ctypes.c_double
+        _LIB.tor_mo_qwall.argtypes = [ctypes.c_double] * 9
     return _FNS
 
 
@@ -61,3 +65,13 @@ def poisson_matrix(s: api.Solver):
     L.tor_poisson_matrix(s.h, rp.ctypes.data_as(ctypes.c_void_p), col.ctypes.data_as(ctypes.c_void_p),
                          val.ctypes.data_as(ctypes.c_void_p))
     return sp.csr_matrix((val, col, rp), shape=(n, n))
+
+
+def mo_ustar(U, dist, z0, gamma_m, kappa, qwall, theta_ref) -> float:
+    """The restatement's uStarShumann (friction velocity for a wall heat flux)."""
+    return lib().tor_mo_ustar(U, dist, z0, gamma_m, kappa, qwall, theta_ref)
+
+
+def mo_qwall(U, dist, z0, gamma_m, gamma_h, alpha_h, theta_ref, delta_theta, kappa) -> float:
+    """The restatement's qWallShumann (wall heat flux for a temperature difference)."""
+    return lib().tor_mo_qwall(U, dist, z0, gamma_m, gamma_h, alpha_h, theta_ref, delta_theta, kappa)

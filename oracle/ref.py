@@ -55,6 +55,10 @@ def load(prebuilt_only: bool = False):
         _LIB.ref_poisson_nnz.argtypes = [ctypes.c_void_p]
         _LIB.ref_poisson_matrix.restype = ctypes.c_int
         _LIB.ref_poisson_matrix.argtypes = [ctypes.c_void_p] * 4
+        _LIB.ref_mo_ustar.restype = ctypes.c_double
+        _LIB.ref_mo_ustar.argtypes = [ctypes.c_double] * 7
+        _LIB.ref_mo_qwall.restype = ctypes.c_double
+        _LIB.ref_mo_qwall.argtypes = [ctypes.c_double] * 9
     return _FNS
 
 
@@ -75,3 +79,15 @@ def poisson_matrix(s: api.Solver):
     L.ref_poisson_matrix(s.h, rp.ctypes.data_as(ctypes.c_void_p), col.ctypes.data_as(ctypes.c_void_p),
                          val.ctypes.data_as(ctypes.c_void_p))
     return sp.csr_matrix((val, col, rp), shape=(n, n))
+
+
+def mo_ustar(U, dist, z0, gamma_m, kappa, qwall, theta_ref) -> float:
+    """TOSCA's uStarShumann (wallfunctions.c:12-130)."""
+    load()
+    return _LIB.ref_mo_ustar(U, dist, z0, gamma_m, kappa, qwall, theta_ref)
+
+
+def mo_qwall(U, dist, z0, gamma_m, gamma_h, alpha_h, theta_ref, delta_theta, kappa) -> float:
+    """TOSCA's qWallShumann (wallfunctions.c:133-290)."""
+    load()
+    return _LIB.ref_mo_qwall(U, dist, z0, gamma_m, gamma_h, alpha_h, theta_ref, delta_theta, kappa)

@@ -8,18 +8,23 @@
 //
 // The harness builds TOSCA's structures the way its set-up code would for one
 // rank (SetDistributedArrays, mesh.c:34-447; InitializeUEqn, ueqn.c:27-393;
-// InitializePEqn, peqn.c:35-103; InitializeLES, les.c:20-150; SetWallModels,
-// boundary.c:4640-4990), with the values a control.dat and boundary/ files
-// would hold, and then calls the reference's functions. Supported: periodic,
-// slip, noSlip and the Schumann velocity wall function (-3, averaged u*) on
-// jLeft; central and QUICK convection; FE and RK4; no LES or Smagorinsky
-// (TOSCA's hard-coded Cs^2 = 0.0289, les.c:10,175); the mean pressure
-// gradient. The HYPRE solve inside SolvePEqn is replaced by a tight solve of
-// the captured matrix (petsc_stub.cpp).
+// InitializePEqn, peqn.c:35-103; InitializeLES, les.c:20-150; InitializeTEqn,
+// teqn.c:19-257; SetWallModels, boundary.c:4640-5200), with the values a
+// control.dat and boundary/ files would hold, and then calls the reference's
+// functions. Supported: periodic, slip, noSlip and the Schumann velocity wall
+// function (-3, averaged u*) on jLeft; central and QUICK convection; FE and
+// RK4; no LES or Smagorinsky (TOSCA's hard-coded Cs^2 = 0.0289,
+// les.c:10,175); the mean pressure gradient; the potential temperature
+// (teqn.c, solvers/teqn_solvers.c) with RK4, Boussinesq buoyancy or the
+// p-tilde form, zeroGradient / fixedValue / fixedGradient / periodic
+// patches and the jLeft thetaWallFunction (-2, -3). The HYPRE solve inside
+// SolvePEqn is replaced by a tight solve of the captured matrix
+// (petsc_stub.cpp).
 #include "include/base.h"
 #include "include/domain.h"
 #include "include/io.h"
 #include "include/inline.h"
+#include "include/wallfunctions.h"
 
 #include <memory>
 #include <stdexcept>
@@ -84,9 +89,52 @@ wallModel *make_shumann(const tg_config &c)
     Shumann *s = new Shumann();
     s->wfEvalType = "averaged";                 // plane-averaged friction velocity
     s->kappa = c.wall_kappa;
-    s->thetaRef = c.t_ref;
+    s->thetaRef = c.wall_theta_ref;             // these two enter only stratified (qWall != 0) evaluations
     s->roughness = c.wall_roughness;
-    s->gammaM = 4.8;                            // enters only stratified (qWall != 0) evaluations
+    s->gammaM = c.wall_gamma_m;
+    w->wmShumann = s;
+    return w;
+}
+
+const char *t_bc_name(int t)
+{
+    switch (t) {
+    case TG_TBC_ZERO_GRADIENT: return "zeroGradient";
+    case TG_TBC_FIXED_VALUE: return "fixedValue";
+    case TG_TBC_FIXED_GRADIENT: return "fixedGradient";
+    case TG_TBC_PERIODIC: return "periodic";
+    case TG_TBC_WALL_FUNCTION: return "thetaWallFunction";
+    default: return "";
+    }
+}
+
+// the jLeft thetaWallFunction of SetWallModels (boundary.c:5110-5160): the
+// qWall patch field (zero), the Shumann constants, tLast = -1, surfaceTheta unset
+wallModel *make_theta_wall(const tg_config &c)
+{
+    wallModel *w = new wallModel();
+    const PetscInt mz = c.mz, mx = c.mx;
+    PetscReal **q[3];
+    for (PetscReal **&a : q) {
+        a = new PetscReal *[mz];
+        for (PetscInt k = 0; k < mz; k++) a[k] = new PetscReal[mx]();
+    }
+    w->qWall.x = q[0]; w->qWall.y = q[1]; w->qWall.z = q[2];
+    Shumann *s = new Shumann();
+    if (c.t_wall_type == TG_TWALL_SHUMANN) {
+        s->wfEvalType = c.t_wall_localized ? "localized" : "averaged";
+        s->kappa = c.t_wall_kappa;
+        s->thetaRef = c.t_wall_theta_ref;
+        s->roughness = c.t_wall_roughness;
+        s->gammaM = c.t_wall_gamma_m;
+        s->gammaH = c.t_wall_gamma_h;
+        s->alphaH = c.t_wall_alpha_h;
+        s->heatingRate = c.t_wall_heating_rate;
+        s->tLast = -1.0;
+        s->surfaceThetaSet = 0;
+    } else {
+        s->qWall = c.t_wall_qwall;
+    }
     w->wmShumann = s;
     return w;
 }
@@ -106,6 +154,7 @@ struct tg_ctx {
     ueqn_ ueqn{};
     peqn_ peqn{};
     les_ les{};
+    teqn_ teqn{};
     double last_div = 0.0;
 };
 
@@ -265,6 +314,40 @@ void build(tg_ctx &X)
     VecDuplicate(m.lCsi, &l.lSy);
     VecDuplicate(m.lCsi, &l.lSz);
     VecDuplicate(m.lAj, &l.lS);
+
+    // ---- temperature (InitializeTEqn, teqn.c:19-257, RK4; bTheta, ueqn.c:56-60;
+    // the boundary/T patches and the thetaWallFunction of SetWallModels)
+    if (c.teqn) {
+        f.isTeqnActive = 1;
+        teqn_ &t = X.teqn;
+        t.access = &a;
+        a.teqn = &t;
+        d.teqn = &t;
+        t.pTildeFormulation = c.p_tilde ? 1 : 0;
+        for (Vec *v : {&t.TmprtTmp, &t.Tmprt, &t.Tmprt_o, &t.bT, &t.Rhs, &t.sourceT}) VecDuplicate(m.Nvert, v);
+        for (Vec *v : {&t.lTmprt, &t.lTmprt_o}) VecDuplicate(m.lAj, v);
+        for (Vec *v : {&t.lDivT, &t.lViscT}) VecDuplicate(m.lCent, v);
+        if (t.pTildeFormulation) {
+            VecDuplicate(m.lAj, &t.lRhoK);
+            VecDuplicate(m.Cent, &t.ghGradRhok);
+            VecDuplicate(m.Cent, &t.ghGradRhok_o);
+        }
+        t.ddtScheme = "RK4";
+        t.solverType = "EXP";
+        t.hyperVisc4i = t.hyperVisc4j = t.hyperVisc4k = 0.0;
+        VecDuplicate(m.Cent, &u.bTheta);
+        VecDuplicate(m.Cent, &u.bTheta_o);
+        scalarBC &bt = m.boundaryT;
+        word *names[6] = {&bt.iLeft, &bt.iRight, &bt.jLeft, &bt.jRight, &bt.kLeft, &bt.kRight};
+        PetscReal *vals[6] = {&bt.iLval, &bt.iRval, &bt.jLval, &bt.jRval, &bt.kLval, &bt.kRval};
+        for (int q = 0; q < 6; q++) { *names[q] = t_bc_name(c.t_bc[q]); *vals[q] = c.t_bc_value[q]; }
+        bt.iLWF = bt.iRWF = bt.jRWF = bt.kLWF = bt.kRWF = 0;
+        bt.jLWF = 0;
+        if (c.t_bc[2] == TG_TBC_WALL_FUNCTION) {
+            bt.jLWF = c.t_wall_type;
+            t.jLWM = make_theta_wall(c);
+        }
+    }
 }
 
 // ------------------------------------------------------------ field access
@@ -307,6 +390,10 @@ FieldRef field(tg_ctx &X, int w)
     case TG_F_P: r = {m.da, p.P, p.lP}; break;
     case TG_F_PHI: r = {m.da, p.Phi, p.lPhi}; break;
     case TG_F_NUT: r = {m.da, nullptr, X.cfg.les ? X.les.lNu_t : nullptr}; break;
+    case TG_F_TMPRT: if (X.cfg.teqn) r = {m.da, X.teqn.Tmprt, X.teqn.lTmprt}; break;
+    case TG_F_BTHETA:
+        if (X.cfg.teqn) r = {m.fda, X.cfg.p_tilde ? X.teqn.ghGradRhok : u.bTheta, nullptr};
+        break;
     default: break;
     }
     return r;
@@ -351,7 +438,15 @@ tg_status ref_create(const tg_config *cfg, tg_ctx **out)
     }
     // supported subset of the workloads (see the file header)
     if (c.ddt_scheme != TG_DDT_FE && c.ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
-    if (c.buoyancy || c.teqn || c.source || c.p_tilde) return TG_ERR_BAD_ARG;
+    // the reference applies buoyancy exactly when the temperature equation is on
+    if (c.source || (c.buoyancy != 0) != (c.teqn != 0)) return TG_ERR_BAD_ARG;
+    if (c.teqn && c.t_ddt_scheme != TG_TDDT_RK4) return TG_ERR_BAD_ARG;
+    for (int q = 0; q < 6; q++) {
+        if (c.teqn && (c.t_bc[q] < 0 || c.t_bc[q] > TG_TBC_WALL_FUNCTION)) return TG_ERR_BAD_ARG;
+        if (c.teqn && c.t_bc[q] == TG_TBC_WALL_FUNCTION && q != 2) return TG_ERR_BAD_ARG;
+    }
+    if (c.teqn && c.t_bc[2] == TG_TBC_WALL_FUNCTION &&
+        (!c.les || (c.t_wall_type != TG_TWALL_SHUMANN && c.t_wall_type != TG_TWALL_FIXED_FLUX))) return TG_ERR_BAD_ARG;
     if (c.les && std::fabs(c.cs - TOSCA_STD_CS) > 1e-15) return TG_ERR_BAD_ARG;
     tg_ctx *C = new tg_ctx();
     C->cfg = c;
@@ -444,6 +539,21 @@ tg_status ref_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
                     h[0] = C->ueqn.jLWM->tauWall.x[k][i];
                     h[1] = C->ueqn.jLWM->tauWall.y[k][i];
                     h[2] = C->ueqn.jLWM->tauWall.z[k][i];
+                }
+            return TG_OK;
+        }
+        if (w == TG_F_QWALL || w == TG_F_SURF_THETA) {
+            wallModel *wm = C->cfg.teqn ? C->teqn.jLWM : nullptr;
+            if (!wm) return fail(C, TG_ERR_BAD_ARG, "no thetaWallFunction");
+            const Shumann *sh = wm->wmShumann;
+            const PetscInt mx = C->cfg.mx, mz = C->cfg.mz;
+            for (PetscInt k = 0; k < mz; k++)
+                for (PetscInt i = 0; i < mx; i++) {
+                    double v = 0.0;
+                    if (w == TG_F_QWALL) v = wm->qWall.z[k][i];
+                    else if (C->cfg.t_wall_type == TG_TWALL_SHUMANN && sh->surfaceThetaSet && k >= 1 && k <= mz - 2 && i >= 1 && i <= mx - 2)
+                        v = sh->surfaceTheta[k][i];
+                    host[(size_t)k * mx + i] = v;
                 }
             return TG_OK;
         }
@@ -547,19 +657,37 @@ tg_status ref_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
         ueqn_ &u = C->ueqn;
         peqn_ &p = C->peqn;
         tg_stats local{};
+        teqn_ *t = C->cfg.teqn ? &C->teqn : nullptr;
         for (int32_t s = 0; s < nsteps; s++) {
-            VecCopy(u.Ucont, u.Ucont_o);                            // main.c:77
-            if (C->cfg.les) {                                       // main.c:104-117
+            VecCopy(u.Ucont, u.Ucont_o);                            // main.c:81
+            if (t) VecCopy(t->Tmprt, t->Tmprt_o);                   // main.c:83-99 (RK4)
+            if (C->cfg.les) {                                       // main.c:108-113
                 UpdateCs(&C->les);
                 UpdateNut(&C->les);
                 UpdateWallModelsU(&u);
             }
             GradP(&p);                                              // main.c:146-153
-            SolveUEqn(&u);                                          // main.c:183
-            SolvePEqn(&p);                                          // main.c:186
-            contravariantToCartesian(&u);                           // main.c:189
+            if (t) {                                                // main.c:166-182
+                if (C->clock.it > C->clock.itStart) {
+                    if (t->pTildeFormulation) VecCopy(t->ghGradRhok, t->ghGradRhok_o);
+                    else VecCopy(u.bTheta, u.bTheta_o);
+                }
+                if (t->pTildeFormulation) ghGradRhoK(t);
+                else Buoyancy(&u, 1.0);
+            }
+            SolveUEqn(&u);                                          // main.c:185
+            SolvePEqn(&p);                                          // main.c:188
+            contravariantToCartesian(&u);                           // main.c:191
+            if (t) {                                                // main.c:194-205
+                // UpdateCsk / UpdatekT (lesScalar.c, not compiled here) set the
+                // scalar SGS fields of the dynamic models, which FormT reads
+                // only for those models, not for Smagorinsky
+                UpdateWallModelsT(t);
+                SolveTEqn(t);
+            }
             ContinuityErrorsOptimized(&p);                          // main.c:211
             tgref_printed_value("Time step continuity error:", &C->last_div);
+            if (t) UpdateTemperatureBCs(t);                         // main.c:274-278
             UpdateCartesianBCs(&u);                                 // main.c:284
             UpdateContravariantBCs(&u);                             // main.c:287
             SyncPressureAcrossDomains(C->dom.get());                // main.c:318
@@ -585,7 +713,49 @@ tg_status ref_poisson_matrix(tg_ctx *, int64_t *rowptr, int64_t *col, double *va
     return TG_OK;
 }
 
-tg_status ref_buoyancy(tg_ctx *C) { return fail(C, TG_ERR_BAD_ARG, "not provided by the reference harness"); }
+// Buoyancy (ueqn_sources.c:2726-2820) or, with -pTildeBuoyancy, ghGradRhoK (teqn.c:278-652)
+tg_status ref_buoyancy(tg_ctx *C)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!C->cfg.teqn) return fail(C, TG_ERR_STATE, "the reference applies buoyancy only with its temperature equation");
+        if (C->teqn.pTildeFormulation) ghGradRhoK(&C->teqn);
+        else Buoyancy(&C->ueqn, 1.0);
+        return TG_OK;
+    });
+}
+
+// UpdateWallModelsT (boundary.c:3858-4520) and UpdateTemperatureBCs (boundary.c:2052-2616)
+tg_status ref_update_wall_models_t(tg_ctx *C)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!C->cfg.teqn) return fail(C, TG_ERR_STATE, "no temperature equation");
+        UpdateWallModelsT(&C->teqn);
+        return TG_OK;
+    });
+}
+tg_status ref_update_temperature_bcs(tg_ctx *C)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (!C->cfg.teqn) return fail(C, TG_ERR_STATE, "no temperature equation");
+        UpdateTemperatureBCs(&C->teqn);
+        return TG_OK;
+    });
+}
+
+// the Monin-Obukhov functions themselves (wallfunctions.c:12-290)
+double ref_mo_ustar(double U, double dist, double z0, double gammaM, double kappa, double qwall, double thetaRef)
+{
+    double us = 0.0, phiM = 0.0, L = 0.0;
+    uStarShumann(U, dist, z0, gammaM, kappa, qwall, thetaRef, us, phiM, L, 0, 0, 0);
+    return us;
+}
+double ref_mo_qwall(double U, double dist, double z0, double gammaM, double gammaH, double alphaH, double thetaRef,
+                    double deltaTheta, double kappa)
+{
+    double q = 0.0, us = 0.0, phiM = 0.0, phiH = 0.0, L = 0.0;
+    qWallShumann(U, dist, z0, gammaM, gammaH, alphaH, thetaRef, deltaTheta, kappa, q, us, phiM, phiH, L, 0, 0, 0);
+    return q;
+}
 
 // entry points of the C-ABI the harness does not provide
 #define REF_UNSUPPORTED(name, ...) \

@@ -122,6 +122,10 @@ struct tg_ctx {
     // adjoints of the wall-model state (ufx, ufy, umean) and, within one
     // reversed step, of the wall stress (tosca_oracle_adjoint.inc)
     std::vector<double> wadj_x, wadj_y, wadj_m, twa_x, twa_y, twa_z;
+    // jLeft thetaWallFunction: qWall.z and the -3 model's surfaceTheta
+    // (planes k*mx + i), surfaceThetaSet (tosca_oracle_teqn.inc)
+    std::vector<double> qwall, surf_theta;
+    bool surf_set = false;
 
     // pressure system
     Csr A;
@@ -933,8 +937,134 @@ void updateNut(tg_ctx &C)
 }
 
 // ---------------------------------------------------------------------------
+// Monin-Obukhov surface-layer relations of the Schumann-Grotzbach wall
+// functions (wallfunctions.c:12-290). Both iterate the friction velocity (and
+// the heat flux) with under-relaxation 0.5 to a change below 1e-5 or 500
+// sweeps (then the neutral values), clamp |L| >= 1e-10, cap the unstable
+// zeta at -1/15 + 1e-8 and use the Businger-Dyer psi functions; a stable
+// result with u* < 1e-2 (no root) is replaced by the u* of the bisection on
+// the slope of U_model(u*) (at most 50 halvings of [1e-6, u*_neutral]).
+// The steps are those of the reference so that the stopping sweep, and with
+// it the result, is the same.
+// ---------------------------------------------------------------------------
+constexpr double kMoG = 9.81, kMoTol = 1e-5, kMoOmega = 0.5;
+constexpr int kMoIterMax = 500;
+
+// Businger-Dyer stability functions at zeta = z/L (psiM, psiH, phiM, phiH)
+void moStability(double zeta, bool stable, double gammaM, double gammaH, double alphaH,
+                 double &psiM, double &psiH, double &phiM, double &phiH)
+{
+    if (stable) {
+        psiM = -gammaM * zeta; psiH = -gammaH * zeta;
+        phiM = 1.0 + gammaM * zeta; phiH = alphaH + gammaH * zeta;
+    } else {
+        if (zeta < -1.0 / 15.0) zeta = -1.0 / 15.0 + 1e-8;
+        const double xi = std::pow(1.0 - 15.0 * zeta, 0.25);
+        psiM = 2.0 * std::log((1.0 + xi) / 2.0) + std::log((1.0 + xi * xi) / 2.0) - 2.0 * std::atan(xi) + M_PI / 2.0;
+        psiH = 2.0 * std::log((1.0 + xi * xi) / 2.0);
+        phiM = std::pow(1.0 - 15.0 * zeta, -0.25);
+        phiH = alphaH * std::pow(1.0 - 15.0 * zeta, -0.5);
+    }
+}
+
+double moClampL(double L) { return (L > 0) ? std::max(1e-10, L) : std::min(-1e-10, L); }
+
+// the slope proxy (U_model(u) - U) / u of the stable bisection, L from a fixed heat flux q
+double moStableSlope(double u, double U, double wallDist, double z0, double gammaM, double kappa, double q, double thetaRef)
+{
+    const double Lq = std::max(1e-10, -std::pow(u, 3.0) / (kappa * (kMoG / thetaRef) * q));
+    const double psiM = -gammaM * (wallDist / Lq);
+    return ((u / kappa) * (std::log(wallDist / z0) - psiM) - U) / u;
+}
+
+// bisection for the extremum of U_model (wallfunctions.c:88-128, 240-286)
+double moStableBisection(double U, double wallDist, double z0, double gammaM, double kappa, double q, double thetaRef,
+                         double uNeutral)
+{
+    double uLow = 1e-6, uHigh = uNeutral, uMid = 0.0;
+    for (int it = 0; it < 50; it++) {
+        uMid = 0.5 * (uLow + uHigh);
+        const double dfMid = moStableSlope(uMid, U, wallDist, z0, gammaM, kappa, q, thetaRef);
+        if (std::fabs(uHigh - uLow) < 1e-6 || std::fabs(dfMid) < kMoTol) break;
+        const double dfLow = moStableSlope(uLow, U, wallDist, z0, gammaM, kappa, q, thetaRef);
+        if ((dfLow > 0 && dfMid > 0) || (dfLow < 0 && dfMid < 0)) uLow = uMid;
+        else uHigh = uMid;
+    }
+    return uMid;
+}
+
+// uStarShumann, wallfunctions.c:12-130: friction velocity for a given wall heat flux
+double uStarShumann(double U, double wallDist, double z0, double gammaM, double kappa, double qwall, double thetaRef)
+{
+    if (wallDist <= z0) throw OracleError("wall distance is smaller than the roughness length");
+    const double logLaw = std::log(wallDist / z0);
+    const double uN = std::max(0.0, (kappa * U) / logLaw);
+    if (std::fabs(qwall) < 1e-6) return uN;
+    double u0 = uN, diff = 1e30;
+    int iter = 0;
+    do {
+        const double L0 = moClampL(-std::pow(u0, 3.0) / (kappa * (kMoG / thetaRef) * qwall));
+        double psiM, psiH, phiM, phiH;
+        moStability(wallDist / L0, L0 > 0, gammaM, 0.0, 0.0, psiM, psiH, phiM, phiH);
+        const double uNew = std::max(0.0, (kappa * U) / (logLaw - psiM));
+        u0 = kMoOmega * uNew + (1.0 - kMoOmega) * u0;
+        diff = std::fabs(uNew - u0);
+        iter++;
+    } while (diff > kMoTol && iter < kMoIterMax);
+    if (iter == kMoIterMax) return uN;
+    const double L = moClampL(-std::pow(u0, 3.0) / (kappa * (kMoG / thetaRef) * qwall));
+    if (L > 0 && u0 < 1e-2) return moStableBisection(U, wallDist, z0, gammaM, kappa, qwall, thetaRef, uN);
+    return u0;
+}
+
+// qWallShumann, wallfunctions.c:133-290: wall heat flux (and u*) for a
+// temperature difference deltaTheta between the first cell and the surface
+double qWallShumann(double U, double wallDist, double z0, double gammaM, double gammaH, double alphaH, double thetaRef,
+                    double deltaTheta, double kappa)
+{
+    if (wallDist <= z0) throw OracleError("wall distance is smaller than the roughness length");
+    const double uN = std::max(0.0, (kappa * U) / std::log(wallDist / z0));
+    double qN = (-deltaTheta * uN * kappa) / (alphaH * std::log(wallDist / z0));
+    if (std::fabs(qN) < 1e-6) qN = (qN < 0 ? -1.0 : 1.0) * 1e-6;        // signNonZero, inline.h:335-341
+    if (deltaTheta == 0.0) return qN;
+    double u0 = uN, q0 = qN, du = 1e30, dq = 1e30;
+    int iter = 0;
+    do {
+        const double L0 = moClampL(-std::pow(u0, 3.0) / (kappa * (kMoG / thetaRef) * q0));
+        double psiM, psiH, phiM, phiH;
+        moStability(wallDist / L0, L0 > 0, gammaM, gammaH, alphaH, psiM, psiH, phiM, phiH);
+        const double uNew = std::max(0.0, (kappa * U) / (std::log(wallDist / z0) - psiM));
+        u0 = kMoOmega * uNew + (1.0 - kMoOmega) * u0;
+        const double qNew = (-deltaTheta * u0 * kappa) / (alphaH * std::log(wallDist / z0) - psiH);
+        q0 = kMoOmega * qNew + (1.0 - kMoOmega) * q0;
+        du = std::fabs(uNew - u0);
+        dq = std::fabs(qNew - q0);
+        iter++;
+    } while ((du > kMoTol || dq > kMoTol) && iter < kMoIterMax);
+    if (iter == kMoIterMax) return qN;
+    const double L = moClampL(-std::pow(u0, 3.0) / (kappa * (kMoG / thetaRef) * q0));
+    if (L > 0 && u0 < 1e-2) {
+        // the bisection's L uses the neutral heat flux
+        const double us = moStableBisection(U, wallDist, z0, gammaM, kappa, qN, thetaRef, uN);
+        const double Lf = std::max(1e-10, -std::pow(us, 3.0) / (kappa * (kMoG / thetaRef) * qN));
+        const double psiH = -gammaH * (wallDist / Lf);
+        return (-deltaTheta * us * kappa) / (alphaH * std::log(wallDist / z0) - psiH);
+    }
+    return q0;
+}
+
+// the jLeft temperature patch carries a thetaWallFunction whose qWall enters
+// the velocity wall function (boundary.c:3348-3356)
+bool thetaWallCoupled(const tg_ctx &C)
+{
+    return C.c.teqn && C.c.t_bc[TG_JLEFT] == TG_TBC_WALL_FUNCTION;
+}
+
+// ---------------------------------------------------------------------------
 // UpdateWallModelsU, boundary.c:3257-3600: jLeft wall function -3 (Schumann,
-// neutral, plane-averaged friction velocity; wallfunctions.c:12-84)
+// plane-averaged friction velocity, wallfunctions.c:12-130; stratified by
+// the plane mean of the last temperature wall heat flux when the temperature
+// jLeft patch is a thetaWallFunction, neutral otherwise)
 // ---------------------------------------------------------------------------
 void updateWallModels(tg_ctx &C)
 {
@@ -962,11 +1092,15 @@ void updateWallModels(tg_ctx &C)
         V3 Up, n; parallel(k, i, Up, n);
         sumU += mag(Up); sumD += s; cnt++;
     }
+    double qWall = 0.0;
+    if (thetaWallCoupled(C)) {
+        for (int k = 1; k < mz - 1; k++)
+        for (int i = 1; i < mx - 1; i++) qWall += C.qwall[C.W(k, i)];
+        qWall = qWall / cnt;
+    }
     double Umean = sumU / cnt, dist = sumD / cnt;
     double z0 = C.c.wall_roughness, kappa = C.c.wall_kappa;
-    if (dist <= z0) throw OracleError("wall distance is smaller than the roughness length");
-    double logLaw = std::log(dist / z0);
-    double uStar = std::max(0.0, (kappa * Umean) / logLaw);   // neutral branch, qWall = 0
+    double uStar = uStarShumann(Umean, dist, z0, C.c.wall_gamma_m, kappa, qWall, C.c.wall_theta_ref);
     if (!C.ufilt_set) {
         for (int k = 1; k < mz - 1; k++)
         for (int i = 1; i < mx - 1; i++) {
@@ -1622,6 +1756,7 @@ int step(tg_ctx &C, tg_stats *st)
     else if (rc != 2) rc |= urc;
     contravariantToCartesian(C);                         // main.c:201
     if (C.c.teqn) {                                      // main.c:194-205
+        updateWallModelsT(C);                            // main.c:201
         const int trc = solveTEqn(C);
         if (trc == 2) rc = 2;
         else if (rc != 2) rc |= trc;
@@ -1649,7 +1784,7 @@ void allocState(tg_ctx &C)
     zero(C.rhs_o, G);
     const size_t P = (size_t)C.mx * C.mz;
     for (auto *v : {&C.twx, &C.twy, &C.twz, &C.umean, &C.ufx, &C.ufy, &C.ufz, &C.wadj_x, &C.wadj_y, &C.wadj_m,
-                    &C.twa_x, &C.twa_y, &C.twa_z}) zero(*v, P);
+                    &C.twa_x, &C.twa_y, &C.twa_z, &C.qwall, &C.surf_theta}) zero(*v, P);
 }
 
 std::vector<V3> *vecField(tg_ctx &C, int w)
@@ -1731,6 +1866,22 @@ const char *tor_status_string(tg_status s)
 
 const char *tor_last_error(const tg_ctx *C) { return C ? C->err.c_str() : "null context"; }
 
+// a thetaWallFunction needs LES (UpdateWallModelsT returns without it and
+// FormT applies qWall only with LES), one of the two types, and with -3 the
+// positive constants its logarithms and divisions use; with the velocity
+// wall function it also needs that one's thetaRef
+static bool theta_wall_config_ok(const tg_config *cfg)
+{
+    if (!cfg->les) return false;
+    if (cfg->t_wall_type == TG_TWALL_SHUMANN) {
+        if (!(cfg->t_wall_kappa > 0) || !(cfg->t_wall_theta_ref > 0) || !(cfg->t_wall_roughness > 0) || !(cfg->t_wall_alpha_h > 0))
+            return false;
+        if (cfg->t_wall_localized != 0 && cfg->t_wall_localized != 1) return false;
+    } else if (cfg->t_wall_type != TG_TWALL_FIXED_FLUX) return false;
+    if (cfg->bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && !(cfg->wall_theta_ref > 0)) return false;
+    return true;
+}
+
 tg_status tor_create(const tg_config *cfg, tg_ctx **out)
 {
     if (!cfg || !out) return TG_ERR_BAD_ARG;
@@ -1751,9 +1902,11 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
         if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;
         if (cfg->t_gmres_restart < 0 || cfg->t_gmres_restart > 60) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
-            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
+            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > TG_TBC_WALL_FUNCTION) return TG_ERR_BAD_ARG;
+            if (cfg->t_bc[p] == TG_TBC_WALL_FUNCTION && p != TG_JLEFT) return TG_ERR_BAD_ARG;
             if ((cfg->t_bc[p] == TG_TBC_PERIODIC) != (cfg->bc[p] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
         }
+        if (cfg->t_bc[TG_JLEFT] == TG_TBC_WALL_FUNCTION && !theta_wall_config_ok(cfg)) return TG_ERR_BAD_ARG;
     }
     tg_ctx *C = new (std::nothrow) tg_ctx();
     if (!C) return TG_ERR_ALLOC;
@@ -1797,6 +1950,12 @@ tg_status tor_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
             for (size_t q = 0; q < (size_t)C->mx * C->mz; q++) { C->wadj_x[q] = host[3 * q]; C->wadj_y[q] = host[3 * q + 1]; C->wadj_m[q] = host[3 * q + 2]; }
             return TG_OK;
         }
+        if (w == TG_F_QWALL || w == TG_F_SURF_THETA) {
+            std::vector<double> &d = w == TG_F_QWALL ? C->qwall : C->surf_theta;
+            std::memcpy(d.data(), host, sizeof(double) * d.size());
+            if (w == TG_F_SURF_THETA) C->surf_set = true;
+            return TG_OK;
+        }
         if (auto *v = vecField(*C, w)) { copyIn<3>(*C, (double *)v->data(), host, halo); return TG_OK; }
         if (auto *s = scalField(*C, w)) { copyIn<1>(*C, s->data(), host, halo); return TG_OK; }
         return fail(C, TG_ERR_BAD_ARG, "field not settable");
@@ -1814,6 +1973,11 @@ tg_status tor_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
         }
         if (w == TG_F_WALL_ADJ) {
             for (size_t q = 0; q < (size_t)C->mx * C->mz; q++) { host[3 * q] = C->wadj_x[q]; host[3 * q + 1] = C->wadj_y[q]; host[3 * q + 2] = C->wadj_m[q]; }
+            return TG_OK;
+        }
+        if (w == TG_F_QWALL || w == TG_F_SURF_THETA) {
+            const std::vector<double> &d = w == TG_F_QWALL ? C->qwall : C->surf_theta;
+            std::memcpy(host, d.data(), sizeof(double) * d.size());
             return TG_OK;
         }
         if (auto *v = vecField(*C, w)) { copyOut<3>(*C, host, (const double *)v->data(), halo); return TG_OK; }
@@ -1916,6 +2080,23 @@ TOR_STAGE(tor_solve_u, solveUEqn(*C))
 TOR_STAGE(tor_update_cartesian_bcs, updateCartesianBCs(*C))
 TOR_STAGE(tor_update_contravariant_bcs, updateContravariantBCs(*C))
 TOR_STAGE(tor_sync_pressure, syncPressure(*C))
+TOR_STAGE(tor_update_wall_models_t,
+          if (!C->c.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); updateWallModelsT(*C))
+TOR_STAGE(tor_update_temperature_bcs,
+          if (!C->c.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); updateTemperatureBCs(*C))
+
+// the Monin-Obukhov functions of the restatement, for comparison with the reference's
+double tor_mo_ustar(double U, double dist, double z0, double gammaM, double kappa, double qwall, double thetaRef)
+{
+    try { return uStarShumann(U, dist, z0, gammaM, kappa, qwall, thetaRef); }
+    catch (...) { return std::nan(""); }
+}
+double tor_mo_qwall(double U, double dist, double z0, double gammaM, double gammaH, double alphaH, double thetaRef,
+                    double deltaTheta, double kappa)
+{
+    try { return qWallShumann(U, dist, z0, gammaM, gammaH, alphaH, thetaRef, deltaTheta, kappa); }
+    catch (...) { return std::nan(""); }
+}
 
 tg_status tor_form_u(tg_ctx *C, double scale, int32_t zero_rhs)
 {

@@ -117,3 +117,92 @@ def test_p_tilde_buoyancy():
     cfg.buoyancy = 0
     with pytest.raises(api.TgError):
         oracle.solver(cfg)
+
+
+# ------------------------------------------------------ thermal wall function
+def _sabl(**kw):
+    cfg, nodes, ucat, p, T = cases.stratified_abl_case(16, 12, 12, t_amp=0.5, **kw)
+    cfg.poisson_rtol = 1e-14
+    return cfg, nodes, ucat, p, T
+
+
+def test_fixed_heat_flux_enters_the_heat_budget():
+    """qWall = q (-2) at the ground, zero-gradient top and periodic sides: the
+    volume integral of T grows by q * (ground area) * dt per step; the RK4
+    convection and the interior diffusion telescope (wall-normal fluxes
+    vanish). The air above the 100 m perturbed layer is uniform (no lapse
+    rate), so that the top ghosts, which the RK4 stages do not update, carry
+    no flux within the three steps."""
+    cfg, nodes, ucat, p, T = _sabl(lapse=0.0)
+    cases.thermal_wall(cfg, api.TWALL_FIXED_FLUX, qwall=0.08)
+    cfg.t_bc_value = (0.0,) * 6
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    vol = 1.0 / s.get("AJ")[1:-1, 1:-1, 1:-1]
+    area = s.get("JETA")[1:-1, 0, 1:-1, 2].sum()
+    heat = lambda: float((s.get("TMPRT")[1:-1, 1:-1, 1:-1] * vol).sum())
+    h0 = heat()
+    s.step(3)
+    expect = 3 * cfg.dt * 0.08 * area
+    assert abs(heat() - h0 - expect) <= 1e-9 * expect
+    assert np.all(s.get("QWALL")[1:-1, 1:-1] == 0.08)
+    s.close()
+
+
+@pytest.mark.parametrize("heating_rate,sign", [(-0.02, -1.0), (0.02, 1.0)])
+def test_surface_temperature_and_heat_flux_sign(heating_rate, sign):
+    """-3: the surface starts at the wall value and moves by heatingRate * dt
+    per step; a cooling surface draws heat out of the air (qWall < 0, stable),
+    a heating one puts heat in (qWall > 0, unstable); averaged: one value."""
+    cfg, nodes, ucat, p, T = _sabl(heating_rate=heating_rate)
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    t_wall = 0.5 * (T[1:-1, 1, 1:-1] + T[1:-1, 0, 1:-1])
+    s.step(4)
+    st = s.get("SURF_THETA")[1:-1, 1:-1]
+    assert np.abs(st - (t_wall + 4 * heating_rate * cfg.dt)).max() <= 1e-12 * 300.0
+    q = s.get("QWALL")[1:-1, 1:-1]
+    assert np.all(q == q[0, 0]) and sign * q[0, 0] > 0
+    s.close()
+
+
+def test_localized_heat_flux_varies_per_cell():
+    cfg, nodes, ucat, p, T = _sabl(heating_rate=0.02, localized=True)
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    s.step(2)
+    q = s.get("QWALL")[1:-1, 1:-1]
+    assert q.std() > 0 and np.all(q > 0)
+    s.close()
+
+
+def test_stratification_changes_the_friction_velocity():
+    """The velocity wall function reads the plane mean of the last qWall: the
+    wall stress of a stable step differs from the neutral one, and is
+    neutral on the first step (qWall still zero)."""
+    taus = []
+    for kind in (None, api.TWALL_SHUMANN):
+        cfg, nodes, ucat, p, T = _sabl(heating_rate=-0.05)
+        if kind is None:
+            bc = list(cfg.t_bc); bc[2] = api.TBC_ZERO_GRADIENT; cfg.t_bc = tuple(bc)
+        s = oracle.solver(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        s.set("SURF_THETA", np.full((cfg.mz, cfg.mx), 299.0))    # 1 K below the air: unstable
+        out = []
+        for _ in range(2):
+            s.step(1)
+            out.append(s.get("TAUWALL"))
+        taus.append(out)
+        s.close()
+    assert np.array_equal(taus[0][0], taus[1][0])
+    assert rel_l2(taus[1][1], taus[0][1], lambda a: a) > 1e-3
+
+
+def test_thermal_wall_configuration_checked():
+    cfg, nodes, ucat, p, T = _sabl()
+    for bad in (dict(les=0), dict(t_wall_type=-1), dict(t_wall_theta_ref=0.0), dict(wall_theta_ref=0.0),
+                dict(t_wall_localized=2), dict(t_bc=(api.TBC_PERIODIC, api.TBC_PERIODIC, api.TBC_ZERO_GRADIENT,
+                                                     api.TBC_WALL_FUNCTION, api.TBC_PERIODIC, api.TBC_PERIODIC))):
+        c = api.Config(**{**cfg.__dict__, **bad})
+        with pytest.raises(api.TgError):
+            oracle.solver(c)

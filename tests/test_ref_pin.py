@@ -18,16 +18,28 @@ file compares, stage by stage and over whole steps:
   the time step of main.c:54-327 (SolveUEqn with FE / RK4, SolvePEqn with
   SetRHS, UpdatePressure, ProjectVelocity, the BC updates, the gauge of
   SyncPressureAcrossDomains)                 Ucont, Ucat, P after 3 steps
+  Buoyancy (ueqn_sources.c:2726), ghGradRhoK (teqn.c:278-652),
+  UpdateTemperatureBCs (boundary.c:2052-2616) bTheta, the T ghosts
+  uStarShumann, qWallShumann (wallfunctions.c:12-290), swept over their
+  branches
+  the step with the temperature equation (SolveTEqn with TeqnRK4 and FormT,
+  teqn.c:259, teqn_solvers.c:6-818), Boussinesq buoyancy, and the jLeft
+  thetaWallFunction (UpdateWallModelsT, boundary.c:3858-4520) coupled into
+  the velocity wall function (boundary.c:3336-3420)
+                                             Ucont, Ucat, P, T, qWall and
+                                             the surface temperature after 3 steps
 
 on the Taylor-Green box, the ABL (Smagorinsky, Schumann wall stress, mean
-pressure gradient) and the curvilinear hill (QUICK, Smagorinsky, wall stress).
+pressure gradient), the curvilinear hill (QUICK, Smagorinsky, wall stress)
+and the stratified ABL and hill with the thermal wall function.
 The HYPRE solve inside SolvePEqn is the one stand-in that computes: a tight
 Krylov solve of the captured pinned matrix (unique solution), like the
 oracle's own solve. The reference hard-codes the Smagorinsky constant
 (Cs^2 = 0.0289, les.c:10), so these cases use cs = 0.0289; the hill runs
 without buoyancy, which the reference applies only with its temperature
-equation. The harness compiles from the reference checkout; without it and
-without a prebuilt oracle/_ref/libtosca_ref.so the tests skip."""
+equation (with it, the hill cases below). The harness compiles from the
+reference checkout; without it and without a prebuilt
+oracle/_ref/libtosca_ref.so the tests skip."""
 import numpy as np
 import pytest
 
@@ -165,3 +177,101 @@ def test_unsupported_configuration_is_refused():
     cfg.cs = 0.01               # the reference hard-codes Cs^2 = 0.0289
     with pytest.raises(api.TgError):
         R.solver(cfg)
+
+
+# ---------------------------------------------------------------- temperature
+def _pair_t(case, kind=api.TWALL_SHUMANN, heating_rate=-0.01, localized=False, qwall=0.0, p_tilde=0):
+    if case == "sabl":
+        cfg, nodes, ucat, p, T = cases.stratified_abl_case(16, 12, 12, heating_rate=heating_rate, localized=localized,
+                                                           t_amp=0.5)
+    else:
+        cfg, nodes, ucat, p, T = cases.hill_case(24, 12, 12, teqn=True, t_amp=0.5)
+        if kind is not None:
+            cases.thermal_wall(cfg, api.TWALL_SHUMANN, heating_rate=heating_rate, localized=localized)
+    if kind is not None:
+        cfg.t_wall_type, cfg.t_wall_qwall = kind, qwall
+    cfg.cs, cfg.poisson_rtol, cfg.p_tilde = 0.0289, 1e-14, p_tilde
+    o = oracle.solver(cfg)
+    cases.setup(o, nodes, ucat, p, T)
+    r = R.solver(cfg)
+    r.set_mesh_nodes(nodes)
+    for f in ("UCONT", "UCAT", "P", "TMPRT"):
+        r.set(f, o.get(f))
+    return o, r
+
+
+@pytest.mark.parametrize("p_tilde", [0, 1])
+def test_buoyancy_and_temperature_bcs(p_tilde):
+    """Buoyancy / ghGradRhoK and UpdateTemperatureBCs on the stratified hill.
+    With -pTildeBuoyancy the C-ABI's TG_F_BTHETA holds -ghGradRhok (the AB2
+    sum of ExplicitRhsU then reads like the Buoyancy one)."""
+    o, r = _pair_t("hill", kind=None, p_tilde=p_tilde)
+    o.Buoyancy(); r.Buoyancy()
+    sign = -1.0 if p_tilde else 1.0
+    assert rel_l2(sign * r.get("BTHETA"), o.get("BTHETA"), _full) < 1e-14
+    t = o.get("TMPRT")
+    t[:, 0, :] += 3.0                                       # stale ghosts, rewritten by the update
+    t[:, -1, :] -= 2.0
+    for s in (o, r):
+        s.set("TMPRT", t)
+        s.UpdateTemperatureBCs()
+    assert np.array_equal(r.get("TMPRT"), o.get("TMPRT"))
+    o.close(); r.close()
+
+
+def _mo_samples():
+    """Inputs that reach every branch of the Monin-Obukhov functions: neutral
+    (dT = 0, |q| < 1e-6), stable, unstable with and without the zeta cap, the
+    stable no-root case that bisects, and wide ranges of U, distance and z0."""
+    rng = np.random.default_rng(11)
+    out = [(5.0, 10.0, 0.1, 0.0), (5.0, 10.0, 0.1, 1.0), (5.0, 10.0, 0.1, -1.0),
+           (0.1, 1.0, 0.1, 5.0), (0.05, 3.0, 0.1, 8.0), (20.0, 50.0, 0.01, -10.0)]
+    for _ in range(3000):
+        out.append((10 ** rng.uniform(-2, 1.3), 10 ** rng.uniform(-0.2, 2), 10 ** rng.uniform(-3, -0.7),
+                    rng.choice([0.0, rng.normal(0, 3), rng.normal(0, 0.05)])))
+    return out
+
+
+def test_monin_obukhov_functions():
+    worst_q = worst_u = 0.0
+    bisect = unstable_cap = 0
+    for U, d, z0, dT in _mo_samples():
+        q_ref = R.mo_qwall(U, d, z0, 4.8, 7.8, 1.0, 300.0, dT, 0.4)
+        q_or = oracle.mo_qwall(U, d, z0, 4.8, 7.8, 1.0, 300.0, dT, 0.4)
+        worst_q = max(worst_q, abs(q_or - q_ref) / max(abs(q_ref), 1e-300))
+        for q in (0.0, 5e-7, q_ref, -q_ref):
+            u_ref = R.mo_ustar(U, d, z0, 4.8, 0.4, q, 300.0)
+            u_or = oracle.mo_ustar(U, d, z0, 4.8, 0.4, q, 300.0)
+            worst_u = max(worst_u, abs(u_or - u_ref) / max(abs(u_ref), 1e-300))
+            bisect += 0 < u_ref < 1e-2 and q < 0
+            unstable_cap += q > 0 and -(u_ref ** 3) / (0.4 * 9.81 / 300.0 * q) > -15.0 * d
+    # the reference is compiled without FMA contraction, the restatement with it
+    assert worst_q < 1e-13 and worst_u < 1e-13, (worst_q, worst_u)
+    assert bisect > 10 and unstable_cap > 10
+
+
+@pytest.mark.parametrize("case,kind,localized,heating_rate,qwall", [
+    ("sabl", api.TWALL_SHUMANN, False, -0.01, 0.0),      # cooling surface: stable
+    ("sabl", api.TWALL_SHUMANN, True, 0.02, 0.0),        # heating surface: unstable, per cell
+    ("sabl", api.TWALL_FIXED_FLUX, False, 0.0, 0.05),
+    ("hill", api.TWALL_SHUMANN, False, -0.01, 0.0),
+    ("hill", api.TWALL_SHUMANN, True, -0.01, 0.0),
+    ("hill", None, False, 0.0, 0.0),                     # temperature without a wall function
+])
+def test_steps_with_temperature(case, kind, localized, heating_rate, qwall):
+    """Three steps with the temperature equation against TOSCA's loop: the
+    velocity wall function of each step reads the qWall of the step before."""
+    o, r = _pair_t(case, kind, heating_rate, localized, qwall)
+    for _ in range(3):
+        so, sr = o.step(1), r.step(1)
+        assert sr.max_divergence < 1e-12 and so.max_divergence < 1e-12
+    for f in ("UCONT", "UCAT", "TMPRT"):
+        assert rel_l2(r.get(f), o.get(f)) < 1e-12, f
+    assert rel_l2(r.get("P"), o.get("P")) < (1e-9 if case == "hill" else 1e-10)
+    if kind is not None:
+        qr, qo = r.get("QWALL"), o.get("QWALL")
+        assert np.abs(qr).max() > 0
+        assert np.abs(qo - qr).max() <= 1e-9 * np.abs(qr).max()
+        assert np.abs(o.get("SURF_THETA") - r.get("SURF_THETA")).max() <= 1e-12 * 300.0
+        assert rel_l2(r.get("TAUWALL"), o.get("TAUWALL"), _full) < 1e-12
+    o.close(); r.close()

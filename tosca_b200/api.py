@@ -23,7 +23,8 @@ NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
 TDDT_RK4, TDDT_ABBE, TDDT_BE, TDDT_BDF2 = 0, 1, 2, 3
-TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC = 0, 1, 2, 3
+TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION = 0, 1, 2, 3, 4
+TWALL_FIXED_FLUX, TWALL_SHUMANN = -2, -3
 PREC_FP64, PREC_MIXED = 0, 1
 
 FIELDS = [
@@ -33,6 +34,7 @@ FIELDS = [
     "P", "PHI", "NUT", "TMPRT", "TAUWALL", "SOURCE",
     "UCONT_ADJ", "UCAT_ADJ", "P_ADJ", "SOURCE_ADJ",
     "FARM_FORCE", "FARM_CONT", "WALL_ADJ",
+    "QWALL", "SURF_THETA",
 ]
 F = {name: i for i, name in enumerate(FIELDS)}
 SCALAR_FIELDS = {"AJ", "IAJ", "JAJ", "KAJ", "P", "PHI", "NUT", "TMPRT", "P_ADJ"}
@@ -78,6 +80,18 @@ class TgConfig(C.Structure):
         ("t_rtol", C.c_double),
         ("p_tilde", C.c_int32),
         ("poisson_guess", C.c_int32),
+        ("t_wall_type", C.c_int32),
+        ("t_wall_localized", C.c_int32),
+        ("t_wall_qwall", C.c_double),
+        ("t_wall_heating_rate", C.c_double),
+        ("t_wall_kappa", C.c_double),
+        ("t_wall_theta_ref", C.c_double),
+        ("t_wall_roughness", C.c_double),
+        ("t_wall_gamma_m", C.c_double),
+        ("t_wall_gamma_h", C.c_double),
+        ("t_wall_alpha_h", C.c_double),
+        ("wall_gamma_m", C.c_double),
+        ("wall_theta_ref", C.c_double),
     ]
 
 
@@ -175,6 +189,20 @@ class Config:
     t_rtol: float = 1e-30
     p_tilde: int = 0
     poisson_guess: int = 2
+    # thetaWallFunction on the jLeft temperature patch (t_bc[2] = TBC_WALL_FUNCTION)
+    t_wall_type: int = TWALL_SHUMANN
+    t_wall_localized: int = 0
+    t_wall_qwall: float = 0.0
+    t_wall_heating_rate: float = 0.0
+    t_wall_kappa: float = 0.4
+    t_wall_theta_ref: float = 300.0
+    t_wall_roughness: float = 0.1
+    t_wall_gamma_m: float = 4.8
+    t_wall_gamma_h: float = 7.8
+    t_wall_alpha_h: float = 1.0
+    # stability correction of the velocity wall function (with a thetaWallFunction)
+    wall_gamma_m: float = 4.8
+    wall_theta_ref: float = 300.0
 
     def to_c(self) -> TgConfig:
         c = TgConfig()
@@ -207,6 +235,8 @@ _SIGS = {
     "update_wall_models": (C.c_int, [C.c_void_p]),
     "grad_p": (C.c_int, [C.c_void_p]),
     "buoyancy": (C.c_int, [C.c_void_p]),
+    "update_wall_models_t": (C.c_int, [C.c_void_p]),
+    "update_temperature_bcs": (C.c_int, [C.c_void_p]),
     "form_u": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "explicit_rhs": (C.c_int, [C.c_void_p]),
     "solve_u": (C.c_int, [C.c_void_p]),
@@ -318,18 +348,27 @@ class Solver:
         assert nodes.shape == self.shape + (3,)
         self._check(self.fns["set_mesh_nodes"](self.h, _ptr(nodes)), "set_mesh_nodes")
 
-    def get(self, name: str, halo: int = 0) -> np.ndarray:
+    def field_shape(self, name: str, halo: int = 0) -> tuple:
+        """Host array shape of a field: planes (mz, mx[, 3]) for the wall-model
+        fields, (mz, my, mx[, 3]) plus 2*halo per direction otherwise."""
         mz, my, mx = self.shape
         if name in ("TAUWALL", "WALL_ADJ"):
-            out = np.zeros((mz, mx, 3))
-        else:
-            shp = (mz + 2 * halo, my + 2 * halo, mx + 2 * halo)
-            out = np.zeros(shp if name in SCALAR_FIELDS else shp + (3,))
+            return (mz, mx, 3)
+        if name in ("QWALL", "SURF_THETA"):
+            return (mz, mx)
+        shp = (mz + 2 * halo, my + 2 * halo, mx + 2 * halo)
+        return shp if name in SCALAR_FIELDS else shp + (3,)
+
+    def get(self, name: str, halo: int = 0) -> np.ndarray:
+        out = np.zeros(self.field_shape(name, halo))
         self._check(self.fns["get_field"](self.h, F[name], _ptr(out), halo), f"get_field {name}")
         return out
 
     def set(self, name: str, arr: np.ndarray, halo: int = 0):
         arr = np.ascontiguousarray(arr, dtype=np.float64)
+        want = self.field_shape(name, halo)
+        if arr.size != int(np.prod(want)):
+            raise ValueError(f"set_field {name}: {arr.shape} does not match {want}")
         self._check(self.fns["set_field"](self.h, F[name], _ptr(arr), halo), f"set_field {name}")
 
     # ----------------------------------------------------- TOSCA field files
@@ -379,6 +418,12 @@ class Solver:
 
     def Buoyancy(self):
         self._check(self.fns["buoyancy"](self.h), "Buoyancy")
+
+    def UpdateWallModelsT(self):
+        self._check(self.fns["update_wall_models_t"](self.h), "UpdateWallModelsT")
+
+    def UpdateTemperatureBCs(self):
+        self._check(self.fns["update_temperature_bcs"](self.h), "UpdateTemperatureBCs")
 
     def FormU(self, scale: float = 1.0, zero_rhs: bool = True):
         self._check(self.fns["form_u"](self.h, scale, 1 if zero_rhs else 0), "FormU")

@@ -14,6 +14,8 @@ Workloads (synthetic, seeded; no dataset is involved):
   hill       terrain-following mesh over a 2-D cosine hill, QUICK, stable
              Boussinesq stratification, frozen or transported temperature
   farm       abl with uniform actuator disks
+  sabl       stratified abl: transported potential temperature with Boussinesq
+             buoyancy and a thetaWallFunction at the ground (thermal_wall)
 """
 from __future__ import annotations
 
@@ -22,7 +24,8 @@ import math
 import numpy as np
 
 from .api import (BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, DDT_FE, DDT_RK4, DIV_CENTRAL, DIV_QUICK,
-                  NUTBC_FIXEDVALUE, NUTBC_PERIODIC, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_ZERO_GRADIENT, Config)
+                  NUTBC_FIXEDVALUE, NUTBC_PERIODIC, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION,
+                  TBC_ZERO_GRADIENT, TWALL_FIXED_FLUX, TWALL_SHUMANN, Config)
 
 
 # --------------------------------------------------------------------- grids
@@ -257,6 +260,61 @@ def hill_case(nx: int = 192, ny: int = 96, nz: int = 96, dt: float = 0.5, ustar:
         if t_amp:
             T = T + t_amp * uniform_noise(seed + 11, G, 0).reshape(mz, my, mx) * interior
     p = np.zeros((mz, my, mx))
+    return cfg, nodes, ucat, p, T
+
+
+def thermal_wall(cfg: Config, kind: int = TWALL_SHUMANN, heating_rate: float = 0.0, qwall: float = 0.0,
+                 localized: bool = False, gamma_m: float = 4.8, gamma_h: float = 7.8, alpha_h: float = 1.0) -> Config:
+    """Puts a thetaWallFunction on the ground (jLeft) temperature patch of a
+    configuration with transported temperature and LES: Schumann-Grotzbach
+    with a surface heating rate (K/s), or a fixed heat flux qwall (K m/s).
+    The roughness, kappa and thetaRef follow the velocity wall function and
+    tRef; the same gammaM and thetaRef correct the velocity wall function."""
+    bc = list(cfg.t_bc)
+    bc[2] = TBC_WALL_FUNCTION
+    cfg.t_bc = tuple(bc)
+    cfg.t_wall_type = kind
+    cfg.t_wall_localized = int(localized)
+    cfg.t_wall_qwall = qwall
+    cfg.t_wall_heating_rate = heating_rate
+    cfg.t_wall_kappa = cfg.wall_kappa
+    cfg.t_wall_theta_ref = cfg.t_ref
+    cfg.t_wall_roughness = cfg.wall_roughness
+    cfg.t_wall_gamma_m, cfg.t_wall_gamma_h, cfg.t_wall_alpha_h = gamma_m, gamma_h, alpha_h
+    cfg.wall_gamma_m, cfg.wall_theta_ref = gamma_m, cfg.t_ref
+    return cfg
+
+
+def stratified_abl_case(nx: int = 256, ny: int = 256, nz: int = 128, theta0: float = 300.0, lapse: float = 0.01,
+                        inversion: float = 100.0, t_amp: float = 0.1, heating_rate: float = -0.25 / 3600.0,
+                        localized: bool = False, seed: int = 31, **kw):
+    """Stably stratified ABL (abl_case grid and flow) with transported
+    potential temperature: theta0 up to `inversion` m, then rising by `lapse`
+    K/m, seeded +-t_amp K perturbations below the inversion, Boussinesq
+    buoyancy (tRef = theta0), RK4 for both equations, Pr 0.7, the lapse rate
+    as the fixed gradient at the top and a Schumann-Grotzbach
+    thetaWallFunction at the ground whose surface cools at `heating_rate`
+    K/s (the GABLS1 rate by default). Returns cfg, nodes, ucat, p, T."""
+    cfg, nodes, ucat, p = abl_case(nx=nx, ny=ny, nz=nz, **kw)
+    cfg.ddt_scheme = DDT_RK4
+    cfg.buoyancy, cfg.t_ref = 1, theta0
+    cfg.teqn, cfg.prandtl = 1, 0.7
+    cfg.t_bc = (TBC_PERIODIC, TBC_PERIODIC, TBC_ZERO_GRADIENT, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_PERIODIC)
+    cfg.t_bc_value = (0.0, 0.0, 0.0, lapse, 0.0, 0.0)
+    thermal_wall(cfg, TWALL_SHUMANN, heating_rate=heating_rate, localized=localized)
+    cent = cell_centres(nodes)
+    z = cent[..., 2]
+    mz, my, mx = z.shape
+    T = theta0 + lapse * np.maximum(z - inversion, 0.0)
+    below = (z < inversion)
+    T = T + t_amp * uniform_noise(seed, mx * my * mz, 0).reshape(mz, my, mx) * below
+    T[:, 0, :] = T[:, 1, :]
+    dz_top = nodes[:, my - 2, :, 2] - nodes[:, my - 3, :, 2]          # height of the top cells
+    T[:, -1, :] = T[:, -2, :] + lapse * dz_top
+    T[:, :, 0] = T[:, :, -2]
+    T[:, :, -1] = T[:, :, 1]
+    T[0] = T[-2]
+    T[-1] = T[1]
     return cfg, nodes, ucat, p, T
 
 

@@ -197,6 +197,22 @@ const char *tg_status_string(tg_status s)
 
 const char *tg_last_error(const tg_ctx *C) { return C ? C->err.c_str() : "null context"; }
 
+// a thetaWallFunction needs LES (UpdateWallModelsT returns without it and
+// FormT applies qWall only with LES), one of the two types, and with -3 the
+// positive constants its logarithms and divisions use; with the velocity
+// wall function it also needs that one's thetaRef
+static bool theta_wall_config_ok(const tg_config *cfg)
+{
+    if (!cfg->les) return false;
+    if (cfg->t_wall_type == TG_TWALL_SHUMANN) {
+        if (!(cfg->t_wall_kappa > 0) || !(cfg->t_wall_theta_ref > 0) || !(cfg->t_wall_roughness > 0) || !(cfg->t_wall_alpha_h > 0))
+            return false;
+        if (cfg->t_wall_localized != 0 && cfg->t_wall_localized != 1) return false;
+    } else if (cfg->t_wall_type != TG_TWALL_FIXED_FLUX) return false;
+    if (cfg->bc[TG_JLEFT] == TG_BC_WALL_SHUMANN && !(cfg->wall_theta_ref > 0)) return false;
+    return true;
+}
+
 tg_status tg_create(const tg_config *cfg, tg_ctx **out)
 {
     if (!cfg || !out) return TG_ERR_BAD_ARG;
@@ -217,9 +233,11 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         if (cfg->t_ddt_scheme < TG_TDDT_RK4 || cfg->t_ddt_scheme > TG_TDDT_BDF2) return TG_ERR_BAD_ARG;
         if (cfg->t_gmres_restart < 0 || cfg->t_gmres_restart > 60) return TG_ERR_BAD_ARG;
         for (int p = 0; p < 6; p++) {
-            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > 3) return TG_ERR_BAD_ARG;
+            if (cfg->t_bc[p] < 0 || cfg->t_bc[p] > TG_TBC_WALL_FUNCTION) return TG_ERR_BAD_ARG;
+            if (cfg->t_bc[p] == TG_TBC_WALL_FUNCTION && p != TG_JLEFT) return TG_ERR_BAD_ARG;
             if ((cfg->t_bc[p] == TG_TBC_PERIODIC) != (cfg->bc[p] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
         }
+        if (cfg->t_bc[TG_JLEFT] == TG_TBC_WALL_FUNCTION && !theta_wall_config_ok(cfg)) return TG_ERR_BAD_ARG;
     }
     tg_ctx *C = new (std::nothrow) tg_ctx();
     if (!C) return TG_ERR_ALLOC;
@@ -242,6 +260,13 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         p.z0 = cfg->wall_roughness; p.kappa = cfg->wall_kappa;
         p.teqn = cfg->teqn; p.prandtl = cfg->prandtl;
         for (int q = 0; q < 6; q++) { p.t_bc[q] = cfg->t_bc[q]; p.t_bc_value[q] = cfg->t_bc_value[q]; }
+        p.t_wall = (cfg->teqn && cfg->t_bc[TG_JLEFT] == TG_TBC_WALL_FUNCTION) ? cfg->t_wall_type : 0;
+        p.wall_coupled = p.t_wall != 0;
+        p.t_wall_localized = cfg->t_wall_localized;
+        p.tw_qwall = cfg->t_wall_qwall; p.tw_heating = cfg->t_wall_heating_rate; p.tw_kappa = cfg->t_wall_kappa;
+        p.tw_theta_ref = cfg->t_wall_theta_ref; p.tw_z0 = cfg->t_wall_roughness; p.tw_gamma_m = cfg->t_wall_gamma_m;
+        p.tw_gamma_h = cfg->t_wall_gamma_h; p.tw_alpha_h = cfg->t_wall_alpha_h;
+        p.wall_gamma_m = cfg->wall_gamma_m; p.wall_theta_ref = cfg->wall_theta_ref;
         C->it = cfg->it_start;
         const size_t G = (size_t)g.size();
         Metrics &m = C->m;
@@ -264,7 +289,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
             if (cfg->t_ddt_scheme == TG_TDDT_BDF2) C->tmprt_oo = dallocd(C, G);
         }
         const size_t P = (size_t)g.mx * g.mz;
-        double **ws[] = {&st.twx, &st.twy, &st.twz, &st.umean, &st.ufx, &st.ufy, &st.ufz};
+        double **ws[] = {&st.twx, &st.twy, &st.twz, &st.umean, &st.ufx, &st.ufy, &st.ufz, &st.qwall, &st.surf_theta};
         for (auto **v : ws) *v = dallocd(C, P);
         C->red_blocks = 148 * 4;
         C->d_red = dallocd(C, 4 * (size_t)C->red_blocks + 64);
@@ -383,6 +408,12 @@ tg_status tg_set_field(tg_ctx *C, int32_t w, const double *host, int32_t halo)
             TG_CUDA(cudaMemcpy(m, c.data(), P * sizeof(double), cudaMemcpyHostToDevice));
             return TG_OK;
         }
+        if (w == TG_F_QWALL || w == TG_F_SURF_THETA) {
+            const size_t P = (size_t)C->g.mx * C->g.mz;
+            TG_CUDA(cudaMemcpy(w == TG_F_QWALL ? C->s.qwall : C->s.surf_theta, host, P * sizeof(double), cudaMemcpyHostToDevice));
+            if (w == TG_F_SURF_THETA) C->surf_set = true;
+            return TG_OK;
+        }
         V3f<double> v;
         double *sp = nullptr;
         if (adj_field(C, w, v, sp)) {
@@ -427,6 +458,12 @@ tg_status tg_get_field(tg_ctx *C, int32_t w, double *host, int32_t halo)
             for (size_t q = 0; q < P; q++) { host[3 * q] = a[q]; host[3 * q + 1] = b[q]; host[3 * q + 2] = c[q]; }
             return TG_OK;
         }
+        if (w == TG_F_QWALL || w == TG_F_SURF_THETA) {
+            TG_CUDA(cudaStreamSynchronize(C->stream));
+            const size_t P = (size_t)C->g.mx * C->g.mz;
+            TG_CUDA(cudaMemcpy(host, w == TG_F_QWALL ? C->s.qwall : C->s.surf_theta, P * sizeof(double), cudaMemcpyDeviceToHost));
+            return TG_OK;
+        }
         V3f<double> v;
         double *sp = nullptr;
         if (adj_field(C, w, v, sp)) {
@@ -449,7 +486,7 @@ constexpr int64_t kPetscVecClassId = 1211214;     // VEC_FILE_CLASSID
 // entries per point of a field in the file (0: not a grid field)
 int field_dof(tg_ctx *C, int w)
 {
-    if (w == TG_F_TAUWALL || w == TG_F_WALL_ADJ || w < 0 || w >= TG_F_COUNT) return 0;
+    if (w == TG_F_TAUWALL || w == TG_F_WALL_ADJ || w == TG_F_QWALL || w == TG_F_SURF_THETA || w < 0 || w >= TG_F_COUNT) return 0;
     if (w == TG_F_P_ADJ || scal_field(C, w)) return 1;
     return 3;
 }
@@ -557,6 +594,10 @@ TG_STAGE(tg_solve_u, solve_u(C))
 TG_STAGE(tg_update_cartesian_bcs, update_cartesian_bcs(C))
 TG_STAGE(tg_update_contravariant_bcs, update_contravariant_bcs(C))
 TG_STAGE(tg_sync_pressure, sync_pressure(C))
+TG_STAGE(tg_update_wall_models_t,
+         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); update_wall_models_t(C))
+TG_STAGE(tg_update_temperature_bcs,
+         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); update_temperature_bcs(C))
 
 tg_status tg_form_u(tg_ctx *C, double scale, int32_t zero_rhs)
 {

@@ -92,6 +92,8 @@ struct State {
     double *p, *phi, *nut, *tmprt, *ssnap;
     // jLeft wall model (plane mz x mx)
     double *twx, *twy, *twz, *umean, *ufx, *ufy, *ufz;
+    // jLeft thetaWallFunction (plane mz x mx): qWall.z and surfaceTheta
+    double *qwall, *surf_theta;
 };
 
 struct Params {
@@ -102,7 +104,33 @@ struct Params {
     double cs, nu, dt, t_ref, mgp[3], z0, kappa;
     int teqn, t_bc[6];
     double prandtl, t_bc_value[6];
+    // jLeft thetaWallFunction (0: none, else TG_TWALL_*), its constants, and
+    // whether its qWall corrects the velocity wall function (wall_coupled)
+    int t_wall, t_wall_localized, wall_coupled;
+    double tw_qwall, tw_heating, tw_kappa, tw_theta_ref, tw_z0, tw_gamma_m, tw_gamma_h, tw_alpha_h;
+    double wall_gamma_m, wall_theta_ref;
 };
+
+// ------------------------------------------------------------------------
+// calculateNormal (inline.h:1210-1268): unit covariant direction of a cell
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void calc_normal(R3<double> csi, R3<double> eta, R3<double> zet, int dir, R3<double> &n)
+{
+    const double a11 = csi.x, a12 = csi.y, a13 = csi.z;
+    const double a21 = eta.x, a22 = eta.y, a23 = eta.z;
+    const double a31 = zet.x, a32 = zet.y, a33 = zet.z;
+    double det = a11 * (a33 * a22 - a32 * a23) - a21 * (a33 * a12 - a32 * a13) + a31 * (a23 * a12 - a22 * a13);
+    double x, y, z;
+    if (dir == 0) {        // G[:,0]
+        x = (a33 * a22 - a32 * a23) / det; y = -(a33 * a21 - a31 * a23) / det; z = (a32 * a21 - a31 * a22) / det;
+    } else if (dir == 1) { // G[:,1]
+        x = -(a33 * a12 - a32 * a13) / det; y = (a33 * a11 - a31 * a13) / det; z = -(a32 * a11 - a31 * a12) / det;
+    } else {               // G[:,2]
+        x = (a23 * a12 - a22 * a13) / det; y = -(a23 * a11 - a21 * a13) / det; z = (a22 * a11 - a21 * a12) / det;
+    }
+    double sm = sqrt(x * x + y * y + z * z);
+    n = R3<double>{x / sm, y / sm, z / sm};
+}
 
 struct PoissonCtx;   // tg_poisson.cu
 struct AdjState;     // tg_adjoint.cu
@@ -148,6 +176,7 @@ struct tg_ctx {
     // a mesh of planes): FormU reads only those components
     bool axis_aligned = false;
     bool ufilt_set = false;
+    bool surf_set = false;               // thetaWallFunction -3 surfaceTheta seeded
     int it = 0;
     // mixed precision: FP32 copies of the stencil metrics (and FP32 FormU
     // planes when the policy stores the face fluxes in FP32)
@@ -287,6 +316,8 @@ constexpr int ST_IT = 0, ST_RES0 = 1, ST_RES = 2, ST_TOT = 3, ST_NOCONV = 4, ST_
 constexpr int SC_G = 60, SC_ADJ = 70, SC_IT = 80;
 // solutions in the Poisson guess history (0, 1, 2 or more: order of the extrapolation)
 constexpr int SC_PHIST = 96;
+// thetaWallFunction averaged model: plane means and the resulting qWall
+constexpr int SC_TWALL = 24;
 constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
               SC_GNOCONV = SC_G + ST_NOCONV, SC_GNAN = SC_G + ST_NAN;
 void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol);
@@ -318,6 +349,7 @@ void mask_non_resolved(tg_ctx *C, V3f<double> v);               // resetNonResol
 void contra_to_cart_stage(tg_ctx *C);
 int solve_t(tg_ctx *C);      // 0, or the ABBE GMRES status (1 iteration cap, 2 breakdown)
 void update_temperature_bcs(tg_ctx *C);
+void update_wall_models_t(tg_ctx *C);   // UpdateWallModelsT: jLeft thetaWallFunction qWall
 // wind farm (tg_farm.cu)
 void farm_update(tg_ctx *C);                 // sampling, forces, projection, face body force
 void farm_destroy(tg_ctx *C);

@@ -6,6 +6,7 @@
 #include <type_traits>
 
 #include "tg_internal.cuh"
+#include "tg_mo.cuh"
 
 namespace tg {
 namespace {
@@ -136,27 +137,6 @@ __global__ void k_no_penetration(Grid g, State s, int dir, int left, int right)
         if (left) s.ucont.z[g.lin(0, b, a)] = 0.0;
         if (right) s.ucont.z[g.lin(g.mz - 2, b, a)] = 0.0;
     }
-}
-
-// ------------------------------------------------------------------------
-// calculateNormal (inline.h:1210-1268): unit covariant direction of a cell
-// ------------------------------------------------------------------------
-__device__ void calc_normal(R3<double> csi, R3<double> eta, R3<double> zet, int dir, R3<double> &n)
-{
-    const double a11 = csi.x, a12 = csi.y, a13 = csi.z;
-    const double a21 = eta.x, a22 = eta.y, a23 = eta.z;
-    const double a31 = zet.x, a32 = zet.y, a33 = zet.z;
-    double det = a11 * (a33 * a22 - a32 * a23) - a21 * (a33 * a12 - a32 * a13) + a31 * (a23 * a12 - a22 * a13);
-    double x, y, z;
-    if (dir == 0) {        // G[:,0]
-        x = (a33 * a22 - a32 * a23) / det; y = -(a33 * a21 - a31 * a23) / det; z = (a32 * a21 - a31 * a22) / det;
-    } else if (dir == 1) { // G[:,1]
-        x = -(a33 * a12 - a32 * a13) / det; y = (a33 * a11 - a31 * a13) / det; z = -(a32 * a11 - a31 * a12) / det;
-    } else {               // G[:,2]
-        x = (a23 * a12 - a22 * a13) / det; y = -(a23 * a11 - a21 * a13) / det; z = (a22 * a11 - a21 * a12) / det;
-    }
-    double sm = sqrt(x * x + y * y + z * z);
-    n = R3<double>{x / sm, y / sm, z / sm};
 }
 
 // ------------------------------------------------------------------------
@@ -350,7 +330,9 @@ __global__ void k_nut_bcs(Grid g, State s, Params p)
 
 // ------------------------------------------------------------------------
 // UpdateWallModelsU for jLeft wall function -3 (boundary.c:3257-3600):
-// plane averages, neutral friction velocity (wallfunctions.c:12-34), filtered
+// plane averages, friction velocity (uStarShumann, wallfunctions.c:12-130:
+// neutral, or corrected by the plane mean of the thetaWallFunction's last
+// heat flux when the temperature jLeft patch has one), filtered
 // wall-parallel velocity and the contravariant wall stress.
 // ------------------------------------------------------------------------
 __device__ __forceinline__ void wall_parallel(Grid g, Metrics m, State s, int k, int i, R3<double> &Up, R3<double> &n)
@@ -361,12 +343,13 @@ __device__ __forceinline__ void wall_parallel(Grid g, Metrics m, State s, int k,
     Up = U - dot3(U, n) * n;
 }
 
-// per-block partial sums of |U_par| and wall distance over the j=1 plane
-__global__ void k_wall_plane_sums(Grid g, Metrics m, State s, double *part)
+// per-block partial sums of |U_par|, the wall distance and (coupled) qWall
+// over the j=1 plane
+__global__ void k_wall_plane_sums(Grid g, Metrics m, State s, Params p, double *part)
 {
-    __shared__ double sh[2][256];
+    __shared__ double sh[3][256];
     int nI = g.mx - 2, nK = g.mz - 2;
-    double su = 0.0, sd = 0.0;
+    double su = 0.0, sd = 0.0, sq = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
         int i = t % nI + 1, k = t / nI + 1;
         int c = g.lin(k, 1, i);
@@ -374,26 +357,29 @@ __global__ void k_wall_plane_sums(Grid g, Metrics m, State s, double *part)
         R3<double> Up, n; wall_parallel(g, m, s, k, i, Up, n);
         su += sqrt(dot3(Up, Up));
         sd += 0.5 / m.aj[c] / area;
+        if (p.wall_coupled) sq += s.qwall[k * g.mx + i];
     }
-    sh[0][threadIdx.x] = su; sh[1][threadIdx.x] = sd;
+    sh[0][threadIdx.x] = su; sh[1][threadIdx.x] = sd; sh[2][threadIdx.x] = sq;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) { sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w]; }
+        if (threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+            sh[2][threadIdx.x] += sh[2][threadIdx.x + w];
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) { part[2 * blockIdx.x] = sh[0][0]; part[2 * blockIdx.x + 1] = sh[1][0]; }
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = sh[0][0]; part[3 * blockIdx.x + 1] = sh[1][0]; part[3 * blockIdx.x + 2] = sh[2][0]; }
 }
 
-// final sum (deterministic order) and neutral u* = kappa <|U_par|> / ln(<s>/z0)
+// final sums (deterministic order) and u* = uStarShumann(<|U_par|>, <s>, qWall)
 __global__ void k_wall_ustar(Grid g, Params p, const double *part, int nb, double *out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double su = 0.0, sd = 0.0;
-    for (int b = 0; b < nb; b++) { su += part[2 * b]; sd += part[2 * b + 1]; }
+    double su = 0.0, sd = 0.0, sq = 0.0;
+    for (int b = 0; b < nb; b++) { su += part[3 * b]; sd += part[3 * b + 1]; sq += part[3 * b + 2]; }
     double cnt = (double)(g.mx - 2) * (double)(g.mz - 2);
-    double Umean = su / cnt, dist = sd / cnt;
-    double logLaw = log(dist / p.z0);
-    double us = fmax(0.0, (p.kappa * Umean) / logLaw);
+    double Umean = su / cnt, dist = sd / cnt, q = sq / cnt;
+    double us = mo::ustar(Umean, dist, p.z0, p.wall_gamma_m, p.kappa, p.wall_coupled ? q : 0.0, p.wall_theta_ref);
     out[0] = Umean; out[1] = dist; out[2] = us;
 }
 
@@ -1317,7 +1303,7 @@ void update_wall_models(tg_ctx *C)
     if (!C->prm.les || C->prm.bc[TG_JLEFT] != TG_BC_WALL_SHUMANN) return;
     const Grid g = C->g;
     const int nb = 148;
-    TG_PROF(C, "wall_plane_sums", k_wall_plane_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->d_red));
+    TG_PROF(C, "wall_plane_sums", k_wall_plane_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_red));
     k_wall_ustar<<<1, 32, 0, C->stream>>>(g, C->prm, C->d_red, nb, C->d_scal + 8);
     dim3 grid((g.mx - 2 + 31) / 32, (g.mz - 2 + 7) / 8);
     if (!C->ufilt_set) {
@@ -1634,6 +1620,7 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
     pressure_update_and_project(C);
     contra_to_cart(C);
     if (C->prm.teqn) {                  // main.c:194-205
+        update_wall_models_t(C);
         const int trc = solve_t(C);
         if (trc == 2) rc = 2;
         else if (rc != 2) rc |= trc;
@@ -1653,7 +1640,7 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
 
 // A step replays as one CUDA graph once every choice the host makes in it is
 // fixed: after the first step (Adams-Bashforth flag, btheta_o copy), with the
-// wall filter seeded, no pending clear of a caller-written Rhs or dP, the FP32
+// wall filter (and thetaWallFunction surface temperature) seeded, no pending clear of a caller-written Rhs or dP, the FP32
 // metric copies current, and profiling and taping off. The Krylov loop of the
 // captured step runs under device control (poisson_solve_capture).
 static bool graph_eligible(const tg_ctx *C)
@@ -1662,7 +1649,9 @@ static bool graph_eligible(const tg_ctx *C)
     return C->graphs && !C->graph_failed && !C->prof.on && (!C->taping || tape_in_work(C)) && C->pois &&
            C->cfg.ddt_scheme != TG_DDT_CN && !imex_scheme(C->cfg.ddt_scheme) &&   // host-driven Krylov loops
            !(C->prm.teqn && C->cfg.t_ddt_scheme != TG_TDDT_RK4) &&
-           C->it > C->cfg.it_start && (!wall || C->ufilt_set) && !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
+           C->it > C->cfg.it_start && (!wall || C->ufilt_set) &&
+           !(C->prm.les && C->prm.t_wall == TG_TWALL_SHUMANN && !C->surf_set) &&   // surfaceTheta seeded
+           !C->clear_rhs && !C->clear_dp && !(C->mixed && C->met32_stale);
 }
 
 void graph_destroy(tg_ctx *C)

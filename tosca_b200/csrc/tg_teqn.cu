@@ -8,10 +8,14 @@
 // l = min(delta, 7.6 nu_t/delta sqrt(tRef/|g dT/deta|)) in stable
 // stratification (teqn_solvers.c:180-195). Boundary ghosts follow
 // UpdateTemperatureBCs (boundary.c:2052-2616) for zeroGradient, fixedValue,
-// fixedGradient and periodic patches. FP64 in every precision mode.
+// fixedGradient, periodic and (zero-gradient) thetaWallFunction patches; the
+// thetaWallFunction's heat flux (UpdateWallModelsT, boundary.c:3858-4178)
+// replaces the diffusive flux of the jLeft wall faces. FP64 in every
+// precision mode.
 #include <cmath>
 
 #include "tg_internal.cuh"
+#include "tg_mo.cuh"
 
 namespace tg {
 
@@ -115,8 +119,15 @@ __global__ void k_t_face_fluxes(Grid g, Metrics m, State s, Params p, V3f<double
         const double g11 = cs.x * et.x + cs.y * et.y + cs.z * et.z, g21 = et.x * et.x + et.y * et.y + et.z * et.z,
                      g31 = ze.x * et.x + ze.y * et.y + ze.z * et.z;
         const double ajc = m.jaj[f];
-        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)) : 0.0, dtde, ajc);
-        vs.y[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+        double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)) : 0.0, dtde, ajc);
+        double v0 = 0.0;
+        if (p.t_wall && j == 0) {
+            // thetaWallFunction (teqn_solvers.c:337-352): the modelled flux
+            // -qWall . jEta, qWall = (0, 0, q), replaces the diffusive one
+            v0 = -1.0 * (0.0 * et.x + 0.0 * et.y + s.qwall[k * mx + i] * et.z);
+            ke = 0.0;
+        }
+        vs.y[f] = v0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
     }
     // k faces (Compute_dscalar_k, inline.h:3294-3331)
     if (i != 0 && j != 0 && !(g.pk && k == 0)) {
@@ -220,7 +231,7 @@ __global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
         const int ci = side == 0 ? 1 : mdir - 2, gh = side == 0 ? 0 : mdir - 1;
         const int c = at(ci), q = at(gh);
         const int type = p.t_bc[patch];
-        if (type == TG_TBC_ZERO_GRADIENT) t[q] = t[c];
+        if (type == TG_TBC_ZERO_GRADIENT || type == TG_TBC_WALL_FUNCTION) t[q] = t[c];
         else if (type == TG_TBC_FIXED_VALUE) t[q] = p.t_bc_value[patch];
         else if (type == TG_TBC_FIXED_GRADIENT) {
             const double area = sqrt(S.x[c] * S.x[c] + S.y[c] * S.y[c] + S.z[c] * S.z[c]);
@@ -230,6 +241,92 @@ __global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
             t[q] = t[at(side == 0 ? mdir - 2 : 1)];   // periodic: the opposite interior cell
         }
     }
+}
+
+// ---- UpdateWallModelsT, jLeft thetaWallFunction (boundary.c:3858-4178) ----
+// wall-parallel velocity magnitude and wall distance 0.5 / (aj |eta|) of the
+// wall cell (k, 1, i)
+__device__ __forceinline__ void twall_cell(Grid g, Metrics m, State s, int k, int i, double &upm, double &dist)
+{
+    const int c = g.lin(k, 1, i);
+    R3<double> n;
+    const R3<double> et = ld3(m.eta, c);
+    calc_normal(ld3(m.csi, c), et, ld3(m.zet, c), 1, n);
+    const R3<double> U = ld3(s.ucat, c);
+    const R3<double> Up = U - dot3(U, n) * n;
+    upm = sqrt(dot3(Up, Up));
+    dist = 0.5 / m.aj[c] / sqrt(dot3(et, et));
+}
+
+// -3, first call: surfaceTheta = the wall value 0.5 (T(j=1) + T(j=0))
+__global__ void k_twall_seed(Grid g, State s)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.mx - 2 || k > g.mz - 2) return;
+    s.surf_theta[k * g.mx + i] = 0.5 * (s.tmprt[g.lin(k, 1, i)] + s.tmprt[g.lin(k, 0, i)]);
+}
+
+// -3 localized: surfaceTheta += heatingRate dt, then qWallShumann per cell
+__global__ void k_twall_local(Grid g, Metrics m, State s, Params p)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i > g.mx - 2 || k > g.mz - 2) return;
+    const int w = k * g.mx + i;
+    double upm, dist;
+    twall_cell(g, m, s, k, i, upm, dist);
+    const double st = s.surf_theta[w] + p.tw_heating * p.dt;
+    s.surf_theta[w] = st;
+    s.qwall[w] = mo::qwall(upm, dist, p.tw_z0, p.tw_gamma_m, p.tw_gamma_h, p.tw_alpha_h, p.tw_theta_ref,
+                           s.tmprt[g.lin(k, 1, i)] - st, p.tw_kappa);
+}
+
+// -3 averaged, pass 1: surfaceTheta += heatingRate dt and per-block partial
+// sums of T(j=1) - surfaceTheta, |U_par| and the wall distance
+__global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part)
+{
+    __shared__ double sh[3][256];
+    const int nI = g.mx - 2, nK = g.mz - 2;
+    double sT = 0.0, sU = 0.0, sD = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
+        const int i = t % nI + 1, k = t / nI + 1, w = k * g.mx + i;
+        double upm, dist;
+        twall_cell(g, m, s, k, i, upm, dist);
+        const double st = s.surf_theta[w] + p.tw_heating * p.dt;
+        s.surf_theta[w] = st;
+        sT += (s.tmprt[g.lin(k, 1, i)] - st);
+        sU += upm;
+        sD += dist;
+    }
+    sh[0][threadIdx.x] = sT; sh[1][threadIdx.x] = sU; sh[2][threadIdx.x] = sD;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int q = 0; q < 3; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) part[3 * blockIdx.x + q] = sh[q][0];
+}
+
+// -3 averaged, pass 2 (one block): the plane means in a fixed order,
+// qWallShumann once, the result into every wall cell; -2 (fixed): the
+// prescribed flux into every wall cell (nb = 0)
+__global__ void k_twall_fill(Grid g, Params p, const double *part, int nb, double *sc, State s)
+{
+    __shared__ double q;
+    if (threadIdx.x == 0) {
+        if (nb > 0) {
+            double sT = 0.0, sU = 0.0, sD = 0.0;
+            for (int b = 0; b < nb; b++) { sT += part[3 * b]; sU += part[3 * b + 1]; sD += part[3 * b + 2]; }
+            const double n = (double)(g.mx - 2) * (double)(g.mz - 2);
+            sc[0] = sT / n; sc[1] = sU / n; sc[2] = sD / n;
+            q = mo::qwall(sU / n, sD / n, p.tw_z0, p.tw_gamma_m, p.tw_gamma_h, p.tw_alpha_h, p.tw_theta_ref, sT / n, p.tw_kappa);
+        } else q = p.tw_qwall;
+        sc[3] = q;
+    }
+    __syncthreads();
+    const int nI = g.mx - 2, nK = g.mz - 2;
+    for (int t = threadIdx.x; t < nI * nK; t += blockDim.x) s.qwall[(t / nI + 1) * g.mx + t % nI + 1] = q;
 }
 
 }  // namespace
@@ -336,6 +433,34 @@ int solve_t(tg_ctx *C)
     }
     reset_cell_periodic_s(C, s.tmprt);
     return 0;
+}
+
+// UpdateWallModelsT (boundary.c:3858-4178), jLeft thetaWallFunction: the
+// wall heat flux qWall of the wall cells for the temperature step that
+// follows and the velocity wall function of the next step. -2: the
+// prescribed flux. -3: surfaceTheta is seeded from the wall value on the
+// first call and rises by heatingRate * dt on every call; qWallShumann once
+// from the plane means ("averaged", two launches) or per cell ("localized")
+void update_wall_models_t(tg_ctx *C)
+{
+    if (!C->prm.les || !C->prm.t_wall) return;
+    const Grid g = C->g;
+    const dim3 b2(32, 8), grid((g.mx - 2 + 31) / 32, (g.mz - 2 + 7) / 8);
+    if (C->prm.t_wall == TG_TWALL_FIXED_FLUX) {
+        TG_PROF(C, "twall_fill", k_twall_fill<<<1, 256, 0, C->stream>>>(g, C->prm, C->d_red, 0, C->d_scal + SC_TWALL, C->s));
+        return;
+    }
+    if (!C->surf_set) {
+        k_twall_seed<<<grid, b2, 0, C->stream>>>(g, C->s);
+        C->surf_set = true;
+    }
+    if (C->prm.t_wall_localized) {
+        TG_PROF(C, "twall_local", k_twall_local<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm));
+        return;
+    }
+    const int nb = 148;
+    TG_PROF(C, "twall_sums", k_twall_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_red));
+    TG_PROF(C, "twall_fill", k_twall_fill<<<1, 256, 0, C->stream>>>(g, C->prm, C->d_red, nb, C->d_scal + SC_TWALL, C->s));
 }
 
 void update_temperature_bcs(tg_ctx *C)
