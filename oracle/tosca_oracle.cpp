@@ -41,6 +41,7 @@
 #include <functional>
 #include <stdexcept>
 #include <string>
+#include <memory>
 #include <vector>
 
 #ifdef _OPENMP
@@ -78,6 +79,8 @@ struct Turbine {
 };
 
 } // namespace
+
+struct OracleMg;   // pressure-solve multigrid (tosca_oracle_mg.inc)
 
 struct tg_ctx {
     tg_config c{};
@@ -134,6 +137,7 @@ struct tg_ctx {
     int64_t N = 0;
     int64_t pinned_row = -1;
     bool symmetric = true;
+    std::shared_ptr<OracleMg> mg;     // preconditioner hierarchy of A (built on first use)
 
     // ------------------------------------------------------------ indexing --
     inline int wi(int i) const { if (pi) { if (i < 0) i += mx; else if (i >= mx) i -= mx; } return i; }
@@ -418,6 +422,7 @@ void setCoeffMatrix(tg_ctx &C)
          &g31 = C.g31, &g32 = C.g32, &g33 = C.g33;
     C.A.rowptr.assign(C.N + 1, 0);
     C.A.col.clear(); C.A.val.clear();
+    C.mg.reset();
     C.A.col.reserve(C.N * 19); C.A.val.reserve(C.N * 19);
     const double r = 1.0;
     int64_t row = 0;
@@ -561,10 +566,15 @@ double dotv(const std::vector<double> &a, const std::vector<double> &b)
     return s;
 }
 
+} // namespace
+#include "tosca_oracle_mg.inc"
+namespace {
+
 // Pressure solve. The reference calls HYPRE GMRES/BoomerAMG (peqn.c:3856-3929);
-// here: Jacobi-preconditioned CG on the pinned system when the operator is
-// symmetric (the pinned unknown is identically zero, so it is eliminated),
-// otherwise Jacobi-preconditioned BiCGStab.
+// here: CG on the pinned system when the operator is symmetric (the pinned
+// unknown is identically zero, so it is eliminated), otherwise BiCGStab, both
+// preconditioned by one V-cycle of the aggregation multigrid
+// (tosca_oracle_mg.inc), or by the diagonal where no hierarchy can be built.
 int solvePoisson(tg_ctx &C, const std::vector<double> &b, std::vector<double> &x, tg_stats *st)
 {
     const int64_t n = C.N;
@@ -572,6 +582,17 @@ int solvePoisson(tg_ctx &C, const std::vector<double> &b, std::vector<double> &x
     for (int64_t r = 0; r < n; r++)
         for (int64_t q = C.A.rowptr[r]; q < C.A.rowptr[r + 1]; q++)
             if (C.A.col[q] == r) dinv[r] = 1.0 / C.A.val[q];
+    if (!C.mg) {
+        auto M = std::make_shared<OracleMg>();
+        try { mgBuild(C, *M); C.mg = M; }
+        catch (const OracleError &) { C.mg.reset(); }
+    }
+    // z = M^-1 v
+    auto precond = [&](const std::vector<double> &v, std::vector<double> &z) {
+        if (C.mg) { mgApply(*C.mg, v, z); return; }
+        #pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * v[i];
+    };
     const double bn = std::sqrt(dotv(b, b));
     std::vector<double> r(n), z(n), pv(n), Ap(n);
     const int maxit = C.c.poisson_maxit > 0 ? C.c.poisson_maxit : 10000;
@@ -587,8 +608,9 @@ int solvePoisson(tg_ctx &C, const std::vector<double> &b, std::vector<double> &x
     double rn = rn0;
     if (C.symmetric) {
         // CG on the reduced SPD system (negated operator is positive definite)
-        for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * r[i];
-        if (pin >= 0) { r[pin] = 0.0; z[pin] = 0.0; }
+        if (pin >= 0) r[pin] = 0.0;
+        precond(r, z);
+        if (pin >= 0) z[pin] = 0.0;
         pv = z;
         double rz = dotv(r, z);
         while (rn / bn > rtol && iters < maxit) {
@@ -597,8 +619,7 @@ int solvePoisson(tg_ctx &C, const std::vector<double> &b, std::vector<double> &x
             double alpha = rz / dotv(pv, Ap);
             #pragma omp parallel for schedule(static)
             for (int64_t i = 0; i < n; i++) { x[i] += alpha * pv[i]; r[i] -= alpha * Ap[i]; }
-            #pragma omp parallel for schedule(static)
-            for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * r[i];
+            precond(r, z);
             if (pin >= 0) z[pin] = 0.0;
             double rz1 = dotv(r, z);
             double beta = rz1 / rz; rz = rz1;
@@ -622,11 +643,11 @@ int solvePoisson(tg_ctx &C, const std::vector<double> &b, std::vector<double> &x
             double beta = (rho1 / rho) * (alpha / omega);
             rho = rho1;
             for (int64_t i = 0; i < n; i++) pv[i] = r[i] + beta * (pv[i] - omega * v[i]);
-            for (int64_t i = 0; i < n; i++) phat[i] = dinv[i] * pv[i];
+            precond(pv, phat);
             spmv(C, phat, v);
             alpha = rho / dotv(rhat, v);
             for (int64_t i = 0; i < n; i++) s[i] = r[i] - alpha * v[i];
-            for (int64_t i = 0; i < n; i++) shat[i] = dinv[i] * s[i];
+            precond(s, shat);
             spmv(C, shat, t);
             double tt = dotv(t, t);
             omega = tt > 0 ? dotv(t, s) / tt : 0.0;
