@@ -246,7 +246,7 @@ def cpu_model() -> str:
     return platform.processor() or platform.machine()
 
 
-def cpu_baseline(workload, steps, full=False):
+def cpu_baseline(workload, steps, full=False, cells=None):
     """CPU restatement of the reference step (the oracle, OpenMP on all host
     threads) on the workload: the full configuration (`full`), or a bounded
     sample of it (the ABL at 128 x 128 x 64 cells with the same 10 m spacing
@@ -257,7 +257,7 @@ def cpu_baseline(workload, steps, full=False):
     import oracle
     from tosca_b200 import cases
     if full:
-        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64")
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=cells)
     elif workload == "abl":
         cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=(128, 128, 64))
     else:
@@ -313,7 +313,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     steps = max(1, min(args.steps, 2))
-    base = cpu_baseline(args.workload, steps, full=True)
+    base = cpu_baseline(args.workload, steps, full=True, cells=args.cells)
     line = {
         "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": 1, "ms_per_step": base["seconds"] / steps * 1e3, "higher_is_better": True,
