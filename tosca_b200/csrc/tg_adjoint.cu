@@ -534,7 +534,34 @@ __device__ __forceinline__ void visc_adj(R3<double> s0, R3<double> s1, R3<double
     for (int q = 0; q < 3; q++) dd[q] = ajc * (dot3(sm[q], n) * va + dot3(sm[q], va) * n);
 }
 
-// pass 1 transpose: per face, scatter to Ucat (atomics), Ucont (own face) and nut
+// the transpose of the axis-aligned viscous flux (visc_flux_ax of the forward
+// step: cs = csi.y, et = eta.z, ze = zet.x of the face, the other metric
+// components left out), term by term
+__device__ __forceinline__ void visc_adj_ax(double cs, double et, double ze, int dir, R3<double> va, double ajc, R3<double> dd[3])
+{
+    if (dir == 0) {
+        const double g11 = cs * cs;
+        dd[0] = ajc * R3<double>{g11 * va.x, g11 * va.y + (cs * va.y) * cs, g11 * va.z};
+        dd[1] = ajc * R3<double>{0.0, (et * va.z) * cs, 0.0};
+        dd[2] = ajc * R3<double>{0.0, (ze * va.x) * cs, 0.0};
+    } else if (dir == 1) {
+        const double g21 = et * et;
+        dd[0] = ajc * R3<double>{0.0, 0.0, (cs * va.y) * et};
+        dd[1] = ajc * R3<double>{g21 * va.x, g21 * va.y, g21 * va.z + (et * va.z) * et};
+        dd[2] = ajc * R3<double>{0.0, 0.0, (ze * va.x) * et};
+    } else {
+        const double g31 = ze * ze;
+        dd[0] = ajc * R3<double>{(cs * va.y) * ze, 0.0, 0.0};
+        dd[1] = ajc * R3<double>{(et * va.z) * ze, 0.0, 0.0};
+        dd[2] = ajc * R3<double>{g31 * va.x + (ze * va.x) * ze, g31 * va.y, g31 * va.z};
+    }
+}
+
+// pass 1 transpose: per face, scatter to Ucat (atomics), Ucont (own face) and
+// nut. AX: the mesh is axis-aligned and the forward step formed the
+// axis-aligned viscous flux, whose exact transpose reads 3 of the 9 face
+// metric components
+template <bool AX>
 __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double> uc, const double *nut, Params p,
                                   V3f<double> f1a, V3f<double> f2a, V3f<double> f3a,
                                   V3f<double> uta, V3f<double> cta, double *na, V3f<double> twa)
@@ -582,7 +609,8 @@ __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double>
             else { nuEff = nu + 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1)); vnut = true; }
         } else nuEff = nu;
         R3<double> dd[3];
-        visc_adj(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, gv, m.iaj[f], dd);
+        if (AX) visc_adj_ax(m.icsi.y[f], m.ieta.z[f], m.izet.x[f], 0, gv, m.iaj[f], dd);
+        else visc_adj(ld3(m.icsi, f), ld3(m.ieta, f), ld3(m.izet, f), 0, gv, m.iaj[f], dd);
         bool edge = (i == 0 || i == mx - 2);
         // stencil weights of (dc, de, dz): dc = U(i+1) - U(i)
         int jo = (j == my - 2 && edge && (npj || npi)) ? 1 : ((j == 1 && edge && (npj || npi)) ? 2 : 0);
@@ -639,7 +667,8 @@ __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double>
             else { nuEff = nu + 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)); vnut = true; }
         } else nuEff = nu;
         R3<double> dd[3];
-        visc_adj(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, gv, m.jaj[f], dd);
+        if (AX) visc_adj_ax(m.jcsi.y[f], m.jeta.z[f], m.jzet.x[f], 1, gv, m.jaj[f], dd);
+        else visc_adj(ld3(m.jcsi, f), ld3(m.jeta, f), ld3(m.jzet, f), 1, gv, m.jaj[f], dd);
         bool edge = (j == 0 || j == my - 2);
         int io = (i == mx - 2 && edge && (npi || npj)) ? 1 : ((i == 1 && edge && (npi || npj)) ? 2 : 0);
         int ko = (k == mz - 2 && edge && (npk || npj)) ? 1 : ((k == 1 && edge && (npk || npj)) ? 2 : 0);
@@ -691,7 +720,8 @@ __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double>
             else { nuEff = nu + 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i)); vnut = true; }
         } else nuEff = nu;
         R3<double> dd[3];
-        visc_adj(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, gv, m.kaj[f], dd);
+        if (AX) visc_adj_ax(m.kcsi.y[f], m.keta.z[f], m.kzet.x[f], 2, gv, m.kaj[f], dd);
+        else visc_adj(ld3(m.kcsi, f), ld3(m.keta, f), ld3(m.kzet, f), 2, gv, m.kaj[f], dd);
         bool edge = (k == 0 || k == mz - 2);
         int io = (i == mx - 2 && edge && (npi || npk)) ? 1 : ((i == 1 && edge && (npi || npk)) ? 2 : 0);
         int jo = (j == my - 2 && edge && (npj || npk)) ? 1 : ((j == 1 && edge && (npj || npk)) ? 2 : 0);
@@ -1195,8 +1225,12 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
         TG_PROF(C, "adj_cell_fp", k_adj_cell_fp<<<gfc(g), block3(), 0, st>>>(g, A.fpa, A.f1a, A.f2a, A.f3a));
         zero3(C, A.uta);
         zero3(C, A.cta);
-        TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<<<gfc(g), block3(), 0, st>>>(g, C->m, T.ut[s], T.uc[s], T.nut, C->prm,
-                                                                                    A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na, twa));
+        if (C->axis_aligned)
+            TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<true><<<gfc(g), block3(), 0, st>>>(g, C->m, T.ut[s], T.uc[s], T.nut,
+                                                          C->prm, A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na, twa));
+        else
+            TG_PROF(C, "adj_face_fluxes", k_adj_face_fluxes<false><<<gfc(g), block3(), 0, st>>>(g, C->m, T.ut[s], T.uc[s], T.nut,
+                                                           C->prm, A.f1a, A.f2a, A.f3a, A.uta, A.cta, A.na, twa));
         // stage Ucat: periodic copies, interior from contravariantToCartesian, other ghosts from the state Ucat
         adj_periodic(C, A.cta, 0);
         adj_contra(C, A.cta, A.uta);
