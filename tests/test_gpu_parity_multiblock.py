@@ -116,7 +116,10 @@ def test_step_host_halo3_against_oracle():
         ref = o.get(name)
         for c in range(3):
             assert rel_l2(arr[core][..., c], ref[..., c]) < 1e-10, (name, c)
-    assert rel_l2(p[core], o.get("P")) < 1e-10
+    # both pressure solves stop at a relative residual of 1e-13, with different
+    # multigrid preconditioners; on this grid two such solves differ by about
+    # 5e-10 in p (the oracle's own 1e-13 and 1e-14 solutions differ by 5.8e-10)
+    assert rel_l2(p[core], o.get("P")) < 1e-9
     assert rel_l2(nut[core], o.get("NUT")) < 1e-10
     for arr in (ucont, ucat, p, nut):
         m = np.ones(arr.shape[:3], bool)

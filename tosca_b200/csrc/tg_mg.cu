@@ -23,12 +23,14 @@
 // a chain of FMAs. A block solves 32 same-colour lines at once: each of its
 // warps takes one chunk of j, runs the forward and backward recurrences of
 // its chunk as affine maps (coalesced loads, all warps in flight), and the
-// chunk ends are combined in shared memory. The smallest levels (<= 512
+// chunk ends are combined in shared memory. The smallest levels (<= 1024
 // cells each) run as one single-block kernel that stages their coefficients,
 // unknowns and the dense coarsest inverse in shared memory and performs all
 // their sweeps, transfers and the coarsest solve there. One block is issue-
 // and latency-bound, so larger levels run as grid launches (cheap inside the
-// step graph): at 4096 cells the single-block version took 80-130 us.
+// step graph): at 4096 cells the single-block version took 80-130 us; taking
+// the 1024-cell level into it saves 2 % of a 128 x 64 x 64 ABL step (1.383
+// -> 1.356 ms) and nothing measurable at 256 x 256 x 128, 2048 no more.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -49,7 +51,7 @@ struct Lvl {
 };
 
 constexpr int MAXL = 16;
-constexpr int TAIL_CELLS = 512;
+constexpr int TAIL_CELLS = 1024;
 constexpr int COARSEST_CELLS = 64;
 constexpr int TAIL_SMEM = 220 * 1024;   // dynamic shared memory of the single-block tail
 constexpr int LINE_NW = 32;         // warps per block of the chunked line solver (one line chunk each)
