@@ -76,6 +76,7 @@ struct AdjState {
     // work
     V3f<double> uoa, usa, uta, cta, ra, dpa, fpa, f1a, f2a, f3a, qa;
     double *pha = nullptr, *na = nullptr, *lam = nullptr, *rhsc = nullptr;
+    double *lam_prev = nullptr, *lam_prev2 = nullptr;   // solutions of the two steps reversed before
     // tape of the step being reversed: the work tape, or one of the stored
     // tapes of a forward run that kept every step's tape
     Tape work_tape;
@@ -1014,6 +1015,7 @@ static void adj_work(tg_ctx *C)
     for (auto *p : v) *p = alloc3(C);
     A.pha = dallocd(C, G); A.na = dallocd(C, G);
     A.lam = dallocd(C, (size_t)poisson_n(C)); A.rhsc = dallocd(C, (size_t)poisson_n(C));
+    A.lam_prev = dallocd(C, (size_t)poisson_n(C)); A.lam_prev2 = dallocd(C, (size_t)poisson_n(C));
     A.work_tape = make_tape(C);
     A.cur = &A.work_tape;
     for (int q = 0; q < 3; q++) A.twa[q] = dallocd(C, wall_plane(C));
@@ -1183,7 +1185,8 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
     k_adj_update_pressure<<<gint(g), block3(), 0, st>>>(g, A.pa, A.pha, A.rhsc);
     adj_scalar_ghosts(C, A.pha);
     k_adj_phi_compact<<<gint(g), block3(), 0, st>>>(g, A.pha, A.rhsc);
-    // started from the previous reversed step's solution, to the context's
+    // started from the solutions of the previously reversed steps,
+    // extrapolated like the forward solve's guess, to the context's
     // relative tolerance when that lies in [1e-14, 1e-8]; when the forward
     // solve stops on the divergence bound instead, to 1e-7, the relative
     // residual that bound leaves in the forward solve; else to 1e-8
@@ -1191,9 +1194,11 @@ static int adjoint_reverse_body(tg_ctx *C, bool capture)
     const double artol = (rt >= 1e-14 && rt <= 1e-8) ? rt : (C->cfg.poisson_div_tol > 0.0 ? 1e-7 : 1e-8);
     int rc = 0;
     if (capture) {
+        adjoint_guess(C, A.lam, A.lam_prev, A.lam_prev2, C->d_scal + SC_LHIST);
         poisson_solve_adjoint_capture(C, A.rhsc, A.lam, artol);
     } else {
         tg_stats ps{};
+        adjoint_guess(C, A.lam, A.lam_prev, A.lam_prev2, C->d_scal + SC_LHIST);
         rc = poisson_solve_adjoint(C, A.rhsc, A.lam, artol, &ps);
         A.adj_iters += ps.poisson_iterations;
         if (rc == 3) return 3;
@@ -1614,6 +1619,9 @@ tg_status tg_adjoint_reverse(tg_ctx *C, tg_adjoint_stats *stats)
         R.build(A.nsteps, (int)A.snaps.size() - 2);
         A.adj_iters = 0;
         step_stats_reset(C);
+        // a new reversal: its first transposed solve starts from the last
+        // solution without extrapolating across the two reversals
+        TG_CUDA(cudaMemsetAsync(C->d_scal + SC_LHIST, 0, sizeof(double), C->stream));
         TG_CUDA(cudaEventRecord(C->ev0, C->stream));
         if (A.stored) {
             for (int n = A.nsteps - 1; n >= 0; n--) {

@@ -318,9 +318,15 @@ constexpr int SC_G = 60, SC_ADJ = 70, SC_IT = 80;
 constexpr int SC_PHIST = 96;
 // thetaWallFunction averaged model: plane means and the resulting qWall
 constexpr int SC_TWALL = 24;
+// number of transposed-solve solutions in the adjoint guess history
+constexpr int SC_LHIST = 76;
 constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
               SC_GNOCONV = SC_G + ST_NOCONV, SC_GNAN = SC_G + ST_NAN;
 void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol);
+// initial guess of a transposed pressure solve: lam extrapolated from the
+// solutions of the previously reversed steps (lam, lp, lp2; hist counts them),
+// of the order the forward solve uses; the history shifts
+void adjoint_guess(tg_ctx *C, double *lam, double *lp, double *lp2, double *hist);
 // capture body() (launches on C->stream) into an instantiated graph; false when
 // capture or instantiation fails (nothing is left capturing)
 bool capture_graph(tg_ctx *C, cudaGraphExec_t *out, const std::function<void()> &body);

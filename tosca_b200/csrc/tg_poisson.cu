@@ -800,7 +800,7 @@ void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, do
 // SetCoeffMatrix (rhs and lam compact, pinned entry of rhs ignored,
 // lam[pin] = 0). On orthogonal grids the operator without the pinned row and
 // column is symmetric, so this is the forward Krylov solve started from the
-// value lam holds on entry (the previous reversed step's solution); the
+// value lam holds on entry (the caller's guess, adjoint_guess); the
 // forward warm start P.x is kept. Returns 3 for the non-symmetric curvilinear
 // operator.
 int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol, tg_stats *st)
@@ -817,6 +817,16 @@ int poisson_solve_adjoint(tg_ctx *C, const double *rhs, double *lam, double rtol
     TG_CUDA(cudaMemcpyAsync(lam, P.x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     TG_CUDA(cudaMemcpyAsync(P.x, P.v, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     return rc;
+}
+
+void adjoint_guess(tg_ctx *C, double *lam, double *lp, double *lp2, double *hist)
+{
+    PoissonCtx &P = *C->pois;
+    cudaStream_t s = C->stream;
+    k_extrapolate<<<vblocks(P.n), RB, 0, s>>>(P.n, lam, lp, lp2, hist, guess_order(C));
+    k_hist_next<<<1, 1, 0, s>>>(hist);
+    k_zero_at<<<1, 1, 0, s>>>(lam, P.pin);
+    TG_CUDA(cudaGetLastError());
 }
 
 // compact Poisson solution vectors (the next solve extrapolates x, xprev, xprev2): snapshots
