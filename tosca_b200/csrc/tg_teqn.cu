@@ -21,7 +21,6 @@ namespace tg {
 
 namespace {
 
-inline dim3 gfaces(const Grid &g) { return grid3(g.mx - 1, g.my - 1, g.mz - 1); }
 inline dim3 gint(const Grid &g) { return grid3(g.mx - 2, g.my - 2, g.mz - 2); }
 inline int nblk(int64_t n) { int64_t b = (n + 255) / 256; return (int)(b < 148 * 16 ? b : 148 * 16); }
 
@@ -66,91 +65,182 @@ __device__ __forceinline__ void stencil4(int i, int m, int per, int &L, int &R)
     } else { L = i - 1; R = i + 2; }
 }
 
-// pass 1: convective and diffusive fluxes at the faces of cell (k, j, i),
-// i in [0, mx-2] etc.; face 0 of a periodic direction is read from face m-2
-// by the budget and is not formed
-__global__ void k_t_face_fluxes(Grid g, Metrics m, State s, Params p, V3f<double> dv, V3f<double> vs)
+// pass 1: convective and diffusive fluxes at the faces of the interior
+// cells. One thread per interior cell (k, j, i) forms the i, j and k faces on
+// the cell's + side, and a cell next to a non-periodic 0 boundary also the
+// face on its - side (face 0; face 0 of a periodic direction is read from
+// face m-2 by the budget and is not formed). T and nut are staged in a
+// shared-memory tile of the block's cells with one cell below and two above
+// in every direction (the DMDA wrap of periodic directions applied once, at
+// staging), so every stencil read is a fixed tile offset; the WENO points of
+// the boundary faces, which may lie outside the tile (periodic i = mx + 2 and
+// i = -3), are read from global memory.
+//
+// AX: the mesh is axis-aligned (csi || y, eta || z, zet || x; tg_mesh_info):
+// the metric tensor of a face is its normal component squared, g11 = csi.y^2
+// at i faces, g21 = eta.z^2 at j faces, g31 = zet.x^2 at k faces, and the
+// cross terms, zero up to the round-off of the metric evaluation, are left
+// out with the derivatives they multiply; kappa_eff still reads the eta
+// derivative of every face (the stability correction of Pr_t).
+constexpr int TBX = 32, TBY = 4, TBZ = 2, TBN = TBX * TBY * TBZ;
+constexpr int TTX = TBX + 3, TTY = TBY + 3, TTZ = TBZ + 3, TTN = TTX * TTY * TTZ;
+
+template <bool AX>
+__global__ void __launch_bounds__(TBN) k_t_face_fluxes(Grid g, Metrics m, State s, Params p, V3f<double> dv, V3f<double> vs)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    __shared__ double st[TTN];
+    __shared__ double sn[TTN];
     const int mx = g.mx, my = g.my, mz = g.mz;
-    const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
-    const int f = g.lin(k, j, i);
-    auto T = [&](int kk, int jj, int ii) { return s.tmprt[g.id(kk, jj, ii)]; };
-    auto NUT = [&](int kk, int jj, int ii) { return s.nut[g.id(kk, jj, ii)]; };
-    // i faces (Compute_dscalar_i, inline.h:3210-3247)
-    if (j != 0 && k != 0 && !(g.pi && i == 0)) {
-        const double dtdc = T(k, j, i + 1) - T(k, j, i);
-        const bool edge = (i == 0 || i == mx - 2);
-        double dtde, dtdz;
-        if (j == my - 2 && edge && (npj || npi))      dtde = (T(k, j, i + 1) + T(k, j, i) - T(k, j - 1, i + 1) - T(k, j - 1, i)) * 0.5;
-        else if (j == 1 && edge && (npj || npi))      dtde = (T(k, j + 1, i + 1) + T(k, j + 1, i) - T(k, j, i + 1) - T(k, j, i)) * 0.5;
-        else                                          dtde = (T(k, j + 1, i + 1) + T(k, j + 1, i) - T(k, j - 1, i + 1) - T(k, j - 1, i)) * 0.25;
-        if (k == mz - 2 && edge && (npk || npi))      dtdz = (T(k, j, i + 1) + T(k, j, i) - T(k - 1, j, i + 1) - T(k - 1, j, i)) * 0.5;
-        else if (k == 1 && edge && (npk || npi))      dtdz = (T(k + 1, j, i + 1) + T(k + 1, j, i) - T(k, j, i + 1) - T(k, j, i)) * 0.5;
-        else                                          dtdz = (T(k + 1, j, i + 1) + T(k + 1, j, i) - T(k - 1, j, i + 1) - T(k - 1, j, i)) * 0.25;
-        int iL, iR;
-        stencil4(i, mx, g.pi, iL, iR);
-        const double uc = s.ucont.x[f];
-        dv.x[f] = -uc * weno3(T(k, j, iL), T(k, j, i), T(k, j, i + 1), T(k, j, iR), uc);
-        const R3<double> cs = ld3(m.icsi, f), et = ld3(m.ieta, f), ze = ld3(m.izet, f);
-        const double g11 = cs.x * cs.x + cs.y * cs.y + cs.z * cs.z, g21 = et.x * cs.x + et.y * cs.y + et.z * cs.z,
-                     g31 = ze.x * cs.x + ze.y * cs.y + ze.z * cs.z;
-        const double ajc = m.iaj[f];
-        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j, i + 1)) : 0.0, dtde, ajc);
-        vs.x[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+    const int i0 = 1 + blockIdx.x * TBX, j0 = 1 + blockIdx.y * TBY, k0 = 1 + blockIdx.z * TBZ;
+    for (int q = (threadIdx.z * TBY + threadIdx.y) * TBX + threadIdx.x; q < TTN; q += TBN) {
+        const int tx = q % TTX, ty = (q / TTX) % TTY, tz = q / (TTX * TTY);
+        const int gi = g.wi(i0 - 1 + tx), gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz);
+        double tv = 0.0, nv = 0.0;
+        if (gi >= 0 && gi < mx && gj >= 0 && gj < my && gk >= 0 && gk < mz) {
+            const int c = (gk * my + gj) * mx + gi;
+            tv = s.tmprt[c];
+            if (p.les) nv = s.nut[c];
+        }
+        st[q] = tv; sn[q] = nv;
     }
-    // j faces (Compute_dscalar_j, inline.h:3252-3289)
-    if (i != 0 && k != 0 && !(g.pj && j == 0)) {
-        const bool edge = (j == 0 || j == my - 2);
-        double dtdc, dtdz;
-        if (i == mx - 2 && edge && (npi || npj))      dtdc = (T(k, j + 1, i) + T(k, j, i) - T(k, j + 1, i - 1) - T(k, j, i - 1)) * 0.5;
-        else if (i == 1 && edge && (npi || npj))      dtdc = (T(k, j + 1, i + 1) + T(k, j, i + 1) - T(k, j + 1, i) - T(k, j, i)) * 0.5;
-        else                                          dtdc = (T(k, j + 1, i + 1) + T(k, j, i + 1) - T(k, j + 1, i - 1) - T(k, j, i - 1)) * 0.25;
-        const double dtde = T(k, j + 1, i) - T(k, j, i);
-        if (k == mz - 2 && edge && (npk || npj))      dtdz = (T(k, j + 1, i) + T(k, j, i) - T(k - 1, j + 1, i) - T(k - 1, j, i)) * 0.5;
-        else if (k == 1 && edge && (npk || npj))      dtdz = (T(k + 1, j + 1, i) + T(k + 1, j, i) - T(k, j + 1, i) - T(k, j, i)) * 0.5;
-        else                                          dtdz = (T(k + 1, j + 1, i) + T(k + 1, j, i) - T(k - 1, j + 1, i) - T(k - 1, j, i)) * 0.25;
-        int jL, jR;
-        stencil4(j, my, g.pj, jL, jR);
+    __syncthreads();
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0 + threadIdx.z;
+    if (i > mx - 2 || j > my - 2 || k > mz - 2) return;
+    const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
+    const int t0 = ((threadIdx.z + 1) * TTY + threadIdx.y + 1) * TTX + threadIdx.x + 1;
+    auto T = [&](int dk, int dj, int di) { return st[t0 + (dk * TTY + dj) * TTX + di]; };
+    auto NUT = [&](int dk, int dj, int di) { return sn[t0 + (dk * TTY + dj) * TTX + di]; };
+    auto TG = [&](int kk, int jj, int ii) { return s.tmprt[g.id(kk, jj, ii)]; };
+
+    // ---- i face fi = i + e (Compute_dscalar_i, inline.h:3210-3247)
+    auto iface = [&](int fi, int e) {
+        const int f = g.lin(k, j, fi);
+        const bool edge = (fi == 0 || fi == mx - 2);
+        const double dtdc = T(0, 0, e + 1) - T(0, 0, e);
+        double dtde, dtdz = 0.0;
+        if (j == my - 2 && edge && (npj || npi))      dtde = (T(0, 0, e + 1) + T(0, 0, e) - T(0, -1, e + 1) - T(0, -1, e)) * 0.5;
+        else if (j == 1 && edge && (npj || npi))      dtde = (T(0, 1, e + 1) + T(0, 1, e) - T(0, 0, e + 1) - T(0, 0, e)) * 0.5;
+        else                                          dtde = (T(0, 1, e + 1) + T(0, 1, e) - T(0, -1, e + 1) - T(0, -1, e)) * 0.25;
+        if (!AX) {
+            if (k == mz - 2 && edge && (npk || npi))  dtdz = (T(0, 0, e + 1) + T(0, 0, e) - T(-1, 0, e + 1) - T(-1, 0, e)) * 0.5;
+            else if (k == 1 && edge && (npk || npi))  dtdz = (T(1, 0, e + 1) + T(1, 0, e) - T(0, 0, e + 1) - T(0, 0, e)) * 0.5;
+            else                                      dtdz = (T(1, 0, e + 1) + T(1, 0, e) - T(-1, 0, e + 1) - T(-1, 0, e)) * 0.25;
+        }
+        const double uc = s.ucont.x[f];
+        double w;
+        if (edge) {
+            int iL, iR;
+            stencil4(fi, mx, g.pi, iL, iR);
+            w = weno3(TG(k, j, iL), T(0, 0, e), T(0, 0, e + 1), TG(k, j, iR), uc);
+        } else w = weno3(T(0, 0, e - 1), T(0, 0, e), T(0, 0, e + 1), T(0, 0, e + 2), uc);
+        dv.x[f] = -uc * w;
+        const double ajc = m.iaj[f];
+        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(0, 0, e) + NUT(0, 0, e + 1)) : 0.0, dtde, ajc);
+        if (AX) {
+            const double cs = m.icsi.y[f];
+            vs.x[f] = 0.0 + ((cs * cs) * dtdc) * ajc * ke;
+        } else {
+            const R3<double> cs = ld3(m.icsi, f), et = ld3(m.ieta, f), ze = ld3(m.izet, f);
+            const double g11 = cs.x * cs.x + cs.y * cs.y + cs.z * cs.z, g21 = et.x * cs.x + et.y * cs.y + et.z * cs.z,
+                         g31 = ze.x * cs.x + ze.y * cs.y + ze.z * cs.z;
+            vs.x[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+        }
+    };
+    // ---- j face fj = j + e (Compute_dscalar_j, inline.h:3252-3289)
+    auto jface = [&](int fj, int e) {
+        const int f = g.lin(k, fj, i);
+        const bool edge = (fj == 0 || fj == my - 2);
+        const double dtde = T(0, e + 1, 0) - T(0, e, 0);
+        double dtdc = 0.0, dtdz = 0.0;
+        if (!AX) {
+            if (i == mx - 2 && edge && (npi || npj))  dtdc = (T(0, e + 1, 0) + T(0, e, 0) - T(0, e + 1, -1) - T(0, e, -1)) * 0.5;
+            else if (i == 1 && edge && (npi || npj))  dtdc = (T(0, e + 1, 1) + T(0, e, 1) - T(0, e + 1, 0) - T(0, e, 0)) * 0.5;
+            else                                      dtdc = (T(0, e + 1, 1) + T(0, e, 1) - T(0, e + 1, -1) - T(0, e, -1)) * 0.25;
+            if (k == mz - 2 && edge && (npk || npj))  dtdz = (T(0, e + 1, 0) + T(0, e, 0) - T(-1, e + 1, 0) - T(-1, e, 0)) * 0.5;
+            else if (k == 1 && edge && (npk || npj))  dtdz = (T(1, e + 1, 0) + T(1, e, 0) - T(0, e + 1, 0) - T(0, e, 0)) * 0.5;
+            else                                      dtdz = (T(1, e + 1, 0) + T(1, e, 0) - T(-1, e + 1, 0) - T(-1, e, 0)) * 0.25;
+        }
         const double uc = s.ucont.y[f];
-        dv.y[f] = -uc * weno3(T(k, jL, i), T(k, j, i), T(k, j + 1, i), T(k, jR, i), uc);
-        const R3<double> cs = ld3(m.jcsi, f), et = ld3(m.jeta, f), ze = ld3(m.jzet, f);
-        const double g11 = cs.x * et.x + cs.y * et.y + cs.z * et.z, g21 = et.x * et.x + et.y * et.y + et.z * et.z,
-                     g31 = ze.x * et.x + ze.y * et.y + ze.z * et.z;
+        double w;
+        if (edge) {
+            int jL, jR;
+            stencil4(fj, my, g.pj, jL, jR);
+            w = weno3(TG(k, jL, i), T(0, e, 0), T(0, e + 1, 0), TG(k, jR, i), uc);
+        } else w = weno3(T(0, e - 1, 0), T(0, e, 0), T(0, e + 1, 0), T(0, e + 2, 0), uc);
+        dv.y[f] = -uc * w;
         const double ajc = m.jaj[f];
-        double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k, j + 1, i)) : 0.0, dtde, ajc);
+        double ke = kappa_eff(p, p.les ? 0.5 * (NUT(0, e, 0) + NUT(0, e + 1, 0)) : 0.0, dtde, ajc);
         double v0 = 0.0;
-        if (p.t_wall && j == 0) {
+        if (p.t_wall && fj == 0) {
             // thetaWallFunction (teqn_solvers.c:337-352): the modelled flux
             // -qWall . jEta, qWall = (0, 0, q), replaces the diffusive one
+            const R3<double> et = ld3(m.jeta, f);
             v0 = -1.0 * (0.0 * et.x + 0.0 * et.y + s.qwall[k * mx + i] * et.z);
             ke = 0.0;
         }
-        vs.y[f] = v0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
-    }
-    // k faces (Compute_dscalar_k, inline.h:3294-3331)
-    if (i != 0 && j != 0 && !(g.pk && k == 0)) {
-        const bool edge = (k == 0 || k == mz - 2);
-        double dtdc, dtde;
-        if (i == mx - 2 && edge && (npi || npk))      dtdc = (T(k + 1, j, i) + T(k, j, i) - T(k + 1, j, i - 1) - T(k, j, i - 1)) * 0.5;
-        else if (i == 1 && edge && (npi || npk))      dtdc = (T(k + 1, j, i + 1) + T(k, j, i + 1) - T(k + 1, j, i) - T(k, j, i)) * 0.5;
-        else                                          dtdc = (T(k + 1, j, i + 1) + T(k, j, i + 1) - T(k + 1, j, i - 1) - T(k, j, i - 1)) * 0.25;
-        if (j == my - 2 && edge && (npj || npk))      dtde = (T(k + 1, j, i) + T(k, j, i) - T(k + 1, j - 1, i) - T(k, j - 1, i)) * 0.5;
-        else if (j == 1 && edge && (npj || npk))      dtde = (T(k + 1, j + 1, i) + T(k, j + 1, i) - T(k + 1, j, i) - T(k, j, i)) * 0.5;
-        else                                          dtde = (T(k + 1, j + 1, i) + T(k, j + 1, i) - T(k + 1, j - 1, i) - T(k, j - 1, i)) * 0.25;
-        const double dtdz = T(k + 1, j, i) - T(k, j, i);
-        int kL, kR;
-        stencil4(k, mz, g.pk, kL, kR);
+        if (AX) {
+            const double et = m.jeta.z[f];
+            vs.y[f] = v0 + ((et * et) * dtde) * ajc * ke;
+        } else {
+            const R3<double> cs = ld3(m.jcsi, f), et = ld3(m.jeta, f), ze = ld3(m.jzet, f);
+            const double g11 = cs.x * et.x + cs.y * et.y + cs.z * et.z, g21 = et.x * et.x + et.y * et.y + et.z * et.z,
+                         g31 = ze.x * et.x + ze.y * et.y + ze.z * et.z;
+            vs.y[f] = v0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+        }
+    };
+    // ---- k face fk = k + e (Compute_dscalar_k, inline.h:3294-3331)
+    auto kface = [&](int fk, int e) {
+        const int f = g.lin(fk, j, i);
+        const bool edge = (fk == 0 || fk == mz - 2);
+        double dtdc = 0.0, dtde;
+        if (!AX) {
+            if (i == mx - 2 && edge && (npi || npk))  dtdc = (T(e + 1, 0, 0) + T(e, 0, 0) - T(e + 1, 0, -1) - T(e, 0, -1)) * 0.5;
+            else if (i == 1 && edge && (npi || npk))  dtdc = (T(e + 1, 0, 1) + T(e, 0, 1) - T(e + 1, 0, 0) - T(e, 0, 0)) * 0.5;
+            else                                      dtdc = (T(e + 1, 0, 1) + T(e, 0, 1) - T(e + 1, 0, -1) - T(e, 0, -1)) * 0.25;
+        }
+        if (j == my - 2 && edge && (npj || npk))      dtde = (T(e + 1, 0, 0) + T(e, 0, 0) - T(e + 1, -1, 0) - T(e, -1, 0)) * 0.5;
+        else if (j == 1 && edge && (npj || npk))      dtde = (T(e + 1, 1, 0) + T(e, 1, 0) - T(e + 1, 0, 0) - T(e, 0, 0)) * 0.5;
+        else                                          dtde = (T(e + 1, 1, 0) + T(e, 1, 0) - T(e + 1, -1, 0) - T(e, -1, 0)) * 0.25;
+        const double dtdz = T(e + 1, 0, 0) - T(e, 0, 0);
         const double uc = s.ucont.z[f];
-        dv.z[f] = -uc * weno3(T(kL, j, i), T(k, j, i), T(k + 1, j, i), T(kR, j, i), uc);
-        const R3<double> cs = ld3(m.kcsi, f), et = ld3(m.keta, f), ze = ld3(m.kzet, f);
-        const double g11 = cs.x * ze.x + cs.y * ze.y + cs.z * ze.z, g21 = et.x * ze.x + et.y * ze.y + et.z * ze.z,
-                     g31 = ze.x * ze.x + ze.y * ze.y + ze.z * ze.z;
+        double w;
+        if (edge) {
+            int kL, kR;
+            stencil4(fk, mz, g.pk, kL, kR);
+            w = weno3(TG(kL, j, i), T(e, 0, 0), T(e + 1, 0, 0), TG(kR, j, i), uc);
+        } else w = weno3(T(e - 1, 0, 0), T(e, 0, 0), T(e + 1, 0, 0), T(e + 2, 0, 0), uc);
+        dv.z[f] = -uc * w;
         const double ajc = m.kaj[f];
-        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(k, j, i) + NUT(k + 1, j, i)) : 0.0, dtde, ajc);
-        vs.z[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
-    }
+        const double ke = kappa_eff(p, p.les ? 0.5 * (NUT(e, 0, 0) + NUT(e + 1, 0, 0)) : 0.0, dtde, ajc);
+        if (AX) {
+            const double ze = m.kzet.x[f];
+            vs.z[f] = 0.0 + ((ze * ze) * dtdz) * ajc * ke;
+        } else {
+            const R3<double> cs = ld3(m.kcsi, f), et = ld3(m.keta, f), ze = ld3(m.kzet, f);
+            const double g11 = cs.x * ze.x + cs.y * ze.y + cs.z * ze.z, g21 = et.x * ze.x + et.y * ze.y + et.z * ze.z,
+                         g31 = ze.x * ze.x + ze.y * ze.y + ze.z * ze.z;
+            vs.z[f] = 0.0 + (g11 * dtdc + g21 * dtde + g31 * dtdz) * ajc * ke;
+        }
+    };
+    const int ni = (i == 1 && npi) ? 2 : 1, nj = (j == 1 && npj) ? 2 : 1, nk = (k == 1 && npk) ? 2 : 1;
+#pragma unroll 1
+    for (int e = 0; e > -ni; e--) iface(i + e, e);
+#pragma unroll 1
+    for (int e = 0; e > -nj; e--) jface(j + e, e);
+#pragma unroll 1
+    for (int e = 0; e > -nk; e--) kface(k + e, e);
+}
+
+// FormT pass 1 on the context's stream
+void t_face_fluxes(tg_ctx *C)
+{
+    const Grid g = C->g;
+    const dim3 gr((g.mx - 2 + TBX - 1) / TBX, (g.my - 2 + TBY - 1) / TBY, (g.mz - 2 + TBZ - 1) / TBZ), bl(TBX, TBY, TBZ);
+    State &s = C->s;
+    if (C->axis_aligned)
+        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<true><<<gr, bl, 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+    else
+        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<false><<<gr, bl, 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
 }
 
 // pass 2 (teqn_solvers.c:520-566): rhs = (div budget + visc budget) aj at
@@ -347,7 +437,7 @@ static int solve_t_abbe(tg_ctx *C)
     if (!C->tgm) C->tgm = gmres_alloc(C, G, C->cfg.t_gmres_restart > 0 ? C->cfg.t_gmres_restart : 30);
     // Steps 1-2: periodic ghosts, convective right-hand side at T^n
     reset_cell_periodic_s(C, s.tmprt);
-    TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+    t_face_fluxes(C);
     TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, C->tconv, 1));
     // Steps 3-4: b (in Ttmp) and the guess; as in the reference the solution
     // goes into RhsConv_o, whose AB2 history this kernel consumes first
@@ -358,7 +448,7 @@ static int solve_t_abbe(tg_ctx *C)
     auto A = [&](const double *v, double *Av) {
         TG_CUDA(cudaMemcpyAsync(s.tmprt, v, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         reset_cell_periodic_s(C, s.tmprt);
-        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        t_face_fluxes(C);
         TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 2));
         TG_PROF(C, "teqn_abbe_av", k_t_abbe_av<<<nblk(G), 256, 0, C->stream>>>(G, Av, v, s.trhs, dt));
     };
@@ -390,7 +480,7 @@ static int solve_t_snes(tg_ctx *C)
     auto Feval = [&](const double *t, double *F) {
         TG_CUDA(cudaMemcpyAsync(s.tmprt, t, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         reset_cell_periodic_s(C, s.tmprt);
-        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        t_face_fluxes(C);
         TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 0));
         TG_PROF(C, "teqn_snes_f", k_t_snes_f<<<nblk(G), 256, 0, C->stream>>>(G, F, s.trhs, t, s.tmprt_o,
                                                                            bdf2 ? C->tmprt_oo : s.tmprt_o, dt, bdf2));
@@ -426,7 +516,7 @@ int solve_t(tg_ctx *C)
     for (int st = 0; st < 4; st++) {
         // FormExplicitRhsT: periodic ghosts, FormT (Rhs zero off the interior)
         reset_cell_periodic_s(C, s.tmprt);
-        TG_PROF(C, "teqn_face_fluxes", k_t_face_fluxes<<<gfaces(g), block3(), 0, C->stream>>>(g, C->m, s, C->prm, s.tdiv, s.tvisc));
+        t_face_fluxes(C);
         TG_PROF(C, "teqn_rhs", k_t_rhs<<<gint(g), block3(), 0, C->stream>>>(g, C->m, s.tdiv, s.tvisc, s.trhs, 0));
         TG_PROF(C, "teqn_rk_update", k_t_rk<<<nblk(G), 256, 0, C->stream>>>(G, s.tmprt, s.tmprt_o, s.ttmp, s.trhs,
                                                                           dt * b[st], st < 3 ? a[st + 1] * dt : 0.0, st == 0, st == 3));
