@@ -60,6 +60,9 @@ def bytes_per_cell(kernel, precision, axis=False):
             "grad_p": 4 * 8 + 6 * m,
             # phi 1, ucont 3 -> ucont 3; icsi.y, jeta.z, kzet.x and the face aj 3
             "project": 7 * 8 + 6 * m,
+            # T 1, nut 1, ucont 3; icsi.y, jeta.z, kzet.x and the face aj 3 (FP64
+            # in every mode) -> convective and diffusive fluxes 6
+            "teqn_face_fluxes": (5 + 6 + 6) * 8,
         }
         if kernel in table:
             return table[kernel]
@@ -91,6 +94,8 @@ def bytes_per_cell(kernel, precision, axis=False):
         "pois_cg_update": 48,          # x, r read/write; p, q read
         "pois_cg_dir": 24,             # z, p read; p write
         "pois_dot": 16,                # two vectors
+        # T 1, nut 1, ucont 3; face metrics 27 + 3 (FP64) -> fluxes 6
+        "teqn_face_fluxes": (5 + 30 + 6) * 8,
     }
     return table.get(kernel)
 
