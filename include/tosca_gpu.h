@@ -414,7 +414,9 @@ tg_status tg_adjoint_reverse(tg_ctx *ctx, tg_adjoint_stats *stats);
  * new state; nut (LES on) is only written, since the step recomputes it from
  * Ucat before any use (UpdateNut at the start of the step, main.c:54-99). This
  * is the call a host time loop makes when the state lives in its own (PETSc)
- * vectors. */
+ * vectors. With teqn = 1 the temperature stays in the context between calls;
+ * a host that keeps it in its own vector moves it with tg_set_field /
+ * tg_get_field (TG_F_TMPRT) around the call. */
 tg_status tg_step_host(tg_ctx *ctx, double *ucont, double *ucat, double *p,
                        double *nut, int32_t halo, tg_stats *stats);
 
