@@ -126,3 +126,24 @@ def test_thermal_wall_configuration_checked():
     for bad in (dict(les=0), dict(t_wall_type=-4), dict(t_wall_kappa=0.0), dict(wall_theta_ref=-1.0)):
         with pytest.raises(api.TgError):
             tosca_b200.gpu_solver(api.Config(**{**cfg.__dict__, **bad}))
+
+
+def test_drop_in_step_with_temperature():
+    """The drop-in step with the state in host arrays and the temperature
+    handed over around it (tg_set_field / tg_get_field TG_F_TMPRT), as a host
+    that keeps T in its own vector does, against three oracle steps."""
+    cfg, nodes, ucat, p, T = _case("sabl", api.TWALL_SHUMANN, heating_rate=-0.01)
+    g = tosca_b200.gpu_solver(cfg)
+    o = oracle.solver(cfg)
+    for s in (g, o):
+        cases.setup(s, nodes, ucat, p, T)
+    uc, ut, pp, tt = (np.ascontiguousarray(o.get(f)) for f in ("UCONT", "UCAT", "P", "TMPRT"))
+    for _ in range(3):
+        g.set("TMPRT", tt)
+        g.step_host(uc, ut, pp)
+        tt = g.get("TMPRT")
+        o.step(1)
+    assert rel_l2(tt, o.get("TMPRT")) < 1e-10
+    assert rel_l2(ut, o.get("UCAT")) < 1e-10 and rel_l2(uc, o.get("UCONT")) < 1e-10
+    assert rel_l2(pp, o.get("P")) < 1e-9
+    g.close(); o.close()
