@@ -429,10 +429,12 @@ def farm_adjoint(dev, precision, steps, warmup=5, fwd_steps=10):
     """Gradient of the farm power summed over `steps` steps with respect to the
     turbines' C_T' (tg_set_farm_objective) on the farm workload (Schumann wall
     function on the ground), forward in
-    `precision`: tg_adjoint_forward with binomial checkpointing in as many
-    device snapshots as half the free HBM holds, then tg_adjoint_reverse from
-    zero adjoint fields. Device time per reversed step against the device time
-    of a plain step of the same solver."""
+    `precision`: tg_adjoint_forward offered as many device snapshots as half
+    the free HBM holds (the library then takes the segment schedule when the
+    tapes of a segment fit beside them: a snapshot per segment, each segment
+    re-run once taped in the reversal; binomial checkpointing otherwise),
+    then tg_adjoint_reverse from zero adjoint fields. Device time per reversed
+    step against the device time of a plain step of the same solver."""
     import torch
     import tosca_b200
     from tosca_b200 import api, cases
