@@ -77,7 +77,7 @@ enum { TG_ILEFT = 0, TG_IRIGHT = 1, TG_JLEFT = 2, TG_JRIGHT = 3, TG_KLEFT = 4, T
 enum { TG_TBC_ZERO_GRADIENT = 0, TG_TBC_FIXED_VALUE = 1, TG_TBC_FIXED_GRADIENT = 2, TG_TBC_PERIODIC = 3,
        TG_TBC_WALL_FUNCTION = 4 };
 /* thetaWallFunction types (boundary/T "type", boundary.c:5110-5180) */
-enum { TG_TWALL_FIXED_FLUX = -2, TG_TWALL_SHUMANN = -3 };
+enum { TG_TWALL_FIXED_FLUX = -2, TG_TWALL_SHUMANN = -3, TG_TWALL_SURFACE_SERIES = -4 };
 /* -dTdtScheme (teqn.c:66-230): explicit RK4; ABBE (Adams-Bashforth 2
  * convection, backward-Euler diffusion solved by GMRES on ABBEMatVec,
  * teqn_solvers.c:821-945); BE and BDF2 (implicit, Newton-Krylov on
@@ -153,7 +153,13 @@ typedef struct tg_config {
      * at the wall value and rises by t_wall_heating_rate * dt every step;
      * t_wall_localized 0 ("averaged") evaluates it once from plane means,
      * 1 ("localized") per wall cell. TG_TWALL_FIXED_FLUX (-2): qWall =
-     * t_wall_qwall everywhere. */
+     * t_wall_qwall everywhere. TG_TWALL_SURFACE_SERIES (-4): as -3, with the
+     * surface temperature interpolated in time from the series given by
+     * tg_set_surface_temperature (findInterpolationWeights,
+     * inline.h:5873-5940) at the clock time of the step, t_start +
+     * (it - it_start + 1) dt (fixed time step, clock.c:347-367), and from
+     * the second step on the ghost temperature 2 T_s - T(j=1) on the ground
+     * (boundary.c:2390-2411). */
     int32_t t_wall_type;
     int32_t t_wall_localized;
     double  t_wall_qwall;          /* -2: heat flux (K m/s)                                  */
@@ -170,6 +176,7 @@ typedef struct tg_config {
      * friction velocity; gammaM and thetaRef of velocityWallFunction */
     double  wall_gamma_m;
     double  wall_theta_ref;
+    double  t_start;               /* -startTime: clock time at it_start (thetaWallFunction -4) */
 } tg_config;
 
 /* per-call statistics */
@@ -261,6 +268,10 @@ tg_status tg_buoyancy(tg_ctx *ctx);                    /* ueqn_sources.h:23 / ue
  * qWall (TG_F_QWALL, TG_F_SURF_THETA) and the temperature ghost cells */
 tg_status tg_update_wall_models_t(tg_ctx *ctx);        /* boundary.h:191 / boundary.c:3858-4520    */
 tg_status tg_update_temperature_bcs(tg_ctx *ctx);      /* boundary.h:170 / boundary.c:2052-2616    */
+/* the surface temperature series of thetaWallFunction -4: n >= 2 times and
+ * temperatures (the reference reads them from inflowDatabase/mesoscaleData,
+ * readSurfaceTempData boundary.c:5269-5400); copied, kept until replaced */
+tg_status tg_set_surface_temperature(tg_ctx *ctx, int32_t n, const double *time, const double *temp);
 /* Rhs (TG_F_RHS) += scale * FormU on the current lUcont/lUcat/nut:
  * ueqn_solvers.h:15 / ueqn_solvers.c:6-1083 with formMode 0. Rhs is
  * zeroed first when zero_rhs. */

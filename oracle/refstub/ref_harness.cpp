@@ -121,7 +121,7 @@ wallModel *make_theta_wall(const tg_config &c)
     }
     w->qWall.x = q[0]; w->qWall.y = q[1]; w->qWall.z = q[2];
     Shumann *s = new Shumann();
-    if (c.t_wall_type == TG_TWALL_SHUMANN) {
+    if (c.t_wall_type == TG_TWALL_SHUMANN || c.t_wall_type == TG_TWALL_SURFACE_SERIES) {
         s->wfEvalType = c.t_wall_localized ? "localized" : "averaged";
         s->kappa = c.t_wall_kappa;
         s->thetaRef = c.t_wall_theta_ref;
@@ -132,6 +132,7 @@ wallModel *make_theta_wall(const tg_config &c)
         s->heatingRate = c.t_wall_heating_rate;
         s->tLast = -1.0;
         s->surfaceThetaSet = 0;
+        s->numT = 0;                 // -4: the series comes from ref_set_surface_temperature
     } else {
         s->qWall = c.t_wall_qwall;
     }
@@ -224,7 +225,8 @@ void build(tg_ctx &X)
     X.clock.dtOld = c.dt;
     X.clock.itStart = c.it_start;
     X.clock.it = c.it_start;
-    X.clock.time = 0.0;
+    X.clock.startTime = c.t_start;
+    X.clock.time = c.t_start;
 
     // ---- mesh (SetDistributedArrays, mesh.c:34-447)
     mesh_ &m = X.mesh;
@@ -446,7 +448,8 @@ tg_status ref_create(const tg_config *cfg, tg_ctx **out)
         if (c.teqn && c.t_bc[q] == TG_TBC_WALL_FUNCTION && q != 2) return TG_ERR_BAD_ARG;
     }
     if (c.teqn && c.t_bc[2] == TG_TBC_WALL_FUNCTION &&
-        (!c.les || (c.t_wall_type != TG_TWALL_SHUMANN && c.t_wall_type != TG_TWALL_FIXED_FLUX))) return TG_ERR_BAD_ARG;
+        (!c.les || (c.t_wall_type != TG_TWALL_SHUMANN && c.t_wall_type != TG_TWALL_FIXED_FLUX &&
+                    c.t_wall_type != TG_TWALL_SURFACE_SERIES))) return TG_ERR_BAD_ARG;
     if (c.les && std::fabs(c.cs - TOSCA_STD_CS) > 1e-15) return TG_ERR_BAD_ARG;
     tg_ctx *C = new tg_ctx();
     C->cfg = c;
@@ -659,6 +662,9 @@ tg_status ref_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
         tg_stats local{};
         teqn_ *t = C->cfg.teqn ? &C->teqn : nullptr;
         for (int32_t s = 0; s < nsteps; s++) {
+            // adjustTimeStep with a fixed time step (clock.c:347-367): the
+            // clock time of the step, it counted from itStart
+            C->clock.time = C->clock.startTime + (C->clock.it - C->clock.itStart) * C->clock.dt + C->clock.dt;
             VecCopy(u.Ucont, u.Ucont_o);                            // main.c:81
             if (t) VecCopy(t->Tmprt, t->Tmprt_o);                   // main.c:83-99 (RK4)
             if (C->cfg.les) {                                       // main.c:108-113
@@ -691,8 +697,7 @@ tg_status ref_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
             UpdateCartesianBCs(&u);                                 // main.c:284
             UpdateContravariantBCs(&u);                             // main.c:287
             SyncPressureAcrossDomains(C->dom.get());                // main.c:318
-            C->clock.it++;                                          // main.c:321
-            C->clock.time += C->clock.dt;
+            C->clock.it++;                                          // main.c:319
             local.steps++;
             local.poisson_iterations = (int32_t)p.poissonIterations;
             local.poisson_total_iterations += (int32_t)p.poissonIterations;
@@ -738,6 +743,22 @@ tg_status ref_update_temperature_bcs(tg_ctx *C)
     return guarded(C, [&]() -> tg_status {
         if (!C->cfg.teqn) return fail(C, TG_ERR_STATE, "no temperature equation");
         UpdateTemperatureBCs(&C->teqn);
+        return TG_OK;
+    });
+}
+
+// the series readSurfaceTempData (boundary.c:5269-5400) would read from
+// inflowDatabase/mesoscaleData: timeVec, surfTemp and numT of the jLeft Shumann model
+tg_status ref_set_surface_temperature(tg_ctx *C, int32_t n, const double *time, const double *temp)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (n < 2 || !time || !temp) return fail(C, TG_ERR_BAD_ARG, "a surface temperature series needs n >= 2 points");
+        if (!C->cfg.teqn || !C->teqn.jLWM) return fail(C, TG_ERR_STATE, "no thetaWallFunction");
+        Shumann *wm = C->teqn.jLWM->wmShumann;
+        wm->timeVec = new PetscReal[n];
+        wm->surfTemp = new PetscReal[n];
+        for (int32_t q = 0; q < n; q++) { wm->timeVec[q] = time[q]; wm->surfTemp[q] = temp[q]; }
+        wm->numT = n;
         return TG_OK;
     });
 }

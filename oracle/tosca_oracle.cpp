@@ -129,6 +129,7 @@ struct tg_ctx {
     // (planes k*mx + i), surfaceThetaSet (tosca_oracle_teqn.inc)
     std::vector<double> qwall, surf_theta;
     bool surf_set = false;
+    std::vector<double> surf_series_t, surf_series_v;   // -4: surface temperature series
 
     // pressure system
     Csr A;
@@ -1894,7 +1895,7 @@ const char *tor_last_error(const tg_ctx *C) { return C ? C->err.c_str() : "null 
 static bool theta_wall_config_ok(const tg_config *cfg)
 {
     if (!cfg->les) return false;
-    if (cfg->t_wall_type == TG_TWALL_SHUMANN) {
+    if (cfg->t_wall_type == TG_TWALL_SHUMANN || cfg->t_wall_type == TG_TWALL_SURFACE_SERIES) {
         if (!(cfg->t_wall_kappa > 0) || !(cfg->t_wall_theta_ref > 0) || !(cfg->t_wall_roughness > 0) || !(cfg->t_wall_alpha_h > 0))
             return false;
         if (cfg->t_wall_localized != 0 && cfg->t_wall_localized != 1) return false;
@@ -2105,6 +2106,16 @@ TOR_STAGE(tor_update_wall_models_t,
           if (!C->c.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); updateWallModelsT(*C))
 TOR_STAGE(tor_update_temperature_bcs,
           if (!C->c.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); updateTemperatureBCs(*C))
+
+tg_status tor_set_surface_temperature(tg_ctx *C, int32_t n, const double *time, const double *temp)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (n < 2 || !time || !temp) return fail(C, TG_ERR_BAD_ARG, "a surface temperature series needs n >= 2 points");
+        C->surf_series_t.assign(time, time + n);
+        C->surf_series_v.assign(temp, temp + n);
+        return TG_OK;
+    });
+}
 
 // the Monin-Obukhov functions of the restatement, for comparison with the reference's
 double tor_mo_ustar(double U, double dist, double z0, double gammaM, double kappa, double qwall, double thetaRef)

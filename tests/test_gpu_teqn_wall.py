@@ -123,7 +123,7 @@ def test_thermal_wall_replay_and_mixed():
 
 def test_thermal_wall_configuration_checked():
     cfg, *_ = _case("sabl", api.TWALL_SHUMANN)
-    for bad in (dict(les=0), dict(t_wall_type=-4), dict(t_wall_kappa=0.0), dict(wall_theta_ref=-1.0)):
+    for bad in (dict(les=0), dict(t_wall_type=-5), dict(t_wall_kappa=0.0), dict(wall_theta_ref=-1.0)):
         with pytest.raises(api.TgError):
             tosca_b200.gpu_solver(api.Config(**{**cfg.__dict__, **bad}))
 
@@ -147,3 +147,55 @@ def test_drop_in_step_with_temperature():
     assert rel_l2(ut, o.get("UCAT")) < 1e-10 and rel_l2(uc, o.get("UCONT")) < 1e-10
     assert rel_l2(pp, o.get("P")) < 1e-9
     g.close(); o.close()
+
+
+SERIES = (np.array([0.0, 50.0, 100.0, 100.5, 101.0, 102.0]), np.array([302.0, 301.0, 300.5, 299.8, 299.0, 298.0]))
+
+
+@pytest.mark.parametrize("case,localized", [("sabl", False), ("sabl", True), ("hill", False)])
+def test_surface_temperature_series_matches_oracle(case, localized):
+    """thetaWallFunction -4 (surface temperature interpolated in time from a
+    series, ground ghost 2 T_s - T(j=1) after the first step) after 5 steps
+    from t_start = 100 s, through and beyond the series' points."""
+    cfg, nodes, ucat, p, T = _case(case, api.TWALL_SURFACE_SERIES, localized=localized)
+    cfg.t_start = 100.0
+    out = []
+    for make in (tosca_b200.gpu_solver, oracle.solver):
+        s = make(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        s.set_surface_temperature(*SERIES)
+        s.step(5)
+        out.append(s)
+    g, o = out
+    for f in ("TMPRT", "UCAT", "UCONT"):
+        assert rel_l2(g.get(f), o.get(f)) < 1e-10, f
+    assert rel_l2(g.get("P"), o.get("P")) < 1e-9
+    assert np.abs(g.get("TMPRT") - o.get("TMPRT")).max() <= 1e-10 * 300.0     # ghosts included
+    qg, qo = g.get("QWALL"), o.get("QWALL")
+    assert np.abs(qg - qo).max() <= 1e-8 * np.abs(qo).max() and np.abs(qo).max() > 0
+    g.close(); o.close()
+
+
+def test_surface_temperature_series_replay_and_refusal():
+    """The -4 step replays from its graph bitwise (the surface temperature is
+    interpolated on the device from the step counter), a new series of another
+    length rebuilds the graph, and a step without a series is refused."""
+    cfg, nodes, ucat, p, T = _case("sabl", api.TWALL_SURFACE_SERIES)
+    cfg.t_start = 100.0
+    res = []
+    for graphs in (False, True):
+        s = tosca_b200.gpu_solver(cfg)
+        cases.setup(s, nodes, ucat, p, T)
+        if graphs:
+            with pytest.raises(api.TgError):
+                s.step(1)
+        s.set_surface_temperature(*SERIES)
+        s.set_graphs(graphs)
+        s.step(3)
+        s.set_surface_temperature(np.array([0.0, 200.0]), np.array([301.0, 297.0]))
+        s.step(3)
+        res.append((s, s.get("TMPRT"), s.get("QWALL")))
+    (e, te, qe), (r, tr, qr) = res
+    assert np.array_equal(te, tr) and np.array_equal(qe, qr)
+    assert r.graph_info()[0] >= 3
+    e.close(); r.close()

@@ -206,3 +206,26 @@ def test_thermal_wall_configuration_checked():
         c = api.Config(**{**cfg.__dict__, **bad})
         with pytest.raises(api.TgError):
             oracle.solver(c)
+
+
+def test_surface_temperature_series_ghost_rule():
+    """-4: the ground ghost is zero-gradient after the first step and 2 T_s -
+    T(j=1) after the later ones (boundary.c:2392-2408); qWall follows the
+    series' surface temperature; without a series the step is refused."""
+    cfg, nodes, ucat, p, T = _sabl()
+    cfg.t_wall_type, cfg.t_start = api.TWALL_SURFACE_SERIES, 0.0
+    s = oracle.solver(cfg)
+    cases.setup(s, nodes, ucat, p, T)
+    with pytest.raises(api.TgError):
+        s.step(1)
+    ts = 299.5
+    s.set_surface_temperature([0.0, 10.0], [ts, ts])
+    s.step(1)
+    t = s.get("TMPRT")
+    assert np.array_equal(t[1:-1, 0, 1:-1], t[1:-1, 1, 1:-1])
+    s.step(1)
+    t = s.get("TMPRT")
+    assert np.abs(t[1:-1, 0, 1:-1] + t[1:-1, 1, 1:-1] - 2 * ts).max() <= 1e-12 * ts
+    q = s.get("QWALL")[1:-1, 1:-1]
+    assert np.all(q == q[0, 0]) and q[0, 0] < 0        # air at ~300 K over a 299.5 K surface: stable
+    s.close()

@@ -191,6 +191,7 @@ def _pair_t(case, kind=api.TWALL_SHUMANN, heating_rate=-0.01, localized=False, q
     if kind is not None:
         cfg.t_wall_type, cfg.t_wall_qwall = kind, qwall
     cfg.cs, cfg.poisson_rtol, cfg.p_tilde = 0.0289, 1e-14, p_tilde
+    cfg.t_start = 100.0
     o = oracle.solver(cfg)
     cases.setup(o, nodes, ucat, p, T)
     r = R.solver(cfg)
@@ -274,4 +275,27 @@ def test_steps_with_temperature(case, kind, localized, heating_rate, qwall):
         assert np.abs(qo - qr).max() <= 1e-9 * np.abs(qr).max()
         assert np.abs(o.get("SURF_THETA") - r.get("SURF_THETA")).max() <= 1e-12 * 300.0
         assert rel_l2(r.get("TAUWALL"), o.get("TAUWALL"), _full) < 1e-12
+    o.close(); r.close()
+
+
+SERIES = (np.array([0.0, 50.0, 100.0, 100.5, 101.0, 102.0]), np.array([302.0, 301.0, 300.5, 299.8, 299.0, 298.0]))
+
+
+@pytest.mark.parametrize("case,localized", [("sabl", False), ("sabl", True), ("hill", False)])
+def test_steps_with_surface_temperature_series(case, localized):
+    """thetaWallFunction -4: the surface temperature interpolated in time
+    (findInterpolationWeights) at the clock time of each step, from t_start =
+    100 s, between and beyond the series' points; the ghost rule 2 T_s - T(j=1)
+    from the second step on."""
+    o, r = _pair_t(case, api.TWALL_SURFACE_SERIES, localized=localized)
+    for s in (o, r):
+        s.set_surface_temperature(*SERIES)
+    for _ in range(3):
+        o.step(1); r.step(1)
+    for f in ("UCONT", "UCAT", "TMPRT"):
+        assert rel_l2(r.get(f), o.get(f)) < 1e-12, f
+    assert rel_l2(r.get("P"), o.get("P")) < (1e-9 if case == "hill" else 1e-10)
+    qr, qo = r.get("QWALL"), o.get("QWALL")
+    assert np.abs(qo - qr).max() <= 1e-9 * np.abs(qr).max() and np.abs(qr).max() > 0
+    assert np.abs(o.get("TMPRT") - r.get("TMPRT")).max() <= 1e-12 * 300.0      # ghosts included
     o.close(); r.close()

@@ -24,7 +24,7 @@ DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
 TDDT_RK4, TDDT_ABBE, TDDT_BE, TDDT_BDF2 = 0, 1, 2, 3
 TBC_ZERO_GRADIENT, TBC_FIXED_VALUE, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION = 0, 1, 2, 3, 4
-TWALL_FIXED_FLUX, TWALL_SHUMANN = -2, -3
+TWALL_FIXED_FLUX, TWALL_SHUMANN, TWALL_SURFACE_SERIES = -2, -3, -4
 PREC_FP64, PREC_MIXED = 0, 1
 
 FIELDS = [
@@ -92,6 +92,7 @@ class TgConfig(C.Structure):
         ("t_wall_alpha_h", C.c_double),
         ("wall_gamma_m", C.c_double),
         ("wall_theta_ref", C.c_double),
+        ("t_start", C.c_double),
     ]
 
 
@@ -203,6 +204,7 @@ class Config:
     # stability correction of the velocity wall function (with a thetaWallFunction)
     wall_gamma_m: float = 4.8
     wall_theta_ref: float = 300.0
+    t_start: float = 0.0
 
     def to_c(self) -> TgConfig:
         c = TgConfig()
@@ -237,6 +239,7 @@ _SIGS = {
     "buoyancy": (C.c_int, [C.c_void_p]),
     "update_wall_models_t": (C.c_int, [C.c_void_p]),
     "update_temperature_bcs": (C.c_int, [C.c_void_p]),
+    "set_surface_temperature": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
     "form_u": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "explicit_rhs": (C.c_int, [C.c_void_p]),
     "solve_u": (C.c_int, [C.c_void_p]),
@@ -424,6 +427,14 @@ class Solver:
 
     def UpdateTemperatureBCs(self):
         self._check(self.fns["update_temperature_bcs"](self.h), "UpdateTemperatureBCs")
+
+    def set_surface_temperature(self, time, temp):
+        """The surface temperature series of thetaWallFunction -4."""
+        t = np.ascontiguousarray(time, dtype=np.float64)
+        v = np.ascontiguousarray(temp, dtype=np.float64)
+        if t.shape != v.shape or t.ndim != 1:
+            raise ValueError("time and temperature must be 1-D arrays of one length")
+        self._check(self.fns["set_surface_temperature"](self.h, int(t.size), _ptr(t), _ptr(v)), "set_surface_temperature")
 
     def FormU(self, scale: float = 1.0, zero_rhs: bool = True):
         self._check(self.fns["form_u"](self.h, scale, 1 if zero_rhs else 0), "FormU")

@@ -204,7 +204,7 @@ const char *tg_last_error(const tg_ctx *C) { return C ? C->err.c_str() : "null c
 static bool theta_wall_config_ok(const tg_config *cfg)
 {
     if (!cfg->les) return false;
-    if (cfg->t_wall_type == TG_TWALL_SHUMANN) {
+    if (cfg->t_wall_type == TG_TWALL_SHUMANN || cfg->t_wall_type == TG_TWALL_SURFACE_SERIES) {
         if (!(cfg->t_wall_kappa > 0) || !(cfg->t_wall_theta_ref > 0) || !(cfg->t_wall_roughness > 0) || !(cfg->t_wall_alpha_h > 0))
             return false;
         if (cfg->t_wall_localized != 0 && cfg->t_wall_localized != 1) return false;
@@ -595,9 +595,30 @@ TG_STAGE(tg_update_cartesian_bcs, update_cartesian_bcs(C))
 TG_STAGE(tg_update_contravariant_bcs, update_contravariant_bcs(C))
 TG_STAGE(tg_sync_pressure, sync_pressure(C))
 TG_STAGE(tg_update_wall_models_t,
-         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); update_wall_models_t(C))
+         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off");
+         if (const char *why = theta_wall_missing(C)) return fail(C, TG_ERR_STATE, why); update_wall_models_t(C))
 TG_STAGE(tg_update_temperature_bcs,
-         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off"); update_temperature_bcs(C))
+         if (!C->prm.teqn) return fail(C, TG_ERR_STATE, "temperature equation off");
+         if (const char *why = theta_wall_missing(C)) return fail(C, TG_ERR_STATE, why); update_temperature_bcs(C))
+
+tg_status tg_set_surface_temperature(tg_ctx *C, int32_t n, const double *time, const double *temp)
+{
+    return guarded(C, [&]() -> tg_status {
+        if (n < 2 || !time || !temp) return fail(C, TG_ERR_BAD_ARG, "a surface temperature series needs n >= 2 points");
+        if (n > C->series_n) {
+            // captured step graphs hold the old arrays: rebuild them
+            graph_destroy(C);
+            C->series_t = dallocd(C, (size_t)n);
+            C->series_v = dallocd(C, (size_t)n);
+        }
+        TG_CUDA(cudaMemcpyAsync(C->series_t, time, sizeof(double) * n, cudaMemcpyHostToDevice, C->stream));
+        TG_CUDA(cudaMemcpyAsync(C->series_v, temp, sizeof(double) * n, cudaMemcpyHostToDevice, C->stream));
+        TG_CUDA(cudaStreamSynchronize(C->stream));
+        if (n != C->series_n) graph_destroy(C);     // the count is a launch argument of the captured steps
+        C->series_n = n;
+        return TG_OK;
+    });
+}
 
 tg_status tg_form_u(tg_ctx *C, double scale, int32_t zero_rhs)
 {
@@ -637,6 +658,7 @@ tg_status tg_step(tg_ctx *C, int32_t nsteps, tg_stats *st)
     return guarded(C, [&]() -> tg_status {
         if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
         if (nsteps < 0) return fail(C, TG_ERR_BAD_ARG, "negative step count");
+        if (const char *why = theta_wall_missing(C)) return fail(C, TG_ERR_STATE, why);
         tg_stats local{};
         tg_stats *s = st ? st : &local;
         *s = tg_stats{};
@@ -712,6 +734,7 @@ tg_status tg_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double
     return guarded(C, [&]() -> tg_status {
         if (!ucont || !ucat || !p || halo < 0) return fail(C, TG_ERR_BAD_ARG, "null state");
         if (!C->has_mesh) return fail(C, TG_ERR_STATE, "mesh not set");
+        if (const char *why = theta_wall_missing(C)) return fail(C, TG_ERR_STATE, why);
         upload(C, ucont, halo, C->s.ucont.x, C->s.ucont.y, C->s.ucont.z);
         upload(C, ucat, halo, C->s.ucat.x, C->s.ucat.y, C->s.ucat.z);
         upload(C, p, halo, C->s.p, nullptr, nullptr);

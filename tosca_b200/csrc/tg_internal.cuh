@@ -177,6 +177,8 @@ struct tg_ctx {
     bool axis_aligned = false;
     bool ufilt_set = false;
     bool surf_set = false;               // thetaWallFunction -3 surfaceTheta seeded
+    double *series_t = nullptr, *series_v = nullptr;   // thetaWallFunction -4 surface temperature series
+    int series_n = 0;
     int it = 0;
     // mixed precision: FP32 copies of the stencil metrics (and FP32 FormU
     // planes when the policy stores the face fluxes in FP32)
@@ -317,7 +319,7 @@ constexpr int SC_G = 60, SC_ADJ = 70, SC_IT = 80;
 // solutions in the Poisson guess history (0, 1, 2 or more: order of the extrapolation)
 constexpr int SC_PHIST = 96;
 // thetaWallFunction averaged model: plane means and the resulting qWall
-constexpr int SC_TWALL = 24;
+constexpr int SC_TWALL = 24;       // 24..26 plane means, 27 qWall, 28 surface temperature (-4)
 // number of transposed-solve solutions in the adjoint guess history
 constexpr int SC_LHIST = 76;
 constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
@@ -356,6 +358,8 @@ void contra_to_cart_stage(tg_ctx *C);
 int solve_t(tg_ctx *C);      // 0, or the ABBE GMRES status (1 iteration cap, 2 breakdown)
 void update_temperature_bcs(tg_ctx *C);
 void update_wall_models_t(tg_ctx *C);   // UpdateWallModelsT: jLeft thetaWallFunction qWall
+// thetaWallFunction -4 without its surface temperature series: the error text, else nullptr
+const char *theta_wall_missing(const tg_ctx *C);
 // wind farm (tg_farm.cu)
 void farm_update(tg_ctx *C);                 // sampling, forces, projection, face body force
 void farm_destroy(tg_ctx *C);

@@ -313,7 +313,7 @@ __global__ void k_t_rk(int64_t n, double *t, const double *to, double *ttmp, con
 
 // UpdateTemperatureBCs (boundary.c:2052-2616) on the face ghosts of one patch
 // pair (dir: 0 i, 1 j, 2 k), from the interior next to them
-__global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
+__global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir, const double *series_st, const double *d_it, double it_start)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x + 1, b = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
@@ -326,7 +326,10 @@ __global__ void k_t_bcs(Grid g, Metrics m, Params p, double *t, int dir)
         const int ci = side == 0 ? 1 : mdir - 2, gh = side == 0 ? 0 : mdir - 1;
         const int c = at(ci), q = at(gh);
         const int type = p.t_bc[patch];
-        if (type == TG_TBC_ZERO_GRADIENT || type == TG_TBC_WALL_FUNCTION) t[q] = t[c];
+        if (type == TG_TBC_WALL_FUNCTION && patch == TG_JLEFT && p.t_wall == TG_TWALL_SURFACE_SERIES && series_st &&
+            d_it[0] != it_start)
+            t[q] = 2.0 * series_st[0] - t[c];        // -4 after the first step, boundary.c:2392-2408
+        else if (type == TG_TBC_ZERO_GRADIENT || type == TG_TBC_WALL_FUNCTION) t[q] = t[c];
         else if (type == TG_TBC_FIXED_VALUE) t[q] = p.t_bc_value[patch];
         else if (type == TG_TBC_FIXED_GRADIENT) {
             const double area = sqrt(S.x[c] * S.x[c] + S.y[c] * S.y[c] + S.z[c] * S.z[c]);
@@ -353,6 +356,32 @@ __device__ __forceinline__ void twall_cell(Grid g, Metrics m, State s, int k, in
     dist = 0.5 / m.aj[c] / sqrt(dot3(et, et));
 }
 
+// -4: the surface temperature at the clock time of the step, t_start + (it -
+// it_start) dt + dt (clock.c:366), interpolated in the series as
+// findInterpolationWeights does (inline.h:5873-5940: the two nearest points,
+// points within a relative 1e-5 of the nearer one's distance skipped,
+// extrapolating beyond the ends); one thread, out[0]
+__global__ void k_twall_series(const double *tv, const double *vv, int n, const double *d_it, double it_start, double t_start,
+                               double dt, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (n < 2 || !tv || !vv) { out[0] = 0.0; return; }     // no series: not launched by the host
+    const double pval = t_start + (d_it[0] - it_start) * dt + dt;
+    const double eqTol = 1e-5;
+    int i1 = 0, i2 = 1;
+    for (int q = 0; q < n; q++) {
+        const double dq = fabs(tv[q] - pval);
+        const double tol1 = fabs(dq - fabs(tv[i2] - pval)) / dq;
+        if (dq < fabs(tv[i1] - pval) && tol1 > eqTol) { i2 = i1; i1 = q; }
+        const double tol2 = fabs(dq - fabs(tv[i1] - pval)) / dq;
+        if (dq < fabs(tv[i2] - pval) && q != i1 && tol2 > eqTol) i2 = q;
+    }
+    if (tv[i2] < tv[i1]) { const int t = i1; i1 = i2; i2 = t; }
+    const double idx = (double)(i2 - i1) / (tv[i2] - tv[i1]) * (pval - tv[i1]) + (double)i1;
+    const double w0 = ((double)i2 - idx) / (double)(i2 - i1), w1 = (idx - (double)i1) / (double)(i2 - i1);
+    out[0] = w0 * vv[i1] + w1 * vv[i2];
+}
+
 // -3, first call: surfaceTheta = the wall value 0.5 (T(j=1) + T(j=0))
 __global__ void k_twall_seed(Grid g, State s)
 {
@@ -362,22 +391,23 @@ __global__ void k_twall_seed(Grid g, State s)
 }
 
 // -3 localized: surfaceTheta += heatingRate dt, then qWallShumann per cell
-__global__ void k_twall_local(Grid g, Metrics m, State s, Params p)
+__global__ void k_twall_local(Grid g, Metrics m, State s, Params p, const double *sts)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i > g.mx - 2 || k > g.mz - 2) return;
     const int w = k * g.mx + i;
     double upm, dist;
     twall_cell(g, m, s, k, i, upm, dist);
-    const double st = s.surf_theta[w] + p.tw_heating * p.dt;
-    s.surf_theta[w] = st;
+    double st;
+    if (sts) st = sts[0];
+    else { st = s.surf_theta[w] + p.tw_heating * p.dt; s.surf_theta[w] = st; }
     s.qwall[w] = mo::qwall(upm, dist, p.tw_z0, p.tw_gamma_m, p.tw_gamma_h, p.tw_alpha_h, p.tw_theta_ref,
                            s.tmprt[g.lin(k, 1, i)] - st, p.tw_kappa);
 }
 
 // -3 averaged, pass 1: surfaceTheta += heatingRate dt and per-block partial
 // sums of T(j=1) - surfaceTheta, |U_par| and the wall distance
-__global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part)
+__global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part, const double *sts)
 {
     __shared__ double sh[3][256];
     const int nI = g.mx - 2, nK = g.mz - 2;
@@ -386,8 +416,9 @@ __global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part)
         const int i = t % nI + 1, k = t / nI + 1, w = k * g.mx + i;
         double upm, dist;
         twall_cell(g, m, s, k, i, upm, dist);
-        const double st = s.surf_theta[w] + p.tw_heating * p.dt;
-        s.surf_theta[w] = st;
+        double st;
+        if (sts) st = sts[0];
+        else { st = s.surf_theta[w] + p.tw_heating * p.dt; s.surf_theta[w] = st; }
         sT += (s.tmprt[g.lin(k, 1, i)] - st);
         sU += upm;
         sD += dist;
@@ -536,6 +567,26 @@ int solve_t(tg_ctx *C)
 // prescribed flux. -3: surfaceTheta is seeded from the wall value on the
 // first call and rises by heatingRate * dt on every call; qWallShumann once
 // from the plane means ("averaged", two launches) or per cell ("localized")
+// -4: the surface temperature of the step into its device slot (nullptr
+// when the series is not set yet: the steps refuse to run then, and the ghost
+// update at initialisation, on the first step's clock, is zero-gradient)
+static const double *series_surface(tg_ctx *C)
+{
+    if (C->prm.t_wall != TG_TWALL_SURFACE_SERIES || C->series_n < 2 || !C->series_t || !C->series_v) return nullptr;
+    double *out = C->d_scal + SC_TWALL + 4;
+    k_twall_series<<<1, 32, 0, C->stream>>>(C->series_t, C->series_v, C->series_n, C->d_scal + SC_IT, (double)C->cfg.it_start,
+                                            C->cfg.t_start, C->prm.dt, out);
+    TG_CUDA(cudaGetLastError());
+    return out;
+}
+
+const char *theta_wall_missing(const tg_ctx *C)
+{
+    if (C->prm.t_wall == TG_TWALL_SURFACE_SERIES && C->series_n < 2)
+        return "thetaWallFunction -4 needs its surface temperature series (tg_set_surface_temperature)";
+    return nullptr;
+}
+
 void update_wall_models_t(tg_ctx *C)
 {
     if (!C->prm.les || !C->prm.t_wall) return;
@@ -545,16 +596,19 @@ void update_wall_models_t(tg_ctx *C)
         TG_PROF(C, "twall_fill", k_twall_fill<<<1, 256, 0, C->stream>>>(g, C->prm, C->d_red, 0, C->d_scal + SC_TWALL, C->s));
         return;
     }
-    if (!C->surf_set) {
+    const double *sts = series_surface(C);
+    if (C->prm.t_wall == TG_TWALL_SURFACE_SERIES && !sts)     // the entry points refuse this case before any launch
+        throw CudaError{cudaErrorInvalidValue, "thetaWallFunction -4 without its surface temperature series"};
+    if (!sts && !C->surf_set) {
         k_twall_seed<<<grid, b2, 0, C->stream>>>(g, C->s);
         C->surf_set = true;
     }
     if (C->prm.t_wall_localized) {
-        TG_PROF(C, "twall_local", k_twall_local<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm));
+        TG_PROF(C, "twall_local", k_twall_local<<<grid, b2, 0, C->stream>>>(g, C->m, C->s, C->prm, sts));
         return;
     }
     const int nb = 148;
-    TG_PROF(C, "twall_sums", k_twall_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_red));
+    TG_PROF(C, "twall_sums", k_twall_sums<<<nb, 256, 0, C->stream>>>(g, C->m, C->s, C->prm, C->d_red, sts));
     TG_PROF(C, "twall_fill", k_twall_fill<<<1, 256, 0, C->stream>>>(g, C->prm, C->d_red, nb, C->d_scal + SC_TWALL, C->s));
 }
 
@@ -563,9 +617,11 @@ void update_temperature_bcs(tg_ctx *C)
     const Grid g = C->g;
     const dim3 b2(32, 8);
     auto g2 = [](int na, int nb) { return dim3((na - 2 + 31) / 32, (nb - 2 + 7) / 8); };
-    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 0));
-    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 1));
-    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 2));
+    const double *sts = series_surface(C);
+    const double *dit = C->d_scal + SC_IT, its = (double)C->cfg.it_start;
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 0, sts, dit, its));
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 1, sts, dit, its));
+    TG_PROF(C, "teqn_bcs", k_t_bcs<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->m, C->prm, C->s.tmprt, 2, sts, dit, its));
 }
 
 }  // namespace tg
