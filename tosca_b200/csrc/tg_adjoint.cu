@@ -874,16 +874,12 @@ __device__ __forceinline__ void wall_par(const Grid &g, const Metrics &m, const 
 }
 
 // block sums of (a, b) into part[2 blockIdx], part[2 blockIdx + 1]
+// (blocks of 256 threads)
 __device__ __forceinline__ void block_sum2(double a, double b, double *part)
 {
-    __shared__ double sh[2][256];
-    sh[0][threadIdx.x] = a; sh[1][threadIdx.x] = b;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) { sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w]; }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) { part[2 * blockIdx.x] = sh[0][0]; part[2 * blockIdx.x + 1] = sh[1][0]; }
+    double v[2] = {a, b};
+    block_reduce<256>(v, RedSum{}, RedSum{});
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = v[0]; part[2 * blockIdx.x + 1] = v[1]; }
 }
 
 // forward plane sums of |Up| and the wall distance (the step-start Ucat)

@@ -43,25 +43,19 @@ namespace {
 
 constexpr int DB = 256;
 
-__global__ void k_dot_part(int64_t n, const double *a, const double *b, double *part)
+__global__ void __launch_bounds__(DB) k_dot_part(int64_t n, const double *a, const double *b, double *part)
 {
-    __shared__ double sh[DB];
-    double s = 0.0;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) s += a[t] * b[t];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w]; __syncthreads(); }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+    double v[1] = {0.0};
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) v[0] += a[t] * b[t];
+    block_reduce<DB>(v, RedSum{});
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
-__global__ void k_dot_sum(const double *part, int nb, double *out)
+__global__ void __launch_bounds__(DB) k_dot_sum(const double *part, int nb, double *out)
 {
-    __shared__ double sh[DB];
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w]; __syncthreads(); }
-    if (threadIdx.x == 0) out[0] = sh[0];
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v[0] += part[b];
+    block_reduce<DB>(v, RedSum{});
+    if (threadIdx.x == 0) out[0] = v[0];
 }
 // y = a x + b y
 __global__ void k_axpby(int64_t n, double a, const double *x, double b, double *y)

@@ -77,19 +77,6 @@ void upload(tg_ctx *C, T *dst, const std::vector<T> &src)
     if (!src.empty()) TG_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, C->stream));
 }
 
-__device__ __forceinline__ double block_sum(double v, double *sh)
-{
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
-    }
-    double r = sh[0];
-    __syncthreads();
-    return r;
-}
-
 // trilinear interpolation in TOSCA's form c0 + c1 dC + c2 dE + c3 dZ + c4 dC dE
 // + c5 dE dZ + c6 dZ dC + c7 dC dE dZ (inline.h:7203-7263)
 __device__ __forceinline__ double tri(const double *v, const double d[3], const int *cl)
@@ -118,7 +105,6 @@ __device__ __forceinline__ void point_speed(const Farm &F, V3f<double> u, int p,
 // one block per turbine: disk speed, force scale, thrust and power
 __global__ void __launch_bounds__(FB) k_farm_sample(Farm F, V3f<double> u, double *out, int stride)
 {
-    __shared__ double sh[FB];
     const int t = blockIdx.x;
     double s = 0.0;
     for (int p = F.pt_off[t] + threadIdx.x; p < F.pt_off[t + 1]; p += blockDim.x) {
@@ -126,7 +112,7 @@ __global__ void __launch_bounds__(FB) k_farm_sample(Farm F, V3f<double> u, doubl
         point_speed(F, u, p, ubx, uby, m);
         s += m * F.pt_da[p];
     }
-    s = block_sum(s, sh);
+    s = block_sum_all<FB>(s);
     if (threadIdx.x == 0) {
         const double U = s / F.t_area[t];
         const double sc = 0.5 * U * U * F.t_ct[t];
@@ -214,7 +200,6 @@ __global__ void k_farm_adj_stage(Farm F, Grid g, Metrics m, V3f<double> ra)
 // the adjoint of the disk speed (with the power objective, + dP/dC_T', dP/dU)
 __global__ void __launch_bounds__(FB) k_farm_adj_turbine(Farm F, int objective)
 {
-    __shared__ double sh[FB];
     const int t = blockIdx.x;
     const double ax = F.t_axis[3 * t], ay = F.t_axis[3 * t + 1], az = F.t_axis[3 * t + 2];
     double d = 0.0;
@@ -222,7 +207,7 @@ __global__ void __launch_bounds__(FB) k_farm_adj_turbine(Farm F, int objective)
         const int q = F.te_cov[e];
         d += F.te_g[e] * (ax * F.fsa[3 * q] + ay * F.fsa[3 * q + 1] + az * F.fsa[3 * q + 2]);
     }
-    d = block_sum(d, sh);
+    d = block_sum_all<FB>(d);
     if (threadIdx.x == 0) {
         const double U = F.astate[2 * t], ct = F.t_ct[t];
         double gct = 0.5 * U * U * d, ub = ct * U * d;

@@ -250,6 +250,59 @@ V3f<double> dalloc3(tg_ctx *C, size_t n);
 // NaN-propagating maximum (fmax ignores NaN operands)
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
 
+// per-slot combiners of block_reduce
+struct RedSum { __device__ __forceinline__ double operator()(double a, double b) const { return a + b; } };
+struct RedMax { __device__ __forceinline__ double operator()(double a, double b) const { return fmax(a, b); } };
+struct RedNanMax { __device__ __forceinline__ double operator()(double a, double b) const { return nanmax(a, b); } };
+
+// Block-wide reduction of NV per-thread values for a block of NT threads (NT
+// a power of two, 64..1024): a shuffle tree inside each warp, the warp
+// results through shared memory, a second shuffle tree in warp 0. The
+// combination order is fixed, so the result is deterministic; it is valid in
+// thread 0 only. Every thread of the block must call it.
+template <int NT, int NV, class... Ops>
+__device__ __forceinline__ void block_reduce(double (&v)[NV], Ops... ops)
+{
+    static_assert(NT >= 64 && NT <= 1024 && (NT & (NT - 1)) == 0, "block size");
+    static_assert(sizeof...(Ops) == NV, "one combiner per slot");
+    constexpr int NW = NT / 32;
+    __shared__ double ws[NV][NW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        int q = 0;
+        ((v[q] = ops(v[q], __shfl_down_sync(0xffffffffu, v[q], o)), q++), ...);
+    }
+    if (lane == 0) {
+        #pragma unroll
+        for (int q = 0; q < NV; q++) ws[q][w] = v[q];
+    }
+    __syncthreads();
+    if (w == 0) {
+        #pragma unroll
+        for (int q = 0; q < NV; q++) v[q] = ws[q][lane < NW ? lane : 0];
+        #pragma unroll
+        for (int o = NW / 2; o > 0; o >>= 1) {
+            int q = 0;
+            ((v[q] = ops(v[q], __shfl_down_sync(0xffffffffu, v[q], o)), q++), ...);
+        }
+    }
+}
+
+// block_reduce of one sum, returned to every thread of the block
+template <int NT>
+__device__ __forceinline__ double block_sum_all(double x)
+{
+    __shared__ double out;
+    double v[1] = {x};
+    block_reduce<NT>(v, RedSum{});
+    if (threadIdx.x == 0) out = v[0];
+    __syncthreads();
+    const double r = out;
+    __syncthreads();
+    return r;
+}
+
 // profiling brackets around one kernel launch on C->stream
 void prof_begin(tg_ctx *C, const char *name, cudaEvent_t *a, cudaEvent_t *b, int *slot);
 void prof_end(tg_ctx *C, cudaEvent_t a, cudaEvent_t b, int slot);

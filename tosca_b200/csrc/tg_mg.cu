@@ -597,11 +597,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
         const double *Bp = tl.stage_b ? Bs : B;
         double s = 0.0;
         for (int t = threadIdx.x; t < nc; t += blockDim.x) { dr[t] = (double)L.r[t]; s += dr[t]; }
-        red[threadIdx.x] = s;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-        const double mean = red[0] / nc;
-        __syncthreads();
+        const double mean = block_sum_all<1024>(s) / nc;
         for (int t = threadIdx.x; t < nc; t += blockDim.x) dr[t] -= mean;
         __syncthreads();
         const int g = nc <= (int)blockDim.x ? (int)blockDim.x / nc : 1;
@@ -619,11 +615,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
             dr[t] = acc;
             sx += acc;
         }
-        __syncthreads();
-        red[threadIdx.x] = sx;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) { if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w]; __syncthreads(); }
-        const double mx = red[0] / nc;
+        const double mx = block_sum_all<1024>(sx) / nc;
         for (int t = threadIdx.x; t < nc; t += blockDim.x) L.x[t] = (T)(dr[t] - mx);
         __syncthreads();
     }

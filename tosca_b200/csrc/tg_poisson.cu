@@ -195,48 +195,61 @@ __global__ void k_apply19(PoissonCtx P, const double *__restrict__ x, double *__
 }
 
 // ------------------------------------------------------ vector kernels
+// The vectors are separate cudaMalloc allocations (256-byte aligned), so the
+// grid-stride loops below move two doubles per access (double2, 16-byte
+// loads and stores); an odd last element is taken by thread 0 of block 0
+// after its loop.
+__device__ __forceinline__ const double2 *v2(const double *a) { return reinterpret_cast<const double2 *>(a); }
+__device__ __forceinline__ double2 *v2(double *a) { return reinterpret_cast<double2 *>(a); }
+__device__ __forceinline__ bool odd_tail(int64_t n) { return (n & 1) && blockIdx.x == 0 && threadIdx.x == 0; }
+#define TG_PAIRS(t, n2) for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (n2); t += (int64_t)gridDim.x * blockDim.x)
+
 // partial sums: slot 0 = a.b, slot 1 = sum(a), slot 2 = max |a * w|
-__global__ void k_dot_partial(int64_t n, const double *a, const double *b, const double *w, double *part)
+__device__ __forceinline__ void dot_acc(double av, double bv, double wv, double (&v)[3])
 {
-    __shared__ double s0[RB], s1[RB], s2[RB];
-    double d = 0.0, sa = 0.0, mx = 0.0;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        double av = a[t];
-        d += av * b[t];
-        sa += av;
-        if (w) mx = fmax(mx, fabs(av * w[t]));
+    v[0] += av * bv;
+    v[1] += av;
+    v[2] = fmax(v[2], fabs(av * wv));
+}
+__device__ __forceinline__ void dot_store(double (&v)[3], double *part)
+{
+    block_reduce<RB>(v, RedSum{}, RedSum{}, RedMax{});
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = v[0]; part[3 * blockIdx.x + 1] = v[1]; part[3 * blockIdx.x + 2] = v[2]; }
+}
+__global__ void __launch_bounds__(RB) k_dot_partial(int64_t n, const double *a, const double *b, const double *w, double *part)
+{
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) {
+        const double2 av = v2(a)[t], bv = v2(b)[t];
+        const double2 wv = w ? v2(w)[t] : double2{0.0, 0.0};
+        dot_acc(av.x, bv.x, wv.x, v);
+        dot_acc(av.y, bv.y, wv.y, v);
     }
-    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
-    __syncthreads();
-    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) { part[3 * blockIdx.x] = s0[0]; part[3 * blockIdx.x + 1] = s1[0]; part[3 * blockIdx.x + 2] = s2[0]; }
+    if (odd_tail(n)) dot_acc(a[n - 1], b[n - 1], w ? w[n - 1] : 0.0, v);
+    dot_store(v, part);
 }
 // final: out[0..2] = totals
-__global__ void k_dot_final(const double *part, int nb, double *out)
+__global__ void __launch_bounds__(RB) k_dot_final(const double *part, int nb, double *out)
 {
-    __shared__ double s0[RB], s1[RB], s2[RB];
-    double d = 0.0, sa = 0.0, mx = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) { d += part[3 * b]; sa += part[3 * b + 1]; mx = fmax(mx, part[3 * b + 2]); }
-    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
-    __syncthreads();
-    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; out[2] = s2[0]; }
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) { v[0] += part[3 * b]; v[1] += part[3 * b + 1]; v[2] = fmax(v[2], part[3 * b + 2]); }
+    block_reduce<RB>(v, RedSum{}, RedSum{}, RedMax{});
+    if (threadIdx.x == 0) { out[0] = v[0]; out[1] = v[1]; out[2] = v[2]; }
 }
 
 // y = b - y (residual from y = L x)
 __global__ void k_resid(int64_t n, const double *b, double *y)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) y[t] = b[t] - y[t];
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) { const double2 bv = v2(b)[t], yv = v2(y)[t]; v2(y)[t] = double2{bv.x - yv.x, bv.y - yv.y}; }
+    if (odd_tail(n)) y[n - 1] = b[n - 1] - y[n - 1];
 }
 __global__ void k_copy(int64_t n, const double *a, double *b)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) b[t] = a[t];
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) v2(b)[t] = v2(a)[t];
+    if (odd_tail(n)) b[n - 1] = a[n - 1];
 }
 __global__ void k_zero_at(double *z, int pin) { z[pin] = 0.0; }
 // initial guess of the step's solve from the last three solutions (the
@@ -265,33 +278,36 @@ __global__ void k_negcopy(int64_t n, const double *a, double *b)
 // CG: alpha = rz / pq ; x += alpha p ; r -= alpha q, with the partials of
 // k_dot_partial(r, r, w) formed in the same grid-stride order (same grid), so
 // the totals equal those of a separate update and dot product
-__global__ void k_cg_update_rr(int64_t n, const double *rz, const double *pq, double *x, const double *p, double *r,
-                               const double *q, const double *w, double *part)
+__global__ void __launch_bounds__(RB, 4) k_cg_update_rr(int64_t n, const double *rz, const double *pq, double *x, const double *p,
+                                                     double *r, const double *q, const double *w, double *part)
 {
-    __shared__ double s0[RB], s1[RB], s2[RB];
     const double alpha = rz[0] / pq[0];
-    double d = 0.0, sa = 0.0, mx = 0.0;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        x[t] += alpha * p[t];
-        r[t] -= alpha * q[t];
-        const double av = r[t];
-        d += av * av;
-        sa += av;
-        if (w) mx = fmax(mx, fabs(av * w[t]));
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) {
+        const double2 xv = v2(x)[t], pv = v2(p)[t], rv = v2(r)[t], qv = v2(q)[t];
+        const double2 xn{xv.x + alpha * pv.x, xv.y + alpha * pv.y}, rn{rv.x - alpha * qv.x, rv.y - alpha * qv.y};
+        v2(x)[t] = xn;
+        v2(r)[t] = rn;
+        const double2 wv = w ? v2(w)[t] : double2{0.0, 0.0};
+        dot_acc(rn.x, rn.x, wv.x, v);
+        dot_acc(rn.y, rn.y, wv.y, v);
     }
-    s0[threadIdx.x] = d; s1[threadIdx.x] = sa; s2[threadIdx.x] = mx;
-    __syncthreads();
-    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-        if (threadIdx.x < k) { s0[threadIdx.x] += s0[threadIdx.x + k]; s1[threadIdx.x] += s1[threadIdx.x + k]; s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + k]); }
-        __syncthreads();
+    if (odd_tail(n)) {
+        x[n - 1] += alpha * p[n - 1];
+        r[n - 1] -= alpha * q[n - 1];
+        const double rv = r[n - 1];
+        dot_acc(rv, rv, w ? w[n - 1] : 0.0, v);
     }
-    if (threadIdx.x == 0) { part[3 * blockIdx.x] = s0[0]; part[3 * blockIdx.x + 1] = s1[0]; part[3 * blockIdx.x + 2] = s2[0]; }
+    dot_store(v, part);
 }
 // CG: beta = rz_new / rz_old ; p = z + beta p
 __global__ void k_cg_dir(int64_t n, const double *rznew, const double *rzold, const double *z, double *p)
 {
-    double beta = rznew[0] / rzold[0];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) p[t] = z[t] + beta * p[t];
+    const double beta = rznew[0] / rzold[0];
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) { const double2 zv = v2(z)[t], pv = v2(p)[t]; v2(p)[t] = double2{zv.x + beta * pv.x, zv.y + beta * pv.y}; }
+    if (odd_tail(n)) p[n - 1] = z[n - 1] + beta * p[n - 1];
 }
 __global__ void k_scalar_copy(const double *a, double *b, int n) { for (int t = 0; t < n; t++) b[t] = a[t]; }
 
@@ -363,8 +379,13 @@ __global__ void k_cg_dir_loop(int64_t n, const double *sc, const double *z, doub
 {
     const bool first = sc[51] != 0.0;
     const double beta = first ? 0.0 : sc[6] / sc[14];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-        p[t] = first ? z[t] : z[t] + beta * p[t];
+    const int64_t n2 = n >> 1;
+    TG_PAIRS(t, n2) {
+        const double2 zv = v2(z)[t];
+        if (first) v2(p)[t] = zv;
+        else { const double2 pv = v2(p)[t]; v2(p)[t] = double2{zv.x + beta * pv.x, zv.y + beta * pv.y}; }
+    }
+    if (odd_tail(n)) p[n - 1] = first ? z[n - 1] : z[n - 1] + beta * p[n - 1];
 }
 
 inline dim3 cgrid(int nx, int ny, int nz) { return grid3(nx, ny, nz); }

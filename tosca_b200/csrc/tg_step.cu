@@ -345,9 +345,8 @@ __device__ __forceinline__ void wall_parallel(Grid g, Metrics m, State s, int k,
 
 // per-block partial sums of |U_par|, the wall distance and (coupled) qWall
 // over the j=1 plane
-__global__ void k_wall_plane_sums(Grid g, Metrics m, State s, Params p, double *part)
+__global__ void __launch_bounds__(256) k_wall_plane_sums(Grid g, Metrics m, State s, Params p, double *part)
 {
-    __shared__ double sh[3][256];
     int nI = g.mx - 2, nK = g.mz - 2;
     double su = 0.0, sd = 0.0, sq = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
@@ -359,16 +358,9 @@ __global__ void k_wall_plane_sums(Grid g, Metrics m, State s, Params p, double *
         sd += 0.5 / m.aj[c] / area;
         if (p.wall_coupled) sq += s.qwall[k * g.mx + i];
     }
-    sh[0][threadIdx.x] = su; sh[1][threadIdx.x] = sd; sh[2][threadIdx.x] = sq;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + w]; sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-            sh[2][threadIdx.x] += sh[2][threadIdx.x + w];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) { part[3 * blockIdx.x] = sh[0][0]; part[3 * blockIdx.x + 1] = sh[1][0]; part[3 * blockIdx.x + 2] = sh[2][0]; }
+    double v[3] = {su, sd, sq};
+    block_reduce<256>(v, RedSum{}, RedSum{}, RedSum{});
+    if (threadIdx.x == 0) { part[3 * blockIdx.x] = v[0]; part[3 * blockIdx.x + 1] = v[1]; part[3 * blockIdx.x + 2] = v[2]; }
 }
 
 // final sums (deterministic order) and u* = uStarShumann(<|U_par|>, <s>, qWall)
@@ -1073,9 +1065,8 @@ __global__ void k_gauge(int64_t n, double *p, const double *ref_cell)
 __global__ void k_copy1(const double *src, double *dst) { dst[0] = src[0]; }
 
 // ContinuityErrorsOptimized (peqn.c:4114-4181): max |div(V)| * aj, block partials
-__global__ void k_div_partial(Grid g, Metrics m, State s, double *part)
+__global__ void __launch_bounds__(256) k_div_partial(Grid g, Metrics m, State s, double *part)
 {
-    __shared__ double sh[256];
     int nI = g.mx - 2, nJ = g.my - 2, nK = g.mz - 2;
     int64_t n = (int64_t)nI * nJ * nK;
     double mm = 0.0;
@@ -1086,26 +1077,16 @@ __global__ void k_div_partial(Grid g, Metrics m, State s, double *part)
                         + s.ucont.z[c] - s.ucont.z[c - g.mx * g.my]) * m.aj[c]);
         mm = nanmax(mm, d);
     }
-    sh[threadIdx.x] = mm;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] = nanmax(sh[threadIdx.x], sh[threadIdx.x + w]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+    double v[1] = {mm};
+    block_reduce<256>(v, RedNanMax{});
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
-__global__ void k_max_final(const double *part, int nb, double *out)
+__global__ void __launch_bounds__(256) k_max_final(const double *part, int nb, double *out)
 {
-    __shared__ double sh[256];
-    double mm = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) mm = nanmax(mm, part[b]);
-    sh[threadIdx.x] = mm;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] = nanmax(sh[threadIdx.x], sh[threadIdx.x + w]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) out[0] = sh[0];
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v[0] = nanmax(v[0], part[b]);
+    block_reduce<256>(v, RedNanMax{});
+    if (threadIdx.x == 0) out[0] = v[0];
 }
 
 // initial face fluxes from the cell-centre velocity (initialField.c:1140-1190)

@@ -407,9 +407,8 @@ __global__ void k_twall_local(Grid g, Metrics m, State s, Params p, const double
 
 // -3 averaged, pass 1: surfaceTheta += heatingRate dt and per-block partial
 // sums of T(j=1) - surfaceTheta, |U_par| and the wall distance
-__global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part, const double *sts)
+__global__ void __launch_bounds__(256) k_twall_sums(Grid g, Metrics m, State s, Params p, double *part, const double *sts)
 {
-    __shared__ double sh[3][256];
     const int nI = g.mx - 2, nK = g.mz - 2;
     double sT = 0.0, sU = 0.0, sD = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nI * nK; t += gridDim.x * blockDim.x) {
@@ -423,15 +422,10 @@ __global__ void k_twall_sums(Grid g, Metrics m, State s, Params p, double *part,
         sU += upm;
         sD += dist;
     }
-    sh[0][threadIdx.x] = sT; sh[1][threadIdx.x] = sU; sh[2][threadIdx.x] = sD;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-        if (threadIdx.x < h)
-            for (int q = 0; q < 3; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + h];
-        __syncthreads();
-    }
+    double v[3] = {sT, sU, sD};
+    block_reduce<256>(v, RedSum{}, RedSum{}, RedSum{});
     if (threadIdx.x == 0)
-        for (int q = 0; q < 3; q++) part[3 * blockIdx.x + q] = sh[q][0];
+        for (int q = 0; q < 3; q++) part[3 * blockIdx.x + q] = v[q];
 }
 
 // -3 averaged, pass 2 (one block): the plane means in a fixed order,
