@@ -623,9 +623,10 @@ __global__ void __launch_bounds__(FBN, FMINB) k_face_fluxes(Grid g, FaceMet<M> m
     const int mx = g.mx, my = g.my, mz = g.mz;
     const int i0 = 1 + blockIdx.x * FBX, j0 = 1 + blockIdx.y * FBY, k0 = 1 + blockIdx.z * FBZ;
     const bool les = p.les;
-    for (int q = (threadIdx.z * FBY + threadIdx.y) * FBX + threadIdx.x; q < FTN; q += FBN) {
-        const int tx = q % FTX, ty = (q / FTX) % FTY, tz = q / (FTX * FTY);
-        const int gi = g.wi(i0 - 1 + tx), gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz);
+    // staging: tile point (tx, ty, tz) <- DMDA (i0-1+tx, j0-1+ty, k0-1+tz),
+    // wrapped; 0 outside a non-periodic extent
+    auto stage = [&](int tx, int ty, int tz, int gi) {
+        const int gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz), q = (tz * FTY + ty) * FTX + tx;
         double ux = 0.0, uy = 0.0, uz = 0.0, nt = 0.0;
         if (gi >= 0 && gi < mx && gj >= 0 && gj < my && gk >= 0 && gk < mz) {
             const int c = (gk * my + gj) * mx + gi;
@@ -633,6 +634,20 @@ __global__ void __launch_bounds__(FBN, FMINB) k_face_fluxes(Grid g, FaceMet<M> m
             if (mode != 1 && les) nt = s.nut[c];
         }
         su[0][q] = ux; su[1][q] = uy; su[2][q] = uz; sn[q] = nt;
+    };
+    {
+        // each warp stages whole tile rows (its lane is tx, the row index is
+        // warp-uniform), then every thread at most one of the 3 x FTY x FTZ
+        // points of the last three columns
+        static_assert(FBX == 32 && FBN % 32 == 0 && 3 * FTY * FTZ <= FBN, "one warp per tile row, one pass for the last columns");
+        const int lane = threadIdx.x, wid = threadIdx.z * FBY + threadIdx.y;
+        const int gi = g.wi(i0 - 1 + lane);
+        for (int r = wid; r < FTY * FTZ; r += FBN / 32) stage(lane, r % FTY, r / FTY, gi);
+        const int q = wid * 32 + lane;
+        if (q < 3 * FTY * FTZ) {
+            const int r = q / 3, tx = FBX + (q - 3 * r);
+            stage(tx, r % FTY, r / FTY, g.wi(i0 - 1 + tx));
+        }
     }
     __syncthreads();
     const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0 + threadIdx.z;

@@ -97,9 +97,10 @@ __global__ void __launch_bounds__(TBN) k_t_face_fluxes(Grid g, Metrics m, State 
     __shared__ double sn[TTN];
     const int mx = g.mx, my = g.my, mz = g.mz;
     const int i0 = 1 + blockIdx.x * TBX, j0 = 1 + blockIdx.y * TBY, k0 = 1 + blockIdx.z * TBZ;
-    for (int q = (threadIdx.z * TBY + threadIdx.y) * TBX + threadIdx.x; q < TTN; q += TBN) {
-        const int tx = q % TTX, ty = (q / TTX) % TTY, tz = q / (TTX * TTY);
-        const int gi = g.wi(i0 - 1 + tx), gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz);
+    // staging: tile point (tx, ty, tz) <- DMDA (i0-1+tx, j0-1+ty, k0-1+tz),
+    // wrapped; 0 outside a non-periodic extent
+    auto stage = [&](int tx, int ty, int tz, int gi) {
+        const int gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz), q = (tz * TTY + ty) * TTX + tx;
         double tv = 0.0, nv = 0.0;
         if (gi >= 0 && gi < mx && gj >= 0 && gj < my && gk >= 0 && gk < mz) {
             const int c = (gk * my + gj) * mx + gi;
@@ -107,6 +108,19 @@ __global__ void __launch_bounds__(TBN) k_t_face_fluxes(Grid g, Metrics m, State 
             if (p.les) nv = s.nut[c];
         }
         st[q] = tv; sn[q] = nv;
+    };
+    {
+        // each warp stages whole tile rows (lane = tx, warp-uniform row), then
+        // every thread at most one point of the last three columns
+        static_assert(TBX == 32 && TBN % 32 == 0 && 3 * TTY * TTZ <= TBN, "one warp per tile row, one pass for the last columns");
+        const int lane = threadIdx.x, wid = threadIdx.z * TBY + threadIdx.y;
+        const int gi = g.wi(i0 - 1 + lane);
+        for (int r = wid; r < TTY * TTZ; r += TBN / 32) stage(lane, r % TTY, r / TTY, gi);
+        const int q = wid * 32 + lane;
+        if (q < 3 * TTY * TTZ) {
+            const int r = q / 3, tx = TBX + (q - 3 * r);
+            stage(tx, r % TTY, r / TTY, g.wi(i0 - 1 + tx));
+        }
     }
     __syncthreads();
     const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0 + threadIdx.z;
