@@ -196,7 +196,11 @@ __device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i)
 // same-colour lines (flattened over (k, t)), warp w -> j in [w*CJ, (w+1)*CJ).
 // dp_j = (rhs_j + aS_j dp_{j-1}) / m_j and x_j = dp_j - c'_j x_{j+1} are first
 // order affine recurrences: each warp composes its chunk into (offset,
-// multiplier) pairs, warp 0 chains the chunk ends, each warp finishes its chunk.
+// multiplier) pairs, the chunk ends of a line are chained by a shuffle scan of
+// those affine maps (warp w scans line w over the 32 chunks, one per lane),
+// and each warp finishes its chunk. The chunk-end arrays are padded to a row
+// stride of 33 so that both the per-chunk writes and the per-line scan reads
+// are free of bank conflicts.
 // The loads of a chunk do not depend on each other, so they are issued in an
 // unrolled pass of compile-time length CJ before the recurrence runs on
 // shared memory.
@@ -206,9 +210,9 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
     extern __shared__ unsigned char smraw[];
     T *D = reinterpret_cast<T *>(smraw);            // [NW*CJ][32] offsets
     T *Mu = D + LINE_NW * CJ * 32;                  // [NW*CJ][32] multipliers
-    T *SD = Mu + LINE_NW * CJ * 32;                 // [NW][32] chunk offsets
-    T *SM = SD + LINE_NW * 32;                      // [NW][32] chunk multipliers
-    T *ST = SM + LINE_NW * 32;                      // [NW][32] chunk boundary values
+    T *SD = Mu + LINE_NW * CJ * 32;                 // [NW][33] chunk offsets
+    T *SM = SD + LINE_NW * 33;                      // [NW][33] chunk multipliers
+    T *ST = SM + LINE_NW * 33;                      // [NW][33] chunk boundary values
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int half = L.nx >> 1;
     const int lid = blockIdx.x * 32 + lane;
@@ -246,16 +250,24 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
             Mu[q] = ml;
         }
     }
-    SD[w * 32 + lane] = dl;
-    SM[w * 32 + lane] = ml;
+    static_assert(LINE_NW == 32, "one lane per chunk in the chunk-end scans");
+    SD[w * 33 + lane] = dl;
+    SM[w * 33 + lane] = ml;
     __syncthreads();
-    if (w == 0) {
-        T s = T(0);
+    {
+        // warp w, lane q: chunk q of line w; inclusive scan of s -> B + A s
+        // over the chunks, then shifted by one (the value entering chunk q)
+        T A = SM[lane * 33 + w], B = SD[lane * 33 + w];
         #pragma unroll
-        for (int q = 0; q < LINE_NW; q++) { ST[q * 32 + lane] = s; s = SD[q * 32 + lane] + SM[q * 32 + lane] * s; }
+        for (int d = 1; d < 32; d <<= 1) {
+            const T Ap = __shfl_up_sync(0xffffffffu, A, d), Bp = __shfl_up_sync(0xffffffffu, B, d);
+            if (lane >= d) { B = A * Bp + B; A = A * Ap; }
+        }
+        const T in = __shfl_up_sync(0xffffffffu, B, 1);
+        ST[lane * 33 + w] = lane == 0 ? T(0) : in;
     }
     __syncthreads();
-    const T st = ST[w * 32 + lane];
+    const T st = ST[w * 33 + lane];
     // (3) backward recurrence of the chunk; c' loaded before the chain
     T cpv[CJ];
     if (active) {
@@ -275,17 +287,22 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
             Mu[q] = nl;
         }
     }
+    SD[w * 33 + lane] = xl;
+    SM[w * 33 + lane] = nl;
     __syncthreads();
-    SD[w * 32 + lane] = xl;
-    SM[w * 32 + lane] = nl;
-    __syncthreads();
-    if (w == 0) {
-        T xn = T(0);
+    {
+        // backward: inclusive scan from the last chunk down, shifted by one
+        T C = SM[lane * 33 + w], E = SD[lane * 33 + w];
         #pragma unroll
-        for (int q = LINE_NW - 1; q >= 0; q--) { ST[q * 32 + lane] = xn; xn = SD[q * 32 + lane] + SM[q * 32 + lane] * xn; }
+        for (int d = 1; d < 32; d <<= 1) {
+            const T Cn = __shfl_down_sync(0xffffffffu, C, d), En = __shfl_down_sync(0xffffffffu, E, d);
+            if (lane + d < 32) { E = C * En + E; C = C * Cn; }
+        }
+        const T in = __shfl_down_sync(0xffffffffu, E, 1);
+        ST[lane * 33 + w] = lane == 31 ? T(0) : in;
     }
     __syncthreads();
-    const T xnext = ST[w * 32 + lane];
+    const T xnext = ST[w * 33 + lane];
     if (active) {
         const int c0 = sidx(L, k, j0, i);
         #pragma unroll
@@ -298,7 +315,7 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
 }
 
 template <class T>
-size_t line_chunk_smem_cj(int cj) { return sizeof(T) * (2 * (size_t)LINE_NW * cj * 32 + 3 * LINE_NW * 32); }
+size_t line_chunk_smem_cj(int cj) { return sizeof(T) * (2 * (size_t)LINE_NW * cj * 32 + 3 * LINE_NW * 33); }
 
 // chunk length (power of two >= ceil(ny / NW)) of the line solver; 0 if the
 // lines are too long for its shared memory
