@@ -404,12 +404,36 @@ __device__ __forceinline__ void restrict_cell(const Lvl<T> &F, const Lvl<T> &Cc,
     Cc.x[cc] = T(0);
 }
 
+// Grid restriction: a block takes 32 consecutive coarse cells of one coarse
+// row (J, K) and one thread per fine cell under them (up to 64 x 2 x 2), so
+// the loads of all fine residuals issue at once; the residuals meet in shared
+// memory and thread I of the block sums its coarse cell in the k, j, i order
+// of restrict_cell (the same sum).
+constexpr int RS_I = 32;    // coarse cells per block
 template <class T>
-__global__ void k_restrict(Lvl<T> F, Lvl<T> Cc)
+__global__ void __launch_bounds__(8 * RS_I) k_restrict(Lvl<T> F, Lvl<T> Cc)
 {
-    int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y, K = blockIdx.z * blockDim.z + threadIdx.z;
-    if (I >= Cc.nx || J >= Cc.ny || K >= Cc.nz) return;
-    restrict_cell(F, Cc, I, J, K);
+    __shared__ T res[2][2][2 * RS_I];
+    const int t = threadIdx.x, fo = t & (2 * RS_I - 1), dj = (t >> 6) & 1, dk = t >> 7;
+    const int I0 = blockIdx.x * RS_I, J = blockIdx.y, K = blockIdx.z;
+    const int i = F.cx * I0 + fo, j = F.cy * J + dj, k = F.cz * K + dk;
+    T v = T(0);
+    if (fo < F.cx * RS_I && dj < F.cy && dk < F.cz && i < F.nx && j < F.ny && k < F.nz) {
+        const int c = sidx(F, k, j, i);
+        v = F.r[c] - F.diag[c] * F.x[c] + nb_sum(F, k, j, i, c, true);
+    }
+    res[dk][dj][fo] = v;
+    __syncthreads();
+    const int I = I0 + t;
+    if (t < RS_I && I < Cc.nx) {
+        T sum = T(0);
+        const int i1 = min(F.cx * I + F.cx, F.nx) - F.cx * I0, j1 = min(F.cy * J + F.cy, F.ny) - F.cy * J,
+                  k1 = min(F.cz * K + F.cz, F.nz) - F.cz * K;
+        for (int a = 0; a < k1; a++) for (int b = 0; b < j1; b++) for (int q = F.cx * t; q < i1; q++) sum += res[a][b][q];
+        const int cc = sidx(Cc, K, J, I);
+        Cc.r[cc] = sum;
+        Cc.x[cc] = T(0);
+    }
 }
 
 template <class T>
@@ -701,7 +725,7 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
     };
     for (int s = 0; s < mg->nu; s++) { smooth(0); smooth(1); }
     Lvl<T> &Cc = L[l + 1];
-    TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict<T><<<g3(Cc.nx, Cc.ny, Cc.nz), block3(), 0, st>>>(F, Cc));
+    TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict<T><<<dim3((Cc.nx + RS_I - 1) / RS_I, Cc.ny, Cc.nz), 8 * RS_I, 0, st>>>(F, Cc));
     vcycle(C, mg, L, l + 1);
     TG_PROF(C, fine ? "mg_prolong_L0" : "mg_prolong_coarse", k_prolong<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, Cc));
     for (int s = 0; s < mg->nu; s++) { smooth(1); smooth(0); }
