@@ -3,15 +3,16 @@
 //
 //  * coarsening: every direction with >= 3 cells is halved (n -> ceil(n/2):
 //    fine cells 2I and 2I+1 form coarse cell I; the last coarse cell of an
-//    odd direction holds one fine cell) until a level has <= 64 cells, so
+//    odd direction holds one fine cell) until a level has <= 1024 cells, so
 //    every grid size coarsens; coarse face coefficients are face sums of the
 //    fine ones, halved when the face-normal direction is coarsened
 //  * transfers: summed residual restriction, piecewise-constant prolongation
 //  * smoothing: zebra j-line Gauss-Seidel when j (the wall-normal direction)
 //    is non-periodic, red-black point Gauss-Seidel otherwise; 2 pre + 2 post
 //    sweeps in reversed colour order, so the cycle is a symmetric operator
-//  * coarsest level: dense (A + 11^T/n)^-1, i.e. the pseudo-inverse on
-//    mean-free vectors
+//  * coarsest level (<= 1024 cells): the pseudo-inverse on mean-free vectors,
+//    (I - 11^T/n) (A + 11^T/n)^-1 (I - 11^T/n), formed densely at set-up and
+//    applied as one matrix-vector product (a warp per row)
 //
 // Layout: on every level the cells of an (k, j) row are stored with even i
 // first and odd i second. The cells of one zebra colour in a k-row then form
@@ -20,17 +21,14 @@
 //
 // The tridiagonal line matrices never change, so their LU factors (c' and
 // 1/m of the Thomas algorithm) are computed once at setup and a line solve is
-// a chain of FMAs. A block solves 32 same-colour lines at once: each of its
-// warps takes one chunk of j, runs the forward and backward recurrences of
-// its chunk as affine maps (coalesced loads, all warps in flight), and the
-// chunk ends are combined in shared memory. The smallest levels (<= 1024
-// cells each) run as one single-block kernel that stages their coefficients,
-// unknowns and the dense coarsest inverse in shared memory and performs all
-// their sweeps, transfers and the coarsest solve there. One block is issue-
-// and latency-bound, so larger levels run as grid launches (cheap inside the
-// step graph): at 4096 cells the single-block version took 80-130 us; taking
-// the 1024-cell level into it saves 2 % of a 128 x 64 x 64 ABL step (1.383
-// -> 1.356 ms) and nothing measurable at 256 x 256 x 128, 2048 no more.
+// a chain of FMAs. On the large levels a block solves 32 same-colour lines at
+// once: each of its warps takes one chunk of j, runs the forward and backward
+// recurrences of its chunk as affine maps (coalesced loads, all warps in
+// flight), and the chunk ends are combined by shuffle scans. The small levels
+// use one warp segment per line (k_line_warp). An earlier design ran the
+// levels of <= 1024 cells, smoothing included, in one single-block kernel:
+// 71-73 us per V-cycle at 128 x 64 x 64, one SM's latency chain; the dense
+// solve at the first level of <= 1024 cells replaces it.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -51,30 +49,22 @@ struct Lvl {
 };
 
 constexpr int MAXL = 16;
-constexpr int TAIL_CELLS = 1024;
-constexpr int COARSEST_CELLS = 64;
-constexpr int TAIL_SMEM = 220 * 1024;   // dynamic shared memory of the single-block tail
+constexpr int COARSEST_CELLS = 1024;   // coarsening stops at the first level this small
 constexpr int LINE_NW = 32;         // warps per block of the chunked line solver (one line chunk each)
-
-template <class T>
-struct Tail {
-    Lvl<T> L[MAXL];
-    int nl;
-    int line;
-    int nu;
-    int stage_b;             // the dense coarsest inverse is staged in shared memory
-};
 
 struct MG {
     bool fp32;
-    int nlev, tail_start, line, nu;
+    int nlev, line, nu;
     Lvl<double> Ld[MAXL];
     Lvl<float> Lf[MAXL];
-    double *B;               // dense coarsest inverse (double)
+    double *Bd;              // projected dense pseudo-inverse of the coarsest level (FP64 multigrid)
+    float *Bf;               // the same in FP32 (mixed-precision multigrid)
     int nc;
-    size_t tail_shm;         // dynamic shared memory of the tail kernel
-    int stage_b;
 };
+
+template <class T> inline const T *mg_dense(const MG *mg);
+template <> inline const double *mg_dense<double>(const MG *mg) { return mg->Bd; }
+template <> inline const float *mg_dense<float>(const MG *mg) { return mg->Bf; }
 
 int mg_levels(const MG *mg) { return mg->nlev; }
 
@@ -349,7 +339,7 @@ void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
 // a line is a segment of P lanes (P a power of two, P CJ >= ny), each lane
 // CJ consecutive cells held in registers; the forward and backward Thomas
 // recurrences are composed per lane into affine maps and chained across the
-// segment by shuffle scans, as in the single-block tail. No block barrier and
+// segment by shuffle scans. No block barrier and
 // no scratch array: on the small levels a launch costs about one round of
 // loads plus the two scans.
 template <class T, int CJ>
@@ -481,25 +471,11 @@ __global__ void k_smooth_rb(Lvl<T> L, int color)
 }
 
 // ------------------------------------------------------------------ transfers
-template <class T>
-__device__ __forceinline__ void restrict_cell(const Lvl<T> &F, const Lvl<T> &Cc, int I, int J, int K)
-{
-    T sum = T(0);
-    const int i1 = min(F.cx * I + F.cx, F.nx), j1 = min(F.cy * J + F.cy, F.ny), k1 = min(F.cz * K + F.cz, F.nz);
-    for (int k = F.cz * K; k < k1; k++) for (int j = F.cy * J; j < j1; j++) for (int i = F.cx * I; i < i1; i++) {
-        int c = sidx(F, k, j, i);
-        sum += F.r[c] - F.diag[c] * F.x[c] + nb_sum(F, k, j, i, c, true);
-    }
-    int cc = sidx(Cc, K, J, I);
-    Cc.r[cc] = sum;
-    Cc.x[cc] = T(0);
-}
-
 // Grid restriction: a block takes 32 consecutive coarse cells of one coarse
 // row (J, K) and one thread per fine cell under them (up to 64 x 2 x 2), so
 // the loads of all fine residuals issue at once; the residuals meet in shared
-// memory and thread I of the block sums its coarse cell in the k, j, i order
-// of restrict_cell (the same sum).
+// memory and thread I of the block sums its coarse cell's fine residuals
+// r - diag x + (off-diagonal terms) in k, j, i order.
 constexpr int RS_I = 32;    // coarse cells per block
 template <class T>
 __global__ void __launch_bounds__(8 * RS_I) k_restrict(Lvl<T> F, Lvl<T> Cc)
@@ -535,237 +511,24 @@ __global__ void k_prolong(Lvl<T> F, Lvl<T> Cc)
     F.x[sidx(F, k, j, i)] += Cc.x[sidx(Cc, k / F.cz, j / F.cy, i / F.cx)];
 }
 
-// -------------------------------------------------------- single-block tail
-// The tail runs every sweep of a level on one block, so its cost is the
-// instruction latency of the block's active warps. Rows (k, j) are spread over
-// the warps and the cells of a row over the lanes (one index division per
-// row, none per cell); a j-line is solved by a segment of P lanes (P a power
-// of two, P >= min(ny, 32)), each lane a chunk of consecutive cells: the
-// forward and backward Thomas recurrences are first-order affine maps, which
-// the segment composes with a shuffle scan.
-
-// red-black point Gauss-Seidel sweep of one colour: thread -> (row, m), the
-// m-th cell of the colour in the row
+// ------------------------------------------------------- coarsest level
+// x = Bp r with Bp = (I - 11^T/n) (A + 11^T/n)^-1 (I - 11^T/n): the
+// pseudo-inverse of the singular coarsest operator applied to the mean-free
+// part of r, returned mean-free (the two projections are folded into Bp at
+// set-up). One warp per row, FP64 accumulation; Bp is symmetric.
 template <class T>
-__device__ void blk_smooth_points(const Lvl<T> &L, int color)
+__global__ void __launch_bounds__(256) k_coarse_dense(const T *Bp, Lvl<T> L)
 {
-    const int half = (L.nx + 1) >> 1, n = half * L.ny * L.nz;
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        const int r = t / half, m = t - r * half;
-        const int k = r / L.ny, j = r - k * L.ny;
-        const int p = (color ^ j ^ k) & 1;                     // parity of i for this colour
-        if (m < (p ? (L.nx >> 1) : half)) point_update(L, k, j, 2 * m + p);
-    }
+    const int n = (int)L.n, row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;   // row is uniform over the warp
+    const T *b = Bp + (size_t)row * n;
+    double acc = 0.0;
+    for (int u = lane; u < n; u += 32) acc += (double)b[u] * (double)L.r[u];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) L.x[row] = (T)acc;
 }
 
-// zebra j-line sweep of one colour (lines at i of parity colour ^ k)
-template <class T>
-__device__ void blk_smooth_lines(const Lvl<T> &L, int color)
-{
-    const int ny = L.ny, nx = L.nx;
-    int P = 1;
-    while (P < ny && P < 32) P <<= 1;
-    const int cj = (ny + P - 1) / P;
-    const int lane = threadIdx.x & 31, sl = lane & (P - 1);
-    const int segs = (int)blockDim.x / P;
-    const int myseg = (int)threadIdx.x / P;
-    const int rowcnt = (nx + 1) >> 1;
-    const int nlines = rowcnt * L.nz;
-    const int j0 = sl * cj, j1 = min(j0 + cj, ny);
-    for (int b0 = 0; b0 < nlines; b0 += segs) {               // uniform over the block
-        const int t = b0 + myseg;
-        bool on = false;
-        int k = 0, i = 0;
-        if (t < nlines) {
-            k = t / rowcnt;
-            const int tt = t - k * rowcnt, q = (color ^ k) & 1;
-            const int cnt = q ? (nx >> 1) : rowcnt;
-            if (tt < cnt) { on = true; i = 2 * tt + q; }
-        }
-        const int c0 = on ? sidx(L, k, 0, i) : 0;
-        // forward: dp_j = minv_j aS_j dp_{j-1} + minv_j rhs_j; b_j kept in tmp
-        T A = T(1), B = T(0);
-        if (on)
-            for (int j = j0; j < j1; j++) {
-                const int c = c0 + j * nx;
-                const T mi = L.minv[c];
-                const T a = j > 0 ? mi * L.aN[c - nx] : T(0);
-                const T b = mi * (L.r[c] + nb_sum(L, k, j, i, c, false));
-                L.tmp[c] = b;
-                B = a * B + b;
-                A = a * A;
-            }
-        for (int d = 1; d < P; d <<= 1) {
-            const T Ap = __shfl_up_sync(0xffffffffu, A, d, P), Bp = __shfl_up_sync(0xffffffffu, B, d, P);
-            if (sl >= d) { B = A * Bp + B; A = A * Ap; }
-        }
-        T dp = __shfl_up_sync(0xffffffffu, B, 1, P);
-        if (sl == 0) dp = T(0);
-        if (on)
-            for (int j = j0; j < j1; j++) {
-                const int c = c0 + j * nx;
-                const T a = j > 0 ? L.minv[c] * L.aN[c - nx] : T(0);
-                dp = a * dp + L.tmp[c];
-                L.tmp[c] = dp;
-            }
-        // backward: x_j = -cp_j x_{j+1} + dp_j, composed from the top
-        T Cm = T(1), D = T(0);
-        if (on)
-            for (int j = j1 - 1; j >= j0; j--) {
-                const int c = c0 + j * nx;
-                const T cc = -L.cp[c];
-                D = cc * D + L.tmp[c];
-                Cm = cc * Cm;
-            }
-        for (int d = 1; d < P; d <<= 1) {
-            const T Cn = __shfl_down_sync(0xffffffffu, Cm, d, P), Dn = __shfl_down_sync(0xffffffffu, D, d, P);
-            if (sl + d < P) { D = Cm * Dn + D; Cm = Cm * Cn; }
-        }
-        T xv = __shfl_down_sync(0xffffffffu, D, 1, P);
-        if (sl == P - 1) xv = T(0);
-        if (on)
-            for (int j = j1 - 1; j >= j0; j--) {
-                const int c = c0 + j * nx;
-                xv = L.tmp[c] - L.cp[c] * xv;
-                L.x[c] = xv;
-            }
-    }
-}
-
-template <class T>
-__device__ __forceinline__ void blk_smooth(const Lvl<T> &L, int color, bool line)
-{
-    if (line) blk_smooth_lines(L, color);
-    else blk_smooth_points(L, color);
-}
-
-// restriction to every coarse cell (rows over warps, cells over lanes)
-template <class T>
-__device__ void blk_restrict(const Lvl<T> &F, const Lvl<T> &Cc)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r = warp; r < Cc.ny * Cc.nz; r += nw) {
-        const int K = r / Cc.ny, J = r - K * Cc.ny;
-        for (int I = lane; I < Cc.nx; I += 32) restrict_cell(F, Cc, I, J, K);
-    }
-}
-
-// x_fine += x_coarse (piecewise constant)
-template <class T>
-__device__ void blk_prolong(const Lvl<T> &F, const Lvl<T> &Cc)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int r = warp; r < F.ny * F.nz; r += nw) {
-        const int k = r / F.ny, j = r - k * F.ny;
-        const int crow = ((k / F.cz) * Cc.ny + j / F.cy) * Cc.nx;
-        for (int i = lane; i < F.nx; i += 32)
-            F.x[(k * F.ny + j) * F.nx + spos(i, F.h0)] += Cc.x[crow + spos(i / F.cx, Cc.h0)];
-    }
-}
-
-// bytes of shared memory a tail level occupies: coefficients, Thomas factors,
-// line scratch, x and r; the coarsest level holds x and r only
-template <class T>
-__host__ __device__ inline size_t tail_level_bytes(int64_t n, bool coarsest) { return sizeof(T) * (size_t)n * (coarsest ? 2 : 9); }
-// dense-solve scratch ahead of the levels: B (when staged), r, partial sums
-// and reduction (max(1024, nc))
-__host__ __device__ inline int tail_part(int nc) { return nc > 1024 ? nc : 1024; }
-inline size_t tail_dense_bytes(int nc, bool stage_b)
-{
-    return sizeof(double) * ((stage_b ? (size_t)nc * nc : 0) + (size_t)nc + (size_t)tail_part(nc));
-}
-
-template <class T>
-__global__ void __launch_bounds__(1024, 1) k_tail(Tail<T> tl, const double *B)
-{
-    extern __shared__ __align__(16) double sh[];
-    __shared__ Lvl<T> S[MAXL];
-    const int nl = tl.nl;
-    const int nc = (int)tl.L[nl - 1].n;
-    double *Bs = sh;
-    double *dr = sh + (tl.stage_b ? (size_t)nc * nc : 0), *red = dr + nc;
-    T *base = (T *)(red + tail_part(nc));
-    if (threadIdx.x == 0) {
-        T *q = base;
-        for (int l = 0; l < nl; l++) {
-            Lvl<T> v = tl.L[l];
-            const int64_t n = v.n;
-            if (l + 1 < nl) {
-                v.aE = q; q += n; v.aN = q; q += n; v.aT = q; q += n; v.diag = q; q += n;
-                v.cp = q; q += n; v.minv = q; q += n; v.tmp = q; q += n;
-            }
-            v.x = q; q += n; v.r = q; q += n;
-            S[l] = v;
-        }
-    }
-    __syncthreads();
-    // stage the coefficients of the smoothed levels, the inverse, r and x of the first level
-    for (int l = 0; l + 1 < nl; l++) {
-        const Lvl<T> &G = tl.L[l];
-        const Lvl<T> &V = S[l];
-        for (int t = threadIdx.x; t < V.n; t += blockDim.x) {
-            V.aE[t] = G.aE[t]; V.aN[t] = G.aN[t]; V.aT[t] = G.aT[t];
-            V.diag[t] = G.diag[t]; V.cp[t] = G.cp[t]; V.minv[t] = G.minv[t];
-        }
-    }
-    if (tl.stage_b)
-        for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) Bs[t] = B[t];
-    for (int t = threadIdx.x; t < S[0].n; t += blockDim.x) { S[0].r[t] = tl.L[0].r[t]; S[0].x[t] = tl.L[0].x[t]; }
-    __syncthreads();
-    // descend
-    for (int l = 0; l < nl - 1; l++) {
-        const Lvl<T> &L = S[l];
-        for (int s = 0; s < tl.nu; s++) {
-            blk_smooth(L, 0, tl.line != 0); __syncthreads();
-            blk_smooth(L, 1, tl.line != 0); __syncthreads();
-        }
-        blk_restrict(L, S[l + 1]);
-        __syncthreads();
-    }
-    // coarsest: x = B (r - mean r), then remove the mean of x; each entry of
-    // B r is split over g = blockDim / nc threads
-    {
-        const Lvl<T> &L = S[nl - 1];
-        const double *Bp = tl.stage_b ? Bs : B;
-        double s = 0.0;
-        for (int t = threadIdx.x; t < nc; t += blockDim.x) { dr[t] = (double)L.r[t]; s += dr[t]; }
-        const double mean = block_sum_all<1024>(s) / nc;
-        for (int t = threadIdx.x; t < nc; t += blockDim.x) dr[t] -= mean;
-        __syncthreads();
-        const int g = nc <= (int)blockDim.x ? (int)blockDim.x / nc : 1;
-        for (int q = threadIdx.x; q < nc * g; q += blockDim.x) {
-            const int t = q % nc, h = q / nc;
-            double acc = 0.0;
-            for (int u = h; u < nc; u += g) acc += Bp[(size_t)u * nc + t] * dr[u];   // B symmetric: column t
-            red[q] = acc;                                        // nc * g <= tail_part(nc)
-        }
-        __syncthreads();
-        double sx = 0.0;
-        for (int t = threadIdx.x; t < nc; t += blockDim.x) {
-            double acc = 0.0;
-            for (int h = 0; h < g; h++) acc += red[h * nc + t];
-            dr[t] = acc;
-            sx += acc;
-        }
-        const double mx = block_sum_all<1024>(sx) / nc;
-        for (int t = threadIdx.x; t < nc; t += blockDim.x) L.x[t] = (T)(dr[t] - mx);
-        __syncthreads();
-    }
-    // ascend
-    for (int l = nl - 2; l >= 0; l--) {
-        const Lvl<T> &L = S[l];
-        blk_prolong(L, S[l + 1]);
-        __syncthreads();
-        for (int s = 0; s < tl.nu; s++) {
-            blk_smooth(L, 1, tl.line != 0); __syncthreads();
-            blk_smooth(L, 0, tl.line != 0); __syncthreads();
-        }
-    }
-    for (int t = threadIdx.x; t < S[0].n; t += blockDim.x) tl.L[0].x[t] = S[0].x[t];
-}
-
-// --------------------------------------------------------- level-0 in/out
-// L0.r <- r (natural order, FP64) with the pinned entry replaced by -sum(r); L0.x <- 0
 template <class T>
 __global__ void k_in(const double *r, const double *d_sum, Lvl<T> L)
 {
@@ -792,12 +555,8 @@ template <class T>
 void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
 {
     cudaStream_t st = C->stream;
-    if (l == mg->tail_start) {
-        Tail<T> tl{};
-        tl.nl = mg->nlev - l;
-        for (int q = 0; q < tl.nl; q++) tl.L[q] = L[l + q];
-        tl.line = mg->line; tl.nu = mg->nu; tl.stage_b = mg->stage_b;
-        TG_PROF(C, "mg_tail", k_tail<T><<<1, 1024, mg->tail_shm, st>>>(tl, mg->B));
+    if (l == mg->nlev - 1) {
+        TG_PROF(C, "mg_coarse_dense", k_coarse_dense<T><<<(int)((L[l].n * 32 + 255) / 256), 256, 0, st>>>(mg_dense<T>(mg), L[l]));
         return;
     }
     Lvl<T> &F = L[l];
@@ -827,24 +586,46 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
 // split-layout index on the host
 inline int hsidx(int nx, int ny, int h0, int k, int j, int i) { return (k * ny + j) * nx + ((i & 1) ? (h0 + (i >> 1)) : (i >> 1)); }
 
-bool dense_inverse(std::vector<double> &A, int n, std::vector<double> &inv)
+// inverse of the symmetric positive definite n x n matrix A (row-major):
+// Cholesky factor A = L L^T (lower, row-oriented), X = L^-1 by columns (kept
+// transposed, Xt[c][q] = X(q, c), so every inner loop runs over contiguous
+// memory), A^-1 = X^T X. About n^3 / 2 multiply-adds; false if A is not
+// positive definite to working precision. A is overwritten.
+bool spd_inverse(std::vector<double> &A, int n, std::vector<double> &inv)
 {
-    inv.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; i++) inv[(size_t)i * n + i] = 1.0;
-    for (int col = 0; col < n; col++) {
-        int piv = col;
-        for (int r = col + 1; r < n; r++) if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col])) piv = r;
-        if (std::fabs(A[(size_t)piv * n + col]) < 1e-300) return false;
-        if (piv != col) for (int k = 0; k < n; k++) { std::swap(A[(size_t)piv * n + k], A[(size_t)col * n + k]); std::swap(inv[(size_t)piv * n + k], inv[(size_t)col * n + k]); }
-        double d = 1.0 / A[(size_t)col * n + col];
-        for (int k = 0; k < n; k++) { A[(size_t)col * n + k] *= d; inv[(size_t)col * n + k] *= d; }
-        for (int r = 0; r < n; r++) {
-            if (r == col) continue;
-            double f = A[(size_t)r * n + col];
-            if (f == 0.0) continue;
-            for (int k = 0; k < n; k++) { A[(size_t)r * n + k] -= f * A[(size_t)col * n + k]; inv[(size_t)r * n + k] -= f * inv[(size_t)col * n + k]; }
+    auto a = [&](int r, int c) -> double & { return A[(size_t)r * n + c]; };
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k <= i; k++) {
+            double v = a(i, k);
+            const double *li = &a(i, 0), *lk = &a(k, 0);
+            for (int q = 0; q < k; q++) v -= li[q] * lk[q];
+            if (i == k) {
+                if (!(v > 0.0)) return false;
+                a(i, i) = std::sqrt(v);
+            } else {
+                a(i, k) = v / a(k, k);
+            }
+        }
+    std::vector<double> Xt((size_t)n * n, 0.0);
+    for (int c = 0; c < n; c++) {
+        double *x = &Xt[(size_t)c * n];
+        x[c] = 1.0 / a(c, c);
+        for (int r = c + 1; r < n; r++) {
+            const double *lr = &a(r, 0);
+            double v = 0.0;
+            for (int q = c; q < r; q++) v += lr[q] * x[q];
+            x[r] = -v / lr[r];
         }
     }
+    inv.assign((size_t)n * n, 0.0);
+    for (int r = 0; r < n; r++)
+        for (int c = r; c < n; c++) {
+            const double *xr = &Xt[(size_t)r * n], *xc = &Xt[(size_t)c * n];
+            double v = 0.0;
+            for (int q = c; q < n; q++) v += xr[q] * xc[q];
+            inv[(size_t)r * n + c] = v;
+            inv[(size_t)c * n + r] = v;
+        }
     return true;
 }
 
@@ -882,22 +663,10 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         if (mg->line) k_line_factors<T><<<dim3((L[l].nx + 31) / 32, (L[l].nz + 7) / 8), dim3(32, 8), 0, st>>>(L[l]);
     }
     if (mg->line) set_line_smem_attrs<T>();
-    // dense coarsest inverse of (A + 11^T/n) in the level's own (split) order
+    // dense pseudo-inverse of the coarsest level in its own (split) order
     Lvl<T> &Lc = L[mg->nlev - 1];
-    if (Lc.n > 4096) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 4096 cells"};
+    if (Lc.n > COARSEST_CELLS) throw CudaError{cudaErrorInvalidValue, "grid does not coarsen to <= 1024 cells"};
     const int nc = (int)Lc.n;
-    // the single-block tail: as many of the smallest levels (<= TAIL_CELLS each)
-    // as fit in its shared memory next to the dense-solve scratch
-    mg->stage_b = tail_dense_bytes(nc, true) + tail_level_bytes<T>(nc, true) <= (size_t)TAIL_SMEM / 2;
-    size_t used = tail_dense_bytes(nc, mg->stage_b) + tail_level_bytes<T>(nc, true);
-    if (used > (size_t)TAIL_SMEM) throw CudaError{cudaErrorInvalidValue, "coarsest multigrid level too large"};
-    mg->tail_start = mg->nlev - 1;
-    while (mg->tail_start > 0 && L[mg->tail_start - 1].n <= TAIL_CELLS &&
-           used + tail_level_bytes<T>(L[mg->tail_start - 1].n, false) <= (size_t)TAIL_SMEM) {
-        used += tail_level_bytes<T>(L[mg->tail_start - 1].n, false);
-        mg->tail_start--;
-    }
-    mg->tail_shm = used;
     std::vector<T> hE(nc), hN(nc), hT(nc);
     TG_CUDA(cudaMemcpyAsync(hE.data(), Lc.aE, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
     TG_CUDA(cudaMemcpyAsync(hN.data(), Lc.aN, sizeof(T) * nc, cudaMemcpyDeviceToHost, st));
@@ -919,11 +688,24 @@ void setup_levels(tg_ctx *C, MG *mg, Lvl<T> *L, const double *aE, const double *
         if (k > 0 || Lc.pk)         { int b = id(k - 1, j, i); add(b, hT[b]); }
     }
     std::vector<double> inv;
-    if (!dense_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
-    mg->B = (double *)dalloc(C, sizeof(double) * (size_t)nc * nc);
+    if (!spd_inverse(A, nc, inv)) throw CudaError{cudaErrorInvalidValue, "singular coarsest multigrid operator"};
+    // Bp = (I - J/n) inv (I - J/n): subtract row and column means, add the grand mean
+    std::vector<double> rm(nc, 0.0);
+    double gm = 0.0;
+    for (int r = 0; r < nc; r++) {
+        for (int c = 0; c < nc; c++) rm[r] += inv[(size_t)r * nc + c];
+        rm[r] /= nc;
+        gm += rm[r];
+    }
+    gm /= nc;
+    std::vector<T> Bp((size_t)nc * nc);
+    for (int r = 0; r < nc; r++)
+        for (int c = 0; c < nc; c++) Bp[(size_t)r * nc + c] = (T)(inv[(size_t)r * nc + c] - rm[r] - rm[c] + gm);
+    T *dB = (T *)dalloc(C, sizeof(T) * (size_t)nc * nc);
+    if (sizeof(T) == sizeof(double)) mg->Bd = (double *)dB;
+    else mg->Bf = (float *)dB;
     mg->nc = nc;
-    TG_CUDA(cudaFuncSetAttribute(k_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, TAIL_SMEM));
-    TG_CUDA(cudaMemcpyAsync(mg->B, inv.data(), sizeof(double) * (size_t)nc * nc, cudaMemcpyHostToDevice, st));
+    TG_CUDA(cudaMemcpyAsync(dB, Bp.data(), sizeof(T) * (size_t)nc * nc, cudaMemcpyHostToDevice, st));
     TG_CUDA(cudaStreamSynchronize(st));
     TG_CUDA(cudaGetLastError());
 }
