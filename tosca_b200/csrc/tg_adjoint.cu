@@ -567,16 +567,55 @@ __global__ void k_adj_face_fluxes(Grid g, Metrics m, V3f<double> ut, V3f<double>
                                   V3f<double> f1a, V3f<double> f2a, V3f<double> f3a,
                                   V3f<double> uta, V3f<double> cta, double *na, V3f<double> twa)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
-    if (i > g.mx - 2 || j > g.my - 2 || k > g.mz - 2) return;
+    // Ucat and nut of the block's faces with one point below and two above
+    // in every direction, staged in shared memory as in the forward pass 1
+    // (rows per warp, wrapped DMDA index, 0 outside a non-periodic extent);
+    // the QUICK points of the periodic boundary faces that fall outside the
+    // tile are read from global memory.
+    constexpr int ATX = BX + 3, ATY = BY + 3, ATZ = BZ + 3, ATN = ATX * ATY * ATZ;
+    static_assert(BX == 32 && (BX * BY * BZ) % 32 == 0 && 3 * ATY * ATZ <= BX * BY * BZ, "tile staging layout");
+    __shared__ double su[3][ATN];
+    __shared__ double sn[ATN];
     const int mx = g.mx, my = g.my, mz = g.mz;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY, k0 = blockIdx.z * BZ;
+    {
+        auto stage = [&](int tx, int ty, int tz, int gi) {
+            const int gj = g.wj(j0 - 1 + ty), gk = g.wk(k0 - 1 + tz), q = (tz * ATY + ty) * ATX + tx;
+            double ux = 0.0, uy = 0.0, uz = 0.0, nt = 0.0;
+            if (gi >= 0 && gi < mx && gj >= 0 && gj < my && gk >= 0 && gk < mz) {
+                const int c = (gk * my + gj) * mx + gi;
+                ux = uc.x[c]; uy = uc.y[c]; uz = uc.z[c];
+                if (p.les) nt = nut[c];
+            }
+            su[0][q] = ux; su[1][q] = uy; su[2][q] = uz; sn[q] = nt;
+        };
+        const int lane = threadIdx.x, wid = threadIdx.z * BY + threadIdx.y;
+        const int gi = g.wi(i0 - 1 + lane);
+        for (int r = wid; r < ATY * ATZ; r += BX * BY * BZ / 32) stage(lane, r % ATY, r / ATY, gi);
+        const int q = wid * 32 + lane;
+        if (q < 3 * ATY * ATZ) {
+            const int r = q / 3, tx = BX + (q - 3 * r);
+            stage(tx, r % ATY, r / ATY, g.wi(i0 - 1 + tx));
+        }
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0 + threadIdx.z;
+    if (i > mx - 2 || j > my - 2 || k > mz - 2) return;
     const bool npi = !g.pi, npj = !g.pj, npk = !g.pk;
     const bool quickDiv = p.div_scheme == TG_DIV_QUICK;
     const double nu = p.nu;
     int f = g.lin(k, j, i);
-    auto U = [&](int kk, int jj, int ii) { return ld3(uc, g.id(kk, jj, ii)); };
+    // tile index of (kk, jj, ii), or -1 outside the tile
+    auto tq = [&](int kk, int jj, int ii) {
+        const int tx = ii - i0 + 1, ty = jj - j0 + 1, tz = kk - k0 + 1;
+        return ((unsigned)tx < (unsigned)ATX && (unsigned)ty < (unsigned)ATY && (unsigned)tz < (unsigned)ATZ) ? (tz * ATY + ty) * ATX + tx : -1;
+    };
+    auto U = [&](int kk, int jj, int ii) {
+        const int q = tq(kk, jj, ii);
+        return q >= 0 ? R3<double>{su[0][q], su[1][q], su[2][q]} : ld3(uc, g.id(kk, jj, ii));
+    };
     auto UA = [&](int kk, int jj, int ii, double w, R3<double> v) { aadd3(cta, g.id(kk, jj, ii), w, v); };
-    auto NUT = [&](int kk, int jj, int ii) { return nut[g.id(kk, jj, ii)]; };
+    auto NUT = [&](int kk, int jj, int ii) { const int q = tq(kk, jj, ii); return q >= 0 ? sn[q] : nut[g.id(kk, jj, ii)]; };
     auto NA = [&](int kk, int jj, int ii, double v) { aadd(na + g.id(kk, jj, ii), v); };
     auto quickW = [](double w, double q[4]) {
         if (w > 0) { q[0] = -0.125; q[1] = 0.75; q[2] = 0.375; q[3] = 0.0; }
