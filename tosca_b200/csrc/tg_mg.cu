@@ -30,6 +30,7 @@
 // 71-73 us per V-cycle at 128 x 64 x 64, one SM's latency chain; the dense
 // solve at the first level of <= 1024 cells replaces it.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <vector>
 
@@ -161,13 +162,13 @@ __global__ void k_line_factors(Lvl<T> L)
 // one j-line of colour `color` (zebra Gauss-Seidel): forward substitution with
 // the stored factors, then back substitution
 template <class T>
-__device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i)
+__device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i, bool zx)
 {
     T dprev = T(0);
     const int nx = L.nx;
     int c = sidx(L, k, 0, i);
     for (int j = 0; j < L.ny; j++, c += nx) {
-        T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
+        T rhs = zx ? L.r[c] : L.r[c] + nb_sum(L, k, j, i, c, false);
         T aS = j > 0 ? L.aN[c - nx] : T(0);
         T dp = (rhs + aS * dprev) * L.minv[c];
         L.tmp[c] = dp;
@@ -194,7 +195,7 @@ __device__ __forceinline__ void line_solve(const Lvl<T> &L, int k, int i)
 // The loads of a chunk do not depend on each other, so they are issued in an
 // unrolled pass of compile-time length CJ before the recurrence runs on
 // shared memory.
-template <class T, int CJ>
+template <class T, int CJ, bool ZX>
 __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int color)
 {
     extern __shared__ unsigned char smraw[];
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(LINE_NW * 32) k_line_chunked(Lvl<T> L, int col
             const int j = j0 + u;
             if (j < ny) {
                 const int c = c0 + u * nx;
-                T rhs = L.r[c] + nb_sum(L, k, j, i, c, false);
+                T rhs = ZX ? L.r[c] : L.r[c] + nb_sum(L, k, j, i, c, false);
                 T mi = L.minv[c];
                 T aS = j > 0 ? L.aN[c - nx] : T(0);
                 D[(w * CJ + u) * 32 + lane] = rhs * mi;
@@ -318,21 +319,30 @@ int line_cj(int ny)
     return (cj <= 32 && line_chunk_smem_cj<T>(cj) <= 200 * 1024) ? cj : 0;
 }
 
+template <class T, bool ZX>
+void launch_line_chunked_zx(Lvl<T> &F, int color, int cj, int nb, size_t shm, cudaStream_t st)
+{
+    switch (cj) {
+    case 1: k_line_chunked<T, 1, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 2: k_line_chunked<T, 2, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 4: k_line_chunked<T, 4, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 8: k_line_chunked<T, 8, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    case 16: k_line_chunked<T, 16, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    default: k_line_chunked<T, 32, ZX><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
+    }
+}
+
+// zx: the unknown is zero on the level (the first sweep after k_in or the
+// restriction), so the off-line neighbour terms are skipped
 template <class T>
-void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
+void launch_line_chunked(Lvl<T> &F, int color, bool zx, cudaStream_t st)
 {
     const int lines = (F.nx >> 1) * F.nz;
     const int nb = (lines + 31) / 32;
     const int cj = line_cj<T>(F.ny);
     const size_t shm = line_chunk_smem_cj<T>(cj);
-    switch (cj) {
-    case 1: k_line_chunked<T, 1><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    case 2: k_line_chunked<T, 2><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    case 4: k_line_chunked<T, 4><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    case 8: k_line_chunked<T, 8><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    case 16: k_line_chunked<T, 16><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    default: k_line_chunked<T, 32><<<nb, LINE_NW * 32, shm, st>>>(F, color); break;
-    }
+    if (zx) launch_line_chunked_zx<T, true>(F, color, cj, nb, shm, st);
+    else launch_line_chunked_zx<T, false>(F, color, cj, nb, shm, st);
 }
 
 // Warp-segmented zebra line solve for the coarse levels (nx even, ny <= 32 CJ):
@@ -342,7 +352,7 @@ void launch_line_chunked(Lvl<T> &F, int color, cudaStream_t st)
 // segment by shuffle scans. No block barrier and
 // no scratch array: on the small levels a launch costs about one round of
 // loads plus the two scans.
-template <class T, int CJ>
+template <class T, int CJ, bool ZX>
 __global__ void __launch_bounds__(256) k_line_warp(Lvl<T> L, int color, int P)
 {
     const int lane = threadIdx.x & 31, sl = lane & (P - 1);
@@ -363,7 +373,7 @@ __global__ void __launch_bounds__(256) k_line_warp(Lvl<T> L, int color, int P)
             const int c = c0 + u * nx;
             const T mi = L.minv[c];
             a[u] = j > 0 ? mi * L.aN[c - nx] : T(0);
-            b[u] = mi * (L.r[c] + nb_sum(L, k, j, i, c, false));
+            b[u] = mi * (ZX ? L.r[c] : L.r[c] + nb_sum(L, k, j, i, c, false));
             cp[u] = L.cp[c];
             B = a[u] * B + b[u];
             A = a[u] * A;
@@ -411,7 +421,7 @@ constexpr int64_t LINE_WARP_CELLS = 65536;
 inline int line_warp_cj(int ny) { return ny <= 32 ? 1 : ny <= 64 ? 2 : ny <= 128 ? 4 : 0; }
 
 template <class T>
-void launch_line_warp(Lvl<T> &F, int color, cudaStream_t st)
+void launch_line_warp(Lvl<T> &F, int color, bool zx, cudaStream_t st)
 {
     const int cj = line_warp_cj(F.ny);
     int P = 1;
@@ -419,11 +429,16 @@ void launch_line_warp(Lvl<T> &F, int color, cudaStream_t st)
     const int lines = (F.nx >> 1) * F.nz, per_warp = 32 / P;
     const int warps = (lines + per_warp - 1) / per_warp;
     const int nb = (warps * 32 + 255) / 256;
-    switch (cj) {
-    case 1: k_line_warp<T, 1><<<nb, 256, 0, st>>>(F, color, P); break;
-    case 2: k_line_warp<T, 2><<<nb, 256, 0, st>>>(F, color, P); break;
-    default: k_line_warp<T, 4><<<nb, 256, 0, st>>>(F, color, P); break;
-    }
+    auto go = [&](auto zxc) {
+        constexpr bool Z = decltype(zxc)::value;
+        switch (cj) {
+        case 1: k_line_warp<T, 1, Z><<<nb, 256, 0, st>>>(F, color, P); break;
+        case 2: k_line_warp<T, 2, Z><<<nb, 256, 0, st>>>(F, color, P); break;
+        default: k_line_warp<T, 4, Z><<<nb, 256, 0, st>>>(F, color, P); break;
+        }
+    };
+    if (zx) go(std::true_type{});
+    else go(std::false_type{});
 }
 
 template <class T>
@@ -433,41 +448,47 @@ void set_line_smem_attrs()
         const size_t b = line_chunk_smem_cj<T>(cj);
         if (b <= 200 * 1024) TG_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b));
     };
-    set((const void *)k_line_chunked<T, 1>, 1);
-    set((const void *)k_line_chunked<T, 2>, 2);
-    set((const void *)k_line_chunked<T, 4>, 4);
-    set((const void *)k_line_chunked<T, 8>, 8);
-    set((const void *)k_line_chunked<T, 16>, 16);
-    set((const void *)k_line_chunked<T, 32>, 32);
+    set((const void *)k_line_chunked<T, 1, false>, 1);
+    set((const void *)k_line_chunked<T, 2, false>, 2);
+    set((const void *)k_line_chunked<T, 4, false>, 4);
+    set((const void *)k_line_chunked<T, 8, false>, 8);
+    set((const void *)k_line_chunked<T, 16, false>, 16);
+    set((const void *)k_line_chunked<T, 32, false>, 32);
+    set((const void *)k_line_chunked<T, 1, true>, 1);
+    set((const void *)k_line_chunked<T, 2, true>, 2);
+    set((const void *)k_line_chunked<T, 4, true>, 4);
+    set((const void *)k_line_chunked<T, 8, true>, 8);
+    set((const void *)k_line_chunked<T, 16, true>, 16);
+    set((const void *)k_line_chunked<T, 32, true>, 32);
 }
 
 
 // lines of one colour: (i + k) & 1 == color, i.e. i of parity (color ^ k) & 1
 template <class T>
-__global__ void k_smooth_line(Lvl<T> L, int color)
+__global__ void k_smooth_line(Lvl<T> L, int color, int zx)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
     if (k >= L.nz) return;
     int q = (color ^ k) & 1;
     int cnt = q ? (L.nx >> 1) : ((L.nx + 1) >> 1);
     if (t >= cnt) return;
-    line_solve(L, k, 2 * t + q);
+    line_solve(L, k, 2 * t + q, zx != 0);
 }
 
 template <class T>
-__device__ __forceinline__ void point_update(const Lvl<T> &L, int k, int j, int i)
+__device__ __forceinline__ void point_update(const Lvl<T> &L, int k, int j, int i, bool zx)
 {
     int c = sidx(L, k, j, i);
-    L.x[c] = (L.r[c] + nb_sum(L, k, j, i, c, true)) / L.diag[c];
+    L.x[c] = (zx ? L.r[c] : L.r[c] + nb_sum(L, k, j, i, c, true)) / L.diag[c];
 }
 
 template <class T>
-__global__ void k_smooth_rb(Lvl<T> L, int color)
+__global__ void k_smooth_rb(Lvl<T> L, int color, int zx)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= L.nx || j >= L.ny || k >= L.nz) return;
     if (((i + j + k) & 1) != color) return;
-    point_update(L, k, j, i);
+    point_update(L, k, j, i, zx != 0);
 }
 
 // ------------------------------------------------------------------ transfers
@@ -561,26 +582,29 @@ void vcycle(tg_ctx *C, MG *mg, Lvl<T> *L, int l)
     }
     Lvl<T> &F = L[l];
     const bool fine = l == 0;
-    auto smooth = [&](int color) {
+    // zx: the level's unknown is still the zero written by k_in or the
+    // restriction (the first sweep of the pre-smoothing), so the sweep skips
+    // the off-line (off-point) neighbour terms, which are zero
+    auto smooth = [&](int color, bool zx) {
         if (mg->line && !fine && F.n <= LINE_WARP_CELLS && (F.nx % 2) == 0 && line_warp_cj(F.ny) > 0) {
-            TG_PROF(C, "mg_smooth_line_coarse", launch_line_warp<T>(F, color, st));
+            TG_PROF(C, "mg_smooth_line_coarse", launch_line_warp<T>(F, color, zx, st));
         } else if (mg->line && (F.nx % 2) == 0 && line_cj<T>(F.ny) > 0) {
-            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse", launch_line_chunked<T>(F, color, st));
+            TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse", launch_line_chunked<T>(F, color, zx, st));
         } else if (mg->line) {
             int half = (F.nx + 1) >> 1;
             TG_PROF(C, fine ? "mg_smooth_line_L0" : "mg_smooth_line_coarse",
-                    k_smooth_line<T><<<dim3((half + 31) / 32, (F.nz + 7) / 8), dim3(32, 8), 0, st>>>(F, color));
+                    k_smooth_line<T><<<dim3((half + 31) / 32, (F.nz + 7) / 8), dim3(32, 8), 0, st>>>(F, color, zx ? 1 : 0));
         } else {
             TG_PROF(C, fine ? "mg_smooth_rb_L0" : "mg_smooth_rb_coarse",
-                    k_smooth_rb<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, color));
+                    k_smooth_rb<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, color, zx ? 1 : 0));
         }
     };
-    for (int s = 0; s < mg->nu; s++) { smooth(0); smooth(1); }
+    for (int s = 0; s < mg->nu; s++) { smooth(0, s == 0); smooth(1, false); }
     Lvl<T> &Cc = L[l + 1];
     TG_PROF(C, fine ? "mg_restrict_L0" : "mg_restrict_coarse", k_restrict<T><<<dim3((Cc.nx + RS_I - 1) / RS_I, Cc.ny, Cc.nz), 8 * RS_I, 0, st>>>(F, Cc));
     vcycle(C, mg, L, l + 1);
     TG_PROF(C, fine ? "mg_prolong_L0" : "mg_prolong_coarse", k_prolong<T><<<g3(F.nx, F.ny, F.nz), block3(), 0, st>>>(F, Cc));
-    for (int s = 0; s < mg->nu; s++) { smooth(1); smooth(0); }
+    for (int s = 0; s < mg->nu; s++) { smooth(1, false); smooth(0, false); }
 }
 
 // split-layout index on the host
