@@ -656,9 +656,17 @@ def main():
     barrier()
     bytes_in = h_ucont.nbytes + h_ucat.nbytes + h_p.nbytes          # nut is output only
     bytes_out = bytes_in + (h_nut.nbytes if cfg.les else 0)
+    # what bounds it: the step's device time against the wall time per call;
+    # the rest is the host<->device copies (and the layout conversions)
+    e2e_ms = t_e2e / e2e_steps * 1e3
+    dev_ms = head["t_dev"] / args.steps * 1e3
+    copy_ms = max(e2e_ms - dev_ms, 1e-9)
     e2e = {"value": cells * e2e_steps * world / t_e2e / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(bytes_out),
-           "steps": e2e_steps, "precision": head_prec, "max_divergence": se.max_divergence}
+           "steps": e2e_steps, "precision": head_prec, "max_divergence": se.max_divergence,
+           "ms_per_step": e2e_ms, "device_step_ms": dev_ms, "transfer_ms_per_step": copy_ms,
+           "transfer_gbs": (bytes_in + bytes_out) / (copy_ms * 1e-3) / 1e9,
+           "limiter": "host<->device copies of the state (PCIe), %.0f %% of the call" % (100.0 * copy_ms / e2e_ms)}
 
     adj = None
     if rank == 0 and not args.no_adjoint and args.workload == "abl":
