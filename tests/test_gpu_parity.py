@@ -1,7 +1,8 @@
 """Parity of the CUDA step with the CPU restatement (oracle) on identical
 seeded inputs, stage by stage and over full steps. FP64 tolerances: metrics
 and single stages to <= 1e-12 relative L2 (rounding-order differences only),
-full steps to the north-star bound of 1e-10 relative L2 on u, v, w and p."""
+full steps to 1e-10 relative L2 on u, v, w and p (the parity bar of the
+FP64 step)."""
 import numpy as np
 import pytest
 
