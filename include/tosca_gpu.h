@@ -46,7 +46,18 @@ enum {
     TG_BC_PERIODIC        = 0,
     TG_BC_NOSLIP          = 1,  /* "noSlip"                                        */
     TG_BC_SLIP            = 2,  /* "slip"                                          */
-    TG_BC_WALL_SHUMANN    = 3   /* "velocityWallFunction" type -3 (jLeft only)     */
+    TG_BC_WALL_SHUMANN    = 3,  /* "velocityWallFunction" type -3 (jLeft only)     */
+    /* patch type 0 (not a wall, checkBCsAndSetPatchTypes boundary.c:321-350):
+     * the boundary face flux is interpolated from the ghost and first cells
+     * (UpdateContravariantBCs boundary.c:651-689), and the outflow faces of
+     * all such patches take the mass imbalance (adjustFluxesLocal,
+     * ueqn.c:748-1135, at the end of the momentum solve); explicit schemes
+     * (TG_DDT_FE, TG_DDT_RK4) only, no adjoint                                  */
+    TG_BC_FIXED_VALUE     = 4,  /* "fixedValue": ghost cell = bc_value of the      */
+                                /* patch (boundary.c:1632-1673), an inflow          */
+    TG_BC_ZERO_GRADIENT   = 5   /* "zeroGradient": ghost 2 U(1) - U(2)             */
+                                /* (boundary.c:1897-1970), reverse flow through the */
+                                /* face set to zero (boundary.c:718-741), an outflow */
 };
 /* eddy-viscosity patch types (boundary/nut) */
 enum {
@@ -177,6 +188,8 @@ typedef struct tg_config {
     double  wall_gamma_m;
     double  wall_theta_ref;
     double  t_start;               /* -startTime: clock time at it_start (thetaWallFunction -4) */
+    double  bc_value[18];          /* TG_BC_FIXED_VALUE: Cartesian velocity (x, y, z) of  */
+                                   /* patch p at [3p, 3p+2] (boundaryU *val, boundary.c)  */
 } tg_config;
 
 /* per-call statistics */

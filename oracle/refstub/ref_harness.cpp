@@ -11,7 +11,7 @@
 // InitializePEqn, peqn.c:35-103; InitializeLES, les.c:20-150; InitializeTEqn,
 // teqn.c:19-257; SetWallModels, boundary.c:4640-5200), with the values a
 // control.dat and boundary/ files would hold, and then calls the reference's
-// functions. Supported: periodic, slip, noSlip and the Schumann velocity wall
+// functions. Supported: periodic, slip, noSlip, fixedValue, zeroGradient and the Schumann velocity wall
 // function (-3, averaged u*) on jLeft; central and QUICK convection; FE and
 // RK4; no LES or Smagorinsky (TOSCA's hard-coded Cs^2 = 0.0289,
 // les.c:10,175); the mean pressure gradient; the potential temperature
@@ -59,6 +59,8 @@ const char *u_bc_name(int t)
     case TG_BC_NOSLIP: return "noSlip";
     case TG_BC_SLIP: return "slip";
     case TG_BC_WALL_SHUMANN: return "velocityWallFunction";
+    case TG_BC_FIXED_VALUE: return "fixedValue";
+    case TG_BC_ZERO_GRADIENT: return "zeroGradient";
     default: return "";
     }
 }
@@ -261,6 +263,13 @@ void build(tg_ctx &X)
     setU(m.boundaryU.iLeft, c.bc[0]); setU(m.boundaryU.iRight, c.bc[1]);
     setU(m.boundaryU.jLeft, c.bc[2]); setU(m.boundaryU.jRight, c.bc[3]);
     setU(m.boundaryU.kLeft, c.bc[4]); setU(m.boundaryU.kRight, c.bc[5]);
+    {
+        Cmpnts *vals[6] = {&m.boundaryU.iLval, &m.boundaryU.iRval, &m.boundaryU.jLval, &m.boundaryU.jRval,
+                           &m.boundaryU.kLval, &m.boundaryU.kRval};
+        for (int q = 0; q < 6; q++) {
+            vals[q]->x = c.bc_value[3 * q]; vals[q]->y = c.bc_value[3 * q + 1]; vals[q]->z = c.bc_value[3 * q + 2];
+        }
+    }
     m.boundaryU.jLWF = c.bc[2] == TG_BC_WALL_SHUMANN ? -3 : 0;
     m.boundaryU.jRWF = c.bc[3] == TG_BC_WALL_SHUMANN ? -3 : 0;
     auto setS = [&](word &w, PetscReal &val, int t, double v) { w = nut_bc_name(t); val = v; };
@@ -435,7 +444,7 @@ tg_status ref_create(const tg_config *cfg, tg_ctx **out)
     const tg_config &c = *cfg;
     if (c.mx < 6 || c.my < 6 || c.mz < 6) return TG_ERR_BAD_ARG;
     for (int q = 0; q < 6; q++) {
-        if (c.bc[q] < 0 || c.bc[q] > TG_BC_WALL_SHUMANN) return TG_ERR_BAD_ARG;
+        if (c.bc[q] < 0 || c.bc[q] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
         if (c.bc[q] == TG_BC_WALL_SHUMANN && q != 2) return TG_ERR_BAD_ARG;
     }
     // supported subset of the workloads (see the file header)

@@ -830,6 +830,24 @@ void updateCartesianBCs(tg_ctx &C)
         if (j == my - 2 && bc[TG_JRIGHT] == TG_BC_NOSLIP) C.ucat[C.I(k, j + 1, i)] = -1.0 * L(k, j, i);
         if (k == 1 && bc[TG_KLEFT] == TG_BC_NOSLIP)       C.ucat[C.I(k - 1, j, i)] = -1.0 * L(k, j, i);
         if (k == mz - 2 && bc[TG_KRIGHT] == TG_BC_NOSLIP) C.ucat[C.I(k + 1, j, i)] = -1.0 * L(k, j, i);
+        // fixedValue, boundary.c:1632-1673: the ghost takes the patch value
+        auto fixedv = [&](int patch, int gk, int gj, int gi) {
+            if (bc[patch] == TG_BC_FIXED_VALUE)
+                C.ucat[C.I(gk, gj, gi)] = mk(C.c.bc_value[3 * patch], C.c.bc_value[3 * patch + 1], C.c.bc_value[3 * patch + 2]);
+        };
+        if (i == 1)      fixedv(TG_ILEFT, k, j, i - 1);
+        if (i == mx - 2) fixedv(TG_IRIGHT, k, j, i + 1);
+        if (j == 1)      fixedv(TG_JLEFT, k, j - 1, i);
+        if (j == my - 2) fixedv(TG_JRIGHT, k, j + 1, i);
+        if (k == 1)      fixedv(TG_KLEFT, k - 1, j, i);
+        if (k == mz - 2) fixedv(TG_KRIGHT, k + 1, j, i);
+        // zeroGradient (outflow), boundary.c:1897-1970: linear extrapolation
+        if (i == 1 && bc[TG_ILEFT] == TG_BC_ZERO_GRADIENT)       C.ucat[C.I(k, j, i - 1)] = 2.0 * L(k, j, i) - L(k, j, i + 1);
+        if (i == mx - 2 && bc[TG_IRIGHT] == TG_BC_ZERO_GRADIENT) C.ucat[C.I(k, j, i + 1)] = 2.0 * L(k, j, i) - L(k, j, i - 1);
+        if (j == 1 && bc[TG_JLEFT] == TG_BC_ZERO_GRADIENT)       C.ucat[C.I(k, j - 1, i)] = 2.0 * L(k, j, i) - L(k, j + 1, i);
+        if (j == my - 2 && bc[TG_JRIGHT] == TG_BC_ZERO_GRADIENT) C.ucat[C.I(k, j + 1, i)] = 2.0 * L(k, j, i) - L(k, j - 1, i);
+        if (k == 1 && bc[TG_KLEFT] == TG_BC_ZERO_GRADIENT)       C.ucat[C.I(k - 1, j, i)] = 2.0 * L(k, j, i) - L(k + 1, j, i);
+        if (k == mz - 2 && bc[TG_KRIGHT] == TG_BC_ZERO_GRADIENT) C.ucat[C.I(k + 1, j, i)] = 2.0 * L(k, j, i) - L(k - 1, j, i);
         // periodic, boundary.c:1990-2018
         if (bc[TG_ILEFT] == TG_BC_PERIODIC && i == 1)       C.ucat[C.I(k, j, i - 1)] = L(k, j, -2);
         if (bc[TG_IRIGHT] == TG_BC_PERIODIC && i == mx - 2) C.ucat[C.I(k, j, i + 1)] = L(k, j, mx + 1);
@@ -869,6 +887,14 @@ void updateContravariantBCs(tg_ctx &C)
         if ((!type0(TG_ILEFT) && i == 0) || (!type0(TG_IRIGHT) && i == mx - 2)) u.x = 0.0;
         if ((!type0(TG_JLEFT) && j == 0) || (!type0(TG_JRIGHT) && j == my - 2)) u.y = 0.0;
         if ((!type0(TG_KLEFT) && k == 0) || (!type0(TG_KRIGHT) && k == mz - 2)) u.z = 0.0;
+        // zeroGradient: no flow back in through the face, boundary.c:718-741
+        const auto zg = [&](int patch) { return bc[patch] == TG_BC_ZERO_GRADIENT; };
+        if (zg(TG_ILEFT) && i == 0 && u.x > 0.0) u.x = 0.0;
+        if (zg(TG_IRIGHT) && i == mx - 2 && u.x < 0.0) u.x = 0.0;
+        if (zg(TG_JLEFT) && j == 0 && u.y > 0.0) u.y = 0.0;
+        if (zg(TG_JRIGHT) && j == my - 2 && u.y < 0.0) u.y = 0.0;
+        if (zg(TG_KLEFT) && k == 0 && u.z > 0.0) u.z = 0.0;
+        if (zg(TG_KRIGHT) && k == mz - 2 && u.z < 0.0) u.z = 0.0;
         if (bc[TG_ILEFT] == TG_BC_PERIODIC && i == 0) u.x = lc[C.I(k, j, -2)].x;
         if (bc[TG_JLEFT] == TG_BC_PERIODIC && j == 0) u.y = lc[C.I(k, -2, i)].y;
         if (bc[TG_KLEFT] == TG_BC_PERIODIC && k == 0) u.z = lc[C.I(-2, j, i)].z;
@@ -1544,15 +1570,18 @@ void resetNonResolvedCellFaces(tg_ctx &C, std::vector<V3> &V)
         size_t c = C.I(k, j, i);
         V3 &v = V[c];
         const V3 &uo = C.ucont_o[c];
-        if (i == 0) { if (!(uo.x < 0)) v.x = 0.0; }
+        // a boundary face keeps its value on a zeroGradient patch or where
+        // the flow left the domain at the step start
+        auto zg = [&](int patch) { return C.c.bc[patch] == TG_BC_ZERO_GRADIENT; };
+        if (i == 0) { if (!(zg(TG_ILEFT) || uo.x < 0)) v.x = 0.0; }
         else if (i == mx - 1) v.x = 0.0;
-        else if (i == mx - 2 && !C.pi) { if (!(uo.x > 0)) v.x = 0.0; }
-        if (j == 0) { if (!(uo.y < 0)) v.y = 0.0; }
+        else if (i == mx - 2 && !C.pi) { if (!(zg(TG_IRIGHT) || uo.x > 0)) v.x = 0.0; }
+        if (j == 0) { if (!(zg(TG_JLEFT) || uo.y < 0)) v.y = 0.0; }
         else if (j == my - 1) v.y = 0.0;
-        else if (j == my - 2 && !C.pj) { if (!(uo.y > 0)) v.y = 0.0; }
-        if (k == 0) { if (!(uo.z < 0)) v.z = 0.0; }
+        else if (j == my - 2 && !C.pj) { if (!(zg(TG_JRIGHT) || uo.y > 0)) v.y = 0.0; }
+        if (k == 0) { if (!(zg(TG_KLEFT) || uo.z < 0)) v.z = 0.0; }
         else if (k == mz - 1) v.z = 0.0;
-        else if (k == mz - 2 && !C.pk) { if (!(uo.z > 0)) v.z = 0.0; }
+        else if (k == mz - 2 && !C.pk) { if (!(zg(TG_KRIGHT) || uo.z > 0)) v.z = 0.0; }
     }
 }
 
@@ -1589,6 +1618,53 @@ void explicitRhsU(tg_ctx &C, int mode = 0)
 
 #include "tosca_oracle_imex.inc"
 
+// adjustFluxesLocal, ueqn.c:748-1135. The faces of the non-periodic, non-wall
+// patches (patch type 0) are split by the sign of their flux into inflow (into
+// the domain) and outflow; the outflow faces then take the imbalance
+// FluxOut - FluxIn in proportion to their own flux, so that the boundary
+// fluxes sum to zero. A face with zero (or non-finite) flux is set to zero.
+// Patches are visited in the reference's order (k, j, i; left, right) and
+// their faces in its loop order.
+void adjustFluxesLocal(tg_ctx &C)
+{
+    const int mx = C.mx, my = C.my, mz = C.mz;
+    const int *bc = C.c.bc;
+    auto type0 = [&](int patch) { return bc[patch] != TG_BC_PERIODIC && !isWall(bc[patch]); };
+    auto faces = [&](int patch, auto &&fn) {
+        const int dir = patch >> 1, right = patch & 1;
+        if (dir == 2) {
+            const int k = right ? mz - 2 : 0;
+            for (int j = 1; j < my - 1; j++) for (int i = 1; i < mx - 1; i++) fn(C.ucont[C.I(k, j, i)].z);
+        } else if (dir == 1) {
+            const int j = right ? my - 2 : 0;
+            for (int k = 1; k < mz - 1; k++) for (int i = 1; i < mx - 1; i++) fn(C.ucont[C.I(k, j, i)].y);
+        } else {
+            const int i = right ? mx - 2 : 0;
+            for (int k = 1; k < mz - 1; k++) for (int j = 1; j < my - 1; j++) fn(C.ucont[C.I(k, j, i)].x);
+        }
+    };
+    const int order[6] = {TG_KLEFT, TG_KRIGHT, TG_JLEFT, TG_JRIGHT, TG_ILEFT, TG_IRIGHT};
+    double in = 0.0, out = 0.0;
+    for (int patch : order) {
+        if (!type0(patch)) continue;
+        const bool right = patch & 1;
+        faces(patch, [&](double &u) {
+            if (u > 0.0) { if (right) out += u; else in += u; }
+            else if (u < 0.0) { if (right) in += std::fabs(u); else out += std::fabs(u); }
+            else u = 0.0;
+        });
+    }
+    const double gf = out - in;
+    for (int patch : order) {
+        if (!type0(patch)) continue;
+        const bool right = patch & 1;
+        faces(patch, [&](double &u) {
+            if (!right && u < 0.0) u += gf * (std::fabs(u) / out);
+            if (right && u > 0.0) u -= gf * (u / out);
+        });
+    }
+}
+
 // SolveUEqn with UeqnFE / UeqnRK4, ueqn.c:397-440, ueqn_solvers.c:1411-1504
 // (UeqnSNES and the IMEX schemes in their own files)
 int solveUEqn(tg_ctx &C)
@@ -1620,8 +1696,7 @@ int solveUEqn(tg_ctx &C)
     resetFacePeriodic(C, C.ucont);
     contravariantToCartesian(C);
     resetCellPeriodic(C, C.ucat);
-    // adjustFluxesLocal (ueqn.c:748-1135) only acts on non-periodic, non-wall
-    // patches; every patch type accepted here is periodic or a wall.
+    adjustFluxesLocal(C);
     return rc;
 }
 
@@ -1909,7 +1984,10 @@ tg_status tor_create(const tg_config *cfg, tg_ctx **out)
     if (!cfg || !out) return TG_ERR_BAD_ARG;
     *out = nullptr;
     if (cfg->mx < 6 || cfg->my < 6 || cfg->mz < 6) return TG_ERR_BAD_ARG;
-    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > 3) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++)
+        if ((cfg->bc[p] == TG_BC_FIXED_VALUE || cfg->bc[p] == TG_BC_ZERO_GRADIENT) &&
+            cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     if (cfg->bc[TG_IRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_ILEFT] == TG_BC_WALL_SHUMANN ||
@@ -2290,6 +2368,9 @@ tg_status tor_adjoint_step(tg_ctx *C)
         if (C->c.teqn) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the temperature equation is not implemented");
         if (C->c.ddt_scheme == TG_DDT_CN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the Crank-Nicolson scheme is not implemented");
         if (C->c.ddt_scheme >= TG_DDT_ABCN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the IMEX schemes is not implemented");
+        for (int q = 0; q < 6; q++)
+            if (C->c.bc[q] == TG_BC_FIXED_VALUE || C->c.bc[q] == TG_BC_ZERO_GRADIENT)
+                return fail(C, TG_ERR_BAD_ARG, "the adjoint of the inflow/outflow patches is not implemented");
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;
         auto p = C->p, phi = C->phi, phi1d = C->phi1d, nut = C->nut;

@@ -46,6 +46,9 @@ def build_case(name: str, **kw):
         return cfg, nodes, ucat, p, None
     if name == "hill":
         return cases.hill_case(**kw)
+    if name == "channel":
+        cfg, nodes, ucat, p = cases.channel_case(**kw)
+        return cfg, nodes, ucat, p, None
     raise ValueError(name)
 
 
@@ -66,4 +69,6 @@ SMALL = {
     "tgv": dict(n=16),
     "abl": dict(nx=16, ny=16, nz=12, Lx=160.0, Ly=160.0, H=100.0),
     "hill": dict(nx=24, ny=12, nz=12),
+    # inflow at x = 0, outflow at x = Lx, noSlip ground (cases.channel_case)
+    "channel": dict(nx=20, ny=12, nz=10, Lx=200.0, Ly=120.0, H=100.0),
 }

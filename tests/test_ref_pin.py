@@ -30,8 +30,11 @@ file compares, stage by stage and over whole steps:
                                              the surface temperature after 3 steps
 
 on the Taylor-Green box, the ABL (Smagorinsky, Schumann wall stress, mean
-pressure gradient), the curvilinear hill (QUICK, Smagorinsky, wall stress)
-and the stratified ABL and hill with the thermal wall function.
+pressure gradient), the curvilinear hill (QUICK, Smagorinsky, wall stress),
+an open channel with a fixedValue inflow and a zeroGradient outflow
+(UpdateCartesianBCs and UpdateContravariantBCs for those patches,
+adjustFluxesLocal, ueqn.c:748-1135) and the stratified ABL and hill with the
+thermal wall function.
 The HYPRE solve inside SolvePEqn is the one stand-in that computes: a tight
 Krylov solve of the captured pinned matrix (unique solution), like the
 oracle's own solve. The reference hard-codes the Smagorinsky constant
@@ -52,7 +55,7 @@ pytestmark = pytest.mark.skipif(not R.available(), reason="reference sources / o
 
 METRICS = ["CSI", "ETA", "ZET", "ICSI", "IETA", "IZET", "JCSI", "JETA", "JZET",
            "KCSI", "KETA", "KZET", "AJ", "IAJ", "JAJ", "KAJ"]
-CASES = ["tgv", "abl", "hill"]
+CASES = ["tgv", "abl", "hill", "channel"]
 
 
 def _full(a):
@@ -155,7 +158,8 @@ def test_explicit_rhs(case):
 
 
 @pytest.mark.parametrize("name,ddt", [("tgv", api.DDT_FE), ("tgv", api.DDT_RK4), ("abl", api.DDT_FE),
-                                      ("abl", api.DDT_RK4), ("hill", api.DDT_FE), ("hill", api.DDT_RK4)])
+                                      ("abl", api.DDT_RK4), ("hill", api.DDT_FE), ("hill", api.DDT_RK4),
+                                      ("channel", api.DDT_FE), ("channel", api.DDT_RK4)])
 def test_steps(name, ddt):
     """Three time steps of TOSCA's loop against three oracle steps. Both solve
     the pressure equation to 1e-14 relative residual or below; the hill's
@@ -169,6 +173,44 @@ def test_steps(name, ddt):
     for f in ("UCONT", "UCAT"):
         assert rel_l2(r.get(f), o.get(f)) < 1e-12, f
     assert rel_l2(r.get("P"), o.get("P")) < (1e-9 if name == "hill" else 1e-10)
+    o.close(); r.close()
+
+
+@pytest.mark.parametrize("wall,div", [(api.BC_WALL_SHUMANN, api.DIV_CENTRAL), (api.BC_NOSLIP, api.DIV_QUICK)])
+def test_inflow_outflow_steps(wall, div):
+    """The channel (fixedValue inflow at x = 0, zeroGradient outflow at
+    x = Lx: UpdateCartesianBCs, UpdateContravariantBCs with its reverse-flow
+    clip, resetNonResolvedCellFaces keeping the outflow faces solved, and
+    adjustFluxesLocal at the end of SolveUEqn) with the Schumann wall function
+    or QUICK convection, three RK4 steps."""
+    o, r = _pair("channel", ddt_scheme=api.DDT_RK4, div_scheme=div, bc=(api.BC_PERIODIC, api.BC_PERIODIC, wall,
+                 api.BC_SLIP, api.BC_FIXED_VALUE, api.BC_ZERO_GRADIENT))
+    for _ in range(3):
+        o.step(1)
+        r.step(1)
+    for f in ("UCONT", "UCAT"):
+        assert rel_l2(r.get(f), o.get(f)) < 1e-12, f
+    assert rel_l2(r.get("P"), o.get("P")) < 1e-10
+    o.close(); r.close()
+
+
+def test_solve_u_balances_the_boundary_flux():
+    """SolveUEqn on the channel from the step-start state: the momentum
+    update, the outflow faces solved by it (resetNonResolvedCellFaces) and
+    adjustFluxesLocal leave the outflow flux equal to the inflow flux, as in
+    the reference. (After the step, UpdateContravariantBCs re-interpolates
+    the inflow faces from the updated first cells, so the balance holds at
+    the pressure solve, not at the end of the step.)"""
+    o, r = _pair("channel", ddt_scheme=api.DDT_RK4)
+    for s in (o, r):
+        s.set("UCONT_O", s.get("UCONT"))
+        s.UpdateNut(); s.UpdateWallModelsU(); s.GradP()
+        s.SolveUEqn()
+        u = s.get("UCONT")[..., 2]
+        fin, fout = u[0, 1:-1, 1:-1].sum(), u[-2, 1:-1, 1:-1].sum()
+        assert abs(fin - fout) <= 1e-12 * abs(fin)
+    assert rel_l2(r.get("UCONT"), o.get("UCONT")) < 1e-14
+    assert rel_l2(r.get("UCAT"), o.get("UCAT")) < 1e-14
     o.close(); r.close()
 
 

@@ -18,7 +18,7 @@ import numpy as np
 # ------------------------------------------------------------------ constants
 TG_OK, TG_ERR_CUDA, TG_ERR_BAD_ARG, TG_ERR_NOT_CONVERGED, TG_ERR_NAN, TG_ERR_ALLOC, TG_ERR_STATE = range(7)
 
-BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN = 0, 1, 2, 3
+BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN, BC_FIXED_VALUE, BC_ZERO_GRADIENT = 0, 1, 2, 3, 4, 5
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
@@ -93,6 +93,7 @@ class TgConfig(C.Structure):
         ("wall_gamma_m", C.c_double),
         ("wall_theta_ref", C.c_double),
         ("t_start", C.c_double),
+        ("bc_value", C.c_double * 18),
     ]
 
 
@@ -205,6 +206,8 @@ class Config:
     wall_gamma_m: float = 4.8
     wall_theta_ref: float = 300.0
     t_start: float = 0.0
+    # TG_BC_FIXED_VALUE patches: Cartesian velocity of patch p at [3p, 3p + 2]
+    bc_value: tuple = (0.0,) * 18
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

@@ -23,8 +23,8 @@ import math
 
 import numpy as np
 
-from .api import (BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, DDT_FE, DDT_RK4, DIV_CENTRAL, DIV_QUICK,
-                  NUTBC_FIXEDVALUE, NUTBC_PERIODIC, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION,
+from .api import (BC_FIXED_VALUE, BC_NOSLIP, BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, BC_ZERO_GRADIENT, DDT_FE,
+                  DDT_RK4, DIV_CENTRAL, DIV_QUICK, NUTBC_FIXEDVALUE, NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION,
                   TBC_ZERO_GRADIENT, TWALL_FIXED_FLUX, TWALL_SHUMANN, Config)
 
 
@@ -183,6 +183,24 @@ def abl_case(nx: int = 256, ny: int = 256, nz: int = 128, Lx: float = 2560.0, Ly
     interior[1:-1, 1:-1, 1:-1] = True
     ucat[~interior] = 0.0
     p = np.zeros((mz, my, mx))
+    return cfg, nodes, ucat, p
+
+
+def channel_case(nx: int = 256, ny: int = 128, nz: int = 64, Lx: float = 2560.0, Ly: float = 1280.0,
+                 H: float = 500.0, u_in: float = 8.0, wall: int = BC_NOSLIP, **kw):
+    """Open channel with an inflow and an outflow (flow along +x, the k
+    direction): a fixedValue patch (BC_FIXED_VALUE, uniform Cartesian
+    velocity (u_in, 0, 0)) at x = 0, a zeroGradient outflow patch
+    (BC_ZERO_GRADIENT) at x = Lx, the bottom patch `wall` (noSlip or the
+    Schumann wall function), slip top, periodic y; zero-gradient nut on the
+    inflow and outflow patches, no mean pressure gradient. Grid and initial
+    field as abl_case."""
+    cfg, nodes, ucat, p = abl_case(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, H=H, wall=wall, **kw)
+    b = list(cfg.bc); b[4], b[5] = BC_FIXED_VALUE, BC_ZERO_GRADIENT
+    nb = list(cfg.nut_bc); nb[4], nb[5] = NUTBC_ZEROGRADIENT, NUTBC_ZEROGRADIENT
+    v = [0.0] * 18; v[12] = u_in
+    cfg.bc, cfg.nut_bc, cfg.bc_value = tuple(b), tuple(nb), tuple(v)
+    cfg.mean_grad_p, cfg.mean_grad_p_value = 0, (0.0, 0.0, 0.0)
     return cfg, nodes, ucat, p
 
 
