@@ -219,7 +219,11 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     *out = nullptr;
     if (cfg->mx < 6 || cfg->my < 6 || cfg->mz < 6) return TG_ERR_BAD_ARG;
     if ((int64_t)cfg->mx * cfg->my * cfg->mz > (int64_t)INT32_MAX / 4) return TG_ERR_BAD_ARG;
-    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > 3) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
+    // the inflow/outflow patches with the explicit schemes only
+    for (int p = 0; p < 6; p++)
+        if ((cfg->bc[p] == TG_BC_FIXED_VALUE || cfg->bc[p] == TG_BC_ZERO_GRADIENT) &&
+            cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
@@ -253,6 +257,7 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         g.pk = cfg->bc[TG_KLEFT] == TG_BC_PERIODIC;
         Params &p = C->prm;
         for (int q = 0; q < 6; q++) { p.bc[q] = cfg->bc[q]; p.nut_bc[q] = cfg->nut_bc[q]; p.nut_bc_value[q] = cfg->nut_bc_value[q]; }
+        for (int q = 0; q < 18; q++) p.bc_value[q] = cfg->bc_value[q];
         p.curvilinear = cfg->curvilinear; p.les = cfg->les; p.div_scheme = cfg->div_scheme;
         p.buoyancy = cfg->buoyancy; p.mean_grad_p = cfg->mean_grad_p; p.source = cfg->source;
         p.cs = cfg->cs; p.nu = cfg->nu; p.dt = cfg->dt; p.t_ref = cfg->t_ref;

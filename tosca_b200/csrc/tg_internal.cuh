@@ -98,6 +98,7 @@ struct State {
 
 struct Params {
     int bc[6];
+    double bc_value[18];           // TG_BC_FIXED_VALUE: Cartesian velocity of patch p at [3p, 3p+2]
     int nut_bc[6];
     double nut_bc_value[6];
     int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source, farm;
@@ -336,6 +337,7 @@ void reset_face_periodic(tg_ctx *C, V3f<double> v);
 void reset_no_penetration(tg_ctx *C);
 void update_cartesian_bcs(tg_ctx *C);
 void update_contravariant_bcs(tg_ctx *C);
+void adjust_fluxes(tg_ctx *C);               // adjustFluxesLocal (inflow/outflow patches only)
 void update_scalar_ghosts(tg_ctx *C, double *v);
 void update_nut(tg_ctx *C);
 void update_wall_models(tg_ctx *C);
@@ -375,6 +377,8 @@ constexpr int SC_PHIST = 96;
 constexpr int SC_TWALL = 24;       // 24..26 plane means, 27 qWall, 28 surface temperature (-4)
 // number of transposed-solve solutions in the adjoint guess history
 constexpr int SC_LHIST = 76;
+// adjustFluxesLocal: total inflow and outflow through the inflow/outflow patches
+constexpr int SC_FLUX = 100;
 constexpr int SC_GIT = SC_G + ST_IT, SC_GRES0 = SC_G + ST_RES0, SC_GRES = SC_G + ST_RES, SC_GTOT = SC_G + ST_TOT,
               SC_GNOCONV = SC_G + ST_NOCONV, SC_GNAN = SC_G + ST_NAN;
 void poisson_solve_adjoint_capture(tg_ctx *C, const double *rhs, double *lam, double rtol);

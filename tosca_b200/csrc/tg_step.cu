@@ -176,6 +176,13 @@ __global__ void k_cartesian_bcs(Grid g, Metrics m, State s, Params p)
     } else if (type == TG_BC_NOSLIP) {
         // boundary.c:1855-1895
         st3(s.ucat, ghost, -1.0 * U);
+    } else if (type == TG_BC_FIXED_VALUE) {
+        // fixedValue, boundary.c:1632-1673: the ghost takes the patch value
+        st3(s.ucat, ghost, R3<double>{p.bc_value[3 * patch], p.bc_value[3 * patch + 1], p.bc_value[3 * patch + 2]});
+    } else if (type == TG_BC_ZERO_GRADIENT) {
+        // zeroGradient (outflow), boundary.c:1897-1970: linear extrapolation
+        // from the first two cells
+        st3(s.ucat, ghost, 2.0 * U - ld3(s.ucat, right ? c - step : c + step));
     } else {
         // periodic, boundary.c:1990-2018: ghost <- first interior cell of the opposite side
         int src;
@@ -220,7 +227,10 @@ __global__ void k_contra_bc_faces(Grid g, Metrics m, State s, Params p, int dir)
         if (is_wall(type)) { u[f] = 0.0; continue; }
         R3<double> un = ld3(s.ucat, f + step), uc = ld3(s.ucat, f);
         R3<double> S = dir == 0 ? ld3(m.icsi, f) : (dir == 1 ? ld3(m.jeta, f) : ld3(m.kzet, f));
-        u[f] = 0.5 * (un.x + uc.x) * S.x + 0.5 * (un.y + uc.y) * S.y + 0.5 * (un.z + uc.z) * S.z;
+        double v = 0.5 * (un.x + uc.x) * S.x + 0.5 * (un.y + uc.y) * S.y + 0.5 * (un.z + uc.z) * S.z;
+        // zeroGradient: no flow back in through the face, boundary.c:718-741
+        if (type == TG_BC_ZERO_GRADIENT && (side ? v < 0.0 : v > 0.0)) v = 0.0;
+        u[f] = v;
     }
 }
 
@@ -860,10 +870,11 @@ __global__ void __launch_bounds__(256) k_rhs_faces(Grid g, FaceMet<MR> m, State 
     auto finish = [&](double ox, double oy, double oz) {
         if (kind == 2) {
             // resetNonResolvedCellFaces (inline.h:1674-1835) on the + faces of
-            // the last interior cells of a non-periodic direction
-            if (!g.pi && i == g.mx - 2 && !(s.ucont_o.x[c] > 0)) ox = 0.0;
-            if (!g.pj && j == g.my - 2 && !(s.ucont_o.y[c] > 0)) oy = 0.0;
-            if (!g.pk && k == g.mz - 2 && !(s.ucont_o.z[c] > 0)) oz = 0.0;
+            // the last interior cells of a non-periodic direction (kept for
+            // outflow and on a zeroGradient patch)
+            if (!g.pi && i == g.mx - 2 && !(p.bc[TG_IRIGHT] == TG_BC_ZERO_GRADIENT || s.ucont_o.x[c] > 0)) ox = 0.0;
+            if (!g.pj && j == g.my - 2 && !(p.bc[TG_JRIGHT] == TG_BC_ZERO_GRADIENT || s.ucont_o.y[c] > 0)) oy = 0.0;
+            if (!g.pk && k == g.mz - 2 && !(p.bc[TG_KRIGHT] == TG_BC_ZERO_GRADIENT || s.ucont_o.z[c] > 0)) oz = 0.0;
             rk_point(s.ucont.x + c, s.utmp.x + c, s.ucont_o.x + c, ox, rk);
             rk_point(s.ucont.y + c, s.utmp.y + c, s.ucont_o.y + c, oy, rk);
             rk_point(s.ucont.z + c, s.utmp.z + c, s.ucont_o.z + c, oz, rk);
@@ -971,10 +982,90 @@ __global__ void k_rk_shell(Grid g, State s, RkArgs rk)
     rk_point(s.ucont.z + c, s.utmp.z + c, s.ucont_o.z + c, 0.0, rk);
 }
 
+// ------------------------------------------------------------------------
+// adjustFluxesLocal (ueqn.c:748-1135) on the inflow/outflow patches
+// (fixedValue, zeroGradient: the non-periodic, non-wall patch type 0). The
+// faces of a patch are split by the sign of their flux into inflow (into the
+// domain) and outflow; the outflow faces take the imbalance FluxOut - FluxIn
+// in proportion to their own flux, so that the boundary fluxes sum to zero.
+// Pass 1 (blockIdx.y = patch): per-block inflow/outflow sums, faces of zero
+// (or non-finite) flux set to zero; pass 2 (one block): the totals in a fixed
+// order into sc[0] (in) and sc[1] (out); pass 3: the outflow correction.
+// ------------------------------------------------------------------------
+constexpr int AF_BLOCKS = 32;   // pass-1 blocks per patch
+
+__device__ __forceinline__ bool inout_patch(const Params &p, int patch)
+{
+    return p.bc[patch] == TG_BC_FIXED_VALUE || p.bc[patch] == TG_BC_ZERO_GRADIENT;
+}
+// the boundary face (a, b) of a patch (interior range 1..m-2 in both plane
+// directions): its contravariant component array and index
+__device__ __forceinline__ double *patch_face(const Grid &g, const State &s, int dir, int right, int a, int b, int &f)
+{
+    if (dir == 2) { f = g.lin(right ? g.mz - 2 : 0, b, a); return s.ucont.z; }
+    if (dir == 1) { f = g.lin(b, right ? g.my - 2 : 0, a); return s.ucont.y; }
+    f = g.lin(b, a, right ? g.mx - 2 : 0);
+    return s.ucont.x;
+}
+__device__ __forceinline__ void patch_extent(const Grid &g, int dir, int &na, int &nb)
+{
+    na = (dir == 0 ? g.my : g.mx) - 2;
+    nb = (dir == 2 ? g.my : g.mz) - 2;
+}
+
+__global__ void __launch_bounds__(256) k_flux_sums(Grid g, State s, Params p, double *part)
+{
+    const int patch = blockIdx.y, dir = patch >> 1, right = patch & 1;
+    double v[2] = {0.0, 0.0};    // inflow, outflow
+    if (inout_patch(p, patch)) {
+        int na, nb;
+        patch_extent(g, dir, na, nb);
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na * nb; t += gridDim.x * blockDim.x) {
+            int f;
+            double *u = patch_face(g, s, dir, right, t % na + 1, t / na + 1, f);
+            const double x = u[f];
+            if (x > 0.0) v[right ? 1 : 0] += x;
+            else if (x < 0.0) v[right ? 0 : 1] += -x;
+            else u[f] = 0.0;
+        }
+    }
+    block_reduce<256>(v, RedSum{}, RedSum{});
+    if (threadIdx.x == 0) {
+        const int q = patch * gridDim.x + blockIdx.x;
+        part[2 * q] = v[0];
+        part[2 * q + 1] = v[1];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_flux_total(const double *part, int n, double *sc)
+{
+    double v[2] = {0.0, 0.0};
+    for (int q = threadIdx.x; q < n; q += blockDim.x) { v[0] += part[2 * q]; v[1] += part[2 * q + 1]; }
+    block_reduce<256>(v, RedSum{}, RedSum{});
+    if (threadIdx.x == 0) { sc[0] = v[0]; sc[1] = v[1]; }
+}
+
+__global__ void k_flux_correct(Grid g, State s, Params p, const double *sc)
+{
+    const int patch = blockIdx.y, dir = patch >> 1, right = patch & 1;
+    if (!inout_patch(p, patch)) return;
+    int na, nb;
+    patch_extent(g, dir, na, nb);
+    const double in = sc[0], out = sc[1], gf = out - in;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na * nb; t += gridDim.x * blockDim.x) {
+        int f;
+        double *u = patch_face(g, s, dir, right, t % na + 1, t / na + 1, f);
+        const double x = u[f];
+        if (!right && x < 0.0) u[f] = x + gf * (-x / out);
+        if (right && x > 0.0) u[f] = x - gf * (x / out);
+    }
+}
+
 // resetNonResolvedCellFaces (inline.h:1674-1835) on the boundary planes of one
-// direction: face 0 kept only for outflow, face m-1 unused, face m-2 of a
-// non-periodic direction kept only for outflow.
-__global__ void k_non_resolved(Grid g, State s, int dir)
+// direction: face 0 kept only for outflow or on a zeroGradient patch, face m-1
+// unused, face m-2 of a non-periodic direction kept only for outflow or on a
+// zeroGradient patch.
+__global__ void k_non_resolved(Grid g, State s, Params p, int dir)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y * blockDim.y + threadIdx.y;
     int na = dir == 0 ? g.my : g.mx, nb = dir == 2 ? g.my : g.mz;
@@ -984,9 +1075,10 @@ __global__ void k_non_resolved(Grid g, State s, int dir)
     double *v = dir == 0 ? s.rhs.x : (dir == 1 ? s.rhs.y : s.rhs.z);
     const double *uo = dir == 0 ? s.ucont_o.x : (dir == 1 ? s.ucont_o.y : s.ucont_o.z);
     auto at = [&](int l) { return dir == 0 ? g.lin(b, a, l) : (dir == 1 ? g.lin(b, l, a) : g.lin(l, b, a)); };
-    { int q = at(0); if (!(uo[q] < 0)) v[q] = 0.0; }
+    const bool zgl = p.bc[2 * dir] == TG_BC_ZERO_GRADIENT, zgr = p.bc[2 * dir + 1] == TG_BC_ZERO_GRADIENT;
+    { int q = at(0); if (!(zgl || uo[q] < 0)) v[q] = 0.0; }
     { int q = at(m - 1); v[q] = 0.0; }
-    if (!per) { int q = at(m - 2); if (!(uo[q] > 0)) v[q] = 0.0; }
+    if (!per) { int q = at(m - 2); if (!(zgr || uo[q] > 0)) v[q] = 0.0; }
 }
 
 
@@ -1274,6 +1366,18 @@ void update_contravariant_bcs(tg_ctx *C)
     }
 }
 
+void adjust_fluxes(tg_ctx *C)
+{
+    bool any = false;
+    for (int q = 0; q < 6; q++) any |= C->prm.bc[q] == TG_BC_FIXED_VALUE || C->prm.bc[q] == TG_BC_ZERO_GRADIENT;
+    if (!any) return;
+    const Grid g = C->g;
+    static_assert(6 * AF_BLOCKS * 2 <= 4 * 148 * 4, "partials fit the reduction scratch");
+    TG_PROF(C, "bc_adjust_fluxes", k_flux_sums<<<dim3(AF_BLOCKS, 6), 256, 0, C->stream>>>(g, C->s, C->prm, C->d_red));
+    k_flux_total<<<1, 256, 0, C->stream>>>(C->d_red, 6 * AF_BLOCKS, C->d_scal + SC_FLUX);
+    TG_PROF(C, "bc_adjust_fluxes", k_flux_correct<<<dim3(AF_BLOCKS, 6), 256, 0, C->stream>>>(g, C->s, C->prm, C->d_scal + SC_FLUX));
+}
+
 void update_scalar_ghosts(tg_ctx *C, double *v)
 {
     const Grid g = C->g;
@@ -1414,9 +1518,9 @@ void explicit_rhs(tg_ctx *C, int mode)
     const Grid g = C->g;
     explicit_rhs_head(C, mode);
     rhs_faces<1>(C, C->s.rhs, 1.0, C->it > C->cfg.it_start ? 1 : 0);
-    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, 0));
-    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, 1));
-    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, 2));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, C->s, C->prm, 0));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, C->s, C->prm, 1));
+    TG_PROF(C, "bc_non_resolved", k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, C->s, C->prm, 2));
 }
 
 // ExplicitRhsU followed by one explicit update (an RK4 stage or the FE step)
@@ -1437,9 +1541,9 @@ void mask_non_resolved(tg_ctx *C, V3f<double> v)
     const Grid g = C->g;
     State s = C->s;
     s.rhs = v;
-    k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, s, 0);
-    k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, s, 1);
-    k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, s, 2);
+    k_non_resolved<<<g2(g.my, g.mz), b2, 0, C->stream>>>(g, s, C->prm, 0);
+    k_non_resolved<<<g2(g.mx, g.mz), b2, 0, C->stream>>>(g, s, C->prm, 1);
+    k_non_resolved<<<g2(g.mx, g.my), b2, 0, C->stream>>>(g, s, C->prm, 2);
 }
 
 // constant part of the Crank-Nicolson residual (UeqnSNES, ueqn_solvers.c:1097-1163):
@@ -1523,6 +1627,7 @@ static int solve_u_impl(tg_ctx *C, bool cart_tail, tg_stats *st = nullptr)
         TG_PROF(C, "contra_to_cart_shell", k_contra_to_cart_shell<<<grid, b2, 0, C->stream>>>(g, C->fm64, C->s, C->axis_aligned));
     }
     reset_cell_periodic(C, C->s.ucat);
+    adjust_fluxes(C);                  // ueqn.c:437
     return rc;
 }
 
