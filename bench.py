@@ -206,6 +206,18 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="
         desc = ("stable ABL %dx%dx%d cells, RK4, Smagorinsky, Schumann wall with Monin-Obukhov stability, "
                 "transported potential temperature (RK4, WENO3) with Boussinesq buoyancy and a "
                 "Schumann-Grotzbach thetaWallFunction (surface cooling 0.25 K/h), dt=0.25 s" % (cfg.mz - 2, cfg.mx - 2, cfg.my - 2))
+    elif name == "channel":
+        kw = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=250.0) if small else dict(
+            nx=256, ny=256, nz=128, Lx=2560.0, Ly=2560.0, H=1000.0)
+        if cells:
+            nx, ny, nz = cells
+            kw = dict(nx=nx, ny=ny, nz=nz, Lx=10.0 * nx, Ly=10.0 * ny, H=1000.0 * nz / 128.0)
+        cfg, nodes, ucat, p = cases.channel_case(ddt=api.DDT_RK4, seed=20261203 + seed_offset,
+                                                 wall=api.BC_WALL_SHUMANN, **kw)
+        T = None
+        desc = ("open channel %dx%dx%d cells (the ABL grid): fixedValue inflow 8 m/s at x = 0, zeroGradient "
+                "outflow at x = Lx (adjustFluxesLocal), RK4, Smagorinsky, Schumann wall, dt=0.25 s" % (
+                    cfg.mz - 2, cfg.mx - 2, cfg.my - 2))
     elif name == "tgv":
         cfg, nodes, ucat, p = cases.tgv_case(32 if small else 64, ddt=api.DDT_RK4)
         T = None
@@ -522,7 +534,7 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm", "sabl"])
+    ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm", "sabl", "channel"])
     ap.add_argument("--ddt", default="rk4", choices=["rk4", "cn", "abcn", "rk3wcn", "rk3socn"], help="momentum time scheme of the workload")
     ap.add_argument("--farm-adjoint-steps", type=int, default=200,
                     help="farm workload: steps of the C_T' gradient of the summed farm power")
