@@ -2,7 +2,8 @@
 (oracle/_ref/libtosca_ref.so, built from the reference checkout by
 oracle/refstub; see tests/test_ref_pin.py): three FE / RK4 time steps on the
 Taylor-Green box, the ABL with Smagorinsky, the Schumann wall stress and the
-mean pressure gradient, and the curvilinear QUICK hill, plus the ABL at
+mean pressure gradient, the curvilinear QUICK hill and the open channel
+(fixedValue inflow, zeroGradient outflow, adjustFluxesLocal), plus the ABL at
 64 x 64 x 32 cells, which spans several blocks of every kernel. The harness
 is used as built (it travels with the tree); without it the tests skip."""
 import pytest
@@ -43,7 +44,8 @@ def _run(name, ddt, **kw):
 
 
 @pytest.mark.parametrize("name,ddt", [("tgv", api.DDT_FE), ("tgv", api.DDT_RK4), ("abl", api.DDT_RK4),
-                                      ("hill", api.DDT_FE), ("hill", api.DDT_RK4)])
+                                      ("hill", api.DDT_FE), ("hill", api.DDT_RK4),
+                                      ("channel", api.DDT_FE), ("channel", api.DDT_RK4)])
 def test_gpu_steps_against_reference_code(name, ddt):
     g, r, sg, sr = _run(name, ddt, **SMALL[name])
     for f in ("UCONT", "UCAT"):
