@@ -45,6 +45,28 @@ def test_channel_ten_steps(ddt, wall, div):
     g.close(); o.close()
 
 
+@pytest.mark.parametrize("localized", [False, True])
+def test_stratified_channel(localized):
+    """The stratified ABL opened in x (cases.open_x: 8 m/s at 301 K through
+    the fixedValue inflow, zeroGradient outflow for velocity and temperature)
+    with the RK4 temperature equation, Boussinesq buoyancy and the
+    Schumann-Grotzbach thermal wall function on the ground: ten steps, GPU
+    against the oracle (itself pinned to TOSCA's own code on this case)."""
+    cfg, nodes, ucat, p, T = cases.stratified_abl_case(16, 12, 12, heating_rate=-0.01, localized=localized, t_amp=0.5)
+    cases.open_x(cfg, 8.0, 301.0)
+    cfg.poisson_rtol = 1e-13
+    g = tosca_b200.gpu_solver(cfg)
+    o = oracle.solver(cfg)
+    for s in (g, o):
+        cases.setup(s, nodes, ucat, p, T)
+        s.step(10)
+    for f in ("UCAT", "P", "TMPRT"):
+        assert rel_l2(g.get(f), o.get(f)) < 1e-10, f
+    qg, qo = g.get("QWALL"), o.get("QWALL")
+    assert np.abs(qg - qo).max() <= 1e-9 * np.abs(qo).max()
+    g.close(); o.close()
+
+
 def test_channel_multiblock_mixed():
     """A channel spanning several blocks of every kernel (48 x 40 x 16 cells:
     two blocks of the face-flux kernel in i), RK4, FP64 within 1e-10 and

@@ -223,9 +223,12 @@ def test_unsupported_configuration_is_refused():
 
 # ---------------------------------------------------------------- temperature
 def _pair_t(case, kind=api.TWALL_SHUMANN, heating_rate=-0.01, localized=False, qwall=0.0, p_tilde=0):
-    if case == "sabl":
+    if case in ("sabl", "schannel"):
         cfg, nodes, ucat, p, T = cases.stratified_abl_case(16, 12, 12, heating_rate=heating_rate, localized=localized,
                                                            t_amp=0.5)
+        if case == "schannel":
+            # inflow 8 m/s at 301 K through x = 0, outflow at x = Lx
+            cases.open_x(cfg, 8.0, 301.0)
     else:
         cfg, nodes, ucat, p, T = cases.hill_case(24, 12, 12, teqn=True, t_amp=0.5)
         if kind is not None:
@@ -297,6 +300,8 @@ def test_monin_obukhov_functions():
     ("sabl", api.TWALL_SHUMANN, False, -0.01, 0.0),      # cooling surface: stable
     ("sabl", api.TWALL_SHUMANN, True, 0.02, 0.0),        # heating surface: unstable, per cell
     ("sabl", api.TWALL_FIXED_FLUX, False, 0.0, 0.05),
+    ("schannel", api.TWALL_SHUMANN, False, -0.01, 0.0),  # open channel: inflow temperature, outflow
+    ("schannel", api.TWALL_SHUMANN, True, -0.01, 0.0),
     ("hill", api.TWALL_SHUMANN, False, -0.01, 0.0),
     ("hill", api.TWALL_SHUMANN, True, -0.01, 0.0),
     ("hill", None, False, 0.0, 0.0),                     # temperature without a wall function

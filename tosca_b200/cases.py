@@ -24,7 +24,7 @@ import math
 import numpy as np
 
 from .api import (BC_FIXED_VALUE, BC_NOSLIP, BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, BC_ZERO_GRADIENT, DDT_FE,
-                  DDT_RK4, DIV_CENTRAL, DIV_QUICK, NUTBC_FIXEDVALUE, NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, TBC_FIXED_GRADIENT, TBC_PERIODIC, TBC_WALL_FUNCTION,
+                  DDT_RK4, DIV_CENTRAL, DIV_QUICK, NUTBC_FIXEDVALUE, NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, TBC_FIXED_GRADIENT, TBC_FIXED_VALUE, TBC_PERIODIC, TBC_WALL_FUNCTION,
                   TBC_ZERO_GRADIENT, TWALL_FIXED_FLUX, TWALL_SHUMANN, Config)
 
 
@@ -196,12 +196,26 @@ def channel_case(nx: int = 256, ny: int = 128, nz: int = 64, Lx: float = 2560.0,
     inflow and outflow patches, no mean pressure gradient. Grid and initial
     field as abl_case."""
     cfg, nodes, ucat, p = abl_case(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, H=H, wall=wall, **kw)
+    open_x(cfg, u_in)
+    return cfg, nodes, ucat, p
+
+
+def open_x(cfg: Config, u_in: float = 8.0, t_in: float = None) -> Config:
+    """Turns the periodic x (k) direction of a case into an inflow/outflow
+    pair: fixedValue velocity (u_in, 0, 0) at x = 0, zeroGradient at x = Lx,
+    zero-gradient nut on both; with the temperature equation, a fixedValue
+    temperature t_in at the inflow and zeroGradient at the outflow. The mean
+    pressure gradient is switched off."""
     b = list(cfg.bc); b[4], b[5] = BC_FIXED_VALUE, BC_ZERO_GRADIENT
     nb = list(cfg.nut_bc); nb[4], nb[5] = NUTBC_ZEROGRADIENT, NUTBC_ZEROGRADIENT
     v = [0.0] * 18; v[12] = u_in
     cfg.bc, cfg.nut_bc, cfg.bc_value = tuple(b), tuple(nb), tuple(v)
     cfg.mean_grad_p, cfg.mean_grad_p_value = 0, (0.0, 0.0, 0.0)
-    return cfg, nodes, ucat, p
+    if cfg.teqn:
+        tb = list(cfg.t_bc); tb[4], tb[5] = TBC_FIXED_VALUE, TBC_ZERO_GRADIENT
+        tv = list(cfg.t_bc_value); tv[4] = cfg.t_ref if t_in is None else t_in
+        cfg.t_bc, cfg.t_bc_value = tuple(tb), tuple(tv)
+    return cfg
 
 
 def farm_case(nx: int = 384, ny: int = 256, nz: int = 128, Lx: float = 3840.0, Ly: float = 2560.0,
