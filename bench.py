@@ -186,7 +186,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="rk4"):
+def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="rk4", open_x=False):
     from tosca_b200 import api, cases
     if name == "abl":
         kw = dict(nx=64, ny=64, nz=32, Lx=640.0, Ly=640.0, H=250.0) if small else {}
@@ -240,6 +240,11 @@ def make_workload(name, precision, seed_offset=0, small=False, cells=None, ddt="
         raise SystemExit(f"unknown workload {name}")
     if name != "farm":
         turbines = None
+    if open_x and name != "channel":
+        # the inflow/outflow pair of TOSCA's hill and turbine decks
+        # (CosineHillCurvTest, NREL5MWTest: kLeft fixedValue, kRight zeroGradient)
+        cases.open_x(cfg, 8.0, None)
+        desc += "; x open: fixedValue inflow 8 m/s, zeroGradient outflow (adjustFluxesLocal)"
     if ddt == "cn":                   # ddtScheme CN with the reference's SNES defaults (ueqn.c:128-130)
         cfg.ddt_scheme = api.DDT_CN
         cfg.snes_atol, cfg.snes_rtol, cfg.snes_maxit = 1e-5, 1e-30, 20
@@ -272,7 +277,7 @@ def cpu_model() -> str:
     return platform.processor() or platform.machine()
 
 
-def cpu_baseline(workload, steps, full=False, cells=None):
+def cpu_baseline(workload, steps, full=False, cells=None, open_x=False):
     """CPU restatement of the reference step (the oracle, OpenMP on all host
     threads) on the workload: the full configuration (`full`), or a bounded
     sample of it (the ABL at 128 x 128 x 64 cells with the same 10 m spacing
@@ -283,11 +288,11 @@ def cpu_baseline(workload, steps, full=False, cells=None):
     import oracle
     from tosca_b200 import cases
     if full:
-        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=cells)
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=cells, open_x=open_x)
     elif workload == "abl":
-        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=(128, 128, 64))
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", cells=(128, 128, 64), open_x=open_x)
     else:
-        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", small=True)
+        cfg, nodes, ucat, p, T, desc, turbines = make_workload(workload, "fp64", small=True, open_x=open_x)
     cfg.poisson_rtol = 1e-8          # the reference's default poissonTol (peqn.c:54)
     cfg.poisson_div_tol = 0.0
     cfg.poisson_maxit = 20000
@@ -339,7 +344,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     steps = max(1, min(args.steps, 2))
-    base = cpu_baseline(args.workload, steps, full=True, cells=args.cells)
+    base = cpu_baseline(args.workload, steps, full=True, cells=args.cells, open_x=args.open_x)
     line = {
         "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": 1, "ms_per_step": base["seconds"] / steps * 1e3, "higher_is_better": True,
@@ -535,6 +540,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="abl", choices=["abl", "tgv", "hill", "farm", "sabl", "channel"])
+    ap.add_argument("--open-x", action="store_true",
+                    help="replace the periodic x direction by a fixedValue inflow and a zeroGradient outflow")
     ap.add_argument("--ddt", default="rk4", choices=["rk4", "cn", "abcn", "rk3wcn", "rk3socn"], help="momentum time scheme of the workload")
     ap.add_argument("--farm-adjoint-steps", type=int, default=200,
                     help="farm workload: steps of the C_T' gradient of the summed farm power")
@@ -590,7 +597,7 @@ def main():
 
     def arm(precision):
         cfg, nodes, ucat, p, T, desc, turbines = make_workload(args.workload, precision, seed_offset=rank, cells=args.cells,
-                                                               ddt=args.ddt)
+                                                               ddt=args.ddt, open_x=args.open_x)
         cfg.device = dev
         solver = tosca_b200.gpu_solver(cfg)
         cases.setup(solver, nodes, ucat, p, T)
@@ -690,7 +697,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(args.workload, args.cpu_steps)
+        base = cpu_baseline(args.workload, args.cpu_steps, open_x=args.open_x)
         cpu = {k: base[k] for k in ("value", "unit", "cores", "cpu_model", "kind", "sample")}
 
     if rank == 0:

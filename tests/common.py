@@ -49,6 +49,11 @@ def build_case(name: str, **kw):
     if name == "channel":
         cfg, nodes, ucat, p = cases.channel_case(**kw)
         return cfg, nodes, ucat, p, None
+    if name == "ohill":
+        # the hill with the inflow/outflow pair of TOSCA's CosineHillCurvTest deck
+        cfg, nodes, ucat, p, T = cases.hill_case(**kw)
+        cases.open_x(cfg, 8.0)
+        return cfg, nodes, ucat, p, T
     raise ValueError(name)
 
 
@@ -71,4 +76,5 @@ SMALL = {
     "hill": dict(nx=24, ny=12, nz=12),
     # inflow at x = 0, outflow at x = Lx, noSlip ground (cases.channel_case)
     "channel": dict(nx=20, ny=12, nz=10, Lx=200.0, Ly=120.0, H=100.0),
+    "ohill": dict(nx=24, ny=12, nz=12),
 }

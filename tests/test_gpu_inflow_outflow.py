@@ -67,6 +67,29 @@ def test_stratified_channel(localized):
     g.close(); o.close()
 
 
+@pytest.mark.parametrize("prec", [api.PREC_FP64, api.PREC_MIXED])
+def test_open_hill(prec):
+    """The curvilinear QUICK hill with the inflow/outflow pair of TOSCA's
+    CosineHillCurvTest deck (fixedValue inflow, zeroGradient outflow; the
+    general-metric kernels and the BiCGStab pressure solve), RK4 with the
+    transported temperature (inflow at 301 K), ten steps: FP64 within 1e-10
+    of the oracle (P 1e-9, as on the periodic hill), mixed within 1e-6."""
+    cfg, nodes, ucat, p, T = cases.hill_case(24, 12, 12, ddt=api.DDT_RK4, teqn=True, t_amp=0.5)
+    cases.open_x(cfg, 8.0, 301.0)
+    cfg.poisson_rtol = 1e-13
+    cfg.precision = prec
+    g = tosca_b200.gpu_solver(cfg)
+    o = oracle.solver(cfg)
+    for s in (g, o):
+        cases.setup(s, nodes, ucat, p, T)
+        s.step(10)
+    tol = 1e-10 if prec == api.PREC_FP64 else 1e-6
+    for f in ("UCAT", "TMPRT"):
+        assert rel_l2(g.get(f), o.get(f)) < tol, f
+    assert rel_l2(g.get("P"), o.get("P")) < (1e-9 if prec == api.PREC_FP64 else 1e-6)
+    g.close(); o.close()
+
+
 def test_channel_multiblock_mixed():
     """A channel spanning several blocks of every kernel (48 x 40 x 16 cells:
     two blocks of the face-flux kernel in i), RK4, FP64 within 1e-10 and

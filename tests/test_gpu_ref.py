@@ -24,7 +24,7 @@ def _run(name, ddt, **kw):
     cfg.ddt_scheme = ddt
     if cfg.les:
         cfg.cs = 0.0289                    # the reference's hard-coded Cs^2 (les.c:10)
-    if name == "hill":
+    if name in ("hill", "ohill"):
         cfg.buoyancy = 0                   # the reference applies it with its T equation only
     o = oracle.solver(cfg)
     cases.setup(o, nodes, ucat, p, T)      # initial state as SetInitialField restates it
@@ -45,12 +45,13 @@ def _run(name, ddt, **kw):
 
 @pytest.mark.parametrize("name,ddt", [("tgv", api.DDT_FE), ("tgv", api.DDT_RK4), ("abl", api.DDT_RK4),
                                       ("hill", api.DDT_FE), ("hill", api.DDT_RK4),
-                                      ("channel", api.DDT_FE), ("channel", api.DDT_RK4)])
+                                      ("channel", api.DDT_FE), ("channel", api.DDT_RK4),
+                                      ("ohill", api.DDT_RK4)])
 def test_gpu_steps_against_reference_code(name, ddt):
     g, r, sg, sr = _run(name, ddt, **SMALL[name])
     for f in ("UCONT", "UCAT"):
         assert rel_l2(g.get(f), r.get(f)) < 1e-11, f
-    assert rel_l2(g.get("P"), r.get("P")) < (1e-9 if name == "hill" else 1e-10)
+    assert rel_l2(g.get("P"), r.get("P")) < (1e-9 if name in ("hill", "ohill") else 1e-10)
     assert sg.max_divergence < 1e-12
     g.close(); r.close()
 
