@@ -20,7 +20,9 @@ pytestmark = [pytest.mark.gpu,
 
 def _run(name, ddt, **kw):
     cfg, nodes, ucat, p, T = build_case(name, **kw)
-    cfg.poisson_rtol = 1e-14
+    # the open curvilinear hill's BiCGStab stalls a little above 1e-14 (the
+    # attainable residual with open boundaries), so it solves to 1e-13
+    cfg.poisson_rtol = 1e-13 if name == "ohill" else 1e-14
     cfg.ddt_scheme = ddt
     if cfg.les:
         cfg.cs = 0.0289                    # the reference's hard-coded Cs^2 (les.c:10)
