@@ -55,9 +55,13 @@ enum {
      * (TG_DDT_FE, TG_DDT_RK4) only, no adjoint                                  */
     TG_BC_FIXED_VALUE     = 4,  /* "fixedValue": ghost cell = bc_value of the      */
                                 /* patch (boundary.c:1632-1673), an inflow          */
-    TG_BC_ZERO_GRADIENT   = 5   /* "zeroGradient": ghost 2 U(1) - U(2)             */
+    TG_BC_ZERO_GRADIENT   = 5,  /* "zeroGradient": ghost 2 U(1) - U(2)             */
                                 /* (boundary.c:1897-1970), reverse flow through the */
                                 /* face set to zero (boundary.c:718-741), an outflow */
+    TG_BC_INLET_LOG       = 6   /* "inletFunction" type 2 on kLeft only: log-law    */
+                                /* ghost (uTau/0.4) ln(h/z0) Udir, h the first      */
+                                /* cell's height above the ground, constant above   */
+                                /* hInv (boundary.c:1253-1283), an inflow           */
 };
 /* eddy-viscosity patch types (boundary/nut) */
 enum {
@@ -190,6 +194,12 @@ typedef struct tg_config {
     double  t_start;               /* -startTime: clock time at it_start (thetaWallFunction -4) */
     double  bc_value[18];          /* TG_BC_FIXED_VALUE: Cartesian velocity (x, y, z) of  */
                                    /* patch p at [3p, 3p+2] (boundaryU *val, boundary.c)  */
+    /* TG_BC_INLET_LOG (inletFunction type 2, boundary/U): uTau, roughness,
+     * hInv (the profile is constant above it) and the unit direction Udir */
+    double  inlet_u_tau;
+    double  inlet_z0;
+    double  inlet_h_inv;
+    double  inlet_dir[3];
 } tg_config;
 
 /* per-call statistics */

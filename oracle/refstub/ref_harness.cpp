@@ -11,7 +11,8 @@
 // InitializePEqn, peqn.c:35-103; InitializeLES, les.c:20-150; InitializeTEqn,
 // teqn.c:19-257; SetWallModels, boundary.c:4640-5200), with the values a
 // control.dat and boundary/ files would hold, and then calls the reference's
-// functions. Supported: periodic, slip, noSlip, fixedValue, zeroGradient and the Schumann velocity wall
+// functions. Supported: periodic, slip, noSlip, fixedValue, zeroGradient, the kLeft
+// log-law inletFunction (type 2) and the Schumann velocity wall
 // function (-3, averaged u*) on jLeft; central and QUICK convection; FE and
 // RK4; no LES or Smagorinsky (TOSCA's hard-coded Cs^2 = 0.0289,
 // les.c:10,175); the mean pressure gradient; the potential temperature
@@ -61,6 +62,7 @@ const char *u_bc_name(int t)
     case TG_BC_WALL_SHUMANN: return "velocityWallFunction";
     case TG_BC_FIXED_VALUE: return "fixedValue";
     case TG_BC_ZERO_GRADIENT: return "zeroGradient";
+    case TG_BC_INLET_LOG: return "inletFunction";
     default: return "";
     }
 }
@@ -153,6 +155,7 @@ struct tg_ctx {
     std::unique_ptr<domain_> dom;
     clock_ clock{};
     io_ *io = nullptr;
+    std::unique_ptr<inletFunctionTypes> inlet;
     mesh_ mesh{};
     ueqn_ ueqn{};
     peqn_ peqn{};
@@ -269,6 +272,15 @@ void build(tg_ctx &X)
         for (int q = 0; q < 6; q++) {
             vals[q]->x = c.bc_value[3 * q]; vals[q]->y = c.bc_value[3 * q + 1]; vals[q]->z = c.bc_value[3 * q + 2];
         }
+    }
+    // inletFunction type 2 on kLeft (boundary/U inletFunction dictionary, inflow.c:65-72)
+    if (c.bc[4] == TG_BC_INLET_LOG) {
+        X.inlet.reset(new inletFunctionTypes());
+        inletFunctionTypes &f = *X.inlet;
+        f.typeU = 2;
+        f.Udir.x = c.inlet_dir[0]; f.Udir.y = c.inlet_dir[1]; f.Udir.z = c.inlet_dir[2];
+        f.hInv = c.inlet_h_inv; f.uTau = c.inlet_u_tau; f.roughness = c.inlet_z0;
+        m.inletF.kLeft = X.inlet.get();
     }
     m.boundaryU.jLWF = c.bc[2] == TG_BC_WALL_SHUMANN ? -3 : 0;
     m.boundaryU.jRWF = c.bc[3] == TG_BC_WALL_SHUMANN ? -3 : 0;
@@ -444,7 +456,7 @@ tg_status ref_create(const tg_config *cfg, tg_ctx **out)
     const tg_config &c = *cfg;
     if (c.mx < 6 || c.my < 6 || c.mz < 6) return TG_ERR_BAD_ARG;
     for (int q = 0; q < 6; q++) {
-        if (c.bc[q] < 0 || c.bc[q] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
+        if (c.bc[q] < 0 || c.bc[q] > TG_BC_INLET_LOG || (c.bc[q] == TG_BC_INLET_LOG && q != 4)) return TG_ERR_BAD_ARG;
         if (c.bc[q] == TG_BC_WALL_SHUMANN && q != 2) return TG_ERR_BAD_ARG;
     }
     // supported subset of the workloads (see the file header)

@@ -93,6 +93,7 @@ struct tg_ctx {
 
     // metrics (global DMDA extent)
     std::vector<V3> coor, cent, csi, eta, zet, icsi, ieta, izet, jcsi, jeta, jzet, kcsi, keta, kzet;
+    double grnd = 0.0;                          // mesh->grndLevel = bounds.zmin (mesh.c:2014-2063)
     std::vector<double> aj, iaj, jaj, kaj;
     std::vector<double> g11, g12, g13, g21, g22, g23, g31, g32, g33;  // SetCoeffMatrix tensors
 
@@ -841,6 +842,15 @@ void updateCartesianBCs(tg_ctx &C)
         if (j == my - 2) fixedv(TG_JRIGHT, k, j + 1, i);
         if (k == 1)      fixedv(TG_KLEFT, k - 1, j, i);
         if (k == mz - 2) fixedv(TG_KRIGHT, k + 1, j, i);
+        // inletFunction type 2 on kLeft, boundary.c:1253-1283: the log law in
+        // the height of the first cell's centre above the ground, clipped
+        // below at 1e-5 and constant above hInv
+        if (k == 1 && bc[TG_KLEFT] == TG_BC_INLET_LOG) {
+            const double h = C.cent[c].z - C.grnd, kap = 0.4;
+            const double um = h <= C.c.inlet_h_inv ? std::max((C.c.inlet_u_tau / kap) * std::log(h / C.c.inlet_z0), 1e-5)
+                                                   : (C.c.inlet_u_tau / kap) * std::log(C.c.inlet_h_inv / C.c.inlet_z0);
+            C.ucat[C.I(k - 1, j, i)] = mk(um * C.c.inlet_dir[0], um * C.c.inlet_dir[1], um * C.c.inlet_dir[2]);
+        }
         // zeroGradient (outflow), boundary.c:1897-1970: linear extrapolation
         if (i == 1 && bc[TG_ILEFT] == TG_BC_ZERO_GRADIENT)       C.ucat[C.I(k, j, i - 1)] = 2.0 * L(k, j, i) - L(k, j, i + 1);
         if (i == mx - 2 && bc[TG_IRIGHT] == TG_BC_ZERO_GRADIENT) C.ucat[C.I(k, j, i + 1)] = 2.0 * L(k, j, i) - L(k, j, i - 1);
@@ -1979,15 +1989,26 @@ static bool theta_wall_config_ok(const tg_config *cfg)
     return true;
 }
 
+// inletFunction type 2 (inflow.c:65-72): a positive roughness and friction
+// velocity, hInv above the roughness, a unit direction (the reference scales
+// directionU to unit length as it reads it)
+static bool inlet_log_config_ok(const tg_config *cfg)
+{
+    const double *d = cfg->inlet_dir;
+    const double n = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    return cfg->inlet_z0 > 0 && cfg->inlet_u_tau >= 0 && cfg->inlet_h_inv > cfg->inlet_z0 && std::fabs(n - 1.0) < 1e-12;
+}
+
 tg_status tor_create(const tg_config *cfg, tg_ctx **out)
 {
     if (!cfg || !out) return TG_ERR_BAD_ARG;
     *out = nullptr;
     if (cfg->mx < 6 || cfg->my < 6 || cfg->mz < 6) return TG_ERR_BAD_ARG;
-    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_INLET_LOG) return TG_ERR_BAD_ARG;
     for (int p = 0; p < 6; p++)
-        if ((cfg->bc[p] == TG_BC_FIXED_VALUE || cfg->bc[p] == TG_BC_ZERO_GRADIENT) &&
-            cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
+        if (cfg->bc[p] >= TG_BC_FIXED_VALUE && cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++)
+        if (cfg->bc[p] == TG_BC_INLET_LOG && (p != TG_KLEFT || !inlet_log_config_ok(cfg))) return TG_ERR_BAD_ARG;
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     if (cfg->bc[TG_IRIGHT] == TG_BC_WALL_SHUMANN || cfg->bc[TG_ILEFT] == TG_BC_WALL_SHUMANN ||
@@ -2034,6 +2055,10 @@ tg_status tor_set_mesh_nodes(tg_ctx *C, const double *nodes)
         for (int k = 0; k < C->mz; k++) for (int j = 0; j < C->my; j++) for (int i = 0; i < C->mx; i++)
             if (i == C->mx - 1 || j == C->my - 1 || k == C->mz - 1) C->coor[((size_t)k * C->my + j) * C->mx + i] = V3{0, 0, 0};
         setMeshMetrics(*C);
+        // mesh->grndLevel: the lowest node (mesh.c:2014-2063)
+        C->grnd = 1e30;
+        for (int k = 0; k < C->mz - 1; k++) for (int j = 0; j < C->my - 1; j++) for (int i = 0; i < C->mx - 1; i++)
+            C->grnd = std::min(C->grnd, C->coor[((size_t)k * C->my + j) * C->mx + i].z);
         setPoissonConnectivity(*C);
         setCoeffMatrix(*C);
         C->phi1d.assign(C->N, 0.0);
@@ -2369,7 +2394,7 @@ tg_status tor_adjoint_step(tg_ctx *C)
         if (C->c.ddt_scheme == TG_DDT_CN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the Crank-Nicolson scheme is not implemented");
         if (C->c.ddt_scheme >= TG_DDT_ABCN) return fail(C, TG_ERR_BAD_ARG, "the adjoint of the IMEX schemes is not implemented");
         for (int q = 0; q < 6; q++)
-            if (C->c.bc[q] == TG_BC_FIXED_VALUE || C->c.bc[q] == TG_BC_ZERO_GRADIENT)
+            if (C->c.bc[q] >= TG_BC_FIXED_VALUE)
                 return fail(C, TG_ERR_BAD_ARG, "the adjoint of the inflow/outflow patches is not implemented");
         // state saved around the taped forward step
         auto ucont = C->ucont, ucat = C->ucat, btheta = C->btheta, btheta_o = C->btheta_o;

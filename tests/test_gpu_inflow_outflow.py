@@ -168,6 +168,34 @@ def test_channel_replay_bitwise():
     e.close(); r.close()
 
 
+@pytest.mark.parametrize("name,prec", [("channel", api.PREC_FP64), ("channel", api.PREC_MIXED),
+                                       ("ohill", api.PREC_FP64)])
+def test_log_inlet(name, prec):
+    """The kLeft log-law inletFunction (type 2, cases.log_inlet) in place of
+    the fixedValue inflow, hInv = 60 m on the 100 m channel (both branches of
+    the profile) and none on the open hill, a direction with x and y
+    components: ten RK4 steps against the oracle (itself pinned to TOSCA's
+    own code on these cases), FP64 within 1e-10 (P 1e-9 on the hill), mixed
+    within 1e-6; the ghosts after UpdateCartesianBCs within 1e-14."""
+    cfg, nodes, ucat, p, T = build_case(name, **SMALL[name])
+    cases.log_inlet(cfg, 0.4, 0.1, 60.0 if name == "channel" else 1e30, (0.96, 0.28, 0.0))
+    cfg.poisson_rtol = 1e-13
+    cfg.ddt_scheme = api.DDT_RK4
+    cfg.precision = prec
+    g = tosca_b200.gpu_solver(cfg)
+    o = oracle.solver(cfg)
+    for s in (g, o):
+        cases.setup(s, nodes, ucat, p, T)
+        s.UpdateCartesianBCs()
+    assert rel_l2(g.get("UCAT")[0], o.get("UCAT")[0]) < 1e-14
+    for s in (g, o):
+        s.step(10)
+    tol = 1e-10 if prec == api.PREC_FP64 else 1e-6
+    assert rel_l2(g.get("UCAT"), o.get("UCAT")) < tol
+    assert rel_l2(g.get("P"), o.get("P")) < (1e-9 if name == "ohill" and prec == api.PREC_FP64 else tol)
+    g.close(); o.close()
+
+
 def test_unsupported_combinations_are_refused():
     cfg, *_ = build_case("channel", **SMALL["channel"])
     for ddt in (api.DDT_CN, api.DDT_ABCN, api.DDT_RK3WCN, api.DDT_RK3SOCN):
@@ -176,11 +204,22 @@ def test_unsupported_combinations_are_refused():
             tosca_b200.gpu_solver(cfg)
         with pytest.raises(api.TgError):
             oracle.solver(cfg)
+    # the log-law inletFunction on kLeft only, with a unit direction
+    for bad in ({"bc": _bc()[:5] + (api.BC_INLET_LOG,)}, {"inlet_dir": (1.0, 1.0, 0.0)}, {"inlet_z0": -1.0}):
+        cfg, *_ = build_case("channel", **SMALL["channel"])
+        cases.log_inlet(cfg)
+        for k, v in bad.items():
+            setattr(cfg, k, v)
+        with pytest.raises(api.TgError):
+            tosca_b200.gpu_solver(cfg)
     # the adjoint of the inflow/outflow patches is not built
-    cfg, nodes, ucat, p, T = build_case("channel", **SMALL["channel"])
-    cfg.ddt_scheme = api.DDT_RK4
-    g = tosca_b200.gpu_solver(cfg)
-    cases.setup(g, nodes, ucat, p, T)
-    with pytest.raises(api.TgError):
-        g.adjoint_forward(2, 2)
-    g.close()
+    for log in (False, True):
+        cfg, nodes, ucat, p, T = build_case("channel", **SMALL["channel"])
+        cfg.ddt_scheme = api.DDT_RK4
+        if log:
+            cases.log_inlet(cfg)
+        g = tosca_b200.gpu_solver(cfg)
+        cases.setup(g, nodes, ucat, p, T)
+        with pytest.raises(api.TgError):
+            g.adjoint_forward(2, 2)
+        g.close()

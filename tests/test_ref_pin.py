@@ -33,8 +33,9 @@ on the Taylor-Green box, the ABL (Smagorinsky, Schumann wall stress, mean
 pressure gradient), the curvilinear hill (QUICK, Smagorinsky, wall stress),
 an open channel with a fixedValue inflow and a zeroGradient outflow
 (UpdateCartesianBCs and UpdateContravariantBCs for those patches,
-adjustFluxesLocal, ueqn.c:748-1135) and the stratified ABL and hill with the
-thermal wall function.
+adjustFluxesLocal, ueqn.c:748-1135), the kLeft log-law inletFunction
+(boundary.c:1253-1283) on the channel and the open hill, and the stratified
+ABL and hill with the thermal wall function.
 The HYPRE solve inside SolvePEqn is the one stand-in that computes: a tight
 Krylov solve of the captured pinned matrix (unique solution), like the
 oracle's own solve. The reference hard-codes the Smagorinsky constant
@@ -195,6 +196,37 @@ def test_inflow_outflow_steps(wall, div):
     o.close(); r.close()
 
 
+@pytest.mark.parametrize("name,ddt,h_inv", [("channel", api.DDT_RK4, 60.0), ("channel", api.DDT_FE, 60.0),
+                                            ("ohill", api.DDT_RK4, 1e30)])
+def test_log_inlet_steps(name, ddt, h_inv):
+    """The kLeft inletFunction of type 2 (the log-law ghost in the first cell
+    centre's height above the lowest node, boundary.c:1253-1283; grndLevel
+    from SetBoundingBox, mesh.c:2014-2063) in place of the fixedValue inflow:
+    on the channel with hInv = 60 m inside the 100 m domain (both branches of
+    the profile), on the open hill with no inversion; a direction with x and
+    y components. Three steps."""
+    cfg, nodes, ucat, p, T = _cfg(name, ddt_scheme=ddt)
+    cases.log_inlet(cfg, 0.4, 0.1, h_inv, (0.96, 0.28, 0.0))
+    o = oracle.solver(cfg)
+    cases.setup(o, nodes, ucat, p, T)
+    r = R.solver(cfg)
+    r.set_mesh_nodes(nodes)
+    for f in ("UCONT", "UCAT", "P"):
+        r.set(f, o.get(f))
+    for _ in range(3):
+        o.step(1)
+        r.step(1)
+    for f in ("UCONT", "UCAT"):
+        assert rel_l2(r.get(f), o.get(f)) < 1e-12, f
+    assert rel_l2(r.get("P"), o.get("P")) < 1e-10
+    # the ghosts carry the profile: constant above hInv, along the direction
+    g = o.get("UCAT")[0, 1:-1, 1:-1]
+    assert np.allclose(g[..., 1], g[..., 0] * (0.28 / 0.96), rtol=1e-14) and np.all(g[..., 2] == 0.0)
+    if h_inv < 100.0:
+        assert np.isclose(g[..., 0].max(), 0.96 * np.log(h_inv / 0.1), rtol=1e-14)
+    o.close(); r.close()
+
+
 def test_solve_u_balances_the_boundary_flux():
     """SolveUEqn on the channel from the step-start state: the momentum
     update, the outflow faces solved by it (resetNonResolvedCellFaces) and
@@ -220,6 +252,19 @@ def test_unsupported_configuration_is_refused():
     cfg.cs = 0.01               # the reference hard-codes Cs^2 = 0.0289
     with pytest.raises(api.TgError):
         R.solver(cfg)
+    # the log-law inletFunction on kLeft only, with a unit direction
+    for bad in ({"bc": (api.BC_PERIODIC, api.BC_PERIODIC, api.BC_NOSLIP, api.BC_SLIP, api.BC_FIXED_VALUE,
+                        api.BC_INLET_LOG)},
+                {"inlet_dir": (1.0, 1.0, 0.0)}, {"inlet_z0": 0.0}, {"inlet_h_inv": 0.05}):
+        cfg, *_ = _cfg("channel")
+        cases.log_inlet(cfg)
+        for k, v in bad.items():
+            setattr(cfg, k, v)
+        with pytest.raises(api.TgError):
+            oracle.solver(cfg)
+        if "bc" in bad:
+            with pytest.raises(api.TgError):
+                R.solver(cfg)
 
 
 # ---------------------------------------------------------------- temperature

@@ -18,7 +18,7 @@ import numpy as np
 # ------------------------------------------------------------------ constants
 TG_OK, TG_ERR_CUDA, TG_ERR_BAD_ARG, TG_ERR_NOT_CONVERGED, TG_ERR_NAN, TG_ERR_ALLOC, TG_ERR_STATE = range(7)
 
-BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN, BC_FIXED_VALUE, BC_ZERO_GRADIENT = 0, 1, 2, 3, 4, 5
+BC_PERIODIC, BC_NOSLIP, BC_SLIP, BC_WALL_SHUMANN, BC_FIXED_VALUE, BC_ZERO_GRADIENT, BC_INLET_LOG = 0, 1, 2, 3, 4, 5, 6
 NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, NUTBC_FIXEDVALUE = 0, 1, 2
 DIV_CENTRAL, DIV_QUICK = 0, 1
 DDT_FE, DDT_RK4, DDT_CN, DDT_ABCN, DDT_RK3WCN, DDT_RK3SOCN = 0, 1, 2, 3, 4, 5
@@ -94,6 +94,10 @@ class TgConfig(C.Structure):
         ("wall_theta_ref", C.c_double),
         ("t_start", C.c_double),
         ("bc_value", C.c_double * 18),
+        ("inlet_u_tau", C.c_double),
+        ("inlet_z0", C.c_double),
+        ("inlet_h_inv", C.c_double),
+        ("inlet_dir", C.c_double * 3),
     ]
 
 
@@ -208,6 +212,11 @@ class Config:
     t_start: float = 0.0
     # TG_BC_FIXED_VALUE patches: Cartesian velocity of patch p at [3p, 3p + 2]
     bc_value: tuple = (0.0,) * 18
+    # BC_INLET_LOG on kLeft (inletFunction type 2): uTau, roughness, hInv, Udir
+    inlet_u_tau: float = 0.4
+    inlet_z0: float = 0.1
+    inlet_h_inv: float = 1.0e30
+    inlet_dir: tuple = (1.0, 0.0, 0.0)
 
     def to_c(self) -> TgConfig:
         c = TgConfig()

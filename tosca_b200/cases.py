@@ -23,7 +23,7 @@ import math
 
 import numpy as np
 
-from .api import (BC_FIXED_VALUE, BC_NOSLIP, BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, BC_ZERO_GRADIENT, DDT_FE,
+from .api import (BC_FIXED_VALUE, BC_INLET_LOG, BC_NOSLIP, BC_PERIODIC, BC_SLIP, BC_WALL_SHUMANN, BC_ZERO_GRADIENT, DDT_FE,
                   DDT_RK4, DIV_CENTRAL, DIV_QUICK, NUTBC_FIXEDVALUE, NUTBC_PERIODIC, NUTBC_ZEROGRADIENT, TBC_FIXED_GRADIENT, TBC_FIXED_VALUE, TBC_PERIODIC, TBC_WALL_FUNCTION,
                   TBC_ZERO_GRADIENT, TWALL_FIXED_FLUX, TWALL_SHUMANN, Config)
 
@@ -198,6 +198,17 @@ def channel_case(nx: int = 256, ny: int = 128, nz: int = 64, Lx: float = 2560.0,
     cfg, nodes, ucat, p = abl_case(nx=nx, ny=ny, nz=nz, Lx=Lx, Ly=Ly, H=H, wall=wall, **kw)
     open_x(cfg, u_in)
     return cfg, nodes, ucat, p
+
+
+def log_inlet(cfg: Config, u_tau: float = 0.4, z0: float = 0.1, h_inv: float = 1.0e30,
+              direction=(1.0, 0.0, 0.0)) -> Config:
+    """Replaces the x = 0 inflow of an opened case (open_x) by TOSCA's
+    inletFunction type 2: the log-law ghost (u_tau/0.4) ln(h/z0) along
+    `direction` (a unit vector), constant above h_inv."""
+    b = list(cfg.bc); b[4] = BC_INLET_LOG
+    cfg.bc = tuple(b)
+    cfg.inlet_u_tau, cfg.inlet_z0, cfg.inlet_h_inv, cfg.inlet_dir = u_tau, z0, h_inv, tuple(direction)
+    return cfg
 
 
 def open_x(cfg: Config, u_in: float = 8.0, t_in: float = None) -> Config:

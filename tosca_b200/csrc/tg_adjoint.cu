@@ -1185,8 +1185,8 @@ static bool adjoint_supported(tg_ctx *C, std::string &why)
     if (C->cfg.ddt_scheme == TG_DDT_CN) { why = "the adjoint of the Crank-Nicolson scheme is not implemented"; return false; }
     if (imex_scheme(C->cfg.ddt_scheme)) { why = "the adjoint of the IMEX schemes is not implemented"; return false; }
     for (int q = 0; q < 6; q++)
-        if (C->prm.bc[q] == TG_BC_FIXED_VALUE || C->prm.bc[q] == TG_BC_ZERO_GRADIENT) {
-            why = "the adjoint of the inflow/outflow patches (fixedValue, zeroGradient) is not implemented"; return false;
+        if (C->prm.bc[q] >= TG_BC_FIXED_VALUE) {
+            why = "the adjoint of the inflow/outflow patches (fixedValue, zeroGradient, inletFunction) is not implemented"; return false;
         }
     return true;
 }

@@ -219,11 +219,19 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
     *out = nullptr;
     if (cfg->mx < 6 || cfg->my < 6 || cfg->mz < 6) return TG_ERR_BAD_ARG;
     if ((int64_t)cfg->mx * cfg->my * cfg->mz > (int64_t)INT32_MAX / 4) return TG_ERR_BAD_ARG;
-    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_ZERO_GRADIENT) return TG_ERR_BAD_ARG;
+    for (int p = 0; p < 6; p++) if (cfg->bc[p] < 0 || cfg->bc[p] > TG_BC_INLET_LOG) return TG_ERR_BAD_ARG;
     // the inflow/outflow patches with the explicit schemes only
     for (int p = 0; p < 6; p++)
-        if ((cfg->bc[p] == TG_BC_FIXED_VALUE || cfg->bc[p] == TG_BC_ZERO_GRADIENT) &&
-            cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
+        if (cfg->bc[p] >= TG_BC_FIXED_VALUE && cfg->ddt_scheme != TG_DDT_FE && cfg->ddt_scheme != TG_DDT_RK4) return TG_ERR_BAD_ARG;
+    // the log-law inletFunction (type 2) on kLeft: positive roughness, hInv
+    // above it, a unit direction (TOSCA normalises directionU, inflow.c:71)
+    for (int p = 0; p < 6; p++)
+        if (cfg->bc[p] == TG_BC_INLET_LOG) {
+            const double *d = cfg->inlet_dir;
+            const double n = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (p != TG_KLEFT || !(cfg->inlet_z0 > 0) || !(cfg->inlet_u_tau >= 0) || !(cfg->inlet_h_inv > cfg->inlet_z0) ||
+                !(std::fabs(n - 1.0) < 1e-12)) return TG_ERR_BAD_ARG;
+        }
     for (int d = 0; d < 3; d++)
         if ((cfg->bc[2 * d] == TG_BC_PERIODIC) != (cfg->bc[2 * d + 1] == TG_BC_PERIODIC)) return TG_ERR_BAD_ARG;
     for (int p = 0; p < 6; p++) if (cfg->bc[p] == TG_BC_WALL_SHUMANN && p != TG_JLEFT) return TG_ERR_BAD_ARG;
@@ -258,6 +266,9 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         Params &p = C->prm;
         for (int q = 0; q < 6; q++) { p.bc[q] = cfg->bc[q]; p.nut_bc[q] = cfg->nut_bc[q]; p.nut_bc_value[q] = cfg->nut_bc_value[q]; }
         for (int q = 0; q < 18; q++) p.bc_value[q] = cfg->bc_value[q];
+        p.inlet_u_tau = cfg->inlet_u_tau; p.inlet_z0 = cfg->inlet_z0; p.inlet_h_inv = cfg->inlet_h_inv;
+        for (int q = 0; q < 3; q++) p.inlet_dir[q] = cfg->inlet_dir[q];
+        p.grnd = 0.0;
         p.curvilinear = cfg->curvilinear; p.les = cfg->les; p.div_scheme = cfg->div_scheme;
         p.buoyancy = cfg->buoyancy; p.mean_grad_p = cfg->mean_grad_p; p.source = cfg->source;
         p.cs = cfg->cs; p.nu = cfg->nu; p.dt = cfg->dt; p.t_ref = cfg->t_ref;
@@ -350,6 +361,11 @@ tg_status tg_set_mesh_nodes(tg_ctx *C, const double *nodes)
         double *dn = (double *)dalloc(C, 3 * G * sizeof(double));
         TG_CUDA(cudaMemcpyAsync(dn, nodes, 3 * G * sizeof(double), cudaMemcpyHostToDevice, C->stream));
         k_zero_last_nodes<<<grid3(g.mx, g.my, g.mz), block3(), 0, C->stream>>>(g, dn);
+        // mesh->grndLevel (SetBoundingBox, mesh.c:2014-2063): the lowest node
+        double grnd = 1e30;
+        for (int k = 0; k < g.mz - 1; k++) for (int j = 0; j < g.my - 1; j++) for (int i = 0; i < g.mx - 1; i++)
+            grnd = std::min(grnd, nodes[3 * (size_t)g.lin(k, j, i) + 2]);
+        C->prm.grnd = grnd;
         TG_CUDA(cudaStreamSynchronize(C->stream));
         metrics_from_nodes(C, dn);
         refresh_filter(C);

@@ -99,6 +99,9 @@ struct State {
 struct Params {
     int bc[6];
     double bc_value[18];           // TG_BC_FIXED_VALUE: Cartesian velocity of patch p at [3p, 3p+2]
+    // TG_BC_INLET_LOG on kLeft: uTau, roughness, hInv, unit direction, and
+    // the ground level (the lowest mesh node, set with the mesh)
+    double inlet_u_tau, inlet_z0, inlet_h_inv, inlet_dir[3], grnd;
     int nut_bc[6];
     double nut_bc_value[6];
     int curvilinear, les, div_scheme, buoyancy, mean_grad_p, source, farm;

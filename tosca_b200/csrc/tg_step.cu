@@ -179,6 +179,13 @@ __global__ void k_cartesian_bcs(Grid g, Metrics m, State s, Params p)
     } else if (type == TG_BC_FIXED_VALUE) {
         // fixedValue, boundary.c:1632-1673: the ghost takes the patch value
         st3(s.ucat, ghost, R3<double>{p.bc_value[3 * patch], p.bc_value[3 * patch + 1], p.bc_value[3 * patch + 2]});
+    } else if (type == TG_BC_INLET_LOG) {
+        // inletFunction type 2 (kLeft), boundary.c:1253-1283: the log law in
+        // the first cell centre's height above the ground, at least 1e-5,
+        // constant above hInv, along the unit direction
+        const double h = m.cent.z[c] - p.grnd, ks = p.inlet_u_tau / 0.4;
+        const double um = h <= p.inlet_h_inv ? fmax(ks * log(h / p.inlet_z0), 1e-5) : ks * log(p.inlet_h_inv / p.inlet_z0);
+        st3(s.ucat, ghost, R3<double>{um * p.inlet_dir[0], um * p.inlet_dir[1], um * p.inlet_dir[2]});
     } else if (type == TG_BC_ZERO_GRADIENT) {
         // zeroGradient (outflow), boundary.c:1897-1970: linear extrapolation
         // from the first two cells
@@ -996,7 +1003,7 @@ constexpr int AF_BLOCKS = 32;   // pass-1 blocks per patch
 
 __device__ __forceinline__ bool inout_patch(const Params &p, int patch)
 {
-    return p.bc[patch] == TG_BC_FIXED_VALUE || p.bc[patch] == TG_BC_ZERO_GRADIENT;
+    return p.bc[patch] >= TG_BC_FIXED_VALUE;
 }
 // the boundary face (a, b) of a patch (interior range 1..m-2 in both plane
 // directions): its contravariant component array and index
@@ -1369,7 +1376,7 @@ void update_contravariant_bcs(tg_ctx *C)
 void adjust_fluxes(tg_ctx *C)
 {
     bool any = false;
-    for (int q = 0; q < 6; q++) any |= C->prm.bc[q] == TG_BC_FIXED_VALUE || C->prm.bc[q] == TG_BC_ZERO_GRADIENT;
+    for (int q = 0; q < 6; q++) any |= C->prm.bc[q] >= TG_BC_FIXED_VALUE;
     if (!any) return;
     const Grid g = C->g;
     static_assert(6 * AF_BLOCKS * 2 <= 4 * 148 * 4, "partials fit the reduction scratch");
