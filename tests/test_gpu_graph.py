@@ -95,6 +95,28 @@ def test_step_host_replayed():
     e.close(); r.close()
 
 
+def test_step_host_nut_copied_during_the_step():
+    """tg_step_host copies nut out on its own stream from the event recorded
+    after UpdateNut (an external event node inside the replayed step graph):
+    the eager and the replayed drop-in steps return the same nut, bit for
+    bit, equal to the context's own nut after the step (UpdateNut is its only
+    writer), on the LES ABL with the wall function."""
+    e, r = twin("abl", **SMALL["abl"])
+    outs = []
+    for s in (e, r):
+        s.step(1)
+        u, c, p = s.get("UCONT"), s.get("UCAT"), s.get("P")
+        nut = np.full(s.shape, -1.0)
+        for _ in range(4):
+            s.step_host(u, c, p, nut)
+            assert np.array_equal(nut, s.get("NUT"))
+        outs.append((u, c, p, nut))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    assert r.graph_info()[0] == 4
+    e.close(); r.close()
+
+
 def test_graphs_off_then_on():
     e, r = twin("tgv", **SMALL["tgv"])
     e.step(2)

@@ -258,6 +258,8 @@ tg_status tg_create(const tg_config *cfg, tg_ctx **out)
         TG_CUDA(cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking));
         TG_CUDA(cudaEventCreate(&C->ev0));
         TG_CUDA(cudaEventCreate(&C->ev1));
+        // before any step graph is captured, so that every captured step records it
+        if (cfg->les) TG_CUDA(cudaEventCreateWithFlags(&C->ev_nut, cudaEventDisableTiming));
         Grid &g = C->g;
         g.mx = cfg->mx; g.my = cfg->my; g.mz = cfg->mz;
         g.pi = cfg->bc[TG_ILEFT] == TG_BC_PERIODIC;
@@ -347,6 +349,8 @@ tg_status tg_destroy(tg_ctx *C)
     if (C->h_scal) cudaFreeHost(C->h_scal);
     if (C->ev0) cudaEventDestroy(C->ev0);
     if (C->ev1) cudaEventDestroy(C->ev1);
+    if (C->copy_stream) { cudaStreamSynchronize(C->copy_stream); cudaStreamDestroy(C->copy_stream); }
+    if (C->ev_nut) cudaEventDestroy(C->ev_nut);
     if (C->stream) cudaStreamDestroy(C->stream);
     delete C;
     return TG_OK;
@@ -759,7 +763,23 @@ tg_status tg_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double
         upload(C, ucont, halo, C->s.ucont.x, C->s.ucont.y, C->s.ucont.z);
         upload(C, ucat, halo, C->s.ucat.x, C->s.ucat.y, C->s.ucat.z);
         upload(C, p, halo, C->s.p, nullptr, nullptr);
-        // nut is recomputed from Ucat before any read: output only
+        // nut is recomputed from Ucat before any read: output only. It is
+        // final after UpdateNut (the only writer), so it is copied out on the
+        // copy stream from that point while the rest of the step runs.
+        const bool nut_out = nut && C->prm.les && C->ev_nut;
+        const Grid g = C->g;
+        const size_t nn = (size_t)(g.mx + 2 * halo) * (g.my + 2 * halo) * (g.mz + 2 * halo);
+        if (nut_out) {
+            if (!C->copy_stream) TG_CUDA(cudaStreamCreateWithFlags(&C->copy_stream, cudaStreamNonBlocking));
+            if (C->stage_nut_bytes < nn * sizeof(double)) {
+                TG_CUDA(cudaStreamSynchronize(C->copy_stream));
+                C->stage_nut = (double *)dalloc(C, nn * sizeof(double));
+                C->stage_nut_bytes = nn * sizeof(double);
+            }
+            // keep the caller's halo entries: start from the caller's array
+            if (halo > 0)
+                TG_CUDA(cudaMemcpyAsync(C->stage_nut, nut, nn * sizeof(double), cudaMemcpyHostToDevice, C->copy_stream));
+        }
         tg_stats local{};
         tg_stats *s = st ? st : &local;
         *s = tg_stats{};
@@ -767,10 +787,16 @@ tg_status tg_step_host(tg_ctx *C, double *ucont, double *ucat, double *p, double
         bool rep = false;
         int rc = step(C, s, &rep);
         s->steps = 1;
+        if (nut_out) {
+            TG_CUDA(cudaStreamWaitEvent(C->copy_stream, C->ev_nut, 0));
+            k_soa_to_aos<<<grid3(g.mx, g.my, g.mz), block3(), 0, C->copy_stream>>>(g, C->stage_nut, halo, C->s.nut, nullptr, nullptr);
+            TG_CUDA(cudaGetLastError());
+            TG_CUDA(cudaMemcpyAsync(nut, C->stage_nut, nn * sizeof(double), cudaMemcpyDeviceToHost, C->copy_stream));
+        }
         download(C, ucont, halo, C->s.ucont.x, C->s.ucont.y, C->s.ucont.z);
         download(C, ucat, halo, C->s.ucat.x, C->s.ucat.y, C->s.ucat.z);
         download(C, p, halo, C->s.p, nullptr, nullptr);
-        if (nut && C->prm.les) download(C, nut, halo, C->s.nut, nullptr, nullptr);
+        if (nut_out) TG_CUDA(cudaStreamSynchronize(C->copy_stream));
         const int gr = step_stats_read(C, s, rep, rep);
         if (rep) rc = gr;
         s->max_divergence = C->h_scal[16];

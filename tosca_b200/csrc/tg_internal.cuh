@@ -172,6 +172,12 @@ struct tg_ctx {
     double *h_scal = nullptr;            // pinned host mirror of scalars
     double *stage = nullptr;             // staging buffer for AoS host transfers
     size_t stage_bytes = 0;
+    // tg_step_host's early nut download: nut is final once UpdateNut has run,
+    // so its copy overlaps the rest of the step on its own stream and buffer
+    cudaEvent_t ev_nut = nullptr;        // recorded after UpdateNut (an external event node in the step graph)
+    cudaStream_t copy_stream = nullptr;
+    double *stage_nut = nullptr;
+    size_t stage_nut_bytes = 0;
     int red_blocks = 0;
     bool has_mesh = false;
     bool orthogonal = true;              // all cross metric-tensor terms vanish

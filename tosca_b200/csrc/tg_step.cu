@@ -1710,7 +1710,13 @@ static int step_body(tg_ctx *C, tg_stats *st, bool capture)
             TG_CUDA(cudaMemcpyAsync(C->tmprt_oo, C->s.tmprt_o, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
         TG_CUDA(cudaMemcpyAsync(C->s.tmprt_o, C->s.tmprt, sizeof(double) * G, cudaMemcpyDeviceToDevice, C->stream));
     }
-    if (C->prm.les) { update_nut(C); update_wall_models(C); }
+    if (C->prm.les) {
+        update_nut(C);
+        // nut is final for the step: tg_step_host copies it out from here
+        if (C->ev_nut)
+            TG_CUDA(cudaEventRecordWithFlags(C->ev_nut, C->stream, capture ? cudaEventRecordExternal : cudaEventRecordDefault));
+        update_wall_models(C);
+    }
     if (C->taping) tape_nut(C);
     if (C->prm.farm) farm_update(C);
     grad_p(C);
